@@ -1,0 +1,76 @@
+"""Cedar's JSON configuration (``cedar::config``, include/cedar/config.h:12-110).
+
+``get(path, default)`` reads a dotted path such as ``"solver.cycle.nrelax-pre"``.
+Keys and defaults are those of ``ml_settings::init`` (src/multilevel_settings.cc:15-61);
+note that the reference reads ``solver.min_coarse`` (underscore), so the
+``"min-coarse"`` key found in its example configs has no effect there or here.
+GPU options live under the ``"gpu"`` object: ``precision`` ("fp64" | "fp32-ir")
+and ``graph`` (bool).
+"""
+import json
+import os
+
+
+class Config:
+    def __init__(self, src=None):
+        if src is None:
+            self.tree = {}
+        elif isinstance(src, dict):
+            self.tree = src
+        elif isinstance(src, str) and os.path.exists(src):
+            with open(src) as f:
+                self.tree = json.load(f)
+        elif isinstance(src, str) and src == "":
+            self.tree = {}  # config("") is an empty in-memory config (src/config.cc:11-17)
+        else:
+            raise FileNotFoundError(src)
+
+    def get(self, path, default=None):
+        node = self.tree
+        for part in path.split("."):
+            if not isinstance(node, dict) or part not in node:
+                return default
+            node = node[part]
+        return node
+
+    def getconf(self, path):
+        sub = self.get(path)
+        return Config(sub) if isinstance(sub, dict) else None
+
+    def getvec(self, path):
+        return list(self.get(path, []))
+
+
+RELAX_NAMES = ["point", "line-x", "line-y", "line-xy", "plane-xy", "plane-xz", "plane-yz", "plane-xyz"]
+
+
+class MLSettings:
+    """``ml_settings`` (include/cedar/multilevel_settings.h:28-50)."""
+
+    def __init__(self, conf=None):
+        conf = conf if isinstance(conf, Config) else Config(conf)
+        self.relaxation = conf.get("solver.relaxation", "point")
+        if self.relaxation not in RELAX_NAMES:
+            raise ValueError("invalid relaxation type: %s" % self.relaxation)
+        self.cycle = conf.get("solver.cycle.type", "v")
+        if self.cycle not in ("v", "f"):
+            raise ValueError("invalid cycle type: %s" % self.cycle)
+        self.nrelax_pre = int(conf.get("solver.cycle.nrelax-pre", 2))
+        self.nrelax_post = int(conf.get("solver.cycle.nrelax-post", 1))
+        self.num_levels = int(conf.get("solver.num-levels", -1))
+        self.maxiter = int(conf.get("solver.max-iter", 10))
+        self.tol = float(conf.get("solver.tol", 1e-8))
+        self.min_coarse = int(conf.get("solver.min_coarse", 3))
+        self.coarse_solver = conf.get("solver.cg-solver", "LU")
+        if self.coarse_solver not in ("LU", "cedar", "redist"):
+            raise ValueError("invalid value for solver.cg-solver")
+        self.precision = conf.get("gpu.precision", "fp64")
+        if self.precision not in ("fp64", "fp32-ir"):
+            raise ValueError("invalid gpu.precision: %s" % self.precision)
+        self.use_graph = bool(conf.get("gpu.graph", True))
+
+    def __repr__(self):
+        return ("MLSettings(relaxation=%r, cycle=%r, nrelax=(%d,%d), num_levels=%d, maxiter=%d, "
+                "tol=%g, min_coarse=%d, precision=%r)" % (
+                    self.relaxation, self.cycle, self.nrelax_pre, self.nrelax_post, self.num_levels,
+                    self.maxiter, self.tol, self.min_coarse, self.precision))

@@ -1,0 +1,290 @@
+// k2_lines.cu -- zebra line Gauss-Seidel for 2D BoxMG on sm_100a.
+//
+// The reference forms each line's right-hand side from the two neighbouring
+// lines and calls LAPACK DPTTRS on the line's L*D*L^T factors
+// (src/2d/ftn/BMG2_SymStd_relax_lines_x.f90:99-131, ..._y.f90:95-129).  Here one
+// CTA owns G whole lines of one colour:
+//   1. the right-hand sides are formed with coalesced loads into shared memory
+//      (x-lines: consecutive threads walk i; y-lines: consecutive threads walk
+//      the G lines of a row, so each row segment is one or two 128-byte lines);
+//   2. the two substitutions of DPTTRS, y(i) = r(i) - y(i-1) e(i) and
+//      x(i) = y(i)/d(i) - x(i+1) e(i+1), are first-order affine recurrences.
+//      Each of the 256/G threads of a line composes the affine map of its
+//      contiguous chunk, a segmented scan over the chunk maps gives every chunk
+//      its incoming value, and the chunk is then re-run with the exact LAPACK
+//      update (so every element sees the DPTTS2 operation on its inputs);
+//   3. the solution is written back with the coalesced mapping of step 1.
+// Both colours of a sweep are two launches: lines of one colour read only lines
+// of the other colour.
+#include "cdr_common.cuh"
+
+namespace cdrgpu {
+
+constexpr int LT = 256;  // threads per CTA
+
+// ------------------------------------------------------------------ setup
+// BMG2_SymStd_SETUP_lines_{x,y} + DPTTRF: per line d = c, e = -w (x) or -s (y),
+// then e(i) <- e(i)/d(i-1), d(i) <- d(i) - e(i)*e_old(i).  Always FP64; TS is
+// the storage type of the factors.
+template <typename TS, int DIR>
+__global__ void k_lines_setup(const double *__restrict__ so, TS *__restrict__ sor, Dims2 d, int tpitch,
+                              int *__restrict__ info)
+{
+	const int line = blockIdx.x * blockDim.x + threadIdx.x + 1;
+	const int nl = DIR == CDR_DIR_X ? d.ny : d.nx;
+	const int n = DIR == CDR_DIR_X ? d.nx : d.ny;
+	if (line > nl) return;
+	const size_t ps = d.plane();
+	const double *c = so, *off = so + (DIR == CDR_DIR_X ? 1 : 2) * ps;
+	// element at line position p (1..n): grid offset and factor offset
+	auto g = [&](int p) -> size_t { return DIR == CDR_DIR_X ? d.at(p, line) : d.at(line, p); };
+	const size_t fps = DIR == CDR_DIR_X ? ps : (size_t)tpitch * (d.nx + 2);
+	auto fo = [&](int p) -> size_t { return DIR == CDR_DIR_X ? d.at(p, line) : (size_t)line * tpitch + p; };
+	double dprev = c[g(1)];
+	sor[fo(1)] = (TS)dprev;
+	sor[fps + fo(1)] = (TS)(-off[g(1)]);
+	int st = 0;
+	for (int p = 1; p < n; ++p) {
+		if (dprev <= 0.0 && !st) st = p;
+		double ei = -off[g(p + 1)];
+		double e = ei / dprev;
+		double dn = c[g(p + 1)] - e * ei;
+		sor[fps + fo(p + 1)] = (TS)e;
+		sor[fo(p + 1)] = (TS)dn;
+		dprev = dn;
+	}
+	if (dprev <= 0.0 && !st) st = n;
+	if (st && info) atomicCAS(info, 0, line);
+}
+
+template <typename TS>
+int setup_lines_2d(const double *so, int nstencil, TS *sor, Dims2 d, int tpitch, int dir, int *info, cudaStream_t st)
+{
+	(void)nstencil;
+	if (dir == CDR_DIR_Y && tpitch < d.ny + 2) {
+		set_error(CDR_ERR_DIM, "y-line factor pitch %d < ny+2 = %d", tpitch, d.ny + 2);
+		return CDR_ERR_DIM;
+	}
+	const int nl = dir == CDR_DIR_X ? d.ny : d.nx;
+	if (dir == CDR_DIR_X) k_lines_setup<TS, CDR_DIR_X><<<ceil_div(nl, 128), 128, 0, st>>>(so, sor, d, tpitch, info);
+	else k_lines_setup<TS, CDR_DIR_Y><<<ceil_div(nl, 128), 128, 0, st>>>(so, sor, d, tpitch, info);
+	CDR_LAUNCH_CHECK();
+	return CDR_OK;
+}
+template int setup_lines_2d<double>(const double *, int, double *, Dims2, int, int, int *, cudaStream_t);
+template int setup_lines_2d<float>(const double *, int, float *, Dims2, int, int, int *, cudaStream_t);
+
+// ------------------------------------------------------------------ relax
+// Right-hand side of line relaxation at (i, j): b plus the couplings to the two
+// neighbouring lines (operand order of the reference).
+template <typename T, int NS, int DIR>
+__device__ __forceinline__ T line_rhs(const T *__restrict__ so, size_t ps, const T *__restrict__ q,
+                                      const T *__restrict__ qf, size_t k, int p)
+{
+	const T *w = so + ps, *s = so + 2 * ps;
+	if (DIR == CDR_DIR_X) {
+		if (NS == 5) {
+			const T *sw = so + 3 * ps, *nw = so + 4 * ps;
+			return qf[k] + s[k] * q[k - p] + s[k + p] * q[k + p] + sw[k] * q[k - p - 1] + nw[k + 1] * q[k - p + 1]
+			       + nw[k + p] * q[k + p - 1] + sw[k + p + 1] * q[k + p + 1];
+		}
+		return qf[k] + s[k] * q[k - p] + s[k + p] * q[k + p];
+	} else {
+		if (NS == 5) {
+			const T *sw = so + 3 * ps, *nw = so + 4 * ps;
+			return qf[k] + w[k] * q[k - 1] + w[k + 1] * q[k + 1] + sw[k] * q[k - p - 1] + nw[k + 1] * q[k - p + 1]
+			       + nw[k + p] * q[k + p - 1] + sw[k + p + 1] * q[k + p + 1];
+		}
+		return qf[k] + w[k] * q[k - 1] + w[k + 1] * q[k + 1];
+	}
+}
+
+// Segmented inclusive scan of affine maps over the tpl threads of a line.
+// forward: element t composes (later) t o (earlier) t-off; backward: t o t+off.
+template <typename T>
+__device__ __forceinline__ void affine_scan(T &A, T &B, T *sA, T *sB, int t, int tpl, bool forward)
+{
+	const int tid = threadIdx.x;
+	for (int off = 1; off < tpl; off <<= 1) {
+		sA[tid] = A;
+		sB[tid] = B;
+		__syncthreads();
+		if (forward ? t >= off : t + off < tpl) {
+			int o = forward ? tid - off : tid + off;
+			T a2 = sA[o], b2 = sB[o];
+			B = A * b2 + B;
+			A = A * a2;
+		}
+		__syncthreads();
+	}
+	sA[tid] = A;
+	sB[tid] = B;
+	__syncthreads();
+}
+
+template <typename T, int NS, int DIR>
+__global__ void __launch_bounds__(LT) k_lines(const T *__restrict__ so, T *__restrict__ q, const T *__restrict__ qf,
+                                              const T *__restrict__ sor, Dims2 d, int tpitch, int first, int G)
+{
+	extern __shared__ __align__(16) unsigned char smem_raw[];
+	T *sA = reinterpret_cast<T *>(smem_raw);
+	T *sB = sA + LT;
+	T *buf = sB + LT;
+	const size_t ps = d.plane();
+	const int p = d.pitch;
+	const int n = DIR == CDR_DIR_X ? d.nx : d.ny;     // line length
+	const int nl = DIR == CDR_DIR_X ? d.ny : d.nx;    // lines in the grid
+	const int l0 = blockIdx.x * G;                    // first line (of this colour) of the CTA
+	auto line_coord = [&](int g) { return first + 2 * (l0 + g); };
+	int gmax = G;
+	while (gmax > 0 && line_coord(gmax - 1) > nl) --gmax;
+
+	// 1. right-hand sides
+	for (int idx = threadIdx.x; idx < gmax * n; idx += LT) {
+		int g, m;
+		if (DIR == CDR_DIR_X) { g = idx / n; m = idx - g * n; }
+		else { m = idx / gmax; g = idx - m * gmax; }
+		int lc = line_coord(g);
+		size_t k = DIR == CDR_DIR_X ? d.at(m + 1, lc) : d.at(lc, m + 1);
+		buf[g * n + m] = line_rhs<T, NS, DIR>(so, ps, q, qf, k, p);
+	}
+	__syncthreads();
+
+	// 2. substitutions
+	const int tpl = LT / G;
+	const int g = threadIdx.x / tpl, t = threadIdx.x - g * tpl;
+	const int K = (n + tpl - 1) / tpl;
+	const int lo = t * K < n ? t * K : n, hi = lo + K < n ? lo + K : n;
+	const bool active = g < gmax;
+	const int lc = active ? line_coord(g) : 1;
+	const T *D, *E;
+	if (DIR == CDR_DIR_X) {
+		D = sor + (size_t)lc * p;
+		E = sor + ps + (size_t)lc * p;
+	} else {
+		D = sor + (size_t)lc * tpitch;
+		E = sor + (size_t)tpitch * (d.nx + 2) + (size_t)lc * tpitch;
+	}
+	T *r = buf + g * n;  // r[m] is line position m+1
+	// forward: y(m) = r(m) - y(m-1) * E(m+1)
+	T A = T(1), B = T(0);
+	if (active)
+		for (int m = lo; m < hi; ++m) {
+			T a = m == 0 ? T(0) : -E[m + 1];
+			B = a * B + r[m];
+			A = a * A;
+		}
+	affine_scan<T>(A, B, sA, sB, t, tpl, true);
+	if (active) {
+		T y = t == 0 ? T(0) : sB[threadIdx.x - 1];
+		for (int m = lo; m < hi; ++m) {
+			y = m == 0 ? r[0] : r[m] - y * E[m + 1];
+			r[m] = y;
+		}
+	}
+	__syncthreads();
+	// backward: x(m) = y(m)/D(m+1) - x(m+1) * E(m+2)
+	A = T(1);
+	B = T(0);
+	if (active)
+		for (int m = hi - 1; m >= lo; --m) {
+			T a = m == n - 1 ? T(0) : -E[m + 2];
+			B = a * B + r[m] / D[m + 1];
+			A = a * A;
+		}
+	affine_scan<T>(A, B, sA, sB, t, tpl, false);
+	if (active) {
+		T x = t == tpl - 1 ? T(0) : sB[threadIdx.x + 1];
+		for (int m = hi - 1; m >= lo; --m) {
+			x = m == n - 1 ? r[m] / D[m + 1] : r[m] / D[m + 1] - x * E[m + 2];
+			r[m] = x;
+		}
+	}
+	__syncthreads();
+
+	// 3. write back
+	for (int idx = threadIdx.x; idx < gmax * n; idx += LT) {
+		int gg, m;
+		if (DIR == CDR_DIR_X) { gg = idx / n; m = idx - gg * n; }
+		else { m = idx / gmax; gg = idx - m * gmax; }
+		int c2 = line_coord(gg);
+		size_t k = DIR == CDR_DIR_X ? d.at(m + 1, c2) : d.at(c2, m + 1);
+		q[k] = buf[gg * n + m];
+	}
+}
+
+// Opt every line kernel into the large dynamic shared-memory carve-out once per
+// process (before any graph capture: the solver calls this at creation).
+int lines_prepare()
+{
+	static bool done = false;
+	if (done) return CDR_OK;
+	const int big = 227 * 1024;
+	CDR_CUDA_TRY(cudaFuncSetAttribute(k_lines<double, 5, CDR_DIR_X>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+	CDR_CUDA_TRY(cudaFuncSetAttribute(k_lines<double, 5, CDR_DIR_Y>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+	CDR_CUDA_TRY(cudaFuncSetAttribute(k_lines<double, 3, CDR_DIR_X>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+	CDR_CUDA_TRY(cudaFuncSetAttribute(k_lines<double, 3, CDR_DIR_Y>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+	CDR_CUDA_TRY(cudaFuncSetAttribute(k_lines<float, 5, CDR_DIR_X>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+	CDR_CUDA_TRY(cudaFuncSetAttribute(k_lines<float, 5, CDR_DIR_Y>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+	CDR_CUDA_TRY(cudaFuncSetAttribute(k_lines<float, 3, CDR_DIR_X>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+	CDR_CUDA_TRY(cudaFuncSetAttribute(k_lines<float, 3, CDR_DIR_Y>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+	done = true;
+	return CDR_OK;
+}
+
+// Lines per CTA: the largest power of two with G*n*sizeof(T) within the shared
+// memory budget (x-lines: small, rows are contiguous; y-lines: at least 4 lines
+// so that each row segment read is a useful 32-byte sector group).
+template <typename T>
+static int lines_per_cta(int n, int dir)
+{
+	const size_t budget = dir == CDR_DIR_X ? 32 * 1024 : (sizeof(T) == 8 ? 68 * 1024 : 68 * 1024);
+	int G = 1;
+	while (G < 32 && (size_t)(2 * G) * n * sizeof(T) <= budget) G *= 2;
+	return G;
+}
+
+template <typename T, int NS, int DIR>
+static int launch_lines(const T *so, T *x, const T *b, const T *sor, Dims2 d, int tpitch, int first, cudaStream_t st)
+{
+	const int n = DIR == CDR_DIR_X ? d.nx : d.ny;
+	const int nl = DIR == CDR_DIR_X ? d.ny : d.nx;
+	const int G = lines_per_cta<T>(n, DIR);
+	const int nlines = first > nl ? 0 : (nl - first) / 2 + 1;
+	if (nlines == 0) return CDR_OK;
+	size_t smem = sizeof(T) * (2 * LT + (size_t)G * n);
+	if (smem > 227 * 1024) {
+		set_error(CDR_ERR_DIM, "line length %d too long for one CTA", n);
+		return CDR_ERR_DIM;
+	}
+	CDR_TRY(lines_prepare());
+	k_lines<T, NS, DIR><<<ceil_div(nlines, G), LT, smem, st>>>(so, x, b, sor, d, tpitch, first, G);
+	CDR_LAUNCH_CHECK();
+	return CDR_OK;
+}
+
+template <typename T>
+int relax_lines_2d(const T *so, int nstencil, T *x, const T *b, const T *sor, Dims2 d, int tpitch, int dir,
+                   int updown, cudaStream_t st)
+{
+	// DOWN: lines with Fortran start index 3 (0-based even) first, then 2 (odd);
+	// UP: the opposite (relax_lines_x.f90:82-97).
+	const int firsts[2] = {updown == CDR_DOWN ? 2 : 1, updown == CDR_DOWN ? 1 : 2};
+	for (int c = 0; c < 2; ++c) {
+		int f = firsts[c];
+		if (dir == CDR_DIR_X) {
+			if (nstencil == 5) CDR_TRY((launch_lines<T, 5, CDR_DIR_X>(so, x, b, sor, d, tpitch, f, st)));
+			else CDR_TRY((launch_lines<T, 3, CDR_DIR_X>(so, x, b, sor, d, tpitch, f, st)));
+		} else {
+			if (nstencil == 5) CDR_TRY((launch_lines<T, 5, CDR_DIR_Y>(so, x, b, sor, d, tpitch, f, st)));
+			else CDR_TRY((launch_lines<T, 3, CDR_DIR_Y>(so, x, b, sor, d, tpitch, f, st)));
+		}
+	}
+	return CDR_OK;
+}
+template int relax_lines_2d<double>(const double *, int, double *, const double *, const double *, Dims2, int, int,
+                                    int, cudaStream_t);
+template int relax_lines_2d<float>(const float *, int, float *, const float *, const float *, Dims2, int, int, int,
+                                   cudaStream_t);
+
+}  // namespace cdrgpu

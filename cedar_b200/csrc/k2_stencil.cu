@@ -1,0 +1,669 @@
+// k2_stencil.cu -- 2D BoxMG point kernels for sm_100a.
+//
+// All kernels are HBM-bandwidth bound stencil sweeps: one thread per output
+// point, coalesced along i, no tensor cores.  Arithmetic is written in the
+// reference's operand order and the library is compiled without FMA
+// contraction, so residual, point Gauss-Seidel, restriction, interpolation and
+// the interpolation setup give the same bits as Cedar's serial kernels.
+#include "cdr_common.cuh"
+
+namespace cdrgpu {
+
+constexpr int TX = 32, TY = 8;
+constexpr int NORM_MAX_BLOCKS = 2048;
+
+// ------------------------------------------------------------------ residual
+// BMG2_SymStd_residual (src/2d/ftn/BMG2_SymStd_residual.f90:89-117).
+template <typename T, int NS>
+__device__ __forceinline__ T resid_at(const T *__restrict__ so, size_t ps, const T *__restrict__ q,
+                                      const T *__restrict__ qf, size_t k, int pitch)
+{
+	const T *c = so, *w = so + ps, *s = so + 2 * ps;
+	if (NS == 5) {
+		const T *sw = so + 3 * ps, *nw = so + 4 * ps;
+		return qf[k] + w[k] * q[k - 1] + w[k + 1] * q[k + 1] + s[k] * q[k - pitch] + s[k + pitch] * q[k + pitch]
+		       + sw[k] * q[k - pitch - 1] + nw[k + 1] * q[k - pitch + 1] + nw[k + pitch] * q[k + pitch - 1]
+		       + sw[k + pitch + 1] * q[k + pitch + 1] - c[k] * q[k];
+	} else {
+		return qf[k] + w[k] * q[k - 1] + w[k + 1] * q[k + 1] + s[k] * q[k - pitch] + s[k + pitch] * q[k + pitch]
+		       - c[k] * q[k];
+	}
+}
+
+template <int NW>
+__device__ __forceinline__ double block_sum(double v, double *sh)
+{
+	for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+	int lane = (threadIdx.y * blockDim.x + threadIdx.x) & 31;
+	int warp = (threadIdx.y * blockDim.x + threadIdx.x) >> 5;
+	if (lane == 0) sh[warp] = v;
+	__syncthreads();
+	double t = 0;
+	if (warp == 0) {
+		t = lane < NW ? sh[lane] : 0.0;
+		for (int o = 16; o > 0; o >>= 1) t += __shfl_down_sync(0xffffffffu, t, o);
+	}
+	return t;
+}
+
+// Grid-stride over 32x8 tiles; with NORM each block leaves the sum of r^2 over
+// its tiles in partial[blockIdx.x] (fixed tile->block map: deterministic).
+template <typename T, int NS, bool NORM>
+__global__ void __launch_bounds__(TX *TY) k_residual(const T *__restrict__ so, const T *__restrict__ q,
+                                                     const T *__restrict__ qf, T *__restrict__ res, Dims2 d,
+                                                     double *__restrict__ partial)
+{
+	__shared__ double sh[TX * TY / 32];
+	const int tiles_x = (d.nx + TX - 1) / TX;
+	const int ntiles = tiles_x * ((d.ny + TY - 1) / TY);
+	const size_t ps = d.plane();
+	double acc = 0.0;
+	for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+		int i = (t % tiles_x) * TX + threadIdx.x + 1;
+		int j = (t / tiles_x) * TY + threadIdx.y + 1;
+		if (i <= d.nx && j <= d.ny) {
+			size_t k = d.at(i, j);
+			T r = resid_at<T, NS>(so, ps, q, qf, k, d.pitch);
+			res[k] = r;
+			if (NORM) acc += (double)r * (double)r;
+		}
+	}
+	if (NORM) {
+		double s = block_sum<TX * TY / 32>(acc, sh);
+		if (threadIdx.x == 0 && threadIdx.y == 0) partial[blockIdx.x] = s;
+	}
+}
+
+__global__ void __launch_bounds__(1024) k_norm_finish(const double *__restrict__ partial, int n, double *out)
+{
+	__shared__ double sh[32];
+	double v = 0;
+	for (int i = threadIdx.x; i < n; i += blockDim.x) v += partial[i];
+	for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+	if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = v;
+	__syncthreads();
+	if (threadIdx.x < 32) {
+		v = sh[threadIdx.x];
+		for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+		if (threadIdx.x == 0) *out = sqrt(v);
+	}
+}
+
+template <typename T>
+int residual_2d(const T *so, int nstencil, const T *x, const T *b, T *r, Dims2 d, double *norm_out,
+                double *partial, cudaStream_t st)
+{
+	const int ntiles = ceil_div(d.nx, TX) * ceil_div(d.ny, TY);
+	dim3 blk(TX, TY);
+	if (norm_out) {
+		int nb = ntiles < NORM_MAX_BLOCKS ? ntiles : NORM_MAX_BLOCKS;
+		if (nstencil == 5) k_residual<T, 5, true><<<nb, blk, 0, st>>>(so, x, b, r, d, partial);
+		else k_residual<T, 3, true><<<nb, blk, 0, st>>>(so, x, b, r, d, partial);
+		CDR_LAUNCH_CHECK();
+		k_norm_finish<<<1, 1024, 0, st>>>(partial, nb, norm_out);
+	} else {
+		if (nstencil == 5) k_residual<T, 5, false><<<ntiles, blk, 0, st>>>(so, x, b, r, d, nullptr);
+		else k_residual<T, 3, false><<<ntiles, blk, 0, st>>>(so, x, b, r, d, nullptr);
+	}
+	CDR_LAUNCH_CHECK();
+	return CDR_OK;
+}
+template int residual_2d<double>(const double *, int, const double *, const double *, double *, Dims2, double *,
+                                 double *, cudaStream_t);
+template int residual_2d<float>(const float *, int, const float *, const float *, float *, Dims2, double *,
+                                double *, cudaStream_t);
+
+// ------------------------------------------------------------ point smoother
+// BMG2_SymStd_SETUP_recip (src/2d/ftn/BMG2_SymStd_SETUP_recip.f90:63-67).
+template <typename T>
+__global__ void k_recip(const T *__restrict__ so, T *__restrict__ sor, Dims2 d)
+{
+	int i = blockIdx.x * TX + threadIdx.x + 1, j = blockIdx.y * TY + threadIdx.y + 1;
+	if (i <= d.nx && j <= d.ny) sor[d.at(i, j)] = T(1) / so[d.at(i, j)];
+}
+
+template <typename T>
+int setup_recip_2d(const T *so, T *sor, Dims2 d, cudaStream_t st)
+{
+	k_recip<T><<<dim3(ceil_div(d.nx, TX), ceil_div(d.ny, TY)), dim3(TX, TY), 0, st>>>(so, sor, d);
+	CDR_LAUNCH_CHECK();
+	return CDR_OK;
+}
+template int setup_recip_2d<double>(const double *, double *, Dims2, cudaStream_t);
+template int setup_recip_2d<float>(const float *, float *, Dims2, cudaStream_t);
+
+// One colour of BMG2_SymStd_relax_GS (src/2d/ftn/BMG2_SymStd_relax_GS.f90:93-133).
+// 5-point: points with (i + j) % 2 == par (red-black); 9-point: points with
+// i % 2 == pi and j % 2 == pj (four colours).  Points of one colour are
+// independent, so one launch per colour reproduces the sequential sweep.
+template <typename T, int NS>
+__global__ void __launch_bounds__(TX *TY) k_gs_colour(const T *__restrict__ so, T *__restrict__ q,
+                                                      const T *__restrict__ qf, const T *__restrict__ sor,
+                                                      Dims2 d, int pi, int pj)
+{
+	const size_t ps = d.plane();
+	const int pitch = d.pitch;
+	int j, i;
+	if (NS == 3) {
+		j = blockIdx.y * TY + threadIdx.y + 1;
+		int i0 = ((1 + j) & 1) == pi ? 1 : 2;  // pi carries the (i+j) parity here
+		i = i0 + 2 * (blockIdx.x * TX + threadIdx.x);
+	} else {
+		j = (pj ? 1 : 2) + 2 * (blockIdx.y * TY + threadIdx.y);
+		i = (pi ? 1 : 2) + 2 * (blockIdx.x * TX + threadIdx.x);
+	}
+	if (i > d.nx || j > d.ny) return;
+	size_t k = d.at(i, j);
+	const T *w = so + ps, *s = so + 2 * ps;
+	T acc;
+	if (NS == 5) {
+		const T *sw = so + 3 * ps, *nw = so + 4 * ps;
+		acc = qf[k] + w[k] * q[k - 1] + w[k + 1] * q[k + 1] + s[k] * q[k - pitch] + s[k + pitch] * q[k + pitch]
+		      + sw[k] * q[k - pitch - 1] + nw[k + 1] * q[k - pitch + 1] + nw[k + pitch] * q[k + pitch - 1]
+		      + sw[k + pitch + 1] * q[k + pitch + 1];
+	} else {
+		acc = qf[k] + w[k] * q[k - 1] + w[k + 1] * q[k + 1] + s[k] * q[k - pitch] + s[k + pitch] * q[k + pitch];
+	}
+	q[k] = acc * sor[k];
+}
+
+template <typename T>
+int relax_point_2d(const T *so, int nstencil, T *x, const T *b, const T *sor, Dims2 d, int updown,
+                   cudaStream_t st)
+{
+	dim3 blk(TX, TY);
+	if (nstencil == 5) {
+		// DOWN: (JBEG, IBEG) = (2,2),(2,3),(3,2),(3,3) with JBEG outer; UP reversed.
+		// Fortran index 2 is 0-based 1 (odd), 3 is 0-based 2 (even).
+		const int order[4][2] = {{1, 1}, {1, 0}, {0, 1}, {0, 0}};  // (j odd?, i odd?)
+		dim3 grd(ceil_div((d.nx + 1) / 2, TX), ceil_div((d.ny + 1) / 2, TY));
+		for (int c = 0; c < 4; ++c) {
+			int o = updown == CDR_DOWN ? c : 3 - c;
+			k_gs_colour<T, 5><<<grd, blk, 0, st>>>(so, x, b, sor, d, order[o][1], order[o][0]);
+			CDR_LAUNCH_CHECK();
+		}
+	} else {
+		// DOWN: JO = 2 then 3; a point is swept in pass JO when (I + J + JO) is even,
+		// i.e. 0-based (i + j) even first, odd second.  UP reversed.
+		dim3 grd(ceil_div((d.nx + 1) / 2, TX), ceil_div(d.ny, TY));
+		for (int c = 0; c < 2; ++c) {
+			int par = updown == CDR_DOWN ? c : 1 - c;
+			k_gs_colour<T, 3><<<grd, blk, 0, st>>>(so, x, b, sor, d, par, 0);
+			CDR_LAUNCH_CHECK();
+		}
+	}
+	return CDR_OK;
+}
+template int relax_point_2d<double>(const double *, int, double *, const double *, const double *, Dims2, int,
+                                    cudaStream_t);
+template int relax_point_2d<float>(const float *, int, float *, const float *, const float *, Dims2, int,
+                                   cudaStream_t);
+
+// ---------------------------------------------------------------- restriction
+// BMG2_SymStd_restrict (src/2d/ftn/BMG2_SymStd_restrict.f90:72-92): coarse
+// (ic, jc) sits on fine (2ic-1, 2jc-1) (0-based, ghosts at 0).
+template <typename T>
+__global__ void __launch_bounds__(TX *TY) k_restrict(const T *__restrict__ ci, const T *__restrict__ q,
+                                                     T *__restrict__ qc, Dims2 f, Dims2 c)
+{
+	int ic = blockIdx.x * TX + threadIdx.x + 1, jc = blockIdx.y * TY + threadIdx.y + 1;
+	if (ic > c.nx || jc > c.ny) return;
+	const size_t cps = c.plane();
+	const int cp = c.pitch, fp = f.pitch;
+	size_t kc = c.at(ic, jc), kf = f.at(2 * ic - 1, 2 * jc - 1);
+	const T *cL = ci + IL * cps, *cR = ci + IR * cps, *cA = ci + IA * cps, *cB = ci + IB * cps;
+	const T *cSW = ci + ISW * cps, *cNW = ci + INW * cps, *cNE = ci + INE * cps, *cSE = ci + ISE * cps;
+	qc[kc] = cNE[kc] * q[kf - fp - 1] + cA[kc] * q[kf - fp] + cNW[kc + 1] * q[kf - fp + 1] + cR[kc] * q[kf - 1]
+	         + q[kf] + cL[kc + 1] * q[kf + 1] + cSE[kc + cp] * q[kf + fp - 1] + cB[kc + cp] * q[kf + fp]
+	         + cSW[kc + cp + 1] * q[kf + fp + 1];
+}
+
+template <typename T>
+int restrict_2d(const T *ci, const T *rf, T *bc, Dims2 f, Dims2 c, cudaStream_t st)
+{
+	k_restrict<T><<<dim3(ceil_div(c.nx, TX), ceil_div(c.ny, TY)), dim3(TX, TY), 0, st>>>(ci, rf, bc, f, c);
+	CDR_LAUNCH_CHECK();
+	return CDR_OK;
+}
+template int restrict_2d<double>(const double *, const double *, double *, Dims2, Dims2, cudaStream_t);
+template int restrict_2d<float>(const float *, const float *, float *, Dims2, Dims2, cudaStream_t);
+
+// ------------------------------------------------------------ interpolate-add
+// BMG2_SymStd_interp_add (src/2d/ftn/BMG2_SymStd_interp_add.f90:101-137).  One
+// thread per coarse cell (IC, JC) of the reference loop (0-based ic in
+// [1, nxf/2+1]); it owns fine points (i, j), (i-1, j), (i, j-1), (i-1, j-1) with
+// i = 2ic-1.  r/c is formed on the fly instead of dividing r in place.
+template <typename T>
+__global__ void __launch_bounds__(TX *TY) k_interp_add(const T *__restrict__ ci, const T *__restrict__ qc,
+                                                       const T *__restrict__ res, const T *__restrict__ soc,
+                                                       T *__restrict__ q, Dims2 f, Dims2 c)
+{
+	int ic = blockIdx.x * TX + threadIdx.x + 1, jc = blockIdx.y * TY + threadIdx.y + 1;
+	if (ic > f.nx / 2 + 1 || jc > f.ny / 2 + 1) return;
+	const size_t cps = c.plane();
+	const int cp = c.pitch, fp = f.pitch;
+	size_t kc = c.at(ic, jc), kf = f.at(2 * ic - 1, 2 * jc - 1);
+	T qcc = qc[kc];
+	q[kf] = q[kf] + qcc;
+	if (ic >= 2) {
+		T a = ci[IR * cps + kc] * qcc + ci[IL * cps + kc] * qc[kc - 1];
+		size_t k = kf - 1;
+		q[k] = q[k] + a + res[k] / soc[k];
+	}
+	if (jc >= 2) {
+		T aq = ci[IA * cps + kc] * qcc + ci[IB * cps + kc] * qc[kc - cp];
+		size_t k = kf - fp;
+		q[k] = q[k] + aq + res[k] / soc[k];
+	}
+	if (ic >= 2 && jc >= 2) {
+		T a = ci[ISW * cps + kc] * qc[kc - cp - 1] + ci[INW * cps + kc] * qc[kc - 1] + ci[INE * cps + kc] * qcc
+		      + ci[ISE * cps + kc] * qc[kc - cp];
+		size_t k = kf - fp - 1;
+		q[k] = q[k] + a + res[k] / soc[k];
+	}
+}
+
+template <typename T>
+int interp_add_2d(const T *ci, const T *xc, const T *rf, const T *sof, T *xf, Dims2 f, Dims2 c, cudaStream_t st)
+{
+	k_interp_add<T><<<dim3(ceil_div(f.nx / 2 + 1, TX), ceil_div(f.ny / 2 + 1, TY)), dim3(TX, TY), 0, st>>>(
+	    ci, xc, rf, sof, xf, f, c);
+	CDR_LAUNCH_CHECK();
+	return CDR_OK;
+}
+template int interp_add_2d<double>(const double *, const double *, const double *, const double *, double *,
+                                   Dims2, Dims2, cudaStream_t);
+template int interp_add_2d<float>(const float *, const float *, const float *, const float *, float *, Dims2,
+                                  Dims2, cudaStream_t);
+
+// ------------------------------------------------ operator-induced interpolation
+// BMG2_SymStd_SETUP_interp_OI (src/2d/ftn/BMG2_SymStd_SETUP_interp_OI.f90:109-253).
+// Phase 1 computes the edge weights, phase 2 the corner weights that read
+// neighbouring edge weights.  emach = D1MACH(3) = 2^-53.
+
+template <int NS>
+__global__ void k_oi_edges(const double *__restrict__ so, double *__restrict__ ci, Dims2 f, Dims2 c)
+{
+	int ic = blockIdx.x * TX + threadIdx.x + 1, jc = blockIdx.y * TY + threadIdx.y + 1;
+	const size_t ps = f.plane(), cps = c.plane();
+	const int fp = f.pitch;
+	const double *C = so, *W = so + ps, *S = so + 2 * ps, *SW = so + 3 * ps, *NW = so + 4 * ps;
+	size_t kc = c.at(ic, jc);
+	// x-edge weights at coarse (ic, jc), ic in [2, nxf/2+1], jc in [1, nyc]
+	if (ic >= 2 && ic <= f.nx / 2 + 1 && jc <= c.ny) {
+		size_t k = f.at(2 * ic - 1, 2 * jc - 1);  // fine point right of the x-edge point k-1
+		double A, B;
+		if (NS == 5) {
+			A = W[k] + NW[k] + SW[k + fp];
+			B = W[k - 1] + SW[k - 1] + NW[k - 1 + fp];
+		} else {
+			A = W[k];
+			B = W[k - 1];
+		}
+		double o = C[k - 1];
+		double ep = fmin(fabs(A / o), fabs(B / o));
+		double sum = A + B + S[k - 1] + S[k - 1 + fp];
+		sum = A + B + (o - sum) * fmax(o - (1.0 + ep) * sum, 0.0) / (fabs(o - (1.0 + ep) * sum) + 1.1102230246251565e-16);
+		sum = 1.0 / sum;
+		ci[IR * cps + kc] = A * sum;
+		ci[IL * cps + kc] = B * sum;
+	}
+	// y-edge weights at coarse (ic, jc), ic in [1, nxc], jc in [2, nyf/2+1]
+	if (ic <= c.nx && jc >= 2 && jc <= f.ny / 2 + 1) {
+		size_t k = f.at(2 * ic - 1, 2 * jc - 1);  // fine point above the y-edge point k-fp
+		double A, B;
+		if (NS == 5) {
+			A = S[k] + NW[k] + SW[k + 1];
+			B = S[k - fp] + SW[k - fp] + NW[k + 1 - fp];
+		} else {
+			A = S[k];
+			B = S[k - fp];
+		}
+		double o = C[k - fp];
+		double ep = fmin(fabs(A / o), fabs(B / o));
+		double sum = A + B + W[k - fp] + W[k + 1 - fp];
+		sum = A + B + (o - sum) * fmax(o - (1.0 + ep) * sum, 0.0) / (fabs(o - (1.0 + ep) * sum) + 1.1102230246251565e-16);
+		sum = 1.0 / sum;
+		ci[IA * cps + kc] = A * sum;
+		ci[IB * cps + kc] = B * sum;
+	}
+}
+
+template <int NS>
+__global__ void k_oi_corners(const double *__restrict__ so, double *__restrict__ ci, Dims2 f, Dims2 c)
+{
+	int ic = blockIdx.x * TX + threadIdx.x + 2, jc = blockIdx.y * TY + threadIdx.y + 2;
+	if (ic > f.nx / 2 + 1 || jc > f.ny / 2 + 1) return;
+	const size_t ps = f.plane(), cps = c.plane();
+	const int fp = f.pitch, cp = c.pitch;
+	const double *C = so, *W = so + ps, *S = so + 2 * ps, *SW = so + 3 * ps, *NW = so + 4 * ps;
+	size_t kc = c.at(ic, jc);
+	size_t k = f.at(2 * ic - 1, 2 * jc - 1);  // (I, J); the centre point is (I-1, J-1)
+	size_t kw = k - 1, ks = k - fp, ksw = k - fp - 1;
+	double o = C[ksw];
+	double ciLL_s = ci[IL * cps + kc - cp], ciLR_s = ci[IR * cps + kc - cp];
+	double ciLB_w = ci[IB * cps + kc - 1], ciLA_w = ci[IA * cps + kc - 1];
+	double ciLL = ci[IL * cps + kc], ciLR = ci[IR * cps + kc], ciLB = ci[IB * cps + kc], ciLA = ci[IA * cps + kc];
+	double sum, ep;
+	if (NS == 5) {
+		sum = W[ksw] + NW[kw] + S[kw] + SW[k] + W[ks] + NW[ks] + S[ksw] + SW[ksw];
+		ep = fmin(fmin(fabs((SW[ksw] + W[ksw] + NW[kw]) / o), fabs((NW[kw] + S[kw] + SW[k]) / o)),
+		          fmin(fabs((SW[k] + W[ks] + NW[ks]) / o), fabs((NW[ks] + S[ksw] + SW[ksw]) / o)));
+	} else {
+		sum = W[ksw] + S[kw] + W[ks] + S[ksw];
+		ep = fmin(fmin(fabs(W[ksw] / o), fabs(S[kw] / o)), fmin(fabs(W[ks] / o), fabs(S[ksw] / o)));
+	}
+	sum = sum + (o - sum) * fmax(o - (1.0 + ep) * sum, 0.0) / (fabs(o - (1.0 + ep) * sum) + 1.1102230246251565e-16);
+	double s = 1.0 / sum;
+	if (NS == 5) {
+		ci[ISW * cps + kc] = (S[ksw] * ciLL_s + W[ksw] * ciLB_w + SW[ksw]) * s;
+		ci[ISE * cps + kc] = (S[ksw] * ciLR_s + W[ks] * ciLB + NW[ks]) * s;
+		ci[INW * cps + kc] = (W[ksw] * ciLA_w + S[kw] * ciLL + NW[kw]) * s;
+		ci[INE * cps + kc] = (S[kw] * ciLR + W[ks] * ciLA + SW[k]) * s;
+	} else {
+		ci[ISW * cps + kc] = (S[ksw] * ciLL_s + W[ksw] * ciLB_w) * s;
+		ci[ISE * cps + kc] = (S[ksw] * ciLR_s + W[ks] * ciLB) * s;
+		ci[INW * cps + kc] = (W[ksw] * ciLA_w + S[kw] * ciLL) * s;
+		ci[INE * cps + kc] = (S[kw] * ciLR + W[ks] * ciLA) * s;
+	}
+}
+
+int setup_interp_2d(const double *so, int nstencil, double *ci, Dims2 f, Dims2 c, cudaStream_t st)
+{
+	CDR_CUDA_TRY(cudaMemsetAsync(ci, 0, sizeof(double) * c.plane() * 8, st));
+	dim3 blk(TX, TY);
+	dim3 g1(ceil_div(c.nx + 1, TX), ceil_div(c.ny + 1, TY));
+	dim3 g2(ceil_div(f.nx / 2, TX), ceil_div(f.ny / 2, TY));
+	if (nstencil == 5) {
+		k_oi_edges<5><<<g1, blk, 0, st>>>(so, ci, f, c);
+		CDR_LAUNCH_CHECK();
+		k_oi_corners<5><<<g2, blk, 0, st>>>(so, ci, f, c);
+	} else {
+		k_oi_edges<3><<<g1, blk, 0, st>>>(so, ci, f, c);
+		CDR_LAUNCH_CHECK();
+		k_oi_corners<3><<<g2, blk, 0, st>>>(so, ci, f, c);
+	}
+	CDR_LAUNCH_CHECK();
+	return CDR_OK;
+}
+
+// ------------------------------------------------------------ Galerkin coarse op
+// Coarse operator P^T A P, computed per coarse point as a local product over
+// the 3x3 fine support of each coarse basis function.  Same result as the
+// reference's expanded formulas (BMG2_SymStd_SETUP_ITLI_ex.f90:94-331) up to
+// summation order.
+//
+// Weight of coarse point (ic, jc) at fine point F + (dx, dy), F = (2ic-1, 2jc-1):
+// the entries of CI that interp_add/restrict use for that fine point.
+__device__ __forceinline__ double pweight(const double *__restrict__ ci, size_t cps, int cp, size_t kc, int dx,
+                                          int dy)
+{
+	if (dx == 0 && dy == 0) return 1.0;
+	if (dx == -1 && dy == 0) return ci[IR * cps + kc];
+	if (dx == 1 && dy == 0) return ci[IL * cps + kc + 1];
+	if (dx == 0 && dy == -1) return ci[IA * cps + kc];
+	if (dx == 0 && dy == 1) return ci[IB * cps + kc + cp];
+	if (dx == -1 && dy == -1) return ci[INE * cps + kc];
+	if (dx == 1 && dy == -1) return ci[INW * cps + kc + 1];
+	if (dx == -1 && dy == 1) return ci[ISE * cps + kc + cp];
+	return ci[ISW * cps + kc + cp + 1];  // (1, 1)
+}
+
+// A[(i,j), (i+di, j+dj)] from the lower-half storage.
+template <int NS>
+__device__ __forceinline__ double aentry(const double *__restrict__ so, size_t ps, int fp, size_t k, int di, int dj)
+{
+	if (di == 0 && dj == 0) return so[k];
+	if (di == -1 && dj == 0) return -so[ps + k];
+	if (di == 1 && dj == 0) return -so[ps + k + 1];
+	if (di == 0 && dj == -1) return -so[2 * ps + k];
+	if (di == 0 && dj == 1) return -so[2 * ps + k + fp];
+	if (NS == 3) return 0.0;
+	if (di == -1 && dj == -1) return -so[3 * ps + k];
+	if (di == 1 && dj == 1) return -so[3 * ps + k + fp + 1];
+	if (di == 1 && dj == -1) return -so[4 * ps + k + 1];
+	return -so[4 * ps + k + fp];  // (-1, 1)
+}
+
+// sum over f1 in supp(c1), f2 in supp(c2) of P(f1,c1) A(f1,f2) P(f2,c2); c2 = c1 + (ox, oy)*(-1)
+template <int NS, int OX1, int OY1, int OX2, int OY2>
+__device__ __forceinline__ double rap_entry(const double *__restrict__ so, const double *__restrict__ ci, Dims2 f,
+                                            Dims2 c, int ic, int jc)
+{
+	const size_t ps = f.plane(), cps = c.plane();
+	const int fp = f.pitch, cp = c.pitch;
+	const int F1x = 2 * (ic + OX1) - 1, F1y = 2 * (jc + OY1) - 1;
+	const size_t kc1 = c.at(ic + OX1, jc + OY1), kc2 = c.at(ic + OX2, jc + OY2);
+	double tot = 0.0;
+#pragma unroll
+	for (int dy1 = -1; dy1 <= 1; ++dy1)
+#pragma unroll
+		for (int dx1 = -1; dx1 <= 1; ++dx1) {
+			const int fx = F1x + dx1, fy = F1y + dy1;
+			if (fx < 1 || fx > f.nx || fy < 1 || fy > f.ny) continue;
+			const size_t kf = f.at(fx, fy);
+			double inner = 0.0;
+#pragma unroll
+			for (int ddy = -1; ddy <= 1; ++ddy)
+#pragma unroll
+				for (int ddx = -1; ddx <= 1; ++ddx) {
+					// offset of f2 = f1 + (ddx, ddy) from F2 = F1 + 2*(OX2-OX1, OY2-OY1)
+					const int ex = dx1 + ddx - 2 * (OX2 - OX1), ey = dy1 + ddy - 2 * (OY2 - OY1);
+					if (ex < -1 || ex > 1 || ey < -1 || ey > 1) continue;
+					if (NS == 3 && ddx != 0 && ddy != 0) continue;
+					inner += aentry<NS>(so, ps, fp, kf, ddx, ddy) * pweight(ci, cps, cp, kc2, ex, ey);
+				}
+			tot += pweight(ci, cps, cp, kc1, dx1, dy1) * inner;
+		}
+	return tot;
+}
+
+template <int NS>
+__global__ void k_galerkin(const double *__restrict__ so, const double *__restrict__ ci, double *__restrict__ soc,
+                           Dims2 f, Dims2 c)
+{
+	int ic = blockIdx.x * TX + threadIdx.x + 1, jc = blockIdx.y * TY + threadIdx.y + 1;
+	if (ic > c.nx || jc > c.ny) return;
+	const size_t cps = c.plane();
+	const size_t kc = c.at(ic, jc);
+	soc[PC * cps + kc] = rap_entry<NS, 0, 0, 0, 0>(so, ci, f, c, ic, jc);
+	soc[PW * cps + kc] = -rap_entry<NS, 0, 0, -1, 0>(so, ci, f, c, ic, jc);
+	soc[PS * cps + kc] = -rap_entry<NS, 0, 0, 0, -1>(so, ci, f, c, ic, jc);
+	soc[PSW * cps + kc] = -rap_entry<NS, 0, 0, -1, -1>(so, ci, f, c, ic, jc);
+	soc[PNW * cps + kc] = -rap_entry<NS, -1, 0, 0, -1>(so, ci, f, c, ic, jc);
+}
+
+int galerkin_2d(const double *so, int nstencil, const double *ci, double *soc, Dims2 f, Dims2 c, cudaStream_t st)
+{
+	CDR_CUDA_TRY(cudaMemsetAsync(soc, 0, sizeof(double) * c.plane() * 5, st));
+	dim3 g(ceil_div(c.nx, TX), ceil_div(c.ny, TY));
+	if (nstencil == 5) k_galerkin<5><<<g, dim3(TX, TY), 0, st>>>(so, ci, soc, f, c);
+	else k_galerkin<3><<<g, dim3(TX, TY), 0, st>>>(so, ci, soc, f, c);
+	CDR_LAUNCH_CHECK();
+	return CDR_OK;
+}
+
+// --------------------------------------------------- coarsest banded Cholesky
+// ABD fill of BMG2_SymStd_SETUP_cg_LU (src/2d/ftn/BMG2_SymStd_SETUP_cg_LU.f90:92-104,
+// 229-241) and LAPACK DPBTF2('U') (unblocked upper band Cholesky; DPBTRF takes it
+// for KD < 32).  The grid is at most a few dozen points: one thread.
+__global__ void k_cg_factor(const double *__restrict__ so, int ns, Dims2 d, double *__restrict__ ab, int *info)
+{
+	if (threadIdx.x != 0 || blockIdx.x != 0) return;
+	const int ldab = d.nx + 2, kd = d.nx + 1, n = d.nx * d.ny;
+	const size_t ps = d.plane();
+	for (size_t e = 0; e < (size_t)ldab * n; ++e) ab[e] = 0.0;
+	int kk = 0;
+	for (int j = 1; j <= d.ny; ++j)
+		for (int i = 1; i <= d.nx; ++i, ++kk) {
+			size_t k = d.at(i, j);
+			double *col = ab + (size_t)kk * ldab;  // column kk, rows 0..ldab-1
+			col[ldab - 1] = so[k];
+			col[ldab - 2] = -so[ps + k];
+			col[2] = ns == 5 ? -so[4 * ps + k + 1] : 0.0;
+			col[1] = -so[2 * ps + k];
+			col[0] = ns == 5 ? -so[3 * ps + k] : 0.0;
+		}
+	int kld = ldab - 1;
+	int st = 0;
+	for (int jj = 0; jj < n; ++jj) {
+		double ajj = ab[(size_t)jj * ldab + kd];
+		if (ajj <= 0.0) { st = jj + 1; break; }
+		ajj = sqrt(ajj);
+		ab[(size_t)jj * ldab + kd] = ajj;
+		int kn = kd < n - jj - 1 ? kd : n - jj - 1;
+		if (kn > 0) {
+			double rcp = 1.0 / ajj;
+			double *x = ab + (size_t)(jj + 1) * ldab + (kd - 1);
+			for (int p = 0; p < kn; ++p) x[(size_t)p * kld] = rcp * x[(size_t)p * kld];
+			double *a = ab + (size_t)(jj + 1) * ldab + kd;
+			for (int q = 0; q < kn; ++q) {
+				double xq = x[(size_t)q * kld];
+				if (xq != 0.0) {
+					double temp = -1.0 * xq;
+					for (int p = 0; p <= q; ++p)
+						a[(size_t)p + (size_t)q * kld] = a[(size_t)p + (size_t)q * kld] + x[(size_t)p * kld] * temp;
+				}
+			}
+		}
+	}
+	if (info) *info = st;
+}
+
+// BMG2_SymStd_SOLVE_cg (src/2d/ftn/BMG2_SymStd_SOLVE_cg.f90:93-123) with DPBTRS('U'):
+// U^T y = b then U x = y, in FP64 whatever the grid-function type.
+template <typename T>
+__global__ void k_cg_solve(const double *__restrict__ ab, T *__restrict__ q, const T *__restrict__ qf, Dims2 d)
+{
+	extern __shared__ double xs[];
+	if (threadIdx.x != 0 || blockIdx.x != 0) return;
+	const int ldab = d.nx + 2, kd = d.nx + 1, n = d.nx * d.ny;
+	int kk = 0;
+	for (int j = 1; j <= d.ny; ++j)
+		for (int i = 1; i <= d.nx; ++i) xs[kk++] = (double)qf[d.at(i, j)];
+	for (int j = 0; j < n; ++j) {
+		double temp = xs[j];
+		int i0 = j - kd > 0 ? j - kd : 0;
+		for (int i = i0; i < j; ++i) temp = temp - ab[(size_t)j * ldab + kd + i - j] * xs[i];
+		xs[j] = temp / ab[(size_t)j * ldab + kd];
+	}
+	for (int j = n - 1; j >= 0; --j) {
+		if (xs[j] != 0.0) {
+			xs[j] = xs[j] / ab[(size_t)j * ldab + kd];
+			double temp = xs[j];
+			int i1 = j - kd > 0 ? j - kd : 0;
+			for (int i = j - 1; i >= i1; --i) xs[i] = xs[i] - temp * ab[(size_t)j * ldab + kd + i - j];
+		}
+	}
+	kk = 0;
+	for (int j = 1; j <= d.ny; ++j)
+		for (int i = 1; i <= d.nx; ++i) q[d.at(i, j)] = (T)xs[kk++];
+}
+
+int setup_cg_2d(const double *so, int nstencil, Dims2 d, double *abd, int *info, cudaStream_t st)
+{
+	k_cg_factor<<<1, 32, 0, st>>>(so, nstencil, d, abd, info);
+	CDR_LAUNCH_CHECK();
+	return CDR_OK;
+}
+
+template <typename T>
+int solve_cg_2d(const double *abd, T *x, const T *b, Dims2 d, cudaStream_t st)
+{
+	size_t sm = sizeof(double) * (size_t)d.nx * d.ny;
+	if (sm > 48 * 1024) {
+		set_error(CDR_ERR_DIM, "coarsest grid %dx%d too large for the direct solve", d.nx, d.ny);
+		return CDR_ERR_DIM;
+	}
+	k_cg_solve<T><<<1, 32, sm, st>>>(abd, x, b, d);
+	CDR_LAUNCH_CHECK();
+	return CDR_OK;
+}
+template int solve_cg_2d<double>(const double *, double *, const double *, Dims2, cudaStream_t);
+template int solve_cg_2d<float>(const double *, float *, const float *, Dims2, cudaStream_t);
+
+// ------------------------------------------------------------ precision helpers
+template <typename TO, typename TI>
+__global__ void k_convert(const TI *__restrict__ in, TO *__restrict__ out, size_t n)
+{
+	for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x)
+		out[e] = (TO)in[e];
+}
+
+int convert_f64_f32(const double *in, float *out, size_t n, cudaStream_t st)
+{
+	int nb = (int)((n + 255) / 256);
+	if (nb > 148 * 16) nb = 148 * 16;
+	if (nb < 1) nb = 1;
+	k_convert<float, double><<<nb, 256, 0, st>>>(in, out, n);
+	CDR_LAUNCH_CHECK();
+	return CDR_OK;
+}
+
+// Outer refinement step of the mixed-precision solve:
+//   x_out = x_in + e32 on the interior, r64 = b64 - A64 x_out, r32 = (float) r64
+//   and ||r64||^2 per block.  The residual at a point needs the corrected x at
+//   its neighbours, so each thread forms x_in + e32 for its 3x3 neighbourhood on
+//   the fly; x_in and x_out are different buffers (ping-pong), so no thread
+//   reads a value another thread has already corrected.  apply = 0 skips e.
+template <int NS>
+__global__ void __launch_bounds__(TX *TY) k_ir_residual(const double *__restrict__ so, const double *__restrict__ x,
+                                                        const float *__restrict__ e, const double *__restrict__ b,
+                                                        double *__restrict__ xo, float *__restrict__ r32, Dims2 d,
+                                                        Dims2 d32, double *__restrict__ partial, int apply)
+{
+	__shared__ double sh[TX * TY / 32];
+	const int tiles_x = (d.nx + TX - 1) / TX;
+	const int ntiles = tiles_x * ((d.ny + TY - 1) / TY);
+	const size_t ps = d.plane();
+	const int p = d.pitch, p32 = d32.pitch;
+	double acc = 0.0;
+	for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+		int i = (t % tiles_x) * TX + threadIdx.x + 1;
+		int j = (t / tiles_x) * TY + threadIdx.y + 1;
+		if (i <= d.nx && j <= d.ny) {
+			const size_t k = d.at(i, j), k32 = d32.at(i, j);
+			double xn[3][3];
+#pragma unroll
+			for (int dj = -1; dj <= 1; ++dj)
+#pragma unroll
+				for (int di = -1; di <= 1; ++di) {
+					double v = x[k + (long)dj * p + di];
+					xn[dj + 1][di + 1] = apply ? v + (double)e[k32 + (long)dj * p32 + di] : v;
+				}
+			const double *c = so, *w = so + ps, *s = so + 2 * ps;
+			double rr;
+			if (NS == 5) {
+				const double *sw = so + 3 * ps, *nw = so + 4 * ps;
+				rr = b[k] + w[k] * xn[1][0] + w[k + 1] * xn[1][2] + s[k] * xn[0][1] + s[k + p] * xn[2][1]
+				     + sw[k] * xn[0][0] + nw[k + 1] * xn[0][2] + nw[k + p] * xn[2][0] + sw[k + p + 1] * xn[2][2]
+				     - c[k] * xn[1][1];
+			} else {
+				rr = b[k] + w[k] * xn[1][0] + w[k + 1] * xn[1][2] + s[k] * xn[0][1] + s[k + p] * xn[2][1]
+				     - c[k] * xn[1][1];
+			}
+			acc += rr * rr;
+			r32[k32] = (float)rr;
+			xo[k] = xn[1][1];
+		}
+	}
+	double s = block_sum<TX * TY / 32>(acc, sh);
+	if (threadIdx.x == 0 && threadIdx.y == 0) partial[blockIdx.x] = s;
+}
+
+int ir_residual_2d(const double *so, int nstencil, const double *x, const float *e, const double *b, double *xo,
+                   float *r32, Dims2 d, Dims2 d32, double *norm_out, double *partial, int apply, cudaStream_t st)
+{
+	const int ntiles = ceil_div(d.nx, TX) * ceil_div(d.ny, TY);
+	int nb = ntiles < NORM_MAX_BLOCKS ? ntiles : NORM_MAX_BLOCKS;
+	if (nstencil == 5)
+		k_ir_residual<5><<<nb, dim3(TX, TY), 0, st>>>(so, x, e, b, xo, r32, d, d32, partial, apply);
+	else
+		k_ir_residual<3><<<nb, dim3(TX, TY), 0, st>>>(so, x, e, b, xo, r32, d, d32, partial, apply);
+	CDR_LAUNCH_CHECK();
+	k_norm_finish<<<1, 1024, 0, st>>>(partial, nb, norm_out);
+	CDR_LAUNCH_CHECK();
+	return CDR_OK;
+}
+
+}  // namespace cdrgpu

@@ -1,0 +1,587 @@
+// solver2d.cu -- 2D BoxMG multilevel solver on the device.
+//
+// Host control mirrors Cedar's multilevel driver: setup builds the hierarchy
+// level by level (interpolation, Galerkin operator, smoother) and factors the
+// coarsest operator (multilevel::setup, include/cedar/multilevel.h:243-265);
+// the V-cycle recursion is cycle::vcycle::ncycle_helper
+// (include/cedar/cycle/vcycle.h:57-115); the solve loop with its relative l2
+// stopping test is multilevel::solve (multilevel.h:278-298).  Every step is a
+// stream-ordered kernel launch; the whole cycle is captured once as a CUDA
+// graph and replayed, and only the per-iteration residual norm comes back to
+// the host.
+//
+// Two solve forms:
+//   CDR_PREC_F64     plain FP64 cycles (the drop-in path);
+//   CDR_PREC_F32_IR  FP64 iterative refinement: r = b - A x in FP64, one FP32
+//                    V-cycle on r (FP32 copies of every operator, interpolation
+//                    and line factor; FP64 coarsest Cholesky), x += e in FP64.
+#include <vector>
+#include <cstring>
+#include <cmath>
+
+#include "kernels2d.cuh"
+
+using namespace cdrgpu;
+
+namespace {
+
+inline int round_up(int v, int m) { return (v + m - 1) / m * m; }
+
+struct Level {
+	int nx = 0, ny = 0, ns = 5;
+	Dims2 d{};      // pitch for grid arrays
+	int tpitch = 0; // pitch of the transposed y-line factors
+	// FP64
+	double *so = nullptr, *x = nullptr, *b = nullptr, *r = nullptr, *sor = nullptr, *sory = nullptr, *ci = nullptr;
+	// FP32 preconditioner copies
+	float *so32 = nullptr, *x32 = nullptr, *b32 = nullptr, *r32 = nullptr, *sor32 = nullptr, *sory32 = nullptr,
+	      *ci32 = nullptr;
+};
+
+}  // namespace
+
+struct cdr_gpu_solver {
+	cdr_gpu_settings s{};
+	std::vector<Level> lv;
+	std::vector<void *> allocs;
+	double *abd = nullptr;
+	int *info = nullptr;
+	double *norm = nullptr;     // device scalars
+	double *partial = nullptr;  // norm scratch
+	double *x64[2] = {nullptr, nullptr};
+	double *h_norm = nullptr;   // pinned host copy of the norm
+	cudaStream_t st = nullptr;
+	bool own_stream = false;
+	cudaGraphExec_t gexec[2] = {nullptr, nullptr};  // cycle graphs: [0] FP64, [1] FP32
+	long long glaunches[2] = {0, 0};                 // kernel launches per replay
+	cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+	float setup_ms = 0.f, solve_ms = 0.f;
+
+	template <typename T>
+	int alloc(T **p, size_t n)
+	{
+		void *q = nullptr;
+		CDR_CUDA_TRY(cudaMalloc(&q, n * sizeof(T) + 256));
+		CDR_CUDA_TRY(cudaMemsetAsync(q, 0, n * sizeof(T) + 256, st));
+		allocs.push_back(q);
+		*p = (T *)q;
+		return CDR_OK;
+	}
+
+	bool mixed() const { return s.precision == CDR_PREC_F32_IR; }
+	int L() const { return (int)lv.size(); }
+
+	// -------------------------------------------------------------- smoothing
+	template <typename T>
+	int smooth(int l, T *x, const T *b, int updown);
+	template <typename T>
+	int ncycle(int l, T *x, const T *b);
+	template <typename T>
+	int cycle(T *x, const T *b);
+	int run_cycle(int prec);
+	int setup();
+};
+
+namespace {
+template <typename T> struct Arr;
+template <> struct Arr<double> {
+	static double *so(Level &L) { return L.so; }
+	static double *x(Level &L) { return L.x; }
+	static double *b(Level &L) { return L.b; }
+	static double *r(Level &L) { return L.r; }
+	static double *sor(Level &L) { return L.sor; }
+	static double *sory(Level &L) { return L.sory; }
+	static double *ci(Level &L) { return L.ci; }
+};
+template <> struct Arr<float> {
+	static float *so(Level &L) { return L.so32; }
+	static float *x(Level &L) { return L.x32; }
+	static float *b(Level &L) { return L.b32; }
+	static float *r(Level &L) { return L.r32; }
+	static float *sor(Level &L) { return L.sor32; }
+	static float *sory(Level &L) { return L.sory32; }
+	static float *ci(Level &L) { return L.ci32; }
+};
+}  // namespace
+
+// multilevel::setup_relax_helper smoother closures (include/cedar/multilevel.h:160-222)
+template <typename T>
+int cdr_gpu_solver::smooth(int l, T *x, const T *b, int updown)
+{
+	Level &L = lv[l];
+	const int n = updown == CDR_DOWN ? s.nrelax_pre : s.nrelax_post;
+	const T *so = Arr<T>::so(L), *sor = Arr<T>::sor(L), *sory = Arr<T>::sory(L);
+	for (int it = 0; it < n; ++it) {
+		switch (s.relaxation) {
+		case CDR_RELAX_POINT: CDR_TRY(relax_point_2d<T>(so, L.ns, x, b, sor, L.d, updown, st)); break;
+		case CDR_RELAX_LINE_X:
+			CDR_TRY(relax_lines_2d<T>(so, L.ns, x, b, sor, L.d, L.tpitch, CDR_DIR_X, updown, st));
+			break;
+		case CDR_RELAX_LINE_Y:
+			CDR_TRY(relax_lines_2d<T>(so, L.ns, x, b, sory, L.d, L.tpitch, CDR_DIR_Y, updown, st));
+			break;
+		case CDR_RELAX_LINE_XY:
+			if (updown == CDR_DOWN) {
+				CDR_TRY(relax_lines_2d<T>(so, L.ns, x, b, sor, L.d, L.tpitch, CDR_DIR_X, updown, st));
+				CDR_TRY(relax_lines_2d<T>(so, L.ns, x, b, sory, L.d, L.tpitch, CDR_DIR_Y, updown, st));
+			} else {
+				CDR_TRY(relax_lines_2d<T>(so, L.ns, x, b, sory, L.d, L.tpitch, CDR_DIR_Y, updown, st));
+				CDR_TRY(relax_lines_2d<T>(so, L.ns, x, b, sor, L.d, L.tpitch, CDR_DIR_X, updown, st));
+			}
+			break;
+		default: set_error(CDR_ERR_ARG, "unknown relaxation %d", s.relaxation); return CDR_ERR_ARG;
+		}
+	}
+	return CDR_OK;
+}
+
+// cycle::vcycle::ncycle_helper (include/cedar/cycle/vcycle.h:57-115), n = 1
+template <typename T>
+int cdr_gpu_solver::ncycle(int l, T *x, const T *b)
+{
+	Level &F = lv[l], &C = lv[l + 1];
+	CDR_TRY(smooth<T>(l, x, b, CDR_DOWN));
+	CDR_TRY(residual_2d<T>(Arr<T>::so(F), F.ns, x, b, Arr<T>::r(F), F.d, nullptr, nullptr, st));
+	CDR_TRY(restrict_2d<T>(Arr<T>::ci(C), Arr<T>::r(F), Arr<T>::b(C), F.d, C.d, st));
+	CDR_CUDA_TRY(cudaMemsetAsync(Arr<T>::x(C), 0, sizeof(T) * C.d.plane(), st));
+	if (l + 1 == L() - 1) CDR_TRY(solve_cg_2d<T>(abd, Arr<T>::x(C), Arr<T>::b(C), C.d, st));
+	else CDR_TRY(ncycle<T>(l + 1, Arr<T>::x(C), Arr<T>::b(C)));
+	CDR_TRY(interp_add_2d<T>(Arr<T>::ci(C), Arr<T>::x(C), Arr<T>::r(F), Arr<T>::so(F), x, F.d, C.d, st));
+	CDR_TRY(smooth<T>(l, x, b, CDR_UP));
+	return CDR_OK;
+}
+
+template <typename T>
+int cdr_gpu_solver::cycle(T *x, const T *b)
+{
+	if (L() == 1) return solve_cg_2d<T>(abd, x, b, lv[0].d, st);
+	return ncycle<T>(0, x, b);
+}
+
+// One cycle on the level-0 work buffers, replayed from a CUDA graph when enabled.
+int cdr_gpu_solver::run_cycle(int prec)
+{
+	auto body = [&]() -> int {
+		if (prec == 0) return cycle<double>(lv[0].x, lv[0].b);
+		return cycle<float>(lv[0].x32, lv[0].b32);
+	};
+	if (!s.use_graph) return body();
+	if (!gexec[prec]) {
+		cudaGraph_t g = nullptr;
+		CDR_CUDA_TRY(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+		const long long before = cdr_gpu_launch_count();
+		int rc = body();
+		glaunches[prec] = cdr_gpu_launch_count() - before;
+		count_launches(-glaunches[prec]);  // captured, not launched
+		cudaError_t e = cudaStreamEndCapture(st, &g);
+		if (rc != CDR_OK) {
+			if (g) cudaGraphDestroy(g);
+			return rc;
+		}
+		if (e != cudaSuccess) {
+			set_error(CDR_ERR_CUDA, "graph capture: %s", cudaGetErrorString(e));
+			return CDR_ERR_CUDA;
+		}
+		CDR_CUDA_TRY(cudaGraphInstantiate(&gexec[prec], g, 0));
+		cudaGraphDestroy(g);
+	}
+	CDR_CUDA_TRY(cudaGraphLaunch(gexec[prec], st));
+	count_launches(glaunches[prec]);
+	return CDR_OK;
+}
+
+// multilevel::setup (include/cedar/multilevel.h:243-265) on the device.
+int cdr_gpu_solver::setup()
+{
+	for (int l = 0; l + 1 < L(); ++l) {
+		Level &F = lv[l], &C = lv[l + 1];
+		CDR_TRY(setup_interp_2d(F.so, F.ns, C.ci, F.d, C.d, st));
+		CDR_TRY(galerkin_2d(F.so, F.ns, C.ci, C.so, F.d, C.d, st));
+		// smoother setup (multilevel::setup_relax_helper, multilevel.h:134-158)
+		switch (s.relaxation) {
+		case CDR_RELAX_POINT: CDR_TRY(setup_recip_2d<double>(F.so, F.sor, F.d, st)); break;
+		case CDR_RELAX_LINE_X:
+			CDR_TRY(setup_lines_2d<double>(F.so, F.ns, F.sor, F.d, F.tpitch, CDR_DIR_X, info, st));
+			break;
+		case CDR_RELAX_LINE_Y:
+			CDR_TRY(setup_lines_2d<double>(F.so, F.ns, F.sory, F.d, F.tpitch, CDR_DIR_Y, info, st));
+			break;
+		case CDR_RELAX_LINE_XY:
+			CDR_TRY(setup_lines_2d<double>(F.so, F.ns, F.sor, F.d, F.tpitch, CDR_DIR_X, info, st));
+			CDR_TRY(setup_lines_2d<double>(F.so, F.ns, F.sory, F.d, F.tpitch, CDR_DIR_Y, info, st));
+			break;
+		}
+	}
+	Level &Cg = lv[L() - 1];
+	CDR_TRY(setup_cg_2d(Cg.so, Cg.ns, Cg.d, abd, info + 1, st));
+	if (mixed()) {
+		for (int l = 0; l < L(); ++l) {
+			Level &F = lv[l];
+			CDR_TRY(convert_f64_f32(F.so, F.so32, F.d.plane() * F.ns, st));
+			if (l > 0) CDR_TRY(convert_f64_f32(F.ci, F.ci32, F.d.plane() * 8, st));
+			if (l + 1 == L()) continue;
+			switch (s.relaxation) {
+			case CDR_RELAX_POINT: CDR_TRY(convert_f64_f32(F.sor, F.sor32, F.d.plane(), st)); break;
+			case CDR_RELAX_LINE_X:
+				CDR_TRY(setup_lines_2d<float>(F.so, F.ns, F.sor32, F.d, F.tpitch, CDR_DIR_X, info, st));
+				break;
+			case CDR_RELAX_LINE_Y:
+				CDR_TRY(setup_lines_2d<float>(F.so, F.ns, F.sory32, F.d, F.tpitch, CDR_DIR_Y, info, st));
+				break;
+			case CDR_RELAX_LINE_XY:
+				CDR_TRY(setup_lines_2d<float>(F.so, F.ns, F.sor32, F.d, F.tpitch, CDR_DIR_X, info, st));
+				CDR_TRY(setup_lines_2d<float>(F.so, F.ns, F.sory32, F.d, F.tpitch, CDR_DIR_Y, info, st));
+				break;
+			}
+		}
+	}
+	int hinfo[2] = {0, 0};
+	CDR_CUDA_TRY(cudaMemcpyAsync(hinfo, info, sizeof(hinfo), cudaMemcpyDeviceToHost, st));
+	CDR_CUDA_TRY(cudaStreamSynchronize(st));
+	if (hinfo[0]) {
+		set_error(CDR_ERR_SETUP, "line factorization: non-positive pivot in line %d", hinfo[0]);
+		return CDR_ERR_SETUP;
+	}
+	if (hinfo[1]) {
+		set_error(CDR_ERR_SETUP, "coarse-grid Cholesky failed at column %d", hinfo[1]);
+		return CDR_ERR_SETUP;
+	}
+	return CDR_OK;
+}
+
+// cdr2::solver::compute_num_levels (include/cedar/2d/solver.h:63-79)
+static int num_levels(int nx, int ny, int min_coarse)
+{
+	float nxc, nyc;
+	int ng = 0;
+	do {
+		ng++;
+		nxc = (float)((nx - 1) / (1 << ng) + 1);
+		nyc = (float)((ny - 1) / (1 << ng) + 1);
+	} while ((nxc < nyc ? nxc : nyc) >= min_coarse);
+	return ng;
+}
+
+extern "C" {
+
+int cdr_gpu_settings_default(cdr_gpu_settings *s)
+{
+	if (!s) return CDR_ERR_ARG;
+	// defaults of ml_settings::init (src/multilevel_settings.cc:15-61)
+	s->relaxation = CDR_RELAX_POINT;
+	s->nrelax_pre = 2;
+	s->nrelax_post = 1;
+	s->num_levels = -1;
+	s->maxiter = 10;
+	s->tol = 1e-8;
+	s->min_coarse = 3;
+	s->precision = CDR_PREC_F64;
+	s->use_graph = 1;
+	return CDR_OK;
+}
+
+int cdr_gpu_solver_destroy(cdr_gpu_solver *h)
+{
+	if (!h) return CDR_ERR_HANDLE;
+	if (h->st) cudaStreamSynchronize(h->st);
+	for (auto &g : h->gexec)
+		if (g) cudaGraphExecDestroy(g);
+	for (void *p : h->allocs) cudaFree(p);
+	if (h->h_norm) cudaFreeHost(h->h_norm);
+	if (h->ev0) cudaEventDestroy(h->ev0);
+	if (h->ev1) cudaEventDestroy(h->ev1);
+	if (h->own_stream && h->st) cudaStreamDestroy(h->st);
+	delete h;
+	return CDR_OK;
+}
+
+static int create_impl(cdr_gpu_solver *h, const double *so_host, int ns, int nx, int ny)
+{
+	const cdr_gpu_settings &s = h->s;
+	int nl = num_levels(nx, ny, s.min_coarse);
+	if (s.num_levels > 0) {
+		if (s.num_levels > nl) {
+			set_error(CDR_ERR_ARG, "too many levels specified (%d > %d)", s.num_levels, nl);
+			return CDR_ERR_ARG;
+		}
+		nl = s.num_levels;
+	}
+	h->lv.resize(nl);
+	for (int l = 0; l < nl; ++l) {
+		Level &L = h->lv[l];
+		if (l == 0) { L.nx = nx; L.ny = ny; L.ns = ns; }
+		else {
+			// cdr2::solver::setup_space (include/cedar/2d/solver.h:93-94)
+			L.nx = (int)((h->lv[l - 1].nx - 1) / 2. + 1);
+			L.ny = (int)((h->lv[l - 1].ny - 1) / 2. + 1);
+			L.ns = 5;
+		}
+		L.d = Dims2{L.nx, L.ny, round_up(L.nx + 2, 32)};
+		L.tpitch = round_up(L.ny + 2, 32);
+		const size_t pl = L.d.plane();
+		const size_t tpl = (size_t)L.tpitch * (L.nx + 2);
+		CDR_TRY(h->alloc(&L.so, pl * L.ns));
+		CDR_TRY(h->alloc(&L.x, pl));
+		CDR_TRY(h->alloc(&L.b, pl));
+		CDR_TRY(h->alloc(&L.r, pl));
+		if (l > 0) CDR_TRY(h->alloc(&L.ci, pl * 8));
+		if (l + 1 < nl) {
+			CDR_TRY(h->alloc(&L.sor, pl * 2));
+			CDR_TRY(h->alloc(&L.sory, tpl * 2));
+		}
+		if (h->mixed()) {
+			CDR_TRY(h->alloc(&L.so32, pl * L.ns));
+			CDR_TRY(h->alloc(&L.x32, pl));
+			CDR_TRY(h->alloc(&L.b32, pl));
+			CDR_TRY(h->alloc(&L.r32, pl));
+			if (l > 0) CDR_TRY(h->alloc(&L.ci32, pl * 8));
+			if (l + 1 < nl) {
+				CDR_TRY(h->alloc(&L.sor32, pl * 2));
+				CDR_TRY(h->alloc(&L.sory32, tpl * 2));
+			}
+		}
+	}
+	Level &Cg = h->lv[nl - 1];
+	if ((size_t)Cg.nx * Cg.ny > 4096) {
+		set_error(CDR_ERR_DIM, "coarsest grid %dx%d too large for the banded Cholesky", Cg.nx, Cg.ny);
+		return CDR_ERR_DIM;
+	}
+	CDR_TRY(h->alloc(&h->abd, (size_t)(Cg.nx + 2) * Cg.nx * Cg.ny));
+	CDR_TRY(h->alloc(&h->info, 2));
+	CDR_TRY(h->alloc(&h->norm, 4));
+	CDR_TRY(h->alloc(&h->partial, kNormScratchBytes / sizeof(double)));
+	if (h->mixed()) {
+		CDR_TRY(h->alloc(&h->x64[0], h->lv[0].d.plane()));
+		CDR_TRY(h->alloc(&h->x64[1], h->lv[0].d.plane()));
+	}
+	CDR_CUDA_TRY(cudaMallocHost(&h->h_norm, 4 * sizeof(double)));
+	// fine operator, Cedar layout (pitch nx+2) -> device pitch
+	Level &F = h->lv[0];
+	CDR_CUDA_TRY(cudaMemcpy2DAsync(F.so, F.d.pitch * sizeof(double), so_host, (nx + 2) * sizeof(double),
+	                               (nx + 2) * sizeof(double), (size_t)(ny + 2) * ns, cudaMemcpyHostToDevice, h->st));
+	CDR_CUDA_TRY(cudaEventRecord(h->ev0, h->st));
+	CDR_TRY(h->setup());
+	CDR_CUDA_TRY(cudaEventRecord(h->ev1, h->st));
+	CDR_CUDA_TRY(cudaEventSynchronize(h->ev1));
+	CDR_CUDA_TRY(cudaEventElapsedTime(&h->setup_ms, h->ev0, h->ev1));
+	return CDR_OK;
+}
+
+int cdr_gpu_solver_create_2d(const cdr_gpu_settings *s, const double *so_host, int ns, int nx, int ny,
+                             cudaStream_t stream, cdr_gpu_solver **out)
+{
+	if (!s || !so_host || !out) { set_error(CDR_ERR_ARG, "null argument"); return CDR_ERR_ARG; }
+	if (ns != 3 && ns != 5) { set_error(CDR_ERR_ARG, "nstencil must be 3 or 5"); return CDR_ERR_ARG; }
+	if (nx < 1 || ny < 1) { set_error(CDR_ERR_DIM, "bad grid %dx%d", nx, ny); return CDR_ERR_DIM; }
+	if (s->relaxation < CDR_RELAX_POINT || s->relaxation > CDR_RELAX_LINE_XY) {
+		set_error(CDR_ERR_ARG, "invalid relaxation %d", s->relaxation);
+		return CDR_ERR_ARG;
+	}
+	if (s->precision != CDR_PREC_F64 && s->precision != CDR_PREC_F32_IR) {
+		set_error(CDR_ERR_ARG, "invalid precision %d", s->precision);
+		return CDR_ERR_ARG;
+	}
+	*out = nullptr;
+	cdr_gpu_solver *h = new cdr_gpu_solver();
+	h->s = *s;
+	if (stream) h->st = stream;
+	else {
+		if (cudaStreamCreateWithFlags(&h->st, cudaStreamNonBlocking) != cudaSuccess) {
+			set_error(CDR_ERR_CUDA, "cannot create stream");
+			delete h;
+			return CDR_ERR_CUDA;
+		}
+		h->own_stream = true;
+	}
+	cudaEventCreate(&h->ev0);
+	cudaEventCreate(&h->ev1);
+	int rc = lines_prepare();
+	if (rc == CDR_OK) rc = create_impl(h, so_host, ns, nx, ny);
+	if (rc != CDR_OK) {
+		cdr_gpu_solver_destroy(h);
+		return rc;
+	}
+	*out = h;
+	return CDR_OK;
+}
+
+// multilevel::solve (include/cedar/multilevel.h:278-298) on the level-0 buffers.
+static int solve_loaded(cdr_gpu_solver *h, int *iters, double *hist, int maxhist)
+{
+	Level &F = h->lv[0];
+	cudaStream_t st = h->st;
+	double res0 = 0;
+	int it = 0;
+	CDR_CUDA_TRY(cudaEventRecord(h->ev0, st));
+	if (!h->mixed()) {
+		CDR_TRY(residual_2d<double>(F.so, F.ns, F.x, F.b, F.r, F.d, h->norm, h->partial, st));
+		CDR_CUDA_TRY(cudaMemcpyAsync(h->h_norm, h->norm, sizeof(double), cudaMemcpyDeviceToHost, st));
+		CDR_CUDA_TRY(cudaStreamSynchronize(st));
+		res0 = h->h_norm[0];
+		for (it = 0; it < h->s.maxiter;) {
+			CDR_TRY(h->run_cycle(0));
+			CDR_TRY(residual_2d<double>(F.so, F.ns, F.x, F.b, F.r, F.d, h->norm, h->partial, st));
+			CDR_CUDA_TRY(cudaMemcpyAsync(h->h_norm, h->norm, sizeof(double), cudaMemcpyDeviceToHost, st));
+			CDR_CUDA_TRY(cudaStreamSynchronize(st));
+			double rel = h->h_norm[0] / res0;
+			if (hist && it < maxhist) hist[it] = rel;
+			++it;
+			if (!std::isfinite(rel)) {
+				set_error(CDR_ERR_NUMERIC, "non-finite residual norm at iteration %d", it - 1);
+				return CDR_ERR_NUMERIC;
+			}
+			if (rel < h->s.tol) break;
+		}
+	} else {
+		// x64[0] = x; r = b - A x (FP64), r32 -> level-0 FP32 right-hand side
+		int cur = 0;
+		CDR_CUDA_TRY(cudaMemcpyAsync(h->x64[0], F.x, sizeof(double) * F.d.plane(), cudaMemcpyDeviceToDevice, st));
+		CDR_TRY(ir_residual_2d(F.so, F.ns, h->x64[0], F.x32, F.b, h->x64[1], F.b32, F.d, F.d, h->norm, h->partial, 0,
+		                       st));
+		CDR_CUDA_TRY(cudaMemcpyAsync(h->h_norm, h->norm, sizeof(double), cudaMemcpyDeviceToHost, st));
+		CDR_CUDA_TRY(cudaStreamSynchronize(st));
+		res0 = h->h_norm[0];
+		for (it = 0; it < h->s.maxiter;) {
+			CDR_CUDA_TRY(cudaMemsetAsync(F.x32, 0, sizeof(float) * F.d.plane(), st));
+			CDR_TRY(h->run_cycle(1));
+			CDR_TRY(ir_residual_2d(F.so, F.ns, h->x64[cur], F.x32, F.b, h->x64[1 - cur], F.b32, F.d, F.d, h->norm,
+			                       h->partial, 1, st));
+			cur = 1 - cur;
+			CDR_CUDA_TRY(cudaMemcpyAsync(h->h_norm, h->norm, sizeof(double), cudaMemcpyDeviceToHost, st));
+			CDR_CUDA_TRY(cudaStreamSynchronize(st));
+			double rel = h->h_norm[0] / res0;
+			if (hist && it < maxhist) hist[it] = rel;
+			++it;
+			if (!std::isfinite(rel)) {
+				set_error(CDR_ERR_NUMERIC, "non-finite residual norm at iteration %d", it - 1);
+				return CDR_ERR_NUMERIC;
+			}
+			if (rel < h->s.tol) break;
+		}
+		CDR_CUDA_TRY(cudaMemcpyAsync(F.x, h->x64[cur], sizeof(double) * F.d.plane(), cudaMemcpyDeviceToDevice, st));
+	}
+	CDR_CUDA_TRY(cudaEventRecord(h->ev1, st));
+	CDR_CUDA_TRY(cudaEventSynchronize(h->ev1));
+	CDR_CUDA_TRY(cudaEventElapsedTime(&h->solve_ms, h->ev0, h->ev1));
+	if (iters) *iters = it;
+	return CDR_OK;
+}
+
+int cdr_gpu_solver_solve(cdr_gpu_solver *h, const double *b_host, double *x_host, int *iters, double *hist,
+                         int maxhist)
+{
+	if (!h) { set_error(CDR_ERR_HANDLE, "null solver"); return CDR_ERR_HANDLE; }
+	if (!b_host || !x_host) { set_error(CDR_ERR_ARG, "null buffer"); return CDR_ERR_ARG; }
+	Level &F = h->lv[0];
+	const size_t w = (F.nx + 2) * sizeof(double);
+	CDR_CUDA_TRY(cudaMemcpy2DAsync(F.b, F.d.pitch * sizeof(double), b_host, w, w, F.ny + 2, cudaMemcpyHostToDevice,
+	                               h->st));
+	CDR_CUDA_TRY(cudaMemcpy2DAsync(F.x, F.d.pitch * sizeof(double), x_host, w, w, F.ny + 2, cudaMemcpyHostToDevice,
+	                               h->st));
+	CDR_TRY(solve_loaded(h, iters, hist, maxhist));
+	CDR_CUDA_TRY(cudaMemcpy2DAsync(x_host, w, F.x, F.d.pitch * sizeof(double), w, F.ny + 2, cudaMemcpyDeviceToHost,
+	                               h->st));
+	CDR_CUDA_TRY(cudaStreamSynchronize(h->st));
+	return CDR_OK;
+}
+
+int cdr_gpu_solver_solve_device(cdr_gpu_solver *h, const double *b_dev, double *x_dev, int pitch, int *iters,
+                                double *hist, int maxhist)
+{
+	if (!h) { set_error(CDR_ERR_HANDLE, "null solver"); return CDR_ERR_HANDLE; }
+	if (!b_dev || !x_dev) { set_error(CDR_ERR_ARG, "null buffer"); return CDR_ERR_ARG; }
+	Level &F = h->lv[0];
+	if (pitch < F.nx + 2) { set_error(CDR_ERR_DIM, "pitch %d < nx+2", pitch); return CDR_ERR_DIM; }
+	const size_t w = (F.nx + 2) * sizeof(double);
+	CDR_CUDA_TRY(cudaMemcpy2DAsync(F.b, F.d.pitch * sizeof(double), b_dev, pitch * sizeof(double), w, F.ny + 2,
+	                               cudaMemcpyDeviceToDevice, h->st));
+	CDR_CUDA_TRY(cudaMemcpy2DAsync(F.x, F.d.pitch * sizeof(double), x_dev, pitch * sizeof(double), w, F.ny + 2,
+	                               cudaMemcpyDeviceToDevice, h->st));
+	CDR_TRY(solve_loaded(h, iters, hist, maxhist));
+	CDR_CUDA_TRY(cudaMemcpy2DAsync(x_dev, pitch * sizeof(double), F.x, F.d.pitch * sizeof(double), w, F.ny + 2,
+	                               cudaMemcpyDeviceToDevice, h->st));
+	CDR_CUDA_TRY(cudaStreamSynchronize(h->st));
+	return CDR_OK;
+}
+
+int cdr_gpu_solver_vcycle_device(cdr_gpu_solver *h, const double *b_dev, double *x_dev, int pitch)
+{
+	if (!h) { set_error(CDR_ERR_HANDLE, "null solver"); return CDR_ERR_HANDLE; }
+	if (!b_dev || !x_dev) { set_error(CDR_ERR_ARG, "null buffer"); return CDR_ERR_ARG; }
+	Level &F = h->lv[0];
+	if (pitch < F.nx + 2) { set_error(CDR_ERR_DIM, "pitch %d < nx+2", pitch); return CDR_ERR_DIM; }
+	const size_t w = (F.nx + 2) * sizeof(double);
+	CDR_CUDA_TRY(cudaMemcpy2DAsync(F.b, F.d.pitch * sizeof(double), b_dev, pitch * sizeof(double), w, F.ny + 2,
+	                               cudaMemcpyDeviceToDevice, h->st));
+	CDR_CUDA_TRY(cudaMemcpy2DAsync(F.x, F.d.pitch * sizeof(double), x_dev, pitch * sizeof(double), w, F.ny + 2,
+	                               cudaMemcpyDeviceToDevice, h->st));
+	CDR_TRY(h->run_cycle(0));
+	CDR_CUDA_TRY(cudaMemcpy2DAsync(x_dev, pitch * sizeof(double), F.x, F.d.pitch * sizeof(double), w, F.ny + 2,
+	                               cudaMemcpyDeviceToDevice, h->st));
+	CDR_CUDA_TRY(cudaStreamSynchronize(h->st));
+	return CDR_OK;
+}
+
+int cdr_gpu_solver_nlevels(const cdr_gpu_solver *h) { return h ? (int)h->lv.size() : -1; }
+
+int cdr_gpu_solver_level(const cdr_gpu_solver *h, int level, int which, void **ptr, int *nx, int *ny, int *pitch,
+                         int *tpitch, int *nstencil)
+{
+	if (!h) { set_error(CDR_ERR_HANDLE, "null solver"); return CDR_ERR_HANDLE; }
+	if (level < 0 || level >= (int)h->lv.size()) { set_error(CDR_ERR_ARG, "bad level %d", level); return CDR_ERR_ARG; }
+	const Level &L = h->lv[level];
+	void *p = nullptr;
+	switch (which) {
+	case 0: p = L.so; break;
+	case 1: p = L.x; break;
+	case 2: p = L.b; break;
+	case 3: p = L.r; break;
+	case 4: p = L.sor; break;
+	case 5: p = L.sory; break;
+	case 6: p = L.ci; break;
+	case 16: p = L.so32; break;
+	case 17: p = L.x32; break;
+	case 18: p = L.b32; break;
+	case 19: p = L.r32; break;
+	case 20: p = L.sor32; break;
+	case 21: p = L.sory32; break;
+	case 22: p = L.ci32; break;
+	case 100: p = h->abd; break;
+	default: set_error(CDR_ERR_ARG, "bad array id %d", which); return CDR_ERR_ARG;
+	}
+	if (ptr) *ptr = p;
+	if (nx) *nx = L.nx;
+	if (ny) *ny = L.ny;
+	if (pitch) *pitch = L.d.pitch;
+	if (tpitch) *tpitch = L.tpitch;
+	if (nstencil) *nstencil = L.ns;
+	return CDR_OK;
+}
+
+int cdr_gpu_solver_level_get(const cdr_gpu_solver *h, int level, int which, void *host, size_t bytes)
+{
+	void *p = nullptr;
+	int nx, ny, pitch, tpitch, ns;
+	CDR_TRY(cdr_gpu_solver_level(h, level, which, &p, &nx, &ny, &pitch, &tpitch, &ns));
+	if (!p) { set_error(CDR_ERR_ARG, "array %d not allocated on level %d", which, level); return CDR_ERR_ARG; }
+	const int w = which & 15;
+	const size_t elem = which >= 16 && which < 100 ? sizeof(float) : sizeof(double);
+	size_t n;
+	if (which == 100) n = (size_t)(nx + 2) * nx * ny;
+	else if (w == 5) n = (size_t)2 * tpitch * (nx + 2);
+	else n = (size_t)(w == 0 ? ns : w == 4 ? 2 : w == 6 ? 8 : 1) * pitch * (ny + 2);
+	if (!host || bytes < n * elem) { set_error(CDR_ERR_ARG, "host buffer too small (%zu < %zu)", bytes, n * elem); return CDR_ERR_ARG; }
+	CDR_CUDA_TRY(cudaMemcpyAsync(host, p, n * elem, cudaMemcpyDeviceToHost, h->st));
+	CDR_CUDA_TRY(cudaStreamSynchronize(h->st));
+	return CDR_OK;
+}
+
+int cdr_gpu_solver_timings(const cdr_gpu_solver *h, double *setup_ms, double *solve_ms)
+{
+	if (!h) return CDR_ERR_HANDLE;
+	if (setup_ms) *setup_ms = h->setup_ms;
+	if (solve_ms) *solve_ms = h->solve_ms;
+	return CDR_OK;
+}
+
+}  // extern "C"

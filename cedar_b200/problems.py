@@ -1,0 +1,96 @@
+"""Seeded synthetic problems for the benchmark and the parity tests.
+
+No dataset is involved: every input is generated here from numpy
+``default_rng(seed)`` streams, identically for the oracle and the GPU.
+
+* ``poisson_noise(n)``      5-point Poisson, b = (sin(pi x) sin(pi y) + U[-1e-3,1e-3]) h^2.
+* ``hetero_diffusion(n)``   9-point bilinear-FE operator of -div(K grad u) on an
+  (n+1)^2 cell mesh: K = exp(g), g a Gaussian random field (Gaussian covariance,
+  correlation length ell, standard deviation sigma), optional axis-aligned
+  rectangular inclusions with a contrast factor, optional anisotropy
+  (ky = eps * kx in cells whose centre has y > 0.5); b = U[0,1] h^2.
+"""
+import math
+
+import numpy as np
+
+from . import gallery
+
+
+def poisson_noise(n, seed=0):
+    """5-point Poisson, n x n interior nodes, h = 1/(n+1)."""
+    so = gallery.poisson(n, n)
+    h = 1.0 / (n + 1)
+    x = np.arange(1, n + 1) * h
+    f = np.sin(math.pi * x)[None, :] * np.sin(math.pi * x)[:, None]
+    rng = np.random.default_rng(seed)
+    f = f + rng.uniform(-1e-3, 1e-3, size=(n, n))
+    b = np.zeros((n + 2, n + 2))
+    b[1:-1, 1:-1] = f * h * h
+    return so, b
+
+
+def gaussian_field(ncx, ncy, ell, sigma, seed):
+    """Stationary Gaussian random field on the cell centres of the unit square.
+
+    FFT synthesis on a periodic box twice the domain (to suppress wrap-around
+    correlation): white noise times the square root of the spectral density of
+    the Gaussian covariance exp(-r^2 / (2 ell^2)), scaled to standard deviation
+    sigma.
+    """
+    rng = np.random.default_rng(seed)
+    mx, my = 2 * ncx, 2 * ncy
+    hx, hy = 1.0 / ncx, 1.0 / ncy
+    kx = np.fft.fftfreq(mx, d=hx) * 2 * math.pi
+    ky = np.fft.rfftfreq(my, d=hy) * 2 * math.pi
+    K2 = kx[:, None] ** 2 + ky[None, :] ** 2
+    spec = np.exp(-0.5 * ell * ell * K2)
+    noise = rng.standard_normal((mx, my))
+    fld = np.fft.irfft2(np.fft.rfft2(noise) * np.sqrt(spec), s=(mx, my))[:ncx, :ncy]
+    fld = fld - fld.mean()
+    std = fld.std()
+    if std > 0:
+        fld = fld * (sigma / std)
+    return np.ascontiguousarray(fld.T)  # (ncy, ncx)
+
+
+def inclusions(ncx, ncy, count, contrast, seed, smin=1.0 / 64, smax=1.0 / 8):
+    """Multiplicative factor per cell: ``contrast`` inside ``count`` random rectangles."""
+    rng = np.random.default_rng(seed)
+    fac = np.ones((ncy, ncx))
+    xc = (np.arange(ncx) + 0.5) / ncx
+    yc = (np.arange(ncy) + 0.5) / ncy
+    for _ in range(count):
+        w, hgt = rng.uniform(smin, smax, size=2)
+        x0, y0 = rng.uniform(0, 1 - w), rng.uniform(0, 1 - hgt)
+        mx = (xc >= x0) & (xc < x0 + w)
+        my = (yc >= y0) & (yc < y0 + hgt)
+        fac[np.ix_(my, mx)] = contrast
+    return fac
+
+
+def hetero_coefficients(n, ell=1.0 / 32, sigma=2.0, n_incl=64, contrast=1e4, aniso=1e-3,
+                        seed_field=1, seed_incl=2):
+    """(kx, ky) per cell for an (n+1) x (n+1) cell mesh."""
+    nc = n + 1
+    k = np.exp(gaussian_field(nc, nc, ell, sigma, seed_field))
+    if n_incl:
+        k = k * inclusions(nc, nc, n_incl, contrast, seed_incl)
+    kx = k
+    ky = k.copy()
+    if aniso is not None and aniso != 1.0:
+        yc = (np.arange(nc) + 0.5) / nc
+        ky[yc > 0.5, :] *= aniso
+    return kx, ky
+
+
+def hetero_diffusion(n, ell=1.0 / 32, sigma=2.0, n_incl=64, contrast=1e4, aniso=1e-3,
+                     seed_field=1, seed_incl=2, seed_rhs=3):
+    """9-point heterogeneous diffusion problem on n x n interior nodes."""
+    kx, ky = hetero_coefficients(n, ell, sigma, n_incl, contrast, aniso, seed_field, seed_incl)
+    so = gallery.fe_hetero(kx, ky)
+    h = 1.0 / (n + 1)
+    rng = np.random.default_rng(seed_rhs)
+    b = np.zeros((n + 2, n + 2))
+    b[1:-1, 1:-1] = rng.uniform(0.0, 1.0, size=(n, n)) * h * h
+    return so, b

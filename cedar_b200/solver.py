@@ -1,0 +1,131 @@
+"""``cdr2::solver`` on the GPU: setup in the constructor, ``solve``/``vcycle`` after.
+
+Mirrors include/cedar/2d/solver.h:45-129 and include/cedar/multilevel.h:80-298:
+
+    so = gallery.poisson(nx, ny)          # stencil_op<five_pt>, Cedar layout
+    bmg = Solver2D(so, Config("config.json"))
+    x = bmg.solve(b)                      # zeros initial guess, like solve(b)
+    bmg.history                           # relative l2 residual per cycle
+
+All arithmetic runs in libcdrgpu.so on the current CUDA device; host arrays
+are numpy arrays in Cedar's layout (grid functions (ny+2, nx+2), stencils
+(nstencil, ny+2, nx+2)).  Device arrays may be torch CUDA tensors.
+"""
+import ctypes
+
+import numpy as np
+
+from . import _lib
+from .config import Config, MLSettings
+
+PLANE_NAMES = {"so": 0, "x": 1, "b": 2, "res": 3, "sor": 4, "sory": 5, "ci": 6}
+
+
+def _settings(ms: MLSettings):
+    if ms.relaxation not in _lib.RELAX:
+        raise NotImplementedError("relaxation %r is a 3D smoother" % ms.relaxation)
+    if ms.cycle != "v":
+        raise NotImplementedError("only the V-cycle is implemented on the GPU")
+    if ms.coarse_solver != "LU":
+        raise NotImplementedError("only the LU (banded Cholesky) coarse solver is implemented")
+    s = _lib.Settings()
+    _lib.check(_lib.load().cdr_gpu_settings_default(ctypes.byref(s)))
+    s.relaxation = _lib.RELAX[ms.relaxation]
+    s.nrelax_pre = ms.nrelax_pre
+    s.nrelax_post = ms.nrelax_post
+    s.num_levels = ms.num_levels
+    s.maxiter = ms.maxiter
+    s.tol = ms.tol
+    s.min_coarse = ms.min_coarse
+    s.precision = _lib.PREC[ms.precision]
+    s.use_graph = 1 if ms.use_graph else 0
+    return s
+
+
+class Solver2D:
+    """BoxMG 2D solver whose setup and solve run on the GPU."""
+
+    def __init__(self, so, conf=None, stream=0):
+        self.lib = _lib.load()
+        so = np.ascontiguousarray(so, dtype=np.float64)
+        if so.ndim != 3 or so.shape[0] not in (3, 5):
+            raise ValueError("stencil must have shape (3|5, ny+2, nx+2)")
+        self.nstencil = so.shape[0]
+        self.ny, self.nx = so.shape[1] - 2, so.shape[2] - 2
+        self.settings = conf if isinstance(conf, MLSettings) else MLSettings(conf)
+        self._s = _settings(self.settings)
+        h = ctypes.c_void_p()
+        _lib.check(self.lib.cdr_gpu_solver_create_2d(ctypes.byref(self._s), so.ctypes.data, self.nstencil,
+                                                     self.nx, self.ny, ctypes.c_void_p(stream), ctypes.byref(h)))
+        self.h = h
+        self.history = np.zeros(0)
+        self.iters = 0
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.cdr_gpu_solver_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def nlevels(self):
+        return self.lib.cdr_gpu_solver_nlevels(self.h)
+
+    def timings(self):
+        a, b = ctypes.c_double(), ctypes.c_double()
+        _lib.check(self.lib.cdr_gpu_solver_timings(self.h, ctypes.byref(a), ctypes.byref(b)))
+        return a.value, b.value
+
+    def level_info(self, level, which="so", fp32=False):
+        """(device pointer, nx, ny, pitch, tpitch, nstencil) of a level array."""
+        p = ctypes.c_void_p()
+        vals = [ctypes.c_int() for _ in range(5)]
+        wid = PLANE_NAMES[which] + (16 if fp32 else 0) if which != "abd" else 100
+        _lib.check(self.lib.cdr_gpu_solver_level(self.h, level, wid, ctypes.byref(p), *[ctypes.byref(v) for v in vals]))
+        return (p.value,) + tuple(v.value for v in vals)
+
+    def level_array(self, level, which="so", fp32=False):
+        """Host copy of a level array in Cedar's layout (planes, ny+2, nx+2); the
+        transposed y-line factors come back as (2, nx+2, ny+2)."""
+        p, nx, ny, pitch, tpitch, ns = self.level_info(level, which, fp32)
+        wid = PLANE_NAMES[which] + (16 if fp32 else 0)
+        planes = {"so": ns, "sor": 2, "ci": 8}.get(which, 1)
+        dt = np.float32 if fp32 else np.float64
+        if which == "sory":
+            buf = np.zeros((2, nx + 2, tpitch), dtype=dt)
+        else:
+            buf = np.zeros((planes, ny + 2, pitch), dtype=dt)
+        _lib.check(self.lib.cdr_gpu_solver_level_get(self.h, level, wid, buf.ctypes.data, buf.nbytes))
+        out = buf[..., :ny + 2] if which == "sory" else buf[..., :nx + 2]
+        return np.ascontiguousarray(out if planes > 1 or which == "sory" else out[0])
+
+    def solve(self, b, x=None):
+        """Solve A x = b from host arrays (Cedar layout); returns x (numpy)."""
+        b = np.ascontiguousarray(b, dtype=np.float64)
+        if b.shape != (self.ny + 2, self.nx + 2):
+            raise ValueError("rhs shape %s does not match the grid" % (b.shape,))
+        x = np.zeros_like(b) if x is None else np.ascontiguousarray(x, dtype=np.float64).copy()
+        hist = np.zeros(max(self.settings.maxiter, 1))
+        it = ctypes.c_int()
+        _lib.check(self.lib.cdr_gpu_solver_solve(self.h, b.ctypes.data, x.ctypes.data, ctypes.byref(it),
+                                                 hist.ctypes.data, len(hist)))
+        self.iters = it.value
+        self.history = hist[:it.value].copy()
+        return x
+
+    def solve_device(self, b_ptr, x_ptr, pitch):
+        """Solve with device buffers (e.g. ``tensor.data_ptr()``), x holds the initial guess."""
+        hist = np.zeros(max(self.settings.maxiter, 1))
+        it = ctypes.c_int()
+        _lib.check(self.lib.cdr_gpu_solver_solve_device(self.h, ctypes.c_void_p(b_ptr), ctypes.c_void_p(x_ptr),
+                                                        pitch, ctypes.byref(it), hist.ctypes.data, len(hist)))
+        self.iters = it.value
+        self.history = hist[:it.value].copy()
+
+    def vcycle_device(self, b_ptr, x_ptr, pitch):
+        _lib.check(self.lib.cdr_gpu_solver_vcycle_device(self.h, ctypes.c_void_p(b_ptr), ctypes.c_void_p(x_ptr), pitch))

@@ -1,0 +1,218 @@
+/*
+ * cdr_gpu.h -- C ABI of cedar_b200, the B200 (sm_100a) BoxMG kernels and solver.
+ *
+ * Every entry point is extern "C", takes plain pointers and sizes and returns
+ * an int status (CDR_OK = 0).  Kernel entry points take DEVICE pointers and a
+ * cudaStream_t and are stream ordered; they replace the Fortran BIND(C)
+ * routines that Cedar's serial C++ kernels call (the call each one replaces is
+ * cited beside it, as path:line in cedar-framework/cedar).
+ *
+ * 2D array layout (Cedar's, include/cedar/stencil_op_nd.h:41-78): one ghost
+ * ring, i fastest, one plane per stencil direction.  A grid of nx*ny interior
+ * points has (nx+2)*(ny+2) entries per plane; "pitch" is the number of
+ * elements between row starts (pitch >= nx+2; Cedar's own host arrays have
+ * pitch = nx+2) and planes are pitch*(ny+2) elements apart.  Stencil planes:
+ * five_pt {c, w, s} (nstencil = 3), nine_pt {c, w, s, sw, nw} (nstencil = 5)
+ * (include/cedar/2d/stencil_op.h:9-10).  Interpolation weights: 8 planes
+ * {L, R, A, B, SW, NW, NE, SE} on the coarse grid (include/cedar/2d/prolong_op.h:14).
+ */
+#ifndef CDR_GPU_H
+#define CDR_GPU_H
+
+#include <stddef.h>
+#include <cuda_runtime_api.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes (modelled on include/cedar/capi.h:12-24). */
+#define CDR_OK              0
+#define CDR_ERR_ARG         1  /* bad argument (null pointer, bad enum)        */
+#define CDR_ERR_DIM         2  /* dimension / pitch mismatch                   */
+#define CDR_ERR_CUDA        3  /* CUDA runtime error (launch, copy, alloc)     */
+#define CDR_ERR_SETUP       4  /* factorization failed (non-positive pivot)    */
+#define CDR_ERR_HANDLE      5  /* invalid solver handle                        */
+#define CDR_ERR_NUMERIC     6  /* NaN or Inf met in a residual norm            */
+#define CDR_ERR_UNSUPPORTED 7  /* option not implemented                       */
+#define CDR_ERR_TIMEOUT     8  /* bounded device wait gave up                  */
+
+/* cycle::Dir (include/cedar/cycle/types.h); BMG_DOWN=0, BMG_UP=1 (BMG_parameters_c.h:240-244) */
+#define CDR_DOWN 0
+#define CDR_UP   1
+
+/* ml_settings::relax_type (include/cedar/multilevel_settings.h:30-31) */
+#define CDR_RELAX_POINT   0
+#define CDR_RELAX_LINE_X  1
+#define CDR_RELAX_LINE_Y  2
+#define CDR_RELAX_LINE_XY 3
+
+/* Precision of the solve. */
+#define CDR_PREC_F64    0  /* plain FP64 V-cycles: the drop-in path                    */
+#define CDR_PREC_F32_IR 1  /* FP32 V-cycle preconditioner in an FP64 refinement loop  */
+
+/* Line direction */
+#define CDR_DIR_X 0
+#define CDR_DIR_Y 1
+
+/* Text of the last error raised on the calling host thread. */
+const char *cdr_gpu_last_error(void);
+int cdr_gpu_version(void);
+/* Kernel launches issued by this library so far in this process (a replayed
+ * cycle graph counts the launches it holds). */
+long long cdr_gpu_launch_count(void);
+
+/* ------------------------------------------------------------------------
+ * 2D kernels.  T = double (_f64) or float (_f32).
+ * ------------------------------------------------------------------------ */
+
+/* r = b - A x on interior points; replaces kernels::residual::run
+ * (include/cedar/kernels/residual.h:19-26) -> BMG2_SymStd_residual
+ * (include/cedar/2d/residual.h:9-10, src/2d/ftn/BMG2_SymStd_residual.f90:85-119).
+ * If norm_out (device, one double) is non-null it receives ||r||_2 over the
+ * interior (grid_func::lp_norm<2>, include/cedar/2d/grid_func.h:43-54), summed
+ * in FP64 in a fixed order; scratch (device) must then hold
+ * cdr_gpu_norm_scratch_bytes() bytes. */
+size_t cdr_gpu_norm_scratch_bytes(void);
+int cdr_gpu_residual_2d_f64(const double *so, int nstencil, const double *x, const double *b, double *r,
+                            int nx, int ny, int pitch, double *norm_out, void *scratch, cudaStream_t stream);
+int cdr_gpu_residual_2d_f32(const float *so, int nstencil, const float *x, const float *b, float *r,
+                            int nx, int ny, int pitch, double *norm_out, void *scratch, cudaStream_t stream);
+
+/* sor = 1/c; replaces point_relax::setup (include/cedar/kernels/point_relax.h:31-46)
+ * -> BMG2_SymStd_SETUP_recip (src/2d/relax.cc:23-33, src/2d/ftn/BMG2_SymStd_SETUP_recip.f90:63-67).
+ * sor is one plane (Cedar keeps it in plane 2 of a 2-plane relax_stencil). */
+int cdr_gpu_setup_recip_2d_f64(const double *so, double *sor, int nx, int ny, int pitch, cudaStream_t stream);
+int cdr_gpu_setup_recip_2d_f32(const float *so, float *sor, int nx, int ny, int pitch, cudaStream_t stream);
+
+/* One red-black (5-pt) / four-colour (9-pt) Gauss-Seidel sweep; replaces
+ * point_relax::run (include/cedar/kernels/point_relax.h:48-71) -> BMG2_SymStd_relax_GS
+ * (src/2d/relax.cc:38-68, src/2d/ftn/BMG2_SymStd_relax_GS.f90:78-137). */
+int cdr_gpu_relax_point_2d_f64(const double *so, int nstencil, double *x, const double *b, const double *sor,
+                               int nx, int ny, int pitch, int updown, cudaStream_t stream);
+int cdr_gpu_relax_point_2d_f32(const float *so, int nstencil, float *x, const float *b, const float *sor,
+                               int nx, int ny, int pitch, int updown, cudaStream_t stream);
+
+/* Line smoother setup: L*D*L^T factors of every line's tridiagonal, plane 0 = D,
+ * plane 1 = multipliers (LAPACK DPTTRF storage).  Replaces line_relax::setup
+ * (include/cedar/kernels/line_relax.h:22-30) -> BMG2_SymStd_SETUP_lines_{x,y}
+ * (src/2d/relax.cc:79-95, src/2d/ftn/BMG2_SymStd_SETUP_lines_x.f90:68-87,
+ * BMG2_SymStd_SETUP_lines_y.f90:69-88).  dir = CDR_DIR_X: sor has the grid's layout.
+ * dir = CDR_DIR_Y: sor is stored transposed as Cedar does (SOR(JJ,II,2)): element
+ * (j, i) at i*tpitch + j with tpitch >= ny+2, planes tpitch*(nx+2) apart.
+ * The factorization is always done in FP64; the f32 variant rounds the factors. */
+int cdr_gpu_setup_lines_2d_f64(const double *so, int nstencil, double *sor, int nx, int ny, int pitch,
+                               int tpitch, int dir, int *info_dev, cudaStream_t stream);
+int cdr_gpu_setup_lines_2d_f32(const double *so, int nstencil, float *sor, int nx, int ny, int pitch,
+                               int tpitch, int dir, int *info_dev, cudaStream_t stream);
+
+/* One zebra line Gauss-Seidel sweep (both colours); replaces line_relax::run
+ * (include/cedar/kernels/line_relax.h:31-39) -> BMG2_SymStd_relax_lines_{x,y}
+ * (src/2d/relax.cc:98-133, src/2d/ftn/BMG2_SymStd_relax_lines_x.f90:74-131,
+ * BMG2_SymStd_relax_lines_y.f90:74-129). */
+int cdr_gpu_relax_lines_2d_f64(const double *so, int nstencil, double *x, const double *b, const double *sor,
+                               int nx, int ny, int pitch, int tpitch, int dir, int updown, cudaStream_t stream);
+int cdr_gpu_relax_lines_2d_f32(const float *so, int nstencil, float *x, const float *b, const float *sor,
+                               int nx, int ny, int pitch, int tpitch, int dir, int updown, cudaStream_t stream);
+
+/* b_coarse = P^T r_fine; replaces restriction::run (include/cedar/kernels/restrict.h:17-19)
+ * -> BMG2_SymStd_restrict (src/2d/restrict.cc:14-29, src/2d/ftn/BMG2_SymStd_restrict.f90:72-92). */
+int cdr_gpu_restrict_2d_f64(const double *ci, const double *r_fine, double *b_coarse,
+                            int nxf, int nyf, int pitchf, int nxc, int nyc, int pitchc, cudaStream_t stream);
+int cdr_gpu_restrict_2d_f32(const float *ci, const float *r_fine, float *b_coarse,
+                            int nxf, int nyf, int pitchf, int nxc, int nyc, int pitchc, cudaStream_t stream);
+
+/* x_fine += P x_coarse + r/c at fine-only points; replaces interp_add::run
+ * (include/cedar/kernels/interp_add.h:17-20) -> BMG2_SymStd_interp_add (src/2d/interp.cc:20-46,
+ * src/2d/ftn/BMG2_SymStd_interp_add.f90:89-137).  so_fine is the fine operator
+ * (only its c plane is read).  Unlike the reference, res_fine is not overwritten
+ * by res/c (no later step reads it). */
+int cdr_gpu_interp_add_2d_f64(const double *ci, const double *x_coarse, const double *res_fine,
+                              const double *so_fine, double *x_fine,
+                              int nxf, int nyf, int pitchf, int nxc, int nyc, int pitchc, cudaStream_t stream);
+int cdr_gpu_interp_add_2d_f32(const float *ci, const float *x_coarse, const float *res_fine,
+                              const float *so_fine, float *x_fine,
+                              int nxf, int nyf, int pitchf, int nxc, int nyc, int pitchc, cudaStream_t stream);
+
+/* Operator-induced interpolation weights; replaces setup_interp::run
+ * (include/cedar/kernels/setup_interp.h:30-47) -> BMG2_SymStd_SETUP_interp_OI
+ * (src/2d/interp.cc:49-106, src/2d/ftn/BMG2_SymStd_SETUP_interp_OI.f90:85-257). */
+int cdr_gpu_setup_interp_2d_f64(const double *so_fine, int nstencil, double *ci,
+                                int nxf, int nyf, int pitchf, int nxc, int nyc, int pitchc, cudaStream_t stream);
+
+/* Galerkin coarse operator so_coarse = P^T A P (5 planes); replaces coarsen_op::run
+ * (include/cedar/kernels/coarsen_op.h:23-40) -> BMG2_SymStd_SETUP_ITLI_ex
+ * (include/cedar/2d/coarsen.h:34-61, src/2d/ftn/BMG2_SymStd_SETUP_ITLI_ex.f90:94-331). */
+int cdr_gpu_galerkin_2d_f64(const double *so_fine, int nstencil, const double *ci, double *so_coarse,
+                            int nxf, int nyf, int pitchf, int nxc, int nyc, int pitchc, cudaStream_t stream);
+
+/* Coarsest-grid banded Cholesky, LAPACK upper band storage ABD(nx+2, nx*ny)
+ * (column-major, ldab = nx+2, KD = nx+1); replaces solve_cg::setup/run
+ * (include/cedar/kernels/solve_cg.h:20-28) -> BMG2_SymStd_SETUP_cg_LU + DPBTRF
+ * (include/cedar/2d/solve_cg.h:32-55, src/2d/ftn/BMG2_SymStd_SETUP_cg_LU.f90:92-118,229-255)
+ * and BMG2_SymStd_SOLVE_cg + DPBTRS (src/2d/solve_cg.cc:13-28,
+ * src/2d/ftn/BMG2_SymStd_SOLVE_cg.f90:93-123).  The solve is FP64 for both variants. */
+int cdr_gpu_setup_cg_2d_f64(const double *so, int nstencil, int nx, int ny, int pitch, double *abd,
+                            int *info_dev, cudaStream_t stream);
+int cdr_gpu_solve_cg_2d_f64(const double *abd, double *x, const double *b, int nx, int ny, int pitch,
+                            cudaStream_t stream);
+int cdr_gpu_solve_cg_2d_f32(const double *abd, float *x, const float *b, int nx, int ny, int pitch,
+                            cudaStream_t stream);
+
+/* ------------------------------------------------------------------------
+ * 2D multilevel solver: setup in create (multilevel::setup,
+ * include/cedar/multilevel.h:243-265), solve (multilevel::solve, :278-298),
+ * vcycle (multilevel::vcycle, :80-84).
+ * ------------------------------------------------------------------------ */
+
+/* Mirrors ml_settings (include/cedar/multilevel_settings.h:28-50) plus the GPU options. */
+typedef struct cdr_gpu_settings {
+	int relaxation;   /* CDR_RELAX_*            "solver.relaxation"   (default point)  */
+	int nrelax_pre;   /* "solver.cycle.nrelax-pre"  (default 2)                        */
+	int nrelax_post;  /* "solver.cycle.nrelax-post" (default 1)                        */
+	int num_levels;   /* "solver.num-levels"  (-1 = from min_coarse)                   */
+	int maxiter;      /* "solver.max-iter"    (default 10)                             */
+	double tol;       /* "solver.tol"         (default 1e-8)                           */
+	int min_coarse;   /* "solver.min_coarse"  (default 3)                              */
+	int precision;    /* CDR_PREC_F64 (default) or CDR_PREC_F32_IR                     */
+	int use_graph;    /* replay the cycle as a CUDA graph (default 1)                  */
+} cdr_gpu_settings;
+
+typedef struct cdr_gpu_solver cdr_gpu_solver;
+
+int cdr_gpu_settings_default(cdr_gpu_settings *s);
+
+/* Set up the hierarchy from a host fine operator in Cedar's layout
+ * (pitch nx+2, nstencil planes).  stream may be 0 (the library creates its own). */
+int cdr_gpu_solver_create_2d(const cdr_gpu_settings *s, const double *so_host, int nstencil, int nx, int ny,
+                             cudaStream_t stream, cdr_gpu_solver **out);
+int cdr_gpu_solver_destroy(cdr_gpu_solver *h);
+
+/* Solve with HOST buffers in Cedar's layout ((nx+2)*(ny+2) doubles).  x holds the
+ * initial guess on entry (Cedar's solve(b) starts from zero: pass zeros).
+ * iters (may be null) receives the number of cycles run, hist (may be null) the
+ * relative l2 residual after each cycle. */
+int cdr_gpu_solver_solve(cdr_gpu_solver *h, const double *b_host, double *x_host, int *iters,
+                         double *hist, int maxhist);
+/* Same with DEVICE buffers of the given pitch. */
+int cdr_gpu_solver_solve_device(cdr_gpu_solver *h, const double *b_dev, double *x_dev, int pitch,
+                                int *iters, double *hist, int maxhist);
+/* One cycle x <- x + B(b - A x) on DEVICE buffers (multilevel::vcycle). */
+int cdr_gpu_solver_vcycle_device(cdr_gpu_solver *h, const double *b_dev, double *x_dev, int pitch);
+
+int cdr_gpu_solver_nlevels(const cdr_gpu_solver *h);
+/* Level geometry and device arrays, for tests and tooling.  which: 0 so, 1 x,
+ * 2 b, 3 res, 4 sor (point: 1/c; lines: x factors), 5 y factors, 6 ci.  For the
+ * FP32 preconditioner arrays add 16 to which. */
+int cdr_gpu_solver_level(const cdr_gpu_solver *h, int level, int which, void **ptr, int *nx, int *ny,
+                         int *pitch, int *tpitch, int *nstencil);
+/* Copy a level array (as returned by cdr_gpu_solver_level, all planes, padded
+ * rows) into a host buffer of at least `bytes` bytes. */
+int cdr_gpu_solver_level_get(const cdr_gpu_solver *h, int level, int which, void *host, size_t bytes);
+/* Setup and solve timings of the last calls (ms, from CUDA events). */
+int cdr_gpu_solver_timings(const cdr_gpu_solver *h, double *setup_ms, double *solve_ms);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,290 @@
+"""ctypes wrapper of the CPU parity oracle (``liboracle.so``).
+
+TEST INFRASTRUCTURE ONLY: imported by ``tests/``, ``__graft_entry__.smoke`` and the
+CPU-baseline leg of ``bench.py``.  The product path (``cedar_b200``) never imports it.
+
+Array convention (same as the reference, Fortran order with one ghost ring):
+a grid function is a numpy array of shape ``(ny+2, nx+2)`` (C order, so i is
+fastest) and a stencil with ``k`` planes has shape ``(k, ny+2, nx+2)``.
+"""
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB = None
+
+RELAX = {"point": 0, "line-x": 1, "line-y": 2, "line-xy": 3}
+ARR = {"so": 0, "x": 1, "b": 2, "res": 3, "sor0": 4, "sor1": 5, "ci": 6, "abd": 7}
+DOWN, UP = 0, 1
+
+
+class Settings(ctypes.Structure):
+    """Mirror of ``ml_settings`` (include/cedar/multilevel_settings.h:28-50)."""
+    _fields_ = [("relax", ctypes.c_int), ("nrelax_pre", ctypes.c_int),
+                ("nrelax_post", ctypes.c_int), ("num_levels", ctypes.c_int),
+                ("maxiter", ctypes.c_int), ("tol", ctypes.c_double),
+                ("min_coarse", ctypes.c_int)]
+
+
+def build():
+    """Compile ``liboracle.so`` from the C restatement (idempotent)."""
+    subprocess.run(["make", "-s", "-C", _HERE], check=True)
+
+
+def lib():
+    global _LIB
+    if _LIB is None:
+        path = os.path.join(_HERE, "liboracle.so")
+        if not os.path.exists(path):
+            build()
+        L = ctypes.CDLL(path)
+        P = ctypes.c_void_p
+        I = ctypes.c_int
+        D = ctypes.c_double
+        sig = {
+            "o_dpttrf": (I, [I, P, P]),
+            "o_dpttrs": (None, [I, P, P, P]),
+            "o_dpbtrf_u": (I, [I, I, P, I]),
+            "o_dpbtrs_u": (None, [I, I, P, I, P]),
+            "o2_residual": (None, [P, P, P, P, I, I, I]),
+            "o2_setup_recip": (None, [P, P, I, I]),
+            "o2_relax_gs": (None, [P, P, P, P, I, I, I, I]),
+            "o2_setup_lines_x": (I, [P, P, I, I]),
+            "o2_setup_lines_y": (I, [P, P, I, I]),
+            "o2_relax_lines_x": (None, [P, P, P, P, I, I, I, I]),
+            "o2_relax_lines_y": (None, [P, P, P, P, I, I, I, I]),
+            "o2_restrict": (None, [P, P, P, I, I, I, I]),
+            "o2_interp_add": (None, [P, P, P, P, P, I, I, I, I]),
+            "o2_setup_interp": (None, [P, P, I, I, I, I, I]),
+            "o2_setup_galerkin": (None, [P, P, P, I, I, I, I, I]),
+            "o2_setup_cg": (I, [P, I, I, I, P, I]),
+            "o2_solve_cg": (None, [P, P, I, I, P, P, I]),
+            "o2_l2norm": (D, [P, I, I]),
+            "o2_inf_norm": (D, [P, I, I]),
+            "o2_num_levels": (I, [I, I, I]),
+            "o2_create": (P, [ctypes.POINTER(Settings), P, I, I, I]),
+            "o2_destroy": (None, [P]),
+            "o2_vcycle": (None, [P, P, P]),
+            "o2_solve": (I, [P, P, P, P, I]),
+            "o2_nlevels": (I, [P]),
+            "o2_info": (I, [P, I]),
+            "o2_level_dims": (None, [P, P]),
+            "o2_level_array": (ctypes.POINTER(ctypes.c_double), [P, I, I]),
+            "o2_abd_dims": (None, [P, P]),
+        }
+        for name, (res, args) in sig.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _LIB = L
+    return _LIB
+
+
+def _p(a):
+    assert a.dtype == np.float64 and a.flags.c_contiguous
+    return a.ctypes.data
+
+
+def _dims(so_or_gf):
+    return so_or_gf.shape[-1], so_or_gf.shape[-2]  # II, JJ
+
+
+# ----------------------------------------------------------------- kernels
+def residual(so, x, b):
+    II, JJ = _dims(x)
+    r = np.zeros_like(x)
+    lib().o2_residual(_p(so), _p(b), _p(x), _p(r), II, JJ, 1 if so.shape[0] == 3 else 0)
+    return r
+
+
+def setup_recip(so):
+    II, JJ = _dims(so)
+    sor = np.zeros((2, JJ, II))
+    lib().o2_setup_recip(_p(so), _p(sor), II, JJ)
+    return sor
+
+
+def relax_gs(so, x, b, sor, updown):
+    II, JJ = _dims(x)
+    lib().o2_relax_gs(_p(so), _p(b), _p(x), _p(sor), II, JJ, 1 if so.shape[0] == 3 else 0, updown)
+    return x
+
+
+def setup_lines_x(so):
+    II, JJ = _dims(so)
+    sor = np.zeros((2, JJ, II))
+    info = lib().o2_setup_lines_x(_p(so), _p(sor), II, JJ)
+    return sor, info
+
+
+def setup_lines_y(so):
+    """Returns SOR stored transposed, shape (2, II, JJ) (Fortran SOR(JJ,II,2))."""
+    II, JJ = _dims(so)
+    sor = np.zeros((2, II, JJ))
+    info = lib().o2_setup_lines_y(_p(so), _p(sor), II, JJ)
+    return sor, info
+
+
+def relax_lines_x(so, x, b, sor, updown):
+    II, JJ = _dims(x)
+    lib().o2_relax_lines_x(_p(so), _p(b), _p(x), _p(sor), II, JJ, 1 if so.shape[0] == 3 else 0, updown)
+    return x
+
+
+def relax_lines_y(so, x, b, sor, updown):
+    II, JJ = _dims(x)
+    lib().o2_relax_lines_y(_p(so), _p(b), _p(x), _p(sor), II, JJ, 1 if so.shape[0] == 3 else 0, updown)
+    return x
+
+
+def restrict(ci, r_fine):
+    IIF, JJF = _dims(r_fine)
+    IIC, JJC = _dims(ci)
+    bc = np.zeros((JJC, IIC))
+    lib().o2_restrict(_p(ci), _p(r_fine), _p(bc), IIF, JJF, IIC, JJC)
+    return bc
+
+
+def interp_add(ci, xc, res, so_fine, x):
+    """x += P xc + res/c at fine-only points; ``res`` is divided in place (as the reference)."""
+    IIC, JJC = _dims(ci)
+    IIF, JJF = _dims(x)
+    ko = np.ascontiguousarray(so_fine[0])
+    lib().o2_interp_add(_p(x), _p(xc), _p(res), _p(ko), _p(ci), IIC, JJC, IIF, JJF)
+    return x
+
+
+def setup_interp(so_fine, nxc, nyc):
+    IIF, JJF = _dims(so_fine)
+    ci = np.zeros((8, nyc + 2, nxc + 2))
+    lib().o2_setup_interp(_p(so_fine), _p(ci), IIF, JJF, nxc + 2, nyc + 2, 1 if so_fine.shape[0] == 3 else 0)
+    return ci
+
+
+def galerkin(so_fine, ci):
+    IIF, JJF = _dims(so_fine)
+    IIC, JJC = _dims(ci)
+    soc = np.zeros((5, JJC, IIC))
+    lib().o2_setup_galerkin(_p(so_fine), _p(soc), _p(ci), IIF, JJF, IIC, JJC, 1 if so_fine.shape[0] == 3 else 0)
+    return soc
+
+
+def setup_cg(so):
+    II, JJ = _dims(so)
+    nx, ny = II - 2, JJ - 2
+    abd = np.zeros((nx * ny, nx + 2))  # Fortran ABD(nx+2, nx*ny)
+    info = lib().o2_setup_cg(_p(so), II, JJ, so.shape[0], _p(abd), nx + 2)
+    return abd, info
+
+
+def solve_cg(abd, b):
+    II, JJ = _dims(b)
+    x = np.zeros_like(b)
+    bbd = np.zeros((II - 2) * (JJ - 2))
+    lib().o2_solve_cg(_p(x), _p(b), II, JJ, _p(abd), _p(bbd), abd.shape[1])
+    return x
+
+
+def l2norm(r):
+    II, JJ = _dims(r)
+    return lib().o2_l2norm(_p(r), II, JJ)
+
+
+def inf_norm(r):
+    II, JJ = _dims(r)
+    return lib().o2_inf_norm(_p(r), II, JJ)
+
+
+def dpttrf(d, e):
+    d = np.array(d, dtype=np.float64)
+    e = np.array(e, dtype=np.float64)
+    info = lib().o_dpttrf(len(d), _p(d), _p(e))
+    return d, e, info
+
+
+def dpttrs(d, e, b):
+    b = np.array(b, dtype=np.float64)
+    lib().o_dpttrs(len(d), _p(np.ascontiguousarray(d)), _p(np.ascontiguousarray(e)), _p(b))
+    return b
+
+
+def dpbtrf_u(ab_fortran, kd):
+    """``ab_fortran``: (ldab, n) band matrix in LAPACK upper storage."""
+    ab = np.ascontiguousarray(np.asarray(ab_fortran, dtype=np.float64).T)  # column-major
+    ldab, n = ab_fortran.shape
+    info = lib().o_dpbtrf_u(n, kd, _p(ab), ldab)
+    return ab.T.copy(), info
+
+
+def dpbtrs_u(ab_fortran, kd, b):
+    ab = np.ascontiguousarray(np.asarray(ab_fortran, dtype=np.float64).T)
+    ldab, n = ab_fortran.shape
+    x = np.array(b, dtype=np.float64)
+    lib().o_dpbtrs_u(n, kd, _p(ab), ldab, _p(x))
+    return x
+
+
+def num_levels(nx, ny, min_coarse=3):
+    return lib().o2_num_levels(nx, ny, min_coarse)
+
+
+# ------------------------------------------------------------------ solver
+class Solver:
+    """Serial BoxMG solver: setup in the constructor, as ``cdr2::solver``."""
+
+    def __init__(self, so, relax="point", nrelax_pre=2, nrelax_post=1, num_levels=-1,
+                 maxiter=10, tol=1e-8, min_coarse=3):
+        so = np.ascontiguousarray(so, dtype=np.float64)
+        self.nstncl = so.shape[0]
+        self.ny, self.nx = so.shape[1] - 2, so.shape[2] - 2
+        self.settings = Settings(RELAX[relax], nrelax_pre, nrelax_post, num_levels, maxiter, tol, min_coarse)
+        self._so = so
+        self.h = lib().o2_create(ctypes.byref(self.settings), _p(so), self.nstncl, self.nx, self.ny)
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib().o2_destroy(self.h)
+            self.h = None
+
+    @property
+    def nlevels(self):
+        return lib().o2_nlevels(self.h)
+
+    def info(self):
+        return lib().o2_info(self.h, 0), lib().o2_info(self.h, 1)
+
+    def level_dims(self, l):
+        d = (ctypes.c_int * 3)()
+        lib().o2_level_dims(self.h, l, d)
+        return d[0], d[1], d[2]
+
+    def level_array(self, l, which):
+        """Copy of a level array in numpy layout."""
+        nx, ny, ns = self.level_dims(l)
+        II, JJ = nx + 2, ny + 2
+        ptr = lib().o2_level_array(self.h, l, ARR[which])
+        if which == "abd":
+            d = (ctypes.c_int * 2)()
+            lib().o2_abd_dims(self.h, d)
+            n = d[0] * d[1]
+            return np.ctypeslib.as_array(ptr, shape=(n,)).copy().reshape(d[1], d[0])
+        shape = {"so": (ns, JJ, II), "ci": (8, JJ, II), "sor0": (2, JJ, II),
+                 "sor1": (2, II, JJ)}.get(which, (JJ, II))
+        n = int(np.prod(shape))
+        return np.ctypeslib.as_array(ptr, shape=(n,)).copy().reshape(shape)
+
+    def vcycle(self, x, b):
+        lib().o2_vcycle(self.h, _p(x), _p(b))
+        return x
+
+    def solve(self, b, x=None):
+        """Returns (x, history of relative l2 residuals)."""
+        b = np.ascontiguousarray(b, dtype=np.float64)
+        if x is None:
+            x = np.zeros_like(b)
+        hist = np.zeros(max(self.settings.maxiter, 1))
+        n = lib().o2_solve(self.h, _p(b), _p(x), _p(hist), len(hist))
+        return x, hist[:n].copy()

@@ -1,0 +1,204 @@
+"""Parity of every 2D CUDA kernel with the CPU oracle, through the C ABI.
+
+Bit-exact: residual, point Gauss-Seidel, restriction, interpolate-add,
+interpolation setup, line factorization and the coarsest Cholesky (same
+operand order, no FMA).  Tolerances: Galerkin 1e-13 (different summation
+order), line relaxation 1e-12 (the substitutions run as a parallel scan),
+FP32 kernels 1e-5 relative to the FP64 oracle.
+"""
+import ctypes
+
+import numpy as np
+import pytest
+
+from cedar_b200 import _lib
+from cedar_b200 import gallery as G
+from cedar_b200 import problems as P
+from tests.gpu_util import dev, host, padded, ptr, rel_err, stream
+
+pytestmark = pytest.mark.gpu
+
+SIZES = [(9, 9, 3), (10, 8, 3), (17, 12, 5), (32, 33, 5), (63, 64, 5), (64, 63, 3), (130, 97, 5)]
+
+
+@pytest.fixture(scope="module")
+def lib():
+    from cedar_b200 import build
+    build.build()
+    return _lib.load()
+
+
+def make_op(nx, ny, ns, seed=0):
+    rng = np.random.default_rng(seed + 7 * nx + ny)
+    if ns == 3:
+        so = G.diag_diffusion(nx, ny, 1.0, 0.5)
+        so[1:] *= 1 + 0.5 * rng.random(so[1:].shape)
+        so[1, :, :2] = 0; so[2, :2, :] = 0; so[:, 0, :] = 0; so[:, :, 0] = 0
+        so[:, -1, :] = 0; so[:, :, -1] = 0
+        so[0, 1:-1, 1:-1] = 2.2 * (so[1, 1:-1, 1:-1] + so[1, 1:-1, 2:] + so[2, 1:-1, 1:-1] + so[2, 2:, 1:-1]) / 2
+        so[0, 1:-1, 1:-1] += 0.1
+    else:
+        kx, ky = P.hetero_coefficients(nx if nx == ny else max(nx, ny), sigma=1.0, n_incl=3, contrast=50.0,
+                                       aniso=0.3, seed_field=seed + 11, seed_incl=seed + 12)
+        so = G.fe_hetero(kx[:ny + 1, :nx + 1], ky[:ny + 1, :nx + 1])
+    return np.ascontiguousarray(so)
+
+
+def grid(nx, ny, seed=1):
+    rng = np.random.default_rng(seed + nx * 3 + ny)
+    a = np.zeros((ny + 2, nx + 2))
+    a[1:-1, 1:-1] = rng.standard_normal((ny, nx))
+    return a
+
+
+@pytest.mark.parametrize("nx,ny,ns", SIZES)
+def test_residual_bitwise_and_norm(lib, oracle, nx, ny, ns):
+    so, x, b = make_op(nx, ny, ns), grid(nx, ny, 1), grid(nx, ny, 2)
+    r_ref = oracle.residual(so, x, b)
+    dso, dx, db = dev(so), dev(x), dev(b)
+    dr = dev(np.zeros_like(x))
+    nrm = dev(np.zeros(1))
+    scratch = dev(np.zeros(lib.cdr_gpu_norm_scratch_bytes() // 8))
+    _lib.check(lib.cdr_gpu_residual_2d_f64(ptr(dso), ns, ptr(dx), ptr(db), ptr(dr), nx, ny, nx + 2, ptr(nrm),
+                                           ptr(scratch), stream()))
+    np.testing.assert_array_equal(host(dr), r_ref)
+    assert abs(host(nrm)[0] - oracle.l2norm(r_ref)) <= 1e-13 * oracle.l2norm(r_ref)
+
+
+@pytest.mark.parametrize("nx,ny,ns", SIZES[:4])
+def test_residual_padded_pitch_and_f32(lib, oracle, nx, ny, ns):
+    so, x, b = make_op(nx, ny, ns), grid(nx, ny, 1), grid(nx, ny, 2)
+    r_ref = oracle.residual(so, x, b)
+    pitch = ((nx + 2 + 31) // 32) * 32
+    dso, dx, db = padded(so, pitch), padded(x, pitch), padded(b, pitch)
+    dr = padded(np.zeros_like(x), pitch)
+    _lib.check(lib.cdr_gpu_residual_2d_f64(ptr(dso), ns, ptr(dx), ptr(db), ptr(dr), nx, ny, pitch, None, None,
+                                           stream()))
+    np.testing.assert_array_equal(host(dr)[:, :nx + 2], r_ref)
+    import torch
+    fso, fx, fb = dso.float(), dx.float(), db.float()
+    fr = torch.zeros_like(fx)
+    _lib.check(lib.cdr_gpu_residual_2d_f32(ptr(fso), ns, ptr(fx), ptr(fb), ptr(fr), nx, ny, pitch, None, None,
+                                           stream()))
+    assert rel_err(host(fr)[:, :nx + 2], r_ref) < 1e-5
+
+
+@pytest.mark.parametrize("nx,ny,ns", SIZES)
+@pytest.mark.parametrize("updown", [0, 1])
+def test_point_relax_bitwise(lib, oracle, nx, ny, ns, updown):
+    so, x, b = make_op(nx, ny, ns), grid(nx, ny, 3), grid(nx, ny, 4)
+    sor = oracle.setup_recip(so)
+    xr = x.copy()
+    for _ in range(2):
+        oracle.relax_gs(so, xr, b, sor, updown)
+    dso, dx, db = dev(so), dev(x), dev(b)
+    dsor = dev(np.zeros_like(x))
+    _lib.check(lib.cdr_gpu_setup_recip_2d_f64(ptr(dso), ptr(dsor), nx, ny, nx + 2, stream()))
+    np.testing.assert_array_equal(host(dsor), sor[1])
+    for _ in range(2):
+        _lib.check(lib.cdr_gpu_relax_point_2d_f64(ptr(dso), ns, ptr(dx), ptr(db), ptr(dsor), nx, ny, nx + 2, updown,
+                                                  stream()))
+    np.testing.assert_array_equal(host(dx), xr)
+
+
+@pytest.mark.parametrize("nx,ny,ns", SIZES)
+def test_interp_setup_transfer_and_galerkin(lib, oracle, nx, ny, ns):
+    so = make_op(nx, ny, ns)
+    nxc, nyc = (nx - 1) // 2 + 1, (ny - 1) // 2 + 1
+    ci = oracle.setup_interp(so, nxc, nyc)
+    soc = oracle.galerkin(so, ci)
+    dso = dev(so)
+    dci = dev(np.zeros_like(ci))
+    _lib.check(lib.cdr_gpu_setup_interp_2d_f64(ptr(dso), ns, ptr(dci), nx, ny, nx + 2, nxc, nyc, nxc + 2, stream()))
+    np.testing.assert_array_equal(host(dci), ci)
+    dsoc = dev(np.zeros_like(soc))
+    _lib.check(lib.cdr_gpu_galerkin_2d_f64(ptr(dso), ns, ptr(dci), ptr(dsoc), nx, ny, nx + 2, nxc, nyc, nxc + 2,
+                                           stream()))
+    assert rel_err(host(dsoc), soc) < 1e-13
+    # restriction and interpolate-add
+    r = grid(nx, ny, 5)
+    bc = oracle.restrict(ci, r)
+    dbc = dev(np.zeros_like(bc))
+    _lib.check(lib.cdr_gpu_restrict_2d_f64(ptr(dci), ptr(dev(r)), ptr(dbc), nx, ny, nx + 2, nxc, nyc, nxc + 2,
+                                           stream()))
+    np.testing.assert_array_equal(host(dbc), bc)
+    xc = grid(nxc, nyc, 6)
+    x = grid(nx, ny, 7)
+    xr = x.copy()
+    oracle.interp_add(ci, xc, r.copy(), so, xr)
+    dx = dev(x)
+    _lib.check(lib.cdr_gpu_interp_add_2d_f64(ptr(dci), ptr(dev(xc)), ptr(dev(r)), ptr(dso), ptr(dx), nx, ny,
+                                             nx + 2, nxc, nyc, nxc + 2, stream()))
+    np.testing.assert_array_equal(host(dx), xr)
+    # FP32 transfer kernels
+    import torch
+    fbc = torch.zeros_like(dbc).float()
+    _lib.check(lib.cdr_gpu_restrict_2d_f32(ptr(dci.float()), ptr(dev(r).float()), ptr(fbc), nx, ny, nx + 2, nxc, nyc,
+                                           nxc + 2, stream()))
+    assert rel_err(host(fbc), bc) < 1e-5
+
+
+@pytest.mark.parametrize("nx,ny,ns", SIZES)
+@pytest.mark.parametrize("updown", [0, 1])
+def test_line_relax(lib, oracle, nx, ny, ns, updown):
+    so, x, b = make_op(nx, ny, ns), grid(nx, ny, 8), grid(nx, ny, 9)
+    sx, ix = oracle.setup_lines_x(so)
+    sy, iy = oracle.setup_lines_y(so)
+    assert ix == 0 and iy == 0
+    dso = dev(so)
+    info = dev(np.zeros(2, dtype=np.int32))
+    dsx = dev(np.zeros_like(sx))
+    dsy = dev(np.zeros_like(sy))
+    _lib.check(lib.cdr_gpu_setup_lines_2d_f64(ptr(dso), ns, ptr(dsx), nx, ny, nx + 2, ny + 2, _lib.DIR_X, ptr(info),
+                                              stream()))
+    _lib.check(lib.cdr_gpu_setup_lines_2d_f64(ptr(dso), ns, ptr(dsy), nx, ny, nx + 2, ny + 2, _lib.DIR_Y, ptr(info),
+                                              stream()))
+    np.testing.assert_array_equal(host(dsx)[:, 1:-1, 1:-1], sx[:, 1:-1, 1:-1])
+    np.testing.assert_array_equal(host(dsy)[:, 1:-1, 1:-1], sy[:, 1:-1, 1:-1])
+    assert (host(info) == 0).all()
+    for direction, sor, dsor, fn in ((_lib.DIR_X, sx, dsx, oracle.relax_lines_x), (_lib.DIR_Y, sy, dsy, oracle.relax_lines_y)):
+        xr = x.copy()
+        fn(so, xr, b, sor, updown)
+        fn(so, xr, b, sor, 1 - updown)
+        dx = dev(x)
+        for ud in (updown, 1 - updown):
+            _lib.check(lib.cdr_gpu_relax_lines_2d_f64(ptr(dso), ns, ptr(dx), ptr(dev(b)), ptr(dsor), nx, ny, nx + 2,
+                                                      ny + 2, direction, ud, stream()))
+        assert rel_err(host(dx), xr) < 1e-12, direction
+        # FP32 factors and sweep
+        fs = dev(np.zeros_like(sor)).float()
+        _lib.check(lib.cdr_gpu_setup_lines_2d_f32(ptr(dso), ns, ptr(fs), nx, ny, nx + 2, ny + 2, direction, ptr(info),
+                                                  stream()))
+        fx = dev(x).float()
+        for ud in (updown, 1 - updown):
+            _lib.check(lib.cdr_gpu_relax_lines_2d_f32(ptr(dso.float()), ns, ptr(fx), ptr(dev(b).float()), ptr(fs), nx,
+                                                      ny, nx + 2, ny + 2, direction, ud, stream()))
+        assert rel_err(host(fx), xr) < 1e-4, direction
+
+
+def test_line_setup_reports_nonpositive_pivot(lib):
+    nx = ny = 8
+    so = G.diag_diffusion(nx, ny, 1.0, 1.0)
+    so[0, 4, 3] = -1.0  # negative diagonal on line j=4
+    info = dev(np.zeros(2, dtype=np.int32))
+    dsx = dev(np.zeros((2, ny + 2, nx + 2)))
+    _lib.check(lib.cdr_gpu_setup_lines_2d_f64(ptr(dev(so)), 3, ptr(dsx), nx, ny, nx + 2, ny + 2, _lib.DIR_X,
+                                              ptr(info), stream()))
+    assert host(info)[0] == 4
+
+
+@pytest.mark.parametrize("n", [3, 4, 5, 7])
+def test_coarse_cholesky_bitwise(lib, oracle, n):
+    so = make_op(n, n, 5)
+    abd, info = oracle.setup_cg(so)
+    assert info == 0
+    b = grid(n, n, 10)
+    x = oracle.solve_cg(abd, b)
+    dabd = dev(np.zeros_like(abd))
+    dinfo = dev(np.zeros(1, dtype=np.int32))
+    _lib.check(lib.cdr_gpu_setup_cg_2d_f64(ptr(dev(so)), 5, n, n, n + 2, ptr(dabd), ptr(dinfo), stream()))
+    np.testing.assert_array_equal(host(dabd), abd)
+    assert host(dinfo)[0] == 0
+    dx = dev(np.zeros_like(b))
+    _lib.check(lib.cdr_gpu_solve_cg_2d_f64(ptr(dabd), ptr(dx), ptr(dev(b)), n, n, n + 2, stream()))
+    np.testing.assert_array_equal(host(dx), x)

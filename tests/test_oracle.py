@@ -1,0 +1,171 @@
+"""CPU tests of the parity oracle (oracle/cdr2_oracle.c) against the reference's
+published golden output, LAPACK, and algebraic identities.  No GPU."""
+import json
+import os
+
+import numpy as np
+import pytest
+import scipy.linalg.lapack as lapack
+
+from cedar_b200 import gallery as G
+from cedar_b200 import problems as P
+
+GOLD = os.path.join(os.path.dirname(__file__), "golden")
+
+
+def test_readme_history_pinned(oracle):
+    """Residual history of README.md:49-63 to the 6 printed digits, all 10 iterations."""
+    g = json.load(open(os.path.join(GOLD, "readme_poisson400.json")))
+    so = G.poisson(400, 400)
+    b = G.poisson_rhs_sin2pi(400, 400)
+    s = oracle.Solver(so, relax="point", nrelax_pre=1, nrelax_post=1, maxiter=10, tol=1e-10,
+                      num_levels=g["num_levels"])
+    x, h = s.solve(b)
+    assert len(h) == 10
+    for got, ref in zip(h, g["history"]):
+        assert float("%.6g" % got) == ref
+    err = oracle.inf_norm(np.ascontiguousarray(G.poisson_exact_sin2pi(400, 400) - x))
+    assert float("%.6g" % abs(err)) == g["solution_norm_abs"]
+
+
+def test_serial_level_rule(oracle):
+    """compute_num_levels of include/cedar/2d/solver.h:63-79 (min_coarse 3)."""
+    assert oracle.num_levels(400, 400, 3) == 8
+    assert oracle.num_levels(511, 511, 3) == 8
+    assert oracle.num_levels(2047, 2047, 3) == 10
+    assert oracle.num_levels(1023, 1023, 3) == 9
+    assert oracle.num_levels(63, 63, 3) == 5
+    s = oracle.Solver(G.poisson(400, 400))
+    assert [s.level_dims(l)[0] for l in range(s.nlevels)] == [400, 200, 100, 50, 25, 13, 7, 4]
+
+
+def test_oracle_fixture_histories(oracle):
+    """Regression pin of the oracle on small cases (fixtures written by make_fixtures.py)."""
+    fx = json.load(open(os.path.join(GOLD, "oracle_histories.json")))
+    from tests.golden.make_fixtures import build_case
+    for case in fx["cases"]:
+        so, b, kw = build_case(case)
+        s = oracle.Solver(so, **kw)
+        x, h = s.solve(b)
+        np.testing.assert_allclose(h, case["history"], rtol=1e-13, atol=0)
+
+
+def test_dpttrf_dpttrs_match_lapack(oracle):
+    rng = np.random.default_rng(0)
+    for n in (2, 5, 37, 200):
+        d = 4 + rng.random(n)
+        e = -rng.random(max(n - 1, 0))
+        d1, e1, info = oracle.dpttrf(d, e)
+        d2, e2, info2 = lapack.dpttrf(d, e)[:3]
+        assert info == info2 == 0
+        np.testing.assert_array_equal(d1, d2)
+        np.testing.assert_array_equal(e1, e2)
+        bb = rng.random(n)
+        np.testing.assert_array_equal(oracle.dpttrs(d1, e1, bb), lapack.dpttrs(d2, e2, bb)[0])
+
+
+def test_dpttrf_reports_nonpositive_pivot(oracle):
+    d, e, info = oracle.dpttrf([1.0, 1.0, 1.0], [-2.0, 0.0])
+    assert info == 2
+
+
+def test_dpbtrf_dpbtrs_match_lapack(oracle):
+    rng = np.random.default_rng(1)
+    for N, kd in ((16, 5), (64, 21), (9, 4)):
+        A = np.zeros((N, N))
+        for i in range(N):
+            A[i, i] = 2 * kd + 1 + rng.random()
+            for k in range(1, kd + 1):
+                if i + k < N:
+                    A[i, i + k] = A[i + k, i] = -rng.random()
+        ab = np.zeros((kd + 1, N))
+        for j in range(N):
+            for i in range(max(0, j - kd), j + 1):
+                ab[kd + i - j, j] = A[i, j]
+        f1, info = oracle.dpbtrf_u(ab, kd)
+        f2, info2 = lapack.dpbtrf(ab, lower=0)
+        assert info == info2 == 0
+        np.testing.assert_allclose(f1, f2, rtol=1e-14, atol=1e-14)
+        b = rng.random(N)
+        np.testing.assert_allclose(oracle.dpbtrs_u(f1, kd, b), np.linalg.solve(A, b), rtol=1e-12)
+
+
+def test_coarse_solve_is_exact_inverse(oracle):
+    so = G.fe_hetero(*P.hetero_coefficients(5, n_incl=2))
+    abd, info = oracle.setup_cg(so)
+    assert info == 0
+    rng = np.random.default_rng(2)
+    b = np.zeros((7, 7))
+    b[1:-1, 1:-1] = rng.random((5, 5))
+    x = oracle.solve_cg(abd, b)
+    A = G.stencil_to_csr(so).toarray()
+    np.testing.assert_allclose(x[1:-1, 1:-1].ravel(), np.linalg.solve(A, b[1:-1, 1:-1].ravel()), rtol=1e-12)
+
+
+@pytest.mark.parametrize("nx,ny,ns", [(9, 9, 3), (10, 8, 3), (9, 12, 5), (12, 11, 5), (8, 8, 5), (15, 14, 5)])
+def test_galerkin_equals_ptap(oracle, nx, ny, ns):
+    """ITLI coarse operator == P^T A P assembled from the interpolation as interp_add applies it."""
+    rng = np.random.default_rng(nx * 100 + ny)
+    if ns == 3:
+        so = G.diag_diffusion(nx, ny, 1.0, 0.3)
+        so[1:] *= 1 + 0.3 * rng.random(so[1:].shape)
+        so[:, 0, :] = 0; so[:, :, 0] = 0
+        so[1, :, 1] = 0; so[2, 1, :] = 0
+    else:
+        kx = np.exp(rng.normal(size=(ny + 1, nx + 1)))
+        so = G.fe_hetero(kx, kx * np.exp(rng.normal(size=(ny + 1, nx + 1))))
+    nxc, nyc = (nx - 1) // 2 + 1, (ny - 1) // 2 + 1
+    ci = oracle.setup_interp(so, nxc, nyc)
+    soc = oracle.galerkin(so, ci)
+    # explicit P from interp_add applied to unit coarse vectors
+    A = G.stencil_to_csr(so).toarray()
+    Pm = np.zeros((nx * ny, nxc * nyc))
+    for jc in range(nyc):
+        for ic in range(nxc):
+            xc = np.zeros((nyc + 2, nxc + 2))
+            xc[jc + 1, ic + 1] = 1.0
+            xf = np.zeros((ny + 2, nx + 2))
+            oracle.interp_add(ci, xc, np.zeros_like(xf), np.ascontiguousarray(so), xf)
+            Pm[:, jc * nxc + ic] = xf[1:-1, 1:-1].ravel()
+    Ac = Pm.T @ A @ Pm
+    Acs = G.stencil_to_csr(soc).toarray()
+    assert np.abs(Ac - Acs).max() <= 1e-13 * np.abs(Ac).max()
+
+
+def test_restrict_is_transpose_of_interp(oracle):
+    nx = ny = 13
+    so = G.fe_hetero(*P.hetero_coefficients(nx, n_incl=3))
+    ci = oracle.setup_interp(so, 7, 7)
+    rng = np.random.default_rng(5)
+    r = np.zeros((ny + 2, nx + 2)); r[1:-1, 1:-1] = rng.random((ny, nx))
+    xc = np.zeros((9, 9)); xc[1:-1, 1:-1] = rng.random((7, 7))
+    bc = oracle.restrict(ci, r)
+    xf = np.zeros_like(r)
+    oracle.interp_add(ci, xc, np.zeros_like(r), np.ascontiguousarray(so), xf)
+    assert abs((bc * xc).sum() - (r * xf).sum()) < 1e-12 * abs((r * xf).sum())
+
+
+def test_gallery_fe_matches_hetero_constant():
+    n = 11
+    so = G.fe_hetero(np.ones((n + 1, n + 1)), np.ones((n + 1, n + 1))) * 3
+    np.testing.assert_allclose(so, G.fe(n, n), atol=1e-15)
+
+
+def test_hetero_operator_symmetric_positive():
+    n = 15
+    so = G.fe_hetero(*P.hetero_coefficients(n))
+    A = G.stencil_to_csr(so).toarray()
+    assert np.abs(A - A.T).max() == 0
+    assert np.linalg.eigvalsh(A).min() > 0
+
+
+def test_line_smoothers_converge_like_reference_tests(oracle):
+    """test/2d/test_poisson.cc:96-159 thresholds: line-x on 800x200-shaped and line-y on
+    200x800-shaped anisotropic problems reach ||r|| < 1e-8 (scaled down here)."""
+    for relax, (nx, ny), (dx, dy) in (("line-x", (160, 40), (1.0, 1e-3)), ("line-y", (40, 160), (1e-3, 1.0))):
+        so = G.diag_diffusion(nx, ny, dx, dy)
+        b = np.zeros((ny + 2, nx + 2)); b[1:-1, 1:-1] = 1.0 / ((nx + 1) * (ny + 1))
+        s = oracle.Solver(so, relax=relax, maxiter=30, tol=1e-10)
+        x, h = s.solve(b)
+        r = oracle.residual(np.ascontiguousarray(so), x, b)
+        assert np.linalg.norm(r) < 1e-8
