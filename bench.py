@@ -265,11 +265,11 @@ def main():
         ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
         for _ in range(3):
             lib.cdr_gpu_relax_lines_2d_f32(ctypes.c_void_p(p_so), ns, ctypes.c_void_p(p_x), ctypes.c_void_p(p_b),
-                                           ctypes.c_void_p(p_sx), nx, ny, pp, tp, 0, 0, ctypes.c_void_p(sh))
+                                           ctypes.c_void_p(p_sx), nx, ny, pp, tp, 0, 0, 0, ctypes.c_void_p(sh))
         ev[0].record(stream)
         for _ in range(reps):
             lib.cdr_gpu_relax_lines_2d_f32(ctypes.c_void_p(p_so), ns, ctypes.c_void_p(p_x), ctypes.c_void_p(p_b),
-                                           ctypes.c_void_p(p_sx), nx, ny, pp, tp, 0, 0, ctypes.c_void_p(sh))
+                                           ctypes.c_void_p(p_sx), nx, ny, pp, tp, 0, 0, 0, ctypes.c_void_p(sh))
         ev[1].record(stream)
     torch.cuda.synchronize()
     sweep_ms = ev[0].elapsed_time(ev[1]) / reps

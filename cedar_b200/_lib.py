@@ -16,6 +16,7 @@ DOWN, UP = 0, 1
 RELAX = {"point": 0, "line-x": 1, "line-y": 2, "line-xy": 3}
 PREC = {"fp64": 0, "fp32-ir": 1}
 DIR_X, DIR_Y = 0, 1
+LINES_EXACT = 1
 
 _lib = None
 
@@ -32,7 +33,7 @@ class Settings(ctypes.Structure):
                 ("nrelax_post", ctypes.c_int), ("num_levels", ctypes.c_int),
                 ("maxiter", ctypes.c_int), ("tol", ctypes.c_double),
                 ("min_coarse", ctypes.c_int), ("precision", ctypes.c_int),
-                ("use_graph", ctypes.c_int)]
+                ("use_graph", ctypes.c_int), ("line_flags", ctypes.c_int)]
 
 
 def header_symbols():
@@ -75,7 +76,7 @@ def load(path=LIB_PATH):
             "cdr_gpu_setup_recip_2d_" + suf: (I, [P, P, I, I, I, S]),
             "cdr_gpu_relax_point_2d_" + suf: (I, [P, I, P, P, P, I, I, I, I, S]),
             "cdr_gpu_setup_lines_2d_" + suf: (I, [P, I, P, I, I, I, I, I, P, S]),
-            "cdr_gpu_relax_lines_2d_" + suf: (I, [P, I, P, P, P, I, I, I, I, I, I, S]),
+            "cdr_gpu_relax_lines_2d_" + suf: (I, [P, I, P, P, P, I, I, I, I, I, I, I, S]),
             "cdr_gpu_restrict_2d_" + suf: (I, [P, P, P, I, I, I, I, I, I, S]),
             "cdr_gpu_interp_add_2d_" + suf: (I, [P, P, P, P, P, I, I, I, I, I, I, S]),
             "cdr_gpu_solve_cg_2d_" + suf: (I, [P, P, P, I, I, I, S]),

@@ -4,8 +4,9 @@
 Keys and defaults are those of ``ml_settings::init`` (src/multilevel_settings.cc:15-61);
 note that the reference reads ``solver.min_coarse`` (underscore), so the
 ``"min-coarse"`` key found in its example configs has no effect there or here.
-GPU options live under the ``"gpu"`` object: ``precision`` ("fp64" | "fp32-ir")
-and ``graph`` (bool).
+GPU options live under the ``"gpu"`` object: ``precision`` ("fp64" | "fp32-ir"),
+``graph`` (bool) and ``line-solve`` ("scan": parallel line substitutions, the
+default; "sequential": DPTTRS order, bit-identical to the reference).
 """
 import json
 import os
@@ -68,6 +69,9 @@ class MLSettings:
         if self.precision not in ("fp64", "fp32-ir"):
             raise ValueError("invalid gpu.precision: %s" % self.precision)
         self.use_graph = bool(conf.get("gpu.graph", True))
+        self.line_solve = conf.get("gpu.line-solve", "scan")
+        if self.line_solve not in ("scan", "sequential"):
+            raise ValueError("invalid gpu.line-solve: %s" % self.line_solve)
 
     def __repr__(self):
         return ("MLSettings(relaxation=%r, cycle=%r, nrelax=(%d,%d), num_levels=%d, maxiter=%d, "

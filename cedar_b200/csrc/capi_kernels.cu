@@ -120,14 +120,14 @@ LSETUP_IMPL(float, f32)
 
 #define LRELAX_IMPL(T, SUF)                                                                                      \
 	int cdr_gpu_relax_lines_2d_##SUF(const T *so, int ns, T *x, const T *b, const T *sor, int nx, int ny,         \
-	                                 int pitch, int tpitch, int dir, int updown, cudaStream_t s)                 \
+	                                 int pitch, int tpitch, int dir, int updown, int flags, cudaStream_t s)      \
 	{                                                                                                            \
 		CDR_TRY(check_grid(nx, ny, pitch));                                                                      \
 		CDR_TRY(check_ns(ns));                                                                                   \
 		CDR_NONNULL(so); CDR_NONNULL(x); CDR_NONNULL(b); CDR_NONNULL(sor);                                       \
 		if (dir != CDR_DIR_X && dir != CDR_DIR_Y) { set_error(CDR_ERR_ARG, "bad dir %d", dir); return CDR_ERR_ARG; } \
 		if (dir == CDR_DIR_Y && tpitch < ny + 2) { set_error(CDR_ERR_DIM, "tpitch %d < ny+2", tpitch); return CDR_ERR_DIM; } \
-		return relax_lines_2d<T>(so, ns, x, b, sor, Dims2{nx, ny, pitch}, tpitch, dir, updown, s);              \
+		return relax_lines_2d<T>(so, ns, x, b, sor, Dims2{nx, ny, pitch}, tpitch, dir, updown, flags, s);       \
 	}
 LRELAX_IMPL(double, f64)
 LRELAX_IMPL(float, f32)

@@ -15,7 +15,8 @@
 //      update (so every element sees the DPTTS2 operation on its inputs);
 //   3. the solution is written back with the coalesced mapping of step 1.
 // Both colours of a sweep are two launches: lines of one colour read only lines
-// of the other colour.
+// of the other colour.  With CDR_LINES_EXACT the substitutions instead run in
+// DPTTS2's sequential order (one thread per line): slower, bit-identical.
 #include "cdr_common.cuh"
 
 namespace cdrgpu {
@@ -122,7 +123,7 @@ __device__ __forceinline__ void affine_scan(T &A, T &B, T *sA, T *sB, int t, int
 	__syncthreads();
 }
 
-template <typename T, int NS, int DIR>
+template <typename T, int NS, int DIR, bool EXACT>
 __global__ void __launch_bounds__(LT) k_lines(const T *__restrict__ so, T *__restrict__ q, const T *__restrict__ qf,
                                               const T *__restrict__ sor, Dims2 d, int tpitch, int first, int G)
 {
@@ -153,8 +154,6 @@ __global__ void __launch_bounds__(LT) k_lines(const T *__restrict__ so, T *__res
 	// 2. substitutions
 	const int tpl = LT / G;
 	const int g = threadIdx.x / tpl, t = threadIdx.x - g * tpl;
-	const int K = (n + tpl - 1) / tpl;
-	const int lo = t * K < n ? t * K : n, hi = lo + K < n ? lo + K : n;
 	const bool active = g < gmax;
 	const int lc = active ? line_coord(g) : 1;
 	const T *D, *E;
@@ -166,41 +165,53 @@ __global__ void __launch_bounds__(LT) k_lines(const T *__restrict__ so, T *__res
 		E = sor + (size_t)tpitch * (d.nx + 2) + (size_t)lc * tpitch;
 	}
 	T *r = buf + g * n;  // r[m] is line position m+1
-	// forward: y(m) = r(m) - y(m-1) * E(m+1)
-	T A = T(1), B = T(0);
-	if (active)
-		for (int m = lo; m < hi; ++m) {
-			T a = m == 0 ? T(0) : -E[m + 1];
-			B = a * B + r[m];
-			A = a * A;
+	if (EXACT) {
+		// DPTTS2 in its own order, one thread per line: bit-identical to LAPACK.
+		if (active && t == 0) {
+			for (int m = 1; m < n; ++m) r[m] = r[m] - r[m - 1] * E[m + 1];
+			r[n - 1] = r[n - 1] / D[n];
+			for (int m = n - 2; m >= 0; --m) r[m] = r[m] / D[m + 1] - r[m + 1] * E[m + 2];
 		}
-	affine_scan<T>(A, B, sA, sB, t, tpl, true);
-	if (active) {
-		T y = t == 0 ? T(0) : sB[threadIdx.x - 1];
-		for (int m = lo; m < hi; ++m) {
-			y = m == 0 ? r[0] : r[m] - y * E[m + 1];
-			r[m] = y;
+		__syncthreads();
+	} else {
+		const int K = (n + tpl - 1) / tpl;
+		const int lo = t * K < n ? t * K : n, hi = lo + K < n ? lo + K : n;
+		// forward: y(m) = r(m) - y(m-1) * E(m+1)
+		T A = T(1), B = T(0);
+		if (active)
+			for (int m = lo; m < hi; ++m) {
+				T a = m == 0 ? T(0) : -E[m + 1];
+				B = a * B + r[m];
+				A = a * A;
+			}
+		affine_scan<T>(A, B, sA, sB, t, tpl, true);
+		if (active) {
+			T y = t == 0 ? T(0) : sB[threadIdx.x - 1];
+			for (int m = lo; m < hi; ++m) {
+				y = m == 0 ? r[0] : r[m] - y * E[m + 1];
+				r[m] = y;
+			}
 		}
+		__syncthreads();
+		// backward: x(m) = y(m)/D(m+1) - x(m+1) * E(m+2)
+		A = T(1);
+		B = T(0);
+		if (active)
+			for (int m = hi - 1; m >= lo; --m) {
+				T a = m == n - 1 ? T(0) : -E[m + 2];
+				B = a * B + r[m] / D[m + 1];
+				A = a * A;
+			}
+		affine_scan<T>(A, B, sA, sB, t, tpl, false);
+		if (active) {
+			T x = t == tpl - 1 ? T(0) : sB[threadIdx.x + 1];
+			for (int m = hi - 1; m >= lo; --m) {
+				x = m == n - 1 ? r[m] / D[m + 1] : r[m] / D[m + 1] - x * E[m + 2];
+				r[m] = x;
+			}
+		}
+		__syncthreads();
 	}
-	__syncthreads();
-	// backward: x(m) = y(m)/D(m+1) - x(m+1) * E(m+2)
-	A = T(1);
-	B = T(0);
-	if (active)
-		for (int m = hi - 1; m >= lo; --m) {
-			T a = m == n - 1 ? T(0) : -E[m + 2];
-			B = a * B + r[m] / D[m + 1];
-			A = a * A;
-		}
-	affine_scan<T>(A, B, sA, sB, t, tpl, false);
-	if (active) {
-		T x = t == tpl - 1 ? T(0) : sB[threadIdx.x + 1];
-		for (int m = hi - 1; m >= lo; --m) {
-			x = m == n - 1 ? r[m] / D[m + 1] : r[m] / D[m + 1] - x * E[m + 2];
-			r[m] = x;
-		}
-	}
-	__syncthreads();
 
 	// 3. write back
 	for (int idx = threadIdx.x; idx < gmax * n; idx += LT) {
@@ -220,14 +231,17 @@ int lines_prepare()
 	static bool done = false;
 	if (done) return CDR_OK;
 	const int big = 227 * 1024;
-	CDR_CUDA_TRY(cudaFuncSetAttribute(k_lines<double, 5, CDR_DIR_X>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
-	CDR_CUDA_TRY(cudaFuncSetAttribute(k_lines<double, 5, CDR_DIR_Y>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
-	CDR_CUDA_TRY(cudaFuncSetAttribute(k_lines<double, 3, CDR_DIR_X>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
-	CDR_CUDA_TRY(cudaFuncSetAttribute(k_lines<double, 3, CDR_DIR_Y>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
-	CDR_CUDA_TRY(cudaFuncSetAttribute(k_lines<float, 5, CDR_DIR_X>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
-	CDR_CUDA_TRY(cudaFuncSetAttribute(k_lines<float, 5, CDR_DIR_Y>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
-	CDR_CUDA_TRY(cudaFuncSetAttribute(k_lines<float, 3, CDR_DIR_X>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
-	CDR_CUDA_TRY(cudaFuncSetAttribute(k_lines<float, 3, CDR_DIR_Y>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+#define CDR_LINES_ATTR(T, NS, DIR, EX) \
+	CDR_CUDA_TRY(cudaFuncSetAttribute(k_lines<T, NS, DIR, EX>, cudaFuncAttributeMaxDynamicSharedMemorySize, big))
+	CDR_LINES_ATTR(double, 5, CDR_DIR_X, false); CDR_LINES_ATTR(double, 5, CDR_DIR_Y, false);
+	CDR_LINES_ATTR(double, 3, CDR_DIR_X, false); CDR_LINES_ATTR(double, 3, CDR_DIR_Y, false);
+	CDR_LINES_ATTR(float, 5, CDR_DIR_X, false); CDR_LINES_ATTR(float, 5, CDR_DIR_Y, false);
+	CDR_LINES_ATTR(float, 3, CDR_DIR_X, false); CDR_LINES_ATTR(float, 3, CDR_DIR_Y, false);
+	CDR_LINES_ATTR(double, 5, CDR_DIR_X, true); CDR_LINES_ATTR(double, 5, CDR_DIR_Y, true);
+	CDR_LINES_ATTR(double, 3, CDR_DIR_X, true); CDR_LINES_ATTR(double, 3, CDR_DIR_Y, true);
+	CDR_LINES_ATTR(float, 5, CDR_DIR_X, true); CDR_LINES_ATTR(float, 5, CDR_DIR_Y, true);
+	CDR_LINES_ATTR(float, 3, CDR_DIR_X, true); CDR_LINES_ATTR(float, 3, CDR_DIR_Y, true);
+#undef CDR_LINES_ATTR
 	done = true;
 	return CDR_OK;
 }
@@ -245,7 +259,8 @@ static int lines_per_cta(int n, int dir)
 }
 
 template <typename T, int NS, int DIR>
-static int launch_lines(const T *so, T *x, const T *b, const T *sor, Dims2 d, int tpitch, int first, cudaStream_t st)
+static int launch_lines(const T *so, T *x, const T *b, const T *sor, Dims2 d, int tpitch, int first, bool exact,
+                        cudaStream_t st)
 {
 	const int n = DIR == CDR_DIR_X ? d.nx : d.ny;
 	const int nl = DIR == CDR_DIR_X ? d.ny : d.nx;
@@ -258,33 +273,35 @@ static int launch_lines(const T *so, T *x, const T *b, const T *sor, Dims2 d, in
 		return CDR_ERR_DIM;
 	}
 	CDR_TRY(lines_prepare());
-	k_lines<T, NS, DIR><<<ceil_div(nlines, G), LT, smem, st>>>(so, x, b, sor, d, tpitch, first, G);
+	if (exact) k_lines<T, NS, DIR, true><<<ceil_div(nlines, G), LT, smem, st>>>(so, x, b, sor, d, tpitch, first, G);
+	else k_lines<T, NS, DIR, false><<<ceil_div(nlines, G), LT, smem, st>>>(so, x, b, sor, d, tpitch, first, G);
 	CDR_LAUNCH_CHECK();
 	return CDR_OK;
 }
 
 template <typename T>
 int relax_lines_2d(const T *so, int nstencil, T *x, const T *b, const T *sor, Dims2 d, int tpitch, int dir,
-                   int updown, cudaStream_t st)
+                   int updown, int flags, cudaStream_t st)
 {
+	const bool exact = (flags & CDR_LINES_EXACT) != 0;
 	// DOWN: lines with Fortran start index 3 (0-based even) first, then 2 (odd);
 	// UP: the opposite (relax_lines_x.f90:82-97).
 	const int firsts[2] = {updown == CDR_DOWN ? 2 : 1, updown == CDR_DOWN ? 1 : 2};
 	for (int c = 0; c < 2; ++c) {
 		int f = firsts[c];
 		if (dir == CDR_DIR_X) {
-			if (nstencil == 5) CDR_TRY((launch_lines<T, 5, CDR_DIR_X>(so, x, b, sor, d, tpitch, f, st)));
-			else CDR_TRY((launch_lines<T, 3, CDR_DIR_X>(so, x, b, sor, d, tpitch, f, st)));
+			if (nstencil == 5) CDR_TRY((launch_lines<T, 5, CDR_DIR_X>(so, x, b, sor, d, tpitch, f, exact, st)));
+			else CDR_TRY((launch_lines<T, 3, CDR_DIR_X>(so, x, b, sor, d, tpitch, f, exact, st)));
 		} else {
-			if (nstencil == 5) CDR_TRY((launch_lines<T, 5, CDR_DIR_Y>(so, x, b, sor, d, tpitch, f, st)));
-			else CDR_TRY((launch_lines<T, 3, CDR_DIR_Y>(so, x, b, sor, d, tpitch, f, st)));
+			if (nstencil == 5) CDR_TRY((launch_lines<T, 5, CDR_DIR_Y>(so, x, b, sor, d, tpitch, f, exact, st)));
+			else CDR_TRY((launch_lines<T, 3, CDR_DIR_Y>(so, x, b, sor, d, tpitch, f, exact, st)));
 		}
 	}
 	return CDR_OK;
 }
 template int relax_lines_2d<double>(const double *, int, double *, const double *, const double *, Dims2, int, int,
-                                    int, cudaStream_t);
+                                    int, int, cudaStream_t);
 template int relax_lines_2d<float>(const float *, int, float *, const float *, const float *, Dims2, int, int, int,
-                                   cudaStream_t);
+                                   int, cudaStream_t);
 
 }  // namespace cdrgpu

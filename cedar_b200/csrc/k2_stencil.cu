@@ -242,24 +242,28 @@ __global__ void __launch_bounds__(TX *TY) k_interp_add(const T *__restrict__ ci,
 	if (ic > f.nx / 2 + 1 || jc > f.ny / 2 + 1) return;
 	const size_t cps = c.plane();
 	const int cp = c.pitch, fp = f.pitch;
-	size_t kc = c.at(ic, jc), kf = f.at(2 * ic - 1, 2 * jc - 1);
+	const int i = 2 * ic - 1, j = 2 * jc - 1;
+	size_t kc = c.at(ic, jc), kf = f.at(i, j);
+	// The reference divides r by c on interior points only; for even grid sizes
+	// the loop also reaches the ghost row/column, where r is added undivided.
+	auto rc = [&](size_t k, int ii, int jj) -> T { return (ii <= f.nx && jj <= f.ny) ? res[k] / soc[k] : res[k]; };
 	T qcc = qc[kc];
 	q[kf] = q[kf] + qcc;
 	if (ic >= 2) {
 		T a = ci[IR * cps + kc] * qcc + ci[IL * cps + kc] * qc[kc - 1];
 		size_t k = kf - 1;
-		q[k] = q[k] + a + res[k] / soc[k];
+		q[k] = q[k] + a + rc(k, i - 1, j);
 	}
 	if (jc >= 2) {
 		T aq = ci[IA * cps + kc] * qcc + ci[IB * cps + kc] * qc[kc - cp];
 		size_t k = kf - fp;
-		q[k] = q[k] + aq + res[k] / soc[k];
+		q[k] = q[k] + aq + rc(k, i, j - 1);
 	}
 	if (ic >= 2 && jc >= 2) {
 		T a = ci[ISW * cps + kc] * qc[kc - cp - 1] + ci[INW * cps + kc] * qc[kc - 1] + ci[INE * cps + kc] * qcc
 		      + ci[ISE * cps + kc] * qc[kc - cp];
 		size_t k = kf - fp - 1;
-		q[k] = q[k] + a + res[k] / soc[k];
+		q[k] = q[k] + a + rc(k, i - 1, j - 1);
 	}
 }
 
@@ -388,89 +392,111 @@ int setup_interp_2d(const double *so, int nstencil, double *ci, Dims2 f, Dims2 c
 }
 
 // ------------------------------------------------------------ Galerkin coarse op
-// Coarse operator P^T A P, computed per coarse point as a local product over
-// the 3x3 fine support of each coarse basis function.  Same result as the
-// reference's expanded formulas (BMG2_SymStd_SETUP_ITLI_ex.f90:94-331) up to
-// summation order.
-//
-// Weight of coarse point (ic, jc) at fine point F + (dx, dy), F = (2ic-1, 2jc-1):
-// the entries of CI that interp_add/restrict use for that fine point.
-__device__ __forceinline__ double pweight(const double *__restrict__ ci, size_t cps, int cp, size_t kc, int dx,
-                                          int dy)
-{
-	if (dx == 0 && dy == 0) return 1.0;
-	if (dx == -1 && dy == 0) return ci[IR * cps + kc];
-	if (dx == 1 && dy == 0) return ci[IL * cps + kc + 1];
-	if (dx == 0 && dy == -1) return ci[IA * cps + kc];
-	if (dx == 0 && dy == 1) return ci[IB * cps + kc + cp];
-	if (dx == -1 && dy == -1) return ci[INE * cps + kc];
-	if (dx == 1 && dy == -1) return ci[INW * cps + kc + 1];
-	if (dx == -1 && dy == 1) return ci[ISE * cps + kc + cp];
-	return ci[ISW * cps + kc + cp + 1];  // (1, 1)
-}
-
-// A[(i,j), (i+di, j+dj)] from the lower-half storage.
-template <int NS>
-__device__ __forceinline__ double aentry(const double *__restrict__ so, size_t ps, int fp, size_t k, int di, int dj)
-{
-	if (di == 0 && dj == 0) return so[k];
-	if (di == -1 && dj == 0) return -so[ps + k];
-	if (di == 1 && dj == 0) return -so[ps + k + 1];
-	if (di == 0 && dj == -1) return -so[2 * ps + k];
-	if (di == 0 && dj == 1) return -so[2 * ps + k + fp];
-	if (NS == 3) return 0.0;
-	if (di == -1 && dj == -1) return -so[3 * ps + k];
-	if (di == 1 && dj == 1) return -so[3 * ps + k + fp + 1];
-	if (di == 1 && dj == -1) return -so[4 * ps + k + 1];
-	return -so[4 * ps + k + fp];  // (-1, 1)
-}
-
-// sum over f1 in supp(c1), f2 in supp(c2) of P(f1,c1) A(f1,f2) P(f2,c2); c2 = c1 + (ox, oy)*(-1)
-template <int NS, int OX1, int OY1, int OX2, int OY2>
-__device__ __forceinline__ double rap_entry(const double *__restrict__ so, const double *__restrict__ ci, Dims2 f,
-                                            Dims2 c, int ic, int jc)
-{
-	const size_t ps = f.plane(), cps = c.plane();
-	const int fp = f.pitch, cp = c.pitch;
-	const int F1x = 2 * (ic + OX1) - 1, F1y = 2 * (jc + OY1) - 1;
-	const size_t kc1 = c.at(ic + OX1, jc + OY1), kc2 = c.at(ic + OX2, jc + OY2);
-	double tot = 0.0;
-#pragma unroll
-	for (int dy1 = -1; dy1 <= 1; ++dy1)
-#pragma unroll
-		for (int dx1 = -1; dx1 <= 1; ++dx1) {
-			const int fx = F1x + dx1, fy = F1y + dy1;
-			if (fx < 1 || fx > f.nx || fy < 1 || fy > f.ny) continue;
-			const size_t kf = f.at(fx, fy);
-			double inner = 0.0;
-#pragma unroll
-			for (int ddy = -1; ddy <= 1; ++ddy)
-#pragma unroll
-				for (int ddx = -1; ddx <= 1; ++ddx) {
-					// offset of f2 = f1 + (ddx, ddy) from F2 = F1 + 2*(OX2-OX1, OY2-OY1)
-					const int ex = dx1 + ddx - 2 * (OX2 - OX1), ey = dy1 + ddy - 2 * (OY2 - OY1);
-					if (ex < -1 || ex > 1 || ey < -1 || ey > 1) continue;
-					if (NS == 3 && ddx != 0 && ddy != 0) continue;
-					inner += aentry<NS>(so, ps, fp, kf, ddx, ddy) * pweight(ci, cps, cp, kc2, ex, ey);
-				}
-			tot += pweight(ci, cps, cp, kc1, dx1, dy1) * inner;
-		}
-	return tot;
-}
-
+// Coarse operator P^T A P for the operator-induced P, BMG2_SymStd_SETUP_ITLI_ex
+// (src/2d/ftn/BMG2_SymStd_SETUP_ITLI_ex.f90:94-214 nine-point fine operator,
+// :252-331 five-point), one thread per coarse point.  The partial products
+// (C*) and their order are the reference's, so the result is bit-identical.
+// (A generic local P^T A P over the 3x3 supports gives the same operator up to
+// summation order; the OI weights of the next level amplify such differences,
+// so the reference's order is kept.)
 template <int NS>
 __global__ void k_galerkin(const double *__restrict__ so, const double *__restrict__ ci, double *__restrict__ soc,
                            Dims2 f, Dims2 c)
 {
-	int ic = blockIdx.x * TX + threadIdx.x + 1, jc = blockIdx.y * TY + threadIdx.y + 1;
+	const int ic = blockIdx.x * TX + threadIdx.x + 1, jc = blockIdx.y * TY + threadIdx.y + 1;
 	if (ic > c.nx || jc > c.ny) return;
-	const size_t cps = c.plane();
-	const size_t kc = c.at(ic, jc);
-	soc[PC * cps + kc] = rap_entry<NS, 0, 0, 0, 0>(so, ci, f, c, ic, jc);
-	soc[PW * cps + kc] = -rap_entry<NS, 0, 0, -1, 0>(so, ci, f, c, ic, jc);
-	soc[PS * cps + kc] = -rap_entry<NS, 0, 0, 0, -1>(so, ci, f, c, ic, jc);
-	soc[PSW * cps + kc] = -rap_entry<NS, 0, 0, -1, -1>(so, ci, f, c, ic, jc);
-	soc[PNW * cps + kc] = -rap_entry<NS, -1, 0, 0, -1>(so, ci, f, c, ic, jc);
+	const size_t ps = f.plane(), cps = c.plane();
+	const int fp = f.pitch, cp = c.pitch;
+	const size_t k0 = f.at(2 * ic - 1, 2 * jc - 1), kc0 = c.at(ic, jc);
+	// fine stencil relative to (I, J) and weights relative to (IC, JC)
+	auto O = [&](int di, int dj) { return so[k0 + (long)dj * fp + di]; };
+	auto W = [&](int di, int dj) { return so[ps + k0 + (long)dj * fp + di]; };
+	auto S = [&](int di, int dj) { return so[2 * ps + k0 + (long)dj * fp + di]; };
+	auto SW = [&](int di, int dj) { return NS == 5 ? so[3 * ps + k0 + (long)dj * fp + di] : 0.0; };
+	auto NW = [&](int di, int dj) { return NS == 5 ? so[4 * ps + k0 + (long)dj * fp + di] : 0.0; };
+	auto P = [&](int di, int dj, int pl) { return ci[pl * cps + kc0 + (long)dj * cp + di]; };
+	double CO, CS, CSW, CW, CNW, CN, CNE, CE, CSE;
+	if (NS == 5) {
+		CO = NW(0, 1) * P(0, 1, ISW) + W(0, 0) * P(0, 0, IL) + SW(0, 0) * P(0, 0, INW);
+		CS = W(0, -1) * P(0, 0, INW) + NW(0, 0) * P(0, 0, IL);
+		CSW = -O(-1, -1) * P(0, 0, INW) + W(-1, -1) * P(-1, 0, IA) + NW(-1, 0) + S(-1, 0) * P(0, 0, IL);
+		CW = -O(-1, 0) * P(0, 0, IL) + S(-1, 0) * P(0, 0, INW) + SW(-1, 0) * P(-1, 0, IA) + W(-1, 0)
+		     + NW(-1, 1) * P(-1, 1, IB) + S(-1, 1) * P(0, 1, ISW);
+		CNW = -O(-1, 1) * P(0, 1, ISW) + S(-1, 1) * P(0, 0, IL) + SW(-1, 1) + W(-1, 1) * P(-1, 1, IB);
+		CN = SW(0, 1) * P(0, 0, IL) + W(0, 1) * P(0, 1, ISW);
+		soc[PW * cps + kc0] = CO + P(0, 0, IA) * CS + P(0, 0, INE) * CSW + P(0, 0, IR) * CW + P(0, 1, ISE) * CNW
+		                      + P(0, 1, IB) * CN;
+		double COSW = SW(0, 0) * P(0, 0, ISW);
+		double CSSW = SW(0, -1) * P(0, -1, IL) + W(0, -1) * P(0, 0, ISW);
+		double CSWSW = -O(-1, -1) * P(0, 0, ISW) + S(-1, -1) * P(0, -1, IL) + SW(-1, -1) + W(-1, -1) * P(-1, 0, IB);
+		double CWSW = S(-1, 0) * P(0, 0, ISW) + SW(-1, 0) * P(-1, 0, IB);
+		soc[PSW * cps + kc0] = COSW + P(0, 0, IA) * CSSW + P(0, 0, INE) * CSWSW + P(0, 0, IR) * CWSW;
+		double COA = SW(0, 0) * P(0, 0, ISE) + S(0, 0) * P(0, 0, IB) + NW(1, 0) * P(1, 0, ISW);
+		double CEA = S(1, 0) * P(1, 0, ISW) + SW(1, 0) * P(0, 0, IB);
+		double CSEA = -O(1, -1) * P(1, 0, ISW) + S(1, -1) * P(1, -1, IL) + SW(1, -1) + W(1, -1) * P(0, 0, IB);
+		double CSA = -O(0, -1) * P(0, 0, IB) + W(1, -1) * P(1, 0, ISW) + NW(1, -1) * P(1, -1, IL) + S(0, -1)
+		             + SW(0, -1) * P(0, -1, IR) + W(0, -1) * P(0, 0, ISE);
+		double CSWA = -O(-1, -1) * P(0, 0, ISE) + W(0, -1) * P(0, 0, IB) + NW(0, -1) + S(-1, -1) * P(0, -1, IR);
+		double CWA = NW(0, 0) * P(0, 0, IB) + S(-1, 0) * P(0, 0, ISE);
+		soc[PS * cps + kc0] = COA + P(1, 0, IL) * CEA + P(1, 0, INW) * CSEA + P(0, 0, IA) * CSA + P(0, 0, INE) * CSWA
+		                      + P(0, 0, IR) * CWA;
+		double CONW = NW(-1, 0) * P(0, 0, ISE);
+		double CENW = NW(0, 0) * P(0, 0, IB) + S(-1, 0) * P(0, 0, ISE);
+		double CSENW = -O(-1, -1) * P(0, 0, ISE) + W(0, -1) * P(0, 0, IB) + NW(0, -1) + S(-1, -1) * P(0, -1, IR);
+		double CFNW = W(-1, -1) * P(0, 0, ISE) + NW(-1, -1) * P(0, -1, IR);
+		soc[PNW * cps + kc0] = CONW + P(0, 0, IL) * CENW + P(0, 0, INW) * CSENW + P(-1, 0, IA) * CFNW;
+		CO = W(0, 0) * P(0, 0, IR) + NW(0, 1) * P(0, 1, ISE) + S(0, 1) * P(0, 1, IB) + SW(1, 1) * P(1, 1, ISW)
+		     + W(1, 0) * P(1, 0, IL) + NW(1, 0) * P(1, 0, INW) + S(0, 0) * P(0, 0, IA) + SW(0, 0) * P(0, 0, INE)
+		     - O(0, 0);
+		CW = -O(-1, 0) * P(0, 0, IR) + S(-1, 1) * P(0, 1, ISE) + SW(0, 1) * P(0, 1, IB) + W(0, 0)
+		     + NW(0, 0) * P(0, 0, IA) + S(-1, 0) * P(0, 0, INE);
+		CNW = -O(-1, 1) * P(0, 1, ISE) + W(0, 1) * P(0, 1, IB) + NW(0, 1) + S(-1, 1) * P(0, 0, IR);
+		CN = -O(0, 1) * P(0, 1, IB) + NW(1, 1) * P(1, 0, IL) + S(0, 1) + SW(0, 1) * P(0, 0, IR)
+		     + W(0, 1) * P(0, 1, ISE) + W(1, 1) * P(1, 1, ISW);
+		CNE = -O(1, 1) * P(1, 1, ISW) + S(1, 1) * P(1, 0, IL) + SW(1, 1) + W(1, 1) * P(0, 1, IB);
+		CE = -O(1, 0) * P(1, 0, IL) + S(1, 0) * P(1, 0, INW) + SW(1, 0) * P(0, 0, IA) + W(1, 0)
+		     + NW(1, 1) * P(0, 1, IB) + S(1, 1) * P(1, 1, ISW);
+		CSE = -O(1, -1) * P(1, 0, INW) + W(1, -1) * P(0, 0, IA) + NW(1, 0) + S(1, 0) * P(1, 0, IL);
+		CS = -O(0, -1) * P(0, 0, IA) + W(0, -1) * P(0, 0, INE) + NW(0, 0) * P(0, 0, IR) + S(0, 0)
+		     + SW(1, 0) * P(1, 0, IL) + W(1, -1) * P(1, 0, INW);
+		CSW = -O(-1, -1) * P(0, 0, INE) + S(-1, 0) * P(0, 0, IR) + SW(0, 0) + W(0, -1) * P(0, 0, IA);
+	} else {
+		CO = W(0, 0) * P(0, 0, IL);
+		CS = W(0, -1) * P(0, 0, INW);
+		CSW = -O(-1, -1) * P(0, 0, INW) + W(-1, -1) * P(-1, 0, IA) + S(-1, 0) * P(0, 0, IL);
+		CW = -O(-1, 0) * P(0, 0, IL) + S(-1, 0) * P(0, 0, INW) + W(-1, 0) + S(-1, 1) * P(0, 1, ISW);
+		CNW = -O(-1, 1) * P(0, 1, ISW) + S(-1, 1) * P(0, 0, IL) + W(-1, 1) * P(-1, 1, IB);
+		CN = W(0, 1) * P(0, 1, ISW);
+		soc[PW * cps + kc0] = CO + P(0, 0, IA) * CS + P(0, 0, INE) * CSW + P(0, 0, IR) * CW + P(0, 1, ISE) * CNW
+		                      + P(0, 1, IB) * CN;
+		double CSSW = W(0, -1) * P(0, 0, ISW);
+		double CSWSW = -O(-1, -1) * P(0, 0, ISW) + S(-1, -1) * P(0, -1, IL) + W(-1, -1) * P(-1, 0, IB);
+		double CWSW = S(-1, 0) * P(0, 0, ISW);
+		soc[PSW * cps + kc0] = P(0, 0, IA) * CSSW + P(0, 0, INE) * CSWSW + P(0, 0, IR) * CWSW;
+		double COA = S(0, 0) * P(0, 0, IB);
+		double CEA = S(1, 0) * P(1, 0, ISW);
+		double CSEA = -O(1, -1) * P(1, 0, ISW) + S(1, -1) * P(1, -1, IL) + W(1, -1) * P(0, 0, IB);
+		double CSA = -O(0, -1) * P(0, 0, IB) + W(1, -1) * P(1, 0, ISW) + S(0, -1) + W(0, -1) * P(0, 0, ISE);
+		double CSWA = -O(-1, -1) * P(0, 0, ISE) + W(0, -1) * P(0, 0, IB) + S(-1, -1) * P(0, -1, IR);
+		double CWA = S(-1, 0) * P(0, 0, ISE);
+		soc[PS * cps + kc0] = COA + P(1, 0, IL) * CEA + P(1, 0, INW) * CSEA + P(0, 0, IA) * CSA + P(0, 0, INE) * CSWA
+		                      + P(0, 0, IR) * CWA;
+		double CENW = S(-1, 0) * P(0, 0, ISE);
+		double CSENW = -O(-1, -1) * P(0, 0, ISE) + W(0, -1) * P(0, 0, IB) + S(-1, -1) * P(0, -1, IR);
+		double CSNW = W(-1, -1) * P(0, 0, ISE);
+		soc[PNW * cps + kc0] = P(0, 0, IL) * CENW + P(0, 0, INW) * CSENW + P(-1, 0, IA) * CSNW;
+		CO = W(0, 0) * P(0, 0, IR) + S(0, 1) * P(0, 1, IB) + W(1, 0) * P(1, 0, IL) + S(0, 0) * P(0, 0, IA) - O(0, 0);
+		CW = -O(-1, 0) * P(0, 0, IR) + S(-1, 1) * P(0, 1, ISE) + W(0, 0) + S(-1, 0) * P(0, 0, INE);
+		CNW = -O(-1, 1) * P(0, 1, ISE) + W(0, 1) * P(0, 1, IB) + S(-1, 1) * P(0, 0, IR);
+		CN = -O(0, 1) * P(0, 1, IB) + S(0, 1) + W(0, 1) * P(0, 1, ISE) + W(1, 1) * P(1, 1, ISW);
+		CNE = -O(1, 1) * P(1, 1, ISW) + S(1, 1) * P(1, 0, IL) + W(1, 1) * P(0, 1, IB);
+		CE = -O(1, 0) * P(1, 0, IL) + S(1, 0) * P(1, 0, INW) + W(1, 0) + S(1, 1) * P(1, 1, ISW);
+		CSE = -O(1, -1) * P(1, 0, INW) + W(1, -1) * P(0, 0, IA) + S(1, 0) * P(1, 0, IL);
+		CS = -O(0, -1) * P(0, 0, IA) + W(0, -1) * P(0, 0, INE) + S(0, 0) + W(1, -1) * P(1, 0, INW);
+		CSW = -O(-1, -1) * P(0, 0, INE) + S(-1, 0) * P(0, 0, IR) + W(0, -1) * P(0, 0, IA);
+	}
+	soc[PC * cps + kc0] = -P(0, 1, ISE) * CNW - P(0, 1, IB) * CN - P(1, 1, ISW) * CNE - P(0, 0, IR) * CW - CO
+	                      - P(1, 0, IL) * CE - P(0, 0, INE) * CSW - P(0, 0, IA) * CS - P(1, 0, INW) * CSE;
 }
 
 int galerkin_2d(const double *so, int nstencil, const double *ci, double *soc, Dims2 f, Dims2 c, cudaStream_t st)

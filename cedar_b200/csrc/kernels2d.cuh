@@ -16,7 +16,7 @@ int setup_lines_2d(const double *so, int nstencil, TS *sor, Dims2 d, int tpitch,
 int lines_prepare();
 template <typename T>
 int relax_lines_2d(const T *so, int nstencil, T *x, const T *b, const T *sor, Dims2 d, int tpitch, int dir,
-                   int updown, cudaStream_t st);
+                   int updown, int flags, cudaStream_t st);
 template <typename T>
 int restrict_2d(const T *ci, const T *rf, T *bc, Dims2 f, Dims2 c, cudaStream_t st);
 template <typename T>

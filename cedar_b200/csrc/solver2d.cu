@@ -69,6 +69,9 @@ struct cdr_gpu_solver {
 	}
 
 	bool mixed() const { return s.precision == CDR_PREC_F32_IR; }
+	// the exact (sequential) line substitution applies to the FP64 cycle only
+	template <typename T>
+	int lflags() const { return sizeof(T) == 8 ? s.line_flags : 0; }
 	int L() const { return (int)lv.size(); }
 
 	// -------------------------------------------------------------- smoothing
@@ -115,18 +118,18 @@ int cdr_gpu_solver::smooth(int l, T *x, const T *b, int updown)
 		switch (s.relaxation) {
 		case CDR_RELAX_POINT: CDR_TRY(relax_point_2d<T>(so, L.ns, x, b, sor, L.d, updown, st)); break;
 		case CDR_RELAX_LINE_X:
-			CDR_TRY(relax_lines_2d<T>(so, L.ns, x, b, sor, L.d, L.tpitch, CDR_DIR_X, updown, st));
+			CDR_TRY(relax_lines_2d<T>(so, L.ns, x, b, sor, L.d, L.tpitch, CDR_DIR_X, updown, lflags<T>(), st));
 			break;
 		case CDR_RELAX_LINE_Y:
-			CDR_TRY(relax_lines_2d<T>(so, L.ns, x, b, sory, L.d, L.tpitch, CDR_DIR_Y, updown, st));
+			CDR_TRY(relax_lines_2d<T>(so, L.ns, x, b, sory, L.d, L.tpitch, CDR_DIR_Y, updown, lflags<T>(), st));
 			break;
 		case CDR_RELAX_LINE_XY:
 			if (updown == CDR_DOWN) {
-				CDR_TRY(relax_lines_2d<T>(so, L.ns, x, b, sor, L.d, L.tpitch, CDR_DIR_X, updown, st));
-				CDR_TRY(relax_lines_2d<T>(so, L.ns, x, b, sory, L.d, L.tpitch, CDR_DIR_Y, updown, st));
+				CDR_TRY(relax_lines_2d<T>(so, L.ns, x, b, sor, L.d, L.tpitch, CDR_DIR_X, updown, lflags<T>(), st));
+				CDR_TRY(relax_lines_2d<T>(so, L.ns, x, b, sory, L.d, L.tpitch, CDR_DIR_Y, updown, lflags<T>(), st));
 			} else {
-				CDR_TRY(relax_lines_2d<T>(so, L.ns, x, b, sory, L.d, L.tpitch, CDR_DIR_Y, updown, st));
-				CDR_TRY(relax_lines_2d<T>(so, L.ns, x, b, sor, L.d, L.tpitch, CDR_DIR_X, updown, st));
+				CDR_TRY(relax_lines_2d<T>(so, L.ns, x, b, sory, L.d, L.tpitch, CDR_DIR_Y, updown, lflags<T>(), st));
+				CDR_TRY(relax_lines_2d<T>(so, L.ns, x, b, sor, L.d, L.tpitch, CDR_DIR_X, updown, lflags<T>(), st));
 			}
 			break;
 		default: set_error(CDR_ERR_ARG, "unknown relaxation %d", s.relaxation); return CDR_ERR_ARG;
@@ -277,6 +280,7 @@ int cdr_gpu_settings_default(cdr_gpu_settings *s)
 	s->min_coarse = 3;
 	s->precision = CDR_PREC_F64;
 	s->use_graph = 1;
+	s->line_flags = 0;
 	return CDR_OK;
 }
 

@@ -109,11 +109,17 @@ int cdr_gpu_setup_lines_2d_f32(const double *so, int nstencil, float *sor, int n
 /* One zebra line Gauss-Seidel sweep (both colours); replaces line_relax::run
  * (include/cedar/kernels/line_relax.h:31-39) -> BMG2_SymStd_relax_lines_{x,y}
  * (src/2d/relax.cc:98-133, src/2d/ftn/BMG2_SymStd_relax_lines_x.f90:74-131,
- * BMG2_SymStd_relax_lines_y.f90:74-129). */
+ * BMG2_SymStd_relax_lines_y.f90:74-129).  flags = 0: the per-line DPTTRS
+ * substitutions run as a parallel affine scan (fast; each element gets the
+ * DPTTS2 update of its inputs, chunk-entry values may differ by rounding);
+ * flags = CDR_LINES_EXACT: sequential substitutions, bit-identical to DPTTRS. */
+#define CDR_LINES_EXACT 1
 int cdr_gpu_relax_lines_2d_f64(const double *so, int nstencil, double *x, const double *b, const double *sor,
-                               int nx, int ny, int pitch, int tpitch, int dir, int updown, cudaStream_t stream);
+                               int nx, int ny, int pitch, int tpitch, int dir, int updown, int flags,
+                               cudaStream_t stream);
 int cdr_gpu_relax_lines_2d_f32(const float *so, int nstencil, float *x, const float *b, const float *sor,
-                               int nx, int ny, int pitch, int tpitch, int dir, int updown, cudaStream_t stream);
+                               int nx, int ny, int pitch, int tpitch, int dir, int updown, int flags,
+                               cudaStream_t stream);
 
 /* b_coarse = P^T r_fine; replaces restriction::run (include/cedar/kernels/restrict.h:17-19)
  * -> BMG2_SymStd_restrict (src/2d/restrict.cc:14-29, src/2d/ftn/BMG2_SymStd_restrict.f90:72-92). */
@@ -176,6 +182,7 @@ typedef struct cdr_gpu_settings {
 	int min_coarse;   /* "solver.min_coarse"  (default 3)                              */
 	int precision;    /* CDR_PREC_F64 (default) or CDR_PREC_F32_IR                     */
 	int use_graph;    /* replay the cycle as a CUDA graph (default 1)                  */
+	int line_flags;   /* CDR_LINES_EXACT for sequential line substitutions (default 0) */
 } cdr_gpu_settings;
 
 typedef struct cdr_gpu_solver cdr_gpu_solver;

@@ -14,7 +14,7 @@ import subprocess
 import numpy as np
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-_LIB = None
+_LIBS = {}
 
 RELAX = {"point": 0, "line-x": 1, "line-y": 2, "line-xy": 3}
 ARR = {"so": 0, "x": 1, "b": 2, "res": 3, "sor0": 4, "sor1": 5, "ci": 6, "abd": 7}
@@ -34,10 +34,10 @@ def build():
     subprocess.run(["make", "-s", "-C", _HERE], check=True)
 
 
-def lib():
-    global _LIB
-    if _LIB is None:
-        path = os.path.join(_HERE, "liboracle.so")
+def lib(variant=""):
+    """variant "" is the reference-faithful build; "fma" contracts a*b+c into FMAs."""
+    if variant not in _LIBS:
+        path = os.path.join(_HERE, "liboracle%s.so" % ("_" + variant if variant else ""))
         if not os.path.exists(path):
             build()
         L = ctypes.CDLL(path)
@@ -79,8 +79,8 @@ def lib():
             f = getattr(L, name)
             f.restype = res
             f.argtypes = args
-        _LIB = L
-    return _LIB
+        _LIBS[variant] = L
+    return _LIBS[variant]
 
 
 def _p(a):
@@ -236,39 +236,40 @@ class Solver:
     """Serial BoxMG solver: setup in the constructor, as ``cdr2::solver``."""
 
     def __init__(self, so, relax="point", nrelax_pre=2, nrelax_post=1, num_levels=-1,
-                 maxiter=10, tol=1e-8, min_coarse=3):
+                 maxiter=10, tol=1e-8, min_coarse=3, variant=""):
+        self.L = lib(variant)
         so = np.ascontiguousarray(so, dtype=np.float64)
         self.nstncl = so.shape[0]
         self.ny, self.nx = so.shape[1] - 2, so.shape[2] - 2
         self.settings = Settings(RELAX[relax], nrelax_pre, nrelax_post, num_levels, maxiter, tol, min_coarse)
         self._so = so
-        self.h = lib().o2_create(ctypes.byref(self.settings), _p(so), self.nstncl, self.nx, self.ny)
+        self.h = self.L.o2_create(ctypes.byref(self.settings), _p(so), self.nstncl, self.nx, self.ny)
 
     def __del__(self):
         if getattr(self, "h", None):
-            lib().o2_destroy(self.h)
+            self.L.o2_destroy(self.h)
             self.h = None
 
     @property
     def nlevels(self):
-        return lib().o2_nlevels(self.h)
+        return self.L.o2_nlevels(self.h)
 
     def info(self):
-        return lib().o2_info(self.h, 0), lib().o2_info(self.h, 1)
+        return self.L.o2_info(self.h, 0), self.L.o2_info(self.h, 1)
 
     def level_dims(self, l):
         d = (ctypes.c_int * 3)()
-        lib().o2_level_dims(self.h, l, d)
+        self.L.o2_level_dims(self.h, l, d)
         return d[0], d[1], d[2]
 
     def level_array(self, l, which):
         """Copy of a level array in numpy layout."""
         nx, ny, ns = self.level_dims(l)
         II, JJ = nx + 2, ny + 2
-        ptr = lib().o2_level_array(self.h, l, ARR[which])
+        ptr = self.L.o2_level_array(self.h, l, ARR[which])
         if which == "abd":
             d = (ctypes.c_int * 2)()
-            lib().o2_abd_dims(self.h, d)
+            self.L.o2_abd_dims(self.h, d)
             n = d[0] * d[1]
             return np.ctypeslib.as_array(ptr, shape=(n,)).copy().reshape(d[1], d[0])
         shape = {"so": (ns, JJ, II), "ci": (8, JJ, II), "sor0": (2, JJ, II),
@@ -277,7 +278,7 @@ class Solver:
         return np.ctypeslib.as_array(ptr, shape=(n,)).copy().reshape(shape)
 
     def vcycle(self, x, b):
-        lib().o2_vcycle(self.h, _p(x), _p(b))
+        self.L.o2_vcycle(self.h, _p(x), _p(b))
         return x
 
     def solve(self, b, x=None):
@@ -286,5 +287,5 @@ class Solver:
         if x is None:
             x = np.zeros_like(b)
         hist = np.zeros(max(self.settings.maxiter, 1))
-        n = lib().o2_solve(self.h, _p(b), _p(x), _p(hist), len(hist))
+        n = self.L.o2_solve(self.h, _p(b), _p(x), _p(hist), len(hist))
         return x, hist[:n].copy()

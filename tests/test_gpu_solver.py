@@ -25,7 +25,8 @@ def gpu_solver(so, relax, **kw):
                                                       "nrelax-post": kw.get("nrelax_post", 1)},
                        "max-iter": kw.get("maxiter", 10), "tol": kw.get("tol", 1e-8),
                        "num-levels": kw.get("num_levels", -1)},
-            "gpu": {"precision": kw.get("precision", "fp64"), "graph": kw.get("graph", True)}}
+            "gpu": {"precision": kw.get("precision", "fp64"), "graph": kw.get("graph", True),
+                    "line-solve": kw.get("line_solve", "sequential")}}
     return Solver2D(so, Config(conf))
 
 
@@ -84,6 +85,21 @@ def test_larger_parity(oracle, n, relax):
     assert rel(x, xo) < 1e-10
 
 
+@pytest.mark.parametrize("n", [127, 200])
+def test_scan_line_solve_within_rounding_envelope(oracle, n):
+    """The parallel-scan line substitutions change only rounding: on the ill-conditioned
+    heterogeneous problem (coefficient contrast ~1e11) the history stays within the
+    spread between two FP64 builds of the oracle itself (with and without FMA)."""
+    so, b = P.hetero_diffusion(n)
+    kw = dict(nrelax_pre=2, nrelax_post=1, maxiter=6, tol=1e-10)
+    s = gpu_solver(so, "line-xy", line_solve="scan", **kw)
+    s.solve(b)
+    xo, ho = oracle.Solver(so, relax="line-xy", **kw).solve(b)
+    xf, hf = oracle.Solver(so, relax="line-xy", variant="fma", **kw).solve(b)
+    envelope = max(np.abs(hf - ho).max(), 1e-12 * max(1.0, ho.max()))
+    assert np.abs(s.history - ho).max() <= 10 * envelope, (s.history - ho, hf - ho)
+
+
 @pytest.mark.parametrize("n", [127, 256])
 def test_fp32_ir_reaches_tolerance(oracle, n):
     so, b = P.hetero_diffusion(n, sigma=1.0, n_incl=0, aniso=1.0)
@@ -121,17 +137,10 @@ def test_device_buffers_match_host(oracle):
 
 
 def test_setup_arrays_match_oracle(oracle):
-    """Interpolation weights (bitwise) and Galerkin operators (1e-13) of every level."""
+    """Interpolation weights and Galerkin operators of every level: same bits as the oracle."""
     so, b = P.hetero_diffusion(65)
     s = gpu_solver(so, "line-xy", maxiter=2)
     o = oracle.Solver(so, relax="line-xy", maxiter=2)
     for l in range(1, s.nlevels):
-        got_ci = s.level_array(l, "ci")
-        ref_ci = o.level_array(l, "ci")
-        if l == 1:  # from the fine operator itself: same bits
-            np.testing.assert_array_equal(got_ci, ref_ci)
-        else:  # from a Galerkin operator that differs from the oracle's by summation order
-            assert np.abs(got_ci - ref_ci).max() <= 1e-11 * np.abs(ref_ci).max()
-        got_so = s.level_array(l, "so")
-        ref_so = o.level_array(l, "so")
-        assert np.abs(got_so - ref_so).max() <= 1e-13 * np.abs(ref_so).max()
+        np.testing.assert_array_equal(s.level_array(l, "ci"), o.level_array(l, "ci"))
+        np.testing.assert_array_equal(s.level_array(l, "so"), o.level_array(l, "so"))
