@@ -17,6 +17,8 @@
 // Both colours of a sweep are two launches: lines of one colour read only lines
 // of the other colour.  With CDR_LINES_EXACT the substitutions instead run in
 // DPTTS2's sequential order (one thread per line): slower, bit-identical.
+#include <cstdint>
+
 #include "cdr_common.cuh"
 
 namespace cdrgpu {
@@ -224,6 +226,281 @@ __global__ void __launch_bounds__(LT) k_lines(const T *__restrict__ so, T *__res
 	}
 }
 
+
+// ------------------------------------------------------------ fast line sweep
+// Register-chunk form of the zebra sweep.  Thread t of a line owns positions
+// [t*K, t*K+K) of the line (0-based, ghost at 0; only 1..n are solved) and keeps
+// their right-hand sides in registers.  x-lines: the threads of a line are
+// consecutive lanes, so each thread reads its chunk with 16-byte vector loads
+// and a warp covers 32*K contiguous elements of a row.  y-lines: the lanes of a
+// warp are line-fastest (G lines side by side, stride-2 columns), so every row
+// segment a warp touches is shared by its G lines; the factors of y-lines are
+// stored transposed (line-contiguous) and still load as vectors.  The affine
+// maps of the chunks are scanned with warp shuffles and, across warps, through
+// shared memory (one slot per line and warp).
+template <typename T> struct Vec16;
+template <> struct Vec16<float> { using type = float4; };
+template <> struct Vec16<double> { using type = double2; };
+
+template <typename T, int K>
+__device__ __forceinline__ void vload(const T *__restrict__ p, T (&v)[K])
+{
+	using VT = typename Vec16<T>::type;
+	constexpr int W = 16 / sizeof(T);
+	const VT *pv = reinterpret_cast<const VT *>(p);
+#pragma unroll
+	for (int c = 0; c < K / W; ++c) {
+		VT t = pv[c];
+		const T *e = reinterpret_cast<const T *>(&t);
+#pragma unroll
+		for (int w = 0; w < W; ++w) v[c * W + w] = e[w];
+	}
+}
+
+template <typename T, int K>
+__device__ __forceinline__ void vstore(T *__restrict__ p, const T (&v)[K])
+{
+	using VT = typename Vec16<T>::type;
+	constexpr int W = 16 / sizeof(T);
+	VT *pv = reinterpret_cast<VT *>(p);
+#pragma unroll
+	for (int c = 0; c < K / W; ++c) {
+		VT t;
+		T *e = reinterpret_cast<T *>(&t);
+#pragma unroll
+		for (int w = 0; w < W; ++w) e[w] = v[c * W + w];
+		pv[c] = t;
+	}
+}
+
+// compose (A,B) <- (A,B) o (a2,b2): apply (a2,b2) first
+template <typename T>
+__device__ __forceinline__ void after(T &A, T &B, T a2, T b2)
+{
+	B = A * b2 + B;
+	A = A * a2;
+}
+
+// Exclusive scan of the chunk maps of a line.  forward: element u composes the
+// maps of the chunks before it (lower t); backward: after it (higher t).  S is
+// the lane distance between consecutive chunks of a line in a warp, CW the
+// number of chunks of one line in a warp, NWG the number of warps a line spans;
+// slot(g, k) indexes the shared-memory carry of line g, warp group k.
+// Returns the map's value at 0 (the incoming value of the chunk).
+template <typename T>
+__device__ __forceinline__ T scan_incoming(T A, T B, bool forward, int u, int S, int CW, int NWG, int k, int slot_self,
+                                           int slot_stride, T *sA, T *sB)
+{
+	const unsigned full = 0xffffffffu;
+	// inclusive within the warp segment
+	for (int off = 1; off < CW; off <<= 1) {
+		T a2 = forward ? __shfl_up_sync(full, A, off * S) : __shfl_down_sync(full, A, off * S);
+		T b2 = forward ? __shfl_up_sync(full, B, off * S) : __shfl_down_sync(full, B, off * S);
+		if (forward ? u >= off : u + off < CW) after(A, B, a2, b2);
+	}
+	// exclusive within the warp segment
+	T ae = forward ? __shfl_up_sync(full, A, S) : __shfl_down_sync(full, A, S);
+	T be = forward ? __shfl_up_sync(full, B, S) : __shfl_down_sync(full, B, S);
+	const bool first = forward ? u == 0 : u == CW - 1;
+	if (first) { ae = T(1); be = T(0); }
+	if (NWG == 1) return be;
+	// carry across warps: slot of group k holds the inclusive map of the whole group
+	const bool last = forward ? u == CW - 1 : u == 0;
+	__syncthreads();
+	if (last) { sA[slot_self] = A; sB[slot_self] = B; }
+	__syncthreads();
+	T ca = T(1), cb = T(0);
+	if (forward) {
+		for (int kk = 0; kk < k; ++kk) {  // carry = M_{k-1} o ... o M_0
+			int sl = slot_self + (kk - k) * slot_stride;
+			T a2 = sA[sl], b2 = sB[sl];
+			T na = a2 * ca, nb = a2 * cb + b2;
+			ca = na; cb = nb;
+		}
+	} else {
+		for (int kk = NWG - 1; kk > k; --kk) {  // carry = M_{k+1} o ... o M_{NWG-1}
+			int sl = slot_self + (kk - k) * slot_stride;
+			T a2 = sA[sl], b2 = sB[sl];
+			T na = a2 * ca, nb = a2 * cb + b2;
+			ca = na; cb = nb;
+		}
+	}
+	return ae * cb + be;
+}
+
+constexpr int FAST_BLOCK_X = 256, FAST_BLOCK_Y = 512;
+
+template <typename T, int NS, int DIR, int K>
+__global__ void __launch_bounds__(DIR == CDR_DIR_X ? FAST_BLOCK_X : FAST_BLOCK_Y)
+    k_lines_fast(const T *__restrict__ so, T *__restrict__ q, const T *__restrict__ qf, const T *__restrict__ sor,
+                 Dims2 d, int tpitch, int first, int tpl_log2)
+{
+	// one carry slot per (warp, line of the warp): at most 16 warps x 32 lines
+	__shared__ T sA[FAST_BLOCK_Y], sB[FAST_BLOCK_Y];
+	const int TPL = 1 << tpl_log2;
+	const int G = blockDim.x >> tpl_log2;  // lines per CTA
+	const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+	int g, t;
+	if (DIR == CDR_DIR_X) { g = tid >> tpl_log2; t = tid & (TPL - 1); }
+	else { g = tid % G; t = tid / G; }
+	const int n = DIR == CDR_DIR_X ? d.nx : d.ny;
+	const int nl = DIR == CDR_DIR_X ? d.ny : d.nx;
+	const int lc = first + 2 * (blockIdx.x * G + g);
+	const bool active = lc <= nl;
+	const int p0 = t * K;
+	const bool has = active && p0 <= n;
+	const size_t ps = d.plane();
+	const int P = d.pitch;
+	const T *D = DIR == CDR_DIR_X ? sor + (size_t)lc * P : sor + (size_t)lc * tpitch;
+	const T *E = DIR == CDR_DIR_X ? sor + ps + (size_t)lc * P : sor + (size_t)tpitch * (d.nx + 2) + (size_t)lc * tpitch;
+
+	// 1. right-hand sides of the chunk
+	T r[K];
+#pragma unroll
+	for (int m = 0; m < K; ++m) r[m] = T(0);
+	if (has) {
+		if (DIR == CDR_DIR_X) {
+			const size_t k0 = d.at(p0, lc);
+			const T *w = so + ps, *s = so + 2 * ps, *sw = so + 3 * ps, *nw = so + 4 * ps;
+			T b_[K], qm[K], qp[K], s0[K], s1[K];
+			vload<T, K>(qf + k0, b_);
+			vload<T, K>(q + k0 - P, qm);
+			vload<T, K>(q + k0 + P, qp);
+			vload<T, K>(s + k0, s0);
+			vload<T, K>(s + k0 + P, s1);
+#pragma unroll
+			for (int m = 0; m < K; ++m) r[m] = b_[m] + s0[m] * qm[m] + s1[m] * qp[m];
+			if (NS == 5) {
+				T sw0[K], nw0[K], nw1[K], sw1[K];
+				vload<T, K>(sw + k0, sw0);
+				vload<T, K>(nw + k0, nw0);
+				vload<T, K>(nw + k0 + P, nw1);
+				vload<T, K>(sw + k0 + P, sw1);
+				const T qm_l = p0 >= 1 ? q[k0 - P - 1] : T(0), qp_l = p0 >= 1 ? q[k0 + P - 1] : T(0);
+				const bool rin = p0 + K <= n + 1;
+				const T qm_r = rin ? q[k0 - P + K] : T(0), qp_r = rin ? q[k0 + P + K] : T(0);
+				const T nw0_r = rin ? nw[k0 + K] : T(0), sw1_r = rin ? sw[k0 + P + K] : T(0);
+#pragma unroll
+				for (int m = 0; m < K; ++m) {
+					const T qml = m > 0 ? qm[m - 1] : qm_l, qmr = m < K - 1 ? qm[m + 1] : qm_r;
+					const T qpl = m > 0 ? qp[m - 1] : qp_l, qpr = m < K - 1 ? qp[m + 1] : qp_r;
+					const T nwr = m < K - 1 ? nw0[m + 1] : nw0_r, swr = m < K - 1 ? sw1[m + 1] : sw1_r;
+					// operand order of relax_lines_x.f90:106-110
+					r[m] = b_[m] + s0[m] * qm[m] + s1[m] * qp[m] + sw0[m] * qml + nwr * qmr + nw1[m] * qpl + swr * qpr;
+				}
+			}
+		} else {
+			const int i = lc;
+			const T *w = so + ps, *sw = so + 3 * ps, *nw = so + 4 * ps;
+#pragma unroll
+			for (int m = 0; m < K; ++m) {
+				const int jj = p0 + m;
+				if (jj < 1 || jj > n) continue;
+				const size_t k = d.at(i, jj);
+				if (NS == 5)
+					r[m] = qf[k] + w[k] * q[k - 1] + w[k + 1] * q[k + 1] + sw[k] * q[k - P - 1] + nw[k + 1] * q[k - P + 1]
+					       + nw[k + P] * q[k + P - 1] + sw[k + P + 1] * q[k + P + 1];
+				else
+					r[m] = qf[k] + w[k] * q[k - 1] + w[k + 1] * q[k + 1];
+			}
+		}
+	}
+
+	// scan geometry
+	int S, CW, NWG, kgrp, slot, sstride;
+	if (DIR == CDR_DIR_X) {
+		S = 1;
+		CW = TPL < 32 ? TPL : 32;
+		NWG = TPL > 32 ? TPL / 32 : 1;
+		kgrp = TPL > 32 ? (tid - (g << tpl_log2)) >> 5 : 0;
+		slot = warp;
+		sstride = 1;
+	} else {
+		S = G < 32 ? G : 32;
+		CW = 32 / S;
+		NWG = blockDim.x / 32;
+		kgrp = warp;
+		slot = warp * (32 / CW) + (lane % S);  // one slot per (warp, line of the warp)
+		sstride = 32 / CW;
+	}
+	const int u = DIR == CDR_DIR_X ? (lane & (CW - 1)) : lane / S;
+
+	// 2a. forward substitution y(p) = r(p) - y(p-1) E(p)
+	T Ev[K];
+	if (has) vload<T, K>(E + p0, Ev);
+	T A = T(1), B = T(0);
+	if (has) {
+#pragma unroll
+		for (int m = 0; m < K; ++m) {
+			const int pos = p0 + m;
+			if (pos < 1 || pos > n) continue;
+			const T a = pos == 1 ? T(0) : -Ev[m];
+			B = a * B + r[m];
+			A = a * A;
+		}
+	}
+	T y = scan_incoming<T>(A, B, true, u, S, CW, NWG, kgrp, slot, sstride, sA, sB);
+	if (has) {
+#pragma unroll
+		for (int m = 0; m < K; ++m) {
+			const int pos = p0 + m;
+			if (pos < 1 || pos > n) continue;
+			y = pos == 1 ? r[m] : r[m] - y * Ev[m];
+			r[m] = y;
+		}
+	}
+	// 2b. backward substitution x(p) = y(p)/D(p) - x(p+1) E(p+1)
+	T Dv[K];
+	if (has) vload<T, K>(D + p0, Dv);
+	const T Enext = has && p0 + K <= n ? E[p0 + K] : T(0);
+	A = T(1);
+	B = T(0);
+	if (has) {
+#pragma unroll
+		for (int m = K - 1; m >= 0; --m) {
+			const int pos = p0 + m;
+			if (pos < 1 || pos > n) continue;
+			const T e1 = m < K - 1 ? Ev[m + 1] : Enext;
+			const T a = pos == n ? T(0) : -e1;
+			B = a * B + r[m] / Dv[m];
+			A = a * A;
+		}
+	}
+	if (NWG > 1) __syncthreads();  // the forward carries are still being read
+	T x = scan_incoming<T>(A, B, false, u, S, CW, NWG, kgrp, slot, sstride, sA, sB);
+	if (has) {
+#pragma unroll
+		for (int m = K - 1; m >= 0; --m) {
+			const int pos = p0 + m;
+			if (pos < 1 || pos > n) continue;
+			const T e1 = m < K - 1 ? Ev[m + 1] : Enext;
+			x = pos == n ? r[m] / Dv[m] : r[m] / Dv[m] - x * e1;
+			r[m] = x;
+		}
+	}
+
+	// 3. write back the interior positions of the chunk
+	if (has) {
+		if (DIR == CDR_DIR_X) {
+			const size_t k0 = d.at(p0, lc);
+			if (p0 >= 1 && p0 + K - 1 <= n) vstore<T, K>(q + k0, r);
+			else {
+#pragma unroll
+				for (int m = 0; m < K; ++m) {
+					const int pos = p0 + m;
+					if (pos >= 1 && pos <= n) q[k0 + m] = r[m];
+				}
+			}
+		} else {
+#pragma unroll
+			for (int m = 0; m < K; ++m) {
+				const int pos = p0 + m;
+				if (pos >= 1 && pos <= n) q[d.at(lc, pos)] = r[m];
+			}
+		}
+	}
+}
+
 // Opt every line kernel into the large dynamic shared-memory carve-out once per
 // process (before any graph capture: the solver calls this at creation).
 int lines_prepare()
@@ -264,9 +541,27 @@ static int launch_lines(const T *so, T *x, const T *b, const T *sor, Dims2 d, in
 {
 	const int n = DIR == CDR_DIR_X ? d.nx : d.ny;
 	const int nl = DIR == CDR_DIR_X ? d.ny : d.nx;
-	const int G = lines_per_cta<T>(n, DIR);
 	const int nlines = first > nl ? 0 : (nl - first) / 2 + 1;
 	if (nlines == 0) return CDR_OK;
+	constexpr int K = 8;
+	// The register-chunk kernel reads whole 16-byte-aligned chunks of K elements:
+	// rows (x) or factor lines (y) must have a pitch that is a multiple of K and
+	// 16-byte aligned base pointers; lines up to 256*K - 1 points.
+	const int fpitch = DIR == CDR_DIR_X ? d.pitch : tpitch;
+	const bool aligned = ((uintptr_t)so | (uintptr_t)x | (uintptr_t)b | (uintptr_t)sor) % 16 == 0;
+	if (!exact && aligned && d.pitch % K == 0 && fpitch % K == 0 && n + 1 <= 256 * K) {
+		int tpl_log2 = 0;
+		while ((1 << tpl_log2) * K < n + 1) ++tpl_log2;
+		const int TPL = 1 << tpl_log2;
+		// x: 256 threads, 256/TPL lines per CTA; y: at most 32 lines per CTA so that
+		// every warp holds the same lines (lanes are line-fastest)
+		const int block = DIR == CDR_DIR_X ? FAST_BLOCK_X : (TPL * 32 < FAST_BLOCK_Y ? TPL * 32 : FAST_BLOCK_Y);
+		const int G = block / TPL;
+		k_lines_fast<T, NS, DIR, K><<<ceil_div(nlines, G), block, 0, st>>>(so, x, b, sor, d, tpitch, first, tpl_log2);
+		CDR_LAUNCH_CHECK();
+		return CDR_OK;
+	}
+	const int G = lines_per_cta<T>(n, DIR);
 	size_t smem = sizeof(T) * (2 * LT + (size_t)G * n);
 	if (smem > 227 * 1024) {
 		set_error(CDR_ERR_DIM, "line length %d too long for one CTA", n);

@@ -183,6 +183,42 @@ def test_line_relax(lib, oracle, nx, ny, ns, updown):
         assert rel_err(host(fx), xr) < 1e-4, direction
 
 
+LINE_SIZES = [(9, 9, 3), (17, 12, 5), (64, 63, 3), (130, 97, 5), (255, 31, 5), (31, 255, 5), (1023, 20, 5),
+              (20, 1023, 5), (2047, 12, 5), (12, 2047, 5), (2047, 9, 3), (9, 2047, 3)]
+
+
+@pytest.mark.parametrize("nx,ny,ns", LINE_SIZES)
+@pytest.mark.parametrize("precision", ["f64", "f32"])
+def test_line_relax_register_chunk_kernel(lib, oracle, nx, ny, ns, precision):
+    """Padded pitches (multiples of 32) select the register-chunk sweep kernel."""
+    import torch
+    so, x, b = make_op(nx, ny, ns), grid(nx, ny, 8), grid(nx, ny, 9)
+    sx, _ = oracle.setup_lines_x(so)
+    sy, _ = oracle.setup_lines_y(so)
+    pitch = ((nx + 2 + 31) // 32) * 32
+    tpitch = ((ny + 2 + 31) // 32) * 32
+    dt = torch.float64 if precision == "f64" else torch.float32
+    fn = lib.cdr_gpu_relax_lines_2d_f64 if precision == "f64" else lib.cdr_gpu_relax_lines_2d_f32
+    dso = padded(so, pitch, dt)
+    dbb = padded(b, pitch, dt)
+    dsx = padded(sx, pitch, dt)
+    dsy = padded(sy, tpitch, dt)
+    for direction, sor, dsor, ofn in ((_lib.DIR_X, sx, dsx, oracle.relax_lines_x), (_lib.DIR_Y, sy, dsy, oracle.relax_lines_y)):
+        for updown in (0, 1):
+            xr = x.copy()
+            ofn(so, xr, b, sor, updown)
+            dx = padded(x, pitch, dt)
+            _lib.check(fn(ptr(dso), ns, ptr(dx), ptr(dbb), ptr(dsor), nx, ny, pitch, tpitch, direction, updown, 0,
+                          stream()))
+            got = host(dx)[:, :nx + 2]
+            tol = 1e-12 if precision == "f64" else 2e-4
+            assert rel_err(got, xr) < tol, (direction, updown, rel_err(got, xr))
+            np.testing.assert_array_equal(got[0], 0.0)
+            np.testing.assert_array_equal(got[-1], 0.0)
+            np.testing.assert_array_equal(got[:, 0], 0.0)
+            np.testing.assert_array_equal(got[:, nx + 1], 0.0)
+
+
 def test_line_setup_reports_nonpositive_pivot(lib):
     nx = ny = 8
     so = G.diag_diffusion(nx, ny, 1.0, 1.0)
