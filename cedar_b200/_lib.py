@@ -82,6 +82,7 @@ def load(path=LIB_PATH):
             "cdr_gpu_solve_cg_2d_" + suf: (I, [P, P, P, I, I, I, S]),
         })
     sig.update({
+        "cdr_gpu_residual_2d_f64_noalloc": (I, [P, I, P, P, P, I, I, I, P, S]),
         "cdr_gpu_setup_interp_2d_f64": (I, [P, I, P, I, I, I, I, I, I, S]),
         "cdr_gpu_galerkin_2d_f64": (I, [P, I, P, P, I, I, I, I, I, I, S]),
         "cdr_gpu_setup_cg_2d_f64": (I, [P, I, I, I, I, P, P, S]),

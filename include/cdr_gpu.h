@@ -79,6 +79,20 @@ int cdr_gpu_residual_2d_f64(const double *so, int nstencil, const double *x, con
 int cdr_gpu_residual_2d_f32(const float *so, int nstencil, const float *x, const float *b, float *r,
                             int nx, int ny, int pitch, double *norm_out, void *scratch, cudaStream_t stream);
 
+/* The same residual and ||r||_2 without any device allocation and without
+ * caller scratch, for callers that cannot allocate device memory when they call
+ * the library (a plugin inside an application that owns every device allocation
+ * and forbids cudaMalloc/cudaFree during a run).  No counterpart in the
+ * reference.  The partial sums live in a fixed 512 KiB array of device memory
+ * (65536 slots, one per 32x8 tile), reserved on every GPU that loads the library
+ * until the process exits; grids of more than 65536 tiles (e.g. beyond
+ * 4096x4096 points) are rejected with CDR_ERR_DIM.  The first call on a device
+ * looks the array up (once per device, device current): make it before any
+ * stream capture.  All calls share the array: calls that overlap on the GPU
+ * race.  norm_out (device, one double) is required. */
+int cdr_gpu_residual_2d_f64_noalloc(const double *so, int nstencil, const double *x, const double *b, double *r,
+                                   int nx, int ny, int pitch, double *norm_out, cudaStream_t stream);
+
 /* sor = 1/c; replaces point_relax::setup (include/cedar/kernels/point_relax.h:31-46)
  * -> BMG2_SymStd_SETUP_recip (src/2d/relax.cc:23-33, src/2d/ftn/BMG2_SymStd_SETUP_recip.f90:63-67).
  * sor is one plane (Cedar keeps it in plane 2 of a 2-plane relax_stencil). */
