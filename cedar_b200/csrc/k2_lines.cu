@@ -328,14 +328,14 @@ __device__ __forceinline__ T scan_incoming(T A, T B, bool forward, int u, int S,
 	return ae * cb + be;
 }
 
-constexpr int FAST_BLOCK_X = 256, FAST_BLOCK_Y = 512;
+constexpr int FAST_BLOCK_X = 256, FAST_BLOCK_Y = 1024;
 
 template <typename T, int NS, int DIR, int K>
-__global__ void __launch_bounds__(DIR == CDR_DIR_X ? FAST_BLOCK_X : FAST_BLOCK_Y)
+__global__ void __launch_bounds__(DIR == CDR_DIR_X ? FAST_BLOCK_X : FAST_BLOCK_Y, DIR == CDR_DIR_X ? 2 : 1)
     k_lines_fast(const T *__restrict__ so, T *__restrict__ q, const T *__restrict__ qf, const T *__restrict__ sor,
                  Dims2 d, int tpitch, int first, int tpl_log2)
 {
-	// one carry slot per (warp, line of the warp): at most 16 warps x 32 lines
+	// one carry slot per (warp, line of the warp): at most 32 warps x 32 lines
 	__shared__ T sA[FAST_BLOCK_Y], sB[FAST_BLOCK_Y];
 	const int TPL = 1 << tpl_log2;
 	const int G = blockDim.x >> tpl_log2;  // lines per CTA
@@ -424,6 +424,7 @@ __global__ void __launch_bounds__(DIR == CDR_DIR_X ? FAST_BLOCK_X : FAST_BLOCK_Y
 		sstride = 32 / CW;
 	}
 	const int u = DIR == CDR_DIR_X ? (lane & (CW - 1)) : lane / S;
+	const bool full = p0 >= 1 && p0 + K - 1 <= n;  // no ghost or beyond-end position in the chunk
 
 	// 2a. forward substitution y(p) = r(p) - y(p-1) E(p)
 	T Ev[K];
@@ -433,8 +434,8 @@ __global__ void __launch_bounds__(DIR == CDR_DIR_X ? FAST_BLOCK_X : FAST_BLOCK_Y
 #pragma unroll
 		for (int m = 0; m < K; ++m) {
 			const int pos = p0 + m;
-			if (pos < 1 || pos > n) continue;
-			const T a = pos == 1 ? T(0) : -Ev[m];
+			if (!full && (pos < 1 || pos > n)) continue;
+			const T a = (!full && pos == 1) ? T(0) : -Ev[m];
 			B = a * B + r[m];
 			A = a * A;
 		}
@@ -444,14 +445,24 @@ __global__ void __launch_bounds__(DIR == CDR_DIR_X ? FAST_BLOCK_X : FAST_BLOCK_Y
 #pragma unroll
 		for (int m = 0; m < K; ++m) {
 			const int pos = p0 + m;
-			if (pos < 1 || pos > n) continue;
-			y = pos == 1 ? r[m] : r[m] - y * Ev[m];
+			if (!full && (pos < 1 || pos > n)) continue;
+			y = (!full && pos == 1) ? r[m] : r[m] - y * Ev[m];
 			r[m] = y;
+		}
+		// y(p)/D(p), the first operation of the DPTTS2 back substitution, in place
+		constexpr int W = 16 / sizeof(T);
+#pragma unroll
+		for (int c = 0; c < K / W; ++c) {
+			T dv[W];
+			vload<T, W>(D + p0 + c * W, dv);
+#pragma unroll
+			for (int w = 0; w < W; ++w) {
+				const int m = c * W + w, pos = p0 + m;
+				if (full || (pos >= 1 && pos <= n)) r[m] = r[m] / dv[w];
+			}
 		}
 	}
 	// 2b. backward substitution x(p) = y(p)/D(p) - x(p+1) E(p+1)
-	T Dv[K];
-	if (has) vload<T, K>(D + p0, Dv);
 	const T Enext = has && p0 + K <= n ? E[p0 + K] : T(0);
 	A = T(1);
 	B = T(0);
@@ -459,10 +470,10 @@ __global__ void __launch_bounds__(DIR == CDR_DIR_X ? FAST_BLOCK_X : FAST_BLOCK_Y
 #pragma unroll
 		for (int m = K - 1; m >= 0; --m) {
 			const int pos = p0 + m;
-			if (pos < 1 || pos > n) continue;
+			if (!full && (pos < 1 || pos > n)) continue;
 			const T e1 = m < K - 1 ? Ev[m + 1] : Enext;
 			const T a = pos == n ? T(0) : -e1;
-			B = a * B + r[m] / Dv[m];
+			B = a * B + r[m];
 			A = a * A;
 		}
 	}
@@ -472,9 +483,9 @@ __global__ void __launch_bounds__(DIR == CDR_DIR_X ? FAST_BLOCK_X : FAST_BLOCK_Y
 #pragma unroll
 		for (int m = K - 1; m >= 0; --m) {
 			const int pos = p0 + m;
-			if (pos < 1 || pos > n) continue;
+			if (!full && (pos < 1 || pos > n)) continue;
 			const T e1 = m < K - 1 ? Ev[m + 1] : Enext;
-			x = pos == n ? r[m] / Dv[m] : r[m] / Dv[m] - x * e1;
+			x = pos == n ? r[m] : r[m] - x * e1;
 			r[m] = x;
 		}
 	}
@@ -543,21 +554,30 @@ static int launch_lines(const T *so, T *x, const T *b, const T *sor, Dims2 d, in
 	const int nl = DIR == CDR_DIR_X ? d.ny : d.nx;
 	const int nlines = first > nl ? 0 : (nl - first) / 2 + 1;
 	if (nlines == 0) return CDR_OK;
-	constexpr int K = 8;
 	// The register-chunk kernel reads whole 16-byte-aligned chunks of K elements:
 	// rows (x) or factor lines (y) must have a pitch that is a multiple of K and
-	// 16-byte aligned base pointers; lines up to 256*K - 1 points.
+	// 16-byte aligned base pointers; lines up to 2048*8 - 1 points.
 	const int fpitch = DIR == CDR_DIR_X ? d.pitch : tpitch;
 	const bool aligned = ((uintptr_t)so | (uintptr_t)x | (uintptr_t)b | (uintptr_t)sor) % 16 == 0;
-	if (!exact && aligned && d.pitch % K == 0 && fpitch % K == 0 && n + 1 <= 256 * K) {
+	// x: K = 8, 256 threads, 256/TPL lines per CTA.  y: K = 16 for long lines so that
+	// a warp holds 8 lines side by side, at most 32 lines per CTA (lanes are
+	// line-fastest: every warp holds the same lines).
+	const int K = (DIR == CDR_DIR_Y && sizeof(T) == 4 && n + 1 > 8 * 128) ? 16 : 8;
+	if (!exact && aligned && d.pitch % 16 == 0 && fpitch % 16 == 0 && n + 1 <= 256 * K) {
 		int tpl_log2 = 0;
 		while ((1 << tpl_log2) * K < n + 1) ++tpl_log2;
 		const int TPL = 1 << tpl_log2;
-		// x: 256 threads, 256/TPL lines per CTA; y: at most 32 lines per CTA so that
-		// every warp holds the same lines (lanes are line-fastest)
 		const int block = DIR == CDR_DIR_X ? FAST_BLOCK_X : (TPL * 32 < FAST_BLOCK_Y ? TPL * 32 : FAST_BLOCK_Y);
 		const int G = block / TPL;
-		k_lines_fast<T, NS, DIR, K><<<ceil_div(nlines, G), block, 0, st>>>(so, x, b, sor, d, tpitch, first, tpl_log2);
+		if constexpr (DIR == CDR_DIR_Y && sizeof(T) == 4) {
+			if (K == 16) {
+				k_lines_fast<T, NS, DIR, 16>
+				    <<<ceil_div(nlines, G), block, 0, st>>>(so, x, b, sor, d, tpitch, first, tpl_log2);
+				CDR_LAUNCH_CHECK();
+				return CDR_OK;
+			}
+		}
+		k_lines_fast<T, NS, DIR, 8><<<ceil_div(nlines, G), block, 0, st>>>(so, x, b, sor, d, tpitch, first, tpl_log2);
 		CDR_LAUNCH_CHECK();
 		return CDR_OK;
 	}
