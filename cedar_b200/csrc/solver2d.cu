@@ -299,7 +299,21 @@ int cdr_gpu_solver_destroy(cdr_gpu_solver *h)
 	return CDR_OK;
 }
 
-static int create_impl(cdr_gpu_solver *h, const double *so_host, int ns, int nx, int ny)
+static int load_and_setup(cdr_gpu_solver *h, const double *so, int src_pitch, cudaMemcpyKind kind)
+{
+	Level &F = h->lv[0];
+	CDR_CUDA_TRY(cudaMemcpy2DAsync(F.so, F.d.pitch * sizeof(double), so, src_pitch * sizeof(double),
+	                               (F.nx + 2) * sizeof(double), (size_t)(F.ny + 2) * F.ns, kind, h->st));
+	CDR_CUDA_TRY(cudaEventRecord(h->ev0, h->st));
+	CDR_TRY(h->setup());
+	CDR_CUDA_TRY(cudaEventRecord(h->ev1, h->st));
+	CDR_CUDA_TRY(cudaEventSynchronize(h->ev1));
+	CDR_CUDA_TRY(cudaEventElapsedTime(&h->setup_ms, h->ev0, h->ev1));
+	return CDR_OK;
+}
+
+static int create_impl(cdr_gpu_solver *h, const double *so_src, int ns, int nx, int ny, int src_pitch,
+                       cudaMemcpyKind kind)
 {
 	const cdr_gpu_settings &s = h->s;
 	int nl = num_levels(nx, ny, s.min_coarse);
@@ -359,22 +373,14 @@ static int create_impl(cdr_gpu_solver *h, const double *so_host, int ns, int nx,
 		CDR_TRY(h->alloc(&h->x64[1], h->lv[0].d.plane()));
 	}
 	CDR_CUDA_TRY(cudaMallocHost(&h->h_norm, 4 * sizeof(double)));
-	// fine operator, Cedar layout (pitch nx+2) -> device pitch
-	Level &F = h->lv[0];
-	CDR_CUDA_TRY(cudaMemcpy2DAsync(F.so, F.d.pitch * sizeof(double), so_host, (nx + 2) * sizeof(double),
-	                               (nx + 2) * sizeof(double), (size_t)(ny + 2) * ns, cudaMemcpyHostToDevice, h->st));
-	CDR_CUDA_TRY(cudaEventRecord(h->ev0, h->st));
-	CDR_TRY(h->setup());
-	CDR_CUDA_TRY(cudaEventRecord(h->ev1, h->st));
-	CDR_CUDA_TRY(cudaEventSynchronize(h->ev1));
-	CDR_CUDA_TRY(cudaEventElapsedTime(&h->setup_ms, h->ev0, h->ev1));
-	return CDR_OK;
+	// fine operator (source pitch) -> device pitch, then the device setup
+	return load_and_setup(h, so_src, src_pitch, kind);
 }
 
-int cdr_gpu_solver_create_2d(const cdr_gpu_settings *s, const double *so_host, int ns, int nx, int ny,
-                             cudaStream_t stream, cdr_gpu_solver **out)
+static int create_any(const cdr_gpu_settings *s, const double *so_src, int ns, int nx, int ny, int src_pitch,
+                      cudaMemcpyKind kind, cudaStream_t stream, cdr_gpu_solver **out)
 {
-	if (!s || !so_host || !out) { set_error(CDR_ERR_ARG, "null argument"); return CDR_ERR_ARG; }
+	if (!s || !so_src || !out) { set_error(CDR_ERR_ARG, "null argument"); return CDR_ERR_ARG; }
 	if (ns != 3 && ns != 5) { set_error(CDR_ERR_ARG, "nstencil must be 3 or 5"); return CDR_ERR_ARG; }
 	if (nx < 1 || ny < 1) { set_error(CDR_ERR_DIM, "bad grid %dx%d", nx, ny); return CDR_ERR_DIM; }
 	if (s->relaxation < CDR_RELAX_POINT || s->relaxation > CDR_RELAX_LINE_XY) {
@@ -400,13 +406,34 @@ int cdr_gpu_solver_create_2d(const cdr_gpu_settings *s, const double *so_host, i
 	cudaEventCreate(&h->ev0);
 	cudaEventCreate(&h->ev1);
 	int rc = lines_prepare();
-	if (rc == CDR_OK) rc = create_impl(h, so_host, ns, nx, ny);
+	if (rc == CDR_OK) rc = create_impl(h, so_src, ns, nx, ny, src_pitch, kind);
 	if (rc != CDR_OK) {
 		cdr_gpu_solver_destroy(h);
 		return rc;
 	}
 	*out = h;
 	return CDR_OK;
+}
+
+int cdr_gpu_solver_create_2d(const cdr_gpu_settings *s, const double *so_host, int ns, int nx, int ny,
+                             cudaStream_t stream, cdr_gpu_solver **out)
+{
+	return create_any(s, so_host, ns, nx, ny, nx + 2, cudaMemcpyHostToDevice, stream, out);
+}
+
+int cdr_gpu_solver_create_2d_device(const cdr_gpu_settings *s, const double *so_dev, int ns, int nx, int ny,
+                                    int pitch, cudaStream_t stream, cdr_gpu_solver **out)
+{
+	if (pitch < nx + 2) { set_error(CDR_ERR_DIM, "pitch %d < nx+2", pitch); return CDR_ERR_DIM; }
+	return create_any(s, so_dev, ns, nx, ny, pitch, cudaMemcpyDeviceToDevice, stream, out);
+}
+
+int cdr_gpu_solver_resetup_device(cdr_gpu_solver *h, const double *so_dev, int pitch)
+{
+	if (!h) { set_error(CDR_ERR_HANDLE, "null solver"); return CDR_ERR_HANDLE; }
+	if (!so_dev) { set_error(CDR_ERR_ARG, "null operator"); return CDR_ERR_ARG; }
+	if (pitch < h->lv[0].nx + 2) { set_error(CDR_ERR_DIM, "pitch %d < nx+2", pitch); return CDR_ERR_DIM; }
+	return load_and_setup(h, so_dev, pitch, cudaMemcpyDeviceToDevice);
 }
 
 // multilevel::solve (include/cedar/multilevel.h:278-298) on the level-0 buffers.

@@ -94,3 +94,25 @@ def hetero_diffusion(n, ell=1.0 / 32, sigma=2.0, n_incl=64, contrast=1e4, aniso=
     b = np.zeros((n + 2, n + 2))
     b[1:-1, 1:-1] = rng.uniform(0.0, 1.0, size=(n, n)) * h * h
     return so, b
+
+
+def inverse_problem(n, n_src=8, ell=1.0 / 32, sigma=1.0, seed_theta=8, seed_src=9, seed_obs=10):
+    """Inverse-diffusion setup on (n+1)^2 cells: (theta, theta_obs, f).
+
+    theta, theta_obs: log-coefficient Gaussian fields (cells); f: n_src unit point
+    sources at seeded interior nodes (ghost-inclusive node array)."""
+    nc = n + 1
+    theta = gaussian_field(nc, nc, ell, sigma, seed_theta)
+    theta_obs = gaussian_field(nc, nc, ell, sigma, seed_obs)
+    rng = np.random.default_rng(seed_src)
+    f = np.zeros((n + 2, n + 2))
+    pts = rng.integers(1, n + 1, size=(n_src, 2))
+    for i, j in pts:
+        f[j, i] += 1.0
+    return theta, theta_obs, f
+
+
+def fd_cells(n, count=32, seed=11):
+    """Seeded cell indices (cj, ci) for finite-difference checks."""
+    rng = np.random.default_rng(seed)
+    return rng.integers(0, n + 1, size=(count, 2))

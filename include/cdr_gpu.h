@@ -180,6 +180,21 @@ int cdr_gpu_solve_cg_2d_f32(const double *abd, float *x, const float *b, int nx,
                             cudaStream_t stream);
 
 /* ------------------------------------------------------------------------
+ * Bilinear finite elements of -div(K grad u), K = diag(kx, ky) per cell, on
+ * the unit square with Dirichlet zero boundary (the reference's gallery has
+ * only constant-coefficient operators, src/2d/gallery.cc:7-113).  Cells form an
+ * (ny+1) x (nx+1) array with row pitch cell_pitch >= nx+1; cell (cj, ci) has
+ * corner nodes (ci..ci+1, cj..cj+1) in the ghost-inclusive node index.
+ * ------------------------------------------------------------------------ */
+/* so (nine_pt, 5 planes) = assembled operator. */
+int cdr_gpu_fe_assemble_2d_f64(const double *kx, const double *ky, int cell_pitch, double *so, int nx, int ny,
+                               int pitch, cudaStream_t stream);
+/* Per-cell dL/dkx = -lam_e^T Ex u_e and dL/dky = -lam_e^T Ey u_e, where u solves
+ * A u = f and lam solves A lam = dL/du (A symmetric). */
+int cdr_gpu_fe_grad_2d_f64(const double *u, const double *lam, int nx, int ny, int pitch, double *gkx,
+                           double *gky, int cell_pitch, cudaStream_t stream);
+
+/* ------------------------------------------------------------------------
  * 2D multilevel solver: setup in create (multilevel::setup,
  * include/cedar/multilevel.h:243-265), solve (multilevel::solve, :278-298),
  * vcycle (multilevel::vcycle, :80-84).
@@ -207,6 +222,12 @@ int cdr_gpu_settings_default(cdr_gpu_settings *s);
  * (pitch nx+2, nstencil planes).  stream may be 0 (the library creates its own). */
 int cdr_gpu_solver_create_2d(const cdr_gpu_settings *s, const double *so_host, int nstencil, int nx, int ny,
                              cudaStream_t stream, cdr_gpu_solver **out);
+/* Same from a DEVICE fine operator of the given pitch. */
+int cdr_gpu_solver_create_2d_device(const cdr_gpu_settings *s, const double *so_dev, int nstencil, int nx, int ny,
+                                    int pitch, cudaStream_t stream, cdr_gpu_solver **out);
+/* Replace the fine operator (same size and stencil) and rerun the whole setup
+ * on the existing allocations; the captured cycle graphs stay valid. */
+int cdr_gpu_solver_resetup_device(cdr_gpu_solver *h, const double *so_dev, int pitch);
 int cdr_gpu_solver_destroy(cdr_gpu_solver *h);
 
 /* Solve with HOST buffers in Cedar's layout ((nx+2)*(ny+2) doubles).  x holds the
