@@ -309,6 +309,7 @@ def main():
 
     if rank == 0 and world == 1 and not args.no_extras:
         out["to_1e-10"] = to_1e10(args, stream)
+        out["inverse_diffusion"] = inverse_batch()
         out["cpu_baseline"] = cpu_arm(args, so, b, it64, "config above")
         del out["cpu_baseline"]["setup_ms"], out["cpu_baseline"]["ms_per_cycle"]
     if rank == 0:
@@ -333,6 +334,47 @@ def vcycle_bytes(s, word):
     p, nx, ny, pitch, tp, ns = s.level_info(0, "so")
     total += nx * ny * 8 * 8  # FP64 outer residual + norm (so, x, b, r) ~ 8 words of 8 bytes
     return total
+
+
+def inverse_batch(batch=16, n=1023):
+    """Forward + backward of 0.5*||u(theta) - u_obs||^2 for a batch of independent
+    inverse-diffusion problems: FP32 log-coefficient parameters on (n+1)^2 cells,
+    8 point sources, FP32-cycle + FP64-refinement solves to 1e-10, adjoint solve
+    and coefficient-gradient kernel in backward."""
+    import numpy as np
+    import torch
+    from cedar_b200 import problems as P
+    from cedar_b200.autograd import solve_log_diffusion
+    probs = []
+    for b in range(batch):
+        theta, theta_obs, f = P.inverse_problem(n, seed_theta=8 + 100 * b, seed_src=9 + 100 * b,
+                                                seed_obs=10 + 100 * b)
+        probs.append((torch.tensor(theta, dtype=torch.float32, device="cuda"),
+                      torch.from_numpy(theta_obs).cuda(), torch.from_numpy(f).cuda()))
+    uobs = [solve_log_diffusion(to, f, tol=1e-10, maxiter=80).detach() for _, to, f in probs]
+
+    def step():
+        loss_tot = 0.0
+        for (theta, _, f), uo in zip(probs, uobs):
+            th = theta.clone().requires_grad_(True)
+            u = solve_log_diffusion(th, f, tol=1e-10, maxiter=80)
+            loss = 0.5 * ((u - uo) ** 2).sum()
+            loss.backward()
+            loss_tot += float(loss.detach())
+        return loss_tot
+
+    step()
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+    torch.cuda.synchronize()
+    ev[0].record()
+    step()
+    ev[1].record()
+    torch.cuda.synchronize()
+    ms = ev[0].elapsed_time(ev[1])
+    return {"workload": "%d inverse-diffusion problems, %d^2 cells, theta FP32 GRF sigma=1 (seed 8+100b), "
+                        "8 point sources, loss 0.5||u-u_obs||^2; forward FP32-cycle+FP64-IR to 1e-10, "
+                        "backward adjoint solve + gradient kernel" % (batch, n + 1),
+            "ms_forward_backward_batch": ms, "ms_per_problem": ms / batch}
 
 
 def to_1e10(args, stream):

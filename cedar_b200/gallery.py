@@ -178,3 +178,95 @@ def stencil_to_csr(so):
         couple((I > 1) & (J < ny), I - 1, J + 1, so[NW, J + 1, I])
     return sp.csr_matrix((np.concatenate(vals), (np.concatenate(rows), np.concatenate(cols))),
                          shape=(nx * ny, nx * ny))
+
+
+# --------------------------------------------------------------------------
+# 3D: trilinear (Q1) finite elements, 27-point operators in Cedar's 14-plane
+# lower-half storage (include/cedar/3d/base_types.h:4-20): p, pw, ps, b, psw,
+# pnw, bw, bnw, bn, bne, be, bse, bs, bsw.  Plane q at point s holds the negated
+# coupling between the two nodes listed in PLANES3[q] (offsets from s).
+# --------------------------------------------------------------------------
+P3, PW3, PS3, B3, PSW3, PNW3, BW3, BNW3, BN3, BNE3, BE3, BSE3, BS3, BSW3 = range(14)
+PLANES3 = {
+    PW3: ((0, 0, 0), (-1, 0, 0)), PS3: ((0, 0, 0), (0, -1, 0)), B3: ((0, 0, 0), (0, 0, -1)),
+    PSW3: ((0, 0, 0), (-1, -1, 0)), PNW3: ((0, -1, 0), (-1, 0, 0)), BW3: ((0, 0, 0), (-1, 0, -1)),
+    BNW3: ((0, -1, 0), (-1, 0, -1)), BN3: ((0, -1, 0), (0, 0, -1)), BNE3: ((-1, -1, 0), (0, 0, -1)),
+    BE3: ((-1, 0, 0), (0, 0, -1)), BSE3: ((-1, 0, 0), (0, -1, -1)), BS3: ((0, 0, 0), (0, -1, -1)),
+    BSW3: ((0, 0, 0), (-1, -1, -1)),
+}
+
+
+def q1_element_matrices_3d():
+    """(Ex, Ey, Ez) on a unit cube, local node l = a + 2b + 4c; A_e = h*k*(Ex+Ey+Ez)."""
+    K1 = np.array([[1.0, -1.0], [-1.0, 1.0]])
+    M1 = np.array([[2.0, 1.0], [1.0, 2.0]]) / 6.0
+    E = [np.zeros((8, 8)) for _ in range(3)]
+    for l1 in range(8):
+        a1, b1, c1 = l1 & 1, (l1 >> 1) & 1, l1 >> 2
+        for l2 in range(8):
+            a2, b2, c2 = l2 & 1, (l2 >> 1) & 1, l2 >> 2
+            E[0][l1, l2] = K1[a1, a2] * M1[b1, b2] * M1[c1, c2]
+            E[1][l1, l2] = M1[a1, a2] * K1[b1, b2] * M1[c1, c2]
+            E[2][l1, l2] = M1[a1, a2] * M1[b1, b2] * K1[c1, c2]
+    return E
+
+
+def fe3_hetero(k):
+    """27-point trilinear-FE operator of -div(k grad u), k per cell (nz+1, ny+1, nx+1),
+    Dirichlet zero boundary, h = 1/(n+1) per direction (cube cells)."""
+    k = np.asarray(k, dtype=np.float64)
+    ncz, ncy, ncx = k.shape
+    nx, ny, nz = ncx - 1, ncy - 1, ncz - 1
+    h = 1.0 / ncx
+    Ex, Ey, Ez = q1_element_matrices_3d()
+    Ae = h * (Ex + Ey + Ez)
+    # coupling arrays C[d][node] = A[node, node + d] for every offset d, ghost-inclusive node index
+    shape = (nz + 2, ny + 2, nx + 2)
+    C = {}
+    for l1 in range(8):
+        o1 = (l1 & 1, (l1 >> 1) & 1, l1 >> 2)
+        for l2 in range(8):
+            o2 = (l2 & 1, (l2 >> 1) & 1, l2 >> 2)
+            d = (o2[0] - o1[0], o2[1] - o1[1], o2[2] - o1[2])
+            arr = C.setdefault(d, np.zeros(shape))
+            arr[o1[2]:o1[2] + ncz, o1[1]:o1[1] + ncy, o1[0]:o1[0] + ncx] += k * Ae[l1, l2]
+    so = np.zeros((14,) + shape)
+    inner = np.zeros(shape, dtype=bool)
+    inner[1:-1, 1:-1, 1:-1] = True
+    so[P3][inner] = C[(0, 0, 0)][inner]
+    for q, (oa, ob) in PLANES3.items():
+        d = (ob[0] - oa[0], ob[1] - oa[1], ob[2] - oa[2])
+        # plane value at s = -A[s+oa, s+ob] = -C[d][s+oa]; both nodes must be interior
+        Z, Y, X = np.meshgrid(np.arange(nz + 2), np.arange(ny + 2), np.arange(nx + 2), indexing="ij")
+        ax, ay, az = X + oa[0], Y + oa[1], Z + oa[2]
+        bx, by, bz = X + ob[0], Y + ob[1], Z + ob[2]
+        ok = ((ax >= 1) & (ax <= nx) & (ay >= 1) & (ay <= ny) & (az >= 1) & (az <= nz)
+              & (bx >= 1) & (bx <= nx) & (by >= 1) & (by <= ny) & (bz >= 1) & (bz <= nz))
+        vals = np.zeros(shape)
+        vals[ok] = -C[d][az[ok], ay[ok], ax[ok]]
+        so[q] = vals
+    return so
+
+
+def stencil3_to_csr(so):
+    """Full sparse matrix of a 14-plane 3D stencil (interior unknowns, i fastest)."""
+    import scipy.sparse as sp
+    _, KK, JJ, II = so.shape
+    nx, ny, nz = II - 2, JJ - 2, KK - 2
+    idx = lambda i, j, k: ((k - 1) * ny + (j - 1)) * nx + (i - 1)
+    rows, cols, vals = [], [], []
+    Z, Y, X = np.meshgrid(np.arange(1, nz + 1), np.arange(1, ny + 1), np.arange(1, nx + 1), indexing="ij")
+    X, Y, Z = X.ravel(), Y.ravel(), Z.ravel()
+    rows.append(idx(X, Y, Z)); cols.append(idx(X, Y, Z)); vals.append(so[P3, Z, Y, X])
+    for q, (oa, ob) in PLANES3.items():
+        # entry at s couples s+oa and s+ob; s ranges over all points with both nodes interior
+        Zs, Ys, Xs = np.meshgrid(np.arange(KK), np.arange(JJ), np.arange(II), indexing="ij")
+        ax, ay, az = Xs + oa[0], Ys + oa[1], Zs + oa[2]
+        bx, by, bz = Xs + ob[0], Ys + ob[1], Zs + ob[2]
+        ok = ((ax >= 1) & (ax <= nx) & (ay >= 1) & (ay <= ny) & (az >= 1) & (az <= nz)
+              & (bx >= 1) & (bx <= nx) & (by >= 1) & (by <= ny) & (bz >= 1) & (bz <= nz))
+        v = -so[q][ok]
+        r1, r2 = idx(ax[ok], ay[ok], az[ok]), idx(bx[ok], by[ok], bz[ok])
+        rows += [r1, r2]; cols += [r2, r1]; vals += [v, v]
+    N = nx * ny * nz
+    return sp.csr_matrix((np.concatenate(vals), (np.concatenate(rows), np.concatenate(cols))), shape=(N, N))

@@ -289,3 +289,168 @@ class Solver:
         hist = np.zeros(max(self.settings.maxiter, 1))
         n = self.L.o2_solve(self.h, _p(b), _p(x), _p(hist), len(hist))
         return x, hist[:n].copy()
+
+
+# ======================================================================= 3D
+# Arrays: grid functions (nz+2, ny+2, nx+2); stencils (14, nz+2, ny+2, nx+2);
+# interpolation (26, nzc+2, nyc+2, nxc+2).
+
+class Settings3(ctypes.Structure):
+    _fields_ = [("nrelax_pre", ctypes.c_int), ("nrelax_post", ctypes.c_int), ("num_levels", ctypes.c_int),
+                ("maxiter", ctypes.c_int), ("tol", ctypes.c_double), ("min_coarse", ctypes.c_int)]
+
+
+_SIG3 = None
+
+
+def lib3(variant=""):
+    global _SIG3
+    L = lib(variant)
+    if not getattr(L, "_sig3", False):
+        P, I, D = ctypes.c_void_p, ctypes.c_int, ctypes.c_double
+        sig = {
+            "o3_residual": (None, [P, P, P, P, I, I, I]),
+            "o3_setup_recip": (None, [P, P, I, I, I]),
+            "o3_relax_gs": (None, [P, P, P, P, I, I, I, I]),
+            "o3_restrict": (None, [P, P, P, I, I, I, I, I, I]),
+            "o3_interp_add": (None, [P, P, P, P, P, I, I, I, I, I, I]),
+            "o3_setup_interp": (None, [P, P, I, I, I, I, I, I]),
+            "o3_galerkin": (None, [P, P, P, I, I, I, I, I, I]),
+            "o3_setup_cg": (I, [P, I, I, I, P, I]),
+            "o3_solve_cg": (None, [P, P, I, I, I, P, P, I]),
+            "o3_l2norm": (D, [P, I, I, I]),
+            "o3_num_levels": (I, [I, I, I, I]),
+            "o3_create": (P, [ctypes.POINTER(Settings3), P, I, I, I]),
+            "o3_destroy": (None, [P]),
+            "o3_vcycle": (None, [P, P, P]),
+            "o3_solve": (I, [P, P, P, P, I]),
+            "o3_nlevels": (I, [P]),
+            "o3_cg_info": (I, [P]),
+            "o3_level_dims": (None, [P, P]),
+            "o3_level_array": (ctypes.POINTER(ctypes.c_double), [P, I, I]),
+        }
+        for name, (res, args) in sig.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        L._sig3 = True
+    return L
+
+
+def _d3(a):
+    return a.shape[-1], a.shape[-2], a.shape[-3]
+
+
+def residual3(so, x, b):
+    II, JJ, KK = _d3(x)
+    r = np.zeros_like(x)
+    lib3().o3_residual(_p(so), _p(b), _p(x), _p(r), II, JJ, KK)
+    return r
+
+
+def setup_recip3(so):
+    II, JJ, KK = _d3(so)
+    sor = np.zeros(so.shape[1:])
+    lib3().o3_setup_recip(_p(so), _p(sor), II, JJ, KK)
+    return sor
+
+
+def relax_gs3(so, x, b, sor, updown):
+    II, JJ, KK = _d3(x)
+    lib3().o3_relax_gs(_p(so), _p(b), _p(x), _p(sor), II, JJ, KK, updown)
+    return x
+
+
+def setup_interp3(so, nxc, nyc, nzc):
+    II, JJ, KK = _d3(so)
+    ci = np.zeros((26, nzc + 2, nyc + 2, nxc + 2))
+    lib3().o3_setup_interp(_p(so), _p(ci), II, JJ, KK, nxc + 2, nyc + 2, nzc + 2)
+    return ci
+
+
+def galerkin3(so, ci):
+    II, JJ, KK = _d3(so)
+    IIC, JJC, KKC = _d3(ci)
+    soc = np.zeros((14, KKC, JJC, IIC))
+    lib3().o3_galerkin(_p(so), _p(soc), _p(ci), II, JJ, KK, IIC, JJC, KKC)
+    return soc
+
+
+def restrict3(ci, r):
+    II, JJ, KK = _d3(r)
+    IIC, JJC, KKC = _d3(ci)
+    bc = np.zeros((KKC, JJC, IIC))
+    lib3().o3_restrict(_p(ci), _p(r), _p(bc), II, JJ, KK, IIC, JJC, KKC)
+    return bc
+
+
+def interp_add3(ci, xc, res, so, x):
+    IIC, JJC, KKC = _d3(ci)
+    II, JJ, KK = _d3(x)
+    kp = np.ascontiguousarray(so[0])
+    lib3().o3_interp_add(_p(x), _p(xc), _p(res), _p(kp), _p(ci), IIC, JJC, KKC, II, JJ, KK)
+    return x
+
+
+def setup_cg3(so):
+    II, JJ, KK = _d3(so)
+    nx, ny, nz = II - 2, JJ - 2, KK - 2
+    nabd1 = nx * (ny + 1) + 2
+    abd = np.zeros((nx * ny * nz, nabd1))
+    info = lib3().o3_setup_cg(_p(so), II, JJ, KK, _p(abd), nabd1)
+    return abd, info
+
+
+def solve_cg3(abd, b):
+    II, JJ, KK = _d3(b)
+    x = np.zeros_like(b)
+    bbd = np.zeros((II - 2) * (JJ - 2) * (KK - 2))
+    lib3().o3_solve_cg(_p(x), _p(b), II, JJ, KK, _p(abd), _p(bbd), abd.shape[1])
+    return x
+
+
+def l2norm3(r):
+    II, JJ, KK = _d3(r)
+    return lib3().o3_l2norm(_p(r), II, JJ, KK)
+
+
+class Solver3:
+    """Serial 3D BoxMG (27-point fine operator, 8-colour point relaxation)."""
+
+    def __init__(self, so, nrelax_pre=2, nrelax_post=1, num_levels=-1, maxiter=10, tol=1e-8, min_coarse=3):
+        self.L = lib3()
+        so = np.ascontiguousarray(so, dtype=np.float64)
+        assert so.shape[0] == 14
+        self.nz, self.ny, self.nx = so.shape[1] - 2, so.shape[2] - 2, so.shape[3] - 2
+        self.s = Settings3(nrelax_pre, nrelax_post, num_levels, maxiter, tol, min_coarse)
+        self._so = so
+        self.h = self.L.o3_create(ctypes.byref(self.s), _p(so), self.nx, self.ny, self.nz)
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            self.L.o3_destroy(self.h)
+            self.h = None
+
+    @property
+    def nlevels(self):
+        return self.L.o3_nlevels(self.h)
+
+    def level_dims(self, l):
+        d = (ctypes.c_int * 3)()
+        self.L.o3_level_dims(self.h, l, d)
+        return d[0], d[1], d[2]
+
+    def level_array(self, l, which):
+        nx, ny, nz = self.level_dims(l)
+        planes = {"so": 14, "ci": 26}.get(which, 1)
+        shape = (planes, nz + 2, ny + 2, nx + 2)
+        ptr = self.L.o3_level_array(self.h, l, {"so": 0, "x": 1, "b": 2, "res": 3, "sor": 4, "ci": 6}[which])
+        a = np.ctypeslib.as_array(ptr, shape=(int(np.prod(shape)),)).copy().reshape(shape)
+        return a if planes > 1 else a[0]
+
+    def solve(self, b, x=None):
+        b = np.ascontiguousarray(b, dtype=np.float64)
+        x = np.zeros_like(b) if x is None else x
+        hist = np.zeros(max(self.s.maxiter, 1))
+        n = self.L.o3_solve(self.h, _p(b), _p(x), _p(hist), len(hist))
+        return x, hist[:n].copy()

@@ -82,7 +82,7 @@ def _loss_and_grad(theta_np, f_np, uobs, precision, tol=1e-12):
     u = solve_log_diffusion(theta, f, tol=tol, maxiter=80, precision=precision)
     loss = 0.5 * ((u - uobs) ** 2).sum()
     loss.backward()
-    return float(loss), theta.grad.cpu().numpy()
+    return float(loss.detach()), theta.grad.cpu().numpy()
 
 
 @pytest.mark.parametrize("precision", ["fp32-ir", "fp64"])

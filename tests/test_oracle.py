@@ -169,3 +169,62 @@ def test_line_smoothers_converge_like_reference_tests(oracle):
         x, h = s.solve(b)
         r = oracle.residual(np.ascontiguousarray(so), x, b)
         assert np.linalg.norm(r) < 1e-8
+
+
+# ------------------------------------------------------------------------- 3D
+@pytest.mark.parametrize("n", [7, 8, 9])
+def test_3d_galerkin_and_restriction_are_ptap_and_pt(oracle, n):
+    rng = np.random.default_rng(n)
+    k = np.exp(rng.normal(size=(n + 1,) * 3))
+    so = G.fe3_hetero(k)
+    nc = (n - 1) // 2 + 1
+    ci = oracle.setup_interp3(so, nc, nc, nc)
+    soc = oracle.galerkin3(so, ci)
+    A = G.stencil3_to_csr(so).toarray()
+    Pm = np.zeros((n ** 3, nc ** 3))
+    for kc in range(nc):
+        for jc in range(nc):
+            for ic in range(nc):
+                xc = np.zeros((nc + 2,) * 3)
+                xc[kc + 1, jc + 1, ic + 1] = 1
+                xf = np.zeros((n + 2,) * 3)
+                oracle.interp_add3(ci, xc, np.zeros_like(xf), so, xf)
+                Pm[:, (kc * nc + jc) * nc + ic] = xf[1:-1, 1:-1, 1:-1].ravel()
+    Ac = Pm.T @ A @ Pm
+    assert np.abs(Ac - G.stencil3_to_csr(soc).toarray()).max() <= 1e-14 * np.abs(Ac).max()
+    r = np.zeros((n + 2,) * 3)
+    r[1:-1, 1:-1, 1:-1] = rng.random((n, n, n))
+    bc = oracle.restrict3(ci, r)
+    np.testing.assert_allclose(bc[1:-1, 1:-1, 1:-1].ravel(), Pm.T @ r[1:-1, 1:-1, 1:-1].ravel(), rtol=1e-13, atol=1e-14)
+    # interpolation reproduces constants away from the boundary on a constant-coefficient operator
+    soc1 = G.fe3_hetero(np.ones((n + 1,) * 3))
+    ci1 = oracle.setup_interp3(soc1, nc, nc, nc)
+    xc = np.zeros((nc + 2,) * 3)
+    xc[1:-1, 1:-1, 1:-1] = 1.0
+    xf = np.zeros((n + 2,) * 3)
+    oracle.interp_add3(ci1, xc, np.zeros_like(xf), soc1, xf)
+    assert abs(xf[n // 2, n // 2, n // 2] - 1.0) < 1e-12
+
+
+def test_3d_residual_matches_assembled_matrix(oracle):
+    n = 9
+    rng = np.random.default_rng(3)
+    so = G.fe3_hetero(np.exp(rng.normal(size=(n + 1,) * 3)))
+    A = G.stencil3_to_csr(so)
+    assert abs(A - A.T).max() == 0
+    x = np.zeros((n + 2,) * 3); x[1:-1, 1:-1, 1:-1] = rng.random((n, n, n))
+    b = np.zeros_like(x); b[1:-1, 1:-1, 1:-1] = rng.random((n, n, n))
+    r = oracle.residual3(so, x, b)
+    np.testing.assert_allclose(r[1:-1, 1:-1, 1:-1].ravel(), b[1:-1, 1:-1, 1:-1].ravel() - A @ x[1:-1, 1:-1, 1:-1].ravel(),
+                               atol=1e-14)
+
+
+def test_3d_boxmg_converges(oracle):
+    n = 15
+    rng = np.random.default_rng(4)
+    so = G.fe3_hetero(np.exp(1.5 * rng.normal(size=(n + 1,) * 3)))
+    b = np.zeros((n + 2,) * 3); b[1:-1, 1:-1, 1:-1] = rng.uniform(-1, 1, (n, n, n)) / (n + 1) ** 3
+    s = oracle.Solver3(so, maxiter=20, tol=1e-10)
+    x, h = s.solve(b)
+    assert h[-1] < 1e-10 and len(h) <= 12
+    assert oracle.num_levels(15, 15, 3) == 3
