@@ -130,3 +130,87 @@ class Solver2D:
 
     def vcycle_device(self, b_ptr, x_ptr, pitch):
         _lib.check(self.lib.cdr_gpu_solver_vcycle_device(self.h, ctypes.c_void_p(b_ptr), ctypes.c_void_p(x_ptr), pitch))
+
+
+class Solver3D:
+    """``cdr3::solver`` (include/cedar/3d/solver.h) on the GPU: 27-point fine
+    operator in Cedar's layout (14, nz+2, ny+2, nx+2), point relaxation."""
+
+    def __init__(self, so, conf=None, stream=0):
+        self.lib = _lib.load()
+        so = np.ascontiguousarray(so, dtype=np.float64)
+        if so.ndim != 4 or so.shape[0] != 14:
+            raise ValueError("stencil must have shape (14, nz+2, ny+2, nx+2)")
+        self.nz, self.ny, self.nx = so.shape[1] - 2, so.shape[2] - 2, so.shape[3] - 2
+        self.settings = conf if isinstance(conf, MLSettings) else MLSettings(conf)
+        if self.settings.relaxation != "point":
+            raise NotImplementedError("3D relaxation %r: only point relaxation runs on the GPU"
+                                      % self.settings.relaxation)
+        self._s = _settings(self.settings)
+        h = ctypes.c_void_p()
+        _lib.check(self.lib.cdr_gpu_solver3_create(ctypes.byref(self._s), so.ctypes.data, self.nx, self.ny, self.nz,
+                                                   ctypes.c_void_p(stream), ctypes.byref(h)))
+        self.h = h
+        self.history = np.zeros(0)
+        self.iters = 0
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.cdr_gpu_solver3_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def nlevels(self):
+        return self.lib.cdr_gpu_solver3_nlevels(self.h)
+
+    def timings(self):
+        a, b = ctypes.c_double(), ctypes.c_double()
+        _lib.check(self.lib.cdr_gpu_solver3_timings(self.h, ctypes.byref(a), ctypes.byref(b)))
+        return a.value, b.value
+
+    def level_info(self, level, which="so", fp32=False):
+        """(device pointer, nx, ny, nz, pitch) of a level array."""
+        p = ctypes.c_void_p()
+        vals = [ctypes.c_int() for _ in range(4)]
+        wid = PLANE_NAMES[which] + (16 if fp32 else 0) if which != "abd" else 100
+        _lib.check(self.lib.cdr_gpu_solver3_level(self.h, level, wid, ctypes.byref(p), *[ctypes.byref(v) for v in vals]))
+        return (p.value,) + tuple(v.value for v in vals)
+
+    def level_array(self, level, which="so", fp32=False):
+        """Host copy of a level array in Cedar's layout (planes, nz+2, ny+2, nx+2)."""
+        p, nx, ny, nz, pitch = self.level_info(level, which, fp32)
+        wid = PLANE_NAMES[which] + (16 if fp32 else 0)
+        planes = {"so": 14, "ci": 26}.get(which, 1)
+        dt = np.float32 if fp32 else np.float64
+        buf = np.zeros((planes, nz + 2, ny + 2, pitch), dtype=dt)
+        _lib.check(self.lib.cdr_gpu_solver3_level_get(self.h, level, wid, buf.ctypes.data, buf.nbytes))
+        out = np.ascontiguousarray(buf[..., :nx + 2])
+        return out if planes > 1 else out[0]
+
+    def solve(self, b, x=None):
+        """Solve A x = b from host arrays (Cedar layout (nz+2, ny+2, nx+2)); returns x."""
+        b = np.ascontiguousarray(b, dtype=np.float64)
+        if b.shape != (self.nz + 2, self.ny + 2, self.nx + 2):
+            raise ValueError("rhs shape %s does not match the grid" % (b.shape,))
+        x = np.zeros_like(b) if x is None else np.ascontiguousarray(x, dtype=np.float64).copy()
+        hist = np.zeros(max(self.settings.maxiter, 1))
+        it = ctypes.c_int()
+        _lib.check(self.lib.cdr_gpu_solver3_solve(self.h, b.ctypes.data, x.ctypes.data, ctypes.byref(it),
+                                                  hist.ctypes.data, len(hist)))
+        self.iters = it.value
+        self.history = hist[:it.value].copy()
+        return x
+
+    def solve_device(self, b_ptr, x_ptr, pitch):
+        hist = np.zeros(max(self.settings.maxiter, 1))
+        it = ctypes.c_int()
+        _lib.check(self.lib.cdr_gpu_solver3_solve_device(self.h, ctypes.c_void_p(b_ptr), ctypes.c_void_p(x_ptr),
+                                                         pitch, ctypes.byref(it), hist.ctypes.data, len(hist)))
+        self.iters = it.value
+        self.history = hist[:it.value].copy()

@@ -254,6 +254,81 @@ int cdr_gpu_solver_level_get(const cdr_gpu_solver *h, int level, int which, void
 /* Setup and solve timings of the last calls (ms, from CUDA events). */
 int cdr_gpu_solver_timings(const cdr_gpu_solver *h, double *setup_ms, double *solve_ms);
 
+/* ------------------------------------------------------------------------
+ * 3D kernels (27-point operators, 14 stencil planes in the order of
+ * include/cedar/3d/base_types.h: p pw ps b psw pnw bw bnw bn bne be bse bs bsw).
+ * A grid of nx*ny*nz interior points has (nx+2)*(ny+2)*(nz+2) entries per
+ * plane: rows of `pitch` elements (pitch >= nx+2), k-slices pitch*(ny+2)
+ * elements apart, planes pitch*(ny+2)*(nz+2) apart.  Interpolation weights: 26
+ * planes on the coarse grid (include/cedar/3d/prolong_op.h).
+ * ------------------------------------------------------------------------ */
+
+/* r = b - A x (BMG3_SymStd_residual via include/cedar/3d/residual.h:58); the
+ * optional norm is as in the 2D call (scratch of cdr_gpu_norm_scratch_bytes()). */
+int cdr_gpu_residual_3d_f64(const double *so, const double *x, const double *b, double *r, int nx, int ny, int nz,
+                            int pitch, double *norm_out, void *scratch, cudaStream_t stream);
+int cdr_gpu_residual_3d_f32(const float *so, const float *x, const float *b, float *r, int nx, int ny, int nz,
+                            int pitch, double *norm_out, void *scratch, cudaStream_t stream);
+/* sor = 1/c (BMG3_SymStd_SETUP_recip via include/cedar/3d/relax.h:62). */
+int cdr_gpu_setup_recip_3d_f64(const double *so, double *sor, int nx, int ny, int nz, int pitch,
+                               cudaStream_t stream);
+/* One 8-colour Gauss-Seidel sweep (BMG3_SymStd_relax_GS via include/cedar/3d/relax.h:96);
+ * updown CDR_DOWN runs the colours 8..1, CDR_UP 1..8. */
+int cdr_gpu_relax_point_3d_f64(const double *so, double *x, const double *b, const double *sor, int nx, int ny,
+                               int nz, int pitch, int updown, cudaStream_t stream);
+int cdr_gpu_relax_point_3d_f32(const float *so, float *x, const float *b, const float *sor, int nx, int ny,
+                               int nz, int pitch, int updown, cudaStream_t stream);
+/* b_coarse = P^T r_fine (BMG3_SymStd_restrict via src/3d/restrict.cc:29).  The
+ * coarse grid must be ((nxf-1)/2+1, (nyf-1)/2+1, (nzf-1)/2+1). */
+int cdr_gpu_restrict_3d_f64(const double *ci, const double *r_fine, double *b_coarse, int nxf, int nyf, int nzf,
+                            int pitch_f, int nxc, int nyc, int nzc, int pitch_c, cudaStream_t stream);
+/* x_fine += P x_coarse + r/c on fine-only points (BMG3_SymStd_interp_add via
+ * src/3d/interp.cc:41); so_fine is the fine operator (its p plane is read),
+ * res_fine the fine residual (not modified). */
+int cdr_gpu_interp_add_3d_f64(const double *ci, const double *x_coarse, const double *res_fine,
+                              const double *so_fine, double *x_fine, int nxf, int nyf, int nzf, int pitch_f,
+                              int nxc, int nyc, int nzc, int pitch_c, cudaStream_t stream);
+/* Operator-induced interpolation weights (BMG3_SymStd_SETUP_interp_OI via
+ * include/cedar/3d/interp.h:68), 27-point fine operator. */
+int cdr_gpu_setup_interp_3d_f64(const double *so_fine, double *ci, int nxf, int nyf, int nzf, int pitch_f,
+                                int nxc, int nyc, int nzc, int pitch_c, cudaStream_t stream);
+/* Galerkin coarse operator P^T A P, 14 planes (BMG3_SymStd_SETUP_ITLI27_ex via
+ * include/cedar/3d/coarsen.h:56). */
+int cdr_gpu_galerkin_3d_f64(const double *so_fine, const double *ci, double *so_coarse, int nxf, int nyf,
+                            int nzf, int pitch_f, int nxc, int nyc, int nzc, int pitch_c, cudaStream_t stream);
+/* Banded Cholesky of the coarsest operator (BMG3_SymStd_SETUP_cg_LU via
+ * include/cedar/3d/solve_cg.h:43): abd holds (nx*(ny+1)+2) * nx*ny*nz doubles;
+ * info (device int, may be null) receives the failing column or 0. */
+int cdr_gpu_setup_cg_3d_f64(const double *so, int nx, int ny, int nz, int pitch, double *abd, int *info,
+                            cudaStream_t stream);
+/* x = A^{-1} b with that factor (BMG3_SymStd_SOLVE_cg via src/3d/solve_cg.cc:28). */
+int cdr_gpu_solve_cg_3d_f64(const double *abd, double *x, const double *b, int nx, int ny, int nz, int pitch,
+                            cudaStream_t stream);
+
+/* ------------------------------------------------------------------------
+ * 3D multilevel solver (cdr3::solver, include/cedar/3d/solver.h): point
+ * relaxation, 27-point fine operator.  Same settings struct as 2D
+ * (relaxation must be CDR_RELAX_POINT; line_flags is ignored).
+ * ------------------------------------------------------------------------ */
+typedef struct cdr_gpu_solver3 cdr_gpu_solver3;
+
+/* Host fine operator in Cedar's layout (pitch nx+2, 14 planes). */
+int cdr_gpu_solver3_create(const cdr_gpu_settings *s, const double *so_host, int nx, int ny, int nz,
+                           cudaStream_t stream, cdr_gpu_solver3 **out);
+int cdr_gpu_solver3_destroy(cdr_gpu_solver3 *h);
+/* Host buffers of (nx+2)*(ny+2)*(nz+2) doubles; as cdr_gpu_solver_solve. */
+int cdr_gpu_solver3_solve(cdr_gpu_solver3 *h, const double *b_host, double *x_host, int *iters, double *hist,
+                          int maxhist);
+/* Device buffers of the given pitch (k-slices pitch*(ny+2) apart). */
+int cdr_gpu_solver3_solve_device(cdr_gpu_solver3 *h, const double *b_dev, double *x_dev, int pitch, int *iters,
+                                 double *hist, int maxhist);
+int cdr_gpu_solver3_nlevels(const cdr_gpu_solver3 *h);
+/* which: 0 so, 1 x, 2 b, 3 res, 4 sor, 6 ci (+16: FP32 copies), 100 coarse factor. */
+int cdr_gpu_solver3_level(const cdr_gpu_solver3 *h, int level, int which, void **ptr, int *nx, int *ny, int *nz,
+                          int *pitch);
+int cdr_gpu_solver3_level_get(const cdr_gpu_solver3 *h, int level, int which, void *host, size_t bytes);
+int cdr_gpu_solver3_timings(const cdr_gpu_solver3 *h, double *setup_ms, double *solve_ms);
+
 #ifdef __cplusplus
 }
 #endif
