@@ -310,6 +310,7 @@ def main():
     if rank == 0 and world == 1 and not args.no_extras:
         out["to_1e-10"] = to_1e10(args, stream)
         out["inverse_diffusion"] = inverse_batch()
+        out["hetero3d"] = hetero3_leg(stream)
         out["cpu_baseline"] = cpu_arm(args, so, b, it64, "config above")
         del out["cpu_baseline"]["setup_ms"], out["cpu_baseline"]["ms_per_cycle"]
     if rank == 0:
@@ -375,6 +376,57 @@ def inverse_batch(batch=16, n=1023):
                         "8 point sources, loss 0.5||u-u_obs||^2; forward FP32-cycle+FP64-IR to 1e-10, "
                         "backward adjoint solve + gradient kernel" % (batch, n + 1),
             "ms_forward_backward_batch": ms, "ms_per_problem": ms / batch}
+
+
+def hetero3_leg(stream, n=255):
+    """3D trilinear-FE diffusion on 256^3 cells (lognormal, correlation length
+    1/16, sigma 1.5, 16 boxes x1e3; b = U[-1,1] h^3), assembled on the device;
+    V(2,1) with 8-colour point Gauss-Seidel, FP64 and FP32-cycle + FP64
+    refinement, both to 1e-10."""
+    import torch
+    from cedar_b200 import _lib, problems as P
+    from cedar_b200.config import Config
+    from cedar_b200.solver import Solver3D
+    lib = _lib.load()
+    k = P.hetero3_coefficients(n)
+    b = P.hetero3_rhs(n)
+    pitch = ((n + 2 + 7) // 8) * 8
+    sh = stream.cuda_stream
+    dk = torch.from_numpy(k).cuda()
+    so = torch.empty((14, n + 2, n + 2, pitch), dtype=torch.float64, device="cuda")
+    _lib.check(lib.cdr_gpu_fe_assemble_3d_f64(ctypes.c_void_p(dk.data_ptr()), n + 1, (n + 1) ** 2,
+                                              ctypes.c_void_p(so.data_ptr()), n, n, n, pitch, ctypes.c_void_p(sh)))
+    bd = torch.zeros((n + 2, n + 2, pitch), dtype=torch.float64, device="cuda")
+    bd[..., :n + 2] = torch.from_numpy(b).cuda()
+    xd = torch.zeros_like(bd)
+    torch.cuda.synchronize()
+    del dk
+    res = {"workload": "3D trilinear FE, %d^3 cells, lognormal k (ell=1/16, sigma=1.5, seed 4) x 16 boxes 1e3 "
+                       "(seed 5), b=U[-1,1]h^3 (seed 6); V(2,1) 8-colour point GS; periodic-box field synthesis"
+                       % (n + 1), "n": n}
+    for prec in ("fp32-ir", "fp64"):
+        s = Solver3D(so.data_ptr(), Config({"solver": {"max-iter": 60, "tol": 1e-10}, "gpu": {"precision": prec}}),
+                     stream=sh, dims=(n, n, n), pitch=pitch)
+        setup_ms, _ = s.timings()
+        xd.zero_()
+        torch.cuda.synchronize()
+        s.solve_device(bd.data_ptr(), xd.data_ptr(), pitch)
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+        reps = 2
+        torch.cuda.synchronize()
+        with torch.cuda.stream(stream):
+            ev[0].record(stream)
+            for _ in range(reps):
+                xd.zero_()
+                s.solve_device(bd.data_ptr(), xd.data_ptr(), pitch)
+            ev[1].record(stream)
+        torch.cuda.synchronize()
+        ms = ev[0].elapsed_time(ev[1]) / reps
+        res[prec] = {"ms": ms, "iterations": int(s.iters), "final_rel_resid": float(s.history[-1]),
+                     "ms_per_cycle": ms / max(s.iters, 1), "setup_ms": setup_ms, "levels": s.nlevels}
+        s.close()
+    res["speedup"] = res["fp64"]["ms"] / res["fp32-ir"]["ms"]
+    return res
 
 
 def to_1e10(args, stream):

@@ -66,6 +66,7 @@ def load(path=LIB_PATH):
         "cdr_gpu_solver_resetup_device": (I, [P, P, I]),
         "cdr_gpu_fe_assemble_2d_f64": (I, [P, P, I, P, I, I, I, S]),
         "cdr_gpu_fe_grad_2d_f64": (I, [P, P, I, I, I, P, P, I, S]),
+        "cdr_gpu_fe_assemble_3d_f64": (I, [P, I, I, P, I, I, I, I, S]),
         "cdr_gpu_solver_solve": (I, [P, P, P, ctypes.POINTER(I), P, I]),
         "cdr_gpu_solver_solve_device": (I, [P, P, P, I, ctypes.POINTER(I), P, I]),
         "cdr_gpu_solver_vcycle_device": (I, [P, P, P, I]),
@@ -103,6 +104,7 @@ def load(path=LIB_PATH):
         "cdr_gpu_setup_cg_3d_f64": (I, [P, I, I, I, I, P, P, S]),
         "cdr_gpu_solve_cg_3d_f64": (I, [P, P, P, I, I, I, I, S]),
         "cdr_gpu_solver3_create": (I, [ctypes.POINTER(Settings), P, I, I, I, S, ctypes.POINTER(P)]),
+        "cdr_gpu_solver3_create_device": (I, [ctypes.POINTER(Settings), P, I, I, I, I, S, ctypes.POINTER(P)]),
         "cdr_gpu_solver3_destroy": (I, [P]),
         "cdr_gpu_solver3_solve": (I, [P, P, P, ctypes.POINTER(I), P, I]),
         "cdr_gpu_solver3_solve_device": (I, [P, P, P, I, ctypes.POINTER(I), P, I]),

@@ -134,3 +134,76 @@ int cdr_gpu_fe_grad_2d_f64(const double *u, const double *lam, int nx, int ny, i
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Trilinear (Q1) elements in 3D: -div(k grad u), k scalar per cell, cube cells
+// of side h = 1/(nx+1).  A_e = h * k * (Ex + Ey + Ez) with
+// Ex = K1 (x) M1 (x) M1, Ey = M1 (x) K1 (x) M1, Ez = M1 (x) M1 (x) K1, local node
+// l = a + 2b + 4c.  Entry of plane q at node s couples nodes s + oa and s + ob
+// (offsets per plane below, both nodes interior) and equals minus the sum over
+// the element pairs (l1, l2) with o(l2) - o(l1) = ob - oa, in the order
+// l1 = 0..7, l2 = 0..7, of k(cell (s + oa) - o(l1)) * A_e[l1, l2]; the p plane
+// is the plain sum at offset 0.  This fixed order makes the result identical to
+// the host assembler in the package's gallery.
+namespace cdrgpu {
+
+__device__ __forceinline__ double q1_ae3(double h, int l1, int l2)
+{
+	const int a1 = l1 & 1, b1 = (l1 >> 1) & 1, c1 = l1 >> 2, a2 = l2 & 1, b2 = (l2 >> 1) & 1, c2 = l2 >> 2;
+	const double ex = q1_k1(a1, a2) * q1_m1(b1, b2) * q1_m1(c1, c2);
+	const double ey = q1_m1(a1, a2) * q1_k1(b1, b2) * q1_m1(c1, c2);
+	const double ez = q1_m1(a1, a2) * q1_m1(b1, b2) * q1_k1(c1, c2);
+	return h * (ex + ey + ez);
+}
+
+// (oa, ob) of the 14 planes p pw ps b psw pnw bw bnw bn bne be bse bs bsw, as (x, y, z)
+__constant__ signed char c_planes3[14][2][3] = {
+    {{0, 0, 0}, {0, 0, 0}},    {{0, 0, 0}, {-1, 0, 0}},    {{0, 0, 0}, {0, -1, 0}},   {{0, 0, 0}, {0, 0, -1}},
+    {{0, 0, 0}, {-1, -1, 0}},  {{0, -1, 0}, {-1, 0, 0}},   {{0, 0, 0}, {-1, 0, -1}},  {{0, -1, 0}, {-1, 0, -1}},
+    {{0, -1, 0}, {0, 0, -1}},  {{-1, -1, 0}, {0, 0, -1}},  {{-1, 0, 0}, {0, 0, -1}},  {{-1, 0, 0}, {0, -1, -1}},
+    {{0, 0, 0}, {0, -1, -1}},  {{0, 0, 0}, {-1, -1, -1}}};
+
+__global__ void k_fe_assemble3(const double *__restrict__ kc, int cp, int cs, double *__restrict__ so, int nx, int ny,
+                               int nz, int pitch)
+{
+	const int i = blockIdx.x * TX + threadIdx.x + 1, j = blockIdx.y * TY + threadIdx.y + 1, k = blockIdx.z + 1;
+	if (i > nx || j > ny) return;
+	const double h = 1.0 / (nx + 1);
+	const size_t slice = (size_t)pitch * (ny + 2), plane = slice * (nz + 2);
+	const size_t at = (size_t)k * slice + (size_t)j * pitch + i;
+	for (int q = 0; q < 14; ++q) {
+		const int ax = i + c_planes3[q][0][0], ay = j + c_planes3[q][0][1], az = k + c_planes3[q][0][2];
+		const int bx = i + c_planes3[q][1][0], by = j + c_planes3[q][1][1], bz = k + c_planes3[q][1][2];
+		if (ax < 1 || ay < 1 || az < 1 || bx < 1 || by < 1 || bz < 1) continue;  // upper bounds hold for s interior
+		const int dx = bx - ax, dy = by - ay, dz = bz - az;
+		double acc = 0.0;
+		for (int l1 = 0; l1 < 8; ++l1)
+			for (int l2 = 0; l2 < 8; ++l2) {
+				if (((l2 & 1) - (l1 & 1)) != dx || (((l2 >> 1) & 1) - ((l1 >> 1) & 1)) != dy || ((l2 >> 2) - (l1 >> 2)) != dz)
+					continue;
+				const int ci = ax - (l1 & 1), cj = ay - ((l1 >> 1) & 1), ck = az - (l1 >> 2);
+				acc = acc + kc[(size_t)ck * cs + (size_t)cj * cp + ci] * q1_ae3(h, l1, l2);
+			}
+		so[(size_t)q * plane + at] = q == 0 ? acc : -acc;
+	}
+}
+
+}  // namespace cdrgpu
+
+extern "C" int cdr_gpu_fe_assemble_3d_f64(const double *k, int cell_pitch, int cell_slice, double *so, int nx, int ny,
+                                          int nz, int pitch, cudaStream_t stream)
+{
+	if (!k || !so) { set_error(CDR_ERR_ARG, "null pointer"); return CDR_ERR_ARG; }
+	if (nx < 1 || ny < 1 || nz < 1 || pitch < nx + 2 || cell_pitch < nx + 1 ||
+	    (size_t)cell_slice < (size_t)cell_pitch * (ny + 1)) {
+		set_error(CDR_ERR_DIM, "bad grid nx=%d ny=%d nz=%d pitch=%d cell_pitch=%d cell_slice=%d", nx, ny, nz, pitch,
+		          cell_pitch, cell_slice);
+		return CDR_ERR_DIM;
+	}
+	const size_t plane = (size_t)pitch * (ny + 2) * (nz + 2);
+	CDR_CUDA_TRY(cudaMemsetAsync(so, 0, sizeof(double) * plane * 14, stream));
+	k_fe_assemble3<<<dim3(ceil_div(nx, TX), ceil_div(ny, TY), nz), dim3(TX, TY), 0, stream>>>(k, cell_pitch, cell_slice,
+	                                                                                         so, nx, ny, nz, pitch);
+	CDR_LAUNCH_CHECK();
+	return CDR_OK;
+}

@@ -186,7 +186,7 @@ static int num_levels3(int nx, int ny, int nz, int min_coarse)
 	return ng;
 }
 
-static int create3(cdr_gpu_solver3 *h, const double *so_host, int nx, int ny, int nz)
+static int create3(cdr_gpu_solver3 *h, const double *so_src, int src_pitch, cudaMemcpyKind kind, int nx, int ny, int nz)
 {
 	const cdr_gpu_settings &s = h->s;
 	int nl = num_levels3(nx, ny, nz, s.min_coarse);
@@ -240,11 +240,10 @@ static int create3(cdr_gpu_solver3 *h, const double *so_host, int nx, int ny, in
 		CDR_TRY(h->alloc(&h->x64[1], h->lv[0].d.plane()));
 	}
 	CDR_CUDA_TRY(cudaMallocHost(&h->h_norm, 4 * sizeof(double)));
-	// host fine operator (pitch nx+2) -> device pitch, one plane-slice row block at a time
+	// fine operator (source pitch) -> device pitch: every row of every k-slice and plane
 	Level3 &F = h->lv[0];
-	CDR_CUDA_TRY(cudaMemcpy2DAsync(F.so, F.d.pitch * sizeof(double), so_host, (nx + 2) * sizeof(double),
-	                               (nx + 2) * sizeof(double), (size_t)(ny + 2) * (nz + 2) * 14, cudaMemcpyHostToDevice,
-	                               h->st));
+	CDR_CUDA_TRY(cudaMemcpy2DAsync(F.so, F.d.pitch * sizeof(double), so_src, src_pitch * sizeof(double),
+	                               (nx + 2) * sizeof(double), (size_t)(ny + 2) * (nz + 2) * 14, kind, h->st));
 	CDR_CUDA_TRY(cudaEventRecord(h->ev0, h->st));
 	CDR_TRY(h->setup());
 	CDR_CUDA_TRY(cudaEventRecord(h->ev1, h->st));
@@ -322,10 +321,10 @@ int cdr_gpu_solver3_destroy(cdr_gpu_solver3 *h)
 	return CDR_OK;
 }
 
-int cdr_gpu_solver3_create(const cdr_gpu_settings *s, const double *so_host, int nx, int ny, int nz,
-                           cudaStream_t stream, cdr_gpu_solver3 **out)
+static int create3_any(const cdr_gpu_settings *s, const double *so_src, int src_pitch, cudaMemcpyKind kind, int nx,
+                       int ny, int nz, cudaStream_t stream, cdr_gpu_solver3 **out)
 {
-	if (!s || !so_host || !out) { set_error(CDR_ERR_ARG, "null argument"); return CDR_ERR_ARG; }
+	if (!s || !so_src || !out) { set_error(CDR_ERR_ARG, "null argument"); return CDR_ERR_ARG; }
 	*out = nullptr;
 	if (nx < 1 || ny < 1 || nz < 1) { set_error(CDR_ERR_DIM, "bad grid %dx%dx%d", nx, ny, nz); return CDR_ERR_DIM; }
 	if (s->relaxation != CDR_RELAX_POINT) {
@@ -349,13 +348,26 @@ int cdr_gpu_solver3_create(const cdr_gpu_settings *s, const double *so_host, int
 	}
 	cudaEventCreate(&h->ev0);
 	cudaEventCreate(&h->ev1);
-	int rc = create3(h, so_host, nx, ny, nz);
+	int rc = create3(h, so_src, src_pitch, kind, nx, ny, nz);
 	if (rc != CDR_OK) {
 		cdr_gpu_solver3_destroy(h);
 		return rc;
 	}
 	*out = h;
 	return CDR_OK;
+}
+
+int cdr_gpu_solver3_create(const cdr_gpu_settings *s, const double *so_host, int nx, int ny, int nz,
+                           cudaStream_t stream, cdr_gpu_solver3 **out)
+{
+	return create3_any(s, so_host, nx + 2, cudaMemcpyHostToDevice, nx, ny, nz, stream, out);
+}
+
+int cdr_gpu_solver3_create_device(const cdr_gpu_settings *s, const double *so_dev, int nx, int ny, int nz, int pitch,
+                                  cudaStream_t stream, cdr_gpu_solver3 **out)
+{
+	if (pitch < nx + 2) { set_error(CDR_ERR_DIM, "pitch %d < nx+2", pitch); return CDR_ERR_DIM; }
+	return create3_any(s, so_dev, pitch, cudaMemcpyDeviceToDevice, nx, ny, nz, stream, out);
 }
 
 static int copy3(void *dst, int dpitch, const void *src, int spitch, int nx, int ny, int nz, cudaMemcpyKind kind,

@@ -9,6 +9,9 @@ No dataset is involved: every input is generated here from numpy
   correlation length ell, standard deviation sigma), optional axis-aligned
   rectangular inclusions with a contrast factor, optional anisotropy
   (ky = eps * kx in cells whose centre has y > 0.5); b = U[0,1] h^2.
+* ``hetero3_coefficients(n)`` / ``hetero3_rhs(n)``  3D lognormal cell coefficient
+  (Gaussian field, correlation length 1/16, sigma 1.5, periodic synthesis box)
+  with 16 boxes of contrast 1e3; b = U[-1,1] h^3.
 """
 import math
 
@@ -116,3 +119,57 @@ def fd_cells(n, count=32, seed=11):
     """Seeded cell indices (cj, ci) for finite-difference checks."""
     rng = np.random.default_rng(seed)
     return rng.integers(0, n + 1, size=(count, 2))
+
+
+def gaussian_field3(nc, ell, sigma, seed):
+    """Stationary Gaussian random field on the cell centres of the unit cube,
+    nc cells per axis: FFT synthesis on the periodic box of the domain (white
+    noise times the square root of the spectral density of the Gaussian
+    covariance exp(-r^2 / (2 ell^2))), scaled to standard deviation sigma.
+    Returns (nc, nc, nc) indexed (z, y, x)."""
+    rng = np.random.default_rng(seed)
+    h = 1.0 / nc
+    kx = np.fft.fftfreq(nc, d=h) * 2 * math.pi
+    kz = np.fft.rfftfreq(nc, d=h) * 2 * math.pi
+    K2 = kx[:, None, None] ** 2 + kx[None, :, None] ** 2 + kz[None, None, :] ** 2
+    spec = np.sqrt(np.exp(-0.5 * ell * ell * K2))
+    noise = rng.standard_normal((nc, nc, nc))
+    fld = np.fft.irfftn(np.fft.rfftn(noise) * spec, s=(nc, nc, nc))
+    fld -= fld.mean()
+    std = fld.std()
+    if std > 0:
+        fld *= sigma / std
+    return np.ascontiguousarray(fld)
+
+
+def inclusions3(nc, count, contrast, seed, smin=1.0 / 32, smax=1.0 / 8):
+    """Multiplicative factor per cell: ``contrast`` inside ``count`` random boxes."""
+    rng = np.random.default_rng(seed)
+    fac = np.ones((nc, nc, nc))
+    c = (np.arange(nc) + 0.5) / nc
+    for _ in range(count):
+        w = rng.uniform(smin, smax, size=3)
+        o = rng.uniform(0, 1 - w)
+        mx = (c >= o[0]) & (c < o[0] + w[0])
+        my = (c >= o[1]) & (c < o[1] + w[1])
+        mz = (c >= o[2]) & (c < o[2] + w[2])
+        fac[np.ix_(mz, my, mx)] = contrast
+    return fac
+
+
+def hetero3_coefficients(n, ell=1.0 / 16, sigma=1.5, n_incl=16, contrast=1e3, seed_field=4, seed_incl=5):
+    """Cell coefficient k = exp(g) * inclusions on an (n+1)^3 cell mesh, (z, y, x)."""
+    nc = n + 1
+    k = np.exp(gaussian_field3(nc, ell, sigma, seed_field))
+    if n_incl:
+        k *= inclusions3(nc, n_incl, contrast, seed_incl)
+    return k
+
+
+def hetero3_rhs(n, seed=6):
+    """b = U[-1, 1] h^3 on the n^3 interior nodes (ghost-inclusive array)."""
+    h = 1.0 / (n + 1)
+    rng = np.random.default_rng(seed)
+    b = np.zeros((n + 2, n + 2, n + 2))
+    b[1:-1, 1:-1, 1:-1] = rng.uniform(-1.0, 1.0, size=(n, n, n)) * h ** 3
+    return b

@@ -136,20 +136,28 @@ class Solver3D:
     """``cdr3::solver`` (include/cedar/3d/solver.h) on the GPU: 27-point fine
     operator in Cedar's layout (14, nz+2, ny+2, nx+2), point relaxation."""
 
-    def __init__(self, so, conf=None, stream=0):
+    def __init__(self, so, conf=None, stream=0, dims=None, pitch=None):
+        """so: host array (14, nz+2, ny+2, nx+2), or a device pointer (int) with
+        dims = (nx, ny, nz) and the row pitch of the device array."""
         self.lib = _lib.load()
-        so = np.ascontiguousarray(so, dtype=np.float64)
-        if so.ndim != 4 or so.shape[0] != 14:
-            raise ValueError("stencil must have shape (14, nz+2, ny+2, nx+2)")
-        self.nz, self.ny, self.nx = so.shape[1] - 2, so.shape[2] - 2, so.shape[3] - 2
         self.settings = conf if isinstance(conf, MLSettings) else MLSettings(conf)
         if self.settings.relaxation != "point":
             raise NotImplementedError("3D relaxation %r: only point relaxation runs on the GPU"
                                       % self.settings.relaxation)
         self._s = _settings(self.settings)
         h = ctypes.c_void_p()
-        _lib.check(self.lib.cdr_gpu_solver3_create(ctypes.byref(self._s), so.ctypes.data, self.nx, self.ny, self.nz,
-                                                   ctypes.c_void_p(stream), ctypes.byref(h)))
+        if dims is not None:
+            self.nx, self.ny, self.nz = dims
+            _lib.check(self.lib.cdr_gpu_solver3_create_device(ctypes.byref(self._s), ctypes.c_void_p(so), self.nx,
+                                                              self.ny, self.nz, pitch, ctypes.c_void_p(stream),
+                                                              ctypes.byref(h)))
+        else:
+            so = np.ascontiguousarray(so, dtype=np.float64)
+            if so.ndim != 4 or so.shape[0] != 14:
+                raise ValueError("stencil must have shape (14, nz+2, ny+2, nx+2)")
+            self.nz, self.ny, self.nx = so.shape[1] - 2, so.shape[2] - 2, so.shape[3] - 2
+            _lib.check(self.lib.cdr_gpu_solver3_create(ctypes.byref(self._s), so.ctypes.data, self.nx, self.ny,
+                                                       self.nz, ctypes.c_void_p(stream), ctypes.byref(h)))
         self.h = h
         self.history = np.zeros(0)
         self.iters = 0

@@ -194,6 +194,13 @@ int cdr_gpu_fe_assemble_2d_f64(const double *kx, const double *ky, int cell_pitc
 int cdr_gpu_fe_grad_2d_f64(const double *u, const double *lam, int nx, int ny, int pitch, double *gkx,
                            double *gky, int cell_pitch, cudaStream_t stream);
 
+/* Trilinear elements in 3D: 27-point operator (14 planes) of -div(k grad u), k
+ * scalar per cell of an (nz+1) x (ny+1) x (nx+1) cell array (row pitch
+ * cell_pitch >= nx+1, k-slices cell_slice >= cell_pitch*(ny+1) apart), cube
+ * cells of side 1/(nx+1), Dirichlet zero boundary. */
+int cdr_gpu_fe_assemble_3d_f64(const double *k, int cell_pitch, int cell_slice, double *so, int nx, int ny, int nz,
+                               int pitch, cudaStream_t stream);
+
 /* ------------------------------------------------------------------------
  * 2D multilevel solver: setup in create (multilevel::setup,
  * include/cedar/multilevel.h:243-265), solve (multilevel::solve, :278-298),
@@ -315,6 +322,9 @@ typedef struct cdr_gpu_solver3 cdr_gpu_solver3;
 /* Host fine operator in Cedar's layout (pitch nx+2, 14 planes). */
 int cdr_gpu_solver3_create(const cdr_gpu_settings *s, const double *so_host, int nx, int ny, int nz,
                            cudaStream_t stream, cdr_gpu_solver3 **out);
+/* Same from a DEVICE fine operator of the given pitch. */
+int cdr_gpu_solver3_create_device(const cdr_gpu_settings *s, const double *so_dev, int nx, int ny, int nz, int pitch,
+                                  cudaStream_t stream, cdr_gpu_solver3 **out);
 int cdr_gpu_solver3_destroy(cdr_gpu_solver3 *h);
 /* Host buffers of (nx+2)*(ny+2)*(nz+2) doubles; as cdr_gpu_solver_solve. */
 int cdr_gpu_solver3_solve(cdr_gpu_solver3 *h, const double *b_host, double *x_host, int *iters, double *hist,

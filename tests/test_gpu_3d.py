@@ -199,3 +199,26 @@ def test_solver3_rejects_unsupported(lib):
     h = ctypes.c_void_p()
     rc = lib.cdr_gpu_solver3_create(ctypes.byref(s), so.ctypes.data, 7, 7, 7, None, ctypes.byref(h))
     assert rc == 7  # CDR_ERR_UNSUPPORTED
+
+
+@pytest.mark.parametrize("n", [(7, 7, 7), (12, 9, 10), (31, 31, 31)])
+def test_fe_assemble3_bitwise_and_device_create(lib, oracle, n):
+    import torch
+    from cedar_b200.solver import Solver3D
+    nx, ny, nz = n
+    rng = np.random.default_rng(nx * ny * nz)
+    k = np.exp(1.5 * rng.standard_normal((nz + 1, ny + 1, nx + 1)))
+    so_ref = G.fe3_hetero(k)
+    p = pitch_of(nx, 7)
+    dk = torch.from_numpy(k).cuda()
+    dso = torch.full((14, nz + 2, ny + 2, p), 7.0, dtype=torch.float64, device="cuda")
+    _lib.check(lib.cdr_gpu_fe_assemble_3d_f64(ptr(dk), nx + 1, (nx + 1) * (ny + 1), ptr(dso), nx, ny, nz, p,
+                                              stream()))
+    assert np.array_equal(unpad(dso, nx), so_ref)
+    if nx == ny == nz:
+        b = _rhs3(nx, ny, nz, seed=15)
+        conf = Config({"solver": {"max-iter": 30, "tol": 1e-10}})
+        s = Solver3D(dso.data_ptr(), conf, stream=0, dims=(nx, ny, nz), pitch=p)
+        x = s.solve(b)
+        x_ref, h_ref = oracle.Solver3(so_ref, maxiter=30, tol=1e-10).solve(b)
+        assert np.array_equal(x, x_ref)
