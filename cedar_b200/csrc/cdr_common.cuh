@@ -23,10 +23,19 @@ enum : int { IL = 0, IR = 1, IA = 2, IB = 3, ISW = 4, INW = 5, INE = 6, ISE = 7 
 struct Dims2 {
 	int nx, ny;     // interior points
 	int pitch;      // elements per row (>= nx + 2)
+	// Batches of independent problems of this size: a launch covers nb of them
+	// (grid z); entry z of the batch is problem z*bstep of the arrays, whose
+	// problems lie back to back (an array of P planes holds P*plane() elements
+	// per problem).  A single problem has nb = bstep = 1.
+	int nb = 1, bstep = 1;
 	__host__ __device__ int ii() const { return nx + 2; }
 	__host__ __device__ int jj() const { return ny + 2; }
 	__host__ __device__ size_t plane() const { return (size_t)pitch * (ny + 2); }
 	__host__ __device__ size_t at(int i, int j) const { return (size_t)j * pitch + i; }
+#ifdef __CUDACC__
+	// element offset of this CTA's problem in an array of `per` elements per problem
+	__device__ __forceinline__ size_t bofs(size_t per) const { return (size_t)blockIdx.z * (size_t)bstep * per; }
+#endif
 };
 
 // Counts kernel launches issued by this library (graph replays add the

@@ -29,8 +29,15 @@ constexpr int LT = 256;  // threads per CTA
 // BMG2_SymStd_SETUP_lines_{x,y} + DPTTRF: per line d = c, e = -w (x) or -s (y),
 // then e(i) <- e(i)/d(i-1), d(i) <- d(i) - e(i)*e_old(i).  Always FP64; TS is
 // the storage type of the factors.
+// Per-problem size of the factor array of one direction (2 planes; y-line
+// factors transposed, planes tpitch*(nx+2) apart).
+__host__ __device__ __forceinline__ size_t line_factor_size(Dims2 d, int tpitch, int dir)
+{
+	return dir == CDR_DIR_X ? 2 * d.plane() : 2 * (size_t)tpitch * (d.nx + 2);
+}
+
 template <typename TS, int DIR>
-__global__ void k_lines_setup(const double *__restrict__ so, TS *__restrict__ sor, Dims2 d, int tpitch,
+__global__ void k_lines_setup(const double *__restrict__ so, int ns, TS *__restrict__ sor, Dims2 d, int tpitch,
                               int *__restrict__ info)
 {
 	const int line = blockIdx.x * blockDim.x + threadIdx.x + 1;
@@ -38,6 +45,8 @@ __global__ void k_lines_setup(const double *__restrict__ so, TS *__restrict__ so
 	const int n = DIR == CDR_DIR_X ? d.nx : d.ny;
 	if (line > nl) return;
 	const size_t ps = d.plane();
+	so += d.bofs(ns * ps);
+	sor += d.bofs(line_factor_size(d, tpitch, DIR));
 	const double *c = so, *off = so + (DIR == CDR_DIR_X ? 1 : 2) * ps;
 	// element at line position p (1..n): grid offset and factor offset
 	auto g = [&](int p) -> size_t { return DIR == CDR_DIR_X ? d.at(p, line) : d.at(line, p); };
@@ -63,14 +72,14 @@ __global__ void k_lines_setup(const double *__restrict__ so, TS *__restrict__ so
 template <typename TS>
 int setup_lines_2d(const double *so, int nstencil, TS *sor, Dims2 d, int tpitch, int dir, int *info, cudaStream_t st)
 {
-	(void)nstencil;
 	if (dir == CDR_DIR_Y && tpitch < d.ny + 2) {
 		set_error(CDR_ERR_DIM, "y-line factor pitch %d < ny+2 = %d", tpitch, d.ny + 2);
 		return CDR_ERR_DIM;
 	}
 	const int nl = dir == CDR_DIR_X ? d.ny : d.nx;
-	if (dir == CDR_DIR_X) k_lines_setup<TS, CDR_DIR_X><<<ceil_div(nl, 128), 128, 0, st>>>(so, sor, d, tpitch, info);
-	else k_lines_setup<TS, CDR_DIR_Y><<<ceil_div(nl, 128), 128, 0, st>>>(so, sor, d, tpitch, info);
+	const dim3 grd(ceil_div(nl, 128), 1, d.nb);
+	if (dir == CDR_DIR_X) k_lines_setup<TS, CDR_DIR_X><<<grd, 128, 0, st>>>(so, nstencil, sor, d, tpitch, info);
+	else k_lines_setup<TS, CDR_DIR_Y><<<grd, 128, 0, st>>>(so, nstencil, sor, d, tpitch, info);
 	CDR_LAUNCH_CHECK();
 	return CDR_OK;
 }
@@ -135,6 +144,10 @@ __global__ void __launch_bounds__(LT) k_lines(const T *__restrict__ so, T *__res
 	T *buf = sB + LT;
 	const size_t ps = d.plane();
 	const int p = d.pitch;
+	so += d.bofs(NS * ps);
+	q += d.bofs(ps);
+	qf += d.bofs(ps);
+	sor += d.bofs(line_factor_size(d, tpitch, DIR));
 	const int n = DIR == CDR_DIR_X ? d.nx : d.ny;     // line length
 	const int nl = DIR == CDR_DIR_X ? d.ny : d.nx;    // lines in the grid
 	const int l0 = blockIdx.x * G;                    // first line (of this colour) of the CTA
@@ -351,6 +364,10 @@ __global__ void __launch_bounds__(DIR == CDR_DIR_X ? FAST_BLOCK_X : FAST_BLOCK_Y
 	const bool has = active && p0 <= n;
 	const size_t ps = d.plane();
 	const int P = d.pitch;
+	so += d.bofs(NS * ps);
+	q += d.bofs(ps);
+	qf += d.bofs(ps);
+	sor += d.bofs(line_factor_size(d, tpitch, DIR));
 	const T *D = DIR == CDR_DIR_X ? sor + (size_t)lc * P : sor + (size_t)lc * tpitch;
 	const T *E = DIR == CDR_DIR_X ? sor + ps + (size_t)lc * P : sor + (size_t)tpitch * (d.nx + 2) + (size_t)lc * tpitch;
 
@@ -572,12 +589,13 @@ static int launch_lines(const T *so, T *x, const T *b, const T *sor, Dims2 d, in
 		if constexpr (DIR == CDR_DIR_Y && sizeof(T) == 4) {
 			if (K == 16) {
 				k_lines_fast<T, NS, DIR, 16>
-				    <<<ceil_div(nlines, G), block, 0, st>>>(so, x, b, sor, d, tpitch, first, tpl_log2);
+				    <<<dim3(ceil_div(nlines, G), 1, d.nb), block, 0, st>>>(so, x, b, sor, d, tpitch, first, tpl_log2);
 				CDR_LAUNCH_CHECK();
 				return CDR_OK;
 			}
 		}
-		k_lines_fast<T, NS, DIR, 8><<<ceil_div(nlines, G), block, 0, st>>>(so, x, b, sor, d, tpitch, first, tpl_log2);
+		k_lines_fast<T, NS, DIR, 8>
+		    <<<dim3(ceil_div(nlines, G), 1, d.nb), block, 0, st>>>(so, x, b, sor, d, tpitch, first, tpl_log2);
 		CDR_LAUNCH_CHECK();
 		return CDR_OK;
 	}
@@ -588,8 +606,9 @@ static int launch_lines(const T *so, T *x, const T *b, const T *sor, Dims2 d, in
 		return CDR_ERR_DIM;
 	}
 	CDR_TRY(lines_prepare());
-	if (exact) k_lines<T, NS, DIR, true><<<ceil_div(nlines, G), LT, smem, st>>>(so, x, b, sor, d, tpitch, first, G);
-	else k_lines<T, NS, DIR, false><<<ceil_div(nlines, G), LT, smem, st>>>(so, x, b, sor, d, tpitch, first, G);
+	const dim3 grd(ceil_div(nlines, G), 1, d.nb);
+	if (exact) k_lines<T, NS, DIR, true><<<grd, LT, smem, st>>>(so, x, b, sor, d, tpitch, first, G);
+	else k_lines<T, NS, DIR, false><<<grd, LT, smem, st>>>(so, x, b, sor, d, tpitch, first, G);
 	CDR_LAUNCH_CHECK();
 	return CDR_OK;
 }

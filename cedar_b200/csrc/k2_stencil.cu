@@ -11,6 +11,17 @@ namespace cdrgpu {
 
 constexpr int NORM_MAX_BLOCKS = 2048;
 
+// Blocks per problem of a residual with norm: all 2048 partial-sum slots for a
+// single problem, an equal share of them for each problem of a batch (the
+// tile -> block map, hence the summation order, is fixed for a given batch).
+int norm_blocks(Dims2 d)
+{
+	const int ntiles = ceil_div(d.nx, TX) * ceil_div(d.ny, TY);
+	int per = NORM_MAX_BLOCKS / (d.nb > 0 ? d.nb : 1);
+	if (per < 1) per = 1;
+	return ntiles < per ? ntiles : per;
+}
+
 // ------------------------------------------------------------------ residual
 // Grid-stride over 32x8 tiles; with NORM each block leaves the sum of r^2 over
 // its tiles in partial[blockIdx.x] (fixed tile->block map: deterministic).
@@ -23,6 +34,10 @@ __global__ void __launch_bounds__(TX *TY) k_residual(const T *__restrict__ so, c
 	const int tiles_x = (d.nx + TX - 1) / TX;
 	const int ntiles = tiles_x * ((d.ny + TY - 1) / TY);
 	const size_t ps = d.plane();
+	so += d.bofs(NS * ps);
+	q += d.bofs(ps);
+	qf += d.bofs(ps);
+	res += d.bofs(ps);
 	double acc = 0.0;
 	for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
 		int i = (t % tiles_x) * TX + threadIdx.x + 1;
@@ -36,13 +51,16 @@ __global__ void __launch_bounds__(TX *TY) k_residual(const T *__restrict__ so, c
 	}
 	if (NORM) {
 		double s = block_sum<TX * TY / 32>(acc, sh);
-		if (threadIdx.x == 0 && threadIdx.y == 0) partial[blockIdx.x] = s;
+		if (threadIdx.x == 0 && threadIdx.y == 0) partial[(size_t)blockIdx.z * gridDim.x + blockIdx.x] = s;
 	}
 }
 
+// one block per problem: out[b] = sqrt(sum of partial[b*n .. b*n+n))
 __global__ void __launch_bounds__(1024) k_norm_finish(const double *__restrict__ partial, int n, double *out)
 {
 	__shared__ double sh[32];
+	partial += (size_t)blockIdx.x * n;
+	out += blockIdx.x;
 	double v = 0;
 	for (int i = threadIdx.x; i < n; i += blockDim.x) v += partial[i];
 	for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
@@ -62,14 +80,14 @@ int residual_2d(const T *so, int nstencil, const T *x, const T *b, T *r, Dims2 d
 	const int ntiles = ceil_div(d.nx, TX) * ceil_div(d.ny, TY);
 	dim3 blk(TX, TY);
 	if (norm_out) {
-		int nb = ntiles < NORM_MAX_BLOCKS ? ntiles : NORM_MAX_BLOCKS;
-		if (nstencil == 5) k_residual<T, 5, true><<<nb, blk, 0, st>>>(so, x, b, r, d, partial);
-		else k_residual<T, 3, true><<<nb, blk, 0, st>>>(so, x, b, r, d, partial);
+		int nb = norm_blocks(d);
+		if (nstencil == 5) k_residual<T, 5, true><<<dim3(nb, 1, d.nb), blk, 0, st>>>(so, x, b, r, d, partial);
+		else k_residual<T, 3, true><<<dim3(nb, 1, d.nb), blk, 0, st>>>(so, x, b, r, d, partial);
 		CDR_LAUNCH_CHECK();
-		k_norm_finish<<<1, 1024, 0, st>>>(partial, nb, norm_out);
+		k_norm_finish<<<d.nb, 1024, 0, st>>>(partial, nb, norm_out);
 	} else {
-		if (nstencil == 5) k_residual<T, 5, false><<<ntiles, blk, 0, st>>>(so, x, b, r, d, nullptr);
-		else k_residual<T, 3, false><<<ntiles, blk, 0, st>>>(so, x, b, r, d, nullptr);
+		if (nstencil == 5) k_residual<T, 5, false><<<dim3(ntiles, 1, d.nb), blk, 0, st>>>(so, x, b, r, d, nullptr);
+		else k_residual<T, 3, false><<<dim3(ntiles, 1, d.nb), blk, 0, st>>>(so, x, b, r, d, nullptr);
 	}
 	CDR_LAUNCH_CHECK();
 	return CDR_OK;
@@ -82,21 +100,23 @@ template int residual_2d<float>(const float *, int, const float *, const float *
 // ------------------------------------------------------------ point smoother
 // BMG2_SymStd_SETUP_recip (src/2d/ftn/BMG2_SymStd_SETUP_recip.f90:63-67).
 template <typename T>
-__global__ void k_recip(const T *__restrict__ so, T *__restrict__ sor, Dims2 d)
+__global__ void k_recip(const T *__restrict__ so, int ns, T *__restrict__ sor, Dims2 d)
 {
+	so += d.bofs(ns * d.plane());
+	sor += d.bofs(2 * d.plane());
 	int i = blockIdx.x * TX + threadIdx.x + 1, j = blockIdx.y * TY + threadIdx.y + 1;
 	if (i <= d.nx && j <= d.ny) sor[d.at(i, j)] = T(1) / so[d.at(i, j)];
 }
 
 template <typename T>
-int setup_recip_2d(const T *so, T *sor, Dims2 d, cudaStream_t st)
+int setup_recip_2d(const T *so, T *sor, Dims2 d, cudaStream_t st, int ns)
 {
-	k_recip<T><<<dim3(ceil_div(d.nx, TX), ceil_div(d.ny, TY)), dim3(TX, TY), 0, st>>>(so, sor, d);
+	k_recip<T><<<dim3(ceil_div(d.nx, TX), ceil_div(d.ny, TY), d.nb), dim3(TX, TY), 0, st>>>(so, ns, sor, d);
 	CDR_LAUNCH_CHECK();
 	return CDR_OK;
 }
-template int setup_recip_2d<double>(const double *, double *, Dims2, cudaStream_t);
-template int setup_recip_2d<float>(const float *, float *, Dims2, cudaStream_t);
+template int setup_recip_2d<double>(const double *, double *, Dims2, cudaStream_t, int);
+template int setup_recip_2d<float>(const float *, float *, Dims2, cudaStream_t, int);
 
 // One colour of BMG2_SymStd_relax_GS (src/2d/ftn/BMG2_SymStd_relax_GS.f90:93-133).
 // 5-point: points with (i + j) % 2 == par (red-black); 9-point: points with
@@ -109,6 +129,10 @@ __global__ void __launch_bounds__(TX *TY) k_gs_colour(const T *__restrict__ so, 
 {
 	const size_t ps = d.plane();
 	const int pitch = d.pitch;
+	so += d.bofs(NS * ps);
+	q += d.bofs(ps);
+	qf += d.bofs(ps);
+	sor += d.bofs(2 * ps);
 	int j, i;
 	if (NS == 3) {
 		j = blockIdx.y * TY + threadIdx.y + 1;
@@ -142,7 +166,7 @@ int relax_point_2d(const T *so, int nstencil, T *x, const T *b, const T *sor, Di
 		// DOWN: (JBEG, IBEG) = (2,2),(2,3),(3,2),(3,3) with JBEG outer; UP reversed.
 		// Fortran index 2 is 0-based 1 (odd), 3 is 0-based 2 (even).
 		const int order[4][2] = {{1, 1}, {1, 0}, {0, 1}, {0, 0}};  // (j odd?, i odd?)
-		dim3 grd(ceil_div((d.nx + 1) / 2, TX), ceil_div((d.ny + 1) / 2, TY));
+		dim3 grd(ceil_div((d.nx + 1) / 2, TX), ceil_div((d.ny + 1) / 2, TY), d.nb);
 		for (int c = 0; c < 4; ++c) {
 			int o = updown == CDR_DOWN ? c : 3 - c;
 			k_gs_colour<T, 5><<<grd, blk, 0, st>>>(so, x, b, sor, d, order[o][1], order[o][0]);
@@ -151,7 +175,7 @@ int relax_point_2d(const T *so, int nstencil, T *x, const T *b, const T *sor, Di
 	} else {
 		// DOWN: JO = 2 then 3; a point is swept in pass JO when (I + J + JO) is even,
 		// i.e. 0-based (i + j) even first, odd second.  UP reversed.
-		dim3 grd(ceil_div((d.nx + 1) / 2, TX), ceil_div(d.ny, TY));
+		dim3 grd(ceil_div((d.nx + 1) / 2, TX), ceil_div(d.ny, TY), d.nb);
 		for (int c = 0; c < 2; ++c) {
 			int par = updown == CDR_DOWN ? c : 1 - c;
 			k_gs_colour<T, 3><<<grd, blk, 0, st>>>(so, x, b, sor, d, par, 0);
@@ -176,6 +200,9 @@ __global__ void __launch_bounds__(TX *TY) k_restrict(const T *__restrict__ ci, c
 	if (ic > c.nx || jc > c.ny) return;
 	const size_t cps = c.plane();
 	const int cp = c.pitch, fp = f.pitch;
+	ci += c.bofs(8 * cps);
+	q += f.bofs(f.plane());
+	qc += c.bofs(cps);
 	size_t kc = c.at(ic, jc), kf = f.at(2 * ic - 1, 2 * jc - 1);
 	const T *cL = ci + IL * cps, *cR = ci + IR * cps, *cA = ci + IA * cps, *cB = ci + IB * cps;
 	const T *cSW = ci + ISW * cps, *cNW = ci + INW * cps, *cNE = ci + INE * cps, *cSE = ci + ISE * cps;
@@ -187,7 +214,7 @@ __global__ void __launch_bounds__(TX *TY) k_restrict(const T *__restrict__ ci, c
 template <typename T>
 int restrict_2d(const T *ci, const T *rf, T *bc, Dims2 f, Dims2 c, cudaStream_t st)
 {
-	k_restrict<T><<<dim3(ceil_div(c.nx, TX), ceil_div(c.ny, TY)), dim3(TX, TY), 0, st>>>(ci, rf, bc, f, c);
+	k_restrict<T><<<dim3(ceil_div(c.nx, TX), ceil_div(c.ny, TY), c.nb), dim3(TX, TY), 0, st>>>(ci, rf, bc, f, c);
 	CDR_LAUNCH_CHECK();
 	return CDR_OK;
 }
@@ -202,12 +229,17 @@ template int restrict_2d<float>(const float *, const float *, float *, Dims2, Di
 template <typename T>
 __global__ void __launch_bounds__(TX *TY) k_interp_add(const T *__restrict__ ci, const T *__restrict__ qc,
                                                        const T *__restrict__ res, const T *__restrict__ soc,
-                                                       T *__restrict__ q, Dims2 f, Dims2 c)
+                                                       T *__restrict__ q, Dims2 f, Dims2 c, int nsf)
 {
 	int ic = blockIdx.x * TX + threadIdx.x + 1, jc = blockIdx.y * TY + threadIdx.y + 1;
 	if (ic > f.nx / 2 + 1 || jc > f.ny / 2 + 1) return;
 	const size_t cps = c.plane();
 	const int cp = c.pitch, fp = f.pitch;
+	ci += c.bofs(8 * cps);
+	qc += c.bofs(cps);
+	res += f.bofs(f.plane());
+	soc += f.bofs(nsf * f.plane());
+	q += f.bofs(f.plane());
 	const int i = 2 * ic - 1, j = 2 * jc - 1;
 	size_t kc = c.at(ic, jc), kf = f.at(i, j);
 	// The reference divides r by c on interior points only; for even grid sizes
@@ -234,17 +266,18 @@ __global__ void __launch_bounds__(TX *TY) k_interp_add(const T *__restrict__ ci,
 }
 
 template <typename T>
-int interp_add_2d(const T *ci, const T *xc, const T *rf, const T *sof, T *xf, Dims2 f, Dims2 c, cudaStream_t st)
+int interp_add_2d(const T *ci, const T *xc, const T *rf, const T *sof, T *xf, Dims2 f, Dims2 c, cudaStream_t st,
+                  int nsf)
 {
-	k_interp_add<T><<<dim3(ceil_div(f.nx / 2 + 1, TX), ceil_div(f.ny / 2 + 1, TY)), dim3(TX, TY), 0, st>>>(
-	    ci, xc, rf, sof, xf, f, c);
+	k_interp_add<T><<<dim3(ceil_div(f.nx / 2 + 1, TX), ceil_div(f.ny / 2 + 1, TY), f.nb), dim3(TX, TY), 0, st>>>(
+	    ci, xc, rf, sof, xf, f, c, nsf);
 	CDR_LAUNCH_CHECK();
 	return CDR_OK;
 }
 template int interp_add_2d<double>(const double *, const double *, const double *, const double *, double *,
-                                   Dims2, Dims2, cudaStream_t);
+                                   Dims2, Dims2, cudaStream_t, int);
 template int interp_add_2d<float>(const float *, const float *, const float *, const float *, float *, Dims2,
-                                  Dims2, cudaStream_t);
+                                  Dims2, cudaStream_t, int);
 
 // ------------------------------------------------ operator-induced interpolation
 // BMG2_SymStd_SETUP_interp_OI (src/2d/ftn/BMG2_SymStd_SETUP_interp_OI.f90:109-253).
@@ -257,6 +290,8 @@ __global__ void k_oi_edges(const double *__restrict__ so, double *__restrict__ c
 	int ic = blockIdx.x * TX + threadIdx.x + 1, jc = blockIdx.y * TY + threadIdx.y + 1;
 	const size_t ps = f.plane(), cps = c.plane();
 	const int fp = f.pitch;
+	so += f.bofs(NS * ps);
+	ci += c.bofs(8 * cps);
 	const double *C = so, *W = so + ps, *S = so + 2 * ps, *SW = so + 3 * ps, *NW = so + 4 * ps;
 	size_t kc = c.at(ic, jc);
 	// x-edge weights at coarse (ic, jc), ic in [2, nxf/2+1], jc in [1, nyc]
@@ -306,6 +341,8 @@ __global__ void k_oi_corners(const double *__restrict__ so, double *__restrict__
 	if (ic > f.nx / 2 + 1 || jc > f.ny / 2 + 1) return;
 	const size_t ps = f.plane(), cps = c.plane();
 	const int fp = f.pitch, cp = c.pitch;
+	so += f.bofs(NS * ps);
+	ci += c.bofs(8 * cps);
 	const double *C = so, *W = so + ps, *S = so + 2 * ps, *SW = so + 3 * ps, *NW = so + 4 * ps;
 	size_t kc = c.at(ic, jc);
 	size_t k = f.at(2 * ic - 1, 2 * jc - 1);  // (I, J); the centre point is (I-1, J-1)
@@ -340,10 +377,10 @@ __global__ void k_oi_corners(const double *__restrict__ so, double *__restrict__
 
 int setup_interp_2d(const double *so, int nstencil, double *ci, Dims2 f, Dims2 c, cudaStream_t st)
 {
-	CDR_CUDA_TRY(cudaMemsetAsync(ci, 0, sizeof(double) * c.plane() * 8, st));
+	CDR_CUDA_TRY(cudaMemsetAsync(ci, 0, sizeof(double) * c.plane() * 8 * c.nb, st));
 	dim3 blk(TX, TY);
-	dim3 g1(ceil_div(c.nx + 1, TX), ceil_div(c.ny + 1, TY));
-	dim3 g2(ceil_div(f.nx / 2, TX), ceil_div(f.ny / 2, TY));
+	dim3 g1(ceil_div(c.nx + 1, TX), ceil_div(c.ny + 1, TY), c.nb);
+	dim3 g2(ceil_div(f.nx / 2, TX), ceil_div(f.ny / 2, TY), c.nb);
 	if (nstencil == 5) {
 		k_oi_edges<5><<<g1, blk, 0, st>>>(so, ci, f, c);
 		CDR_LAUNCH_CHECK();
@@ -373,6 +410,9 @@ __global__ void k_galerkin(const double *__restrict__ so, const double *__restri
 	if (ic > c.nx || jc > c.ny) return;
 	const size_t ps = f.plane(), cps = c.plane();
 	const int fp = f.pitch, cp = c.pitch;
+	so += f.bofs(NS * ps);
+	ci += c.bofs(8 * cps);
+	soc += c.bofs(5 * cps);
 	const size_t k0 = f.at(2 * ic - 1, 2 * jc - 1), kc0 = c.at(ic, jc);
 	// fine stencil relative to (I, J) and weights relative to (IC, JC)
 	auto O = [&](int di, int dj) { return so[k0 + (long)dj * fp + di]; };
@@ -467,8 +507,8 @@ __global__ void k_galerkin(const double *__restrict__ so, const double *__restri
 
 int galerkin_2d(const double *so, int nstencil, const double *ci, double *soc, Dims2 f, Dims2 c, cudaStream_t st)
 {
-	CDR_CUDA_TRY(cudaMemsetAsync(soc, 0, sizeof(double) * c.plane() * 5, st));
-	dim3 g(ceil_div(c.nx, TX), ceil_div(c.ny, TY));
+	CDR_CUDA_TRY(cudaMemsetAsync(soc, 0, sizeof(double) * c.plane() * 5 * c.nb, st));
+	dim3 g(ceil_div(c.nx, TX), ceil_div(c.ny, TY), c.nb);
 	if (nstencil == 5) k_galerkin<5><<<g, dim3(TX, TY), 0, st>>>(so, ci, soc, f, c);
 	else k_galerkin<3><<<g, dim3(TX, TY), 0, st>>>(so, ci, soc, f, c);
 	CDR_LAUNCH_CHECK();
@@ -484,6 +524,8 @@ __global__ void k_cg_factor(const double *__restrict__ so, int ns, Dims2 d, doub
 	if (threadIdx.x != 0 || blockIdx.x != 0) return;
 	const int ldab = d.nx + 2, kd = d.nx + 1, n = d.nx * d.ny;
 	const size_t ps = d.plane();
+	so += d.bofs(ns * ps);
+	ab += d.bofs((size_t)ldab * n);
 	for (size_t e = 0; e < (size_t)ldab * n; ++e) ab[e] = 0.0;
 	int kk = 0;
 	for (int j = 1; j <= d.ny; ++j)
@@ -519,7 +561,11 @@ __global__ void k_cg_factor(const double *__restrict__ so, int ns, Dims2 d, doub
 			}
 		}
 	}
-	if (info) *info = st;
+	// a batch records the first failure it meets (the caller zeroes info)
+	if (info) {
+		if (gridDim.z == 1) *info = st;
+		else if (st) atomicCAS(info, 0, st);
+	}
 }
 
 // BMG2_SymStd_SOLVE_cg (src/2d/ftn/BMG2_SymStd_SOLVE_cg.f90:93-123) with DPBTRS('U'):
@@ -530,6 +576,9 @@ __global__ void k_cg_solve(const double *__restrict__ ab, T *__restrict__ q, con
 	extern __shared__ double xs[];
 	if (threadIdx.x != 0 || blockIdx.x != 0) return;
 	const int ldab = d.nx + 2, kd = d.nx + 1, n = d.nx * d.ny;
+	ab += d.bofs((size_t)ldab * n);
+	q += d.bofs(d.plane());
+	qf += d.bofs(d.plane());
 	int kk = 0;
 	for (int j = 1; j <= d.ny; ++j)
 		for (int i = 1; i <= d.nx; ++i) xs[kk++] = (double)qf[d.at(i, j)];
@@ -554,7 +603,7 @@ __global__ void k_cg_solve(const double *__restrict__ ab, T *__restrict__ q, con
 
 int setup_cg_2d(const double *so, int nstencil, Dims2 d, double *abd, int *info, cudaStream_t st)
 {
-	k_cg_factor<<<1, 32, 0, st>>>(so, nstencil, d, abd, info);
+	k_cg_factor<<<dim3(1, 1, d.nb), 32, 0, st>>>(so, nstencil, d, abd, info);
 	CDR_LAUNCH_CHECK();
 	return CDR_OK;
 }
@@ -567,7 +616,7 @@ int solve_cg_2d(const double *abd, T *x, const T *b, Dims2 d, cudaStream_t st)
 		set_error(CDR_ERR_DIM, "coarsest grid %dx%d too large for the direct solve", d.nx, d.ny);
 		return CDR_ERR_DIM;
 	}
-	k_cg_solve<T><<<1, 32, sm, st>>>(abd, x, b, d);
+	k_cg_solve<T><<<dim3(1, 1, d.nb), 32, sm, st>>>(abd, x, b, d);
 	CDR_LAUNCH_CHECK();
 	return CDR_OK;
 }
@@ -597,18 +646,27 @@ int convert_f64_f32(const double *in, float *out, size_t n, cudaStream_t st)
 //   and ||r64||^2 per block.  The residual at a point needs the corrected x at
 //   its neighbours, so each thread forms x_in + e32 for its 3x3 neighbourhood on
 //   the fly; x_in and x_out are different buffers (ping-pong), so no thread
-//   reads a value another thread has already corrected.  apply = 0 skips e.
+//   reads a value another thread has already corrected.  apply = 0 skips e; in a
+//   batch, a problem whose active[z] is 0 (converged) skips e as well.
 template <int NS>
 __global__ void __launch_bounds__(TX *TY) k_ir_residual(const double *__restrict__ so, const double *__restrict__ x,
                                                         const float *__restrict__ e, const double *__restrict__ b,
                                                         double *__restrict__ xo, float *__restrict__ r32, Dims2 d,
-                                                        Dims2 d32, double *__restrict__ partial, int apply)
+                                                        Dims2 d32, double *__restrict__ partial, int apply,
+                                                        const int *__restrict__ active)
 {
 	__shared__ double sh[TX * TY / 32];
 	const int tiles_x = (d.nx + TX - 1) / TX;
 	const int ntiles = tiles_x * ((d.ny + TY - 1) / TY);
 	const size_t ps = d.plane();
 	const int p = d.pitch, p32 = d32.pitch;
+	so += d.bofs(NS * ps);
+	x += d.bofs(ps);
+	b += d.bofs(ps);
+	xo += d.bofs(ps);
+	e += d32.bofs(d32.plane());
+	r32 += d32.bofs(d32.plane());
+	if (active && !active[blockIdx.z * d.bstep]) apply = 0;
 	double acc = 0.0;
 	for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
 		int i = (t % tiles_x) * TX + threadIdx.x + 1;
@@ -640,20 +698,21 @@ __global__ void __launch_bounds__(TX *TY) k_ir_residual(const double *__restrict
 		}
 	}
 	double s = block_sum<TX * TY / 32>(acc, sh);
-	if (threadIdx.x == 0 && threadIdx.y == 0) partial[blockIdx.x] = s;
+	if (threadIdx.x == 0 && threadIdx.y == 0) partial[(size_t)blockIdx.z * gridDim.x + blockIdx.x] = s;
 }
 
 int ir_residual_2d(const double *so, int nstencil, const double *x, const float *e, const double *b, double *xo,
-                   float *r32, Dims2 d, Dims2 d32, double *norm_out, double *partial, int apply, cudaStream_t st)
+                   float *r32, Dims2 d, Dims2 d32, double *norm_out, double *partial, int apply, cudaStream_t st,
+                   const int *active)
 {
-	const int ntiles = ceil_div(d.nx, TX) * ceil_div(d.ny, TY);
-	int nb = ntiles < NORM_MAX_BLOCKS ? ntiles : NORM_MAX_BLOCKS;
+	const int nb = norm_blocks(d);
+	const dim3 grd(nb, 1, d.nb);
 	if (nstencil == 5)
-		k_ir_residual<5><<<nb, dim3(TX, TY), 0, st>>>(so, x, e, b, xo, r32, d, d32, partial, apply);
+		k_ir_residual<5><<<grd, dim3(TX, TY), 0, st>>>(so, x, e, b, xo, r32, d, d32, partial, apply, active);
 	else
-		k_ir_residual<3><<<nb, dim3(TX, TY), 0, st>>>(so, x, e, b, xo, r32, d, d32, partial, apply);
+		k_ir_residual<3><<<grd, dim3(TX, TY), 0, st>>>(so, x, e, b, xo, r32, d, d32, partial, apply, active);
 	CDR_LAUNCH_CHECK();
-	k_norm_finish<<<1, 1024, 0, st>>>(partial, nb, norm_out);
+	k_norm_finish<<<d.nb, 1024, 0, st>>>(partial, nb, norm_out);
 	CDR_LAUNCH_CHECK();
 	return CDR_OK;
 }

@@ -8,7 +8,7 @@ template <typename T>
 int residual_2d(const T *so, int nstencil, const T *x, const T *b, T *r, Dims2 d, double *norm_out,
                 double *partial, cudaStream_t st);
 template <typename T>
-int setup_recip_2d(const T *so, T *sor, Dims2 d, cudaStream_t st);
+int setup_recip_2d(const T *so, T *sor, Dims2 d, cudaStream_t st, int nstencil = 5);
 template <typename T>
 int relax_point_2d(const T *so, int nstencil, T *x, const T *b, const T *sor, Dims2 d, int updown, cudaStream_t st);
 template <typename TS>
@@ -20,7 +20,8 @@ int relax_lines_2d(const T *so, int nstencil, T *x, const T *b, const T *sor, Di
 template <typename T>
 int restrict_2d(const T *ci, const T *rf, T *bc, Dims2 f, Dims2 c, cudaStream_t st);
 template <typename T>
-int interp_add_2d(const T *ci, const T *xc, const T *rf, const T *sof, T *xf, Dims2 f, Dims2 c, cudaStream_t st);
+int interp_add_2d(const T *ci, const T *xc, const T *rf, const T *sof, T *xf, Dims2 f, Dims2 c, cudaStream_t st,
+                  int nstencil_fine = 5);
 int setup_interp_2d(const double *so, int nstencil, double *ci, Dims2 f, Dims2 c, cudaStream_t st);
 int galerkin_2d(const double *so, int nstencil, const double *ci, double *soc, Dims2 f, Dims2 c, cudaStream_t st);
 int setup_cg_2d(const double *so, int nstencil, Dims2 d, double *abd, int *info, cudaStream_t st);
@@ -28,7 +29,10 @@ template <typename T>
 int solve_cg_2d(const double *abd, T *x, const T *b, Dims2 d, cudaStream_t st);
 int convert_f64_f32(const double *in, float *out, size_t n, cudaStream_t st);
 int ir_residual_2d(const double *so, int nstencil, const double *x, const float *e, const double *b, double *xo,
-                   float *r32, Dims2 d, Dims2 d32, double *norm_out, double *partial, int apply, cudaStream_t st);
+                   float *r32, Dims2 d, Dims2 d32, double *norm_out, double *partial, int apply, cudaStream_t st,
+                   const int *active = nullptr);
+// partial-sum blocks per problem of a residual norm (partial holds nb times that)
+int norm_blocks(Dims2 d);
 
 constexpr size_t kNormScratchBytes = 2048 * sizeof(double);
 

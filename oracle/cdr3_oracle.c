@@ -21,6 +21,7 @@
 #include <stdlib.h>
 #include <string.h>
 
+#include "cdr2_oracle.h"
 #include "cdr3_oracle.h"
 
 enum { KP = 1, KPW, KPS, KB, KPSW, KPNW, KBW, KBNW, KBN, KBNE, KBE, KBSE, KBS, KBSW };
@@ -704,9 +705,18 @@ double o3_l2norm(const double *r, int II, int JJ, int KK)
 }
 
 /* ------------------------------------------------------------ driver */
+/* plane relaxation of one direction on one level: one 2D solver per plane
+ * (planes<rdir>::setup_impl, include/cedar/3d/relax_planes.h:171-222) */
+struct o3_planes {
+	int n, n1, n2;          /* planes, and the plane grid */
+	o2_solver **s;
+	double **so2;           /* each plane's 2D operator (5 planes, kept for inspection) */
+	double *x2, *b2;        /* work grid functions of the plane grid */
+};
 struct o3_level {
 	int nx, ny, nz, ii, jj, kk;
 	double *so, *x, *b, *res, *sor, *ci;
+	struct o3_planes pl[3];
 };
 struct o3_solver {
 	o3_settings s;
@@ -717,6 +727,179 @@ struct o3_solver {
 };
 
 static double *zal(size_t n) { return (double *)calloc(n ? n : 1, sizeof(double)); }
+
+/* ------------------------------------------------------- plane relaxation */
+/* Index helpers in the reference's C++ (0-based, ghost-inclusive) indices. */
+#define X3(a, i, j, k) (a)[ix3((i) + 1, (j) + 1, (k) + 1, II, JJ)]
+#define S3(p, i, j, k) so[ix4((i) + 1, (j) + 1, (k) + 1, p, II, JJ, KK)]
+#define X2(a, i, j) (a)[(size_t)(j) * (n1 + 2) + (i)]
+#define S2(p, i, j) so2[((size_t)(p) * (n2 + 2) + (j)) * (n1 + 2) + (i)]
+
+/* copy_coeff for xxvii_pt -> nine_pt, include/cedar/3d/relax_planes.h:110-149
+ * (2D planes c, w, s, sw, nw = 0..4); ghost rows included */
+static void copy_coeff(const double *so, int II, int JJ, int KK, int dir, int ipl, double *so2, int n1, int n2)
+{
+	if (dir == O3_XY) {
+		for (int j = 0; j < n2 + 2; ++j)
+			for (int i = 0; i < n1 + 2; ++i) {
+				S2(0, i, j) = S3(KP, i, j, ipl);
+				S2(1, i, j) = S3(KPW, i, j, ipl);
+				S2(2, i, j) = S3(KPS, i, j, ipl);
+				S2(3, i, j) = S3(KPSW, i, j, ipl);
+				S2(4, i, j) = S3(KPNW, i, j, ipl);
+			}
+	} else if (dir == O3_XZ) {
+		for (int k = 1; k <= n2; ++k) /* so3.range(2): interior k only */
+			for (int i = 0; i < n1 + 2; ++i) {
+				S2(0, i, k) = S3(KP, i, ipl, k);
+				S2(1, i, k) = S3(KPW, i, ipl, k);
+				S2(2, i, k) = S3(KB, i, ipl, k);
+				S2(3, i, k) = S3(KBW, i, ipl, k);
+				S2(4, i, k) = S3(KBE, i, ipl, k);
+			}
+	} else {
+		for (int k = 0; k < n2 + 2; ++k)
+			for (int j = 0; j < n1 + 2; ++j) {
+				S2(0, j, k) = S3(KP, ipl, j, k);
+				S2(1, j, k) = S3(KPS, ipl, j, k);
+				S2(2, j, k) = S3(KB, ipl, j, k);
+				S2(3, j, k) = S3(KBS, ipl, j, k);
+				S2(4, j, k) = S3(KBN, ipl, j, k);
+			}
+	}
+}
+
+/* copy32 / copy23, src/3d/relax_planes.cc:185-238 (ghost-inclusive) */
+static void copy32(const double *x, int II, int JJ, int dir, int ipl, double *x2, int n1, int n2)
+{
+	for (int b = 0; b < n2 + 2; ++b)
+		for (int a = 0; a < n1 + 2; ++a)
+			X2(x2, a, b) = dir == O3_XY ? X3(x, a, b, ipl) : dir == O3_XZ ? X3(x, a, ipl, b) : X3(x, ipl, a, b);
+}
+static void copy23(const double *x2, double *x, int II, int JJ, int dir, int ipl, int n1, int n2)
+{
+	for (int b = 0; b < n2 + 2; ++b)
+		for (int a = 0; a < n1 + 2; ++a) {
+			if (dir == O3_XY) X3(x, a, b, ipl) = X2(x2, a, b);
+			else if (dir == O3_XZ) X3(x, a, ipl, b) = X2(x2, a, b);
+			else X3(x, ipl, a, b) = X2(x2, a, b);
+		}
+}
+
+/* copy_rhs for xxvii_pt, src/3d/relax_planes.cc:43-72 (xy), :95-127 (xz), :146-178 (yz);
+ * interior of the plane only, in the reference's operand order */
+static void copy_rhs(const double *so, const double *x, const double *b, int II, int JJ, int KK, int dir, int ipl,
+                     double *b2, int n1, int n2)
+{
+	for (int q = 1; q <= n2; ++q)
+		for (int p = 1; p <= n1; ++p) {
+			double v;
+			if (dir == O3_XY) {
+				const int i = p, j = q, k = ipl;
+				v = X3(b, i, j, k) + S3(KB, i, j, k) * X3(x, i, j, k - 1) + S3(KBW, i, j, k) * X3(x, i - 1, j, k - 1)
+				    + S3(KBNW, i, j + 1, k) * X3(x, i - 1, j + 1, k - 1) + S3(KBN, i, j + 1, k) * X3(x, i, j + 1, k - 1)
+				    + S3(KBNE, i + 1, j + 1, k) * X3(x, i + 1, j + 1, k - 1) + S3(KBE, i + 1, j, k) * X3(x, i + 1, j, k - 1)
+				    + S3(KBSE, i + 1, j, k) * X3(x, i + 1, j - 1, k - 1) + S3(KBS, i, j, k) * X3(x, i, j - 1, k - 1)
+				    + S3(KBSW, i, j, k) * X3(x, i - 1, j - 1, k - 1) + S3(KBE, i, j, k + 1) * X3(x, i - 1, j, k + 1)
+				    + S3(KBSE, i, j + 1, k + 1) * X3(x, i - 1, j + 1, k + 1) + S3(KBS, i, j + 1, k + 1) * X3(x, i, j + 1, k + 1)
+				    + S3(KBSW, i + 1, j + 1, k + 1) * X3(x, i + 1, j + 1, k + 1) + S3(KBW, i + 1, j, k + 1) * X3(x, i + 1, j, k + 1)
+				    + S3(KB, i, j, k + 1) * X3(x, i, j, k + 1) + S3(KBNW, i + 1, j, k + 1) * X3(x, i + 1, j - 1, k + 1)
+				    + S3(KBN, i, j, k + 1) * X3(x, i, j - 1, k + 1) + S3(KBNE, i, j, k + 1) * X3(x, i - 1, j - 1, k + 1);
+			} else if (dir == O3_XZ) {
+				const int i = p, k = q, j = ipl;
+				v = X3(b, i, j, k) + S3(KPNW, i, j + 1, k) * X3(x, i - 1, j + 1, k) + S3(KPS, i, j + 1, k) * X3(x, i, j + 1, k)
+				    + S3(KPSW, i + 1, j + 1, k) * X3(x, i + 1, j + 1, k) + S3(KBNW, i, j + 1, k) * X3(x, i - 1, j + 1, k - 1)
+				    + S3(KBN, i, j + 1, k) * X3(x, i, j + 1, k - 1) + S3(KBNE, i + 1, j + 1, k) * X3(x, i + 1, j + 1, k - 1)
+				    + S3(KBSE, i, j + 1, k + 1) * X3(x, i - 1, j + 1, k + 1) + S3(KBS, i, j + 1, k + 1) * X3(x, i, j + 1, k + 1)
+				    + S3(KBSW, i + 1, j + 1, k + 1) * X3(x, i + 1, j + 1, k + 1) + S3(KPSW, i, j, k) * X3(x, i - 1, j - 1, k)
+				    + S3(KPS, i, j, k) * X3(x, i, j - 1, k) + S3(KPNW, i + 1, j, k) * X3(x, i + 1, j - 1, k)
+				    + S3(KBSW, i, j, k) * X3(x, i - 1, j - 1, k - 1) + S3(KBS, i, j, k) * X3(x, i, j - 1, k - 1)
+				    + S3(KBSE, i + 1, j, k) * X3(x, i + 1, j - 1, k - 1) + S3(KBNE, i, j, k + 1) * X3(x, i - 1, j - 1, k + 1)
+				    + S3(KBN, i, j, k + 1) * X3(x, i, j - 1, k + 1) + S3(KBNW, i + 1, j, k + 1) * X3(x, i + 1, j - 1, k + 1);
+			} else {
+				const int j = p, k = q, i = ipl;
+				v = X3(b, i, j, k) + S3(KPNW, i, j + 1, k) * X3(x, i - 1, j + 1, k) + S3(KPW, i, j, k) * X3(x, i - 1, j, k)
+				    + S3(KPSW, i, j, k) * X3(x, i - 1, j - 1, k) + S3(KBNW, i, j + 1, k) * X3(x, i - 1, j + 1, k - 1)
+				    + S3(KBW, i, j, k) * X3(x, i - 1, j, k - 1) + S3(KBSW, i, j, k) * X3(x, i - 1, j - 1, k - 1)
+				    + S3(KBSE, i, j + 1, k + 1) * X3(x, i - 1, j + 1, k + 1) + S3(KBE, i, j, k + 1) * X3(x, i - 1, j, k + 1)
+				    + S3(KBNE, i, j, k + 1) * X3(x, i - 1, j - 1, k + 1) + S3(KPSW, i + 1, j + 1, k) * X3(x, i + 1, j + 1, k)
+				    + S3(KPW, i + 1, j, k) * X3(x, i + 1, j, k) + S3(KPNW, i + 1, j, k) * X3(x, i + 1, j - 1, k)
+				    + S3(KBNE, i + 1, j + 1, k) * X3(x, i + 1, j + 1, k - 1) + S3(KBE, i + 1, j, k) * X3(x, i + 1, j, k - 1)
+				    + S3(KBSE, i + 1, j, k) * X3(x, i + 1, j - 1, k - 1) + S3(KBSW, i + 1, j + 1, k + 1) * X3(x, i + 1, j + 1, k + 1)
+				    + S3(KBW, i + 1, j, k + 1) * X3(x, i + 1, j, k + 1) + S3(KBNW, i + 1, j, k + 1) * X3(x, i + 1, j - 1, k + 1);
+			}
+			X2(b2, p, q) = v;
+		}
+}
+#undef X3
+#undef S3
+#undef X2
+#undef S2
+
+/* the plane solvers' settings: kernel_params plane_config default,
+ * src/kernel_params.cc:83-89 (line-xy, max-iter 1; other keys at their defaults) */
+static void plane_settings(o2_settings *s2)
+{
+	s2->relax = O2_RELAX_LINE_XY;
+	s2->nrelax_pre = 2;
+	s2->nrelax_post = 1;
+	s2->num_levels = -1;
+	s2->maxiter = 1;
+	s2->tol = 1e-8;
+	s2->min_coarse = 3;
+}
+
+static void planes_setup(struct o3_level *L, int dir)
+{
+	struct o3_planes *P = &L->pl[dir];
+	P->n = dir == O3_XY ? L->nz : dir == O3_XZ ? L->ny : L->nx;
+	P->n1 = dir == O3_YZ ? L->ny : L->nx;
+	P->n2 = dir == O3_XY ? L->ny : L->nz;
+	const size_t g2 = (size_t)(P->n1 + 2) * (P->n2 + 2);
+	P->s = (o2_solver **)calloc(P->n, sizeof(o2_solver *));
+	P->so2 = (double **)calloc(P->n, sizeof(double *));
+	P->x2 = (double *)calloc(g2, sizeof(double));
+	P->b2 = (double *)calloc(g2, sizeof(double));
+	o2_settings s2;
+	plane_settings(&s2);
+	for (int ipl = 1; ipl <= P->n; ++ipl) {
+		double *so2 = (double *)calloc(g2 * 5, sizeof(double));
+		copy_coeff(L->so, L->ii, L->jj, L->kk, dir, ipl, so2, P->n1, P->n2);
+		P->so2[ipl - 1] = so2;
+		P->s[ipl - 1] = o2_create(&s2, so2, 5, P->n1, P->n2);
+	}
+}
+
+static void planes_free(struct o3_level *L)
+{
+	for (int d = 0; d < 3; ++d) {
+		struct o3_planes *P = &L->pl[d];
+		for (int i = 0; i < P->n && P->s; ++i) {
+			o2_destroy(P->s[i]);
+			free(P->so2[i]);
+		}
+		free(P->s); free(P->so2); free(P->x2); free(P->b2);
+		memset(P, 0, sizeof(*P));
+	}
+}
+
+/* relax_planes, include/cedar/3d/relax_planes.h:35-70: red-black over planes
+ * (DOWN: odd planes first), each plane one 2D V-cycle (solve with max-iter 1;
+ * its residual norms do not touch x) on b + off-plane couplings */
+static void relax_planes_level(struct o3_level *L, int dir, double *x, const double *b, int updown)
+{
+	struct o3_planes *P = &L->pl[dir];
+	const int beg0 = updown == 0 ? 1 : 2, beg1 = updown == 0 ? 2 : 1;
+	for (int c = 0; c < 2; ++c) {
+		const int beg = c == 0 ? beg0 : beg1;
+		for (int ipl = beg; ipl <= P->n; ipl += 2) {
+			copy32(x, L->ii, L->jj, dir, ipl, P->x2, P->n1, P->n2);
+			copy_rhs(L->so, x, b, L->ii, L->jj, L->kk, dir, ipl, P->b2, P->n1, P->n2);
+			o2_vcycle(P->s[ipl - 1], P->x2, P->b2);
+			copy23(P->x2, x, L->ii, L->jj, dir, ipl, P->n1, P->n2);
+		}
+	}
+}
 
 /* cdr3::solver::compute_num_levels, include/cedar/3d/solver.h:59-77 */
 int o3_num_levels(int nx, int ny, int nz, int min_coarse)
@@ -759,6 +942,13 @@ o3_solver *o3_create(const o3_settings *s, const double *so_fine, int nx, int ny
 		o3_galerkin(F->so, C->so, C->ci, F->ii, F->jj, F->kk, C->ii, C->jj, C->kk);
 		o3_setup_recip(F->so, F->sor, F->ii, F->jj, F->kk);
 	}
+	/* plane smoothers on every level but the coarsest (multilevel.h:147-159) */
+	for (int l = 0; l + 1 < nl; ++l) {
+		struct o3_level *F = &h->lv[l];
+		if (s->relax == O3_RELAX_PLANE_XYZ || s->relax == O3_RELAX_PLANE_XY) planes_setup(F, O3_XY);
+		if (s->relax == O3_RELAX_PLANE_XYZ || s->relax == O3_RELAX_PLANE_XZ) planes_setup(F, O3_XZ);
+		if (s->relax == O3_RELAX_PLANE_XYZ || s->relax == O3_RELAX_PLANE_YZ) planes_setup(F, O3_YZ);
+	}
 	struct o3_level *Cg = &h->lv[nl - 1];
 	h->nabd1 = Cg->nx * (Cg->ny + 1) + 2;
 	int nn = Cg->nx * Cg->ny * Cg->nz;
@@ -773,15 +963,36 @@ void o3_destroy(o3_solver *h)
 	if (!h) return;
 	for (int l = 0; l < h->nlev; ++l) {
 		struct o3_level *L = &h->lv[l];
+		planes_free(L);
 		free(L->so); free(L->x); free(L->b); free(L->res); free(L->sor); free(L->ci);
 	}
 	free(h->lv); free(h->abd); free(h->bbd); free(h);
 }
 
+/* multilevel::setup_relax_helper closures, include/cedar/multilevel.h:160-222:
+ * plane-xyz runs xy, yz, xz going down and xz, yz, xy going up */
 static void smooth3(o3_solver *h, struct o3_level *L, int updown)
 {
 	int n = updown == 0 ? h->s.nrelax_pre : h->s.nrelax_post;
-	for (int it = 0; it < n; ++it) o3_relax_gs(L->so, L->b, L->x, L->sor, L->ii, L->jj, L->kk, updown);
+	for (int it = 0; it < n; ++it) {
+		switch (h->s.relax) {
+		case O3_RELAX_PLANE_XY: relax_planes_level(L, O3_XY, L->x, L->b, updown); break;
+		case O3_RELAX_PLANE_XZ: relax_planes_level(L, O3_XZ, L->x, L->b, updown); break;
+		case O3_RELAX_PLANE_YZ: relax_planes_level(L, O3_YZ, L->x, L->b, updown); break;
+		case O3_RELAX_PLANE_XYZ:
+			if (updown == 0) {
+				relax_planes_level(L, O3_XY, L->x, L->b, updown);
+				relax_planes_level(L, O3_YZ, L->x, L->b, updown);
+				relax_planes_level(L, O3_XZ, L->x, L->b, updown);
+			} else {
+				relax_planes_level(L, O3_XZ, L->x, L->b, updown);
+				relax_planes_level(L, O3_YZ, L->x, L->b, updown);
+				relax_planes_level(L, O3_XY, L->x, L->b, updown);
+			}
+			break;
+		default: o3_relax_gs(L->so, L->b, L->x, L->sor, L->ii, L->jj, L->kk, updown);
+		}
+	}
 }
 
 static void ncycle3(o3_solver *h, int l, double *x, const double *b)
@@ -841,4 +1052,18 @@ double *o3_level_array(o3_solver *h, int l, int which)
 	case 6: return L->ci;
 	default: return NULL;
 	}
+}
+
+void o3_relax_planes(o3_solver *h, int l, int dir, double *x, const double *b, int updown)
+{
+	relax_planes_level(&h->lv[l], dir, x, b, updown);
+}
+
+const double *o3_plane_op(o3_solver *h, int l, int dir, int ipl, int *n1, int *n2)
+{
+	struct o3_planes *P = &h->lv[l].pl[dir];
+	if (!P->s || ipl < 1 || ipl > P->n) return NULL;
+	*n1 = P->n1;
+	*n2 = P->n2;
+	return P->so2[ipl - 1];
 }

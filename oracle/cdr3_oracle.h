@@ -5,10 +5,15 @@
 #ifdef __cplusplus
 extern "C" {
 #endif
+/* relax: O3_RELAX_POINT or one of the plane relaxations (ml_settings::relax_type,
+ * include/cedar/multilevel_settings.h:30-31) */
+enum { O3_RELAX_POINT = 0, O3_RELAX_PLANE_XY = 4, O3_RELAX_PLANE_XZ = 5, O3_RELAX_PLANE_YZ = 6, O3_RELAX_PLANE_XYZ = 7 };
+enum { O3_XY = 0, O3_XZ = 1, O3_YZ = 2 };
 typedef struct {
 	int nrelax_pre, nrelax_post, num_levels, maxiter;
 	double tol;
 	int min_coarse;
+	int relax;
 } o3_settings;
 typedef struct o3_solver o3_solver;
 void o3_residual(const double *so, const double *qf, const double *q, double *res, int II, int JJ, int KK);
@@ -31,6 +36,11 @@ int o3_nlevels(const o3_solver *h);
 int o3_cg_info(const o3_solver *h);
 void o3_level_dims(const o3_solver *h, int l, int *d);
 double *o3_level_array(o3_solver *h, int l, int which);
+/* one plane-relaxation sweep of direction dir on level l of h (x, b: that level's
+ * ghost-inclusive arrays) */
+void o3_relax_planes(o3_solver *h, int l, int dir, double *x, const double *b, int updown);
+/* the 2D operator of plane ipl (1-based) of direction dir of level l, five planes */
+const double *o3_plane_op(o3_solver *h, int l, int dir, int ipl, int *n1, int *n2);
 #ifdef __cplusplus
 }
 #endif

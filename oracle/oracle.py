@@ -297,7 +297,12 @@ class Solver:
 
 class Settings3(ctypes.Structure):
     _fields_ = [("nrelax_pre", ctypes.c_int), ("nrelax_post", ctypes.c_int), ("num_levels", ctypes.c_int),
-                ("maxiter", ctypes.c_int), ("tol", ctypes.c_double), ("min_coarse", ctypes.c_int)]
+                ("maxiter", ctypes.c_int), ("tol", ctypes.c_double), ("min_coarse", ctypes.c_int),
+                ("relax", ctypes.c_int)]
+
+
+RELAX3 = {"point": 0, "plane-xy": 4, "plane-xz": 5, "plane-yz": 6, "plane-xyz": 7}
+PLANE_DIRS = {"xy": 0, "xz": 1, "yz": 2}
 
 
 _SIG3 = None
@@ -328,6 +333,8 @@ def lib3(variant=""):
             "o3_cg_info": (I, [P]),
             "o3_level_dims": (None, [P, P]),
             "o3_level_array": (ctypes.POINTER(ctypes.c_double), [P, I, I]),
+            "o3_relax_planes": (None, [P, I, I, P, P, I]),
+            "o3_plane_op": (ctypes.POINTER(ctypes.c_double), [P, I, I, I, ctypes.POINTER(I), ctypes.POINTER(I)]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -417,12 +424,13 @@ def l2norm3(r):
 class Solver3:
     """Serial 3D BoxMG (27-point fine operator, 8-colour point relaxation)."""
 
-    def __init__(self, so, nrelax_pre=2, nrelax_post=1, num_levels=-1, maxiter=10, tol=1e-8, min_coarse=3):
+    def __init__(self, so, nrelax_pre=2, nrelax_post=1, num_levels=-1, maxiter=10, tol=1e-8, min_coarse=3,
+                 relax="point"):
         self.L = lib3()
         so = np.ascontiguousarray(so, dtype=np.float64)
         assert so.shape[0] == 14
         self.nz, self.ny, self.nx = so.shape[1] - 2, so.shape[2] - 2, so.shape[3] - 2
-        self.s = Settings3(nrelax_pre, nrelax_post, num_levels, maxiter, tol, min_coarse)
+        self.s = Settings3(nrelax_pre, nrelax_post, num_levels, maxiter, tol, min_coarse, RELAX3[relax])
         self._so = so
         self.h = self.L.o3_create(ctypes.byref(self.s), _p(so), self.nx, self.ny, self.nz)
 
@@ -454,3 +462,17 @@ class Solver3:
         hist = np.zeros(max(self.s.maxiter, 1))
         n = self.L.o3_solve(self.h, _p(b), _p(x), _p(hist), len(hist))
         return x, hist[:n].copy()
+
+    def relax_planes(self, level, direction, x, b, updown):
+        """One red-black plane sweep (direction 'xy', 'xz' or 'yz') on level arrays x, b (in place)."""
+        assert x.flags.c_contiguous and x.dtype == np.float64
+        b = np.ascontiguousarray(b, dtype=np.float64)
+        self.L.o3_relax_planes(self.h, level, PLANE_DIRS[direction], _p(x), _p(b), updown)
+        return x
+
+    def plane_op(self, level, direction, ipl):
+        """The 2D nine-point operator (5, n2+2, n1+2) of plane ipl (1-based)."""
+        n1, n2 = ctypes.c_int(), ctypes.c_int()
+        ptr = self.L.o3_plane_op(self.h, level, PLANE_DIRS[direction], ipl, ctypes.byref(n1), ctypes.byref(n2))
+        shape = (5, n2.value + 2, n1.value + 2)
+        return np.ctypeslib.as_array(ptr, shape=(int(np.prod(shape)),)).copy().reshape(shape)

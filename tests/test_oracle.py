@@ -228,3 +228,70 @@ def test_3d_boxmg_converges(oracle):
     x, h = s.solve(b)
     assert h[-1] < 1e-10 and len(h) <= 12
     assert oracle.num_levels(15, 15, 3) == 3
+
+
+def _block_gs_planes(A, nx, ny, nz, direction, x, b, updown):
+    """Red-black block Gauss-Seidel over planes with exact plane solves (dense)."""
+    idx = np.arange(nx * ny * nz).reshape(nz, ny, nx)
+    if direction == "xy":
+        planes = [idx[k].ravel() for k in range(nz)]
+    elif direction == "xz":
+        planes = [idx[:, j, :].ravel() for j in range(ny)]
+    else:
+        planes = [idx[:, :, i].ravel() for i in range(nx)]
+    n = len(planes)
+    order = [range(0, n, 2), range(1, n, 2)]
+    if updown == 1:
+        order = order[::-1]
+    xv = x[1:-1, 1:-1, 1:-1].ravel().copy()
+    bv = b[1:-1, 1:-1, 1:-1].ravel()
+    for rng in order:
+        for p in rng:
+            ip = planes[p]
+            rhs = bv[ip] - A[ip] @ xv + A[np.ix_(ip, ip)] @ xv[ip]
+            xv[ip] = np.linalg.solve(A[np.ix_(ip, ip)], rhs)
+    out = x.copy()
+    out[1:-1, 1:-1, 1:-1] = xv.reshape(nz, ny, nx)
+    return out
+
+
+@pytest.mark.parametrize("direction", ["xy", "xz", "yz"])
+def test_3d_plane_relaxation_is_block_gauss_seidel(oracle, direction):
+    # 4 x 4 planes have a one-level 2D hierarchy, so each plane solve is the exact
+    # banded Cholesky: a plane sweep is then red-black block Gauss-Seidel
+    nx, ny, nz = 4, 4, 4
+    rng = np.random.default_rng(21)
+    so = G.fe3_hetero(np.exp(rng.normal(size=(nz + 1, ny + 1, nx + 1))))
+    A = G.stencil3_to_csr(so).toarray()
+    s = oracle.Solver3(so, relax="plane-xyz", min_coarse=2)
+    assert s.nlevels == 2
+    for updown in (0, 1):
+        x = np.zeros((nz + 2, ny + 2, nx + 2)); x[1:-1, 1:-1, 1:-1] = rng.random((nz, ny, nx))
+        b = np.zeros_like(x); b[1:-1, 1:-1, 1:-1] = rng.random((nz, ny, nx))
+        ref = _block_gs_planes(A, nx, ny, nz, direction, x, b, updown)
+        got = s.relax_planes(0, direction, x.copy(), b, updown)
+        np.testing.assert_allclose(got[1:-1, 1:-1, 1:-1], ref[1:-1, 1:-1, 1:-1], rtol=1e-11, atol=1e-13)
+
+
+def test_3d_plane_operators_are_the_in_plane_couplings(oracle):
+    nx, ny, nz = 5, 6, 7
+    rng = np.random.default_rng(22)
+    so = G.fe3_hetero(np.exp(rng.normal(size=(nz + 1, ny + 1, nx + 1))))
+    A = G.stencil3_to_csr(so).toarray()
+    s = oracle.Solver3(so, relax="plane-xyz", num_levels=2)
+    idx = np.arange(nx * ny * nz).reshape(nz, ny, nx)
+    for direction, ipl in (("xy", 3), ("xz", 2), ("yz", 4)):
+        so2 = s.plane_op(0, direction, ipl)
+        ip = (idx[ipl - 1] if direction == "xy" else idx[:, ipl - 1, :] if direction == "xz" else idx[:, :, ipl - 1]).ravel()
+        A2 = G.stencil_to_csr(so2).toarray()
+        np.testing.assert_array_equal(A2, A[np.ix_(ip, ip)])
+
+
+def test_3d_plane_boxmg_converges(oracle):
+    n = 15
+    rng = np.random.default_rng(23)
+    so = G.fe3_hetero(np.exp(1.5 * rng.normal(size=(n + 1,) * 3)))
+    b = np.zeros((n + 2,) * 3); b[1:-1, 1:-1, 1:-1] = rng.uniform(-1, 1, (n, n, n)) / (n + 1) ** 3
+    _, hp = oracle.Solver3(so, maxiter=12, tol=1e-10, relax="plane-xyz").solve(b)
+    _, h0 = oracle.Solver3(so, maxiter=12, tol=1e-10).solve(b)
+    assert hp[-1] < 1e-10 and len(hp) <= len(h0)
