@@ -13,7 +13,8 @@ HEADER = os.path.join(os.path.dirname(_HERE), "include", "cdr_gpu.h")
 
 CDR_OK = 0
 DOWN, UP = 0, 1
-RELAX = {"point": 0, "line-x": 1, "line-y": 2, "line-xy": 3}
+RELAX = {"point": 0, "line-x": 1, "line-y": 2, "line-xy": 3,
+         "plane-xy": 4, "plane-xz": 5, "plane-yz": 6, "plane-xyz": 7}
 PREC = {"fp64": 0, "fp32-ir": 1}
 DIR_X, DIR_Y = 0, 1
 LINES_EXACT = 1

@@ -13,10 +13,6 @@
 
 namespace cdrgpu {
 
-enum : int { KP = 1, KPW, KPS, KB, KPSW, KPNW, KBW, KBNW, KBN, KBNE, KBE, KBSE, KBS, KBSW };
-enum : int { LXYL = 1, LXYR, LXYA, LXYB, LXZA, LXZB, LXYNE, LXYSE, LXYSW, LXYNW, LXZSW, LXZNW, LXZNE, LXZSE,
-             LYZSW, LYZNW, LYZNE, LYZSE, LBSW, LBNW, LBNE, LBSE, LTSW, LTNW, LTNE, LTSE };
-
 #define SO(i, j, k, p) so[(size_t)((p)-1) * F.plane() + F.at1(i, j, k)]
 #define Q(i, j, k) q[F.at1(i, j, k)]
 #define QF(i, j, k) qf[F.at1(i, j, k)]

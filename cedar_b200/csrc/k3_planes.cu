@@ -1,0 +1,152 @@
+// k3_planes.cu -- plane relaxation of the 3D solver: the data movement between a
+// 3D level and the batch of 2D plane problems.
+//
+// Plane ipl (1-based) of direction xy is the k = ipl slice, of xz the j = ipl
+// slice and of yz the i = ipl slice; its 2D grid is (i, j), (i, k) and (j, k)
+// respectively (include/cedar/3d/relax_planes.h:73-149).  The plane problems of
+// a direction are the entries of a Batch2 (problem ipl-1).  Indices below are
+// the reference's C++ ones: 0-based with the ghost layer at 0 and n+1.
+#include "k2_point.cuh"
+#include "kernels3d.cuh"
+
+namespace cdrgpu {
+
+namespace {
+
+__device__ __forceinline__ size_t o3(const Dims3 &F, int i, int j, int k)
+{
+	return ((size_t)k * (F.ny + 2) + j) * F.pitch + i;
+}
+
+// 3D grid index of plane point (a, b) of plane ipl
+__device__ __forceinline__ size_t plane_at(const Dims3 &F, int dir, int ipl, int a, int b)
+{
+	return dir == 0 ? o3(F, a, b, ipl) : dir == 1 ? o3(F, a, ipl, b) : o3(F, ipl, a, b);
+}
+
+}  // namespace
+
+// copy_coeff for xxvii_pt -> nine_pt (include/cedar/3d/relax_planes.h:110-149):
+// 2D planes c, w, s, sw, nw from the 3D planes
+//   xy: p, pw, ps, psw, pnw;  xz: p, pw, b, bw, be;  yz: p, ps, b, bs, bn.
+// xz copies the interior k rows only (so3.range(2)), the others the ghost rows too.
+__global__ void k3_plane_coeff(const double *__restrict__ so, Dims3 F, int dir, double *__restrict__ so2, int n1,
+                               int n2, int pitch2)
+{
+	const int a = blockIdx.x * TX + threadIdx.x, b = blockIdx.y * TY + threadIdx.y, ipl = blockIdx.z + 1;
+	if (a > n1 + 1 || b > n2 + 1) return;
+	if (dir == 1 && (b < 1 || b > n2)) return;
+	const size_t plane2 = (size_t)pitch2 * (n2 + 2);
+	so2 += (size_t)(ipl - 1) * 5 * plane2 + (size_t)b * pitch2 + a;
+	const size_t g = plane_at(F, dir, ipl, a, b), P = F.plane();
+	const int src[3][5] = {{KP, KPW, KPS, KPSW, KPNW}, {KP, KPW, KB, KBW, KBE}, {KP, KPS, KB, KBS, KBN}};
+#pragma unroll
+	for (int q = 0; q < 5; ++q) so2[q * plane2] = so[(size_t)(src[dir][q] - 1) * P + g];
+}
+
+// copy32 (TO_PLANE) / copy23 (src/3d/relax_planes.cc:185-238): the whole plane,
+// ghost layer included, for planes ipl = first+1, first+1+step, ...
+template <typename T, bool TO_PLANE>
+__global__ void k3_plane_copy(T *__restrict__ x3, Dims3 F, int dir, int first, int step, T *__restrict__ x2, int n1,
+                              int n2, int pitch2)
+{
+	const int a = blockIdx.x * TX + threadIdx.x, b = blockIdx.y * TY + threadIdx.y;
+	const int ipl = first + 1 + blockIdx.z * step;
+	if (a > n1 + 1 || b > n2 + 1) return;
+	const size_t k2 = (size_t)(ipl - 1) * pitch2 * (n2 + 2) + (size_t)b * pitch2 + a;
+	const size_t k3 = plane_at(F, dir, ipl, a, b);
+	if (TO_PLANE) x2[k2] = x3[k3];
+	else x3[k3] = x2[k2];
+}
+
+template <typename T>
+int plane_copy(T *x3, Dims3 F, int dir, int first, int step, int count, T *x2, int n1, int n2, int pitch2,
+               bool to_plane, cudaStream_t st)
+{
+	const dim3 grd(ceil_div(n1 + 2, TX), ceil_div(n2 + 2, TY), count);
+	if (to_plane) k3_plane_copy<T, true><<<grd, dim3(TX, TY), 0, st>>>(x3, F, dir, first, step, x2, n1, n2, pitch2);
+	else k3_plane_copy<T, false><<<grd, dim3(TX, TY), 0, st>>>(x3, F, dir, first, step, x2, n1, n2, pitch2);
+	CDR_LAUNCH_CHECK();
+	return CDR_OK;
+}
+template int plane_copy<double>(double *, Dims3, int, int, int, int, double *, int, int, int, bool, cudaStream_t);
+template int plane_copy<float>(float *, Dims3, int, int, int, int, float *, int, int, int, bool, cudaStream_t);
+
+// copy_rhs for xxvii_pt (src/3d/relax_planes.cc:43-72 xy, :95-127 xz, :146-178 yz):
+// b2 = b + the couplings to the two neighbouring planes, on the plane interior,
+// in the reference's operand order.
+template <typename T>
+__global__ void __launch_bounds__(TX *TY) k3_plane_rhs(const T *__restrict__ so, const T *__restrict__ x,
+                                                       const T *__restrict__ bb, Dims3 F, int dir, int first, int step,
+                                                       T *__restrict__ b2, int n1, int n2, int pitch2)
+{
+	const int p = blockIdx.x * TX + threadIdx.x + 1, q = blockIdx.y * TY + threadIdx.y + 1;
+	const int ipl = first + 1 + blockIdx.z * step;
+	if (p > n1 || q > n2) return;
+	const size_t P = F.plane();
+#define X3(a, i, j, k) a[o3(F, i, j, k)]
+#define S3(pl, i, j, k) so[(size_t)((pl)-1) * P + o3(F, i, j, k)]
+	T v;
+	if (dir == 0) {
+		const int i = p, j = q, k = ipl;
+		v = X3(bb, i, j, k) + S3(KB, i, j, k) * X3(x, i, j, k - 1) + S3(KBW, i, j, k) * X3(x, i - 1, j, k - 1)
+		    + S3(KBNW, i, j + 1, k) * X3(x, i - 1, j + 1, k - 1) + S3(KBN, i, j + 1, k) * X3(x, i, j + 1, k - 1)
+		    + S3(KBNE, i + 1, j + 1, k) * X3(x, i + 1, j + 1, k - 1) + S3(KBE, i + 1, j, k) * X3(x, i + 1, j, k - 1)
+		    + S3(KBSE, i + 1, j, k) * X3(x, i + 1, j - 1, k - 1) + S3(KBS, i, j, k) * X3(x, i, j - 1, k - 1)
+		    + S3(KBSW, i, j, k) * X3(x, i - 1, j - 1, k - 1) + S3(KBE, i, j, k + 1) * X3(x, i - 1, j, k + 1)
+		    + S3(KBSE, i, j + 1, k + 1) * X3(x, i - 1, j + 1, k + 1) + S3(KBS, i, j + 1, k + 1) * X3(x, i, j + 1, k + 1)
+		    + S3(KBSW, i + 1, j + 1, k + 1) * X3(x, i + 1, j + 1, k + 1) + S3(KBW, i + 1, j, k + 1) * X3(x, i + 1, j, k + 1)
+		    + S3(KB, i, j, k + 1) * X3(x, i, j, k + 1) + S3(KBNW, i + 1, j, k + 1) * X3(x, i + 1, j - 1, k + 1)
+		    + S3(KBN, i, j, k + 1) * X3(x, i, j - 1, k + 1) + S3(KBNE, i, j, k + 1) * X3(x, i - 1, j - 1, k + 1);
+	} else if (dir == 1) {
+		const int i = p, k = q, j = ipl;
+		v = X3(bb, i, j, k) + S3(KPNW, i, j + 1, k) * X3(x, i - 1, j + 1, k) + S3(KPS, i, j + 1, k) * X3(x, i, j + 1, k)
+		    + S3(KPSW, i + 1, j + 1, k) * X3(x, i + 1, j + 1, k) + S3(KBNW, i, j + 1, k) * X3(x, i - 1, j + 1, k - 1)
+		    + S3(KBN, i, j + 1, k) * X3(x, i, j + 1, k - 1) + S3(KBNE, i + 1, j + 1, k) * X3(x, i + 1, j + 1, k - 1)
+		    + S3(KBSE, i, j + 1, k + 1) * X3(x, i - 1, j + 1, k + 1) + S3(KBS, i, j + 1, k + 1) * X3(x, i, j + 1, k + 1)
+		    + S3(KBSW, i + 1, j + 1, k + 1) * X3(x, i + 1, j + 1, k + 1) + S3(KPSW, i, j, k) * X3(x, i - 1, j - 1, k)
+		    + S3(KPS, i, j, k) * X3(x, i, j - 1, k) + S3(KPNW, i + 1, j, k) * X3(x, i + 1, j - 1, k)
+		    + S3(KBSW, i, j, k) * X3(x, i - 1, j - 1, k - 1) + S3(KBS, i, j, k) * X3(x, i, j - 1, k - 1)
+		    + S3(KBSE, i + 1, j, k) * X3(x, i + 1, j - 1, k - 1) + S3(KBNE, i, j, k + 1) * X3(x, i - 1, j - 1, k + 1)
+		    + S3(KBN, i, j, k + 1) * X3(x, i, j - 1, k + 1) + S3(KBNW, i + 1, j, k + 1) * X3(x, i + 1, j - 1, k + 1);
+	} else {
+		const int j = p, k = q, i = ipl;
+		v = X3(bb, i, j, k) + S3(KPNW, i, j + 1, k) * X3(x, i - 1, j + 1, k) + S3(KPW, i, j, k) * X3(x, i - 1, j, k)
+		    + S3(KPSW, i, j, k) * X3(x, i - 1, j - 1, k) + S3(KBNW, i, j + 1, k) * X3(x, i - 1, j + 1, k - 1)
+		    + S3(KBW, i, j, k) * X3(x, i - 1, j, k - 1) + S3(KBSW, i, j, k) * X3(x, i - 1, j - 1, k - 1)
+		    + S3(KBSE, i, j + 1, k + 1) * X3(x, i - 1, j + 1, k + 1) + S3(KBE, i, j, k + 1) * X3(x, i - 1, j, k + 1)
+		    + S3(KBNE, i, j, k + 1) * X3(x, i - 1, j - 1, k + 1) + S3(KPSW, i + 1, j + 1, k) * X3(x, i + 1, j + 1, k)
+		    + S3(KPW, i + 1, j, k) * X3(x, i + 1, j, k) + S3(KPNW, i + 1, j, k) * X3(x, i + 1, j - 1, k)
+		    + S3(KBNE, i + 1, j + 1, k) * X3(x, i + 1, j + 1, k - 1) + S3(KBE, i + 1, j, k) * X3(x, i + 1, j, k - 1)
+		    + S3(KBSE, i + 1, j, k) * X3(x, i + 1, j - 1, k - 1) + S3(KBSW, i + 1, j + 1, k + 1) * X3(x, i + 1, j + 1, k + 1)
+		    + S3(KBW, i + 1, j, k + 1) * X3(x, i + 1, j, k + 1) + S3(KBNW, i + 1, j, k + 1) * X3(x, i + 1, j - 1, k + 1);
+	}
+#undef X3
+#undef S3
+	b2[(size_t)(ipl - 1) * pitch2 * (n2 + 2) + (size_t)q * pitch2 + p] = v;
+}
+
+template <typename T>
+int plane_rhs(const T *so, const T *x, const T *b, Dims3 F, int dir, int first, int step, int count, T *b2, int n1,
+              int n2, int pitch2, cudaStream_t st)
+{
+	k3_plane_rhs<T><<<dim3(ceil_div(n1, TX), ceil_div(n2, TY), count), dim3(TX, TY), 0, st>>>(so, x, b, F, dir, first,
+	                                                                                          step, b2, n1, n2, pitch2);
+	CDR_LAUNCH_CHECK();
+	return CDR_OK;
+}
+template int plane_rhs<double>(const double *, const double *, const double *, Dims3, int, int, int, int, double *,
+                               int, int, int, cudaStream_t);
+template int plane_rhs<float>(const float *, const float *, const float *, Dims3, int, int, int, int, float *, int,
+                              int, int, cudaStream_t);
+
+int plane_coeff(const double *so, Dims3 F, int dir, double *so2, int n, int n1, int n2, int pitch2, cudaStream_t st)
+{
+	CDR_CUDA_TRY(cudaMemsetAsync(so2, 0, sizeof(double) * 5 * (size_t)pitch2 * (n2 + 2) * n, st));
+	k3_plane_coeff<<<dim3(ceil_div(n1 + 2, TX), ceil_div(n2 + 2, TY), n), dim3(TX, TY), 0, st>>>(so, F, dir, so2, n1,
+	                                                                                            n2, pitch2);
+	CDR_LAUNCH_CHECK();
+	return CDR_OK;
+}
+
+}  // namespace cdrgpu

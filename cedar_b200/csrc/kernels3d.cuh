@@ -9,6 +9,13 @@
 
 namespace cdrgpu {
 
+// stencil planes p pw ps b psw pnw bw bnw bn bne be bse bs bsw (1-based, as the
+// reference's kp .. kbsw, src/3d/ftn/BMG_stencils_f90.h:46-48) and the 26
+// interpolation planes lxyl .. ltse
+enum : int { KP = 1, KPW, KPS, KB, KPSW, KPNW, KBW, KBNW, KBN, KBNE, KBE, KBSE, KBS, KBSW };
+enum : int { LXYL = 1, LXYR, LXYA, LXYB, LXZA, LXZB, LXYNE, LXYSE, LXYSW, LXYNW, LXZSW, LXZNW, LXZNE, LXZSE,
+             LYZSW, LYZNW, LYZNE, LYZSE, LBSW, LBNW, LBNE, LBSE, LTSW, LTNW, LTNE, LTSE };
+
 struct Dims3 {
 	int nx, ny, nz, pitch;
 	__host__ __device__ size_t slice() const { return (size_t)pitch * (ny + 2); }
@@ -37,6 +44,16 @@ template <typename T>
 int solve_cg_3d(const double *abd, T *x, const T *b, Dims3 d, cudaStream_t st);
 int ir_residual_3d(const double *so, const double *x, const float *e, const double *b, double *xo, float *r32,
                    Dims3 d, Dims3 d32, double *norm_out, double *partial, int apply, cudaStream_t st);
+
+// Plane relaxation data movement (dir 0 = xy, 1 = xz, 2 = yz); plane problems
+// are (n1, n2) grids of row pitch pitch2, problem ipl-1 for plane ipl.
+int plane_coeff(const double *so, Dims3 F, int dir, double *so2, int n, int n1, int n2, int pitch2, cudaStream_t st);
+template <typename T>
+int plane_copy(T *x3, Dims3 F, int dir, int first, int step, int count, T *x2, int n1, int n2, int pitch2,
+               bool to_plane, cudaStream_t st);
+template <typename T>
+int plane_rhs(const T *so, const T *x, const T *b, Dims3 F, int dir, int first, int step, int count, T *b2, int n1,
+              int n2, int pitch2, cudaStream_t st);
 
 // rows of the banded coarse-grid factor: KD + 1 with KD = nx*(ny+1) + 1
 inline int cg3_ldab(Dims3 d) { return d.nx * (d.ny + 1) + 2; }

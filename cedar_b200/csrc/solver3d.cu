@@ -1,5 +1,5 @@
-// solver3d.cu -- 3D BoxMG multilevel solver on the device (27-point operators,
-// 8-colour point Gauss-Seidel).
+// solver3d.cu -- 3D BoxMG multilevel solver on the device (27-point operators;
+// 8-colour point Gauss-Seidel or plane relaxation).
 //
 // Host control mirrors cdr3::solver over Cedar's multilevel driver: setup builds
 // interpolation, Galerkin operator and smoother level by level and factors the
@@ -8,10 +8,20 @@
 // the solve loop with its relative l2 stopping test is multilevel::solve
 // (multilevel.h:278-298).  As in 2D the cycle is captured once as a CUDA graph
 // and replayed; CDR_PREC_F32_IR runs FP32 cycles inside FP64 refinement.
+//
+// Plane relaxation (planes<rdir>, include/cedar/3d/relax_planes.h:35-234): every
+// level but the coarsest keeps, per direction, one 2D hierarchy per plane (a
+// Batch2 of all planes of the level).  A sweep relaxes the odd planes, then the
+// even ones (reversed going up); each colour is one batched pass: gather the
+// planes' x and right-hand sides (b plus the couplings to the neighbouring
+// planes), one 2D V-cycle of line-xy smoothing on every plane of the colour, and
+// scatter x back.  The planes of one colour couple only through planes of the
+// other colour, so the batched pass equals the reference's plane-by-plane loop.
+#include <memory>
 #include <vector>
 #include <cmath>
 
-#include "kernels2d.cuh"
+#include "batch2d.cuh"
 #include "kernels3d.cuh"
 
 using namespace cdrgpu;
@@ -23,6 +33,7 @@ inline int round_up3(int v, int m) { return (v + m - 1) / m * m; }
 struct Level3 {
 	int nx = 0, ny = 0, nz = 0;
 	Dims3 d{};
+	std::unique_ptr<Batch2> pl[3];  // plane problems: xy, xz, yz
 	double *so = nullptr, *x = nullptr, *b = nullptr, *r = nullptr, *sor = nullptr, *ci = nullptr;
 	float *so32 = nullptr, *x32 = nullptr, *b32 = nullptr, *r32 = nullptr, *sor32 = nullptr, *ci32 = nullptr;
 };
@@ -79,12 +90,54 @@ struct cdr_gpu_solver3 {
 	bool mixed() const { return s.precision == CDR_PREC_F32_IR; }
 	int L() const { return (int)lv.size(); }
 
+	bool plane(int dir) const
+	{
+		const int r = s.relaxation;
+		return r == CDR_RELAX_PLANE_XYZ || r == CDR_RELAX_PLANE_XY + dir;
+	}
+
+	// relax_planes (include/cedar/3d/relax_planes.h:35-70) for one direction
+	template <typename T>
+	int relax_planes(int l, int dir, T *x, const T *b, int updown)
+	{
+		Level3 &F = lv[l];
+		Batch2 &P = *F.pl[dir];
+		B2Level &P0 = P.lv[0];
+		T *x2 = sizeof(T) == 8 ? (T *)P0.x : (T *)P0.x32;
+		T *b2 = sizeof(T) == 8 ? (T *)P0.b : (T *)P0.b32;
+		const int n = P.nb;
+		for (int c = 0; c < 2; ++c) {
+			// DOWN: odd planes (1, 3, ...) first; UP: even planes first
+			const int beg = (updown == CDR_DOWN) == (c == 0) ? 1 : 2;
+			if (beg > n) continue;
+			const Sel sel{beg - 1, 2, (n - beg) / 2 + 1};
+			CDR_TRY(plane_copy<T>(x, F.d, dir, sel.first, 2, sel.count, x2, P0.nx, P0.ny, P0.pitch, true, st));
+			CDR_TRY(plane_rhs<T>(Arr3<T>::so(F), x, b, F.d, dir, sel.first, 2, sel.count, b2, P0.nx, P0.ny, P0.pitch,
+			                     st));
+			CDR_TRY(P.cycle<T>(sel));
+			CDR_TRY(plane_copy<T>(x, F.d, dir, sel.first, 2, sel.count, x2, P0.nx, P0.ny, P0.pitch, false, st));
+		}
+		return CDR_OK;
+	}
+
+	// multilevel::setup_relax_helper closures (include/cedar/multilevel.h:160-222):
+	// plane-xyz runs xy, yz, xz going down and xz, yz, xy going up
 	template <typename T>
 	int smooth(int l, T *x, const T *b, int updown)
 	{
 		Level3 &F = lv[l];
 		const int n = updown == CDR_DOWN ? s.nrelax_pre : s.nrelax_post;
-		for (int it = 0; it < n; ++it) CDR_TRY(relax_point_3d<T>(Arr3<T>::so(F), x, b, Arr3<T>::sor(F), F.d, updown, st));
+		static const int down[3] = {0, 2, 1}, up[3] = {1, 2, 0};
+		for (int it = 0; it < n; ++it) {
+			if (s.relaxation == CDR_RELAX_POINT) {
+				CDR_TRY(relax_point_3d<T>(Arr3<T>::so(F), x, b, Arr3<T>::sor(F), F.d, updown, st));
+				continue;
+			}
+			for (int q = 0; q < 3; ++q) {
+				const int dir = updown == CDR_DOWN ? down[q] : up[q];
+				if (plane(dir)) CDR_TRY(relax_planes<T>(l, dir, x, b, updown));
+			}
+		}
 		return CDR_OK;
 	}
 
@@ -150,7 +203,18 @@ struct cdr_gpu_solver3 {
 			CDR_TRY(setup_interp_3d(F.so, C.ci, F.d, C.d, st));
 			CDR_TRY(galerkin_3d(F.so, C.ci, C.so, F.d, C.d, st));
 			CDR_TRY(setup_recip_3d<double>(F.so, F.sor, F.d, st));
+			// plane smoothers: 2D operators from the in-plane couplings, then the 2D setups
+			for (int dir = 0; dir < 3; ++dir) {
+				if (!F.pl[dir]) continue;
+				Batch2 &P = *F.pl[dir];
+				B2Level &P0 = P.lv[0];
+				CDR_TRY(plane_coeff(F.so, F.d, dir, P0.so, P.nb, P0.nx, P0.ny, P0.pitch, st));
+				CDR_TRY(P.setup(false));
+			}
 		}
+		for (int l = 0; l + 1 < L(); ++l)
+			for (int dir = 0; dir < 3; ++dir)
+				if (lv[l].pl[dir]) CDR_TRY(lv[l].pl[dir]->check_info());
 		Level3 &Cg = lv[L() - 1];
 		CDR_TRY(setup_cg_3d(Cg.so, Cg.d, abd, info, st));
 		if (mixed()) {
@@ -215,6 +279,21 @@ static int create3(cdr_gpu_solver3 *h, const double *so_src, int src_pitch, cuda
 		CDR_TRY(h->alloc(&L.r, pl));
 		if (l > 0) CDR_TRY(h->alloc(&L.ci, pl * 26));
 		if (l + 1 < nl) CDR_TRY(h->alloc(&L.sor, pl));
+		// plane problems of this level: the reference's plane config (line-xy,
+		// max-iter 1, other keys at their defaults; src/kernel_params.cc:83-89)
+		for (int dir = 0; dir < 3 && l + 1 < nl; ++dir) {
+			if (!h->plane(dir)) continue;
+			cdr_gpu_settings s2;
+			cdr_gpu_settings_default(&s2);
+			s2.relaxation = CDR_RELAX_LINE_XY;
+			s2.maxiter = 1;
+			s2.precision = s.precision;
+			s2.line_flags = s.line_flags;
+			const int np = dir == 0 ? L.nz : dir == 1 ? L.ny : L.nx;
+			const int n1 = dir == 2 ? L.ny : L.nx, n2 = dir == 0 ? L.ny : L.nz;
+			L.pl[dir].reset(new Batch2());
+			CDR_TRY(L.pl[dir]->init(s2, 5, n1, n2, np, h->st));
+		}
 		if (h->mixed()) {
 			CDR_TRY(h->alloc(&L.so32, pl * 14));
 			CDR_TRY(h->alloc(&L.x32, pl));
@@ -312,6 +391,8 @@ int cdr_gpu_solver3_destroy(cdr_gpu_solver3 *h)
 	if (h->st) cudaStreamSynchronize(h->st);
 	for (auto &g : h->gexec)
 		if (g) cudaGraphExecDestroy(g);
+	for (auto &L : h->lv)  // plane batches before the stream they use
+		for (auto &p : L.pl) p.reset();
 	for (void *p : h->allocs) cudaFree(p);
 	if (h->h_norm) cudaFreeHost(h->h_norm);
 	if (h->ev0) cudaEventDestroy(h->ev0);
@@ -327,8 +408,8 @@ static int create3_any(const cdr_gpu_settings *s, const double *so_src, int src_
 	if (!s || !so_src || !out) { set_error(CDR_ERR_ARG, "null argument"); return CDR_ERR_ARG; }
 	*out = nullptr;
 	if (nx < 1 || ny < 1 || nz < 1) { set_error(CDR_ERR_DIM, "bad grid %dx%dx%d", nx, ny, nz); return CDR_ERR_DIM; }
-	if (s->relaxation != CDR_RELAX_POINT) {
-		set_error(CDR_ERR_UNSUPPORTED, "3D solver: only point relaxation is implemented (got %d)", s->relaxation);
+	if (s->relaxation != CDR_RELAX_POINT && (s->relaxation < CDR_RELAX_PLANE_XY || s->relaxation > CDR_RELAX_PLANE_XYZ)) {
+		set_error(CDR_ERR_UNSUPPORTED, "3D solver: point or plane relaxation (got %d)", s->relaxation);
 		return CDR_ERR_UNSUPPORTED;
 	}
 	if (s->precision != CDR_PREC_F64 && s->precision != CDR_PREC_F32_IR) {

@@ -21,9 +21,11 @@ from .config import Config, MLSettings
 PLANE_NAMES = {"so": 0, "x": 1, "b": 2, "res": 3, "sor": 4, "sory": 5, "ci": 6}
 
 
-def _settings(ms: MLSettings):
-    if ms.relaxation not in _lib.RELAX:
+def _settings(ms: MLSettings, dim=2):
+    if dim == 2 and ms.relaxation.startswith("plane"):
         raise NotImplementedError("relaxation %r is a 3D smoother" % ms.relaxation)
+    if dim == 3 and ms.relaxation.startswith("line"):
+        raise NotImplementedError("relaxation %r is a 2D smoother (3D: point or plane-*)" % ms.relaxation)
     if ms.cycle != "v":
         raise NotImplementedError("only the V-cycle is implemented on the GPU")
     if ms.coarse_solver != "LU":
@@ -141,10 +143,7 @@ class Solver3D:
         dims = (nx, ny, nz) and the row pitch of the device array."""
         self.lib = _lib.load()
         self.settings = conf if isinstance(conf, MLSettings) else MLSettings(conf)
-        if self.settings.relaxation != "point":
-            raise NotImplementedError("3D relaxation %r: only point relaxation runs on the GPU"
-                                      % self.settings.relaxation)
-        self._s = _settings(self.settings)
+        self._s = _settings(self.settings, dim=3)
         h = ctypes.c_void_p()
         if dims is not None:
             self.nx, self.ny, self.nz = dims

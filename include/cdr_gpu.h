@@ -46,6 +46,10 @@ extern "C" {
 #define CDR_RELAX_LINE_X  1
 #define CDR_RELAX_LINE_Y  2
 #define CDR_RELAX_LINE_XY 3
+#define CDR_RELAX_PLANE_XY  4  /* 3D: plane relaxation (include/cedar/3d/relax_planes.h) */
+#define CDR_RELAX_PLANE_XZ  5
+#define CDR_RELAX_PLANE_YZ  6
+#define CDR_RELAX_PLANE_XYZ 7
 
 /* Precision of the solve. */
 #define CDR_PREC_F64    0  /* plain FP64 V-cycles: the drop-in path                    */
@@ -313,9 +317,10 @@ int cdr_gpu_solve_cg_3d_f64(const double *abd, double *x, const double *b, int n
                             cudaStream_t stream);
 
 /* ------------------------------------------------------------------------
- * 3D multilevel solver (cdr3::solver, include/cedar/3d/solver.h): point
- * relaxation, 27-point fine operator.  Same settings struct as 2D
- * (relaxation must be CDR_RELAX_POINT; line_flags is ignored).
+ * 3D multilevel solver (cdr3::solver, include/cedar/3d/solver.h), 27-point fine
+ * operator.  Same settings struct as 2D; relaxation CDR_RELAX_POINT (8-colour
+ * Gauss-Seidel) or CDR_RELAX_PLANE_* (one 2D line-xy V-cycle per plane, red-black
+ * over planes; line_flags applies to those 2D cycles).
  * ------------------------------------------------------------------------ */
 typedef struct cdr_gpu_solver3 cdr_gpu_solver3;
 
