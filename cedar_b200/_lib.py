@@ -113,6 +113,12 @@ def load(path=LIB_PATH):
         "cdr_gpu_solver3_level": (I, [P, I, I, ctypes.POINTER(P)] + [ctypes.POINTER(I)] * 4),
         "cdr_gpu_solver3_level_get": (I, [P, I, I, P, Z]),
         "cdr_gpu_solver3_timings": (I, [P, ctypes.POINTER(D), ctypes.POINTER(D)]),
+        # batches of 2D problems
+        "cdr_gpu_batch2d_create": (I, [ctypes.POINTER(Settings), P, I, I, I, I, I, S, ctypes.POINTER(P)]),
+        "cdr_gpu_batch2d_destroy": (I, [P]),
+        "cdr_gpu_batch2d_solve_device": (I, [P, P, P, I, P, P, P]),
+        "cdr_gpu_batch2d_nlevels": (I, [P]),
+        "cdr_gpu_batch2d_timings": (I, [P, ctypes.POINTER(D), ctypes.POINTER(D)]),
     })
     for name, (res, args) in sig.items():
         f = getattr(L, name)

@@ -1,4 +1,6 @@
 // batch2d.cu -- batched 2D BoxMG hierarchies (see batch2d.cuh).
+#include <cmath>
+
 #include "batch2d.cuh"
 
 namespace cdrgpu {
@@ -240,3 +242,268 @@ template int Batch2::cycle<double>(Sel);
 template int Batch2::cycle<float>(Sel);
 
 }  // namespace cdrgpu
+
+// ------------------------------------------------------------- C ABI: batches
+namespace cdrgpu {
+namespace {
+
+// dst[p] = src[p] for the problems whose flag is set (grid z = problem)
+__global__ void k_masked_copy(const double *__restrict__ src, double *__restrict__ dst, size_t per,
+                              const int *__restrict__ flag)
+{
+	if (!flag[blockIdx.z]) return;
+	const size_t o = (size_t)blockIdx.z * per;
+	for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < per; e += (size_t)gridDim.x * blockDim.x)
+		dst[o + e] = src[o + e];
+}
+
+}  // namespace
+}  // namespace cdrgpu
+
+using namespace cdrgpu;
+
+struct cdr_gpu_batch2d {
+	Batch2 B;
+	cudaStream_t st = nullptr;
+	bool own_stream = false;
+	std::vector<void *> allocs;
+	double *x64[2] = {nullptr, nullptr};  // FP64 iterates (ping-pong in the refinement loop)
+	double *norm = nullptr, *partial = nullptr;
+	int *active = nullptr;                // device: 1 while the problem iterates
+	double *h_norm = nullptr;             // pinned host copy of the norms
+	int *h_active = nullptr;              // pinned host copy of the flags
+	cudaGraphExec_t gexec[2] = {nullptr, nullptr};
+	long long glaunches[2] = {0, 0};
+	std::vector<cudaEvent_t> ev;          // ev[0] start, ev[k] after iteration k
+	float setup_ms = 0.f, solve_ms = 0.f;
+
+	template <typename T>
+	int alloc(T **p, size_t n)
+	{
+		void *q = nullptr;
+		CDR_CUDA_TRY(cudaMalloc(&q, n * sizeof(T) + 256));
+		CDR_CUDA_TRY(cudaMemsetAsync(q, 0, n * sizeof(T) + 256, st));
+		allocs.push_back(q);
+		*p = (T *)q;
+		return CDR_OK;
+	}
+
+	int run_cycle(int prec)
+	{
+		const Sel all{0, 1, B.nb};
+		auto body = [&]() -> int { return prec == 0 ? B.cycle<double>(all) : B.cycle<float>(all); };
+		if (!B.s.use_graph) return body();
+		if (!gexec[prec]) {
+			cudaGraph_t g = nullptr;
+			CDR_CUDA_TRY(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+			const long long before = cdr_gpu_launch_count();
+			int rc = body();
+			glaunches[prec] = cdr_gpu_launch_count() - before;
+			count_launches(-glaunches[prec]);
+			cudaError_t e = cudaStreamEndCapture(st, &g);
+			if (rc != CDR_OK) {
+				if (g) cudaGraphDestroy(g);
+				return rc;
+			}
+			if (e != cudaSuccess) {
+				set_error(CDR_ERR_CUDA, "graph capture: %s", cudaGetErrorString(e));
+				return CDR_ERR_CUDA;
+			}
+			CDR_CUDA_TRY(cudaGraphInstantiate(&gexec[prec], g, 0));
+			cudaGraphDestroy(g);
+		}
+		CDR_CUDA_TRY(cudaGraphLaunch(gexec[prec], st));
+		count_launches(glaunches[prec]);
+		return CDR_OK;
+	}
+};
+
+extern "C" {
+
+int cdr_gpu_batch2d_destroy(cdr_gpu_batch2d *h)
+{
+	if (!h) return CDR_ERR_HANDLE;
+	if (h->st) cudaStreamSynchronize(h->st);
+	for (auto &g : h->gexec)
+		if (g) cudaGraphExecDestroy(g);
+	for (auto &e : h->ev) cudaEventDestroy(e);
+	for (void *p : h->allocs) cudaFree(p);
+	if (h->h_norm) cudaFreeHost(h->h_norm);
+	if (h->h_active) cudaFreeHost(h->h_active);
+	cudaStream_t st = h->st;
+	const bool own = h->own_stream;
+	delete h;  // frees the batch arrays
+	if (own && st) cudaStreamDestroy(st);
+	return CDR_OK;
+}
+
+int cdr_gpu_batch2d_create(const cdr_gpu_settings *s, const double *so_dev, int ns, int nx, int ny, int pitch, int nb,
+                           cudaStream_t stream, cdr_gpu_batch2d **out)
+{
+	if (!s || !so_dev || !out) { set_error(CDR_ERR_ARG, "null argument"); return CDR_ERR_ARG; }
+	*out = nullptr;
+	if (ns != 3 && ns != 5) { set_error(CDR_ERR_ARG, "nstencil must be 3 or 5"); return CDR_ERR_ARG; }
+	if (nx < 1 || ny < 1 || pitch < nx + 2) {
+		set_error(CDR_ERR_DIM, "bad grid %dx%d pitch %d", nx, ny, pitch);
+		return CDR_ERR_DIM;
+	}
+	if (s->relaxation < CDR_RELAX_POINT || s->relaxation > CDR_RELAX_LINE_XY) {
+		set_error(CDR_ERR_ARG, "invalid 2D relaxation %d", s->relaxation);
+		return CDR_ERR_ARG;
+	}
+	if (s->precision != CDR_PREC_F64 && s->precision != CDR_PREC_F32_IR) {
+		set_error(CDR_ERR_ARG, "invalid precision %d", s->precision);
+		return CDR_ERR_ARG;
+	}
+	if (s->maxiter < 1) { set_error(CDR_ERR_ARG, "max-iter must be positive"); return CDR_ERR_ARG; }
+	cdr_gpu_batch2d *h = new cdr_gpu_batch2d();
+	if (stream) h->st = stream;
+	else {
+		if (cudaStreamCreateWithFlags(&h->st, cudaStreamNonBlocking) != cudaSuccess) {
+			set_error(CDR_ERR_CUDA, "cannot create stream");
+			delete h;
+			return CDR_ERR_CUDA;
+		}
+		h->own_stream = true;
+	}
+	auto fail = [&](int rc) {
+		cdr_gpu_batch2d_destroy(h);
+		return rc;
+	};
+	int rc = lines_prepare();
+	if (rc == CDR_OK) rc = h->B.init(*s, ns, nx, ny, nb, h->st);
+	if (rc != CDR_OK) return fail(rc);
+	B2Level &F = h->B.lv[0];
+	const size_t pl = F.plane();
+	const int per = norm_blocks(F.dims(Sel{0, 1, nb}));
+	if ((rc = h->alloc(&h->x64[0], pl * nb)) || (rc = h->alloc(&h->x64[1], pl * nb)) ||
+	    (rc = h->alloc(&h->norm, (size_t)nb)) || (rc = h->alloc(&h->partial, (size_t)per * nb)) ||
+	    (rc = h->alloc(&h->active, (size_t)nb)))
+		return fail(rc);
+	if (cudaMallocHost(&h->h_norm, sizeof(double) * nb) != cudaSuccess ||
+	    cudaMallocHost(&h->h_active, sizeof(int) * nb) != cudaSuccess) {
+		set_error(CDR_ERR_CUDA, "cannot allocate pinned host buffers");
+		return fail(CDR_ERR_CUDA);
+	}
+	h->ev.resize(s->maxiter + 2);
+	for (auto &e : h->ev)
+		if (cudaEventCreate(&e) != cudaSuccess) {
+			e = nullptr;
+			set_error(CDR_ERR_CUDA, "cannot create events");
+			return fail(CDR_ERR_CUDA);
+		}
+	// fine operators (caller pitch) -> batch layout; rows of all problems are contiguous in both
+	if (cudaMemcpy2DAsync(F.so, F.pitch * sizeof(double), so_dev, pitch * sizeof(double), (nx + 2) * sizeof(double),
+	                      (size_t)(ny + 2) * ns * nb, cudaMemcpyDeviceToDevice, h->st) != cudaSuccess) {
+		set_error(CDR_ERR_CUDA, "operator copy failed");
+		return fail(CDR_ERR_CUDA);
+	}
+	if (cudaEventRecord(h->ev[0], h->st) != cudaSuccess) return fail(CDR_ERR_CUDA);
+	rc = h->B.setup(true);
+	if (rc != CDR_OK) return fail(rc);
+	if (cudaEventRecord(h->ev[1], h->st) != cudaSuccess || cudaEventSynchronize(h->ev[1]) != cudaSuccess ||
+	    cudaEventElapsedTime(&h->setup_ms, h->ev[0], h->ev[1]) != cudaSuccess) {
+		set_error(CDR_ERR_CUDA, "setup timing events failed");
+		return fail(CDR_ERR_CUDA);
+	}
+	*out = h;
+	return CDR_OK;
+}
+
+// multilevel::solve (include/cedar/multilevel.h:278-298) for every problem of the
+// batch: each stops at its own relative tolerance (its iterate no longer changes
+// after that), iters/rel/done_ms (host arrays of nb, done_ms may be null) report
+// its cycles, final relative l2 residual and the time from the start of the
+// solve to its last cycle.
+int cdr_gpu_batch2d_solve_device(cdr_gpu_batch2d *h, const double *b_dev, double *x_dev, int pitch, int *iters,
+                                 double *rel, float *done_ms)
+{
+	if (!h) { set_error(CDR_ERR_HANDLE, "null batch"); return CDR_ERR_HANDLE; }
+	if (!b_dev || !x_dev || !iters || !rel) { set_error(CDR_ERR_ARG, "null argument"); return CDR_ERR_ARG; }
+	Batch2 &B = h->B;
+	B2Level &F = B.lv[0];
+	if (pitch < F.nx + 2) { set_error(CDR_ERR_DIM, "pitch %d < nx+2", pitch); return CDR_ERR_DIM; }
+	const int nb = B.nb;
+	const cudaStream_t st = h->st;
+	const Sel all{0, 1, nb};
+	const Dims2 d = F.dims(all);
+	const size_t pl = F.plane(), w = (F.nx + 2) * sizeof(double), rows = (size_t)(F.ny + 2) * nb;
+	const bool mixed = B.mixed();
+	std::vector<double> res0(nb);
+	std::vector<int> last(nb, 0);
+	for (int p = 0; p < nb; ++p) { iters[p] = 0; rel[p] = 1.0; h->h_active[p] = 1; }
+	CDR_CUDA_TRY(cudaMemcpy2DAsync(F.b, F.pitch * sizeof(double), b_dev, pitch * sizeof(double), w, rows,
+	                               cudaMemcpyDeviceToDevice, st));
+	double *xw = mixed ? h->x64[0] : F.x;  // the iterate the cycles update
+	CDR_CUDA_TRY(cudaMemcpy2DAsync(xw, F.pitch * sizeof(double), x_dev, pitch * sizeof(double), w, rows,
+	                               cudaMemcpyDeviceToDevice, st));
+	if (!mixed)
+		CDR_CUDA_TRY(cudaMemcpyAsync(h->x64[0], F.x, sizeof(double) * pl * nb, cudaMemcpyDeviceToDevice, st));
+	CDR_CUDA_TRY(cudaMemcpyAsync(h->active, h->h_active, sizeof(int) * nb, cudaMemcpyHostToDevice, st));
+	CDR_CUDA_TRY(cudaEventRecord(h->ev[0], st));
+	if (mixed) CDR_TRY(ir_residual_2d(F.so, F.ns, h->x64[0], F.x32, F.b, h->x64[1], F.b32, d, d, h->norm, h->partial, 0, st));
+	else CDR_TRY(residual_2d<double>(F.so, F.ns, F.x, F.b, F.r, d, h->norm, h->partial, st));
+	CDR_CUDA_TRY(cudaMemcpyAsync(h->h_norm, h->norm, sizeof(double) * nb, cudaMemcpyDeviceToHost, st));
+	CDR_CUDA_TRY(cudaStreamSynchronize(st));
+	for (int p = 0; p < nb; ++p) res0[p] = h->h_norm[p];
+	int cur = 0, nactive = nb, it = 0, bad = 0;
+	const dim3 cgrid(ceil_div((long)pl, 256) < 256 ? ceil_div((long)pl, 256) : 256, 1, nb);
+	for (it = 0; it < B.s.maxiter && nactive > 0; ++it) {
+		if (mixed) {
+			CDR_CUDA_TRY(cudaMemsetAsync(F.x32, 0, sizeof(float) * pl * nb, st));
+			CDR_TRY(h->run_cycle(1));
+			CDR_TRY(ir_residual_2d(F.so, F.ns, h->x64[cur], F.x32, F.b, h->x64[1 - cur], F.b32, d, d, h->norm,
+			                       h->partial, 1, st, h->active));
+			cur = 1 - cur;
+		} else {
+			CDR_TRY(h->run_cycle(0));
+			CDR_TRY(residual_2d<double>(F.so, F.ns, F.x, F.b, F.r, d, h->norm, h->partial, st));
+			// keep the iterate of every problem still iterating
+			k_masked_copy<<<cgrid, 256, 0, st>>>(F.x, h->x64[0], pl, h->active);
+			CDR_LAUNCH_CHECK();
+		}
+		CDR_CUDA_TRY(cudaEventRecord(h->ev[it + 1], st));
+		CDR_CUDA_TRY(cudaMemcpyAsync(h->h_norm, h->norm, sizeof(double) * nb, cudaMemcpyDeviceToHost, st));
+		CDR_CUDA_TRY(cudaStreamSynchronize(st));
+		for (int p = 0; p < nb; ++p) {
+			if (!h->h_active[p]) continue;
+			const double r = h->h_norm[p] / res0[p];
+			iters[p] = it + 1;
+			rel[p] = r;
+			last[p] = it + 1;
+			if (!std::isfinite(r)) bad = 1;
+			if (!(r >= B.s.tol)) {  // converged (or not finite): stop this problem
+				h->h_active[p] = 0;
+				--nactive;
+			}
+		}
+		CDR_CUDA_TRY(cudaMemcpyAsync(h->active, h->h_active, sizeof(int) * nb, cudaMemcpyHostToDevice, st));
+	}
+	CDR_CUDA_TRY(cudaMemcpy2DAsync(x_dev, pitch * sizeof(double), mixed ? h->x64[cur] : h->x64[0],
+	                               F.pitch * sizeof(double), w, rows, cudaMemcpyDeviceToDevice, st));
+	CDR_CUDA_TRY(cudaStreamSynchronize(st));
+	CDR_CUDA_TRY(cudaEventElapsedTime(&h->solve_ms, h->ev[0], h->ev[it > 0 ? it : 0]));
+	if (done_ms)
+		for (int p = 0; p < nb; ++p) {
+			float t = 0.f;
+			if (last[p] > 0) CDR_CUDA_TRY(cudaEventElapsedTime(&t, h->ev[0], h->ev[last[p]]));
+			done_ms[p] = t;
+		}
+	if (bad) {
+		set_error(CDR_ERR_NUMERIC, "non-finite residual norm in a problem of the batch");
+		return CDR_ERR_NUMERIC;
+	}
+	return CDR_OK;
+}
+
+int cdr_gpu_batch2d_timings(const cdr_gpu_batch2d *h, double *setup_ms, double *solve_ms)
+{
+	if (!h) return CDR_ERR_HANDLE;
+	if (setup_ms) *setup_ms = h->setup_ms;
+	if (solve_ms) *solve_ms = h->solve_ms;
+	return CDR_OK;
+}
+
+int cdr_gpu_batch2d_nlevels(const cdr_gpu_batch2d *h) { return h ? h->B.L() : -1; }
+
+}  // extern "C"

@@ -221,3 +221,50 @@ class Solver3D:
                                                          pitch, ctypes.byref(it), hist.ctypes.data, len(hist)))
         self.iters = it.value
         self.history = hist[:it.value].copy()
+
+
+class BatchSolver2D:
+    """A batch of independent 2D problems of one grid size, solved together on
+    the GPU (each with its own stopping test, as ``cdr2::solver::solve``).
+
+    ``so_ptr``: device pointer to nb fine operators back to back (each
+    nstencil planes of ``pitch*(ny+2)`` doubles)."""
+
+    def __init__(self, so_ptr, nstencil, nx, ny, pitch, nb, conf=None, stream=0):
+        self.lib = _lib.load()
+        self.settings = conf if isinstance(conf, MLSettings) else MLSettings(conf)
+        self._s = _settings(self.settings)
+        self.nx, self.ny, self.pitch, self.nb = nx, ny, pitch, nb
+        h = ctypes.c_void_p()
+        _lib.check(self.lib.cdr_gpu_batch2d_create(ctypes.byref(self._s), ctypes.c_void_p(so_ptr), nstencil, nx, ny,
+                                                   pitch, nb, ctypes.c_void_p(stream), ctypes.byref(h)))
+        self.h = h
+        self.iters = np.zeros(nb, dtype=np.int32)
+        self.rel = np.zeros(nb)
+        self.done_ms = np.zeros(nb, dtype=np.float32)
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.cdr_gpu_batch2d_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def nlevels(self):
+        return self.lib.cdr_gpu_batch2d_nlevels(self.h)
+
+    def timings(self):
+        a, b = ctypes.c_double(), ctypes.c_double()
+        _lib.check(self.lib.cdr_gpu_batch2d_timings(self.h, ctypes.byref(a), ctypes.byref(b)))
+        return a.value, b.value
+
+    def solve_device(self, b_ptr, x_ptr, pitch=None):
+        """Solve every problem; x (device, nb grids back to back) holds the initial guesses."""
+        _lib.check(self.lib.cdr_gpu_batch2d_solve_device(
+            self.h, ctypes.c_void_p(b_ptr), ctypes.c_void_p(x_ptr), pitch or self.pitch,
+            self.iters.ctypes.data, self.rel.ctypes.data, self.done_ms.ctypes.data))

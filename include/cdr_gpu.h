@@ -344,6 +344,30 @@ int cdr_gpu_solver3_level(const cdr_gpu_solver3 *h, int level, int which, void *
 int cdr_gpu_solver3_level_get(const cdr_gpu_solver3 *h, int level, int which, void *host, size_t bytes);
 int cdr_gpu_solver3_timings(const cdr_gpu_solver3 *h, double *setup_ms, double *solve_ms);
 
+/* ------------------------------------------------------------------------
+ * Batches of independent 2D problems of one grid size, solved together (every
+ * kernel launch covers the whole batch).  The reference solves such problems
+ * one cdr2::solver at a time (include/cedar/2d/solver.h:45-129); each problem
+ * here follows multilevel::solve (include/cedar/multilevel.h:278-298) with its
+ * own stopping test.  Arrays hold the nb problems back to back: operators nb x
+ * nstencil planes, grid functions nb planes, each plane pitch*(ny+2) elements.
+ * ------------------------------------------------------------------------ */
+typedef struct cdr_gpu_batch2d cdr_gpu_batch2d;
+
+/* Set up nb hierarchies (2D relaxations only) from DEVICE fine operators. */
+int cdr_gpu_batch2d_create(const cdr_gpu_settings *s, const double *so_dev, int nstencil, int nx, int ny, int pitch,
+                           int nb, cudaStream_t stream, cdr_gpu_batch2d **out);
+int cdr_gpu_batch2d_destroy(cdr_gpu_batch2d *h);
+/* Solve all problems from the initial guesses in x_dev.  Host arrays of nb:
+ * iters receives each problem's cycle count, rel its final relative l2
+ * residual, done_ms (may be null) the time from the start of the solve to that
+ * problem's last cycle.  A problem's iterate is final once it has met the
+ * tolerance; the others keep cycling. */
+int cdr_gpu_batch2d_solve_device(cdr_gpu_batch2d *h, const double *b_dev, double *x_dev, int pitch, int *iters,
+                                 double *rel, float *done_ms);
+int cdr_gpu_batch2d_nlevels(const cdr_gpu_batch2d *h);
+int cdr_gpu_batch2d_timings(const cdr_gpu_batch2d *h, double *setup_ms, double *solve_ms);
+
 #ifdef __cplusplus
 }
 #endif
