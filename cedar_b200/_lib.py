@@ -34,7 +34,7 @@ class Settings(ctypes.Structure):
                 ("nrelax_post", ctypes.c_int), ("num_levels", ctypes.c_int),
                 ("maxiter", ctypes.c_int), ("tol", ctypes.c_double),
                 ("min_coarse", ctypes.c_int), ("precision", ctypes.c_int),
-                ("use_graph", ctypes.c_int), ("line_flags", ctypes.c_int)]
+                ("use_graph", ctypes.c_int), ("line_flags", ctypes.c_int), ("fuse_coarse", ctypes.c_int)]
 
 
 def header_symbols():

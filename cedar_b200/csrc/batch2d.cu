@@ -108,6 +108,12 @@ int Batch2::init(const cdr_gpu_settings &settings, int ns, int nx, int ny, int n
 			}
 		}
 	}
+	if (s.fuse_coarse > 0)
+		for (int l = 1; l + 1 < nl && l < kMaxCoarseLevels; ++l)
+			if (lv[l].nx <= s.fuse_coarse && lv[l].ny <= s.fuse_coarse && nl - l <= kMaxCoarseLevels) {
+				lc = l;
+				break;
+			}
 	const B2Level &Cg = lv.back();
 	if ((size_t)Cg.nx * Cg.ny > 4096) {
 		set_error(CDR_ERR_DIM, "coarsest grid %dx%d too large for the banded Cholesky", Cg.nx, Cg.ny);
@@ -221,10 +227,43 @@ int Batch2::ncycle(int l, Sel sel)
 	// zero the selected coarse iterates: rows of cp elements, step*cp apart
 	CDR_CUDA_TRY(cudaMemset2DAsync(xc, sel.step * cp * sizeof(T), 0, cp * sizeof(T), sel.count, st));
 	if (l + 1 == L() - 1) CDR_TRY(solve_cg_2d<T>(abd + f * abd_size(), xc, bc, dc, st));
+	else if (l + 1 == lc) CDR_TRY(fused<T>(l + 1, sel));
 	else CDR_TRY(ncycle<T>(l + 1, sel));
 	CDR_TRY(interp_add_2d<T>(ci, xc, r, so, x, df, dc, st, F.ns));
 	CDR_TRY(smooth<T>(l, sel, CDR_UP));
 	return CDR_OK;
+}
+
+// Levels l0..L-1 of the selected problems in one launch, one CTA per problem
+template <typename T>
+int Batch2::fused(int l0, Sel sel)
+{
+	CoarseCycle<T> cc;
+	cc.nl = L() - l0;
+	const size_t f = sel.first;
+	for (int l = l0; l < L(); ++l) {
+		B2Level &V = lv[l];
+		CoarseLevel<T> &c = cc.lv[l - l0];
+		const size_t pl = V.plane();
+		c.so = BA<T>::so(V) + f * V.ns * pl;
+		c.sor = BA<T>::sor(V) ? BA<T>::sor(V) + f * 2 * pl : nullptr;
+		c.sory = BA<T>::sory(V) ? BA<T>::sory(V) + f * V.ysize() : nullptr;
+		c.ci = BA<T>::ci(V) ? BA<T>::ci(V) + f * 8 * pl : nullptr;
+		c.x = BA<T>::x(V) + f * pl;
+		c.b = BA<T>::b(V) + f * pl;
+		c.r = BA<T>::r(V) + f * pl;
+		c.nx = V.nx;
+		c.ny = V.ny;
+		c.pitch = V.pitch;
+		c.tpitch = V.tpitch;
+		c.ns = V.ns;
+	}
+	cc.abd = abd + f * abd_size();
+	cc.relax = s.relaxation;
+	cc.npre = s.nrelax_pre;
+	cc.npost = s.nrelax_post;
+	cc.bstep = sel.step;
+	return coarse_cycle<T>(cc, sel.count, st);
 }
 
 template <typename T>

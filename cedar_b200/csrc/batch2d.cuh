@@ -41,6 +41,7 @@ public:
 	std::vector<B2Level> lv;
 	double *abd = nullptr;
 	int *info = nullptr;  // [0] line factorizations, [1] coarse Cholesky
+	int lc = -1;          // first level of the fused coarse cycle (-1: none)
 	cudaStream_t st = nullptr;
 
 	Batch2() = default;
@@ -72,6 +73,8 @@ private:
 	int smooth(int l, Sel sel, int updown);
 	template <typename T>
 	int ncycle(int l, Sel sel);
+	template <typename T>
+	int fused(int l0, Sel sel);
 };
 
 // cdr2::solver::compute_num_levels (include/cedar/2d/solver.h:63-79)

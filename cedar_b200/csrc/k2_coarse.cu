@@ -1,0 +1,286 @@
+// k2_coarse.cu -- the coarse end of a 2D V-cycle in one kernel launch.
+//
+// Below ~64x64 points a level's kernels are latency bound: each launch of the
+// point, line and transfer kernels costs several microseconds however little
+// work it has.  This kernel runs the whole sub-cycle from a coarse level down to
+// the coarsest and back (cycle::vcycle::ncycle_helper,
+// include/cedar/cycle/vcycle.h:57-115: pre-smoothing, residual, restriction,
+// zero coarse iterate, ..., banded Cholesky, ..., interpolate-add,
+// post-smoothing) with one CTA per problem and a barrier between steps.  Every
+// point formula is the shared helper the separate kernels use (k2_point.cuh),
+// and the line solves run DPTTS2's sequential substitutions on rows staged in
+// shared memory (as the exact line kernels do), so the result is the one the
+// separate kernels give in CDR_LINES_EXACT mode.
+//
+// Measured on B200 (FP32 line-xy, levels 64^2 .. 4^2 of a 511^2 problem): 508 us
+// per cycle, against ~300 us for the ~70 separate launches it replaces: each of
+// its ~160 barrier-separated phases waits on L2 latency (2-3 us per phase), so
+// the solvers leave it off unless gpu.fuse-coarse asks for it.  Keeping each
+// level's operator and factors in shared memory across a level visit would make
+// the phases shared-memory bound.
+#include <algorithm>
+
+#include "k2_point.cuh"
+#include "kernels2d.cuh"
+
+namespace cdrgpu {
+
+constexpr int CC_THREADS = 1024;
+
+// r = b - A x on the level (all interior points)
+template <typename T, int NS>
+__device__ void cc_residual(const CoarseLevel<T> &L)
+{
+	const Dims2 d{L.nx, L.ny, L.pitch};
+	const int n = L.nx * L.ny;
+	for (int e = threadIdx.x; e < n; e += CC_THREADS) {
+		const size_t k = d.at(e % L.nx + 1, e / L.nx + 1);
+		L.r[k] = resid_at<T, NS>(L.so, d.plane(), L.x, L.b, k, L.pitch);
+	}
+}
+
+// coarse b = P^T r_fine
+template <typename T>
+__device__ void cc_restrict(const CoarseLevel<T> &F, const CoarseLevel<T> &C)
+{
+	const Dims2 f{F.nx, F.ny, F.pitch}, c{C.nx, C.ny, C.pitch};
+	const int n = C.nx * C.ny;
+	for (int e = threadIdx.x; e < n; e += CC_THREADS) restrict_at<T>(C.ci, F.r, C.b, f, c, e % C.nx + 1, e / C.nx + 1);
+}
+
+// x_fine += P x_coarse + r/c on the fine-only points
+template <typename T>
+__device__ void cc_interp(const CoarseLevel<T> &F, const CoarseLevel<T> &C)
+{
+	const Dims2 f{F.nx, F.ny, F.pitch}, c{C.nx, C.ny, C.pitch};
+	const int mx = F.nx / 2 + 1, n = mx * (F.ny / 2 + 1);
+	for (int e = threadIdx.x; e < n; e += CC_THREADS) interp_at<T>(C.ci, C.x, F.r, F.so, F.x, f, c, e % mx + 1, e / mx + 1);
+}
+
+// the whole coarse iterate, ghosts included, to zero (the cycle's memset)
+template <typename T>
+__device__ void cc_zero(const CoarseLevel<T> &L)
+{
+	const size_t n = (size_t)L.pitch * (L.ny + 2);
+	for (size_t e = threadIdx.x; e < n; e += CC_THREADS) L.x[e] = T(0);
+}
+
+// one Gauss-Seidel sweep, colours in relax_point_2d's order
+template <typename T, int NS>
+__device__ void cc_gs(const CoarseLevel<T> &L, int updown)
+{
+	const Dims2 d{L.nx, L.ny, L.pitch};
+	const size_t ps = d.plane();
+	if (NS == 5) {
+		const int order[4][2] = {{1, 1}, {1, 0}, {0, 1}, {0, 0}};  // (j odd?, i odd?)
+		const int mx = (L.nx + 1) / 2, my = (L.ny + 1) / 2;
+		for (int c = 0; c < 4; ++c) {
+			const int o = updown == CDR_DOWN ? c : 3 - c;
+			for (int e = threadIdx.x; e < mx * my; e += CC_THREADS) {
+				const int i = (order[o][1] ? 1 : 2) + 2 * (e % mx), j = (order[o][0] ? 1 : 2) + 2 * (e / mx);
+				if (i <= L.nx && j <= L.ny) gs_at<T, 5>(L.so, ps, L.x, L.b, L.sor, d.at(i, j), L.pitch);
+			}
+			__syncthreads();
+		}
+	} else {
+		const int mx = (L.nx + 1) / 2;
+		for (int c = 0; c < 2; ++c) {
+			const int par = updown == CDR_DOWN ? c : 1 - c;
+			for (int e = threadIdx.x; e < mx * L.ny; e += CC_THREADS) {
+				const int j = e / mx + 1;
+				const int i = (((1 + j) & 1) == par ? 1 : 2) + 2 * (e % mx);
+				if (i <= L.nx) gs_at<T, 3>(L.so, ps, L.x, L.b, L.sor, d.at(i, j), L.pitch);
+			}
+			__syncthreads();
+		}
+	}
+}
+
+// One zebra line sweep (both colours, relax_lines_2d's order).  Each colour:
+// right-hand sides, pivots and multipliers of its lines are staged in shared
+// memory by all threads, then one thread per line runs DPTTS2's substitutions.
+template <typename T, int NS, int DIR>
+__device__ void cc_lines(const CoarseLevel<T> &L, int updown, T *sm)
+{
+	const Dims2 d{L.nx, L.ny, L.pitch};
+	const size_t ps = d.plane();
+	const int n = DIR == CDR_DIR_X ? L.nx : L.ny;    // line length
+	const int nl = DIR == CDR_DIR_X ? L.ny : L.nx;   // lines
+	const T *fac = DIR == CDR_DIR_X ? L.sor : L.sory;
+	const size_t eplane = DIR == CDR_DIR_X ? ps : (size_t)L.tpitch * (L.nx + 2);
+	const int firsts[2] = {updown == CDR_DOWN ? 2 : 1, updown == CDR_DOWN ? 1 : 2};
+	for (int c = 0; c < 2; ++c) {
+		const int first = firsts[c];
+		const int ml = first > nl ? 0 : (nl - first) / 2 + 1;  // lines of this colour
+		T *R = sm, *D = sm + ml * n, *E = sm + 2 * ml * n;
+		for (int e = threadIdx.x; e < ml * n; e += CC_THREADS) {
+			const int g = e / n, m = e - g * n, lc = first + 2 * g;
+			const size_t k = DIR == CDR_DIR_X ? d.at(m + 1, lc) : d.at(lc, m + 1);
+			R[e] = line_rhs<T, NS, DIR>(L.so, ps, L.x, L.b, k, L.pitch);
+			const size_t fo = DIR == CDR_DIR_X ? (size_t)lc * L.pitch + m + 1 : (size_t)lc * L.tpitch + m + 1;
+			D[e] = fac[fo];
+			E[e] = fac[eplane + fo];
+		}
+		__syncthreads();
+		if (threadIdx.x < ml) {
+			T *r = R + threadIdx.x * n, *dd = D + threadIdx.x * n, *ee = E + threadIdx.x * n;
+			for (int m = 1; m < n; ++m) r[m] = r[m] - r[m - 1] * ee[m];
+			r[n - 1] = pivot_div(r[n - 1], dd[n - 1]);
+			for (int m = n - 2; m >= 0; --m) r[m] = pivot_div(r[m], dd[m]) - r[m + 1] * ee[m + 1];
+		}
+		__syncthreads();
+		for (int e = threadIdx.x; e < ml * n; e += CC_THREADS) {
+			const int g = e / n, m = e - g * n, lc = first + 2 * g;
+			L.x[DIR == CDR_DIR_X ? d.at(m + 1, lc) : d.at(lc, m + 1)] = R[e];
+		}
+		__syncthreads();
+	}
+}
+
+template <typename T, int NS>
+__device__ void cc_smooth(const CoarseCycle<T> &cc, const CoarseLevel<T> &L, int updown, T *sm)
+{
+	const int nrel = updown == CDR_DOWN ? cc.npre : cc.npost;
+	for (int it = 0; it < nrel; ++it) {
+		switch (cc.relax) {
+		case CDR_RELAX_POINT: cc_gs<T, NS>(L, updown); break;
+		case CDR_RELAX_LINE_X: cc_lines<T, NS, CDR_DIR_X>(L, updown, sm); break;
+		case CDR_RELAX_LINE_Y: cc_lines<T, NS, CDR_DIR_Y>(L, updown, sm); break;
+		default:
+			if (updown == CDR_DOWN) {
+				cc_lines<T, NS, CDR_DIR_X>(L, updown, sm);
+				cc_lines<T, NS, CDR_DIR_Y>(L, updown, sm);
+			} else {
+				cc_lines<T, NS, CDR_DIR_Y>(L, updown, sm);
+				cc_lines<T, NS, CDR_DIR_X>(L, updown, sm);
+			}
+		}
+	}
+}
+
+// BMG2_SymStd_SOLVE_cg with DPBTRS('U') on the coarsest level: the factor and
+// the right-hand side staged in shared memory, substitutions by one thread
+// (k_cg_solve's operations)
+template <typename T>
+__device__ void cc_cg(const double *__restrict__ ab, const CoarseLevel<T> &L, double *xs)
+{
+	const Dims2 d{L.nx, L.ny, L.pitch};
+	const int ldab = L.nx + 2, kd = L.nx + 1, n = L.nx * L.ny;
+	double *abs = xs + n;
+	for (int e = threadIdx.x; e < ldab * n; e += CC_THREADS) abs[e] = ab[e];
+	for (int e = threadIdx.x; e < n; e += CC_THREADS) xs[e] = (double)L.b[d.at(e % L.nx + 1, e / L.nx + 1)];
+	__syncthreads();
+	if (threadIdx.x == 0) {
+		for (int j = 0; j < n; ++j) {
+			double temp = xs[j];
+			const int i0 = j - kd > 0 ? j - kd : 0;
+			for (int i = i0; i < j; ++i) temp = temp - abs[(size_t)j * ldab + kd + i - j] * xs[i];
+			xs[j] = temp / abs[(size_t)j * ldab + kd];
+		}
+		for (int j = n - 1; j >= 0; --j) {
+			if (xs[j] != 0.0) {
+				xs[j] = xs[j] / abs[(size_t)j * ldab + kd];
+				const double temp = xs[j];
+				const int i1 = j - kd > 0 ? j - kd : 0;
+				for (int i = j - 1; i >= i1; --i) xs[i] = xs[i] - temp * abs[(size_t)j * ldab + kd + i - j];
+			}
+		}
+	}
+	__syncthreads();
+	for (int e = threadIdx.x; e < n; e += CC_THREADS) L.x[d.at(e % L.nx + 1, e / L.nx + 1)] = (T)xs[e];
+}
+
+// Problem blockIdx.x of a batch: every array of every level moves by that
+// problem's offset (problems back to back, problem step bstep).
+template <typename T>
+__device__ CoarseLevel<T> cc_level(const CoarseCycle<T> &cc, int l)
+{
+	CoarseLevel<T> L = cc.lv[l];
+	const size_t p = (size_t)blockIdx.x * cc.bstep, pl = (size_t)L.pitch * (L.ny + 2);
+	L.so += p * L.ns * pl;
+	L.x += p * pl;
+	L.b += p * pl;
+	L.r += p * pl;
+	if (L.sor) L.sor += p * 2 * pl;
+	if (L.sory) L.sory += p * 2 * (size_t)L.tpitch * (L.nx + 2);
+	if (L.ci) L.ci += p * 8 * pl;
+	return L;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(CC_THREADS) k_coarse_cycle(CoarseCycle<T> cc)
+{
+	extern __shared__ __align__(16) unsigned char cc_smem[];
+	T *sm = reinterpret_cast<T *>(cc_smem);
+	const int nl = cc.nl;
+	for (int l = 0; l + 1 < nl; ++l) {
+		const CoarseLevel<T> F = cc_level(cc, l), C = cc_level(cc, l + 1);
+		if (F.ns == 5) cc_smooth<T, 5>(cc, F, CDR_DOWN, sm);
+		else cc_smooth<T, 3>(cc, F, CDR_DOWN, sm);
+		if (F.ns == 5) cc_residual<T, 5>(F);
+		else cc_residual<T, 3>(F);
+		__syncthreads();
+		cc_restrict<T>(F, C);
+		cc_zero<T>(C);
+		__syncthreads();
+	}
+	{
+		const CoarseLevel<T> Cg = cc_level(cc, nl - 1);
+		const size_t nab = (size_t)(Cg.nx + 2) * Cg.nx * Cg.ny;
+		cc_cg<T>(cc.abd + (size_t)blockIdx.x * cc.bstep * nab, Cg, reinterpret_cast<double *>(cc_smem));
+		__syncthreads();
+	}
+	for (int l = nl - 2; l >= 0; --l) {
+		const CoarseLevel<T> F = cc_level(cc, l), C = cc_level(cc, l + 1);
+		cc_interp<T>(F, C);
+		__syncthreads();
+		if (F.ns == 5) cc_smooth<T, 5>(cc, F, CDR_UP, sm);
+		else cc_smooth<T, 3>(cc, F, CDR_UP, sm);
+		__syncthreads();
+	}
+}
+
+template <typename T>
+size_t coarse_cycle_smem(const CoarseCycle<T> &cc)
+{
+	size_t need = 0;
+	for (int l = 0; l + 1 < cc.nl; ++l) {
+		const CoarseLevel<T> &L = cc.lv[l];
+		const size_t lx = (size_t)((L.ny + 1) / 2) * L.nx, ly = (size_t)((L.nx + 1) / 2) * L.ny;
+		need = std::max(need, 3 * std::max(lx, ly) * sizeof(T));
+	}
+	const CoarseLevel<T> &Cg = cc.lv[cc.nl - 1];
+	const size_t n = (size_t)Cg.nx * Cg.ny;
+	need = std::max(need, (n + (size_t)(Cg.nx + 2) * n) * sizeof(double));
+	return need;
+}
+
+template <typename T>
+int coarse_cycle(const CoarseCycle<T> &cc, int nproblems, cudaStream_t st)
+{
+	if (cc.nl < 1 || cc.nl > kMaxCoarseLevels) {
+		set_error(CDR_ERR_DIM, "fused coarse cycle over %d levels", cc.nl);
+		return CDR_ERR_DIM;
+	}
+	const size_t smem = coarse_cycle_smem(cc);
+	if (smem > 200 * 1024) {
+		set_error(CDR_ERR_DIM, "fused coarse cycle needs %zu bytes of shared memory", smem);
+		return CDR_ERR_DIM;
+	}
+	k_coarse_cycle<T><<<nproblems, CC_THREADS, smem, st>>>(cc);
+	CDR_LAUNCH_CHECK();
+	return CDR_OK;
+}
+template int coarse_cycle<double>(const CoarseCycle<double> &, int, cudaStream_t);
+
+// Opt the fused kernels into the large shared-memory carve-out (once per
+// process, before any graph capture: called from lines_prepare).
+int coarse_prepare()
+{
+	CDR_CUDA_TRY(cudaFuncSetAttribute(k_coarse_cycle<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+	CDR_CUDA_TRY(cudaFuncSetAttribute(k_coarse_cycle<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+	return CDR_OK;
+}
+template int coarse_cycle<float>(const CoarseCycle<float> &, int, cudaStream_t);
+
+}  // namespace cdrgpu

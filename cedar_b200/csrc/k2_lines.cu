@@ -19,7 +19,8 @@
 // DPTTS2's sequential order (one thread per line): slower, bit-identical.
 #include <cstdint>
 
-#include "cdr_common.cuh"
+#include "k2_point.cuh"
+#include "kernels2d.cuh"
 
 namespace cdrgpu {
 
@@ -28,14 +29,9 @@ constexpr int LT = 256;  // threads per CTA
 // ------------------------------------------------------------------ setup
 // BMG2_SymStd_SETUP_lines_{x,y} + DPTTRF: per line d = c, e = -w (x) or -s (y),
 // then e(i) <- e(i)/d(i-1), d(i) <- d(i) - e(i)*e_old(i).  Always FP64; TS is
-// the storage type of the factors.
-// Per-problem size of the factor array of one direction (2 planes; y-line
-// factors transposed, planes tpitch*(nx+2) apart).
-__host__ __device__ __forceinline__ size_t line_factor_size(Dims2 d, int tpitch, int dir)
-{
-	return dir == CDR_DIR_X ? 2 * d.plane() : 2 * (size_t)tpitch * (d.nx + 2);
-}
-
+// the storage type of the factors.  FP32 factors (the preconditioner's) keep the
+// reciprocal pivots 1/d, formed in FP64 and rounded once, so that the FP32 sweeps
+// multiply instead of divide; FP64 factors keep d, as DPTTRF does.
 template <typename TS, int DIR>
 __global__ void k_lines_setup(const double *__restrict__ so, int ns, TS *__restrict__ sor, Dims2 d, int tpitch,
                               int *__restrict__ info)
@@ -53,7 +49,7 @@ __global__ void k_lines_setup(const double *__restrict__ so, int ns, TS *__restr
 	const size_t fps = DIR == CDR_DIR_X ? ps : (size_t)tpitch * (d.nx + 2);
 	auto fo = [&](int p) -> size_t { return DIR == CDR_DIR_X ? d.at(p, line) : (size_t)line * tpitch + p; };
 	double dprev = c[g(1)];
-	sor[fo(1)] = (TS)dprev;
+	sor[fo(1)] = pivot_store<TS>(dprev);
 	sor[fps + fo(1)] = (TS)(-off[g(1)]);
 	int st = 0;
 	for (int p = 1; p < n; ++p) {
@@ -62,7 +58,7 @@ __global__ void k_lines_setup(const double *__restrict__ so, int ns, TS *__restr
 		double e = ei / dprev;
 		double dn = c[g(p + 1)] - e * ei;
 		sor[fps + fo(p + 1)] = (TS)e;
-		sor[fo(p + 1)] = (TS)dn;
+		sor[fo(p + 1)] = pivot_store<TS>(dn);
 		dprev = dn;
 	}
 	if (dprev <= 0.0 && !st) st = n;
@@ -87,30 +83,6 @@ template int setup_lines_2d<double>(const double *, int, double *, Dims2, int, i
 template int setup_lines_2d<float>(const double *, int, float *, Dims2, int, int, int *, cudaStream_t);
 
 // ------------------------------------------------------------------ relax
-// Right-hand side of line relaxation at (i, j): b plus the couplings to the two
-// neighbouring lines (operand order of the reference).
-template <typename T, int NS, int DIR>
-__device__ __forceinline__ T line_rhs(const T *__restrict__ so, size_t ps, const T *__restrict__ q,
-                                      const T *__restrict__ qf, size_t k, int p)
-{
-	const T *w = so + ps, *s = so + 2 * ps;
-	if (DIR == CDR_DIR_X) {
-		if (NS == 5) {
-			const T *sw = so + 3 * ps, *nw = so + 4 * ps;
-			return qf[k] + s[k] * q[k - p] + s[k + p] * q[k + p] + sw[k] * q[k - p - 1] + nw[k + 1] * q[k - p + 1]
-			       + nw[k + p] * q[k + p - 1] + sw[k + p + 1] * q[k + p + 1];
-		}
-		return qf[k] + s[k] * q[k - p] + s[k + p] * q[k + p];
-	} else {
-		if (NS == 5) {
-			const T *sw = so + 3 * ps, *nw = so + 4 * ps;
-			return qf[k] + w[k] * q[k - 1] + w[k + 1] * q[k + 1] + sw[k] * q[k - p - 1] + nw[k + 1] * q[k - p + 1]
-			       + nw[k + p] * q[k + p - 1] + sw[k + p + 1] * q[k + p + 1];
-		}
-		return qf[k] + w[k] * q[k - 1] + w[k + 1] * q[k + 1];
-	}
-}
-
 // Segmented inclusive scan of affine maps over the tpl threads of a line.
 // forward: element t composes (later) t o (earlier) t-off; backward: t o t+off.
 template <typename T>
@@ -184,8 +156,8 @@ __global__ void __launch_bounds__(LT) k_lines(const T *__restrict__ so, T *__res
 		// DPTTS2 in its own order, one thread per line: bit-identical to LAPACK.
 		if (active && t == 0) {
 			for (int m = 1; m < n; ++m) r[m] = r[m] - r[m - 1] * E[m + 1];
-			r[n - 1] = r[n - 1] / D[n];
-			for (int m = n - 2; m >= 0; --m) r[m] = r[m] / D[m + 1] - r[m + 1] * E[m + 2];
+			r[n - 1] = pivot_div(r[n - 1], D[n]);
+			for (int m = n - 2; m >= 0; --m) r[m] = pivot_div(r[m], D[m + 1]) - r[m + 1] * E[m + 2];
 		}
 		__syncthreads();
 	} else {
@@ -214,14 +186,14 @@ __global__ void __launch_bounds__(LT) k_lines(const T *__restrict__ so, T *__res
 		if (active)
 			for (int m = hi - 1; m >= lo; --m) {
 				T a = m == n - 1 ? T(0) : -E[m + 2];
-				B = a * B + r[m] / D[m + 1];
+				B = a * B + pivot_div(r[m], D[m + 1]);
 				A = a * A;
 			}
 		affine_scan<T>(A, B, sA, sB, t, tpl, false);
 		if (active) {
 			T x = t == tpl - 1 ? T(0) : sB[threadIdx.x + 1];
 			for (int m = hi - 1; m >= lo; --m) {
-				x = m == n - 1 ? r[m] / D[m + 1] : r[m] / D[m + 1] - x * E[m + 2];
+				x = m == n - 1 ? pivot_div(r[m], D[m + 1]) : pivot_div(r[m], D[m + 1]) - x * E[m + 2];
 				r[m] = x;
 			}
 		}
@@ -475,7 +447,7 @@ __global__ void __launch_bounds__(DIR == CDR_DIR_X ? FAST_BLOCK_X : FAST_BLOCK_Y
 #pragma unroll
 			for (int w = 0; w < W; ++w) {
 				const int m = c * W + w, pos = p0 + m;
-				if (full || (pos >= 1 && pos <= n)) r[m] = r[m] / dv[w];
+				if (full || (pos >= 1 && pos <= n)) r[m] = pivot_div(r[m], dv[w]);
 			}
 		}
 	}
@@ -547,6 +519,7 @@ int lines_prepare()
 	CDR_LINES_ATTR(float, 5, CDR_DIR_X, true); CDR_LINES_ATTR(float, 5, CDR_DIR_Y, true);
 	CDR_LINES_ATTR(float, 3, CDR_DIR_X, true); CDR_LINES_ATTR(float, 3, CDR_DIR_Y, true);
 #undef CDR_LINES_ATTR
+	CDR_TRY(coarse_prepare());
 	done = true;
 	return CDR_OK;
 }

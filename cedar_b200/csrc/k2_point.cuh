@@ -23,6 +23,120 @@ __device__ __forceinline__ T resid_at(const T *__restrict__ so, size_t ps, const
 	}
 }
 
+// One point of a Gauss-Seidel colour (BMG2_SymStd_relax_GS.f90:93-133):
+// q(k) = (qf + couplings * q) * sor, in the reference's operand order.
+template <typename T, int NS>
+__device__ __forceinline__ void gs_at(const T *__restrict__ so, size_t ps, T *__restrict__ q,
+                                      const T *__restrict__ qf, const T *__restrict__ sor, size_t k, int pitch)
+{
+	const T *w = so + ps, *s = so + 2 * ps;
+	T acc;
+	if (NS == 5) {
+		const T *sw = so + 3 * ps, *nw = so + 4 * ps;
+		acc = qf[k] + w[k] * q[k - 1] + w[k + 1] * q[k + 1] + s[k] * q[k - pitch] + s[k + pitch] * q[k + pitch]
+		      + sw[k] * q[k - pitch - 1] + nw[k + 1] * q[k - pitch + 1] + nw[k + pitch] * q[k + pitch - 1]
+		      + sw[k + pitch + 1] * q[k + pitch + 1];
+	} else {
+		acc = qf[k] + w[k] * q[k - 1] + w[k + 1] * q[k + 1] + s[k] * q[k - pitch] + s[k + pitch] * q[k + pitch];
+	}
+	q[k] = acc * sor[k];
+}
+
+// Coarse point (ic, jc) of BMG2_SymStd_restrict (src/2d/ftn/BMG2_SymStd_restrict.f90:72-92);
+// it sits on fine (2ic-1, 2jc-1) (0-based, ghosts at 0).
+template <typename T>
+__device__ __forceinline__ void restrict_at(const T *__restrict__ ci, const T *__restrict__ q, T *__restrict__ qc,
+                                            const Dims2 &f, const Dims2 &c, int ic, int jc)
+{
+	const size_t cps = c.plane();
+	const int cp = c.pitch, fp = f.pitch;
+	const size_t kc = c.at(ic, jc), kf = f.at(2 * ic - 1, 2 * jc - 1);
+	const T *cL = ci + IL * cps, *cR = ci + IR * cps, *cA = ci + IA * cps, *cB = ci + IB * cps;
+	const T *cSW = ci + ISW * cps, *cNW = ci + INW * cps, *cNE = ci + INE * cps, *cSE = ci + ISE * cps;
+	qc[kc] = cNE[kc] * q[kf - fp - 1] + cA[kc] * q[kf - fp] + cNW[kc + 1] * q[kf - fp + 1] + cR[kc] * q[kf - 1]
+	         + q[kf] + cL[kc + 1] * q[kf + 1] + cSE[kc + cp] * q[kf + fp - 1] + cB[kc + cp] * q[kf + fp]
+	         + cSW[kc + cp + 1] * q[kf + fp + 1];
+}
+
+// Coarse cell (ic, jc) of BMG2_SymStd_interp_add (src/2d/ftn/BMG2_SymStd_interp_add.f90:101-137),
+// ic in [1, nxf/2+1]: fine points (i, j), (i-1, j), (i, j-1), (i-1, j-1), i = 2ic-1.
+// r/c is formed on the fly; the reference divides r by c on interior points
+// only, and for even grid sizes its loop also reaches the ghost row/column,
+// where r is added undivided.
+template <typename T>
+__device__ __forceinline__ void interp_at(const T *__restrict__ ci, const T *__restrict__ qc,
+                                          const T *__restrict__ res, const T *__restrict__ soc, T *__restrict__ q,
+                                          const Dims2 &f, const Dims2 &c, int ic, int jc)
+{
+	const size_t cps = c.plane();
+	const int cp = c.pitch, fp = f.pitch;
+	const int i = 2 * ic - 1, j = 2 * jc - 1;
+	const size_t kc = c.at(ic, jc), kf = f.at(i, j);
+	auto rc = [&](size_t k, int ii, int jj) -> T { return (ii <= f.nx && jj <= f.ny) ? res[k] / soc[k] : res[k]; };
+	const T qcc = qc[kc];
+	q[kf] = q[kf] + qcc;
+	if (ic >= 2) {
+		const T a = ci[IR * cps + kc] * qcc + ci[IL * cps + kc] * qc[kc - 1];
+		const size_t k = kf - 1;
+		q[k] = q[k] + a + rc(k, i - 1, j);
+	}
+	if (jc >= 2) {
+		const T aq = ci[IA * cps + kc] * qcc + ci[IB * cps + kc] * qc[kc - cp];
+		const size_t k = kf - fp;
+		q[k] = q[k] + aq + rc(k, i, j - 1);
+	}
+	if (ic >= 2 && jc >= 2) {
+		const T a = ci[ISW * cps + kc] * qc[kc - cp - 1] + ci[INW * cps + kc] * qc[kc - 1] + ci[INE * cps + kc] * qcc
+		            + ci[ISE * cps + kc] * qc[kc - cp];
+		const size_t k = kf - fp - 1;
+		q[k] = q[k] + a + rc(k, i - 1, j - 1);
+	}
+}
+
+// Right-hand side of line relaxation at (i, j): b plus the couplings to the two
+// neighbouring lines (relax_lines_x.f90:106-110, relax_lines_y.f90:102-106 operand order).
+template <typename T, int NS, int DIR>
+__device__ __forceinline__ T line_rhs(const T *__restrict__ so, size_t ps, const T *__restrict__ q,
+                                      const T *__restrict__ qf, size_t k, int p)
+{
+	const T *w = so + ps, *s = so + 2 * ps;
+	if (DIR == CDR_DIR_X) {
+		if (NS == 5) {
+			const T *sw = so + 3 * ps, *nw = so + 4 * ps;
+			return qf[k] + s[k] * q[k - p] + s[k + p] * q[k + p] + sw[k] * q[k - p - 1] + nw[k + 1] * q[k - p + 1]
+			       + nw[k + p] * q[k + p - 1] + sw[k + p + 1] * q[k + p + 1];
+		}
+		return qf[k] + s[k] * q[k - p] + s[k + p] * q[k + p];
+	} else {
+		if (NS == 5) {
+			const T *sw = so + 3 * ps, *nw = so + 4 * ps;
+			return qf[k] + w[k] * q[k - 1] + w[k + 1] * q[k + 1] + sw[k] * q[k - p - 1] + nw[k + 1] * q[k - p + 1]
+			       + nw[k + p] * q[k + p - 1] + sw[k + p + 1] * q[k + p + 1];
+		}
+		return qf[k] + w[k] * q[k - 1] + w[k + 1] * q[k + 1];
+	}
+}
+
+// Per-problem size of the line-factor array of one direction (2 planes; y-line
+// factors transposed, planes tpitch*(nx+2) apart).
+__host__ __device__ __forceinline__ size_t line_factor_size(Dims2 d, int tpitch, int dir)
+{
+	return dir == CDR_DIR_X ? 2 * d.plane() : 2 * (size_t)tpitch * (d.nx + 2);
+}
+
+// y / d with a stored line pivot: FP64 factors keep d (DPTTS2 divides), FP32
+// factors keep the reciprocal 1/d (the FP32 sweeps multiply).
+template <typename TS>
+__device__ __forceinline__ TS pivot_store(double d)
+{
+	return sizeof(TS) == 4 ? (TS)(1.0 / d) : (TS)d;
+}
+template <typename T>
+__device__ __forceinline__ T pivot_div(T y, T dstored)
+{
+	return sizeof(T) == 4 ? y * dstored : y / dstored;
+}
+
 template <int NW>
 __device__ __forceinline__ double block_sum(double v, double *sh)
 {

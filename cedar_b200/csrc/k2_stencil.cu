@@ -143,18 +143,7 @@ __global__ void __launch_bounds__(TX *TY) k_gs_colour(const T *__restrict__ so, 
 		i = (pi ? 1 : 2) + 2 * (blockIdx.x * TX + threadIdx.x);
 	}
 	if (i > d.nx || j > d.ny) return;
-	size_t k = d.at(i, j);
-	const T *w = so + ps, *s = so + 2 * ps;
-	T acc;
-	if (NS == 5) {
-		const T *sw = so + 3 * ps, *nw = so + 4 * ps;
-		acc = qf[k] + w[k] * q[k - 1] + w[k + 1] * q[k + 1] + s[k] * q[k - pitch] + s[k + pitch] * q[k + pitch]
-		      + sw[k] * q[k - pitch - 1] + nw[k + 1] * q[k - pitch + 1] + nw[k + pitch] * q[k + pitch - 1]
-		      + sw[k + pitch + 1] * q[k + pitch + 1];
-	} else {
-		acc = qf[k] + w[k] * q[k - 1] + w[k + 1] * q[k + 1] + s[k] * q[k - pitch] + s[k + pitch] * q[k + pitch];
-	}
-	q[k] = acc * sor[k];
+	gs_at<T, NS>(so, ps, q, qf, sor, d.at(i, j), pitch);
 }
 
 template <typename T>
@@ -199,16 +188,10 @@ __global__ void __launch_bounds__(TX *TY) k_restrict(const T *__restrict__ ci, c
 	int ic = blockIdx.x * TX + threadIdx.x + 1, jc = blockIdx.y * TY + threadIdx.y + 1;
 	if (ic > c.nx || jc > c.ny) return;
 	const size_t cps = c.plane();
-	const int cp = c.pitch, fp = f.pitch;
 	ci += c.bofs(8 * cps);
 	q += f.bofs(f.plane());
 	qc += c.bofs(cps);
-	size_t kc = c.at(ic, jc), kf = f.at(2 * ic - 1, 2 * jc - 1);
-	const T *cL = ci + IL * cps, *cR = ci + IR * cps, *cA = ci + IA * cps, *cB = ci + IB * cps;
-	const T *cSW = ci + ISW * cps, *cNW = ci + INW * cps, *cNE = ci + INE * cps, *cSE = ci + ISE * cps;
-	qc[kc] = cNE[kc] * q[kf - fp - 1] + cA[kc] * q[kf - fp] + cNW[kc + 1] * q[kf - fp + 1] + cR[kc] * q[kf - 1]
-	         + q[kf] + cL[kc + 1] * q[kf + 1] + cSE[kc + cp] * q[kf + fp - 1] + cB[kc + cp] * q[kf + fp]
-	         + cSW[kc + cp + 1] * q[kf + fp + 1];
+	restrict_at<T>(ci, q, qc, f, c, ic, jc);
 }
 
 template <typename T>
@@ -234,35 +217,12 @@ __global__ void __launch_bounds__(TX *TY) k_interp_add(const T *__restrict__ ci,
 	int ic = blockIdx.x * TX + threadIdx.x + 1, jc = blockIdx.y * TY + threadIdx.y + 1;
 	if (ic > f.nx / 2 + 1 || jc > f.ny / 2 + 1) return;
 	const size_t cps = c.plane();
-	const int cp = c.pitch, fp = f.pitch;
 	ci += c.bofs(8 * cps);
 	qc += c.bofs(cps);
 	res += f.bofs(f.plane());
 	soc += f.bofs(nsf * f.plane());
 	q += f.bofs(f.plane());
-	const int i = 2 * ic - 1, j = 2 * jc - 1;
-	size_t kc = c.at(ic, jc), kf = f.at(i, j);
-	// The reference divides r by c on interior points only; for even grid sizes
-	// the loop also reaches the ghost row/column, where r is added undivided.
-	auto rc = [&](size_t k, int ii, int jj) -> T { return (ii <= f.nx && jj <= f.ny) ? res[k] / soc[k] : res[k]; };
-	T qcc = qc[kc];
-	q[kf] = q[kf] + qcc;
-	if (ic >= 2) {
-		T a = ci[IR * cps + kc] * qcc + ci[IL * cps + kc] * qc[kc - 1];
-		size_t k = kf - 1;
-		q[k] = q[k] + a + rc(k, i - 1, j);
-	}
-	if (jc >= 2) {
-		T aq = ci[IA * cps + kc] * qcc + ci[IB * cps + kc] * qc[kc - cp];
-		size_t k = kf - fp;
-		q[k] = q[k] + aq + rc(k, i, j - 1);
-	}
-	if (ic >= 2 && jc >= 2) {
-		T a = ci[ISW * cps + kc] * qc[kc - cp - 1] + ci[INW * cps + kc] * qc[kc - 1] + ci[INE * cps + kc] * qcc
-		      + ci[ISE * cps + kc] * qc[kc - cp];
-		size_t k = kf - fp - 1;
-		q[k] = q[k] + a + rc(k, i - 1, j - 1);
-	}
+	interp_at<T>(ci, qc, res, soc, q, f, c, ic, jc);
 }
 
 template <typename T>

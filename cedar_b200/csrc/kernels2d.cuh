@@ -36,4 +36,26 @@ int norm_blocks(Dims2 d);
 
 constexpr size_t kNormScratchBytes = 2048 * sizeof(double);
 
+// Levels of a fused coarse cycle (k2_coarse.cu): level 0 holds the restricted
+// right-hand side and a zero iterate on entry; the last level is the coarsest
+// (banded Cholesky factor abd).  Arrays of a batch lie back to back (problem
+// blockIdx.x * bstep; the pointers are those of the first problem).
+constexpr int kMaxCoarseLevels = 12;
+template <typename T>
+struct CoarseLevel {
+	const T *so = nullptr, *sor = nullptr, *sory = nullptr, *ci = nullptr;
+	T *x = nullptr, *b = nullptr, *r = nullptr;
+	int nx = 0, ny = 0, pitch = 0, tpitch = 0, ns = 5;
+};
+template <typename T>
+struct CoarseCycle {
+	CoarseLevel<T> lv[kMaxCoarseLevels];
+	int nl = 0;
+	const double *abd = nullptr;
+	int relax = CDR_RELAX_POINT, npre = 2, npost = 1, bstep = 1;
+};
+template <typename T>
+int coarse_cycle(const CoarseCycle<T> &cc, int nproblems, cudaStream_t st);
+int coarse_prepare();
+
 }  // namespace cdrgpu

@@ -429,7 +429,8 @@ static int create3_any(const cdr_gpu_settings *s, const double *so_src, int src_
 	}
 	cudaEventCreate(&h->ev0);
 	cudaEventCreate(&h->ev1);
-	int rc = create3(h, so_src, src_pitch, kind, nx, ny, nz);
+	int rc = lines_prepare();  // the plane problems' line and fused kernels
+	if (rc == CDR_OK) rc = create3(h, so_src, src_pitch, kind, nx, ny, nz);
 	if (rc != CDR_OK) {
 		cdr_gpu_solver3_destroy(h);
 		return rc;

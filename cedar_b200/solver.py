@@ -42,6 +42,7 @@ def _settings(ms: MLSettings, dim=2):
     s.precision = _lib.PREC[ms.precision]
     s.use_graph = 1 if ms.use_graph else 0
     s.line_flags = _lib.LINES_EXACT if ms.line_solve == "sequential" else 0
+    s.fuse_coarse = ms.fuse_coarse
     return s
 
 

@@ -118,7 +118,8 @@ int cdr_gpu_relax_point_2d_f32(const float *so, int nstencil, float *x, const fl
  * BMG2_SymStd_SETUP_lines_y.f90:69-88).  dir = CDR_DIR_X: sor has the grid's layout.
  * dir = CDR_DIR_Y: sor is stored transposed as Cedar does (SOR(JJ,II,2)): element
  * (j, i) at i*tpitch + j with tpitch >= ny+2, planes tpitch*(nx+2) apart.
- * The factorization is always done in FP64; the f32 variant rounds the factors. */
+ * The factorization is always done in FP64; the f32 variant rounds the factors and
+ * stores the reciprocal pivots 1/d in plane 0 (its sweeps multiply by them). */
 int cdr_gpu_setup_lines_2d_f64(const double *so, int nstencil, double *sor, int nx, int ny, int pitch,
                                int tpitch, int dir, int *info_dev, cudaStream_t stream);
 int cdr_gpu_setup_lines_2d_f32(const double *so, int nstencil, float *sor, int nx, int ny, int pitch,
@@ -223,6 +224,7 @@ typedef struct cdr_gpu_settings {
 	int precision;    /* CDR_PREC_F64 (default) or CDR_PREC_F32_IR                     */
 	int use_graph;    /* replay the cycle as a CUDA graph (default 1)                  */
 	int line_flags;   /* CDR_LINES_EXACT for sequential line substitutions (default 0) */
+	int fuse_coarse;  /* levels with both edges <= this run as one fused kernel (default 0 = off) */
 } cdr_gpu_settings;
 
 typedef struct cdr_gpu_solver cdr_gpu_solver;

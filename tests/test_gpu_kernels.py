@@ -201,8 +201,13 @@ def test_line_relax_register_chunk_kernel(lib, oracle, nx, ny, ns, precision):
     fn = lib.cdr_gpu_relax_lines_2d_f64 if precision == "f64" else lib.cdr_gpu_relax_lines_2d_f32
     dso = padded(so, pitch, dt)
     dbb = padded(b, pitch, dt)
-    dsx = padded(sx, pitch, dt)
-    dsy = padded(sy, tpitch, dt)
+    gx, gy = sx, sy
+    if precision == "f32":  # FP32 factors hold reciprocal pivots
+        gx, gy = sx.copy(), sy.copy()
+        gx[0][1:-1, 1:-1] = 1.0 / sx[0][1:-1, 1:-1]
+        gy[0][1:-1, 1:-1] = 1.0 / sy[0][1:-1, 1:-1]
+    dsx = padded(gx, pitch, dt)
+    dsy = padded(gy, tpitch, dt)
     for direction, sor, dsor, ofn in ((_lib.DIR_X, sx, dsx, oracle.relax_lines_x), (_lib.DIR_Y, sy, dsy, oracle.relax_lines_y)):
         for updown in (0, 1):
             xr = x.copy()

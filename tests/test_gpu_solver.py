@@ -144,3 +144,39 @@ def test_setup_arrays_match_oracle(oracle):
     for l in range(1, s.nlevels):
         np.testing.assert_array_equal(s.level_array(l, "ci"), o.level_array(l, "ci"))
         np.testing.assert_array_equal(s.level_array(l, "so"), o.level_array(l, "so"))
+
+
+@pytest.mark.parametrize("relax,ns,n", [("line-xy", 5, 255), ("point", 3, 200), ("line-x", 5, 130), ("point", 5, 97)])
+def test_fused_coarse_cycle_is_bitwise_the_separate_kernels(relax, ns, n):
+    """The fused coarse cycle (levels of at most 64x64 in one launch) performs the
+    operations of the separate kernels in sequential-substitution mode: the FP64
+    solve is bit-identical with and without it."""
+    from cedar_b200.config import Config
+    from cedar_b200.solver import Solver2D
+    if ns == 5:
+        so, b = P.hetero_diffusion(n, sigma=1.0, n_incl=4, contrast=100.0, aniso=0.5)
+    else:
+        so, b = P.poisson_noise(n)
+    xs, hs = [], []
+    for fuse in (64, 0):
+        conf = Config({"solver": {"relaxation": relax, "max-iter": 8, "tol": 1e-14},
+                       "gpu": {"line-solve": "sequential", "fuse-coarse": fuse}})
+        s = Solver2D(so, conf)
+        xs.append(s.solve(b))
+        hs.append(s.history.copy())
+    assert np.array_equal(xs[0], xs[1])
+    assert np.array_equal(hs[0], hs[1])
+
+
+def test_fused_coarse_cycle_fp32():
+    from cedar_b200.config import Config
+    from cedar_b200.solver import Solver2D
+    so, b = P.hetero_diffusion(255, sigma=1.0, n_incl=4, contrast=100.0, aniso=0.5)
+    its = []
+    for fuse in (64, 0):
+        s = Solver2D(so, Config({"solver": {"relaxation": "line-xy", "max-iter": 30, "tol": 1e-10},
+                                 "gpu": {"precision": "fp32-ir", "fuse-coarse": fuse}}))
+        s.solve(b)
+        assert s.history[-1] < 1e-10
+        its.append(s.iters)
+    assert abs(its[0] - its[1]) <= 1
