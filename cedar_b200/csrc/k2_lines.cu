@@ -262,7 +262,7 @@ __device__ __forceinline__ void vstore(T *__restrict__ p, const T (&v)[K])
 template <typename T>
 __device__ __forceinline__ void after(T &A, T &B, T a2, T b2)
 {
-	B = A * b2 + B;
+	B = madd(A, b2, B);
 	A = A * a2;
 }
 
@@ -299,24 +299,24 @@ __device__ __forceinline__ T scan_incoming(T A, T B, bool forward, int u, int S,
 		for (int kk = 0; kk < k; ++kk) {  // carry = M_{k-1} o ... o M_0
 			int sl = slot_self + (kk - k) * slot_stride;
 			T a2 = sA[sl], b2 = sB[sl];
-			T na = a2 * ca, nb = a2 * cb + b2;
+			T na = a2 * ca, nb = madd(a2, cb, b2);
 			ca = na; cb = nb;
 		}
 	} else {
 		for (int kk = NWG - 1; kk > k; --kk) {  // carry = M_{k+1} o ... o M_{NWG-1}
 			int sl = slot_self + (kk - k) * slot_stride;
 			T a2 = sA[sl], b2 = sB[sl];
-			T na = a2 * ca, nb = a2 * cb + b2;
+			T na = a2 * ca, nb = madd(a2, cb, b2);
 			ca = na; cb = nb;
 		}
 	}
-	return ae * cb + be;
+	return madd(ae, cb, be);
 }
 
 constexpr int FAST_BLOCK_X = 256, FAST_BLOCK_Y = 1024;
 
-template <typename T, int NS, int DIR, int K>
-__global__ void __launch_bounds__(DIR == CDR_DIR_X ? FAST_BLOCK_X : FAST_BLOCK_Y, DIR == CDR_DIR_X ? 2 : 1)
+template <typename T, int NS, int DIR, int K, bool XL = DIR == CDR_DIR_X>
+__global__ void __launch_bounds__(XL ? FAST_BLOCK_X : FAST_BLOCK_Y, XL ? 2 : 1)
     k_lines_fast(const T *__restrict__ so, T *__restrict__ q, const T *__restrict__ qf, const T *__restrict__ sor,
                  Dims2 d, int tpitch, int first, int tpl_log2)
 {
@@ -326,7 +326,7 @@ __global__ void __launch_bounds__(DIR == CDR_DIR_X ? FAST_BLOCK_X : FAST_BLOCK_Y
 	const int G = blockDim.x >> tpl_log2;  // lines per CTA
 	const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
 	int g, t;
-	if (DIR == CDR_DIR_X) { g = tid >> tpl_log2; t = tid & (TPL - 1); }
+	if (XL) { g = tid >> tpl_log2; t = tid & (TPL - 1); }
 	else { g = tid % G; t = tid / G; }
 	const int n = DIR == CDR_DIR_X ? d.nx : d.ny;
 	const int nl = DIR == CDR_DIR_X ? d.ny : d.nx;
@@ -358,7 +358,7 @@ __global__ void __launch_bounds__(DIR == CDR_DIR_X ? FAST_BLOCK_X : FAST_BLOCK_Y
 			vload<T, K>(s + k0, s0);
 			vload<T, K>(s + k0 + P, s1);
 #pragma unroll
-			for (int m = 0; m < K; ++m) r[m] = b_[m] + s0[m] * qm[m] + s1[m] * qp[m];
+			for (int m = 0; m < K; ++m) r[m] = madd(s1[m], qp[m], madd(s0[m], qm[m], b_[m]));
 			if (NS == 5) {
 				T sw0[K], nw0[K], nw1[K], sw1[K];
 				vload<T, K>(sw + k0, sw0);
@@ -375,29 +375,28 @@ __global__ void __launch_bounds__(DIR == CDR_DIR_X ? FAST_BLOCK_X : FAST_BLOCK_Y
 					const T qpl = m > 0 ? qp[m - 1] : qp_l, qpr = m < K - 1 ? qp[m + 1] : qp_r;
 					const T nwr = m < K - 1 ? nw0[m + 1] : nw0_r, swr = m < K - 1 ? sw1[m + 1] : sw1_r;
 					// operand order of relax_lines_x.f90:106-110
-					r[m] = b_[m] + s0[m] * qm[m] + s1[m] * qp[m] + sw0[m] * qml + nwr * qmr + nw1[m] * qpl + swr * qpr;
+					T a = madd(s0[m], qm[m], b_[m]);
+					a = madd(s1[m], qp[m], a);
+					a = madd(sw0[m], qml, a);
+					a = madd(nwr, qmr, a);
+					a = madd(nw1[m], qpl, a);
+					r[m] = madd(swr, qpr, a);
 				}
 			}
 		} else {
 			const int i = lc;
-			const T *w = so + ps, *sw = so + 3 * ps, *nw = so + 4 * ps;
 #pragma unroll
 			for (int m = 0; m < K; ++m) {
 				const int jj = p0 + m;
 				if (jj < 1 || jj > n) continue;
-				const size_t k = d.at(i, jj);
-				if (NS == 5)
-					r[m] = qf[k] + w[k] * q[k - 1] + w[k + 1] * q[k + 1] + sw[k] * q[k - P - 1] + nw[k + 1] * q[k - P + 1]
-					       + nw[k + P] * q[k + P - 1] + sw[k + P + 1] * q[k + P + 1];
-				else
-					r[m] = qf[k] + w[k] * q[k - 1] + w[k + 1] * q[k + 1];
+				r[m] = line_rhs<T, NS, CDR_DIR_Y>(so, ps, q, qf, d.at(i, jj), P);
 			}
 		}
 	}
 
 	// scan geometry
 	int S, CW, NWG, kgrp, slot, sstride;
-	if (DIR == CDR_DIR_X) {
+	if (XL) {
 		S = 1;
 		CW = TPL < 32 ? TPL : 32;
 		NWG = TPL > 32 ? TPL / 32 : 1;
@@ -412,7 +411,7 @@ __global__ void __launch_bounds__(DIR == CDR_DIR_X ? FAST_BLOCK_X : FAST_BLOCK_Y
 		slot = warp * (32 / CW) + (lane % S);  // one slot per (warp, line of the warp)
 		sstride = 32 / CW;
 	}
-	const int u = DIR == CDR_DIR_X ? (lane & (CW - 1)) : lane / S;
+	const int u = XL ? (lane & (CW - 1)) : lane / S;
 	const bool full = p0 >= 1 && p0 + K - 1 <= n;  // no ghost or beyond-end position in the chunk
 
 	// 2a. forward substitution y(p) = r(p) - y(p-1) E(p)
@@ -425,7 +424,7 @@ __global__ void __launch_bounds__(DIR == CDR_DIR_X ? FAST_BLOCK_X : FAST_BLOCK_Y
 			const int pos = p0 + m;
 			if (!full && (pos < 1 || pos > n)) continue;
 			const T a = (!full && pos == 1) ? T(0) : -Ev[m];
-			B = a * B + r[m];
+			B = madd(a, B, r[m]);
 			A = a * A;
 		}
 	}
@@ -435,7 +434,7 @@ __global__ void __launch_bounds__(DIR == CDR_DIR_X ? FAST_BLOCK_X : FAST_BLOCK_Y
 		for (int m = 0; m < K; ++m) {
 			const int pos = p0 + m;
 			if (!full && (pos < 1 || pos > n)) continue;
-			y = (!full && pos == 1) ? r[m] : r[m] - y * Ev[m];
+			y = (!full && pos == 1) ? r[m] : madd(-y, Ev[m], r[m]);
 			r[m] = y;
 		}
 		// y(p)/D(p), the first operation of the DPTTS2 back substitution, in place
@@ -462,7 +461,7 @@ __global__ void __launch_bounds__(DIR == CDR_DIR_X ? FAST_BLOCK_X : FAST_BLOCK_Y
 			if (!full && (pos < 1 || pos > n)) continue;
 			const T e1 = m < K - 1 ? Ev[m + 1] : Enext;
 			const T a = pos == n ? T(0) : -e1;
-			B = a * B + r[m];
+			B = madd(a, B, r[m]);
 			A = a * A;
 		}
 	}
@@ -474,7 +473,7 @@ __global__ void __launch_bounds__(DIR == CDR_DIR_X ? FAST_BLOCK_X : FAST_BLOCK_Y
 			const int pos = p0 + m;
 			if (!full && (pos < 1 || pos > n)) continue;
 			const T e1 = m < K - 1 ? Ev[m + 1] : Enext;
-			x = pos == n ? r[m] : r[m] - x * e1;
+			x = pos == n ? r[m] : madd(-x, e1, r[m]);
 			r[m] = x;
 		}
 	}

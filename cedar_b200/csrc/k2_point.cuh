@@ -6,21 +6,35 @@ namespace cdrgpu {
 
 constexpr int TX = 32, TY = 8;  // 2D tile of the point kernels
 
+// a*b + c: one fused multiply-add in FP32 (the preconditioner's kernels), a
+// separately rounded product and sum in FP64 (the library is built without FMA
+// contraction so that the FP64 kernels give the reference's bits; c + a*b and
+// a*b + c are the same IEEE sum).
+template <typename T>
+__device__ __forceinline__ T madd(T a, T b, T c)
+{
+	if constexpr (sizeof(T) == 4) return __fmaf_rn(a, b, c);
+	else return a * b + c;
+}
+
 // BMG2_SymStd_residual (src/2d/ftn/BMG2_SymStd_residual.f90:89-117).
 template <typename T, int NS>
 __device__ __forceinline__ T resid_at(const T *__restrict__ so, size_t ps, const T *__restrict__ q,
                                       const T *__restrict__ qf, size_t k, int pitch)
 {
 	const T *c = so, *w = so + ps, *s = so + 2 * ps;
+	T a = madd(w[k], q[k - 1], qf[k]);
+	a = madd(w[k + 1], q[k + 1], a);
+	a = madd(s[k], q[k - pitch], a);
+	a = madd(s[k + pitch], q[k + pitch], a);
 	if (NS == 5) {
 		const T *sw = so + 3 * ps, *nw = so + 4 * ps;
-		return qf[k] + w[k] * q[k - 1] + w[k + 1] * q[k + 1] + s[k] * q[k - pitch] + s[k + pitch] * q[k + pitch]
-		       + sw[k] * q[k - pitch - 1] + nw[k + 1] * q[k - pitch + 1] + nw[k + pitch] * q[k + pitch - 1]
-		       + sw[k + pitch + 1] * q[k + pitch + 1] - c[k] * q[k];
-	} else {
-		return qf[k] + w[k] * q[k - 1] + w[k + 1] * q[k + 1] + s[k] * q[k - pitch] + s[k + pitch] * q[k + pitch]
-		       - c[k] * q[k];
+		a = madd(sw[k], q[k - pitch - 1], a);
+		a = madd(nw[k + 1], q[k - pitch + 1], a);
+		a = madd(nw[k + pitch], q[k + pitch - 1], a);
+		a = madd(sw[k + pitch + 1], q[k + pitch + 1], a);
 	}
+	return madd(-c[k], q[k], a);
 }
 
 // One point of a Gauss-Seidel colour (BMG2_SymStd_relax_GS.f90:93-133):
@@ -30,14 +44,16 @@ __device__ __forceinline__ void gs_at(const T *__restrict__ so, size_t ps, T *__
                                       const T *__restrict__ qf, const T *__restrict__ sor, size_t k, int pitch)
 {
 	const T *w = so + ps, *s = so + 2 * ps;
-	T acc;
+	T acc = madd(w[k], q[k - 1], qf[k]);
+	acc = madd(w[k + 1], q[k + 1], acc);
+	acc = madd(s[k], q[k - pitch], acc);
+	acc = madd(s[k + pitch], q[k + pitch], acc);
 	if (NS == 5) {
 		const T *sw = so + 3 * ps, *nw = so + 4 * ps;
-		acc = qf[k] + w[k] * q[k - 1] + w[k + 1] * q[k + 1] + s[k] * q[k - pitch] + s[k + pitch] * q[k + pitch]
-		      + sw[k] * q[k - pitch - 1] + nw[k + 1] * q[k - pitch + 1] + nw[k + pitch] * q[k + pitch - 1]
-		      + sw[k + pitch + 1] * q[k + pitch + 1];
-	} else {
-		acc = qf[k] + w[k] * q[k - 1] + w[k + 1] * q[k + 1] + s[k] * q[k - pitch] + s[k + pitch] * q[k + pitch];
+		acc = madd(sw[k], q[k - pitch - 1], acc);
+		acc = madd(nw[k + 1], q[k - pitch + 1], acc);
+		acc = madd(nw[k + pitch], q[k + pitch - 1], acc);
+		acc = madd(sw[k + pitch + 1], q[k + pitch + 1], acc);
 	}
 	q[k] = acc * sor[k];
 }
@@ -53,9 +69,15 @@ __device__ __forceinline__ void restrict_at(const T *__restrict__ ci, const T *_
 	const size_t kc = c.at(ic, jc), kf = f.at(2 * ic - 1, 2 * jc - 1);
 	const T *cL = ci + IL * cps, *cR = ci + IR * cps, *cA = ci + IA * cps, *cB = ci + IB * cps;
 	const T *cSW = ci + ISW * cps, *cNW = ci + INW * cps, *cNE = ci + INE * cps, *cSE = ci + ISE * cps;
-	qc[kc] = cNE[kc] * q[kf - fp - 1] + cA[kc] * q[kf - fp] + cNW[kc + 1] * q[kf - fp + 1] + cR[kc] * q[kf - 1]
-	         + q[kf] + cL[kc + 1] * q[kf + 1] + cSE[kc + cp] * q[kf + fp - 1] + cB[kc + cp] * q[kf + fp]
-	         + cSW[kc + cp + 1] * q[kf + fp + 1];
+	T a = cNE[kc] * q[kf - fp - 1];
+	a = madd(cA[kc], q[kf - fp], a);
+	a = madd(cNW[kc + 1], q[kf - fp + 1], a);
+	a = madd(cR[kc], q[kf - 1], a);
+	a = a + q[kf];
+	a = madd(cL[kc + 1], q[kf + 1], a);
+	a = madd(cSE[kc + cp], q[kf + fp - 1], a);
+	a = madd(cB[kc + cp], q[kf + fp], a);
+	qc[kc] = madd(cSW[kc + cp + 1], q[kf + fp + 1], a);
 }
 
 // Coarse cell (ic, jc) of BMG2_SymStd_interp_add (src/2d/ftn/BMG2_SymStd_interp_add.f90:101-137),
@@ -76,18 +98,19 @@ __device__ __forceinline__ void interp_at(const T *__restrict__ ci, const T *__r
 	const T qcc = qc[kc];
 	q[kf] = q[kf] + qcc;
 	if (ic >= 2) {
-		const T a = ci[IR * cps + kc] * qcc + ci[IL * cps + kc] * qc[kc - 1];
+		const T a = madd(ci[IL * cps + kc], qc[kc - 1], ci[IR * cps + kc] * qcc);
 		const size_t k = kf - 1;
 		q[k] = q[k] + a + rc(k, i - 1, j);
 	}
 	if (jc >= 2) {
-		const T aq = ci[IA * cps + kc] * qcc + ci[IB * cps + kc] * qc[kc - cp];
+		const T aq = madd(ci[IB * cps + kc], qc[kc - cp], ci[IA * cps + kc] * qcc);
 		const size_t k = kf - fp;
 		q[k] = q[k] + aq + rc(k, i, j - 1);
 	}
 	if (ic >= 2 && jc >= 2) {
-		const T a = ci[ISW * cps + kc] * qc[kc - cp - 1] + ci[INW * cps + kc] * qc[kc - 1] + ci[INE * cps + kc] * qcc
-		            + ci[ISE * cps + kc] * qc[kc - cp];
+		T a = madd(ci[INW * cps + kc], qc[kc - 1], ci[ISW * cps + kc] * qc[kc - cp - 1]);
+		a = madd(ci[INE * cps + kc], qcc, a);
+		a = madd(ci[ISE * cps + kc], qc[kc - cp], a);
 		const size_t k = kf - fp - 1;
 		q[k] = q[k] + a + rc(k, i - 1, j - 1);
 	}
@@ -100,21 +123,22 @@ __device__ __forceinline__ T line_rhs(const T *__restrict__ so, size_t ps, const
                                       const T *__restrict__ qf, size_t k, int p)
 {
 	const T *w = so + ps, *s = so + 2 * ps;
+	T a;
 	if (DIR == CDR_DIR_X) {
-		if (NS == 5) {
-			const T *sw = so + 3 * ps, *nw = so + 4 * ps;
-			return qf[k] + s[k] * q[k - p] + s[k + p] * q[k + p] + sw[k] * q[k - p - 1] + nw[k + 1] * q[k - p + 1]
-			       + nw[k + p] * q[k + p - 1] + sw[k + p + 1] * q[k + p + 1];
-		}
-		return qf[k] + s[k] * q[k - p] + s[k + p] * q[k + p];
+		a = madd(s[k], q[k - p], qf[k]);
+		a = madd(s[k + p], q[k + p], a);
 	} else {
-		if (NS == 5) {
-			const T *sw = so + 3 * ps, *nw = so + 4 * ps;
-			return qf[k] + w[k] * q[k - 1] + w[k + 1] * q[k + 1] + sw[k] * q[k - p - 1] + nw[k + 1] * q[k - p + 1]
-			       + nw[k + p] * q[k + p - 1] + sw[k + p + 1] * q[k + p + 1];
-		}
-		return qf[k] + w[k] * q[k - 1] + w[k + 1] * q[k + 1];
+		a = madd(w[k], q[k - 1], qf[k]);
+		a = madd(w[k + 1], q[k + 1], a);
 	}
+	if (NS == 5) {
+		const T *sw = so + 3 * ps, *nw = so + 4 * ps;
+		a = madd(sw[k], q[k - p - 1], a);
+		a = madd(nw[k + 1], q[k - p + 1], a);
+		a = madd(nw[k + p], q[k + p - 1], a);
+		a = madd(sw[k + p + 1], q[k + p + 1], a);
+	}
+	return a;
 }
 
 // Per-problem size of the line-factor array of one direction (2 planes; y-line

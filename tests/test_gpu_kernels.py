@@ -184,7 +184,9 @@ def test_line_relax(lib, oracle, nx, ny, ns, updown):
 
 
 LINE_SIZES = [(9, 9, 3), (17, 12, 5), (64, 63, 3), (130, 97, 5), (255, 31, 5), (31, 255, 5), (1023, 20, 5),
-              (20, 1023, 5), (2047, 12, 5), (12, 2047, 5), (2047, 9, 3), (9, 2047, 3)]
+              (20, 1023, 5), (2047, 12, 5), (12, 2047, 5), (2047, 9, 3), (9, 2047, 3),
+              # line lengths n = 2^k: the last thread of a line owns the tail point
+              (8, 16, 5), (128, 33, 5), (33, 256, 5), (1024, 9, 5), (9, 1024, 5), (512, 512, 3)]
 
 
 @pytest.mark.parametrize("nx,ny,ns", LINE_SIZES)
