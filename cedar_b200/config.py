@@ -6,7 +6,7 @@ note that the reference reads ``solver.min_coarse`` (underscore), so the
 ``"min-coarse"`` key found in its example configs has no effect there or here.
 GPU options live under the ``"gpu"`` object: ``precision`` ("fp64" | "fp32-ir"),
 ``graph`` (bool), ``fuse-coarse`` (levels with both edges at most this many
-points run as one fused kernel; 0 = off, the default) and ``line-solve`` ("scan": parallel line substitutions, the
+points run as one fused kernel; 0 = off; default 32) and ``line-solve`` ("scan": parallel line substitutions, the
 default; "sequential": DPTTRS order, bit-identical to the reference).
 """
 import json
@@ -73,7 +73,7 @@ class MLSettings:
         self.line_solve = conf.get("gpu.line-solve", "scan")
         if self.line_solve not in ("scan", "sequential"):
             raise ValueError("invalid gpu.line-solve: %s" % self.line_solve)
-        self.fuse_coarse = int(conf.get("gpu.fuse-coarse", 0))
+        self.fuse_coarse = int(conf.get("gpu.fuse-coarse", 32))
         if self.fuse_coarse < 0:
             raise ValueError("invalid gpu.fuse-coarse: %d" % self.fuse_coarse)
 

@@ -108,12 +108,8 @@ int Batch2::init(const cdr_gpu_settings &settings, int ns, int nx, int ny, int n
 			}
 		}
 	}
-	if (s.fuse_coarse > 0)
-		for (int l = 1; l + 1 < nl && l < kMaxCoarseLevels; ++l)
-			if (lv[l].nx <= s.fuse_coarse && lv[l].ny <= s.fuse_coarse && nl - l <= kMaxCoarseLevels) {
-				lc = l;
-				break;
-			}
+	lc[0] = pick_fused<double>();
+	lc[1] = pick_fused<float>();
 	const B2Level &Cg = lv.back();
 	if ((size_t)Cg.nx * Cg.ny > 4096) {
 		set_error(CDR_ERR_DIM, "coarsest grid %dx%d too large for the banded Cholesky", Cg.nx, Cg.ny);
@@ -227,11 +223,33 @@ int Batch2::ncycle(int l, Sel sel)
 	// zero the selected coarse iterates: rows of cp elements, step*cp apart
 	CDR_CUDA_TRY(cudaMemset2DAsync(xc, sel.step * cp * sizeof(T), 0, cp * sizeof(T), sel.count, st));
 	if (l + 1 == L() - 1) CDR_TRY(solve_cg_2d<T>(abd + f * abd_size(), xc, bc, dc, st));
-	else if (l + 1 == lc) CDR_TRY(fused<T>(l + 1, sel));
+	else if (l + 1 == lc[sizeof(T) == 4]) CDR_TRY(fused<T>(l + 1, sel));
 	else CDR_TRY(ncycle<T>(l + 1, sel));
 	CDR_TRY(interp_add_2d<T>(ci, xc, r, so, x, df, dc, st, F.ns));
 	CDR_TRY(smooth<T>(l, sel, CDR_UP));
 	return CDR_OK;
+}
+
+// First level (not the fine one) of the fused coarse cycle: both edges at most
+// fuse_coarse and the level's shared-memory copy within the limit
+template <typename T>
+int Batch2::pick_fused()
+{
+	if (s.fuse_coarse <= 0) return -1;
+	for (int l0 = 1; l0 + 1 < L(); ++l0) {
+		if (lv[l0].nx > s.fuse_coarse || lv[l0].ny > s.fuse_coarse || L() - l0 > kMaxCoarseLevels) continue;
+		CoarseCycle<T> cc;
+		cc.nl = L() - l0;
+		cc.relax = s.relaxation;
+		for (int l = l0; l < L(); ++l) {
+			CoarseLevel<T> &c = cc.lv[l - l0];
+			c.nx = lv[l].nx;
+			c.ny = lv[l].ny;
+			c.ns = lv[l].ns;
+		}
+		if (coarse_cycle_bytes(cc) <= kCoarseSmemMax) return l0;
+	}
+	return -1;
 }
 
 // Levels l0..L-1 of the selected problems in one launch, one CTA per problem

@@ -41,7 +41,7 @@ public:
 	std::vector<B2Level> lv;
 	double *abd = nullptr;
 	int *info = nullptr;  // [0] line factorizations, [1] coarse Cholesky
-	int lc = -1;          // first level of the fused coarse cycle (-1: none)
+	int lc[2] = {-1, -1}; // first level of the fused coarse cycle, [0] FP64, [1] FP32 (-1: none)
 	cudaStream_t st = nullptr;
 
 	Batch2() = default;
@@ -75,6 +75,8 @@ private:
 	int ncycle(int l, Sel sel);
 	template <typename T>
 	int fused(int l0, Sel sel);
+	template <typename T>
+	int pick_fused();
 };
 
 // cdr2::solver::compute_num_levels (include/cedar/2d/solver.h:63-79)

@@ -12,12 +12,14 @@
 // shared memory (as the exact line kernels do), so the result is the one the
 // separate kernels give in CDR_LINES_EXACT mode.
 //
-// Measured on B200 (FP32 line-xy, levels 64^2 .. 4^2 of a 511^2 problem): 508 us
-// per cycle, against ~300 us for the ~70 separate launches it replaces: each of
-// its ~160 barrier-separated phases waits on L2 latency (2-3 us per phase), so
-// the solvers leave it off unless gpu.fuse-coarse asks for it.  Keeping each
-// level's operator and factors in shared memory across a level visit would make
-// the phases shared-memory bound.
+// Each level visit copies the level's operator, smoother factors, b, x and r
+// into shared memory (compact rows), runs every smoothing phase there and
+// writes x and r back: the barrier-separated phases then wait on shared memory
+// instead of L2 (a first version that worked on L2 took 508 us per cycle for
+// levels 64^2 .. 4^2, against ~300 us for the separate launches).  Levels of at
+// most 32^2 are fused by default: FP32+IR and FP64 solves of the 2047^2 line-xy
+// problem are 4-5 % faster than with separate launches; fusing from 64^2 is
+// slower in FP32 (its 64-point sequential line solves dominate).
 #include <algorithm>
 
 #include "k2_point.cuh"
@@ -97,8 +99,9 @@ __device__ void cc_gs(const CoarseLevel<T> &L, int updown)
 }
 
 // One zebra line sweep (both colours, relax_lines_2d's order).  Each colour:
-// right-hand sides, pivots and multipliers of its lines are staged in shared
-// memory by all threads, then one thread per line runs DPTTS2's substitutions.
+// the right-hand sides of its lines are formed by all threads into sm, then one
+// thread per line runs DPTTS2's substitutions with the level's (shared-memory)
+// pivots and multipliers.
 template <typename T, int NS, int DIR>
 __device__ void cc_lines(const CoarseLevel<T> &L, int updown, T *sm)
 {
@@ -112,21 +115,30 @@ __device__ void cc_lines(const CoarseLevel<T> &L, int updown, T *sm)
 	for (int c = 0; c < 2; ++c) {
 		const int first = firsts[c];
 		const int ml = first > nl ? 0 : (nl - first) / 2 + 1;  // lines of this colour
-		T *R = sm, *D = sm + ml * n, *E = sm + 2 * ml * n;
+		T *R = sm;
 		for (int e = threadIdx.x; e < ml * n; e += CC_THREADS) {
 			const int g = e / n, m = e - g * n, lc = first + 2 * g;
 			const size_t k = DIR == CDR_DIR_X ? d.at(m + 1, lc) : d.at(lc, m + 1);
 			R[e] = line_rhs<T, NS, DIR>(L.so, ps, L.x, L.b, k, L.pitch);
-			const size_t fo = DIR == CDR_DIR_X ? (size_t)lc * L.pitch + m + 1 : (size_t)lc * L.tpitch + m + 1;
-			D[e] = fac[fo];
-			E[e] = fac[eplane + fo];
 		}
 		__syncthreads();
 		if (threadIdx.x < ml) {
-			T *r = R + threadIdx.x * n, *dd = D + threadIdx.x * n, *ee = E + threadIdx.x * n;
-			for (int m = 1; m < n; ++m) r[m] = r[m] - r[m - 1] * ee[m];
-			r[n - 1] = pivot_div(r[n - 1], dd[n - 1]);
-			for (int m = n - 2; m >= 0; --m) r[m] = pivot_div(r[m], dd[m]) - r[m + 1] * ee[m + 1];
+			const int lc = first + 2 * threadIdx.x;
+			// factors of position p at dd[p], ee[p] (position 1 is r[0])
+			const T *dd = fac + (DIR == CDR_DIR_X ? (size_t)lc * L.pitch : (size_t)lc * L.tpitch);
+			const T *ee = dd + eplane;
+			T *r = R + threadIdx.x * n;
+			T y = r[0];
+			for (int m = 1; m < n; ++m) {
+				y = r[m] - y * ee[m + 1];
+				r[m] = y;
+			}
+			T xv = pivot_div(y, dd[n]);
+			r[n - 1] = xv;
+			for (int m = n - 2; m >= 0; --m) {
+				xv = pivot_div(r[m], dd[m + 1]) - xv * ee[m + 2];
+				r[m] = xv;
+			}
 		}
 		__syncthreads();
 		for (int e = threadIdx.x; e < ml * n; e += CC_THREADS) {
@@ -207,14 +219,70 @@ __device__ CoarseLevel<T> cc_level(const CoarseCycle<T> &cc, int l)
 	return L;
 }
 
+// Shared-memory copy of a level for one visit: its operator, smoother factors,
+// b, x and r with compact rows (pitch nx+2; y-line factors tpitch ny+2).
+template <typename T>
+__device__ CoarseLevel<T> cc_view(const CoarseLevel<T> &G, int relax, T *base)
+{
+	CoarseLevel<T> S = G;
+	S.pitch = G.nx + 2;
+	S.tpitch = G.ny + 2;
+	const size_t pl = (size_t)(G.nx + 2) * (G.ny + 2);
+	T *p = base;
+	S.so = p;
+	p += G.ns * pl;
+	if (relax == CDR_RELAX_POINT) { S.sor = p; p += pl; }
+	else if (relax != CDR_RELAX_LINE_Y) { S.sor = p; p += 2 * pl; }
+	else S.sor = nullptr;
+	if (relax == CDR_RELAX_LINE_Y || relax == CDR_RELAX_LINE_XY) { S.sory = p; p += 2 * pl; }
+	else S.sory = nullptr;
+	S.b = p; p += pl;
+	S.x = p; p += pl;
+	S.r = p;
+	S.ci = nullptr;
+	return S;
+}
+
+// copy nplanes planes of (ny+2) rows of nx+2 elements between pitches
+template <typename T>
+__device__ void cc_copy(const T *__restrict__ src, int sp, size_t splane, T *__restrict__ dst, int dp, size_t dplane,
+                        int rowlen, int rows, int nplanes)
+{
+	const int per = rowlen * rows;
+	for (int e = threadIdx.x; e < per * nplanes; e += CC_THREADS) {
+		const int q = e / per, rem = e - q * per, j = rem / rowlen, i = rem - j * rowlen;
+		dst[(size_t)q * dplane + (size_t)j * dp + i] = src[(size_t)q * splane + (size_t)j * sp + i];
+	}
+}
+
+template <typename T>
+__device__ void cc_stage(const CoarseLevel<T> &G, const CoarseLevel<T> &S, int relax, bool with_r)
+{
+	const size_t gpl = (size_t)G.pitch * (G.ny + 2), spl = (size_t)S.pitch * (S.ny + 2);
+	const int ii = G.nx + 2, jj = G.ny + 2;
+	cc_copy<T>(G.so, G.pitch, gpl, const_cast<T *>(S.so), S.pitch, spl, ii, jj, G.ns);
+	if (S.sor) cc_copy<T>(G.sor, G.pitch, gpl, const_cast<T *>(S.sor), S.pitch, spl, ii, jj, relax == CDR_RELAX_POINT ? 1 : 2);
+	if (S.sory)  // transposed: nx+2 rows of ny+2 elements
+		cc_copy<T>(G.sory, G.tpitch, (size_t)G.tpitch * ii, const_cast<T *>(S.sory), S.tpitch, (size_t)S.tpitch * ii, jj,
+		           ii, 2);
+	cc_copy<T>(G.b, G.pitch, gpl, S.b, S.pitch, spl, ii, jj, 1);
+	cc_copy<T>(G.x, G.pitch, gpl, S.x, S.pitch, spl, ii, jj, 1);
+	if (with_r) cc_copy<T>(G.r, G.pitch, gpl, S.r, S.pitch, spl, ii, jj, 1);
+	__syncthreads();
+}
+
 template <typename T>
 __global__ void __launch_bounds__(CC_THREADS) k_coarse_cycle(CoarseCycle<T> cc)
 {
 	extern __shared__ __align__(16) unsigned char cc_smem[];
-	T *sm = reinterpret_cast<T *>(cc_smem);
+	T *lvl = reinterpret_cast<T *>(cc_smem);  // the visited level
+	T *sm = lvl + cc.level_elems;              // line right-hand sides
 	const int nl = cc.nl;
 	for (int l = 0; l + 1 < nl; ++l) {
-		const CoarseLevel<T> F = cc_level(cc, l), C = cc_level(cc, l + 1);
+		const CoarseLevel<T> G = cc_level(cc, l), C = cc_level(cc, l + 1);
+		const CoarseLevel<T> F = cc_view(G, cc.relax, lvl);
+		// r too: restriction reads its ghost layer (zero) for odd edges
+		cc_stage(G, F, cc.relax, true);
 		if (F.ns == 5) cc_smooth<T, 5>(cc, F, CDR_DOWN, sm);
 		else cc_smooth<T, 3>(cc, F, CDR_DOWN, sm);
 		if (F.ns == 5) cc_residual<T, 5>(F);
@@ -222,6 +290,10 @@ __global__ void __launch_bounds__(CC_THREADS) k_coarse_cycle(CoarseCycle<T> cc)
 		__syncthreads();
 		cc_restrict<T>(F, C);
 		cc_zero<T>(C);
+		// x and r of this level are needed again on the way up
+		const size_t gpl = (size_t)G.pitch * (G.ny + 2), spl = (size_t)F.pitch * (F.ny + 2);
+		cc_copy<T>(F.x, F.pitch, spl, G.x, G.pitch, gpl, G.nx + 2, G.ny + 2, 1);
+		cc_copy<T>(F.r, F.pitch, spl, G.r, G.pitch, gpl, G.nx + 2, G.ny + 2, 1);
 		__syncthreads();
 	}
 	{
@@ -231,29 +303,57 @@ __global__ void __launch_bounds__(CC_THREADS) k_coarse_cycle(CoarseCycle<T> cc)
 		__syncthreads();
 	}
 	for (int l = nl - 2; l >= 0; --l) {
-		const CoarseLevel<T> F = cc_level(cc, l), C = cc_level(cc, l + 1);
+		const CoarseLevel<T> G = cc_level(cc, l), C = cc_level(cc, l + 1);
+		const CoarseLevel<T> F = cc_view(G, cc.relax, lvl);
+		cc_stage(G, F, cc.relax, true);
 		cc_interp<T>(F, C);
 		__syncthreads();
 		if (F.ns == 5) cc_smooth<T, 5>(cc, F, CDR_UP, sm);
 		else cc_smooth<T, 3>(cc, F, CDR_UP, sm);
 		__syncthreads();
+		cc_copy<T>(F.x, F.pitch, (size_t)F.pitch * (F.ny + 2), G.x, G.pitch, (size_t)G.pitch * (G.ny + 2), G.nx + 2,
+		           G.ny + 2, 1);
+		__syncthreads();
 	}
 }
 
+// Elements of the shared copy of one level (cc_view's layout)
 template <typename T>
-size_t coarse_cycle_smem(const CoarseCycle<T> &cc)
+size_t cc_level_elems(const CoarseLevel<T> &L, int relax)
 {
-	size_t need = 0;
+	const size_t pl = (size_t)(L.nx + 2) * (L.ny + 2);
+	size_t planes = L.ns + 3;  // so, b, x, r
+	if (relax == CDR_RELAX_POINT) planes += 1;
+	else if (relax != CDR_RELAX_LINE_Y) planes += 2;
+	if (relax == CDR_RELAX_LINE_Y || relax == CDR_RELAX_LINE_XY) planes += 2;
+	return planes * pl;
+}
+
+template <typename T>
+size_t coarse_cycle_smem(const CoarseCycle<T> &cc, size_t *level_elems)
+{
+	size_t lvl = 0, lines = 0;
 	for (int l = 0; l + 1 < cc.nl; ++l) {
 		const CoarseLevel<T> &L = cc.lv[l];
-		const size_t lx = (size_t)((L.ny + 1) / 2) * L.nx, ly = (size_t)((L.nx + 1) / 2) * L.ny;
-		need = std::max(need, 3 * std::max(lx, ly) * sizeof(T));
+		lvl = std::max(lvl, cc_level_elems(L, cc.relax));
+		lines = std::max(lines, std::max((size_t)((L.ny + 1) / 2) * L.nx, (size_t)((L.nx + 1) / 2) * L.ny));
 	}
+	lvl = (lvl + 1) / 2 * 2;  // keep the line buffer 8-byte aligned
+	*level_elems = lvl;
 	const CoarseLevel<T> &Cg = cc.lv[cc.nl - 1];
 	const size_t n = (size_t)Cg.nx * Cg.ny;
-	need = std::max(need, (n + (size_t)(Cg.nx + 2) * n) * sizeof(double));
-	return need;
+	return std::max((lvl + lines) * sizeof(T), (n + (size_t)(Cg.nx + 2) * n) * sizeof(double));
 }
+
+// Shared memory a fused coarse cycle from level descriptor lv[0..nl) needs
+template <typename T>
+size_t coarse_cycle_bytes(const CoarseCycle<T> &cc)
+{
+	size_t e;
+	return coarse_cycle_smem(cc, &e);
+}
+template size_t coarse_cycle_bytes<double>(const CoarseCycle<double> &);
+template size_t coarse_cycle_bytes<float>(const CoarseCycle<float> &);
 
 template <typename T>
 int coarse_cycle(const CoarseCycle<T> &cc, int nproblems, cudaStream_t st)
@@ -262,12 +362,15 @@ int coarse_cycle(const CoarseCycle<T> &cc, int nproblems, cudaStream_t st)
 		set_error(CDR_ERR_DIM, "fused coarse cycle over %d levels", cc.nl);
 		return CDR_ERR_DIM;
 	}
-	const size_t smem = coarse_cycle_smem(cc);
-	if (smem > 200 * 1024) {
+	CoarseCycle<T> c2 = cc;
+	size_t lvl = 0;
+	const size_t smem = coarse_cycle_smem(c2, &lvl);
+	c2.level_elems = lvl;
+	if (smem > kCoarseSmemMax) {
 		set_error(CDR_ERR_DIM, "fused coarse cycle needs %zu bytes of shared memory", smem);
 		return CDR_ERR_DIM;
 	}
-	k_coarse_cycle<T><<<nproblems, CC_THREADS, smem, st>>>(cc);
+	k_coarse_cycle<T><<<nproblems, CC_THREADS, smem, st>>>(c2);
 	CDR_LAUNCH_CHECK();
 	return CDR_OK;
 }
@@ -277,8 +380,8 @@ template int coarse_cycle<double>(const CoarseCycle<double> &, int, cudaStream_t
 // process, before any graph capture: called from lines_prepare).
 int coarse_prepare()
 {
-	CDR_CUDA_TRY(cudaFuncSetAttribute(k_coarse_cycle<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
-	CDR_CUDA_TRY(cudaFuncSetAttribute(k_coarse_cycle<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+	CDR_CUDA_TRY(cudaFuncSetAttribute(k_coarse_cycle<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kCoarseSmemMax));
+	CDR_CUDA_TRY(cudaFuncSetAttribute(k_coarse_cycle<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kCoarseSmemMax));
 	return CDR_OK;
 }
 template int coarse_cycle<float>(const CoarseCycle<float> &, int, cudaStream_t);

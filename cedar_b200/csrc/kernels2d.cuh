@@ -53,7 +53,12 @@ struct CoarseCycle {
 	int nl = 0;
 	const double *abd = nullptr;
 	int relax = CDR_RELAX_POINT, npre = 2, npost = 1, bstep = 1;
+	size_t level_elems = 0;  // set by the launcher: shared elements of one level copy
 };
+// shared memory of the fused kernel (bytes) and its limit
+constexpr size_t kCoarseSmemMax = 220 * 1024;
+template <typename T>
+size_t coarse_cycle_bytes(const CoarseCycle<T> &cc);
 template <typename T>
 int coarse_cycle(const CoarseCycle<T> &cc, int nproblems, cudaStream_t st);
 int coarse_prepare();

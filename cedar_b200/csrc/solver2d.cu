@@ -52,7 +52,7 @@ struct cdr_gpu_solver {
 	double *h_norm = nullptr;   // pinned host copy of the norm
 	cudaStream_t st = nullptr;
 	bool own_stream = false;
-	int lc = -1;  // first level of the fused coarse cycle (-1: none)
+	int lc[2] = {-1, -1};  // first level of the fused coarse cycle, [0] FP64, [1] FP32 (-1: none)
 	cudaGraphExec_t gexec[2] = {nullptr, nullptr};  // cycle graphs: [0] FP64, [1] FP32
 	long long glaunches[2] = {0, 0};                 // kernel launches per replay
 	cudaEvent_t ev0 = nullptr, ev1 = nullptr;
@@ -151,7 +151,7 @@ int cdr_gpu_solver::ncycle(int l, T *x, const T *b)
 	CDR_TRY(restrict_2d<T>(Arr<T>::ci(C), Arr<T>::r(F), Arr<T>::b(C), F.d, C.d, st));
 	CDR_CUDA_TRY(cudaMemsetAsync(Arr<T>::x(C), 0, sizeof(T) * C.d.plane(), st));
 	if (l + 1 == L() - 1) CDR_TRY(solve_cg_2d<T>(abd, Arr<T>::x(C), Arr<T>::b(C), C.d, st));
-	else if (l + 1 == lc) CDR_TRY(fused<T>(l + 1));
+	else if (l + 1 == lc[sizeof(T) == 4]) CDR_TRY(fused<T>(l + 1));
 	else CDR_TRY(ncycle<T>(l + 1, Arr<T>::x(C), Arr<T>::b(C)));
 	CDR_TRY(interp_add_2d<T>(Arr<T>::ci(C), Arr<T>::x(C), Arr<T>::r(F), Arr<T>::so(F), x, F.d, C.d, st));
 	CDR_TRY(smooth<T>(l, x, b, CDR_UP));
@@ -161,11 +161,24 @@ int cdr_gpu_solver::ncycle(int l, T *x, const T *b)
 // Levels l0..L-1 in one launch (k2_coarse.cu); same operations as ncycle with
 // the sequential line substitutions.
 template <typename T>
+CoarseCycle<T> coarse_desc(std::vector<Level> &lv, int l0, const cdr_gpu_settings &s);
+
+template <typename T>
 int cdr_gpu_solver::fused(int l0)
 {
+	CoarseCycle<T> cc = coarse_desc<T>(lv, l0, s);
+	cc.abd = abd;
+	return coarse_cycle<T>(cc, 1, st);
+}
+
+// Descriptor of the fused coarse cycle over levels l0..L-1
+template <typename T>
+CoarseCycle<T> coarse_desc(std::vector<Level> &lv, int l0, const cdr_gpu_settings &s)
+{
+	const int L = (int)lv.size();
 	CoarseCycle<T> cc;
-	cc.nl = L() - l0;
-	for (int l = l0; l < L(); ++l) {
+	cc.nl = L - l0;
+	for (int l = l0; l < L; ++l) {
 		Level &V = lv[l];
 		CoarseLevel<T> &c = cc.lv[l - l0];
 		c.so = Arr<T>::so(V);
@@ -181,11 +194,24 @@ int cdr_gpu_solver::fused(int l0)
 		c.tpitch = V.tpitch;
 		c.ns = V.ns;
 	}
-	cc.abd = abd;
 	cc.relax = s.relaxation;
 	cc.npre = s.nrelax_pre;
 	cc.npost = s.nrelax_post;
-	return coarse_cycle<T>(cc, 1, st);
+	return cc;
+}
+
+// First level (not the fine one) from which the fused coarse cycle runs: both
+// edges at most fuse_coarse and the level's shared-memory copy within the limit.
+template <typename T>
+int pick_fused_level(std::vector<Level> &lv, const cdr_gpu_settings &s)
+{
+	const int L = (int)lv.size();
+	if (s.fuse_coarse <= 0) return -1;
+	for (int l = 1; l + 1 < L; ++l) {
+		if (lv[l].nx > s.fuse_coarse || lv[l].ny > s.fuse_coarse || L - l > kMaxCoarseLevels) continue;
+		if (coarse_cycle_bytes(coarse_desc<T>(lv, l, s)) <= kCoarseSmemMax) return l;
+	}
+	return -1;
 }
 
 template <typename T>
@@ -315,7 +341,7 @@ int cdr_gpu_settings_default(cdr_gpu_settings *s)
 	s->precision = CDR_PREC_F64;
 	s->use_graph = 1;
 	s->line_flags = 0;
-	s->fuse_coarse = 0;
+	s->fuse_coarse = 32;
 	return CDR_OK;
 }
 
@@ -396,12 +422,8 @@ static int create_impl(cdr_gpu_solver *h, const double *so_src, int ns, int nx, 
 	}
 	// the fused coarse cycle takes over from the first level that fits (not the
 	// fine level, whose arrays the caller may pass), when it spans two levels or more
-	if (s.fuse_coarse > 0)
-		for (int l = 1; l + 1 < nl && l < kMaxCoarseLevels; ++l)
-			if (h->lv[l].nx <= s.fuse_coarse && h->lv[l].ny <= s.fuse_coarse && nl - l <= kMaxCoarseLevels) {
-				h->lc = l;
-				break;
-			}
+	h->lc[0] = pick_fused_level<double>(h->lv, s);
+	h->lc[1] = pick_fused_level<float>(h->lv, s);
 	Level &Cg = h->lv[nl - 1];
 	if ((size_t)Cg.nx * Cg.ny > 4096) {
 		set_error(CDR_ERR_DIM, "coarsest grid %dx%d too large for the banded Cholesky", Cg.nx, Cg.ny);

@@ -224,7 +224,7 @@ typedef struct cdr_gpu_settings {
 	int precision;    /* CDR_PREC_F64 (default) or CDR_PREC_F32_IR                     */
 	int use_graph;    /* replay the cycle as a CUDA graph (default 1)                  */
 	int line_flags;   /* CDR_LINES_EXACT for sequential line substitutions (default 0) */
-	int fuse_coarse;  /* levels with both edges <= this run as one fused kernel (default 0 = off) */
+	int fuse_coarse;  /* levels with both edges <= this run as one fused kernel (default 32, 0 = off) */
 } cdr_gpu_settings;
 
 typedef struct cdr_gpu_solver cdr_gpu_solver;
