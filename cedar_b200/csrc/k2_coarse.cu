@@ -99,9 +99,11 @@ __device__ void cc_gs(const CoarseLevel<T> &L, int updown)
 }
 
 // One zebra line sweep (both colours, relax_lines_2d's order).  Each colour:
-// the right-hand sides of its lines are formed by all threads into sm, then one
-// thread per line runs DPTTS2's substitutions with the level's (shared-memory)
-// pivots and multipliers.
+// the right-hand sides of its lines are formed by all threads into sm, then the
+// substitutions run with the level's (shared-memory) pivots and multipliers:
+// DPTTS2's sequential order in FP64 (one thread per line), affine-map scans over
+// the lanes of one warp per line in FP32 (the preconditioner has no bitwise
+// target; the separate FP32 kernels scan too).
 template <typename T, int NS, int DIR>
 __device__ void cc_lines(const CoarseLevel<T> &L, int updown, T *sm)
 {
@@ -122,22 +124,74 @@ __device__ void cc_lines(const CoarseLevel<T> &L, int updown, T *sm)
 			R[e] = line_rhs<T, NS, DIR>(L.so, ps, L.x, L.b, k, L.pitch);
 		}
 		__syncthreads();
-		if (threadIdx.x < ml) {
-			const int lc = first + 2 * threadIdx.x;
-			// factors of position p at dd[p], ee[p] (position 1 is r[0])
-			const T *dd = fac + (DIR == CDR_DIR_X ? (size_t)lc * L.pitch : (size_t)lc * L.tpitch);
-			const T *ee = dd + eplane;
-			T *r = R + threadIdx.x * n;
-			T y = r[0];
-			for (int m = 1; m < n; ++m) {
-				y = r[m] - y * ee[m + 1];
-				r[m] = y;
+		if constexpr (sizeof(T) == 8) {
+			// FP64: DPTTS2's sequential substitutions, one thread per line
+			if (threadIdx.x < ml) {
+				const int lc = first + 2 * threadIdx.x;
+				// factors of position p at dd[p], ee[p] (position 1 is r[0])
+				const T *dd = fac + (DIR == CDR_DIR_X ? (size_t)lc * L.pitch : (size_t)lc * L.tpitch);
+				const T *ee = dd + eplane;
+				T *r = R + threadIdx.x * n;
+				T y = r[0];
+				for (int m = 1; m < n; ++m) {
+					y = r[m] - y * ee[m + 1];
+					r[m] = y;
+				}
+				T xv = pivot_div(y, dd[n]);
+				r[n - 1] = xv;
+				for (int m = n - 2; m >= 0; --m) {
+					xv = pivot_div(r[m], dd[m + 1]) - xv * ee[m + 2];
+					r[m] = xv;
+				}
 			}
-			T xv = pivot_div(y, dd[n]);
-			r[n - 1] = xv;
-			for (int m = n - 2; m >= 0; --m) {
-				xv = pivot_div(r[m], dd[m + 1]) - xv * ee[m + 2];
-				r[m] = xv;
+		} else {
+			// FP32: one warp per line, each lane a chunk of consecutive positions;
+			// both substitutions as affine-map scans over the lanes (shuffles)
+			const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+			const int cs = (n + 31) / 32;  // chunk length
+			for (int g = warp; g < ml; g += CC_THREADS / 32) {
+				const int lc = first + 2 * g;
+				const T *dd = fac + (DIR == CDR_DIR_X ? (size_t)lc * L.pitch : (size_t)lc * L.tpitch);
+				const T *ee = dd + eplane;
+				T *r = R + g * n;
+				const int lo = lane * cs < n ? lane * cs : n, hi = lo + cs < n ? lo + cs : n;
+				// forward y(m) = r(m) - y(m-1) E(m+1), y(0) = r(0)
+				T A = T(1), B = T(0);
+				for (int m = lo; m < hi; ++m) {
+					const T a = m == 0 ? T(0) : -ee[m + 1];
+					B = madd(a, B, r[m]);
+					A = a * A;
+				}
+				for (int off = 1; off < 32; off <<= 1) {
+					const T a2 = __shfl_up_sync(0xffffffffu, A, off), b2 = __shfl_up_sync(0xffffffffu, B, off);
+					if (lane >= off) { B = madd(A, b2, B); A = A * a2; }
+				}
+				T y = __shfl_up_sync(0xffffffffu, B, 1);
+				if (lane == 0) y = T(0);
+				for (int m = lo; m < hi; ++m) {
+					y = m == 0 ? r[0] : madd(-y, ee[m + 1], r[m]);
+					r[m] = pivot_div(y, dd[m + 1]);
+				}
+				__syncwarp();
+				// backward x(m) = y(m)/D(m+1) - x(m+1) E(m+2), x(n-1) = y(n-1)/D(n)
+				A = T(1);
+				B = T(0);
+				for (int m = hi - 1; m >= lo; --m) {
+					const T a = m == n - 1 ? T(0) : -ee[m + 2];
+					B = madd(a, B, r[m]);
+					A = a * A;
+				}
+				for (int off = 1; off < 32; off <<= 1) {
+					const T a2 = __shfl_down_sync(0xffffffffu, A, off), b2 = __shfl_down_sync(0xffffffffu, B, off);
+					if (lane + off < 32) { B = madd(A, b2, B); A = A * a2; }
+				}
+				T xv = __shfl_down_sync(0xffffffffu, B, 1);
+				if (lane == 31) xv = T(0);
+				for (int m = hi - 1; m >= lo; --m) {
+					xv = m == n - 1 ? r[m] : madd(-xv, ee[m + 2], r[m]);
+					r[m] = xv;
+				}
+				__syncwarp();
 			}
 		}
 		__syncthreads();

@@ -548,10 +548,12 @@ static int launch_lines(const T *so, T *x, const T *b, const T *sor, Dims2 d, in
 	// 16-byte aligned base pointers; lines up to 2048*8 - 1 points.
 	const int fpitch = DIR == CDR_DIR_X ? d.pitch : tpitch;
 	const bool aligned = ((uintptr_t)so | (uintptr_t)x | (uintptr_t)b | (uintptr_t)sor) % 16 == 0;
-	// x: K = 8, 256 threads, 256/TPL lines per CTA.  y: K = 16 for long lines so that
-	// a warp holds 8 lines side by side, at most 32 lines per CTA (lanes are
-	// line-fastest: every warp holds the same lines).
-	const int K = (DIR == CDR_DIR_Y && sizeof(T) == 4 && n + 1 > 8 * 128) ? 16 : 8;
+	// x: K = 8, 256 threads, 256/TPL lines per CTA.  y: K = 16 for lines longer
+	// than 1024 points so that a warp holds 8 lines side by side, at most 32 lines
+	// per CTA (lanes are line-fastest: every warp holds the same lines).  Fewer
+	// lines per CTA would fill more SMs on mid-size levels but halve the
+	// coalescing across lines, which costs more (measured).
+	const int K = (DIR == CDR_DIR_Y && sizeof(T) == 4 && n > 8 * 128) ? 16 : 8;
 	if (!exact && aligned && d.pitch % 16 == 0 && fpitch % 16 == 0 && n + 1 <= 256 * K) {
 		int tpl_log2 = 0;
 		while ((1 << tpl_log2) * K < n + 1) ++tpl_log2;
