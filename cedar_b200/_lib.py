@@ -93,19 +93,19 @@ def load(path=LIB_PATH):
         "cdr_gpu_galerkin_2d_f64": (I, [P, I, P, P, I, I, I, I, I, I, S]),
         "cdr_gpu_setup_cg_2d_f64": (I, [P, I, I, I, I, P, P, S]),
         # 3D
-        "cdr_gpu_residual_3d_f64": (I, [P, P, P, P, I, I, I, I, P, P, S]),
-        "cdr_gpu_residual_3d_f32": (I, [P, P, P, P, I, I, I, I, P, P, S]),
+        "cdr_gpu_residual_3d_f64": (I, [P, I, P, P, P, I, I, I, I, P, P, S]),
+        "cdr_gpu_residual_3d_f32": (I, [P, I, P, P, P, I, I, I, I, P, P, S]),
         "cdr_gpu_setup_recip_3d_f64": (I, [P, P, I, I, I, I, S]),
-        "cdr_gpu_relax_point_3d_f64": (I, [P, P, P, P, I, I, I, I, I, S]),
-        "cdr_gpu_relax_point_3d_f32": (I, [P, P, P, P, I, I, I, I, I, S]),
+        "cdr_gpu_relax_point_3d_f64": (I, [P, I, P, P, P, I, I, I, I, I, S]),
+        "cdr_gpu_relax_point_3d_f32": (I, [P, I, P, P, P, I, I, I, I, I, S]),
         "cdr_gpu_restrict_3d_f64": (I, [P, P, P] + [I] * 8 + [S]),
         "cdr_gpu_interp_add_3d_f64": (I, [P, P, P, P, P] + [I] * 8 + [S]),
-        "cdr_gpu_setup_interp_3d_f64": (I, [P, P] + [I] * 8 + [S]),
-        "cdr_gpu_galerkin_3d_f64": (I, [P, P, P] + [I] * 8 + [S]),
-        "cdr_gpu_setup_cg_3d_f64": (I, [P, I, I, I, I, P, P, S]),
+        "cdr_gpu_setup_interp_3d_f64": (I, [P, I, P] + [I] * 8 + [S]),
+        "cdr_gpu_galerkin_3d_f64": (I, [P, I, P, P] + [I] * 8 + [S]),
+        "cdr_gpu_setup_cg_3d_f64": (I, [P, I, I, I, I, I, P, P, S]),
         "cdr_gpu_solve_cg_3d_f64": (I, [P, P, P, I, I, I, I, S]),
-        "cdr_gpu_solver3_create": (I, [ctypes.POINTER(Settings), P, I, I, I, S, ctypes.POINTER(P)]),
-        "cdr_gpu_solver3_create_device": (I, [ctypes.POINTER(Settings), P, I, I, I, I, S, ctypes.POINTER(P)]),
+        "cdr_gpu_solver3_create": (I, [ctypes.POINTER(Settings), P, I, I, I, I, S, ctypes.POINTER(P)]),
+        "cdr_gpu_solver3_create_device": (I, [ctypes.POINTER(Settings), P, I, I, I, I, I, S, ctypes.POINTER(P)]),
         "cdr_gpu_solver3_destroy": (I, [P]),
         "cdr_gpu_solver3_solve": (I, [P, P, P, ctypes.POINTER(I), P, I]),
         "cdr_gpu_solver3_solve_device": (I, [P, P, P, I, ctypes.POINTER(I), P, I]),

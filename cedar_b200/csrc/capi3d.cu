@@ -25,6 +25,15 @@ int check_pair3(int nxf, int nyf, int nzf, int pf, int nxc, int nyc, int nzc, in
 	return CDR_OK;
 }
 
+int check_ns3(int ns)
+{
+	if (ns != 4 && ns != 14) {
+		set_error(CDR_ERR_ARG, "nstencil %d: 3D operators have 4 (seven-point) or 14 (27-point) planes", ns);
+		return CDR_ERR_ARG;
+	}
+	return CDR_OK;
+}
+
 #define NONNULL3(p)                                                \
 	do {                                                           \
 		if (!(p)) {                                                \
@@ -37,22 +46,24 @@ int check_pair3(int nxf, int nyf, int nzf, int pf, int nxc, int nyc, int nzc, in
 
 extern "C" {
 
-int cdr_gpu_residual_3d_f64(const double *so, const double *x, const double *b, double *r, int nx, int ny, int nz,
-                            int pitch, double *norm_out, void *scratch, cudaStream_t s)
+int cdr_gpu_residual_3d_f64(const double *so, int nstencil, const double *x, const double *b, double *r, int nx,
+                            int ny, int nz, int pitch, double *norm_out, void *scratch, cudaStream_t s)
 {
 	CDR_TRY(check_grid3(nx, ny, nz, pitch));
+	CDR_TRY(check_ns3(nstencil));
 	NONNULL3(so); NONNULL3(x); NONNULL3(b); NONNULL3(r);
 	if (norm_out) NONNULL3(scratch);
-	return residual_3d<double>(so, x, b, r, Dims3{nx, ny, nz, pitch}, norm_out, (double *)scratch, s);
+	return residual_3d<double>(so, x, b, r, Dims3{nx, ny, nz, pitch}, norm_out, (double *)scratch, s, nstencil);
 }
 
-int cdr_gpu_residual_3d_f32(const float *so, const float *x, const float *b, float *r, int nx, int ny, int nz,
-                            int pitch, double *norm_out, void *scratch, cudaStream_t s)
+int cdr_gpu_residual_3d_f32(const float *so, int nstencil, const float *x, const float *b, float *r, int nx, int ny,
+                            int nz, int pitch, double *norm_out, void *scratch, cudaStream_t s)
 {
 	CDR_TRY(check_grid3(nx, ny, nz, pitch));
+	CDR_TRY(check_ns3(nstencil));
 	NONNULL3(so); NONNULL3(x); NONNULL3(b); NONNULL3(r);
 	if (norm_out) NONNULL3(scratch);
-	return residual_3d<float>(so, x, b, r, Dims3{nx, ny, nz, pitch}, norm_out, (double *)scratch, s);
+	return residual_3d<float>(so, x, b, r, Dims3{nx, ny, nz, pitch}, norm_out, (double *)scratch, s, nstencil);
 }
 
 int cdr_gpu_setup_recip_3d_f64(const double *so, double *sor, int nx, int ny, int nz, int pitch, cudaStream_t s)
@@ -62,20 +73,22 @@ int cdr_gpu_setup_recip_3d_f64(const double *so, double *sor, int nx, int ny, in
 	return setup_recip_3d<double>(so, sor, Dims3{nx, ny, nz, pitch}, s);
 }
 
-int cdr_gpu_relax_point_3d_f64(const double *so, double *x, const double *b, const double *sor, int nx, int ny,
-                               int nz, int pitch, int updown, cudaStream_t s)
+int cdr_gpu_relax_point_3d_f64(const double *so, int nstencil, double *x, const double *b, const double *sor, int nx,
+                               int ny, int nz, int pitch, int updown, cudaStream_t s)
 {
 	CDR_TRY(check_grid3(nx, ny, nz, pitch));
+	CDR_TRY(check_ns3(nstencil));
 	NONNULL3(so); NONNULL3(x); NONNULL3(b); NONNULL3(sor);
-	return relax_point_3d<double>(so, x, b, sor, Dims3{nx, ny, nz, pitch}, updown, s);
+	return relax_point_3d<double>(so, x, b, sor, Dims3{nx, ny, nz, pitch}, updown, s, nstencil);
 }
 
-int cdr_gpu_relax_point_3d_f32(const float *so, float *x, const float *b, const float *sor, int nx, int ny, int nz,
-                               int pitch, int updown, cudaStream_t s)
+int cdr_gpu_relax_point_3d_f32(const float *so, int nstencil, float *x, const float *b, const float *sor, int nx,
+                               int ny, int nz, int pitch, int updown, cudaStream_t s)
 {
 	CDR_TRY(check_grid3(nx, ny, nz, pitch));
+	CDR_TRY(check_ns3(nstencil));
 	NONNULL3(so); NONNULL3(x); NONNULL3(b); NONNULL3(sor);
-	return relax_point_3d<float>(so, x, b, sor, Dims3{nx, ny, nz, pitch}, updown, s);
+	return relax_point_3d<float>(so, x, b, sor, Dims3{nx, ny, nz, pitch}, updown, s, nstencil);
 }
 
 int cdr_gpu_restrict_3d_f64(const double *ci, const double *rf, double *bc, int nxf, int nyf, int nzf, int pf,
@@ -94,28 +107,31 @@ int cdr_gpu_interp_add_3d_f64(const double *ci, const double *xc, const double *
 	return interp_add_3d<double>(ci, xc, rf, sof, xf, Dims3{nxf, nyf, nzf, pf}, Dims3{nxc, nyc, nzc, pc}, s);
 }
 
-int cdr_gpu_setup_interp_3d_f64(const double *so, double *ci, int nxf, int nyf, int nzf, int pf, int nxc, int nyc,
-                                int nzc, int pc, cudaStream_t s)
+int cdr_gpu_setup_interp_3d_f64(const double *so, int nstencil, double *ci, int nxf, int nyf, int nzf, int pf,
+                                int nxc, int nyc, int nzc, int pc, cudaStream_t s)
 {
 	CDR_TRY(check_pair3(nxf, nyf, nzf, pf, nxc, nyc, nzc, pc));
+	CDR_TRY(check_ns3(nstencil));
 	NONNULL3(so); NONNULL3(ci);
-	return setup_interp_3d(so, ci, Dims3{nxf, nyf, nzf, pf}, Dims3{nxc, nyc, nzc, pc}, s);
+	return setup_interp_3d(so, ci, Dims3{nxf, nyf, nzf, pf}, Dims3{nxc, nyc, nzc, pc}, s, nstencil);
 }
 
-int cdr_gpu_galerkin_3d_f64(const double *so, const double *ci, double *soc, int nxf, int nyf, int nzf, int pf,
-                            int nxc, int nyc, int nzc, int pc, cudaStream_t s)
+int cdr_gpu_galerkin_3d_f64(const double *so, int nstencil, const double *ci, double *soc, int nxf, int nyf, int nzf,
+                            int pf, int nxc, int nyc, int nzc, int pc, cudaStream_t s)
 {
 	CDR_TRY(check_pair3(nxf, nyf, nzf, pf, nxc, nyc, nzc, pc));
+	CDR_TRY(check_ns3(nstencil));
 	NONNULL3(so); NONNULL3(ci); NONNULL3(soc);
-	return galerkin_3d(so, ci, soc, Dims3{nxf, nyf, nzf, pf}, Dims3{nxc, nyc, nzc, pc}, s);
+	return galerkin_3d(so, ci, soc, Dims3{nxf, nyf, nzf, pf}, Dims3{nxc, nyc, nzc, pc}, s, nstencil);
 }
 
-int cdr_gpu_setup_cg_3d_f64(const double *so, int nx, int ny, int nz, int pitch, double *abd, int *info,
-                            cudaStream_t s)
+int cdr_gpu_setup_cg_3d_f64(const double *so, int nstencil, int nx, int ny, int nz, int pitch, double *abd,
+                            int *info, cudaStream_t s)
 {
 	CDR_TRY(check_grid3(nx, ny, nz, pitch));
+	CDR_TRY(check_ns3(nstencil));
 	NONNULL3(so); NONNULL3(abd);
-	return setup_cg_3d(so, Dims3{nx, ny, nz, pitch}, abd, info, s);
+	return setup_cg_3d(so, Dims3{nx, ny, nz, pitch}, abd, info, s, nstencil);
 }
 
 int cdr_gpu_solve_cg_3d_f64(const double *abd, double *x, const double *b, int nx, int ny, int nz, int pitch,

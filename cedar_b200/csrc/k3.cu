@@ -1,10 +1,12 @@
-// k3.cu -- 3D BoxMG kernels (27-point fine operators) for sm_100a.
+// k3.cu -- 3D BoxMG kernels (27- and 7-point fine operators) for sm_100a.
 //
 // Layout: Cedar's 3D arrays with one ghost layer, i fastest, rows padded to a
 // pitch; a k-slice is pitch*(ny+2) elements, a stencil plane
 // pitch*(ny+2)*(nz+2).  Stencil planes (include/cedar/3d/base_types.h:4-20,
 // 1-based as in src/3d/ftn/BMG_stencils_f90.h): kp kpw kps kb kpsw kpnw kbw kbnw
 // kbn kbne kbe kbse kbs kbsw; interpolation weights: 26 planes lxyl .. ltse.
+// A seven-point operator (include/cedar/3d/base_types.h seven_pt) keeps the
+// first four planes only: p, pw, ps, b.
 // Kernel bodies address arrays with the reference's 1-based (I, J, K) through
 // the macros below and keep its operand order, so they reproduce its bits
 // (the library is built without FMA contraction).
@@ -42,6 +44,24 @@ __device__ __forceinline__ T nb27(const T *__restrict__ so, XQ xq, T qf, Dims3 F
 	return nb;
 }
 
+// qf plus the 6 neighbour terms of the seven-point branch
+// (BMG3_SymStd_residual.f90:104-119), in its order.
+template <typename T, typename XQ>
+__device__ __forceinline__ T nb7(const T *__restrict__ so, XQ xq, T qf, Dims3 F, int i, int j, int k)
+{
+	return qf + SO(i, j, k, KPW) * xq(i - 1, j, k) + SO(i, j + 1, k, KPS) * xq(i, j + 1, k)
+	       + SO(i + 1, j, k, KPW) * xq(i + 1, j, k) + SO(i, j, k, KPS) * xq(i, j - 1, k)
+	       + SO(i, j, k, KB) * xq(i, j, k - 1) + SO(i, j, k + 1, KB) * xq(i, j, k + 1);
+}
+
+// Neighbour sum of an NS-plane operator: 14 (27-point) or 4 (seven-point).
+template <int NS, typename T, typename XQ>
+__device__ __forceinline__ T nbs(const T *__restrict__ so, XQ xq, T qf, Dims3 F, int i, int j, int k)
+{
+	if constexpr (NS == 4) return nb7<T>(so, xq, qf, F, i, j, k);
+	else return nb27<T>(so, xq, qf, F, i, j, k);
+}
+
 template <typename T>
 struct Load3 {
 	const T *__restrict__ q;
@@ -52,7 +72,7 @@ struct Load3 {
 // --------------------------------------------------------------- residual
 // BMG3_SymStd_residual (src/3d/ftn/BMG3_SymStd_residual.f90:67-121); grid-stride
 // over 32x8 tiles of every k-slice, FP64 partial sums of r^2 per block.
-template <typename T, bool NORM>
+template <typename T, bool NORM, int NS>
 __global__ void __launch_bounds__(TX *TY) k3_residual(const T *__restrict__ so, const T *__restrict__ q,
                                                       const T *__restrict__ qf, T *__restrict__ res, Dims3 F,
                                                       double *__restrict__ partial)
@@ -66,7 +86,7 @@ __global__ void __launch_bounds__(TX *TY) k3_residual(const T *__restrict__ so, 
 		const int rem = (int)(t - (long)kk * tx * ty);
 		const int i = (rem % tx) * TX + threadIdx.x + 2, j = (rem / tx) * TY + threadIdx.y + 2, k = kk + 2;
 		if (i <= F.nx + 1 && j <= F.ny + 1) {
-			const T r = nb27<T>(so, Load3<T>{q, F}, QF(i, j, k), F, i, j, k) - SO(i, j, k, KP) * Q(i, j, k);
+			const T r = nbs<NS, T>(so, Load3<T>{q, F}, QF(i, j, k), F, i, j, k) - SO(i, j, k, KP) * Q(i, j, k);
 			res[F.at1(i, j, k)] = r;
 			if (NORM) acc += (double)r * (double)r;
 		}
@@ -93,25 +113,28 @@ __global__ void __launch_bounds__(1024) k3_norm_finish(const double *__restrict_
 }
 
 template <typename T>
-int residual_3d(const T *so, const T *x, const T *b, T *r, Dims3 F, double *norm_out, double *partial, cudaStream_t st)
+int residual_3d(const T *so, const T *x, const T *b, T *r, Dims3 F, double *norm_out, double *partial, cudaStream_t st,
+                int ns)
 {
 	const long ntiles = (long)ceil_div(F.nx, TX) * ceil_div(F.ny, TY) * F.nz;
 	const int nb = ntiles < 2048 ? (int)ntiles : 2048;
 	if (norm_out) {
-		k3_residual<T, true><<<nb, dim3(TX, TY), 0, st>>>(so, x, b, r, F, partial);
+		if (ns == 4) k3_residual<T, true, 4><<<nb, dim3(TX, TY), 0, st>>>(so, x, b, r, F, partial);
+		else k3_residual<T, true, 14><<<nb, dim3(TX, TY), 0, st>>>(so, x, b, r, F, partial);
 		CDR_LAUNCH_CHECK();
 		k3_norm_finish<<<1, 1024, 0, st>>>(partial, nb, norm_out);
 	} else {
 		const int nb2 = ntiles < 148 * 64 ? (int)ntiles : 148 * 64;
-		k3_residual<T, false><<<nb2, dim3(TX, TY), 0, st>>>(so, x, b, r, F, nullptr);
+		if (ns == 4) k3_residual<T, false, 4><<<nb2, dim3(TX, TY), 0, st>>>(so, x, b, r, F, nullptr);
+		else k3_residual<T, false, 14><<<nb2, dim3(TX, TY), 0, st>>>(so, x, b, r, F, nullptr);
 	}
 	CDR_LAUNCH_CHECK();
 	return CDR_OK;
 }
 template int residual_3d<double>(const double *, const double *, const double *, double *, Dims3, double *, double *,
-                                 cudaStream_t);
+                                 cudaStream_t, int);
 template int residual_3d<float>(const float *, const float *, const float *, float *, Dims3, double *, double *,
-                                cudaStream_t);
+                                cudaStream_t, int);
 
 // ----------------------------------------------------------------- smoother
 // BMG3_SymStd_SETUP_recip (src/3d/ftn/BMG3_SymStd_SETUP_recip.f90:63-69)
@@ -138,9 +161,31 @@ __global__ void __launch_bounds__(TX *TY) k3_gs_colour(const T *__restrict__ so,
 	Q(i, j, k) = acc * sor[F.at1(i, j, k)];
 }
 
+// One colour of the seven-point branch of BMG3_SymStd_relax_GS
+// (BMG3_SymStd_relax_GS.f90:141-180): colour pts (0 or 1) holds the points
+// with I + J + K + pts even.
 template <typename T>
-int relax_point_3d(const T *so, T *x, const T *b, const T *sor, Dims3 F, int updown, cudaStream_t st)
+__global__ void __launch_bounds__(TX *TY) k3_gs7_colour(const T *__restrict__ so, T *__restrict__ q,
+                                                        const T *__restrict__ qf, const T *__restrict__ sor, Dims3 F,
+                                                        int pts)
 {
+	const int j = 2 + blockIdx.y * TY + threadIdx.y, k = 2 + blockIdx.z;
+	const int i = 2 + ((j + k + pts) & 1) + 2 * (blockIdx.x * TX + threadIdx.x);
+	if (i > F.nx + 1 || j > F.ny + 1) return;
+	Q(i, j, k) = nb7<T>(so, Load3<T>{q, F}, QF(i, j, k), F, i, j, k) * sor[F.at1(i, j, k)];
+}
+
+template <typename T>
+int relax_point_3d(const T *so, T *x, const T *b, const T *sor, Dims3 F, int updown, cudaStream_t st, int ns)
+{
+	if (ns == 4) {  // UP (and the non-symmetric sweep): colour 0 then 1; DOWN: 1 then 0
+		const dim3 blk(TX, TY), grd(ceil_div((F.nx + 1) / 2, TX), ceil_div(F.ny, TY), F.nz);
+		for (int c = 0; c < 2; ++c) {
+			k3_gs7_colour<T><<<grd, blk, 0, st>>>(so, x, b, sor, F, updown == CDR_DOWN ? 1 - c : c);
+			CDR_LAUNCH_CHECK();
+		}
+		return CDR_OK;
+	}
 	const dim3 blk(TX, TY), grd(ceil_div((F.nx + 1) / 2, TX), ceil_div((F.ny + 1) / 2, TY), (F.nz + 1) / 2);
 	for (int c = 0; c < 8; ++c) {
 		const int pts = updown == CDR_UP ? c + 1 : 8 - c;  // UP 1..8, DOWN 8..1
@@ -150,8 +195,9 @@ int relax_point_3d(const T *so, T *x, const T *b, const T *sor, Dims3 F, int upd
 	}
 	return CDR_OK;
 }
-template int relax_point_3d<double>(const double *, double *, const double *, const double *, Dims3, int, cudaStream_t);
-template int relax_point_3d<float>(const float *, float *, const float *, const float *, Dims3, int, cudaStream_t);
+template int relax_point_3d<double>(const double *, double *, const double *, const double *, Dims3, int, cudaStream_t,
+                                    int);
+template int relax_point_3d<float>(const float *, float *, const float *, const float *, Dims3, int, cudaStream_t, int);
 
 template <typename T>
 int setup_recip_3d(const T *so, T *sor, Dims3 F, cudaStream_t st)
@@ -467,12 +513,130 @@ __global__ void __launch_bounds__(TX *TY) k3_oi(const double *__restrict__ so, d
 	}
 }
 
-int setup_interp_3d(const double *so, double *ci, Dims3 F, Dims3 C, cudaStream_t st)
+// The seven-point branch of BMG3_SymStd_SETUP_interp_OI
+// (BMG3_SymStd_SETUP_interp_OI.f90:543-807), same three phases.  Kept from the
+// reference: the x-edge ep divides |b| (not b) by so(kp), and the interior
+// correction is added after the product ((o - dp) * ... + dp).
+__global__ void __launch_bounds__(TX *TY) k3_oi7(const double *__restrict__ so, double *__restrict__ ci, Dims3 F,
+                                                 Dims3 C, int phase)
+{
+	const int ic = blockIdx.x * TX + threadIdx.x + 2, jc = blockIdx.y * TY + threadIdx.y + 2, kc = blockIdx.z + 2;
+	const int iic1 = C.nx + 1, jjc1 = C.ny + 1, kkc1 = C.nz + 1;
+	const int iicf1 = F.nx / 2 + 2, jjcf1 = F.ny / 2 + 2, kkcf1 = F.nz / 2 + 2;
+	const double emach = 1.1102230246251565e-16;
+	const int i = 2 * ic - 2, j = 2 * jc - 2, k = 2 * kc - 2;
+	double a, b, c, ep, dn, dw, de, ds, dp, sum, o;
+	if (phase == 0) {
+		if (kc <= kkc1 && jc <= jjc1 && ic >= 3 && ic <= iicf1) {  // x-edges: lxyl, lxyr
+			a = SO(i - 1, j, k, KPW);
+			b = SO(i, j, k, KPW);
+			ep = dmin2(fabs(a / SO(i - 1, j, k, KP)), fabs(b) / SO(i - 1, j, k, KP));
+			c = a + b + SO(i - 1, j, k, KPS) + SO(i - 1, j + 1, k, KPS) + SO(i - 1, j, k, KB) + SO(i - 1, j, k + 1, KB);
+			c = a + b + (SO(i - 1, j, k, KP) - c) * fmax(SO(i - 1, j, k, KP) - (1.0 + ep) * c, 0.0)
+			            / (fabs(SO(i - 1, j, k, KP) - (1.0 + ep) * c) + emach);
+			CI(ic, jc, kc, LXYL) = a / c;
+			CI(ic, jc, kc, LXYR) = b / c;
+		}
+		if (kc <= kkc1 && jc >= 3 && jc <= jjcf1 && ic <= iic1) {  // y-edges: lxya, lxyb
+			a = SO(i, j, k, KPS);
+			b = SO(i, j - 1, k, KPS);
+			c = a + b + SO(i, j - 1, k, KPW) + SO(i + 1, j - 1, k, KPW) + SO(i, j - 1, k, KB) + SO(i, j - 1, k + 1, KB);
+			ep = dmin2(fabs(a / SO(i, j - 1, k, KP)), fabs(b / SO(i, j - 1, k, KP)));
+			c = a + b + (SO(i, j - 1, k, KP) - c) * fmax(SO(i, j - 1, k, KP) - (1.0 + ep) * c, 0.0)
+			            / (fabs(SO(i, j - 1, k, KP) - (1.0 + ep) * c) + emach);
+			CI(ic, jc, kc, LXYA) = a / c;
+			CI(ic, jc, kc, LXYB) = b / c;
+		}
+		if (kc >= 3 && kc <= kkcf1 && jc <= jjc1 && ic <= iic1) {  // z-edges: lxza, lxzb
+			a = SO(i, j, k, KB);
+			b = SO(i, j, k - 1, KB);
+			c = a + b + SO(i, j, k - 1, KPW) + SO(i + 1, j, k - 1, KPW) + SO(i, j + 1, k - 1, KPS) + SO(i, j, k - 1, KPS);
+			ep = dmin2(fabs(a / SO(i, j, k - 1, KP)), fabs(b / SO(i, j, k - 1, KP)));
+			c = a + b + (SO(i, j, k - 1, KP) - c) * fmax(SO(i, j, k - 1, KP) - (1.0 + ep) * c, 0.0)
+			            / (fabs(SO(i, j, k - 1, KP) - (1.0 + ep) * c) + emach);
+			CI(ic, jc, kc, LXZA) = a / c;
+			CI(ic, jc, kc, LXZB) = b / c;
+		}
+	} else if (phase == 1) {
+		if (ic >= 3 && ic <= iicf1 && jc >= 3 && jc <= jjcf1 && kc <= kkc1) {  // xy faces
+			o = SO(i - 1, j - 1, k, KP);
+			dn = SO(i - 1, j, k, KPS);
+			dw = SO(i - 1, j - 1, k, KPW);
+			de = SO(i, j - 1, k, KPW);
+			ds = SO(i - 1, j - 1, k, KPS);
+			dp = dw + dn + de + ds;
+			sum = o - SO(i - 1, j - 1, k, KB) - SO(i - 1, j - 1, k + 1, KB);
+			ep = dmin2(dmin2(dmin2(fabs(dw / o), fabs(dn / o)), fabs(de / o)), fabs(ds / o));
+			dp = dp + (sum - dp) * fmax(sum - (1.0 + ep) * dp, 0.0) / (fabs(sum - (1.0 + ep) * dp) + emach);
+			dp = 1.0 / dp;
+			CI(ic, jc, kc, LXYNW) = dp * (CI(ic - 1, jc, kc, LXYA) * dw + CI(ic, jc, kc, LXYL) * dn);
+			CI(ic, jc, kc, LXYNE) = dp * (CI(ic, jc, kc, LXYR) * dn + CI(ic, jc, kc, LXYA) * de);
+			CI(ic, jc, kc, LXYSE) = dp * (CI(ic, jc, kc, LXYB) * de + CI(ic, jc - 1, kc, LXYR) * ds);
+			CI(ic, jc, kc, LXYSW) = dp * (CI(ic, jc - 1, kc, LXYL) * ds + CI(ic - 1, jc, kc, LXYB) * dw);
+		}
+		if (kc >= 3 && kc <= kkcf1 && jc <= jjc1 && ic >= 3 && ic <= iicf1) {  // xz faces
+			o = SO(i - 1, j, k - 1, KP);
+			dn = SO(i - 1, j, k, KB);
+			dw = SO(i - 1, j, k - 1, KPW);
+			de = SO(i, j, k - 1, KPW);
+			ds = SO(i - 1, j, k - 1, KB);
+			dp = dw + dn + de + ds;
+			sum = o - SO(i - 1, j + 1, k - 1, KPS) - SO(i - 1, j, k - 1, KPS);
+			ep = dmin2(dmin2(dmin2(fabs(dw / o), fabs(dn / o)), fabs(de / o)), fabs(ds / o));
+			dp = dp + (sum - dp) * fmax(sum - (1.0 + ep) * dp, 0.0) / (fabs(sum - (1.0 + ep) * dp) + emach);
+			dp = 1.0 / dp;
+			CI(ic, jc, kc, LXZNW) = dp * (CI(ic - 1, jc, kc, LXZA) * dw + CI(ic, jc, kc, LXYL) * dn);
+			CI(ic, jc, kc, LXZNE) = dp * (CI(ic, jc, kc, LXYR) * dn + CI(ic, jc, kc, LXZA) * de);
+			CI(ic, jc, kc, LXZSE) = dp * (CI(ic, jc, kc, LXZB) * de + CI(ic, jc, kc - 1, LXYR) * ds);
+			CI(ic, jc, kc, LXZSW) = dp * (CI(ic, jc, kc - 1, LXYL) * ds + CI(ic - 1, jc, kc, LXZB) * dw);
+		}
+		if (kc >= 3 && kc <= kkcf1 && jc >= 3 && jc <= jjcf1 && ic <= iic1) {  // yz faces
+			o = SO(i, j - 1, k - 1, KP);
+			dn = SO(i, j - 1, k, KB);
+			dw = SO(i, j, k - 1, KPS);
+			de = SO(i, j - 1, k - 1, KPS);
+			ds = SO(i, j - 1, k - 1, KB);
+			dp = dw + dn + de + ds;
+			sum = o - SO(i, j - 1, k - 1, KPW) - SO(i + 1, j - 1, k - 1, KPW);
+			ep = dmin2(dmin2(dmin2(fabs(dw / o), fabs(dn / o)), fabs(de / o)), fabs(ds / o));
+			dp = dp + (sum - dp) * fmax(sum - (1.0 + ep) * dp, 0.0) / (fabs(sum - (1.0 + ep) * dp) + emach);
+			dp = 1.0 / dp;
+			CI(ic, jc, kc, LYZNW) = dp * (CI(ic, jc, kc, LXZA) * dw + CI(ic, jc, kc, LXYA) * dn);
+			CI(ic, jc, kc, LYZNE) = dp * (CI(ic, jc, kc, LXYB) * dn + CI(ic, jc - 1, kc, LXZA) * de);
+			CI(ic, jc, kc, LYZSE) = dp * (CI(ic, jc - 1, kc, LXZB) * de + CI(ic, jc, kc - 1, LXYB) * ds);
+			CI(ic, jc, kc, LYZSW) = dp * (CI(ic, jc, kc - 1, LXYA) * ds + CI(ic, jc, kc, LXZB) * dw);
+		}
+	} else if (kc >= 3 && kc <= kkcf1 && jc >= 3 && jc <= jjcf1 && ic >= 3 && ic <= iicf1) {  // interior points
+		o = SO(i - 1, j - 1, k - 1, KP);
+		const double sw = SO(i - 1, j - 1, k - 1, KPW), sn = SO(i - 1, j, k - 1, KPS), se = SO(i, j - 1, k - 1, KPW);
+		const double ss = SO(i - 1, j - 1, k - 1, KPS), sb = SO(i - 1, j - 1, k - 1, KB), st = SO(i - 1, j - 1, k, KB);
+		dp = sw + sn + se + ss + sb + st;
+		ep = dmin2(dmin2(dmin2(dmin2(dmin2(fabs(sw / o), fabs(sn / o)), fabs(se / o)), fabs(ss / o)), fabs(sb / o)),
+		           fabs(st / o));
+		dp = (o - dp) * fmax(o - (1.0 + ep) * dp, 0.0) / (fabs(o - (1.0 + ep) * dp) + emach) + dp;
+		dp = 1.0 / dp;
+		CI(ic, jc, kc, LTNW) = dp * (CI(ic - 1, jc, kc, LYZNW) * sw + CI(ic, jc, kc, LXZNW) * sn + CI(ic, jc, kc, LXYNW) * st);
+		CI(ic, jc, kc, LTNE) = dp * (CI(ic, jc, kc, LXZNE) * sn + CI(ic, jc, kc, LYZNW) * se + CI(ic, jc, kc, LXYNE) * st);
+		CI(ic, jc, kc, LBNW) =
+		    dp * (CI(ic, jc, kc - 1, LXYNW) * sb + CI(ic - 1, jc, kc, LYZSW) * sw + CI(ic, jc, kc, LXZSW) * sn);
+		CI(ic, jc, kc, LBNE) = dp * (CI(ic, jc, kc - 1, LXYNE) * sb + CI(ic, jc, kc, LXZSE) * sn + CI(ic, jc, kc, LYZSW) * se);
+		CI(ic, jc, kc, LBSW) =
+		    dp * (CI(ic, jc, kc - 1, LXYSW) * sb + CI(ic - 1, jc, kc, LYZSE) * sw + CI(ic, jc - 1, kc, LXZSW) * ss);
+		CI(ic, jc, kc, LTSW) =
+		    dp * (CI(ic, jc, kc, LXYSW) * st + CI(ic - 1, jc, kc, LYZNE) * sw + CI(ic, jc - 1, kc, LXZNW) * ss);
+		CI(ic, jc, kc, LTSE) = dp * (CI(ic, jc, kc, LXYSE) * st + CI(ic, jc - 1, kc, LXZNE) * ss + CI(ic, jc, kc, LYZNE) * se);
+		CI(ic, jc, kc, LBSE) =
+		    dp * (CI(ic, jc, kc - 1, LXYSE) * sb + CI(ic, jc - 1, kc, LXZSE) * ss + CI(ic, jc, kc, LYZSE) * se);
+	}
+}
+
+int setup_interp_3d(const double *so, double *ci, Dims3 F, Dims3 C, cudaStream_t st, int ns)
 {
 	CDR_CUDA_TRY(cudaMemsetAsync(ci, 0, sizeof(double) * C.plane() * 26, st));
 	const dim3 grd(ceil_div(F.nx / 2 + 1, TX), ceil_div(F.ny / 2 + 1, TY), F.nz / 2 + 1);
 	for (int ph = 0; ph < 3; ++ph) {
-		k3_oi<<<grd, dim3(TX, TY), 0, st>>>(so, ci, F, C, ph);
+		if (ns == 4) k3_oi7<<<grd, dim3(TX, TY), 0, st>>>(so, ci, F, C, ph);
+		else k3_oi<<<grd, dim3(TX, TY), 0, st>>>(so, ci, F, C, ph);
 		CDR_LAUNCH_CHECK();
 	}
 	return CDR_OK;
@@ -481,37 +645,41 @@ int setup_interp_3d(const double *so, double *ci, Dims3 F, Dims3 C, cudaStream_t
 // ------------------------------------------------------------- Galerkin (P^T A P)
 // Same loops, order and skips as the CPU restatement of the product that
 // BMG3_SymStd_SETUP_ITLI27_ex expands (cdr3 oracle).
+// A seven-point operator (NS == 4) has no planes beyond kb: those couplings
+// read as 0, as the zero-filled planes of a 14-plane copy would.
+template <int NS>
 __device__ __forceinline__ double a3(const double *__restrict__ so, Dims3 F, int i, int j, int k, int di, int dj, int dk)
 {
+	auto S = [&](int ii, int jj, int kk, int p) -> double { return (NS == 4 && p > KB) ? 0.0 : SO(ii, jj, kk, p); };
 	if (di == 0 && dj == 0 && dk == 0) return SO(i, j, k, KP);
 	double c = 0.0;
 	switch ((dk + 1) * 9 + (dj + 1) * 3 + (di + 1)) {
-	case 9 + 3 + 0: c = SO(i, j, k, KPW); break;
-	case 9 + 6 + 0: c = SO(i, j + 1, k, KPNW); break;
-	case 9 + 6 + 1: c = SO(i, j + 1, k, KPS); break;
-	case 9 + 6 + 2: c = SO(i + 1, j + 1, k, KPSW); break;
-	case 9 + 3 + 2: c = SO(i + 1, j, k, KPW); break;
-	case 9 + 0 + 2: c = SO(i + 1, j, k, KPNW); break;
-	case 9 + 0 + 1: c = SO(i, j, k, KPS); break;
-	case 9 + 0 + 0: c = SO(i, j, k, KPSW); break;
-	case 0 + 3 + 1: c = SO(i, j, k, KB); break;
-	case 0 + 3 + 0: c = SO(i, j, k, KBW); break;
-	case 0 + 6 + 0: c = SO(i, j + 1, k, KBNW); break;
-	case 0 + 6 + 1: c = SO(i, j + 1, k, KBN); break;
-	case 0 + 6 + 2: c = SO(i + 1, j + 1, k, KBNE); break;
-	case 0 + 3 + 2: c = SO(i + 1, j, k, KBE); break;
-	case 0 + 0 + 2: c = SO(i + 1, j, k, KBSE); break;
-	case 0 + 0 + 1: c = SO(i, j, k, KBS); break;
-	case 0 + 0 + 0: c = SO(i, j, k, KBSW); break;
-	case 18 + 3 + 1: c = SO(i, j, k + 1, KB); break;
-	case 18 + 3 + 0: c = SO(i, j, k + 1, KBE); break;
-	case 18 + 6 + 0: c = SO(i, j + 1, k + 1, KBSE); break;
-	case 18 + 6 + 1: c = SO(i, j + 1, k + 1, KBS); break;
-	case 18 + 6 + 2: c = SO(i + 1, j + 1, k + 1, KBSW); break;
-	case 18 + 3 + 2: c = SO(i + 1, j, k + 1, KBW); break;
-	case 18 + 0 + 2: c = SO(i + 1, j, k + 1, KBNW); break;
-	case 18 + 0 + 1: c = SO(i, j, k + 1, KBN); break;
-	case 18 + 0 + 0: c = SO(i, j, k + 1, KBNE); break;
+	case 9 + 3 + 0: c = S(i, j, k, KPW); break;
+	case 9 + 6 + 0: c = S(i, j + 1, k, KPNW); break;
+	case 9 + 6 + 1: c = S(i, j + 1, k, KPS); break;
+	case 9 + 6 + 2: c = S(i + 1, j + 1, k, KPSW); break;
+	case 9 + 3 + 2: c = S(i + 1, j, k, KPW); break;
+	case 9 + 0 + 2: c = S(i + 1, j, k, KPNW); break;
+	case 9 + 0 + 1: c = S(i, j, k, KPS); break;
+	case 9 + 0 + 0: c = S(i, j, k, KPSW); break;
+	case 0 + 3 + 1: c = S(i, j, k, KB); break;
+	case 0 + 3 + 0: c = S(i, j, k, KBW); break;
+	case 0 + 6 + 0: c = S(i, j + 1, k, KBNW); break;
+	case 0 + 6 + 1: c = S(i, j + 1, k, KBN); break;
+	case 0 + 6 + 2: c = S(i + 1, j + 1, k, KBNE); break;
+	case 0 + 3 + 2: c = S(i + 1, j, k, KBE); break;
+	case 0 + 0 + 2: c = S(i + 1, j, k, KBSE); break;
+	case 0 + 0 + 1: c = S(i, j, k, KBS); break;
+	case 0 + 0 + 0: c = S(i, j, k, KBSW); break;
+	case 18 + 3 + 1: c = S(i, j, k + 1, KB); break;
+	case 18 + 3 + 0: c = S(i, j, k + 1, KBE); break;
+	case 18 + 6 + 0: c = S(i, j + 1, k + 1, KBSE); break;
+	case 18 + 6 + 1: c = S(i, j + 1, k + 1, KBS); break;
+	case 18 + 6 + 2: c = S(i + 1, j + 1, k + 1, KBSW); break;
+	case 18 + 3 + 2: c = S(i + 1, j, k + 1, KBW); break;
+	case 18 + 0 + 2: c = S(i + 1, j, k + 1, KBNW); break;
+	case 18 + 0 + 1: c = S(i, j, k + 1, KBN); break;
+	case 18 + 0 + 0: c = S(i, j, k + 1, KBNE); break;
 	}
 	return -c;
 }
@@ -542,6 +710,7 @@ __device__ __forceinline__ double p3(const double *__restrict__ ci, Dims3 C, int
 	return CI(ic + io, jc + jo, kc + ko, l);
 }
 
+template <int NS>
 __device__ double rap3(const double *__restrict__ so, const double *__restrict__ ci, Dims3 F, Dims3 C, int i1, int j1,
                        int k1, int i2, int j2, int k2)
 {
@@ -560,7 +729,7 @@ __device__ double rap3(const double *__restrict__ so, const double *__restrict__
 						for (int ddx = -1; ddx <= 1; ++ddx) {
 							const int ex = dx1 + ddx - 2 * (i2 - i1), ey = dy1 + ddy - 2 * (j2 - j1), ez = dz1 + ddz - 2 * (k2 - k1);
 							if (ex < -1 || ex > 1 || ey < -1 || ey > 1 || ez < -1 || ez > 1) continue;
-							inner += a3(so, F, fx, fy, fz, ddx, ddy, ddz) * p3(ci, C, i2, j2, k2, ex, ey, ez);
+							inner += a3<NS>(so, F, fx, fy, fz, ddx, ddy, ddz) * p3(ci, C, i2, j2, k2, ex, ey, ez);
 						}
 				tot += p3(ci, C, i1, j1, k1, dx1, dy1, dz1) * inner;
 			}
@@ -568,6 +737,7 @@ __device__ double rap3(const double *__restrict__ so, const double *__restrict__
 }
 
 // One thread per (coarse point, stencil plane): the 14 entries are independent.
+template <int NS>
 __global__ void __launch_bounds__(TX *TY) k3_galerkin(const double *__restrict__ so, const double *__restrict__ ci,
                                                       double *__restrict__ soc, Dims3 F, Dims3 C)
 {
@@ -593,14 +763,16 @@ __global__ void __launch_bounds__(TX *TY) k3_galerkin(const double *__restrict__
 	case KBS: b2 = -1; c2 = -1; break;
 	case KBSW: a2 = -1; b2 = -1; c2 = -1; break;
 	}
-	const double v = rap3(so, ci, F, C, ic + a1, jc + b1, kc + c1, ic + a2, jc + b2, kc + c2);
+	const double v = rap3<NS>(so, ci, F, C, ic + a1, jc + b1, kc + c1, ic + a2, jc + b2, kc + c2);
 	soc[(size_t)(pl - 1) * C.plane() + C.at1(ic, jc, kc)] = pl == KP ? v : -v;
 }
 
-int galerkin_3d(const double *so, const double *ci, double *soc, Dims3 F, Dims3 C, cudaStream_t st)
+int galerkin_3d(const double *so, const double *ci, double *soc, Dims3 F, Dims3 C, cudaStream_t st, int ns)
 {
 	CDR_CUDA_TRY(cudaMemsetAsync(soc, 0, sizeof(double) * C.plane() * 14, st));
-	k3_galerkin<<<dim3(ceil_div(C.nx, TX), ceil_div(C.ny, TY), C.nz * 14), dim3(TX, TY), 0, st>>>(so, ci, soc, F, C);
+	const dim3 grd(ceil_div(C.nx, TX), ceil_div(C.ny, TY), C.nz * 14);
+	if (ns == 4) k3_galerkin<4><<<grd, dim3(TX, TY), 0, st>>>(so, ci, soc, F, C);
+	else k3_galerkin<14><<<grd, dim3(TX, TY), 0, st>>>(so, ci, soc, F, C);
 	CDR_LAUNCH_CHECK();
 	return CDR_OK;
 }
@@ -608,8 +780,12 @@ int galerkin_3d(const double *so, const double *ci, double *soc, Dims3 F, Dims3 
 // ---------------------------------------------------------- coarsest Cholesky
 // ABD fill of BMG3_SymStd_SETUP_cg_LU (src/3d/ftn/BMG3_SymStd_SETUP_cg_LU.f90:106-130),
 // KD = IBW = (II-2)*(JJ-1)+1, then DPBTF2('U') as in 2D.
+// NS == 4: a seven-point operator (a one-level hierarchy); the couplings it
+// lacks enter the band as -0.0, as from zero-filled planes.
+template <int NS>
 __global__ void k3_cg_factor(const double *__restrict__ so, Dims3 F, double *__restrict__ abd, int nabd1, int *info)
 {
+	auto S = [&](int ii, int jj, int kk, int p) -> double { return (NS == 4 && p > KB) ? 0.0 : SO(ii, jj, kk, p); };
 	if (threadIdx.x != 0 || blockIdx.x != 0) return;
 	const int II = F.nx + 2, JJ = F.ny + 2, KK = F.nz + 2;
 	const int i1 = II - 1, j1 = JJ - 1, k1 = KK - 1, i2 = i1 - 1;
@@ -622,20 +798,20 @@ __global__ void k3_cg_factor(const double *__restrict__ so, Dims3 F, double *__r
 		for (int j = 2; j <= j1; ++j)
 			for (int i = 2; i <= i1; ++i) {
 				kl++;
-				ABD(ibw + 1, kl) = SO(i, j, k, KP);
-				ABD(ibw, kl) = -SO(i, j, k, KPW);
-				ABD(ibw - i1 + 3, kl) = -SO(i + 1, j, k, KPNW);
-				ABD(ibw - i1 + 2, kl) = -SO(i, j, k, KPS);
-				ABD(ibw - i1 + 1, kl) = -SO(i, j, k, KPSW);
-				ABD(ibw - (j1 - 2) * i2 + 2, kl) = -SO(i + 1, j + 1, k, KBNE);
-				ABD(ibw - (j1 - 2) * i2 + 1, kl) = -SO(i, j + 1, k, KBN);
-				ABD(ibw - (j1 - 2) * i2, kl) = -SO(i, j + 1, k, KBNW);
-				ABD(ibw - (j1 - 1) * i2 + 2, kl) = -SO(i + 1, j, k, KBE);
-				ABD(ibw - (j1 - 1) * i2 + 1, kl) = -SO(i, j, k, KB);
-				ABD(ibw - (j1 - 1) * i2, kl) = -SO(i, j, k, KBW);
-				ABD(3, kl) = -SO(i + 1, j, k, KBSE);
-				ABD(2, kl) = -SO(i, j, k, KBS);
-				ABD(1, kl) = -SO(i, j, k, KBSW);
+				ABD(ibw + 1, kl) = S(i, j, k, KP);
+				ABD(ibw, kl) = -S(i, j, k, KPW);
+				ABD(ibw - i1 + 3, kl) = -S(i + 1, j, k, KPNW);
+				ABD(ibw - i1 + 2, kl) = -S(i, j, k, KPS);
+				ABD(ibw - i1 + 1, kl) = -S(i, j, k, KPSW);
+				ABD(ibw - (j1 - 2) * i2 + 2, kl) = -S(i + 1, j + 1, k, KBNE);
+				ABD(ibw - (j1 - 2) * i2 + 1, kl) = -S(i, j + 1, k, KBN);
+				ABD(ibw - (j1 - 2) * i2, kl) = -S(i, j + 1, k, KBNW);
+				ABD(ibw - (j1 - 1) * i2 + 2, kl) = -S(i + 1, j, k, KBE);
+				ABD(ibw - (j1 - 1) * i2 + 1, kl) = -S(i, j, k, KB);
+				ABD(ibw - (j1 - 1) * i2, kl) = -S(i, j, k, KBW);
+				ABD(3, kl) = -S(i + 1, j, k, KBSE);
+				ABD(2, kl) = -S(i, j, k, KBS);
+				ABD(1, kl) = -S(i, j, k, KBSW);
 			}
 #undef ABD
 	// DPBTF2('U', n, kd = ibw)
@@ -696,9 +872,10 @@ __global__ void k3_cg_solve(const double *__restrict__ ab, int ldab, T *__restri
 			for (int i = 2; i <= F.nx + 1; ++i) Q(i, j, k) = (T)xs[kk++];
 }
 
-int setup_cg_3d(const double *so, Dims3 F, double *abd, int *info, cudaStream_t st)
+int setup_cg_3d(const double *so, Dims3 F, double *abd, int *info, cudaStream_t st, int ns)
 {
-	k3_cg_factor<<<1, 32, 0, st>>>(so, F, abd, F.nx * (F.ny + 1) + 2, info);
+	if (ns == 4) k3_cg_factor<4><<<1, 32, 0, st>>>(so, F, abd, F.nx * (F.ny + 1) + 2, info);
+	else k3_cg_factor<14><<<1, 32, 0, st>>>(so, F, abd, F.nx * (F.ny + 1) + 2, info);
 	CDR_LAUNCH_CHECK();
 	return CDR_OK;
 }
@@ -734,6 +911,7 @@ struct LoadIR3 {
 	}
 };
 
+template <int NS>
 __global__ void __launch_bounds__(TX *TY) k3_ir_residual(const double *__restrict__ so, const double *__restrict__ x,
                                                          const float *__restrict__ e, const double *__restrict__ b,
                                                          double *__restrict__ xo, float *__restrict__ r32, Dims3 F,
@@ -750,7 +928,7 @@ __global__ void __launch_bounds__(TX *TY) k3_ir_residual(const double *__restric
 		const int i = (rem % tx) * TX + threadIdx.x + 2, j = (rem / tx) * TY + threadIdx.y + 2, k = kk + 2;
 		if (i <= F.nx + 1 && j <= F.ny + 1) {
 			const double xc = xq(i, j, k);
-			const double r = nb27<double>(so, xq, b[F.at1(i, j, k)], F, i, j, k) - SO(i, j, k, KP) * xc;
+			const double r = nbs<NS, double>(so, xq, b[F.at1(i, j, k)], F, i, j, k) - SO(i, j, k, KP) * xc;
 			acc += r * r;
 			r32[E.at1(i, j, k)] = (float)r;
 			xo[F.at1(i, j, k)] = xc;
@@ -761,11 +939,12 @@ __global__ void __launch_bounds__(TX *TY) k3_ir_residual(const double *__restric
 }
 
 int ir_residual_3d(const double *so, const double *x, const float *e, const double *b, double *xo, float *r32,
-                   Dims3 d, Dims3 d32, double *norm_out, double *partial, int apply, cudaStream_t st)
+                   Dims3 d, Dims3 d32, double *norm_out, double *partial, int apply, cudaStream_t st, int ns)
 {
 	const long ntiles = (long)ceil_div(d.nx, TX) * ceil_div(d.ny, TY) * d.nz;
 	const int nb = ntiles < 2048 ? (int)ntiles : 2048;
-	k3_ir_residual<<<nb, dim3(TX, TY), 0, st>>>(so, x, e, b, xo, r32, d, d32, partial, apply);
+	if (ns == 4) k3_ir_residual<4><<<nb, dim3(TX, TY), 0, st>>>(so, x, e, b, xo, r32, d, d32, partial, apply);
+	else k3_ir_residual<14><<<nb, dim3(TX, TY), 0, st>>>(so, x, e, b, xo, r32, d, d32, partial, apply);
 	CDR_LAUNCH_CHECK();
 	k3_norm_finish<<<1, 1024, 0, st>>>(partial, nb, norm_out);
 	CDR_LAUNCH_CHECK();

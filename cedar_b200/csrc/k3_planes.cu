@@ -30,6 +30,9 @@ __device__ __forceinline__ size_t plane_at(const Dims3 &F, int dir, int ipl, int
 // 2D planes c, w, s, sw, nw from the 3D planes
 //   xy: p, pw, ps, psw, pnw;  xz: p, pw, b, bw, be;  yz: p, ps, b, bs, bn.
 // xz copies the interior k rows only (so3.range(2)), the others the ghost rows too.
+// copy_coeff for seven_pt -> five_pt (include/cedar/3d/relax_planes.h:77-107)
+// takes the first three of each list (c, w, s), with the same row ranges.
+template <int NS2>
 __global__ void k3_plane_coeff(const double *__restrict__ so, Dims3 F, int dir, double *__restrict__ so2, int n1,
                                int n2, int pitch2)
 {
@@ -37,11 +40,11 @@ __global__ void k3_plane_coeff(const double *__restrict__ so, Dims3 F, int dir, 
 	if (a > n1 + 1 || b > n2 + 1) return;
 	if (dir == 1 && (b < 1 || b > n2)) return;
 	const size_t plane2 = (size_t)pitch2 * (n2 + 2);
-	so2 += (size_t)(ipl - 1) * 5 * plane2 + (size_t)b * pitch2 + a;
+	so2 += (size_t)(ipl - 1) * NS2 * plane2 + (size_t)b * pitch2 + a;
 	const size_t g = plane_at(F, dir, ipl, a, b), P = F.plane();
 	const int src[3][5] = {{KP, KPW, KPS, KPSW, KPNW}, {KP, KPW, KB, KBW, KBE}, {KP, KPS, KB, KBS, KBN}};
 #pragma unroll
-	for (int q = 0; q < 5; ++q) so2[q * plane2] = so[(size_t)(src[dir][q] - 1) * P + g];
+	for (int q = 0; q < NS2; ++q) so2[q * plane2] = so[(size_t)(src[dir][q] - 1) * P + g];
 }
 
 // copy32 (TO_PLANE) / copy23 (src/3d/relax_planes.cc:185-238): the whole plane,
@@ -75,7 +78,9 @@ template int plane_copy<float>(float *, Dims3, int, int, int, int, float *, int,
 // copy_rhs for xxvii_pt (src/3d/relax_planes.cc:43-72 xy, :95-127 xz, :146-178 yz):
 // b2 = b + the couplings to the two neighbouring planes, on the plane interior,
 // in the reference's operand order.
-template <typename T>
+// NS == 4 (seven_pt, src/3d/relax_planes.cc:25-38 xy, :76-90 xz, :126-140 yz):
+// one coupling to each neighbouring plane.
+template <typename T, int NS>
 __global__ void __launch_bounds__(TX *TY) k3_plane_rhs(const T *__restrict__ so, const T *__restrict__ x,
                                                        const T *__restrict__ bb, Dims3 F, int dir, int first, int step,
                                                        T *__restrict__ b2, int n1, int n2, int pitch2)
@@ -87,7 +92,18 @@ __global__ void __launch_bounds__(TX *TY) k3_plane_rhs(const T *__restrict__ so,
 #define X3(a, i, j, k) a[o3(F, i, j, k)]
 #define S3(pl, i, j, k) so[(size_t)((pl)-1) * P + o3(F, i, j, k)]
 	T v;
-	if (dir == 0) {
+	if (NS == 4) {
+		if (dir == 0) {
+			const int i = p, j = q, k = ipl;
+			v = X3(bb, i, j, k) + S3(KB, i, j, k) * X3(x, i, j, k - 1) + S3(KB, i, j, k + 1) * X3(x, i, j, k + 1);
+		} else if (dir == 1) {
+			const int i = p, k = q, j = ipl;
+			v = X3(bb, i, j, k) + S3(KPS, i, j, k) * X3(x, i, j - 1, k) + S3(KPS, i, j + 1, k) * X3(x, i, j + 1, k);
+		} else {
+			const int j = p, k = q, i = ipl;
+			v = X3(bb, i, j, k) + S3(KPW, i, j, k) * X3(x, i - 1, j, k) + S3(KPW, i + 1, j, k) * X3(x, i + 1, j, k);
+		}
+	} else if (dir == 0) {
 		const int i = p, j = q, k = ipl;
 		v = X3(bb, i, j, k) + S3(KB, i, j, k) * X3(x, i, j, k - 1) + S3(KBW, i, j, k) * X3(x, i - 1, j, k - 1)
 		    + S3(KBNW, i, j + 1, k) * X3(x, i - 1, j + 1, k - 1) + S3(KBN, i, j + 1, k) * X3(x, i, j + 1, k - 1)
@@ -128,23 +144,27 @@ __global__ void __launch_bounds__(TX *TY) k3_plane_rhs(const T *__restrict__ so,
 
 template <typename T>
 int plane_rhs(const T *so, const T *x, const T *b, Dims3 F, int dir, int first, int step, int count, T *b2, int n1,
-              int n2, int pitch2, cudaStream_t st)
+              int n2, int pitch2, cudaStream_t st, int ns)
 {
-	k3_plane_rhs<T><<<dim3(ceil_div(n1, TX), ceil_div(n2, TY), count), dim3(TX, TY), 0, st>>>(so, x, b, F, dir, first,
-	                                                                                          step, b2, n1, n2, pitch2);
+	const dim3 grd(ceil_div(n1, TX), ceil_div(n2, TY), count);
+	if (ns == 4) k3_plane_rhs<T, 4><<<grd, dim3(TX, TY), 0, st>>>(so, x, b, F, dir, first, step, b2, n1, n2, pitch2);
+	else k3_plane_rhs<T, 14><<<grd, dim3(TX, TY), 0, st>>>(so, x, b, F, dir, first, step, b2, n1, n2, pitch2);
 	CDR_LAUNCH_CHECK();
 	return CDR_OK;
 }
 template int plane_rhs<double>(const double *, const double *, const double *, Dims3, int, int, int, int, double *,
-                               int, int, int, cudaStream_t);
+                               int, int, int, cudaStream_t, int);
 template int plane_rhs<float>(const float *, const float *, const float *, Dims3, int, int, int, int, float *, int,
-                              int, int, cudaStream_t);
+                              int, int, cudaStream_t, int);
 
-int plane_coeff(const double *so, Dims3 F, int dir, double *so2, int n, int n1, int n2, int pitch2, cudaStream_t st)
+int plane_coeff(const double *so, Dims3 F, int dir, double *so2, int n, int n1, int n2, int pitch2, cudaStream_t st,
+                int ns)
 {
-	CDR_CUDA_TRY(cudaMemsetAsync(so2, 0, sizeof(double) * 5 * (size_t)pitch2 * (n2 + 2) * n, st));
-	k3_plane_coeff<<<dim3(ceil_div(n1 + 2, TX), ceil_div(n2 + 2, TY), n), dim3(TX, TY), 0, st>>>(so, F, dir, so2, n1,
-	                                                                                            n2, pitch2);
+	const int ns2 = ns == 4 ? 3 : 5;
+	CDR_CUDA_TRY(cudaMemsetAsync(so2, 0, sizeof(double) * ns2 * (size_t)pitch2 * (n2 + 2) * n, st));
+	const dim3 grd(ceil_div(n1 + 2, TX), ceil_div(n2 + 2, TY), n);
+	if (ns == 4) k3_plane_coeff<3><<<grd, dim3(TX, TY), 0, st>>>(so, F, dir, so2, n1, n2, pitch2);
+	else k3_plane_coeff<5><<<grd, dim3(TX, TY), 0, st>>>(so, F, dir, so2, n1, n2, pitch2);
 	CDR_LAUNCH_CHECK();
 	return CDR_OK;
 }

@@ -1,5 +1,6 @@
-// solver3d.cu -- 3D BoxMG multilevel solver on the device (27-point operators;
-// 8-colour point Gauss-Seidel or plane relaxation).
+// solver3d.cu -- 3D BoxMG multilevel solver on the device (27-point or
+// seven-point fine operator, 27-point coarse operators; point Gauss-Seidel or
+// plane relaxation).
 //
 // Host control mirrors cdr3::solver over Cedar's multilevel driver: setup builds
 // interpolation, Galerkin operator and smoother level by level and factors the
@@ -32,6 +33,7 @@ inline int round_up3(int v, int m) { return (v + m - 1) / m * m; }
 
 struct Level3 {
 	int nx = 0, ny = 0, nz = 0;
+	int ns = 14;  // stencil planes: 14, or 4 for a seven-point fine operator
 	Dims3 d{};
 	std::unique_ptr<Batch2> pl[3];  // plane problems: xy, xz, yz
 	double *so = nullptr, *x = nullptr, *b = nullptr, *r = nullptr, *sor = nullptr, *ci = nullptr;
@@ -113,7 +115,7 @@ struct cdr_gpu_solver3 {
 			const Sel sel{beg - 1, 2, (n - beg) / 2 + 1};
 			CDR_TRY(plane_copy<T>(x, F.d, dir, sel.first, 2, sel.count, x2, P0.nx, P0.ny, P0.pitch, true, st));
 			CDR_TRY(plane_rhs<T>(Arr3<T>::so(F), x, b, F.d, dir, sel.first, 2, sel.count, b2, P0.nx, P0.ny, P0.pitch,
-			                     st));
+			                     st, F.ns));
 			CDR_TRY(P.cycle<T>(sel));
 			CDR_TRY(plane_copy<T>(x, F.d, dir, sel.first, 2, sel.count, x2, P0.nx, P0.ny, P0.pitch, false, st));
 		}
@@ -130,7 +132,7 @@ struct cdr_gpu_solver3 {
 		static const int down[3] = {0, 2, 1}, up[3] = {1, 2, 0};
 		for (int it = 0; it < n; ++it) {
 			if (s.relaxation == CDR_RELAX_POINT) {
-				CDR_TRY(relax_point_3d<T>(Arr3<T>::so(F), x, b, Arr3<T>::sor(F), F.d, updown, st));
+				CDR_TRY(relax_point_3d<T>(Arr3<T>::so(F), x, b, Arr3<T>::sor(F), F.d, updown, st, F.ns));
 				continue;
 			}
 			for (int q = 0; q < 3; ++q) {
@@ -147,7 +149,7 @@ struct cdr_gpu_solver3 {
 	{
 		Level3 &F = lv[l], &C = lv[l + 1];
 		CDR_TRY(smooth<T>(l, x, b, CDR_DOWN));
-		CDR_TRY(residual_3d<T>(Arr3<T>::so(F), x, b, Arr3<T>::r(F), F.d, nullptr, nullptr, st));
+		CDR_TRY(residual_3d<T>(Arr3<T>::so(F), x, b, Arr3<T>::r(F), F.d, nullptr, nullptr, st, F.ns));
 		CDR_TRY(restrict_3d<T>(Arr3<T>::ci(C), Arr3<T>::r(F), Arr3<T>::b(C), F.d, C.d, st));
 		CDR_CUDA_TRY(cudaMemsetAsync(Arr3<T>::x(C), 0, sizeof(T) * C.d.plane(), st));
 		if (l + 1 == L() - 1) CDR_TRY(solve_cg_3d<T>(abd, Arr3<T>::x(C), Arr3<T>::b(C), C.d, st));
@@ -200,15 +202,15 @@ struct cdr_gpu_solver3 {
 	{
 		for (int l = 0; l + 1 < L(); ++l) {
 			Level3 &F = lv[l], &C = lv[l + 1];
-			CDR_TRY(setup_interp_3d(F.so, C.ci, F.d, C.d, st));
-			CDR_TRY(galerkin_3d(F.so, C.ci, C.so, F.d, C.d, st));
+			CDR_TRY(setup_interp_3d(F.so, C.ci, F.d, C.d, st, F.ns));
+			CDR_TRY(galerkin_3d(F.so, C.ci, C.so, F.d, C.d, st, F.ns));
 			CDR_TRY(setup_recip_3d<double>(F.so, F.sor, F.d, st));
 			// plane smoothers: 2D operators from the in-plane couplings, then the 2D setups
 			for (int dir = 0; dir < 3; ++dir) {
 				if (!F.pl[dir]) continue;
 				Batch2 &P = *F.pl[dir];
 				B2Level &P0 = P.lv[0];
-				CDR_TRY(plane_coeff(F.so, F.d, dir, P0.so, P.nb, P0.nx, P0.ny, P0.pitch, st));
+				CDR_TRY(plane_coeff(F.so, F.d, dir, P0.so, P.nb, P0.nx, P0.ny, P0.pitch, st, F.ns));
 				CDR_TRY(P.setup(false));
 			}
 		}
@@ -216,11 +218,11 @@ struct cdr_gpu_solver3 {
 			for (int dir = 0; dir < 3; ++dir)
 				if (lv[l].pl[dir]) CDR_TRY(lv[l].pl[dir]->check_info());
 		Level3 &Cg = lv[L() - 1];
-		CDR_TRY(setup_cg_3d(Cg.so, Cg.d, abd, info, st));
+		CDR_TRY(setup_cg_3d(Cg.so, Cg.d, abd, info, st, Cg.ns));
 		if (mixed()) {
 			for (int l = 0; l < L(); ++l) {
 				Level3 &F = lv[l];
-				CDR_TRY(convert_f64_f32(F.so, F.so32, F.d.plane() * 14, st));
+				CDR_TRY(convert_f64_f32(F.so, F.so32, F.d.plane() * F.ns, st));
 				if (l > 0) CDR_TRY(convert_f64_f32(F.ci, F.ci32, F.d.plane() * 26, st));
 				if (l + 1 < L()) CDR_TRY(convert_f64_f32(F.sor, F.sor32, F.d.plane(), st));
 			}
@@ -250,7 +252,8 @@ static int num_levels3(int nx, int ny, int nz, int min_coarse)
 	return ng;
 }
 
-static int create3(cdr_gpu_solver3 *h, const double *so_src, int src_pitch, cudaMemcpyKind kind, int nx, int ny, int nz)
+static int create3(cdr_gpu_solver3 *h, const double *so_src, int src_pitch, cudaMemcpyKind kind, int ns, int nx, int ny,
+                   int nz)
 {
 	const cdr_gpu_settings &s = h->s;
 	int nl = num_levels3(nx, ny, nz, s.min_coarse);
@@ -272,15 +275,17 @@ static int create3(cdr_gpu_solver3 *h, const double *so_src, int src_pitch, cuda
 			L.nz = (int)((P.nz - 1) / 2. + 1);
 		}
 		L.d = Dims3{L.nx, L.ny, L.nz, round_up3(L.nx + 2, 8)};
+		L.ns = l == 0 ? ns : 14;
 		const size_t pl = L.d.plane();
-		CDR_TRY(h->alloc(&L.so, pl * 14));
+		CDR_TRY(h->alloc(&L.so, pl * L.ns));
 		CDR_TRY(h->alloc(&L.x, pl));
 		CDR_TRY(h->alloc(&L.b, pl));
 		CDR_TRY(h->alloc(&L.r, pl));
 		if (l > 0) CDR_TRY(h->alloc(&L.ci, pl * 26));
 		if (l + 1 < nl) CDR_TRY(h->alloc(&L.sor, pl));
 		// plane problems of this level: the reference's plane config (line-xy,
-		// max-iter 1, other keys at their defaults; src/kernel_params.cc:83-89)
+		// max-iter 1, other keys at their defaults; src/kernel_params.cc:83-89);
+		// five-point planes for a seven-point level (relax_planes.h:77-107)
 		for (int dir = 0; dir < 3 && l + 1 < nl; ++dir) {
 			if (!h->plane(dir)) continue;
 			cdr_gpu_settings s2;
@@ -292,10 +297,10 @@ static int create3(cdr_gpu_solver3 *h, const double *so_src, int src_pitch, cuda
 			const int np = dir == 0 ? L.nz : dir == 1 ? L.ny : L.nx;
 			const int n1 = dir == 2 ? L.ny : L.nx, n2 = dir == 0 ? L.ny : L.nz;
 			L.pl[dir].reset(new Batch2());
-			CDR_TRY(L.pl[dir]->init(s2, 5, n1, n2, np, h->st));
+			CDR_TRY(L.pl[dir]->init(s2, L.ns == 4 ? 3 : 5, n1, n2, np, h->st));
 		}
 		if (h->mixed()) {
-			CDR_TRY(h->alloc(&L.so32, pl * 14));
+			CDR_TRY(h->alloc(&L.so32, pl * L.ns));
 			CDR_TRY(h->alloc(&L.x32, pl));
 			CDR_TRY(h->alloc(&L.b32, pl));
 			CDR_TRY(h->alloc(&L.r32, pl));
@@ -322,7 +327,7 @@ static int create3(cdr_gpu_solver3 *h, const double *so_src, int src_pitch, cuda
 	// fine operator (source pitch) -> device pitch: every row of every k-slice and plane
 	Level3 &F = h->lv[0];
 	CDR_CUDA_TRY(cudaMemcpy2DAsync(F.so, F.d.pitch * sizeof(double), so_src, src_pitch * sizeof(double),
-	                               (nx + 2) * sizeof(double), (size_t)(ny + 2) * (nz + 2) * 14, kind, h->st));
+	                               (nx + 2) * sizeof(double), (size_t)(ny + 2) * (nz + 2) * ns, kind, h->st));
 	CDR_CUDA_TRY(cudaEventRecord(h->ev0, h->st));
 	CDR_TRY(h->setup());
 	CDR_CUDA_TRY(cudaEventRecord(h->ev1, h->st));
@@ -346,22 +351,23 @@ static int solve3_loaded(cdr_gpu_solver3 *h, int *iters, double *hist, int maxhi
 	CDR_CUDA_TRY(cudaEventRecord(h->ev0, st));
 	int cur = 0;
 	if (!h->mixed()) {
-		CDR_TRY(residual_3d<double>(F.so, F.x, F.b, F.r, F.d, h->norm, h->partial, st));
+		CDR_TRY(residual_3d<double>(F.so, F.x, F.b, F.r, F.d, h->norm, h->partial, st, F.ns));
 	} else {
 		CDR_CUDA_TRY(cudaMemcpyAsync(h->x64[0], F.x, sizeof(double) * F.d.plane(), cudaMemcpyDeviceToDevice, st));
-		CDR_TRY(ir_residual_3d(F.so, h->x64[0], F.x32, F.b, h->x64[1], F.b32, F.d, F.d, h->norm, h->partial, 0, st));
+		CDR_TRY(ir_residual_3d(F.so, h->x64[0], F.x32, F.b, h->x64[1], F.b32, F.d, F.d, h->norm, h->partial, 0, st,
+		                       F.ns));
 	}
 	CDR_TRY(fetch());
 	res0 = h->h_norm[0];
 	for (it = 0; it < h->s.maxiter;) {
 		if (!h->mixed()) {
 			CDR_TRY(h->run_cycle(0));
-			CDR_TRY(residual_3d<double>(F.so, F.x, F.b, F.r, F.d, h->norm, h->partial, st));
+			CDR_TRY(residual_3d<double>(F.so, F.x, F.b, F.r, F.d, h->norm, h->partial, st, F.ns));
 		} else {
 			CDR_CUDA_TRY(cudaMemsetAsync(F.x32, 0, sizeof(float) * F.d.plane(), st));
 			CDR_TRY(h->run_cycle(1));
 			CDR_TRY(ir_residual_3d(F.so, h->x64[cur], F.x32, F.b, h->x64[1 - cur], F.b32, F.d, F.d, h->norm,
-			                       h->partial, 1, st));
+			                       h->partial, 1, st, F.ns));
 			cur = 1 - cur;
 		}
 		CDR_TRY(fetch());
@@ -402,11 +408,15 @@ int cdr_gpu_solver3_destroy(cdr_gpu_solver3 *h)
 	return CDR_OK;
 }
 
-static int create3_any(const cdr_gpu_settings *s, const double *so_src, int src_pitch, cudaMemcpyKind kind, int nx,
-                       int ny, int nz, cudaStream_t stream, cdr_gpu_solver3 **out)
+static int create3_any(const cdr_gpu_settings *s, const double *so_src, int src_pitch, cudaMemcpyKind kind, int ns,
+                       int nx, int ny, int nz, cudaStream_t stream, cdr_gpu_solver3 **out)
 {
 	if (!s || !so_src || !out) { set_error(CDR_ERR_ARG, "null argument"); return CDR_ERR_ARG; }
 	*out = nullptr;
+	if (ns != 4 && ns != 14) {
+		set_error(CDR_ERR_ARG, "nstencil %d: 3D operators have 4 (seven-point) or 14 (27-point) planes", ns);
+		return CDR_ERR_ARG;
+	}
 	if (nx < 1 || ny < 1 || nz < 1) { set_error(CDR_ERR_DIM, "bad grid %dx%dx%d", nx, ny, nz); return CDR_ERR_DIM; }
 	if (s->relaxation != CDR_RELAX_POINT && (s->relaxation < CDR_RELAX_PLANE_XY || s->relaxation > CDR_RELAX_PLANE_XYZ)) {
 		set_error(CDR_ERR_UNSUPPORTED, "3D solver: point or plane relaxation (got %d)", s->relaxation);
@@ -430,7 +440,7 @@ static int create3_any(const cdr_gpu_settings *s, const double *so_src, int src_
 	cudaEventCreate(&h->ev0);
 	cudaEventCreate(&h->ev1);
 	int rc = lines_prepare();  // the plane problems' line and fused kernels
-	if (rc == CDR_OK) rc = create3(h, so_src, src_pitch, kind, nx, ny, nz);
+	if (rc == CDR_OK) rc = create3(h, so_src, src_pitch, kind, ns, nx, ny, nz);
 	if (rc != CDR_OK) {
 		cdr_gpu_solver3_destroy(h);
 		return rc;
@@ -439,17 +449,17 @@ static int create3_any(const cdr_gpu_settings *s, const double *so_src, int src_
 	return CDR_OK;
 }
 
-int cdr_gpu_solver3_create(const cdr_gpu_settings *s, const double *so_host, int nx, int ny, int nz,
+int cdr_gpu_solver3_create(const cdr_gpu_settings *s, const double *so_host, int nstencil, int nx, int ny, int nz,
                            cudaStream_t stream, cdr_gpu_solver3 **out)
 {
-	return create3_any(s, so_host, nx + 2, cudaMemcpyHostToDevice, nx, ny, nz, stream, out);
+	return create3_any(s, so_host, nx + 2, cudaMemcpyHostToDevice, nstencil, nx, ny, nz, stream, out);
 }
 
-int cdr_gpu_solver3_create_device(const cdr_gpu_settings *s, const double *so_dev, int nx, int ny, int nz, int pitch,
-                                  cudaStream_t stream, cdr_gpu_solver3 **out)
+int cdr_gpu_solver3_create_device(const cdr_gpu_settings *s, const double *so_dev, int nstencil, int nx, int ny,
+                                  int nz, int pitch, cudaStream_t stream, cdr_gpu_solver3 **out)
 {
 	if (pitch < nx + 2) { set_error(CDR_ERR_DIM, "pitch %d < nx+2", pitch); return CDR_ERR_DIM; }
-	return create3_any(s, so_dev, pitch, cudaMemcpyDeviceToDevice, nx, ny, nz, stream, out);
+	return create3_any(s, so_dev, pitch, cudaMemcpyDeviceToDevice, nstencil, nx, ny, nz, stream, out);
 }
 
 static int copy3(void *dst, int dpitch, const void *src, int spitch, int nx, int ny, int nz, cudaMemcpyKind kind,
@@ -533,7 +543,7 @@ int cdr_gpu_solver3_level_get(const cdr_gpu_solver3 *h, int level, int which, vo
 	const size_t elem = which >= 16 && which < 100 ? sizeof(float) : sizeof(double);
 	size_t n;
 	if (which == 100) n = (size_t)cg3_ldab(h->lv.back().d) * h->lv.back().nx * h->lv.back().ny * h->lv.back().nz;
-	else n = (size_t)(w == 0 ? 14 : w == 6 ? 26 : 1) * h->lv[level].d.plane();
+	else n = (size_t)(w == 0 ? h->lv[level].ns : w == 6 ? 26 : 1) * h->lv[level].d.plane();
 	if (!host || bytes < n * elem) {
 		set_error(CDR_ERR_ARG, "host buffer too small (%zu < %zu)", bytes, n * elem);
 		return CDR_ERR_ARG;

@@ -248,9 +248,99 @@ def fe3_hetero(k):
     return so
 
 
+# --------------------------------------------------------------------------
+# 3D seven-point operators (include/cedar/3d/base_types.h seven_pt): 4 planes
+# p, pw, ps, b with pw/ps/b at s the negated couplings to s-(1,0,0), s-(0,1,0)
+# and s-(0,0,1).
+# --------------------------------------------------------------------------
+
+def _seven_pt(nx, ny, nz, cx, cy, cz):
+    so = np.zeros((4, nz + 2, ny + 2, nx + 2))
+    hx, hy, hz = 1.0 / (nx + 1), 1.0 / (ny + 1), 1.0 / (nz + 1)
+    xh = hy * hz / hx
+    yh = hx * hz / hy
+    zh = hx * hy / hz
+    so[PS3, 1:nz + 1, 2:ny + 1, 1:nx + 1] = cy * yh
+    so[PW3, 1:nz + 1, 1:ny + 1, 2:nx + 1] = cx * xh
+    so[B3, 2:nz + 1, 1:ny + 1, 1:nx + 1] = cz * zh
+    so[P3, 1:nz + 1, 1:ny + 1, 1:nx + 1] = 2.0 * cx * xh + 2.0 * cy * yh + 2.0 * cz * zh
+    return so
+
+
+def poisson3(nx, ny, nz):
+    """Seven-point Laplacian scaled by h^3/h^2, as ``cdr3::gallery::poisson`` (src/3d/gallery.cc:7-55)."""
+    return _seven_pt(nx, ny, nz, 1.0, 1.0, 1.0)  # 2.0*1.0*xh == 2.0*xh exactly
+
+
+def diag_diffusion3(nx, ny, nz, dx, dy, dz):
+    """Anisotropic seven-point operator, as ``cdr3::gallery::diag_diffusion`` (src/3d/gallery.cc:58-107)."""
+    return _seven_pt(nx, ny, nz, dx, dy, dz)
+
+
+def fd3_hetero(k):
+    """Seven-point finite-difference operator of -div(k grad u) with k given at
+    the grid points (nz+2, ny+2, nx+2), ghosts included: the coupling between
+    neighbours a, b is the harmonic mean 2 k_a k_b / (k_a + k_b) times xh, yh or
+    zh (the poisson3 scaling), p the sum of a point's six couplings (those into
+    the Dirichlet ghost layer included, then dropped from the stored planes)."""
+    k = np.asarray(k, dtype=np.float64)
+    nz, ny, nx = k.shape[0] - 2, k.shape[1] - 2, k.shape[2] - 2
+    hx, hy, hz = 1.0 / (nx + 1), 1.0 / (ny + 1), 1.0 / (nz + 1)
+    xh, yh, zh = hy * hz / hx, hx * hz / hy, hx * hy / hz
+    hm = lambda a, b: 2.0 * a * b / (a + b)
+    so = np.zeros((4,) + k.shape)
+    cw = np.zeros(k.shape); cs = np.zeros(k.shape); cb = np.zeros(k.shape)
+    cw[:, :, 1:] = hm(k[:, :, 1:], k[:, :, :-1]) * xh   # coupling of s and s-(1,0,0)
+    cs[:, 1:, :] = hm(k[:, 1:, :], k[:, :-1, :]) * yh
+    cb[1:, :, :] = hm(k[1:, :, :], k[:-1, :, :]) * zh
+    I = (slice(1, nz + 1), slice(1, ny + 1), slice(1, nx + 1))
+    p = np.zeros(k.shape)
+    p[I] = cw[I] + cs[I] + cb[I]
+    p[1:nz + 1, 1:ny + 1, 1:nx + 1] += (cw[1:nz + 1, 1:ny + 1, 2:nx + 2] + cs[1:nz + 1, 2:ny + 2, 1:nx + 1]
+                                        + cb[2:nz + 2, 1:ny + 1, 1:nx + 1])
+    so[P3][I] = p[I]
+    so[PW3, 1:nz + 1, 1:ny + 1, 2:nx + 1] = cw[1:nz + 1, 1:ny + 1, 2:nx + 1]
+    so[PS3, 1:nz + 1, 2:ny + 1, 1:nx + 1] = cs[1:nz + 1, 2:ny + 1, 1:nx + 1]
+    so[B3, 2:nz + 1, 1:ny + 1, 1:nx + 1] = cb[2:nz + 1, 1:ny + 1, 1:nx + 1]
+    return so
+
+
+def seven_to_27(so):
+    """The 14-plane storage of a seven-point operator (the other couplings zero)."""
+    out = np.zeros((14,) + so.shape[1:])
+    out[:4] = so
+    return out
+
+
+def poisson3_rhs_sin2pi(nx, ny, nz):
+    """b = 12 pi^2 sin(2 pi x) sin(2 pi y) sin(2 pi z) hx hy hz (test/3d/test_poisson.cc:12-41)."""
+    hx, hy, hz = 1.0 / (nx + 1), 1.0 / (ny + 1), 1.0 / (nz + 1)
+    h2 = hx * hy * hz
+    pi = math.pi
+    sx = np.sin(2 * pi * (np.arange(1, nx + 1) * hx))
+    sy = np.sin(2 * pi * (np.arange(1, ny + 1) * hy))
+    sz = np.sin(2 * pi * (np.arange(1, nz + 1) * hz))
+    b = np.zeros((nz + 2, ny + 2, nx + 2))
+    b[1:-1, 1:-1, 1:-1] = ((12 * (pi * pi)) * sx[None, None, :] * sy[None, :, None]) * sz[:, None, None] * h2
+    return b
+
+
+def poisson3_exact_sin2pi(nx, ny, nz):
+    """sin(2 pi x) sin(2 pi y) sin(2 pi z) on the whole grid including ghosts (test_poisson.cc:44-68)."""
+    hx, hy, hz = 1.0 / (nx + 1), 1.0 / (ny + 1), 1.0 / (nz + 1)
+    pi = math.pi
+    sx = np.sin(2 * pi * (np.arange(nx + 2) * hx))
+    sy = np.sin(2 * pi * (np.arange(ny + 2) * hy))
+    sz = np.sin(2 * pi * (np.arange(nz + 2) * hz))
+    return sx[None, None, :] * sy[None, :, None] * sz[:, None, None]
+
+
 def stencil3_to_csr(so):
-    """Full sparse matrix of a 14-plane 3D stencil (interior unknowns, i fastest)."""
+    """Full sparse matrix of a 14-plane (or seven-point, 4-plane) 3D stencil
+    (interior unknowns, i fastest)."""
     import scipy.sparse as sp
+    if so.shape[0] == 4:
+        so = seven_to_27(so)
     _, KK, JJ, II = so.shape
     nx, ny, nz = II - 2, JJ - 2, KK - 2
     idx = lambda i, j, k: ((k - 1) * ny + (j - 1)) * nx + (i - 1)

@@ -136,28 +136,31 @@ class Solver2D:
 
 
 class Solver3D:
-    """``cdr3::solver`` (include/cedar/3d/solver.h) on the GPU: 27-point fine
-    operator in Cedar's layout (14, nz+2, ny+2, nx+2), point relaxation."""
+    """``cdr3::solver`` (include/cedar/3d/solver.h) on the GPU: 27-point
+    (xxvii_pt, 14 planes) or seven-point (seven_pt, 4 planes: p, pw, ps, b) fine
+    operator in Cedar's layout (planes, nz+2, ny+2, nx+2)."""
 
-    def __init__(self, so, conf=None, stream=0, dims=None, pitch=None):
-        """so: host array (14, nz+2, ny+2, nx+2), or a device pointer (int) with
-        dims = (nx, ny, nz) and the row pitch of the device array."""
+    def __init__(self, so, conf=None, stream=0, dims=None, pitch=None, nstencil=14):
+        """so: host array (nstencil, nz+2, ny+2, nx+2), or a device pointer (int)
+        with dims = (nx, ny, nz), the row pitch of the device array and nstencil."""
         self.lib = _lib.load()
         self.settings = conf if isinstance(conf, MLSettings) else MLSettings(conf)
         self._s = _settings(self.settings, dim=3)
         h = ctypes.c_void_p()
         if dims is not None:
             self.nx, self.ny, self.nz = dims
-            _lib.check(self.lib.cdr_gpu_solver3_create_device(ctypes.byref(self._s), ctypes.c_void_p(so), self.nx,
-                                                              self.ny, self.nz, pitch, ctypes.c_void_p(stream),
-                                                              ctypes.byref(h)))
+            self.nstencil = nstencil
+            _lib.check(self.lib.cdr_gpu_solver3_create_device(ctypes.byref(self._s), ctypes.c_void_p(so), nstencil,
+                                                              self.nx, self.ny, self.nz, pitch,
+                                                              ctypes.c_void_p(stream), ctypes.byref(h)))
         else:
             so = np.ascontiguousarray(so, dtype=np.float64)
-            if so.ndim != 4 or so.shape[0] != 14:
-                raise ValueError("stencil must have shape (14, nz+2, ny+2, nx+2)")
+            if so.ndim != 4 or so.shape[0] not in (4, 14):
+                raise ValueError("stencil must have shape (14 or 4, nz+2, ny+2, nx+2)")
+            self.nstencil = so.shape[0]
             self.nz, self.ny, self.nx = so.shape[1] - 2, so.shape[2] - 2, so.shape[3] - 2
-            _lib.check(self.lib.cdr_gpu_solver3_create(ctypes.byref(self._s), so.ctypes.data, self.nx, self.ny,
-                                                       self.nz, ctypes.c_void_p(stream), ctypes.byref(h)))
+            _lib.check(self.lib.cdr_gpu_solver3_create(ctypes.byref(self._s), so.ctypes.data, self.nstencil, self.nx,
+                                                       self.ny, self.nz, ctypes.c_void_p(stream), ctypes.byref(h)))
         self.h = h
         self.history = np.zeros(0)
         self.iters = 0
@@ -194,7 +197,7 @@ class Solver3D:
         """Host copy of a level array in Cedar's layout (planes, nz+2, ny+2, nx+2)."""
         p, nx, ny, nz, pitch = self.level_info(level, which, fp32)
         wid = PLANE_NAMES[which] + (16 if fp32 else 0)
-        planes = {"so": 14, "ci": 26}.get(which, 1)
+        planes = {"so": self.nstencil if level == 0 else 14, "ci": 26}.get(which, 1)
         dt = np.float32 if fp32 else np.float64
         buf = np.zeros((planes, nz + 2, ny + 2, pitch), dtype=dt)
         _lib.check(self.lib.cdr_gpu_solver3_level_get(self.h, level, wid, buf.ctypes.data, buf.nbytes))

@@ -268,8 +268,10 @@ int cdr_gpu_solver_level_get(const cdr_gpu_solver *h, int level, int which, void
 int cdr_gpu_solver_timings(const cdr_gpu_solver *h, double *setup_ms, double *solve_ms);
 
 /* ------------------------------------------------------------------------
- * 3D kernels (27-point operators, 14 stencil planes in the order of
- * include/cedar/3d/base_types.h: p pw ps b psw pnw bw bnw bn bne be bse bs bsw).
+ * 3D kernels.  Operators have nstencil planes in the order of
+ * include/cedar/3d/base_types.h: 14 for 27-point operators (xxvii_pt: p pw ps b
+ * psw pnw bw bnw bn bne be bse bs bsw), 4 for seven-point ones (seven_pt: p pw
+ * ps b).  Coarse (Galerkin) operators are always 27-point.
  * A grid of nx*ny*nz interior points has (nx+2)*(ny+2)*(nz+2) entries per
  * plane: rows of `pitch` elements (pitch >= nx+2), k-slices pitch*(ny+2)
  * elements apart, planes pitch*(ny+2)*(nz+2) apart.  Interpolation weights: 26
@@ -278,19 +280,21 @@ int cdr_gpu_solver_timings(const cdr_gpu_solver *h, double *setup_ms, double *so
 
 /* r = b - A x (BMG3_SymStd_residual via include/cedar/3d/residual.h:58); the
  * optional norm is as in the 2D call (scratch of cdr_gpu_norm_scratch_bytes()). */
-int cdr_gpu_residual_3d_f64(const double *so, const double *x, const double *b, double *r, int nx, int ny, int nz,
-                            int pitch, double *norm_out, void *scratch, cudaStream_t stream);
-int cdr_gpu_residual_3d_f32(const float *so, const float *x, const float *b, float *r, int nx, int ny, int nz,
-                            int pitch, double *norm_out, void *scratch, cudaStream_t stream);
+int cdr_gpu_residual_3d_f64(const double *so, int nstencil, const double *x, const double *b, double *r, int nx,
+                            int ny, int nz, int pitch, double *norm_out, void *scratch, cudaStream_t stream);
+int cdr_gpu_residual_3d_f32(const float *so, int nstencil, const float *x, const float *b, float *r, int nx, int ny,
+                            int nz, int pitch, double *norm_out, void *scratch, cudaStream_t stream);
 /* sor = 1/c (BMG3_SymStd_SETUP_recip via include/cedar/3d/relax.h:62). */
 int cdr_gpu_setup_recip_3d_f64(const double *so, double *sor, int nx, int ny, int nz, int pitch,
                                cudaStream_t stream);
-/* One 8-colour Gauss-Seidel sweep (BMG3_SymStd_relax_GS via include/cedar/3d/relax.h:96);
- * updown CDR_DOWN runs the colours 8..1, CDR_UP 1..8. */
-int cdr_gpu_relax_point_3d_f64(const double *so, double *x, const double *b, const double *sor, int nx, int ny,
-                               int nz, int pitch, int updown, cudaStream_t stream);
-int cdr_gpu_relax_point_3d_f32(const float *so, float *x, const float *b, const float *sor, int nx, int ny,
-                               int nz, int pitch, int updown, cudaStream_t stream);
+/* One Gauss-Seidel sweep (BMG3_SymStd_relax_GS via include/cedar/3d/relax.h:96):
+ * 27-point: 8 colours, updown CDR_DOWN runs the colours 8..1, CDR_UP 1..8;
+ * seven-point: red-black, CDR_UP the points with i+j+k even first, CDR_DOWN
+ * the odd ones first (1-based indices). */
+int cdr_gpu_relax_point_3d_f64(const double *so, int nstencil, double *x, const double *b, const double *sor, int nx,
+                               int ny, int nz, int pitch, int updown, cudaStream_t stream);
+int cdr_gpu_relax_point_3d_f32(const float *so, int nstencil, float *x, const float *b, const float *sor, int nx,
+                               int ny, int nz, int pitch, int updown, cudaStream_t stream);
 /* b_coarse = P^T r_fine (BMG3_SymStd_restrict via src/3d/restrict.cc:29).  The
  * coarse grid must be ((nxf-1)/2+1, (nyf-1)/2+1, (nzf-1)/2+1). */
 int cdr_gpu_restrict_3d_f64(const double *ci, const double *r_fine, double *b_coarse, int nxf, int nyf, int nzf,
@@ -302,36 +306,37 @@ int cdr_gpu_interp_add_3d_f64(const double *ci, const double *x_coarse, const do
                               const double *so_fine, double *x_fine, int nxf, int nyf, int nzf, int pitch_f,
                               int nxc, int nyc, int nzc, int pitch_c, cudaStream_t stream);
 /* Operator-induced interpolation weights (BMG3_SymStd_SETUP_interp_OI via
- * include/cedar/3d/interp.h:68), 27-point fine operator. */
-int cdr_gpu_setup_interp_3d_f64(const double *so_fine, double *ci, int nxf, int nyf, int nzf, int pitch_f,
-                                int nxc, int nyc, int nzc, int pitch_c, cudaStream_t stream);
-/* Galerkin coarse operator P^T A P, 14 planes (BMG3_SymStd_SETUP_ITLI27_ex via
- * include/cedar/3d/coarsen.h:56). */
-int cdr_gpu_galerkin_3d_f64(const double *so_fine, const double *ci, double *so_coarse, int nxf, int nyf,
-                            int nzf, int pitch_f, int nxc, int nyc, int nzc, int pitch_c, cudaStream_t stream);
+ * include/cedar/3d/interp.h:68), its 27-point or seven-point branch. */
+int cdr_gpu_setup_interp_3d_f64(const double *so_fine, int nstencil, double *ci, int nxf, int nyf, int nzf,
+                                int pitch_f, int nxc, int nyc, int nzc, int pitch_c, cudaStream_t stream);
+/* Galerkin coarse operator P^T A P, 14 planes (BMG3_SymStd_SETUP_ITLI27_ex, or
+ * ITLI07_ex for a seven-point fine operator, via include/cedar/3d/coarsen.h:46-58). */
+int cdr_gpu_galerkin_3d_f64(const double *so_fine, int nstencil, const double *ci, double *so_coarse, int nxf,
+                            int nyf, int nzf, int pitch_f, int nxc, int nyc, int nzc, int pitch_c,
+                            cudaStream_t stream);
 /* Banded Cholesky of the coarsest operator (BMG3_SymStd_SETUP_cg_LU via
  * include/cedar/3d/solve_cg.h:43): abd holds (nx*(ny+1)+2) * nx*ny*nz doubles;
  * info (device int, may be null) receives the failing column or 0. */
-int cdr_gpu_setup_cg_3d_f64(const double *so, int nx, int ny, int nz, int pitch, double *abd, int *info,
-                            cudaStream_t stream);
+int cdr_gpu_setup_cg_3d_f64(const double *so, int nstencil, int nx, int ny, int nz, int pitch, double *abd,
+                            int *info, cudaStream_t stream);
 /* x = A^{-1} b with that factor (BMG3_SymStd_SOLVE_cg via src/3d/solve_cg.cc:28). */
 int cdr_gpu_solve_cg_3d_f64(const double *abd, double *x, const double *b, int nx, int ny, int nz, int pitch,
                             cudaStream_t stream);
 
 /* ------------------------------------------------------------------------
- * 3D multilevel solver (cdr3::solver, include/cedar/3d/solver.h), 27-point fine
- * operator.  Same settings struct as 2D; relaxation CDR_RELAX_POINT (8-colour
+ * 3D multilevel solver (cdr3::solver, include/cedar/3d/solver.h), 27-point or
+ * seven-point fine operator (nstencil 14 or 4).  Same settings struct as 2D; relaxation CDR_RELAX_POINT (8-colour
  * Gauss-Seidel) or CDR_RELAX_PLANE_* (one 2D line-xy V-cycle per plane, red-black
  * over planes; line_flags applies to those 2D cycles).
  * ------------------------------------------------------------------------ */
 typedef struct cdr_gpu_solver3 cdr_gpu_solver3;
 
-/* Host fine operator in Cedar's layout (pitch nx+2, 14 planes). */
-int cdr_gpu_solver3_create(const cdr_gpu_settings *s, const double *so_host, int nx, int ny, int nz,
+/* Host fine operator in Cedar's layout (pitch nx+2, nstencil planes). */
+int cdr_gpu_solver3_create(const cdr_gpu_settings *s, const double *so_host, int nstencil, int nx, int ny, int nz,
                            cudaStream_t stream, cdr_gpu_solver3 **out);
 /* Same from a DEVICE fine operator of the given pitch. */
-int cdr_gpu_solver3_create_device(const cdr_gpu_settings *s, const double *so_dev, int nx, int ny, int nz, int pitch,
-                                  cudaStream_t stream, cdr_gpu_solver3 **out);
+int cdr_gpu_solver3_create_device(const cdr_gpu_settings *s, const double *so_dev, int nstencil, int nx, int ny,
+                                  int nz, int pitch, cudaStream_t stream, cdr_gpu_solver3 **out);
 int cdr_gpu_solver3_destroy(cdr_gpu_solver3 *h);
 /* Host buffers of (nx+2)*(ny+2)*(nz+2) doubles; as cdr_gpu_solver_solve. */
 int cdr_gpu_solver3_solve(cdr_gpu_solver3 *h, const double *b_host, double *x_host, int *iters, double *hist,

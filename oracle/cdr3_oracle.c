@@ -1,6 +1,6 @@
 /*
  * cdr3_oracle.c -- CPU restatement of Cedar's serial 3D BoxMG path
- * (27-point fine operators, point relaxation).
+ * (27-point and seven-point fine operators, point and plane relaxation).
  *
  * TEST INFRASTRUCTURE ONLY: the parity oracle for the 3D CUDA kernels.
  *
@@ -14,8 +14,12 @@
  * that BMG3_SymStd_interp_add applies (the reference's expanded
  * BMG3_SymStd_SETUP_ITLI27_ex formulas are that same product; its 2D
  * counterpart is restated term by term in cdr2_oracle.c and agrees with the
- * direct product to rounding).  Periodic and indefinite branches and 7-point
- * fine operators are not restated.
+ * direct product to rounding).  A seven-point fine operator (seven_pt: planes
+ * p, pw, ps, b) has its own residual, red-black Gauss-Seidel, interpolation
+ * and plane-relaxation branches; its Galerkin product (which the reference
+ * expands separately in BMG3_SymStd_SETUP_ITLI07_ex) is the same P^T A P with
+ * the missing couplings zero.  Periodic and indefinite branches are not
+ * restated.
  */
 #include <math.h>
 #include <stdlib.h>
@@ -525,6 +529,192 @@ void o3_setup_interp(const double *so, double *ci, int iif, int jjf, int kkf, in
 #undef CI
 }
 
+/* ------------------------------------------------ 7-point fine operators */
+/* BMG3_SymStd_residual.f90:104-119 (seven-point branch; planes p, pw, ps, b) */
+void o3_residual7(const double *so, const double *qf, const double *q, double *res, int II, int JJ, int KK)
+{
+#define Q(i, j, k) q[ix3(i, j, k, II, JJ)]
+	for (int k = 2; k <= KK - 1; ++k)
+		for (int j = 2; j <= JJ - 1; ++j)
+			for (int i = 2; i <= II - 1; ++i)
+				res[ix3(i, j, k, II, JJ)] = qf[ix3(i, j, k, II, JJ)] + SO(i, j, k, KPW) * Q(i - 1, j, k)
+				                            + SO(i, j + 1, k, KPS) * Q(i, j + 1, k) + SO(i + 1, j, k, KPW) * Q(i + 1, j, k)
+				                            + SO(i, j, k, KPS) * Q(i, j - 1, k) + SO(i, j, k, KB) * Q(i, j, k - 1)
+				                            + SO(i, j, k + 1, KB) * Q(i, j, k + 1) - SO(i, j, k, KP) * Q(i, j, k);
+}
+
+/* BMG3_SymStd_relax_GS.f90:141-180 (seven-point): two colours, a point of colour
+ * pts has i+j+k+pts even; UP (and the non-symmetric sweep) runs 0 then 1, DOWN 1 then 0 */
+void o3_relax_gs7(const double *so, const double *qf, double *q, const double *sor, int II, int JJ, int KK, int updown)
+{
+	const int p0 = updown == 1 ? 0 : 1, p1 = updown == 1 ? 1 : 0, pst = updown == 1 ? 1 : -1;
+	for (int pts = p0; pst > 0 ? pts <= p1 : pts >= p1; pts += pst)
+		for (int k = 2; k <= KK - 1; ++k)
+			for (int j = 2; j <= JJ - 1; ++j) {
+				const int ibeg = (j + k + pts) % 2 + 2;
+				for (int i = ibeg; i <= II - 1; i += 2)
+					Q(i, j, k) = (qf[ix3(i, j, k, II, JJ)] + SO(i, j, k, KPW) * Q(i - 1, j, k)
+					              + SO(i, j + 1, k, KPS) * Q(i, j + 1, k) + SO(i + 1, j, k, KPW) * Q(i + 1, j, k)
+					              + SO(i, j, k, KPS) * Q(i, j - 1, k) + SO(i, j, k, KB) * Q(i, j, k - 1)
+					              + SO(i, j, k + 1, KB) * Q(i, j, k + 1))
+					             * sor[ix3(i, j, k, II, JJ)];
+			}
+#undef Q
+}
+
+/* BMG3_SymStd_SETUP_interp_OI.f90:543-807, the seven-point branch (used when the
+ * fine level is the finest and its operator seven-point).  Quirk kept: the
+ * x-edge ep takes abs(b)/so(kp) rather than abs(b/so(kp)). */
+void o3_setup_interp7(const double *so, double *ci, int iif, int jjf, int kkf, int iic, int jjc, int kkc)
+{
+	const int II = iif, JJ = jjf, KK = kkf;
+#define CI(i, j, k, l) ci[ix4(i, j, k, l, iic, jjc, kkc)]
+	const double emach = ldexp(1.0, -53);
+	const int iic1 = iic - 1, jjc1 = jjc - 1, kkc1 = kkc - 1;
+	const int iicf1 = (iif - 2) / 2 + 2, jjcf1 = (jjf - 2) / 2 + 2, kkcf1 = (kkf - 2) / 2 + 2;
+	double a, b, c, ep, dn, dw, de, ds, dp, sum;
+	for (int kc = 2; kc <= kkc1; ++kc)
+		for (int jc = 2; jc <= jjc1; ++jc)
+			for (int ic = 3; ic <= iicf1; ++ic) {
+				const int i = 2 * ic - 2, j = 2 * jc - 2, k = 2 * kc - 2;
+				a = SO(i - 1, j, k, KPW);
+				b = SO(i, j, k, KPW);
+				ep = dmin2(fabs(a / SO(i - 1, j, k, KP)), fabs(b) / SO(i - 1, j, k, KP));
+				c = a + b + SO(i - 1, j, k, KPS) + SO(i - 1, j + 1, k, KPS) + SO(i - 1, j, k, KB) + SO(i - 1, j, k + 1, KB);
+				c = a + b + (SO(i - 1, j, k, KP) - c) * fmax(SO(i - 1, j, k, KP) - (1.0 + ep) * c, 0.0)
+				            / (fabs(SO(i - 1, j, k, KP) - (1.0 + ep) * c) + emach);
+				CI(ic, jc, kc, LXYL) = a / c;
+				CI(ic, jc, kc, LXYR) = b / c;
+			}
+	for (int kc = 2; kc <= kkc1; ++kc)
+		for (int jc = 3; jc <= jjcf1; ++jc)
+			for (int ic = 2; ic <= iic1; ++ic) {
+				const int i = 2 * ic - 2, j = 2 * jc - 2, k = 2 * kc - 2;
+				a = SO(i, j, k, KPS);
+				b = SO(i, j - 1, k, KPS);
+				c = a + b + SO(i, j - 1, k, KPW) + SO(i + 1, j - 1, k, KPW) + SO(i, j - 1, k, KB) + SO(i, j - 1, k + 1, KB);
+				ep = dmin2(fabs(a / SO(i, j - 1, k, KP)), fabs(b / SO(i, j - 1, k, KP)));
+				c = a + b + (SO(i, j - 1, k, KP) - c) * fmax(SO(i, j - 1, k, KP) - (1.0 + ep) * c, 0.0)
+				            / (fabs(SO(i, j - 1, k, KP) - (1.0 + ep) * c) + emach);
+				CI(ic, jc, kc, LXYA) = a / c;
+				CI(ic, jc, kc, LXYB) = b / c;
+			}
+	for (int kc = 3; kc <= kkcf1; ++kc)
+		for (int jc = 2; jc <= jjc1; ++jc)
+			for (int ic = 2; ic <= iic1; ++ic) {
+				const int i = 2 * ic - 2, j = 2 * jc - 2, k = 2 * kc - 2;
+				a = SO(i, j, k, KB);
+				b = SO(i, j, k - 1, KB);
+				c = a + b + SO(i, j, k - 1, KPW) + SO(i + 1, j, k - 1, KPW) + SO(i, j + 1, k - 1, KPS) + SO(i, j, k - 1, KPS);
+				ep = dmin2(fabs(a / SO(i, j, k - 1, KP)), fabs(b / SO(i, j, k - 1, KP)));
+				c = a + b + (SO(i, j, k - 1, KP) - c) * fmax(SO(i, j, k - 1, KP) - (1.0 + ep) * c, 0.0)
+				            / (fabs(SO(i, j, k - 1, KP) - (1.0 + ep) * c) + emach);
+				CI(ic, jc, kc, LXZA) = a / c;
+				CI(ic, jc, kc, LXZB) = b / c;
+			}
+	/* xy faces */
+	for (int ic = 3; ic <= iicf1; ++ic)
+		for (int jc = 3; jc <= jjcf1; ++jc)
+			for (int kc = 2; kc <= kkc1; ++kc) {
+				const int i = 2 * ic - 2, j = 2 * jc - 2, k = 2 * kc - 2;
+				const double o = SO(i - 1, j - 1, k, KP);
+				dn = SO(i - 1, j, k, KPS);
+				dw = SO(i - 1, j - 1, k, KPW);
+				de = SO(i, j - 1, k, KPW);
+				ds = SO(i - 1, j - 1, k, KPS);
+				dp = dw + dn + de + ds;
+				sum = o - SO(i - 1, j - 1, k, KB) - SO(i - 1, j - 1, k + 1, KB);
+				ep = dmin2(dmin2(dmin2(fabs(dw / o), fabs(dn / o)), fabs(de / o)), fabs(ds / o));
+				dp = dp + (sum - dp) * fmax(sum - (1.0 + ep) * dp, 0.0) / (fabs(sum - (1.0 + ep) * dp) + emach);
+				dp = 1.0 / dp;
+				CI(ic, jc, kc, LXYNW) = dp * (CI(ic - 1, jc, kc, LXYA) * dw + CI(ic, jc, kc, LXYL) * dn);
+				CI(ic, jc, kc, LXYNE) = dp * (CI(ic, jc, kc, LXYR) * dn + CI(ic, jc, kc, LXYA) * de);
+				CI(ic, jc, kc, LXYSE) = dp * (CI(ic, jc, kc, LXYB) * de + CI(ic, jc - 1, kc, LXYR) * ds);
+				CI(ic, jc, kc, LXYSW) = dp * (CI(ic, jc - 1, kc, LXYL) * ds + CI(ic - 1, jc, kc, LXYB) * dw);
+			}
+	/* xz faces */
+	for (int kc = 3; kc <= kkcf1; ++kc)
+		for (int jc = 2; jc <= jjc1; ++jc)
+			for (int ic = 3; ic <= iicf1; ++ic) {
+				const int i = 2 * ic - 2, j = 2 * jc - 2, k = 2 * kc - 2;
+				const double o = SO(i - 1, j, k - 1, KP);
+				dn = SO(i - 1, j, k, KB);
+				dw = SO(i - 1, j, k - 1, KPW);
+				de = SO(i, j, k - 1, KPW);
+				ds = SO(i - 1, j, k - 1, KB);
+				dp = dw + dn + de + ds;
+				sum = o - SO(i - 1, j + 1, k - 1, KPS) - SO(i - 1, j, k - 1, KPS);
+				ep = dmin2(dmin2(dmin2(fabs(dw / o), fabs(dn / o)), fabs(de / o)), fabs(ds / o));
+				dp = dp + (sum - dp) * fmax(sum - (1.0 + ep) * dp, 0.0) / (fabs(sum - (1.0 + ep) * dp) + emach);
+				dp = 1.0 / dp;
+				CI(ic, jc, kc, LXZNW) = dp * (CI(ic - 1, jc, kc, LXZA) * dw + CI(ic, jc, kc, LXYL) * dn);
+				CI(ic, jc, kc, LXZNE) = dp * (CI(ic, jc, kc, LXYR) * dn + CI(ic, jc, kc, LXZA) * de);
+				CI(ic, jc, kc, LXZSE) = dp * (CI(ic, jc, kc, LXZB) * de + CI(ic, jc, kc - 1, LXYR) * ds);
+				CI(ic, jc, kc, LXZSW) = dp * (CI(ic, jc, kc - 1, LXYL) * ds + CI(ic - 1, jc, kc, LXZB) * dw);
+			}
+	/* yz faces */
+	for (int kc = 3; kc <= kkcf1; ++kc)
+		for (int jc = 3; jc <= jjcf1; ++jc)
+			for (int ic = 2; ic <= iic1; ++ic) {
+				const int i = 2 * ic - 2, j = 2 * jc - 2, k = 2 * kc - 2;
+				const double o = SO(i, j - 1, k - 1, KP);
+				dn = SO(i, j - 1, k, KB);
+				dw = SO(i, j, k - 1, KPS);
+				de = SO(i, j - 1, k - 1, KPS);
+				ds = SO(i, j - 1, k - 1, KB);
+				dp = dw + dn + de + ds;
+				sum = o - SO(i, j - 1, k - 1, KPW) - SO(i + 1, j - 1, k - 1, KPW);
+				ep = dmin2(dmin2(dmin2(fabs(dw / o), fabs(dn / o)), fabs(de / o)), fabs(ds / o));
+				dp = dp + (sum - dp) * fmax(sum - (1.0 + ep) * dp, 0.0) / (fabs(sum - (1.0 + ep) * dp) + emach);
+				dp = 1.0 / dp;
+				CI(ic, jc, kc, LYZNW) = dp * (CI(ic, jc, kc, LXZA) * dw + CI(ic, jc, kc, LXYA) * dn);
+				CI(ic, jc, kc, LYZNE) = dp * (CI(ic, jc, kc, LXYB) * dn + CI(ic, jc - 1, kc, LXZA) * de);
+				CI(ic, jc, kc, LYZSE) = dp * (CI(ic, jc - 1, kc, LXZB) * de + CI(ic, jc, kc - 1, LXYB) * ds);
+				CI(ic, jc, kc, LYZSW) = dp * (CI(ic, jc, kc - 1, LXYA) * ds + CI(ic, jc, kc, LXZB) * dw);
+			}
+	/* interior points */
+	for (int kc = 3; kc <= kkcf1; ++kc)
+		for (int jc = 3; jc <= jjcf1; ++jc)
+			for (int ic = 3; ic <= iicf1; ++ic) {
+				const int i = 2 * ic - 2, j = 2 * jc - 2, k = 2 * kc - 2;
+				const double o = SO(i - 1, j - 1, k - 1, KP);
+				dp = SO(i - 1, j - 1, k - 1, KPW) + SO(i - 1, j, k - 1, KPS) + SO(i, j - 1, k - 1, KPW)
+				     + SO(i - 1, j - 1, k - 1, KPS) + SO(i - 1, j - 1, k - 1, KB) + SO(i - 1, j - 1, k, KB);
+				ep = dmin2(dmin2(dmin2(dmin2(dmin2(fabs(SO(i - 1, j - 1, k - 1, KPW) / o), fabs(SO(i - 1, j, k - 1, KPS) / o)),
+				                             fabs(SO(i, j - 1, k - 1, KPW) / o)),
+				                       fabs(SO(i - 1, j - 1, k - 1, KPS) / o)),
+				                 fabs(SO(i - 1, j - 1, k - 1, KB) / o)),
+				           fabs(SO(i - 1, j - 1, k, KB) / o));
+				dp = (o - dp) * fmax(o - (1.0 + ep) * dp, 0.0) / (fabs(o - (1.0 + ep) * dp) + emach) + dp;
+				dp = 1.0 / dp;
+				CI(ic, jc, kc, LTNW) = dp * (CI(ic - 1, jc, kc, LYZNW) * SO(i - 1, j - 1, k - 1, KPW)
+				                             + CI(ic, jc, kc, LXZNW) * SO(i - 1, j, k - 1, KPS)
+				                             + CI(ic, jc, kc, LXYNW) * SO(i - 1, j - 1, k, KB));
+				CI(ic, jc, kc, LTNE) = dp * (CI(ic, jc, kc, LXZNE) * SO(i - 1, j, k - 1, KPS)
+				                             + CI(ic, jc, kc, LYZNW) * SO(i, j - 1, k - 1, KPW)
+				                             + CI(ic, jc, kc, LXYNE) * SO(i - 1, j - 1, k, KB));
+				CI(ic, jc, kc, LBNW) = dp * (CI(ic, jc, kc - 1, LXYNW) * SO(i - 1, j - 1, k - 1, KB)
+				                             + CI(ic - 1, jc, kc, LYZSW) * SO(i - 1, j - 1, k - 1, KPW)
+				                             + CI(ic, jc, kc, LXZSW) * SO(i - 1, j, k - 1, KPS));
+				CI(ic, jc, kc, LBNE) = dp * (CI(ic, jc, kc - 1, LXYNE) * SO(i - 1, j - 1, k - 1, KB)
+				                             + CI(ic, jc, kc, LXZSE) * SO(i - 1, j, k - 1, KPS)
+				                             + CI(ic, jc, kc, LYZSW) * SO(i, j - 1, k - 1, KPW));
+				CI(ic, jc, kc, LBSW) = dp * (CI(ic, jc, kc - 1, LXYSW) * SO(i - 1, j - 1, k - 1, KB)
+				                             + CI(ic - 1, jc, kc, LYZSE) * SO(i - 1, j - 1, k - 1, KPW)
+				                             + CI(ic, jc - 1, kc, LXZSW) * SO(i - 1, j - 1, k - 1, KPS));
+				CI(ic, jc, kc, LTSW) = dp * (CI(ic, jc, kc, LXYSW) * SO(i - 1, j - 1, k, KB)
+				                             + CI(ic - 1, jc, kc, LYZNE) * SO(i - 1, j - 1, k - 1, KPW)
+				                             + CI(ic, jc - 1, kc, LXZNW) * SO(i - 1, j - 1, k - 1, KPS));
+				CI(ic, jc, kc, LTSE) = dp * (CI(ic, jc, kc, LXYSE) * SO(i - 1, j - 1, k, KB)
+				                             + CI(ic, jc - 1, kc, LXZNE) * SO(i - 1, j - 1, k - 1, KPS)
+				                             + CI(ic, jc, kc, LYZNE) * SO(i, j - 1, k - 1, KPW));
+				CI(ic, jc, kc, LBSE) = dp * (CI(ic, jc, kc - 1, LXYSE) * SO(i - 1, j - 1, k - 1, KB)
+				                             + CI(ic, jc - 1, kc, LXZSE) * SO(i - 1, j - 1, k - 1, KPS)
+				                             + CI(ic, jc, kc, LYZSE) * SO(i, j - 1, k - 1, KPW));
+			}
+#undef CI
+}
+
 /* ---------------------------------------------------------------- Galerkin */
 /* A[(i,j,k), (i,j,k)+(di,dj,dk)] from the lower-half 14-plane storage (the
  * coefficient that multiplies that neighbour in BMG3_SymStd_residual.f90:76-101,
@@ -715,6 +905,7 @@ struct o3_planes {
 };
 struct o3_level {
 	int nx, ny, nz, ii, jj, kk;
+	int ns;                 /* 14 (27-point) or 4 (7-point fine operator, stored in 14 planes) */
 	double *so, *x, *b, *res, *sor, *ci;
 	struct o3_planes pl[3];
 };
@@ -831,6 +1022,40 @@ static void copy_rhs(const double *so, const double *x, const double *b, int II,
 			X2(b2, p, q) = v;
 		}
 }
+/* copy_coeff for seven_pt -> five_pt (include/cedar/3d/relax_planes.h:73-107):
+ * c, w, s from xy: p, pw, ps; xz: p, pw, b (interior k only); yz: p, ps, b */
+static void copy_coeff7(const double *so, int II, int JJ, int KK, int dir, int ipl, double *so2, int n1, int n2)
+{
+	for (int b = 0; b < n2 + 2; ++b) {
+		if (dir == O3_XZ && (b < 1 || b > n2)) continue;
+		for (int a = 0; a < n1 + 2; ++a) {
+			if (dir == O3_XY) {
+				S2(0, a, b) = S3(KP, a, b, ipl); S2(1, a, b) = S3(KPW, a, b, ipl); S2(2, a, b) = S3(KPS, a, b, ipl);
+			} else if (dir == O3_XZ) {
+				S2(0, a, b) = S3(KP, a, ipl, b); S2(1, a, b) = S3(KPW, a, ipl, b); S2(2, a, b) = S3(KB, a, ipl, b);
+			} else {
+				S2(0, a, b) = S3(KP, ipl, a, b); S2(1, a, b) = S3(KPS, ipl, a, b); S2(2, a, b) = S3(KB, ipl, a, b);
+			}
+		}
+	}
+}
+
+/* copy_rhs for seven_pt (src/3d/relax_planes.cc:25-38 xy, :77-90 xz, :130-143 yz) */
+static void copy_rhs7(const double *so, const double *x, const double *b, int II, int JJ, int KK, int dir, int ipl,
+                      double *b2, int n1, int n2)
+{
+	for (int q = 1; q <= n2; ++q)
+		for (int p = 1; p <= n1; ++p) {
+			double v;
+			if (dir == O3_XY)
+				v = X3(b, p, q, ipl) + S3(KB, p, q, ipl) * X3(x, p, q, ipl - 1) + S3(KB, p, q, ipl + 1) * X3(x, p, q, ipl + 1);
+			else if (dir == O3_XZ)
+				v = X3(b, p, ipl, q) + S3(KPS, p, ipl, q) * X3(x, p, ipl - 1, q) + S3(KPS, p, ipl + 1, q) * X3(x, p, ipl + 1, q);
+			else
+				v = X3(b, ipl, p, q) + S3(KPW, ipl, p, q) * X3(x, ipl - 1, p, q) + S3(KPW, ipl + 1, p, q) * X3(x, ipl + 1, p, q);
+			X2(b2, p, q) = v;
+		}
+}
 #undef X3
 #undef S3
 #undef X2
@@ -862,11 +1087,13 @@ static void planes_setup(struct o3_level *L, int dir)
 	P->b2 = (double *)calloc(g2, sizeof(double));
 	o2_settings s2;
 	plane_settings(&s2);
+	const int ns2 = L->ns == 4 ? 3 : 5;  /* five_pt planes for a seven-point level */
 	for (int ipl = 1; ipl <= P->n; ++ipl) {
 		double *so2 = (double *)calloc(g2 * 5, sizeof(double));
-		copy_coeff(L->so, L->ii, L->jj, L->kk, dir, ipl, so2, P->n1, P->n2);
+		if (ns2 == 3) copy_coeff7(L->so, L->ii, L->jj, L->kk, dir, ipl, so2, P->n1, P->n2);
+		else copy_coeff(L->so, L->ii, L->jj, L->kk, dir, ipl, so2, P->n1, P->n2);
 		P->so2[ipl - 1] = so2;
-		P->s[ipl - 1] = o2_create(&s2, so2, 5, P->n1, P->n2);
+		P->s[ipl - 1] = o2_create(&s2, so2, ns2, P->n1, P->n2);
 	}
 }
 
@@ -894,7 +1121,8 @@ static void relax_planes_level(struct o3_level *L, int dir, double *x, const dou
 		const int beg = c == 0 ? beg0 : beg1;
 		for (int ipl = beg; ipl <= P->n; ipl += 2) {
 			copy32(x, L->ii, L->jj, dir, ipl, P->x2, P->n1, P->n2);
-			copy_rhs(L->so, x, b, L->ii, L->jj, L->kk, dir, ipl, P->b2, P->n1, P->n2);
+			if (L->ns == 4) copy_rhs7(L->so, x, b, L->ii, L->jj, L->kk, dir, ipl, P->b2, P->n1, P->n2);
+			else copy_rhs(L->so, x, b, L->ii, L->jj, L->kk, dir, ipl, P->b2, P->n1, P->n2);
 			o2_vcycle(P->s[ipl - 1], P->x2, P->b2);
 			copy23(P->x2, x, L->ii, L->jj, dir, ipl, P->n1, P->n2);
 		}
@@ -915,7 +1143,8 @@ int o3_num_levels(int nx, int ny, int nz, int min_coarse)
 	return ng;
 }
 
-o3_solver *o3_create(const o3_settings *s, const double *so_fine, int nx, int ny, int nz)
+/* so_fine: nstncl = 14 (xxvii_pt) or 4 (seven_pt: p, pw, ps, b) planes */
+o3_solver *o3_create(const o3_settings *s, const double *so_fine, int nstncl, int nx, int ny, int nz)
 {
 	o3_solver *h = (o3_solver *)calloc(1, sizeof(o3_solver));
 	h->s = *s;
@@ -932,13 +1161,15 @@ o3_solver *o3_create(const o3_settings *s, const double *so_fine, int nx, int ny
 			L->nz = (int)((h->lv[l - 1].nz - 1) / 2. + 1);
 		}
 		L->ii = L->nx + 2; L->jj = L->ny + 2; L->kk = L->nz + 2;
+		L->ns = l == 0 ? nstncl : 14;
 		size_t n = (size_t)L->ii * L->jj * L->kk;
 		L->so = zal(n * 14); L->x = zal(n); L->b = zal(n); L->res = zal(n); L->sor = zal(n); L->ci = zal(n * 26);
 	}
-	memcpy(h->lv[0].so, so_fine, sizeof(double) * (size_t)(nx + 2) * (ny + 2) * (nz + 2) * 14);
+	memcpy(h->lv[0].so, so_fine, sizeof(double) * (size_t)(nx + 2) * (ny + 2) * (nz + 2) * nstncl);
 	for (int l = 0; l + 1 < nl; ++l) {
 		struct o3_level *F = &h->lv[l], *C = &h->lv[l + 1];
-		o3_setup_interp(F->so, C->ci, F->ii, F->jj, F->kk, C->ii, C->jj, C->kk);
+		if (F->ns == 4) o3_setup_interp7(F->so, C->ci, F->ii, F->jj, F->kk, C->ii, C->jj, C->kk);
+		else o3_setup_interp(F->so, C->ci, F->ii, F->jj, F->kk, C->ii, C->jj, C->kk);
 		o3_galerkin(F->so, C->so, C->ci, F->ii, F->jj, F->kk, C->ii, C->jj, C->kk);
 		o3_setup_recip(F->so, F->sor, F->ii, F->jj, F->kk);
 	}
@@ -969,6 +1200,12 @@ void o3_destroy(o3_solver *h)
 	free(h->lv); free(h->abd); free(h->bbd); free(h);
 }
 
+static void resid3(struct o3_level *L, const double *b, const double *x)
+{
+	if (L->ns == 4) o3_residual7(L->so, b, x, L->res, L->ii, L->jj, L->kk);
+	else o3_residual(L->so, b, x, L->res, L->ii, L->jj, L->kk);
+}
+
 /* multilevel::setup_relax_helper closures, include/cedar/multilevel.h:160-222:
  * plane-xyz runs xy, yz, xz going down and xz, yz, xy going up */
 static void smooth3(o3_solver *h, struct o3_level *L, int updown)
@@ -990,7 +1227,9 @@ static void smooth3(o3_solver *h, struct o3_level *L, int updown)
 				relax_planes_level(L, O3_XY, L->x, L->b, updown);
 			}
 			break;
-		default: o3_relax_gs(L->so, L->b, L->x, L->sor, L->ii, L->jj, L->kk, updown);
+		default:
+			if (L->ns == 4) o3_relax_gs7(L->so, L->b, L->x, L->sor, L->ii, L->jj, L->kk, updown);
+			else o3_relax_gs(L->so, L->b, L->x, L->sor, L->ii, L->jj, L->kk, updown);
 		}
 	}
 }
@@ -1001,7 +1240,7 @@ static void ncycle3(o3_solver *h, int l, double *x, const double *b)
 	double *sx = L->x, *sb = L->b;
 	L->x = x; L->b = (double *)b;
 	smooth3(h, L, 0);
-	o3_residual(L->so, L->b, L->x, L->res, L->ii, L->jj, L->kk);
+	resid3(L, L->b, L->x);
 	o3_restrict(C->ci, L->res, C->b, L->ii, L->jj, L->kk, C->ii, C->jj, C->kk);
 	memset(C->x, 0, sizeof(double) * (size_t)C->ii * C->jj * C->kk);
 	if (l + 1 == h->nlev - 1) o3_solve_cg(C->x, C->b, C->ii, C->jj, C->kk, h->abd, h->bbd, h->nabd1);
@@ -1024,12 +1263,12 @@ void o3_vcycle(o3_solver *h, double *x, const double *b)
 int o3_solve(o3_solver *h, const double *b, double *x, double *hist, int maxhist)
 {
 	struct o3_level *L = &h->lv[0];
-	o3_residual(L->so, b, x, L->res, L->ii, L->jj, L->kk);
+	resid3(L, b, x);
 	double res0 = o3_l2norm(L->res, L->ii, L->jj, L->kk);
 	int it;
 	for (it = 0; it < h->s.maxiter; ++it) {
 		o3_vcycle(h, x, b);
-		o3_residual(L->so, b, x, L->res, L->ii, L->jj, L->kk);
+		resid3(L, b, x);
 		double rel = o3_l2norm(L->res, L->ii, L->jj, L->kk) / res0;
 		if (hist && it < maxhist) hist[it] = rel;
 		if (rel < h->s.tol) { ++it; break; }

@@ -28,7 +28,10 @@ int o3_setup_cg(const double *so, int II, int JJ, int KK, double *abd, int nabd1
 void o3_solve_cg(double *q, const double *qf, int II, int JJ, int KK, const double *abd, double *bbd, int nabd1);
 double o3_l2norm(const double *r, int II, int JJ, int KK);
 int o3_num_levels(int nx, int ny, int nz, int min_coarse);
-o3_solver *o3_create(const o3_settings *s, const double *so_fine, int nx, int ny, int nz);
+o3_solver *o3_create(const o3_settings *s, const double *so_fine, int nstncl, int nx, int ny, int nz);
+void o3_residual7(const double *so, const double *qf, const double *q, double *res, int II, int JJ, int KK);
+void o3_relax_gs7(const double *so, const double *qf, double *q, const double *sor, int II, int JJ, int KK, int updown);
+void o3_setup_interp7(const double *so, double *ci, int iif, int jjf, int kkf, int iic, int jjc, int kkc);
 void o3_destroy(o3_solver *h);
 void o3_vcycle(o3_solver *h, double *x, const double *b);
 int o3_solve(o3_solver *h, const double *b, double *x, double *hist, int maxhist);

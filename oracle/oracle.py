@@ -325,7 +325,10 @@ def lib3(variant=""):
             "o3_solve_cg": (None, [P, P, I, I, I, P, P, I]),
             "o3_l2norm": (D, [P, I, I, I]),
             "o3_num_levels": (I, [I, I, I, I]),
-            "o3_create": (P, [ctypes.POINTER(Settings3), P, I, I, I]),
+            "o3_create": (P, [ctypes.POINTER(Settings3), P, I, I, I, I]),
+            "o3_residual7": (None, [P, P, P, P, I, I, I]),
+            "o3_relax_gs7": (None, [P, P, P, P, I, I, I, I]),
+            "o3_setup_interp7": (None, [P, P, I, I, I, I, I, I]),
             "o3_destroy": (None, [P]),
             "o3_vcycle": (None, [P, P, P]),
             "o3_solve": (I, [P, P, P, P, I]),
@@ -349,9 +352,11 @@ def _d3(a):
 
 
 def residual3(so, x, b):
+    """27-point (14 planes) or 7-point (4 planes: p, pw, ps, b) residual."""
     II, JJ, KK = _d3(x)
     r = np.zeros_like(x)
-    lib3().o3_residual(_p(so), _p(b), _p(x), _p(r), II, JJ, KK)
+    f = lib3().o3_residual7 if so.shape[0] == 4 else lib3().o3_residual
+    f(_p(so), _p(b), _p(x), _p(r), II, JJ, KK)
     return r
 
 
@@ -364,18 +369,31 @@ def setup_recip3(so):
 
 def relax_gs3(so, x, b, sor, updown):
     II, JJ, KK = _d3(x)
-    lib3().o3_relax_gs(_p(so), _p(b), _p(x), _p(sor), II, JJ, KK, updown)
+    f = lib3().o3_relax_gs7 if so.shape[0] == 4 else lib3().o3_relax_gs
+    f(_p(so), _p(b), _p(x), _p(sor), II, JJ, KK, updown)
     return x
 
 
 def setup_interp3(so, nxc, nyc, nzc):
     II, JJ, KK = _d3(so)
     ci = np.zeros((26, nzc + 2, nyc + 2, nxc + 2))
-    lib3().o3_setup_interp(_p(so), _p(ci), II, JJ, KK, nxc + 2, nyc + 2, nzc + 2)
+    f = lib3().o3_setup_interp7 if so.shape[0] == 4 else lib3().o3_setup_interp
+    f(_p(so), _p(ci), II, JJ, KK, nxc + 2, nyc + 2, nzc + 2)
     return ci
 
 
+def _pad14(so):
+    """A seven-point operator (4 planes) in the 14-plane storage, other couplings 0:
+    the Galerkin product and the coarse factor read all 14 planes."""
+    if so.shape[0] == 14:
+        return so
+    out = np.zeros((14,) + so.shape[1:])
+    out[:so.shape[0]] = so
+    return out
+
+
 def galerkin3(so, ci):
+    so = _pad14(so)
     II, JJ, KK = _d3(so)
     IIC, JJC, KKC = _d3(ci)
     soc = np.zeros((14, KKC, JJC, IIC))
@@ -400,6 +418,7 @@ def interp_add3(ci, xc, res, so, x):
 
 
 def setup_cg3(so):
+    so = _pad14(so)
     II, JJ, KK = _d3(so)
     nx, ny, nz = II - 2, JJ - 2, KK - 2
     nabd1 = nx * (ny + 1) + 2
@@ -422,17 +441,17 @@ def l2norm3(r):
 
 
 class Solver3:
-    """Serial 3D BoxMG (27-point fine operator, 8-colour point relaxation)."""
+    """Serial 3D BoxMG (27-point or seven-point fine operator; point or plane relaxation)."""
 
     def __init__(self, so, nrelax_pre=2, nrelax_post=1, num_levels=-1, maxiter=10, tol=1e-8, min_coarse=3,
                  relax="point"):
         self.L = lib3()
         so = np.ascontiguousarray(so, dtype=np.float64)
-        assert so.shape[0] == 14
+        assert so.shape[0] in (4, 14)
         self.nz, self.ny, self.nx = so.shape[1] - 2, so.shape[2] - 2, so.shape[3] - 2
         self.s = Settings3(nrelax_pre, nrelax_post, num_levels, maxiter, tol, min_coarse, RELAX3[relax])
         self._so = so
-        self.h = self.L.o3_create(ctypes.byref(self.s), _p(so), self.nx, self.ny, self.nz)
+        self.h = self.L.o3_create(ctypes.byref(self.s), _p(so), so.shape[0], self.nx, self.ny, self.nz)
 
     def __del__(self):
         if getattr(self, "h", None):

@@ -4,7 +4,9 @@ Bit-exact: residual, 8-colour Gauss-Seidel (both directions), restriction,
 interpolate-add, operator-induced interpolation, Galerkin coarse operator,
 coarsest banded Cholesky and the whole FP64 solve (iterates identical, history
 within 1e-12: only the norm's summation order differs).  FP32-refined solves
-must reach the tolerance.
+must reach the tolerance.  The same for seven-point fine operators (4 planes,
+red-black Gauss-Seidel, the seven-point interpolation branch), plus the
+reference's 200^3 seven-point Poisson known-answer test.
 """
 import ctypes
 
@@ -59,7 +61,7 @@ def test_residual3_bitwise(lib, oracle, nx, ny, nz):
     dso, dx, db, dr = padded(so, p), padded(x, p), padded(b, p), padded(np.zeros_like(x), p)
     nrm = padded(np.zeros((1, 1)), 1)
     scratch = padded(np.zeros((1, lib.cdr_gpu_norm_scratch_bytes() // 8)), lib.cdr_gpu_norm_scratch_bytes() // 8)
-    _lib.check(lib.cdr_gpu_residual_3d_f64(ptr(dso), ptr(dx), ptr(db), ptr(dr), nx, ny, nz, p, ptr(nrm),
+    _lib.check(lib.cdr_gpu_residual_3d_f64(ptr(dso), 14, ptr(dx), ptr(db), ptr(dr), nx, ny, nz, p, ptr(nrm),
                                            ptr(scratch), stream()))
     r_ref = oracle.residual3(so, x, b)
     r = unpad(dr, nx)
@@ -78,7 +80,7 @@ def test_gs3_bitwise(lib, oracle, nx, ny, nz):
     xr = x.copy()
     for updown in (_lib.DOWN, _lib.UP, _lib.DOWN):
         oracle.relax_gs3(so, xr, b, sor, updown)
-        _lib.check(lib.cdr_gpu_relax_point_3d_f64(ptr(dso), ptr(dx), ptr(db), ptr(dsor), nx, ny, nz, p, updown,
+        _lib.check(lib.cdr_gpu_relax_point_3d_f64(ptr(dso), 14, ptr(dx), ptr(db), ptr(dsor), nx, ny, nz, p, updown,
                                                   stream()))
     assert np.array_equal(unpad(dx, nx), xr)
 
@@ -93,8 +95,8 @@ def test_setup_interp_galerkin3_bitwise(lib, oracle, nx, ny, nz):
     dso = padded(so, pf)
     dci = padded(np.zeros((26, nzc + 2, nyc + 2, nxc + 2)), pc)
     dsoc = padded(np.zeros((14, nzc + 2, nyc + 2, nxc + 2)), pc)
-    _lib.check(lib.cdr_gpu_setup_interp_3d_f64(ptr(dso), ptr(dci), nx, ny, nz, pf, nxc, nyc, nzc, pc, stream()))
-    _lib.check(lib.cdr_gpu_galerkin_3d_f64(ptr(dso), ptr(dci), ptr(dsoc), nx, ny, nz, pf, nxc, nyc, nzc, pc,
+    _lib.check(lib.cdr_gpu_setup_interp_3d_f64(ptr(dso), 14, ptr(dci), nx, ny, nz, pf, nxc, nyc, nzc, pc, stream()))
+    _lib.check(lib.cdr_gpu_galerkin_3d_f64(ptr(dso), 14, ptr(dci), ptr(dsoc), nx, ny, nz, pf, nxc, nyc, nzc, pc,
                                            stream()))
     ci = unpad(dci, nxc)
     soc = unpad(dsoc, nxc)
@@ -138,7 +140,7 @@ def test_coarse_cholesky3_bitwise(lib, oracle, n):
     ldab = nx * (ny + 1) + 2
     dabd = torch.zeros(ldab * nx * ny * nz, dtype=torch.float64, device="cuda")
     dinfo = torch.ones(1, dtype=torch.int32, device="cuda")
-    _lib.check(lib.cdr_gpu_setup_cg_3d_f64(ptr(dso), nx, ny, nz, p, ptr(dabd), ptr(dinfo), stream()))
+    _lib.check(lib.cdr_gpu_setup_cg_3d_f64(ptr(dso), 14, nx, ny, nz, p, ptr(dabd), ptr(dinfo), stream()))
     _lib.check(lib.cdr_gpu_solve_cg_3d_f64(ptr(dabd), ptr(dx), ptr(db), nx, ny, nz, p, stream()))
     assert int(dinfo.cpu()[0]) == 0
     assert np.array_equal(host(dabd).reshape(abd_ref.shape), abd_ref)
@@ -197,7 +199,7 @@ def test_solver3_rejects_unsupported(lib):
     lib.cdr_gpu_settings_default(ctypes.byref(s))
     s.relaxation = 1
     h = ctypes.c_void_p()
-    rc = lib.cdr_gpu_solver3_create(ctypes.byref(s), so.ctypes.data, 7, 7, 7, None, ctypes.byref(h))
+    rc = lib.cdr_gpu_solver3_create(ctypes.byref(s), so.ctypes.data, 14, 7, 7, 7, None, ctypes.byref(h))
     assert rc == 7  # CDR_ERR_UNSUPPORTED
 
 
@@ -272,3 +274,132 @@ def test_solver3_plane_relaxation_fast_path_reaches_tol(lib, oracle, prec):
     assert len(s.history) <= len(h_ref) + 2
     r = oracle.residual3(so, x, b)
     assert oracle.l2norm3(r) / oracle.l2norm3(b) < 1e-10
+
+
+# ------------------------------------------------------- seven-point operators
+def make_op7(nx, ny, nz, seed=0, sigma=1.0):
+    rng = np.random.default_rng(seed + 100 * nx + 10 * ny + nz)
+    return G.fd3_hetero(np.exp(sigma * rng.standard_normal((nz + 2, ny + 2, nx + 2))))
+
+
+@pytest.mark.parametrize("nx,ny,nz", SIZES)
+def test_seven_point_residual_gs_bitwise(lib, oracle, nx, ny, nz):
+    so, x, b = make_op7(nx, ny, nz), grid3(nx, ny, nz, 21), grid3(nx, ny, nz, 22)
+    p = pitch_of(nx, 2)
+    dso, dx, db, dr = padded(so, p), padded(x, p), padded(b, p), padded(np.zeros_like(x), p)
+    nrm = padded(np.zeros((1, 1)), 1)
+    scratch = padded(np.zeros((1, lib.cdr_gpu_norm_scratch_bytes() // 8)), lib.cdr_gpu_norm_scratch_bytes() // 8)
+    _lib.check(lib.cdr_gpu_residual_3d_f64(ptr(dso), 4, ptr(dx), ptr(db), ptr(dr), nx, ny, nz, p, ptr(nrm),
+                                           ptr(scratch), stream()))
+    r_ref = oracle.residual3(so, x, b)
+    assert np.array_equal(unpad(dr, nx)[1:-1, 1:-1, 1:-1], r_ref[1:-1, 1:-1, 1:-1])
+    assert abs(host(nrm)[0, 0] - oracle.l2norm3(r_ref)) <= 1e-13 * oracle.l2norm3(r_ref)
+    sor = oracle.setup_recip3(so)
+    dsor = padded(np.zeros_like(x), p)
+    _lib.check(lib.cdr_gpu_setup_recip_3d_f64(ptr(dso), ptr(dsor), nx, ny, nz, p, stream()))
+    xr = x.copy()
+    for updown in (_lib.DOWN, _lib.UP, _lib.UP, _lib.DOWN):
+        oracle.relax_gs3(so, xr, b, sor, updown)
+        _lib.check(lib.cdr_gpu_relax_point_3d_f64(ptr(dso), 4, ptr(dx), ptr(db), ptr(dsor), nx, ny, nz, p, updown,
+                                                  stream()))
+    assert np.array_equal(unpad(dx, nx), xr)
+
+
+@pytest.mark.parametrize("nx,ny,nz", SIZES)
+def test_seven_point_interp_galerkin_bitwise(lib, oracle, nx, ny, nz):
+    so = make_op7(nx, ny, nz, seed=23, sigma=1.5)
+    nxc, nyc, nzc = coarse(nx), coarse(ny), coarse(nz)
+    ci_ref = oracle.setup_interp3(so, nxc, nyc, nzc)
+    soc_ref = oracle.galerkin3(so, ci_ref)
+    pf, pc = pitch_of(nx, 4), pitch_of(nxc, 1)
+    dso = padded(so, pf)
+    dci = padded(np.zeros((26, nzc + 2, nyc + 2, nxc + 2)), pc)
+    dsoc = padded(np.zeros((14, nzc + 2, nyc + 2, nxc + 2)), pc)
+    _lib.check(lib.cdr_gpu_setup_interp_3d_f64(ptr(dso), 4, ptr(dci), nx, ny, nz, pf, nxc, nyc, nzc, pc, stream()))
+    _lib.check(lib.cdr_gpu_galerkin_3d_f64(ptr(dso), 4, ptr(dci), ptr(dsoc), nx, ny, nz, pf, nxc, nyc, nzc, pc,
+                                           stream()))
+    ci, soc = unpad(dci, nxc), unpad(dsoc, nxc)
+    bad = [l for l in range(26) if not np.array_equal(ci[l], ci_ref[l])]
+    assert not bad, "interpolation planes differ: %s" % bad
+    bad = [q for q in range(14) if not np.array_equal(soc[q], soc_ref[q])]
+    assert not bad, "Galerkin planes differ: %s" % bad
+
+
+def test_seven_point_coarse_cholesky_bitwise(lib, oracle):
+    import torch
+    nx, ny, nz = 5, 4, 6
+    so = make_op7(nx, ny, nz, seed=24)
+    b = grid3(nx, ny, nz, 25)
+    abd_ref, info = oracle.setup_cg3(so)
+    assert info == 0
+    x_ref = oracle.solve_cg3(abd_ref, b)
+    p = pitch_of(nx, 3)
+    dso, db, dx = padded(so, p), padded(b, p), padded(np.zeros_like(b), p)
+    dabd = torch.zeros((nx * (ny + 1) + 2) * nx * ny * nz, dtype=torch.float64, device="cuda")
+    dinfo = torch.ones(1, dtype=torch.int32, device="cuda")
+    _lib.check(lib.cdr_gpu_setup_cg_3d_f64(ptr(dso), 4, nx, ny, nz, p, ptr(dabd), ptr(dinfo), stream()))
+    _lib.check(lib.cdr_gpu_solve_cg_3d_f64(ptr(dabd), ptr(dx), ptr(db), nx, ny, nz, p, stream()))
+    assert int(dinfo.cpu()[0]) == 0
+    assert np.array_equal(host(dabd).reshape(abd_ref.shape), abd_ref)
+    assert np.array_equal(unpad(dx, nx)[1:-1, 1:-1, 1:-1], x_ref[1:-1, 1:-1, 1:-1])
+
+
+@pytest.mark.parametrize("relax,n", [("point", (15, 15, 15)), ("point", (31, 30, 33)), ("plane-xyz", (15, 15, 15)),
+                                     ("plane-xyz", (16, 13, 19))])
+def test_seven_point_solver3_matches_oracle(lib, oracle, relax, n):
+    from cedar_b200.solver import Solver3D
+    nx, ny, nz = n
+    so = make_op7(nx, ny, nz, seed=26, sigma=1.5)
+    b = _rhs3(nx, ny, nz, seed=27)
+    conf = Config({"solver": {"relaxation": relax, "max-iter": 40, "tol": 1e-10}, "gpu": {"line-solve": "sequential"}})
+    s = Solver3D(so, conf)
+    ref = oracle.Solver3(so, maxiter=40, tol=1e-10, relax=relax)
+    assert s.nlevels == ref.nlevels
+    assert np.array_equal(s.level_array(0, "so"), so)
+    for l in range(1, s.nlevels):
+        assert np.array_equal(s.level_array(l, "so"), ref.level_array(l, "so")), "level %d operator" % l
+    x = s.solve(b)
+    x_ref, h_ref = ref.solve(b)
+    assert len(s.history) == len(h_ref)
+    assert np.abs(s.history - h_ref).max() <= 1e-12 * max(1.0, h_ref.max())
+    assert np.array_equal(x, x_ref)
+    assert h_ref[-1] < 1e-10
+
+
+@pytest.mark.parametrize("relax", ["point", "plane-xyz"])
+def test_seven_point_solver3_fp32_ir_reaches_tol(lib, oracle, relax):
+    from cedar_b200.solver import Solver3D
+    n = 31
+    so = make_op7(n, n, n, seed=28, sigma=1.0)  # sigma 2: 57 FP64 point cycles to 1e-10
+    b = _rhs3(n, n, n, seed=29)
+    s = Solver3D(so, Config({"solver": {"relaxation": relax, "max-iter": 30, "tol": 1e-10},
+                             "gpu": {"precision": "fp32-ir"}}))
+    x = s.solve(b)
+    assert s.history[-1] < 1e-10
+    r = oracle.residual3(so, x, b)
+    assert oracle.l2norm3(r) / oracle.l2norm3(b) < 1e-10
+    _, h_ref = oracle.Solver3(so, maxiter=30, tol=1e-10, relax=relax).solve(b)
+    assert len(s.history) <= len(h_ref) + 2
+
+
+def test_seven_point_poisson_known_answer_200(lib, oracle):
+    """test/3d/test_poisson.cc:73-104 (SerialPoisson3.Isotropic) at its own size:
+    200^3 seven-point Poisson, default settings; ||r||_2 < 1e-8 and the error
+    against sin(2 pi x) sin(2 pi y) sin(2 pi z) below 1e-4."""
+    from cedar_b200.solver import Solver3D
+    n = 200
+    so = G.poisson3(n, n, n)
+    b = G.poisson3_rhs_sin2pi(n, n, n)
+    s = Solver3D(so, Config({}))
+    x = s.solve(b)
+    r = oracle.residual3(so, x, b)
+    assert oracle.l2norm3(r) < 1e-8
+    assert np.abs(x - G.poisson3_exact_sin2pi(n, n, n))[1:-1, 1:-1, 1:-1].max() < 1e-4
+
+
+def test_solver3_rejects_bad_nstencil(lib):
+    so = make_op7(7, 7, 7)
+    s = _lib.Settings()
+    lib.cdr_gpu_settings_default(ctypes.byref(s))
+    h = ctypes.c_void_p()
+    assert lib.cdr_gpu_solver3_create(ctypes.byref(s), so.ctypes.data, 5, 7, 7, 7, None, ctypes.byref(h)) == 1

@@ -295,3 +295,129 @@ def test_3d_plane_boxmg_converges(oracle):
     _, hp = oracle.Solver3(so, maxiter=12, tol=1e-10, relax="plane-xyz").solve(b)
     _, h0 = oracle.Solver3(so, maxiter=12, tol=1e-10).solve(b)
     assert hp[-1] < 1e-10 and len(hp) <= len(h0)
+
+
+# ----------------------------------------------------------- 3D seven-point
+def _gs7_dense(A, x, b, updown):
+    """Red-black Gauss-Seidel on the assembled matrix: colour pts holds the points
+    with I+J+K+pts even in the reference's 1-based indices (I = numpy index + 1
+    with the ghost at 0), colour 0 first going up."""
+    nz, ny, nx = x.shape[0] - 2, x.shape[1] - 2, x.shape[2] - 2
+    K, J, I = np.meshgrid(np.arange(1, nz + 1), np.arange(1, ny + 1), np.arange(1, nx + 1), indexing="ij")
+    par = ((I + J + K + 3) % 2).ravel()
+    xv = x[1:-1, 1:-1, 1:-1].ravel().copy()
+    bv = b[1:-1, 1:-1, 1:-1].ravel()
+    for pts in ((0, 1) if updown == 1 else (1, 0)):
+        idx = np.nonzero((par + pts) % 2 == 0)[0]
+        d = A.diagonal()[idx]
+        xv[idx] = (bv[idx] - (A[idx] @ xv - d * xv[idx])) / d
+    out = x.copy()
+    out[1:-1, 1:-1, 1:-1] = xv.reshape(nz, ny, nx)
+    return out
+
+
+def _op7(nx, ny, nz, seed, sigma=1.0):
+    rng = np.random.default_rng(seed)
+    return G.fd3_hetero(np.exp(sigma * rng.normal(size=(nz + 2, ny + 2, nx + 2))))
+
+
+@pytest.mark.parametrize("n", [(7, 6, 5), (8, 9, 10)])
+def test_3d_seven_point_residual_and_gs_match_assembled_matrix(oracle, n):
+    nx, ny, nz = n
+    so = _op7(nx, ny, nz, seed=31)
+    A = G.stencil3_to_csr(so)
+    assert abs(A - A.T).max() == 0
+    rng = np.random.default_rng(32)
+    x = np.zeros((nz + 2, ny + 2, nx + 2)); x[1:-1, 1:-1, 1:-1] = rng.random((nz, ny, nx))
+    b = np.zeros_like(x); b[1:-1, 1:-1, 1:-1] = rng.random((nz, ny, nx))
+    r = oracle.residual3(so, x, b)
+    np.testing.assert_allclose(r[1:-1, 1:-1, 1:-1].ravel(), b[1:-1, 1:-1, 1:-1].ravel() - A @ x[1:-1, 1:-1, 1:-1].ravel(),
+                               atol=1e-14)
+    sor = oracle.setup_recip3(so)
+    for updown in (0, 1):
+        got = oracle.relax_gs3(so, x.copy(), b, sor, updown)
+        np.testing.assert_allclose(got, _gs7_dense(A, x, b, updown), rtol=1e-13, atol=1e-14)
+
+
+@pytest.mark.parametrize("n", [7, 8, 9])
+def test_3d_seven_point_interpolation_and_galerkin(oracle, n):
+    """Edge weights equal the 27-point branch's on the zero-padded operator (the
+    27-point sums reduce to the seven-point ones term by term); the Galerkin
+    operator is P^T A P; constants are reproduced away from the boundary."""
+    so = _op7(n, n, n, seed=n, sigma=1.2)
+    nc = (n - 1) // 2 + 1
+    ci = oracle.setup_interp3(so, nc, nc, nc)
+    ci27 = oracle.setup_interp3(G.seven_to_27(so), nc, nc, nc)
+    for l in range(6):  # lxyl lxyr lxya lxyb lxza lxzb
+        np.testing.assert_array_equal(ci[l], ci27[l])
+    soc = oracle.galerkin3(so, ci)
+    A = G.stencil3_to_csr(so).toarray()
+    Pm = np.zeros((n ** 3, nc ** 3))
+    for kc in range(nc):
+        for jc in range(nc):
+            for ic in range(nc):
+                xc = np.zeros((nc + 2,) * 3)
+                xc[kc + 1, jc + 1, ic + 1] = 1
+                xf = np.zeros((n + 2,) * 3)
+                oracle.interp_add3(ci, xc, np.zeros_like(xf), so, xf)
+                Pm[:, (kc * nc + jc) * nc + ic] = xf[1:-1, 1:-1, 1:-1].ravel()
+    Ac = Pm.T @ A @ Pm
+    assert np.abs(Ac - G.stencil3_to_csr(soc).toarray()).max() <= 1e-14 * np.abs(Ac).max()
+    so1 = G.poisson3(n, n, n)
+    ci1 = oracle.setup_interp3(so1, nc, nc, nc)
+    xc = np.zeros((nc + 2,) * 3); xc[1:-1, 1:-1, 1:-1] = 1.0
+    xf = np.zeros((n + 2,) * 3)
+    oracle.interp_add3(ci1, xc, np.zeros_like(xf), so1, xf)
+    assert abs(xf[n // 2, n // 2, n // 2] - 1.0) < 1e-12
+
+
+def test_3d_seven_point_poisson_known_answer(oracle):
+    """test/3d/test_poisson.cc:73-104 (SerialPoisson3.Isotropic) at n = 39 instead
+    of 200: the default solve ends with ||r||_2 < 1e-8, and the error against
+    sin(2 pi x) sin(2 pi y) sin(2 pi z) is the O(h^2) discretisation error
+    (below 1e-4 at n = 200; scaled by (201/40)^2 here)."""
+    n = 39
+    so = G.poisson3(n, n, n)
+    b = G.poisson3_rhs_sin2pi(n, n, n)
+    s = oracle.Solver3(so)
+    x, h = s.solve(b)
+    r = oracle.residual3(so, x, b)
+    assert oracle.l2norm3(r) < 1e-8
+    err = np.abs(x - G.poisson3_exact_sin2pi(n, n, n))[1:-1, 1:-1, 1:-1].max()
+    assert err < 1e-4 * (201 / 40) ** 2
+    assert h[-1] < 1e-8 and len(h) <= 10
+
+
+@pytest.mark.parametrize("direction", ["xy", "xz", "yz"])
+def test_3d_seven_point_plane_relaxation_is_block_gauss_seidel(oracle, direction):
+    nx, ny, nz = 4, 4, 4
+    so = _op7(nx, ny, nz, seed=33)
+    A = G.stencil3_to_csr(so).toarray()
+    s = oracle.Solver3(so, relax="plane-xyz", min_coarse=2)
+    assert s.nlevels == 2
+    rng = np.random.default_rng(34)
+    for updown in (0, 1):
+        x = np.zeros((nz + 2, ny + 2, nx + 2)); x[1:-1, 1:-1, 1:-1] = rng.random((nz, ny, nx))
+        b = np.zeros_like(x); b[1:-1, 1:-1, 1:-1] = rng.random((nz, ny, nx))
+        ref = _block_gs_planes(A, nx, ny, nz, direction, x, b, updown)
+        got = s.relax_planes(0, direction, x.copy(), b, updown)
+        np.testing.assert_allclose(got[1:-1, 1:-1, 1:-1], ref[1:-1, 1:-1, 1:-1], rtol=1e-11, atol=1e-13)
+    # each plane's five-point operator is the in-plane block of A
+    s2 = oracle.Solver3(_op7(5, 6, 7, seed=35), relax="plane-xyz", num_levels=2)
+    A2full = G.stencil3_to_csr(_op7(5, 6, 7, seed=35)).toarray()
+    idx = np.arange(5 * 6 * 7).reshape(7, 6, 5)
+    ipl = 2
+    so2 = s2.plane_op(0, direction, ipl)
+    ip = (idx[ipl - 1] if direction == "xy" else idx[:, ipl - 1, :] if direction == "xz" else idx[:, :, ipl - 1]).ravel()
+    assert not so2[3:].any()
+    np.testing.assert_array_equal(G.stencil_to_csr(np.ascontiguousarray(so2[:3])).toarray(), A2full[np.ix_(ip, ip)])
+
+
+def test_3d_seven_point_boxmg_converges_both_smoothers(oracle):
+    n = 15
+    so = _op7(n, n, n, seed=36, sigma=1.5)
+    rng = np.random.default_rng(37)
+    b = np.zeros((n + 2,) * 3); b[1:-1, 1:-1, 1:-1] = rng.uniform(-1, 1, (n, n, n)) / (n + 1) ** 3
+    _, h0 = oracle.Solver3(so, maxiter=20, tol=1e-10).solve(b)
+    _, hp = oracle.Solver3(so, maxiter=20, tol=1e-10, relax="plane-xyz").solve(b)
+    assert h0[-1] < 1e-10 and hp[-1] < 1e-10 and len(hp) <= len(h0)
