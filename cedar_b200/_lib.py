@@ -16,6 +16,7 @@ DOWN, UP = 0, 1
 RELAX = {"point": 0, "line-x": 1, "line-y": 2, "line-xy": 3,
          "plane-xy": 4, "plane-xz": 5, "plane-yz": 6, "plane-xyz": 7}
 PREC = {"fp64": 0, "fp32-ir": 1}
+KRYLOV = {"none": 0, "fcg": 1}
 DIR_X, DIR_Y = 0, 1
 LINES_EXACT = 1
 
@@ -34,7 +35,8 @@ class Settings(ctypes.Structure):
                 ("nrelax_post", ctypes.c_int), ("num_levels", ctypes.c_int),
                 ("maxiter", ctypes.c_int), ("tol", ctypes.c_double),
                 ("min_coarse", ctypes.c_int), ("precision", ctypes.c_int),
-                ("use_graph", ctypes.c_int), ("line_flags", ctypes.c_int), ("fuse_coarse", ctypes.c_int)]
+                ("use_graph", ctypes.c_int), ("line_flags", ctypes.c_int), ("fuse_coarse", ctypes.c_int),
+                ("krylov", ctypes.c_int)]
 
 
 def header_symbols():

@@ -6,8 +6,9 @@ note that the reference reads ``solver.min_coarse`` (underscore), so the
 ``"min-coarse"`` key found in its example configs has no effect there or here.
 GPU options live under the ``"gpu"`` object: ``precision`` ("fp64" | "fp32-ir"),
 ``graph`` (bool), ``fuse-coarse`` (levels with both edges at most this many
-points run as one fused kernel; 0 = off; default 32) and ``line-solve`` ("scan": parallel line substitutions, the
-default; "sequential": DPTTRS order, bit-identical to the reference).
+points run as one fused kernel; 0 = off; default 32), ``line-solve`` ("scan": parallel line substitutions, the
+default; "sequential": DPTTRS order, bit-identical to the reference) and ``krylov`` ("none": the reference's
+outer loop, the default; "fcg": the cycle preconditions flexible conjugate gradients, 2D only).
 """
 import json
 import os
@@ -76,6 +77,9 @@ class MLSettings:
         self.fuse_coarse = int(conf.get("gpu.fuse-coarse", 32))
         if self.fuse_coarse < 0:
             raise ValueError("invalid gpu.fuse-coarse: %d" % self.fuse_coarse)
+        self.krylov = conf.get("gpu.krylov", "none")
+        if self.krylov not in ("none", "fcg"):
+            raise ValueError("invalid gpu.krylov: %s" % self.krylov)
 
     def __repr__(self):
         return ("MLSettings(relaxation=%r, cycle=%r, nrelax=(%d,%d), num_levels=%d, maxiter=%d, "

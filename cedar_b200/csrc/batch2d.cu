@@ -412,6 +412,10 @@ int cdr_gpu_batch2d_create(const cdr_gpu_settings *s, const double *so_dev, int 
 		set_error(CDR_ERR_ARG, "invalid precision %d", s->precision);
 		return CDR_ERR_ARG;
 	}
+	if (s->krylov != CDR_KRYLOV_NONE) {
+		set_error(CDR_ERR_UNSUPPORTED, "batched 2D solves: the Krylov outer iteration is implemented for the 2D solver only");
+		return CDR_ERR_UNSUPPORTED;
+	}
 	if (s->maxiter < 1) { set_error(CDR_ERR_ARG, "max-iter must be positive"); return CDR_ERR_ARG; }
 	cdr_gpu_batch2d *h = new cdr_gpu_batch2d();
 	if (stream) h->st = stream;

@@ -34,6 +34,23 @@ int ir_residual_2d(const double *so, int nstencil, const double *x, const float 
 // partial-sum blocks per problem of a residual norm (partial holds nb times that)
 int norm_blocks(Dims2 d);
 
+// Device scalars of a flexible-CG solve (k2_krylov.cu); the partial-sum
+// scratch of its kernels is kNormScratchBytes.
+struct FcgScalars {
+	double zq, pq, beta, alpha, rr;
+	int first, iter;
+	unsigned ticket[3];
+};
+// r -> preconditioner input rin (zero ghost ring), z = 0, restart the recurrences
+template <typename TZ>
+int fcg_load(const double *r, TZ *rin, TZ *z, Dims2 d, FcgScalars *S, cudaStream_t st);
+// One FCG iteration after the preconditioner wrote z (3 launches); leaves the
+// next preconditioner input in rin, z = 0 and |r|^2 in S->rr.  x alternates
+// between x0 and x1: after the step the iterate is in x[S->iter & 1].
+template <typename TZ>
+int fcg_step(const double *so, int ns, TZ *z, TZ *rin, double *x0, double *x1, const double *b, double *r,
+             double *p0, double *p1, double *q, Dims2 d, double *partial, FcgScalars *S, cudaStream_t st);
+
 constexpr size_t kNormScratchBytes = 2048 * sizeof(double);
 
 // Levels of a fused coarse cycle (k2_coarse.cu): level 0 holds the restricted

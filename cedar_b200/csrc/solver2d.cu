@@ -15,6 +15,9 @@
 //   CDR_PREC_F32_IR  FP64 iterative refinement: r = b - A x in FP64, one FP32
 //                    V-cycle on r (FP32 copies of every operator, interpolation
 //                    and line factor; FP64 coarsest Cholesky), x += e in FP64.
+// With settings.krylov = CDR_KRYLOV_FCG either cycle instead preconditions
+// flexible CG (k2_krylov.cu); the iteration (cycle + three FCG kernels) is one
+// CUDA graph.
 #include <vector>
 #include <cstring>
 #include <cmath>
@@ -49,6 +52,11 @@ struct cdr_gpu_solver {
 	double *norm = nullptr;     // device scalars
 	double *partial = nullptr;  // norm scratch
 	double *x64[2] = {nullptr, nullptr};
+	// flexible CG: b, x, r, p (two buffers), q on the fine grid (FP64) and the scalars
+	double *kb = nullptr, *kx[2] = {nullptr, nullptr}, *kr = nullptr, *kp[2] = {nullptr, nullptr}, *kq = nullptr;
+	FcgScalars *ks = nullptr;
+	cudaGraphExec_t kexec[2] = {nullptr, nullptr};  // FCG iteration graphs: [0] FP64, [1] FP32 cycle
+	long long klaunches[2] = {0, 0};
 	double *h_norm = nullptr;   // pinned host copy of the norm
 	cudaStream_t st = nullptr;
 	bool own_stream = false;
@@ -85,6 +93,9 @@ struct cdr_gpu_solver {
 	template <typename T>
 	int cycle(T *x, const T *b);
 	int run_cycle(int prec);
+	template <typename T>
+	int fcg_iteration();
+	int run_fcg(int prec);
 	int setup();
 };
 
@@ -253,6 +264,45 @@ int cdr_gpu_solver::run_cycle(int prec)
 	return CDR_OK;
 }
 
+// One FCG iteration: the cycle on the preconditioner input (zero initial
+// guess) and the three FCG kernels.
+template <typename T>
+int cdr_gpu_solver::fcg_iteration()
+{
+	Level &F = lv[0];
+	T *z = Arr<T>::x(F), *rin = Arr<T>::b(F);
+	CDR_TRY(cycle<T>(z, rin));
+	return fcg_step<T>(F.so, F.ns, z, rin, kx[0], kx[1], kb, kr, kp[0], kp[1], kq, F.d, partial, ks, st);
+}
+
+int cdr_gpu_solver::run_fcg(int prec)
+{
+	auto body = [&]() -> int { return prec == 0 ? fcg_iteration<double>() : fcg_iteration<float>(); };
+	if (!s.use_graph) return body();
+	if (!kexec[prec]) {
+		cudaGraph_t g = nullptr;
+		CDR_CUDA_TRY(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+		const long long before = cdr_gpu_launch_count();
+		int rc = body();
+		klaunches[prec] = cdr_gpu_launch_count() - before;
+		count_launches(-klaunches[prec]);  // captured, not launched
+		cudaError_t e = cudaStreamEndCapture(st, &g);
+		if (rc != CDR_OK) {
+			if (g) cudaGraphDestroy(g);
+			return rc;
+		}
+		if (e != cudaSuccess) {
+			set_error(CDR_ERR_CUDA, "graph capture: %s", cudaGetErrorString(e));
+			return CDR_ERR_CUDA;
+		}
+		CDR_CUDA_TRY(cudaGraphInstantiate(&kexec[prec], g, 0));
+		cudaGraphDestroy(g);
+	}
+	CDR_CUDA_TRY(cudaGraphLaunch(kexec[prec], st));
+	count_launches(klaunches[prec]);
+	return CDR_OK;
+}
+
 // multilevel::setup (include/cedar/multilevel.h:243-265) on the device.
 int cdr_gpu_solver::setup()
 {
@@ -342,6 +392,7 @@ int cdr_gpu_settings_default(cdr_gpu_settings *s)
 	s->use_graph = 1;
 	s->line_flags = 0;
 	s->fuse_coarse = 32;
+	s->krylov = CDR_KRYLOV_NONE;
 	return CDR_OK;
 }
 
@@ -350,6 +401,8 @@ int cdr_gpu_solver_destroy(cdr_gpu_solver *h)
 	if (!h) return CDR_ERR_HANDLE;
 	if (h->st) cudaStreamSynchronize(h->st);
 	for (auto &g : h->gexec)
+		if (g) cudaGraphExecDestroy(g);
+	for (auto &g : h->kexec)
 		if (g) cudaGraphExecDestroy(g);
 	for (void *p : h->allocs) cudaFree(p);
 	if (h->h_norm) cudaFreeHost(h->h_norm);
@@ -437,6 +490,11 @@ static int create_impl(cdr_gpu_solver *h, const double *so_src, int ns, int nx, 
 		CDR_TRY(h->alloc(&h->x64[0], h->lv[0].d.plane()));
 		CDR_TRY(h->alloc(&h->x64[1], h->lv[0].d.plane()));
 	}
+	if (s.krylov == CDR_KRYLOV_FCG) {
+		const size_t pl = h->lv[0].d.plane();
+		for (double **p : {&h->kb, &h->kx[0], &h->kx[1], &h->kr, &h->kp[0], &h->kp[1], &h->kq}) CDR_TRY(h->alloc(p, pl));
+		CDR_TRY(h->alloc(&h->ks, 1));
+	}
 	CDR_CUDA_TRY(cudaMallocHost(&h->h_norm, 4 * sizeof(double)));
 	// fine operator (source pitch) -> device pitch, then the device setup
 	return load_and_setup(h, so_src, src_pitch, kind);
@@ -454,6 +512,10 @@ static int create_any(const cdr_gpu_settings *s, const double *so_src, int ns, i
 	}
 	if (s->precision != CDR_PREC_F64 && s->precision != CDR_PREC_F32_IR) {
 		set_error(CDR_ERR_ARG, "invalid precision %d", s->precision);
+		return CDR_ERR_ARG;
+	}
+	if (s->krylov != CDR_KRYLOV_NONE && s->krylov != CDR_KRYLOV_FCG) {
+		set_error(CDR_ERR_ARG, "invalid krylov %d", s->krylov);
 		return CDR_ERR_ARG;
 	}
 	*out = nullptr;
@@ -501,6 +563,45 @@ int cdr_gpu_solver_resetup_device(cdr_gpu_solver *h, const double *so_dev, int p
 	return load_and_setup(h, so_dev, pitch, cudaMemcpyDeviceToDevice);
 }
 
+// Flexible CG on the level-0 buffers (x in F.x, b in F.b on entry, x out in
+// F.x); the residual of every iteration is the true one, so the stopping test
+// is the reference's (|b - A x| / |b - A x0| < tol).
+static int solve_fcg(cdr_gpu_solver *h, int *iters, double *hist, int maxhist)
+{
+	Level &F = h->lv[0];
+	cudaStream_t st = h->st;
+	const int prec = h->mixed() ? 1 : 0;
+	const size_t bytes = sizeof(double) * F.d.plane();
+	CDR_CUDA_TRY(cudaMemcpyAsync(h->kb, F.b, bytes, cudaMemcpyDeviceToDevice, st));
+	CDR_CUDA_TRY(cudaMemcpyAsync(h->kx[0], F.x, bytes, cudaMemcpyDeviceToDevice, st));
+	CDR_TRY(residual_2d<double>(F.so, F.ns, h->kx[0], h->kb, h->kr, F.d, h->norm, h->partial, st));
+	CDR_CUDA_TRY(cudaMemcpyAsync(h->h_norm, h->norm, sizeof(double), cudaMemcpyDeviceToHost, st));
+	CDR_CUDA_TRY(cudaStreamSynchronize(st));
+	const double res0 = h->h_norm[0];
+	int it = 0;
+	if (res0 > 0) {
+		if (prec) CDR_TRY(fcg_load<float>(h->kr, F.b32, F.x32, F.d, h->ks, st));
+		else CDR_TRY(fcg_load<double>(h->kr, F.b, F.x, F.d, h->ks, st));
+		while (it < h->s.maxiter) {
+			CDR_TRY(h->run_fcg(prec));
+			CDR_CUDA_TRY(cudaMemcpyAsync(h->h_norm, &h->ks->rr, sizeof(double), cudaMemcpyDeviceToHost, st));
+			CDR_CUDA_TRY(cudaStreamSynchronize(st));
+			const double rel = std::sqrt(h->h_norm[0]) / res0;
+			if (hist && it < maxhist) hist[it] = rel;
+			++it;
+			if (!std::isfinite(rel)) {
+				set_error(CDR_ERR_NUMERIC, "non-finite residual norm at iteration %d", it - 1);
+				return CDR_ERR_NUMERIC;
+			}
+			if (rel < h->s.tol) break;
+		}
+	}
+	// iterate of step it is in kx[it & 1] (FcgScalars::iter counts the same steps)
+	CDR_CUDA_TRY(cudaMemcpyAsync(F.x, h->kx[it & 1], bytes, cudaMemcpyDeviceToDevice, st));
+	if (iters) *iters = it;
+	return CDR_OK;
+}
+
 // multilevel::solve (include/cedar/multilevel.h:278-298) on the level-0 buffers.
 static int solve_loaded(cdr_gpu_solver *h, int *iters, double *hist, int maxhist)
 {
@@ -509,7 +610,9 @@ static int solve_loaded(cdr_gpu_solver *h, int *iters, double *hist, int maxhist
 	double res0 = 0;
 	int it = 0;
 	CDR_CUDA_TRY(cudaEventRecord(h->ev0, st));
-	if (!h->mixed()) {
+	if (h->s.krylov == CDR_KRYLOV_FCG) {
+		CDR_TRY(solve_fcg(h, &it, hist, maxhist));
+	} else if (!h->mixed()) {
 		CDR_TRY(residual_2d<double>(F.so, F.ns, F.x, F.b, F.r, F.d, h->norm, h->partial, st));
 		CDR_CUDA_TRY(cudaMemcpyAsync(h->h_norm, h->norm, sizeof(double), cudaMemcpyDeviceToHost, st));
 		CDR_CUDA_TRY(cudaStreamSynchronize(st));

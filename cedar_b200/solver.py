@@ -43,6 +43,9 @@ def _settings(ms: MLSettings, dim=2):
     s.use_graph = 1 if ms.use_graph else 0
     s.line_flags = _lib.LINES_EXACT if ms.line_solve == "sequential" else 0
     s.fuse_coarse = ms.fuse_coarse
+    if ms.krylov != "none" and dim != 2:
+        raise NotImplementedError("gpu.krylov = %r: the Krylov outer iteration is 2D only" % ms.krylov)
+    s.krylov = _lib.KRYLOV[ms.krylov]
     return s
 
 

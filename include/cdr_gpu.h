@@ -55,6 +55,16 @@ extern "C" {
 #define CDR_PREC_F64    0  /* plain FP64 V-cycles: the drop-in path                    */
 #define CDR_PREC_F32_IR 1  /* FP32 V-cycle preconditioner in an FP64 refinement loop  */
 
+/* Outer iteration of the 2D solve (settings.krylov).  CDR_KRYLOV_NONE repeats
+ * the cycle (plain FP64) or the refinement step (FP32-IR), as the reference's
+ * solve loop does.  CDR_KRYLOV_FCG (no counterpart in the reference) uses the
+ * cycle, in the solve's precision, as the preconditioner of flexible conjugate
+ * gradients (Notay's FCG(1)) with FP64 recurrences; for a symmetric
+ * preconditioner choose nrelax_pre == nrelax_post.  The history holds the
+ * recurrence residual; the final entry is the true residual b - A x. */
+#define CDR_KRYLOV_NONE 0
+#define CDR_KRYLOV_FCG  1
+
 /* Line direction */
 #define CDR_DIR_X 0
 #define CDR_DIR_Y 1
@@ -225,6 +235,7 @@ typedef struct cdr_gpu_settings {
 	int use_graph;    /* replay the cycle as a CUDA graph (default 1)                  */
 	int line_flags;   /* CDR_LINES_EXACT for sequential line substitutions (default 0) */
 	int fuse_coarse;  /* levels with both edges <= this run as one fused kernel (default 32, 0 = off) */
+	int krylov;       /* CDR_KRYLOV_NONE (default) or CDR_KRYLOV_FCG; 2D solver only    */
 } cdr_gpu_settings;
 
 typedef struct cdr_gpu_solver cdr_gpu_solver;
