@@ -12,9 +12,9 @@ coefficients span ~12 orders of magnitude), and the reference's own outer loop
 (repeated V(2,1) cycles; the oracle reproduces it bit for bit) stalls near
 residual 1 besides, contracting the error by ~0.97 per cycle.  The headline
 therefore times flexible CG (FP64 recurrences, true residual every iteration)
-preconditioned by one line-xy V(1,1) cycle, FP32 cycle (value) against FP64
-cycle (fp64_ms), to --tol (default 1e-3, the tightest round tolerance both
-reach); `plain_vcycle` records the reference loop on the same problem and
+preconditioned by one line-xy V(1,1) cycle (six levels, the 64^2 coarsest solved
+with its explicit inverse), FP32 cycle (value) against FP64 cycle (fp64_ms), to
+--tol (default 1e-3, the tightest round tolerance both reach); `plain_vcycle` records the reference loop on the same problem and
 `to_1e-10` the 1e-10 solve on the same grid with a constant coefficient, where
 1e-10 is attainable and the reference loop converges.
 
@@ -204,15 +204,20 @@ def main():
     n = args.n
     pitch = ((n + 2 + 31) // 32) * 32
 
-    def mk(prec, krylov, npre, npost, tol, maxiter):
-        conf = Config({"solver": {"relaxation": "line-xy", "max-iter": maxiter, "tol": tol,
+    def mk(prec, krylov, npre, npost, tol, maxiter, levels=-1, coarse="banded"):
+        conf = Config({"solver": {"relaxation": "line-xy", "max-iter": maxiter, "tol": tol, "num-levels": levels,
                                   "cycle": {"nrelax-pre": npre, "nrelax-post": npost}},
-                       "gpu": {"precision": prec, "graph": True, "krylov": krylov}})
+                       "gpu": {"precision": prec, "graph": True, "krylov": krylov, "coarse-solve": coarse}})
         return Solver2D(so, conf, stream=sh)
 
-    # headline: flexible CG preconditioned by one line-xy V(1,1) cycle, FP32 cycle vs FP64 cycle
-    s32 = mk("fp32-ir", "fcg", 1, 1, args.tol, args.maxiter)
-    s64 = mk("fp64", "fcg", 1, 1, args.tol, args.maxiter)
+    # headline: flexible CG preconditioned by one line-xy V(1,1) cycle whose coarsest level is ~64^2,
+    # solved exactly with the inverse product; FP32 cycle vs FP64 cycle
+    nlev, m = 1, n
+    while m > 64:  # cdr2::solver's coarsening: (n - 1) / 2 + 1 per level
+        m = (m - 1) // 2 + 1
+        nlev += 1
+    s32 = mk("fp32-ir", "fcg", 1, 1, args.tol, args.maxiter, nlev, "inverse")
+    s64 = mk("fp64", "fcg", 1, 1, args.tol, args.maxiter, nlev, "inverse")
     setup32, _ = s32.timings()
     setup64, _ = s64.timings()
     with torch.cuda.stream(stream):
@@ -320,7 +325,8 @@ def main():
            "dtype": "f32 cycle + f64 outer iteration", "data": "synthetic",
            "config": {"workload": WORKLOAD, "n": n, "levels": s32.nlevels,
                       "solver": "flexible CG (FP64 recurrences, true residual every iteration) preconditioned by "
-                                "one line-xy V(1,1) cycle; FP32 cycle (value) vs FP64 cycle (fp64_ms)",
+                                "one line-xy V(1,1) cycle over %d levels (coarsest %d^2, solved with its explicit "
+                                "inverse); FP32 cycle (value) vs FP64 cycle (fp64_ms)" % (nlev, m),
                       "tol": args.tol,
                       "tol_note": "1e-10 is below this problem's FP64 rounding floor: eps*|A||x|/|b| = %.1e at "
                                   "the FP64 solution, and no solver's relative residual goes below ~5e-5 here "

@@ -17,8 +17,10 @@ RELAX = {"point": 0, "line-x": 1, "line-y": 2, "line-xy": 3,
          "plane-xy": 4, "plane-xz": 5, "plane-yz": 6, "plane-xyz": 7}
 PREC = {"fp64": 0, "fp32-ir": 1}
 KRYLOV = {"none": 0, "fcg": 1}
+COARSE = {"banded": 0, "inverse": 1}
 DIR_X, DIR_Y = 0, 1
 LINES_EXACT = 1
+LINES_NOTUNE = 2
 
 _lib = None
 
@@ -36,7 +38,7 @@ class Settings(ctypes.Structure):
                 ("maxiter", ctypes.c_int), ("tol", ctypes.c_double),
                 ("min_coarse", ctypes.c_int), ("precision", ctypes.c_int),
                 ("use_graph", ctypes.c_int), ("line_flags", ctypes.c_int), ("fuse_coarse", ctypes.c_int),
-                ("krylov", ctypes.c_int)]
+                ("krylov", ctypes.c_int), ("coarse_solve", ctypes.c_int)]
 
 
 def header_symbols():
@@ -61,6 +63,7 @@ def load(path=LIB_PATH):
         "cdr_gpu_last_error": (ctypes.c_char_p, []),
         "cdr_gpu_version": (I, []),
         "cdr_gpu_launch_count": (ctypes.c_longlong, []),
+        "cdr_gpu_lines_shape": (I, [I, I, I, I, I, I, ctypes.POINTER(I), ctypes.POINTER(I)]),
         "cdr_gpu_norm_scratch_bytes": (Z, []),
         "cdr_gpu_settings_default": (I, [ctypes.POINTER(Settings)]),
         "cdr_gpu_solver_create_2d": (I, [ctypes.POINTER(Settings), P, I, I, I, S, ctypes.POINTER(P)]),

@@ -7,8 +7,11 @@ note that the reference reads ``solver.min_coarse`` (underscore), so the
 GPU options live under the ``"gpu"`` object: ``precision`` ("fp64" | "fp32-ir"),
 ``graph`` (bool), ``fuse-coarse`` (levels with both edges at most this many
 points run as one fused kernel; 0 = off; default 32), ``line-solve`` ("scan": parallel line substitutions, the
-default; "sequential": DPTTRS order, bit-identical to the reference) and ``krylov`` ("none": the reference's
-outer loop, the default; "fcg": the cycle preconditions flexible conjugate gradients, 2D only).
+default; "sequential": DPTTRS order, bit-identical to the reference), ``autotune`` (bool, default true: time
+the line kernels' launch shapes per level at setup, once per shape and process), ``krylov`` ("none": the
+reference's outer loop, the default; "fcg": the cycle preconditions flexible conjugate gradients, 2D only) and
+``coarse-solve`` ("banded": the reference's DPBTRS, the default; "inverse": the setup forms the coarsest
+operator's inverse and every cycle multiplies by it, 2D only — for a coarsest level of thousands of unknowns).
 """
 import json
 import os
@@ -77,9 +80,13 @@ class MLSettings:
         self.fuse_coarse = int(conf.get("gpu.fuse-coarse", 32))
         if self.fuse_coarse < 0:
             raise ValueError("invalid gpu.fuse-coarse: %d" % self.fuse_coarse)
+        self.autotune = bool(conf.get("gpu.autotune", True))
         self.krylov = conf.get("gpu.krylov", "none")
         if self.krylov not in ("none", "fcg"):
             raise ValueError("invalid gpu.krylov: %s" % self.krylov)
+        self.coarse_solve = conf.get("gpu.coarse-solve", "banded")
+        if self.coarse_solve not in ("banded", "inverse"):
+            raise ValueError("invalid gpu.coarse-solve: %s" % self.coarse_solve)
 
     def __repr__(self):
         return ("MLSettings(relaxation=%r, cycle=%r, nrelax=(%d,%d), num_levels=%d, maxiter=%d, "

@@ -156,6 +156,32 @@ int Batch2::setup(bool check)
 	return check ? check_info() : CDR_OK;
 }
 
+// Launch shapes of the line kernels on every non-fused smoothing level, timed
+// on all problems at once (the level arrays are the cycle's scratch; level 0 is
+// reloaded by each solve)
+template <typename T>
+int Batch2::tune_lines()
+{
+	if (s.line_flags & CDR_LINES_NOTUNE) return CDR_OK;
+	if (sizeof(T) == 8 && (s.line_flags & CDR_LINES_EXACT)) return CDR_OK;
+	const int r = s.relaxation;
+	const bool lx = r == CDR_RELAX_LINE_X || r == CDR_RELAX_LINE_XY, ly = r == CDR_RELAX_LINE_Y || r == CDR_RELAX_LINE_XY;
+	const int f = lc[sizeof(T) == 4 ? 1 : 0];
+	const int stop = f >= 0 ? f : L() - 1;
+	const Sel all{0, 1, nb};
+	for (int l = 0; l < stop; ++l) {
+		B2Level &F = lv[l];
+		const Dims2 d = F.dims(all);
+		if (lx)
+			CDR_TRY(lines_autotune<T>(BA<T>::so(F), F.ns, BA<T>::x(F), BA<T>::b(F), BA<T>::sor(F), d, F.tpitch, CDR_DIR_X,
+			                          st));
+		if (ly)
+			CDR_TRY(lines_autotune<T>(BA<T>::so(F), F.ns, BA<T>::x(F), BA<T>::b(F), BA<T>::sory(F), d, F.tpitch,
+			                          CDR_DIR_Y, st));
+	}
+	return CDR_OK;
+}
+
 int Batch2::check_info()
 {
 	int h[2] = {0, 0};
@@ -184,7 +210,7 @@ int Batch2::smooth(int l, Sel sel, int updown)
 	const T *b = BA<T>::b(F) + f * pl;
 	const T *sx = BA<T>::sor(F) ? BA<T>::sor(F) + f * 2 * pl : nullptr;
 	const T *sy = BA<T>::sory(F) ? BA<T>::sory(F) + f * F.ysize() : nullptr;
-	const int flags = sizeof(T) == 8 ? s.line_flags : 0;
+	const int flags = sizeof(T) == 8 ? s.line_flags : (s.line_flags & CDR_LINES_NOTUNE);
 	const int n = updown == CDR_DOWN ? s.nrelax_pre : s.nrelax_post;
 	for (int it = 0; it < n; ++it) {
 		switch (s.relaxation) {
@@ -412,7 +438,7 @@ int cdr_gpu_batch2d_create(const cdr_gpu_settings *s, const double *so_dev, int 
 		set_error(CDR_ERR_ARG, "invalid precision %d", s->precision);
 		return CDR_ERR_ARG;
 	}
-	if (s->krylov != CDR_KRYLOV_NONE) {
+	if (s->krylov != CDR_KRYLOV_NONE || s->coarse_solve != CDR_COARSE_BANDED) {
 		set_error(CDR_ERR_UNSUPPORTED, "batched 2D solves: the Krylov outer iteration is implemented for the 2D solver only");
 		return CDR_ERR_UNSUPPORTED;
 	}
@@ -467,6 +493,8 @@ int cdr_gpu_batch2d_create(const cdr_gpu_settings *s, const double *so_dev, int 
 		set_error(CDR_ERR_CUDA, "setup timing events failed");
 		return fail(CDR_ERR_CUDA);
 	}
+	rc = h->B.tune();
+	if (rc != CDR_OK) return fail(rc);
 	*out = h;
 	return CDR_OK;
 }

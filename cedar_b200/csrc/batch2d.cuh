@@ -55,6 +55,9 @@ public:
 	// multilevel::setup (include/cedar/multilevel.h:243-265) for all problems;
 	// checks the factorizations (synchronises the stream) when check is set.
 	int setup(bool check);
+	// Times the line kernels' launch shapes of every smoothing level (once per
+	// shape and process); runs sweeps on the level arrays.
+	int tune() { return mixed() ? tune_lines<float>() : tune_lines<double>(); }
 	int check_info();
 	// One V-cycle of the selected problems on their level-0 x and b
 	// (cycle::vcycle::ncycle_helper, include/cedar/cycle/vcycle.h:57-115).
@@ -77,6 +80,8 @@ private:
 	int fused(int l0, Sel sel);
 	template <typename T>
 	int pick_fused();
+	template <typename T>
+	int tune_lines();
 };
 
 // cdr2::solver::compute_num_levels (include/cedar/2d/solver.h:63-79)

@@ -70,6 +70,18 @@ int cdr_gpu_version(void) { return 100; }
 long long cdr_gpu_launch_count(void) { return g_launches.load(); }
 size_t cdr_gpu_norm_scratch_bytes(void) { return kNormScratchBytes; }
 
+int cdr_gpu_lines_shape(int dir, int fp32, int nstencil, int n, int nlines, int batch, int *K, int *cap)
+{
+	LineShape sh;
+	if (!lines_shape(dir, fp32 ? 4 : 8, nstencil, n, nlines, batch ? 2 : 1, &sh)) {
+		set_error(CDR_ERR_ARG, "no tuned line shape for n=%d lines=%d", n, nlines);
+		return CDR_ERR_ARG;
+	}
+	if (K) *K = sh.K;
+	if (cap) *cap = sh.cap;
+	return CDR_OK;
+}
+
 #define RESID_IMPL(T, SUF)                                                                                      \
 	int cdr_gpu_residual_2d_##SUF(const T *so, int ns, const T *x, const T *b, T *r, int nx, int ny, int pitch,  \
 	                              double *norm_out, void *scratch, cudaStream_t s)                              \

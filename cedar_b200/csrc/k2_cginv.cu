@@ -1,0 +1,132 @@
+// k2_cginv.cu -- the coarsest 2D solve as a product with the explicit inverse.
+//
+// The reference solves the coarsest level with the banded Cholesky factor of
+// BMG2_SymStd_SETUP_cg_LU (DPBTRS: two triangular sweeps over n unknowns with
+// bandwidth nx+1, src/2d/ftn/BMG2_SymStd_SOLVE_cg.f90).  On the GPU those sweeps
+// are one sequential chain; for a coarsest level of a few thousand unknowns
+// (e.g. 63^2, selected with solver.num-levels) it costs about a millisecond.
+// With settings.coarse_solve = CDR_COARSE_INVERSE the setup instead forms
+// A^{-1} from the same factor (one column per thread, both sweeps per column,
+// FP64) and each cycle applies it as a matrix-vector product (memory bound,
+// ~n^2 words per solve).  The result equals DPBTRS's to rounding, not bitwise.
+#include "k2_point.cuh"
+#include "kernels2d.cuh"
+
+namespace cdrgpu {
+
+namespace {
+
+// Column c of A^{-1} = U^{-1} U^{-T} e_c by the two sweeps of DPBTRS ('U'
+// band storage, U(i, j) at ab[j*ldab + kd + i - j]), one column per thread, 32
+// columns per CTA, the warp walking j in step so that every lane uses the same
+// factor column, which is staged in shared memory one step ahead.  Forward:
+// y(j) = (e_c(j) - sum_i U(i, j) y(i)) / U(j, j); backward (DTBSV's column
+// form): x(j) = y(j) / U(j, j), then y(i) -= x(j) U(i, j) for the kd rows
+// above.  The active window of each column lives in a shared-memory ring; y is
+// parked in ainv[j*n + c] (row c of the symmetric inverse, 32 consecutive words
+// per warp) and overwritten by x.
+constexpr int CGI_RING = 128;  // ring slots per column (>= kd + 2)
+
+__global__ void __launch_bounds__(32) k_cg_inverse(const double *__restrict__ ab, int n, int kd, int ldab,
+                                                   double *__restrict__ ainv)
+{
+	__shared__ double ring[CGI_RING][32];
+	__shared__ double ucol[2][CGI_RING];
+	const int lane = threadIdx.x, c0 = blockIdx.x * 32, c = c0 + lane;
+	const bool on = c < n;
+	constexpr int M = CGI_RING - 1;
+	for (int j = 0; j < CGI_RING; ++j) ring[j][lane] = 0.0;
+	auto stage = [&](int j, int buf) {
+		for (int e = lane; e <= kd; e += 32) ucol[buf][e] = ab[(size_t)j * ldab + e];
+	};
+	stage(c0, 0);
+	__syncwarp();
+	// forward from the warp's first column; y(j) = 0 for j < c
+	for (int j = c0; j < n; ++j) {
+		const int buf = (j - c0) & 1;
+		if (j + 1 < n) stage(j + 1, buf ^ 1);
+		double t = j == c ? 1.0 : 0.0;
+		if (on && j > c) {
+			const int i0 = j - kd > c ? j - kd : c;
+			const double *col = ucol[buf] + kd - j;
+			for (int i = i0; i < j; ++i) t -= col[i] * ring[i & M][lane];
+		}
+		const double y = (on && j >= c) ? t / ucol[buf][kd] : 0.0;
+		ring[j & M][lane] = y;
+		if (on) ainv[(size_t)j * n + c] = y;
+		__syncwarp();
+	}
+	if (on)
+		for (int j = 0; j < c0 && j < n; ++j) ainv[(size_t)j * n + c] = 0.0;  // y below the warp's first column
+	// backward; the ring holds y (being updated) for rows (j - kd - 1, j]
+	stage(n - 1, 0);
+	__syncwarp();
+	for (int j = n - 1; j >= 0; --j) {
+		const int buf = (n - 1 - j) & 1;
+		if (j > 0) stage(j - 1, buf ^ 1);
+		// y(j - 1 - kd) enters the window for the next step (untouched by the backward sweep so far)
+		const int e = j - 1 - kd;
+		const double yin = (on && e >= 0) ? ainv[(size_t)e * n + c] : 0.0;
+		const double x = ring[j & M][lane] / ucol[buf][kd];
+		if (on) ainv[(size_t)j * n + c] = x;
+		const int i0 = j - kd > 0 ? j - kd : 0;
+		const double *col = ucol[buf] + kd - j;
+		for (int i = i0; i < j; ++i) ring[i & M][lane] -= x * col[i];
+		if (e >= 0) ring[e & M][lane] = yin;
+		__syncwarp();
+	}
+}
+
+// x(interior) = A^{-1} b(interior): b compacted into shared memory, one warp
+// per row, FP64 accumulation
+template <typename T>
+__global__ void __launch_bounds__(256) k_cg_inv_apply(const T *__restrict__ ainv, T *__restrict__ q,
+                                                      const T *__restrict__ qf, Dims2 d)
+{
+	extern __shared__ double bs[];
+	const int n = d.nx * d.ny;
+	for (int e = threadIdx.x; e < n; e += blockDim.x) bs[e] = (double)qf[d.at(e % d.nx + 1, e / d.nx + 1)];
+	__syncthreads();
+	const int lane = threadIdx.x & 31;
+	const int warps = gridDim.x * (blockDim.x >> 5);
+	for (int r = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); r < n; r += warps) {
+		const T *row = ainv + (size_t)r * n;
+		double a = 0.0;
+		for (int j = lane; j < n; j += 32) a += (double)row[j] * bs[j];
+		for (int o = 16; o > 0; o >>= 1) a += __shfl_down_sync(0xffffffffu, a, o);
+		if (lane == 0) q[d.at(r % d.nx + 1, r / d.nx + 1)] = (T)a;
+	}
+}
+
+}  // namespace
+
+int cg_inverse_2d(const double *abd, Dims2 d, double *ainv, cudaStream_t st)
+{
+	const int n = d.nx * d.ny, kd = d.nx + 1, ldab = d.nx + 2;
+	if (kd + 2 > CGI_RING) {
+		set_error(CDR_ERR_DIM, "coarsest grid %dx%d too wide for the inverse (bandwidth %d)", d.nx, d.ny, kd);
+		return CDR_ERR_DIM;
+	}
+	k_cg_inverse<<<ceil_div(n, 32), 32, 0, st>>>(abd, n, kd, ldab, ainv);
+	CDR_LAUNCH_CHECK();
+	return CDR_OK;
+}
+
+template <typename T>
+int solve_cg_inv_2d(const T *ainv, T *x, const T *b, Dims2 d, cudaStream_t st)
+{
+	const int n = d.nx * d.ny;
+	const size_t sm = sizeof(double) * (size_t)n;
+	if (sm > 48 * 1024) {
+		set_error(CDR_ERR_DIM, "coarsest grid %dx%d too large for the inverse product", d.nx, d.ny);
+		return CDR_ERR_DIM;
+	}
+	const int rows_per_cta = 256 / 32, grid = ceil_div(n, rows_per_cta) < 148 * 4 ? ceil_div(n, rows_per_cta) : 148 * 4;
+	k_cg_inv_apply<T><<<grid, 256, sm, st>>>(ainv, x, b, d);
+	CDR_LAUNCH_CHECK();
+	return CDR_OK;
+}
+template int solve_cg_inv_2d<double>(const double *, double *, const double *, Dims2, cudaStream_t);
+template int solve_cg_inv_2d<float>(const float *, float *, const float *, Dims2, cudaStream_t);
+
+}  // namespace cdrgpu

@@ -8,18 +8,16 @@
 // zero coarse iterate, ..., banded Cholesky, ..., interpolate-add,
 // post-smoothing) with one CTA per problem and a barrier between steps.  Every
 // point formula is the shared helper the separate kernels use (k2_point.cuh),
-// and the line solves run DPTTS2's sequential substitutions on rows staged in
-// shared memory (as the exact line kernels do), so the result is the one the
-// separate kernels give in CDR_LINES_EXACT mode.
+// and in FP64 the line solves run DPTTS2's sequential substitutions, so the
+// result is the one the separate kernels give in CDR_LINES_EXACT mode.
 //
-// Each level visit copies the level's operator, smoother factors, b, x and r
-// into shared memory (compact rows), runs every smoothing phase there and
-// writes x and r back: the barrier-separated phases then wait on shared memory
-// instead of L2 (a first version that worked on L2 took 508 us per cycle for
-// levels 64^2 .. 4^2, against ~300 us for the separate launches).  Levels of at
-// most 32^2 are fused by default: FP32+IR and FP64 solves of the 2047^2 line-xy
-// problem are 4-5 % faster than with separate launches; fusing from 64^2 is
-// slower in FP32 (its 64-point sequential line solves dominate).
+// All levels of the sub-cycle live in shared memory for the whole launch (with
+// compact rows): the operators, smoother factors and interpolation weights are
+// staged once at entry, b of the first level is read and its x written back at
+// exit, and nothing else touches global memory.  Loops map rows to warps and
+// positions to lanes (no per-element division).  Levels of at most 32^2 are
+// fused by default (the levels of the 2047^2 hierarchy below 63^2 need 83 KB in
+// FP32, 166 KB in FP64; from 63^2 on they would not fit).
 #include <algorithm>
 
 #include "k2_point.cuh"
@@ -28,17 +26,123 @@
 namespace cdrgpu {
 
 constexpr int CC_THREADS = 1024;
+constexpr int CC_WARPS = CC_THREADS / 32;
+
+// f(i, j) for i in [i0, i1], j in [j0, j1]: rows over the warps, positions over the lanes
+template <typename F>
+__device__ __forceinline__ void cc_rows(int i0, int i1, int j0, int j1, F f)
+{
+	const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+	for (int j = j0 + warp; j <= j1; j += CC_WARPS)
+		for (int i = i0 + lane; i <= i1; i += 32) f(i, j);
+}
+
+// Planes of smoother factors kept for a relaxation type
+__host__ __device__ inline int cc_sor_planes(int relax)
+{
+	return relax == CDR_RELAX_POINT ? 1 : relax == CDR_RELAX_LINE_Y ? 0 : 2;
+}
+__host__ __device__ inline int cc_sory_planes(int relax)
+{
+	return relax == CDR_RELAX_LINE_Y || relax == CDR_RELAX_LINE_XY ? 2 : 0;
+}
+
+// Elements of level l's shared copy (rows of nx+2): operator, factors, b, x, r
+// (the coarsest keeps b and x only) and the interpolation weights of every
+// level but the first.
+template <typename T>
+__host__ __device__ inline size_t cc_elems(const CoarseCycle<T> &cc, int l)
+{
+	const CoarseLevel<T> &L = cc.lv[l];
+	const size_t pl = (size_t)(L.nx + 2) * (L.ny + 2);
+	size_t planes = l == cc.nl - 1 ? 2 : L.ns + cc_sor_planes(cc.relax) + cc_sory_planes(cc.relax) + 3;
+	if (l > 0) planes += 8;
+	return planes * pl;
+}
+
+// Global arrays of problem blockIdx.x of a batch: every array of every level
+// moves by that problem's offset (problems back to back, problem step bstep).
+template <typename T>
+__device__ CoarseLevel<T> cc_global(const CoarseCycle<T> &cc, int l)
+{
+	CoarseLevel<T> L = cc.lv[l];
+	const size_t p = (size_t)blockIdx.x * cc.bstep, pl = (size_t)L.pitch * (L.ny + 2);
+	L.so += p * L.ns * pl;
+	L.x += p * pl;
+	L.b += p * pl;
+	L.r += p * pl;
+	if (L.sor) L.sor += p * 2 * pl;
+	if (L.sory) L.sory += p * 2 * (size_t)L.tpitch * (L.nx + 2);
+	if (L.ci) L.ci += p * 8 * pl;
+	return L;
+}
+
+// Shared copy of level l (compact rows: pitch nx+2, y-line factors tpitch ny+2)
+template <typename T>
+__device__ CoarseLevel<T> cc_view(const CoarseCycle<T> &cc, int l, T *base)
+{
+	size_t off = 0;
+	for (int m = 0; m < l; ++m) off += cc_elems(cc, m);
+	const CoarseLevel<T> &G = cc.lv[l];
+	CoarseLevel<T> S = G;
+	S.pitch = G.nx + 2;
+	S.tpitch = G.ny + 2;
+	const size_t pl = (size_t)(G.nx + 2) * (G.ny + 2);
+	T *p = base + off;
+	if (l < cc.nl - 1) {
+		S.so = p;
+		p += G.ns * pl;
+		const int ns1 = cc_sor_planes(cc.relax), ns2 = cc_sory_planes(cc.relax);
+		S.sor = ns1 ? p : nullptr;
+		p += ns1 * pl;
+		S.sory = ns2 ? p : nullptr;
+		p += ns2 * pl;
+	} else {
+		S.so = S.sor = S.sory = nullptr;
+	}
+	S.b = p;
+	p += pl;
+	S.x = p;
+	p += pl;
+	if (l < cc.nl - 1) {
+		S.r = p;
+		p += pl;
+	} else {
+		S.r = nullptr;
+	}
+	S.ci = l > 0 ? p : nullptr;
+	return S;
+}
+
+// copy nplanes planes of `rows` rows of rowlen elements between pitches
+template <typename T>
+__device__ void cc_copy(const T *__restrict__ src, int sp, size_t splane, T *__restrict__ dst, int dp, size_t dplane,
+                        int rowlen, int rows, int nplanes)
+{
+	const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+	for (int row = warp; row < rows * nplanes; row += CC_WARPS) {
+		const int q = row / rows, j = row - q * rows;
+		const T *s = src + (size_t)q * splane + (size_t)j * sp;
+		T *d = dst + (size_t)q * dplane + (size_t)j * dp;
+		for (int i = lane; i < rowlen; i += 32) d[i] = s[i];
+	}
+}
+
+template <typename T>
+__device__ void cc_fill(T *p, size_t n)
+{
+	for (size_t e = threadIdx.x; e < n; e += CC_THREADS) p[e] = T(0);
+}
 
 // r = b - A x on the level (all interior points)
 template <typename T, int NS>
 __device__ void cc_residual(const CoarseLevel<T> &L)
 {
-	const Dims2 d{L.nx, L.ny, L.pitch};
-	const int n = L.nx * L.ny;
-	for (int e = threadIdx.x; e < n; e += CC_THREADS) {
-		const size_t k = d.at(e % L.nx + 1, e / L.nx + 1);
-		L.r[k] = resid_at<T, NS>(L.so, d.plane(), L.x, L.b, k, L.pitch);
-	}
+	const size_t ps = (size_t)L.pitch * (L.ny + 2);
+	cc_rows(1, L.nx, 1, L.ny, [&](int i, int j) {
+		const size_t k = (size_t)j * L.pitch + i;
+		L.r[k] = resid_at<T, NS>(L.so, ps, L.x, L.b, k, L.pitch);
+	});
 }
 
 // coarse b = P^T r_fine
@@ -46,8 +150,7 @@ template <typename T>
 __device__ void cc_restrict(const CoarseLevel<T> &F, const CoarseLevel<T> &C)
 {
 	const Dims2 f{F.nx, F.ny, F.pitch}, c{C.nx, C.ny, C.pitch};
-	const int n = C.nx * C.ny;
-	for (int e = threadIdx.x; e < n; e += CC_THREADS) restrict_at<T>(C.ci, F.r, C.b, f, c, e % C.nx + 1, e / C.nx + 1);
+	cc_rows(1, C.nx, 1, C.ny, [&](int ic, int jc) { restrict_at<T>(C.ci, F.r, C.b, f, c, ic, jc); });
 }
 
 // x_fine += P x_coarse + r/c on the fine-only points
@@ -55,43 +158,31 @@ template <typename T>
 __device__ void cc_interp(const CoarseLevel<T> &F, const CoarseLevel<T> &C)
 {
 	const Dims2 f{F.nx, F.ny, F.pitch}, c{C.nx, C.ny, C.pitch};
-	const int mx = F.nx / 2 + 1, n = mx * (F.ny / 2 + 1);
-	for (int e = threadIdx.x; e < n; e += CC_THREADS) interp_at<T>(C.ci, C.x, F.r, F.so, F.x, f, c, e % mx + 1, e / mx + 1);
+	cc_rows(1, F.nx / 2 + 1, 1, F.ny / 2 + 1, [&](int ic, int jc) { interp_at<T>(C.ci, C.x, F.r, F.so, F.x, f, c, ic, jc); });
 }
 
-// the whole coarse iterate, ghosts included, to zero (the cycle's memset)
-template <typename T>
-__device__ void cc_zero(const CoarseLevel<T> &L)
-{
-	const size_t n = (size_t)L.pitch * (L.ny + 2);
-	for (size_t e = threadIdx.x; e < n; e += CC_THREADS) L.x[e] = T(0);
-}
-
-// one Gauss-Seidel sweep, colours in relax_point_2d's order
 template <typename T, int NS>
 __device__ void cc_gs(const CoarseLevel<T> &L, int updown)
 {
-	const Dims2 d{L.nx, L.ny, L.pitch};
-	const size_t ps = d.plane();
+	const size_t ps = (size_t)L.pitch * (L.ny + 2);
 	if (NS == 5) {
 		const int order[4][2] = {{1, 1}, {1, 0}, {0, 1}, {0, 0}};  // (j odd?, i odd?)
-		const int mx = (L.nx + 1) / 2, my = (L.ny + 1) / 2;
 		for (int c = 0; c < 4; ++c) {
 			const int o = updown == CDR_DOWN ? c : 3 - c;
-			for (int e = threadIdx.x; e < mx * my; e += CC_THREADS) {
-				const int i = (order[o][1] ? 1 : 2) + 2 * (e % mx), j = (order[o][0] ? 1 : 2) + 2 * (e / mx);
-				if (i <= L.nx && j <= L.ny) gs_at<T, 5>(L.so, ps, L.x, L.b, L.sor, d.at(i, j), L.pitch);
-			}
+			const int i0 = order[o][1] ? 1 : 2, j0 = order[o][0] ? 1 : 2;
+			cc_rows(0, (L.nx - i0) / 2, 0, (L.ny - j0) / 2, [&](int a, int b) {
+				gs_at<T, 5>(L.so, ps, L.x, L.b, L.sor, (size_t)(j0 + 2 * b) * L.pitch + i0 + 2 * a, L.pitch);
+			});
 			__syncthreads();
 		}
 	} else {
-		const int mx = (L.nx + 1) / 2;
 		for (int c = 0; c < 2; ++c) {
 			const int par = updown == CDR_DOWN ? c : 1 - c;
-			for (int e = threadIdx.x; e < mx * L.ny; e += CC_THREADS) {
-				const int j = e / mx + 1;
-				const int i = (((1 + j) & 1) == par ? 1 : 2) + 2 * (e % mx);
-				if (i <= L.nx) gs_at<T, 3>(L.so, ps, L.x, L.b, L.sor, d.at(i, j), L.pitch);
+			const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+			for (int j = 1 + warp; j <= L.ny; j += CC_WARPS) {
+				const int i0 = ((1 + j) & 1) == par ? 1 : 2;
+				for (int i = i0 + 2 * lane; i <= L.nx; i += 64)
+					gs_at<T, 3>(L.so, ps, L.x, L.b, L.sor, (size_t)j * L.pitch + i, L.pitch);
 			}
 			__syncthreads();
 		}
@@ -118,11 +209,15 @@ __device__ void cc_lines(const CoarseLevel<T> &L, int updown, T *sm)
 		const int first = firsts[c];
 		const int ml = first > nl ? 0 : (nl - first) / 2 + 1;  // lines of this colour
 		T *R = sm;
-		for (int e = threadIdx.x; e < ml * n; e += CC_THREADS) {
-			const int g = e / n, m = e - g * n, lc = first + 2 * g;
-			const size_t k = DIR == CDR_DIR_X ? d.at(m + 1, lc) : d.at(lc, m + 1);
-			R[e] = line_rhs<T, NS, DIR>(L.so, ps, L.x, L.b, k, L.pitch);
-		}
+		// rows over warps, lanes along the rows of the level (lines for y, positions for x)
+		if (DIR == CDR_DIR_X)
+			cc_rows(0, n - 1, 0, ml - 1, [&](int m, int g) {
+				R[g * n + m] = line_rhs<T, NS, DIR>(L.so, ps, L.x, L.b, d.at(m + 1, first + 2 * g), L.pitch);
+			});
+		else
+			cc_rows(0, ml - 1, 0, n - 1, [&](int g, int m) {
+				R[g * n + m] = line_rhs<T, NS, DIR>(L.so, ps, L.x, L.b, d.at(first + 2 * g, m + 1), L.pitch);
+			});
 		__syncthreads();
 		if constexpr (sizeof(T) == 8) {
 			// FP64: DPTTS2's sequential substitutions, one thread per line
@@ -195,10 +290,10 @@ __device__ void cc_lines(const CoarseLevel<T> &L, int updown, T *sm)
 			}
 		}
 		__syncthreads();
-		for (int e = threadIdx.x; e < ml * n; e += CC_THREADS) {
-			const int g = e / n, m = e - g * n, lc = first + 2 * g;
-			L.x[DIR == CDR_DIR_X ? d.at(m + 1, lc) : d.at(lc, m + 1)] = R[e];
-		}
+		if (DIR == CDR_DIR_X)
+			cc_rows(0, n - 1, 0, ml - 1, [&](int m, int g) { L.x[d.at(m + 1, first + 2 * g)] = R[g * n + m]; });
+		else
+			cc_rows(0, ml - 1, 0, n - 1, [&](int g, int m) { L.x[d.at(first + 2 * g, m + 1)] = R[g * n + m]; });
 		__syncthreads();
 	}
 }
@@ -225,16 +320,15 @@ __device__ void cc_smooth(const CoarseCycle<T> &cc, const CoarseLevel<T> &L, int
 }
 
 // BMG2_SymStd_SOLVE_cg with DPBTRS('U') on the coarsest level: the factor and
-// the right-hand side staged in shared memory, substitutions by one thread
-// (k_cg_solve's operations)
+// the right-hand side staged in shared memory (xs, then the factor), the
+// substitutions by one thread (k_cg_solve's operations)
 template <typename T>
 __device__ void cc_cg(const double *__restrict__ ab, const CoarseLevel<T> &L, double *xs)
 {
-	const Dims2 d{L.nx, L.ny, L.pitch};
 	const int ldab = L.nx + 2, kd = L.nx + 1, n = L.nx * L.ny;
 	double *abs = xs + n;
 	for (int e = threadIdx.x; e < ldab * n; e += CC_THREADS) abs[e] = ab[e];
-	for (int e = threadIdx.x; e < n; e += CC_THREADS) xs[e] = (double)L.b[d.at(e % L.nx + 1, e / L.nx + 1)];
+	cc_rows(1, L.nx, 1, L.ny, [&](int i, int j) { xs[(j - 1) * L.nx + i - 1] = (double)L.b[(size_t)j * L.pitch + i]; });
 	__syncthreads();
 	if (threadIdx.x == 0) {
 		for (int j = 0; j < n; ++j) {
@@ -253,158 +347,105 @@ __device__ void cc_cg(const double *__restrict__ ab, const CoarseLevel<T> &L, do
 		}
 	}
 	__syncthreads();
-	for (int e = threadIdx.x; e < n; e += CC_THREADS) L.x[d.at(e % L.nx + 1, e / L.nx + 1)] = (T)xs[e];
+	cc_rows(1, L.nx, 1, L.ny, [&](int i, int j) { L.x[(size_t)j * L.pitch + i] = (T)xs[(j - 1) * L.nx + i - 1]; });
 }
 
-// Problem blockIdx.x of a batch: every array of every level moves by that
-// problem's offset (problems back to back, problem step bstep).
+// Shared-memory map: the levels' copies (cc_view), the line right-hand sides,
+// then (8-byte aligned) the coarsest solve's vector and factor in FP64.
 template <typename T>
-__device__ CoarseLevel<T> cc_level(const CoarseCycle<T> &cc, int l)
+__host__ __device__ inline void cc_layout(const CoarseCycle<T> &cc, size_t *levels, size_t *lines, size_t *dbl)
 {
-	CoarseLevel<T> L = cc.lv[l];
-	const size_t p = (size_t)blockIdx.x * cc.bstep, pl = (size_t)L.pitch * (L.ny + 2);
-	L.so += p * L.ns * pl;
-	L.x += p * pl;
-	L.b += p * pl;
-	L.r += p * pl;
-	if (L.sor) L.sor += p * 2 * pl;
-	if (L.sory) L.sory += p * 2 * (size_t)L.tpitch * (L.nx + 2);
-	if (L.ci) L.ci += p * 8 * pl;
-	return L;
-}
-
-// Shared-memory copy of a level for one visit: its operator, smoother factors,
-// b, x and r with compact rows (pitch nx+2; y-line factors tpitch ny+2).
-template <typename T>
-__device__ CoarseLevel<T> cc_view(const CoarseLevel<T> &G, int relax, T *base)
-{
-	CoarseLevel<T> S = G;
-	S.pitch = G.nx + 2;
-	S.tpitch = G.ny + 2;
-	const size_t pl = (size_t)(G.nx + 2) * (G.ny + 2);
-	T *p = base;
-	S.so = p;
-	p += G.ns * pl;
-	if (relax == CDR_RELAX_POINT) { S.sor = p; p += pl; }
-	else if (relax != CDR_RELAX_LINE_Y) { S.sor = p; p += 2 * pl; }
-	else S.sor = nullptr;
-	if (relax == CDR_RELAX_LINE_Y || relax == CDR_RELAX_LINE_XY) { S.sory = p; p += 2 * pl; }
-	else S.sory = nullptr;
-	S.b = p; p += pl;
-	S.x = p; p += pl;
-	S.r = p;
-	S.ci = nullptr;
-	return S;
-}
-
-// copy nplanes planes of (ny+2) rows of nx+2 elements between pitches
-template <typename T>
-__device__ void cc_copy(const T *__restrict__ src, int sp, size_t splane, T *__restrict__ dst, int dp, size_t dplane,
-                        int rowlen, int rows, int nplanes)
-{
-	const int per = rowlen * rows;
-	for (int e = threadIdx.x; e < per * nplanes; e += CC_THREADS) {
-		const int q = e / per, rem = e - q * per, j = rem / rowlen, i = rem - j * rowlen;
-		dst[(size_t)q * dplane + (size_t)j * dp + i] = src[(size_t)q * splane + (size_t)j * sp + i];
+	size_t lv = 0, ln = 0;
+	for (int l = 0; l < cc.nl; ++l) {
+		lv += cc_elems(cc, l);
+		if (l + 1 < cc.nl) {
+			const CoarseLevel<T> &L = cc.lv[l];
+			const size_t a = (size_t)((L.ny + 1) / 2) * L.nx, b = (size_t)((L.nx + 1) / 2) * L.ny;
+			ln = ln > a ? ln : a;
+			ln = ln > b ? ln : b;
+		}
 	}
-}
-
-template <typename T>
-__device__ void cc_stage(const CoarseLevel<T> &G, const CoarseLevel<T> &S, int relax, bool with_r)
-{
-	const size_t gpl = (size_t)G.pitch * (G.ny + 2), spl = (size_t)S.pitch * (S.ny + 2);
-	const int ii = G.nx + 2, jj = G.ny + 2;
-	cc_copy<T>(G.so, G.pitch, gpl, const_cast<T *>(S.so), S.pitch, spl, ii, jj, G.ns);
-	if (S.sor) cc_copy<T>(G.sor, G.pitch, gpl, const_cast<T *>(S.sor), S.pitch, spl, ii, jj, relax == CDR_RELAX_POINT ? 1 : 2);
-	if (S.sory)  // transposed: nx+2 rows of ny+2 elements
-		cc_copy<T>(G.sory, G.tpitch, (size_t)G.tpitch * ii, const_cast<T *>(S.sory), S.tpitch, (size_t)S.tpitch * ii, jj,
-		           ii, 2);
-	cc_copy<T>(G.b, G.pitch, gpl, S.b, S.pitch, spl, ii, jj, 1);
-	cc_copy<T>(G.x, G.pitch, gpl, S.x, S.pitch, spl, ii, jj, 1);
-	if (with_r) cc_copy<T>(G.r, G.pitch, gpl, S.r, S.pitch, spl, ii, jj, 1);
-	__syncthreads();
+	const CoarseLevel<T> &Cg = cc.lv[cc.nl - 1];
+	const size_t n = (size_t)Cg.nx * Cg.ny;
+	*levels = lv;
+	*lines = ln;
+	*dbl = n + (size_t)(Cg.nx + 2) * n;
 }
 
 template <typename T>
 __global__ void __launch_bounds__(CC_THREADS) k_coarse_cycle(CoarseCycle<T> cc)
 {
 	extern __shared__ __align__(16) unsigned char cc_smem[];
-	T *lvl = reinterpret_cast<T *>(cc_smem);  // the visited level
-	T *sm = lvl + cc.level_elems;              // line right-hand sides
+	T *base = reinterpret_cast<T *>(cc_smem);
+	size_t nlv, nln, ndbl;
+	cc_layout(cc, &nlv, &nln, &ndbl);
+	T *sm = base + nlv;  // line right-hand sides
+	double *xs = reinterpret_cast<double *>(cc_smem + ((nlv + nln) * sizeof(T) + 7) / 8 * 8);
 	const int nl = cc.nl;
+	// stage: operators, factors and weights of every level; b of the first level;
+	// x, r and the other b zero (ghost rings included)
+	for (int l = 0; l < nl; ++l) {
+		const CoarseLevel<T> G = cc_global(cc, l), S = cc_view(cc, l, base);
+		const size_t gpl = (size_t)G.pitch * (G.ny + 2), spl = (size_t)S.pitch * (S.ny + 2);
+		const int ii = G.nx + 2, jj = G.ny + 2;
+		if (l < nl - 1) {
+			cc_copy<T>(G.so, G.pitch, gpl, const_cast<T *>(S.so), S.pitch, spl, ii, jj, G.ns);
+			if (S.sor) cc_copy<T>(G.sor, G.pitch, gpl, const_cast<T *>(S.sor), S.pitch, spl, ii, jj, cc_sor_planes(cc.relax));
+			if (S.sory)  // transposed: nx+2 rows of ny+2 elements
+				cc_copy<T>(G.sory, G.tpitch, (size_t)G.tpitch * ii, const_cast<T *>(S.sory), S.tpitch,
+				           (size_t)S.tpitch * ii, jj, ii, 2);
+			cc_fill(S.r, spl);
+		}
+		if (l > 0) cc_copy<T>(G.ci, G.pitch, gpl, const_cast<T *>(S.ci), S.pitch, spl, ii, jj, 8);
+		if (l == 0) cc_copy<T>(G.b, G.pitch, gpl, S.b, S.pitch, spl, ii, jj, 1);
+		else cc_fill(S.b, spl);
+		cc_fill(S.x, spl);
+	}
+	__syncthreads();
 	for (int l = 0; l + 1 < nl; ++l) {
-		const CoarseLevel<T> G = cc_level(cc, l), C = cc_level(cc, l + 1);
-		const CoarseLevel<T> F = cc_view(G, cc.relax, lvl);
-		// r too: restriction reads its ghost layer (zero) for odd edges
-		cc_stage(G, F, cc.relax, true);
+		const CoarseLevel<T> F = cc_view(cc, l, base), C = cc_view(cc, l + 1, base);
 		if (F.ns == 5) cc_smooth<T, 5>(cc, F, CDR_DOWN, sm);
 		else cc_smooth<T, 3>(cc, F, CDR_DOWN, sm);
 		if (F.ns == 5) cc_residual<T, 5>(F);
 		else cc_residual<T, 3>(F);
 		__syncthreads();
 		cc_restrict<T>(F, C);
-		cc_zero<T>(C);
-		// x and r of this level are needed again on the way up
-		const size_t gpl = (size_t)G.pitch * (G.ny + 2), spl = (size_t)F.pitch * (F.ny + 2);
-		cc_copy<T>(F.x, F.pitch, spl, G.x, G.pitch, gpl, G.nx + 2, G.ny + 2, 1);
-		cc_copy<T>(F.r, F.pitch, spl, G.r, G.pitch, gpl, G.nx + 2, G.ny + 2, 1);
+		cc_fill(C.x, (size_t)C.pitch * (C.ny + 2));
 		__syncthreads();
 	}
 	{
-		const CoarseLevel<T> Cg = cc_level(cc, nl - 1);
+		const CoarseLevel<T> Cg = cc_view(cc, nl - 1, base);
 		const size_t nab = (size_t)(Cg.nx + 2) * Cg.nx * Cg.ny;
-		cc_cg<T>(cc.abd + (size_t)blockIdx.x * cc.bstep * nab, Cg, reinterpret_cast<double *>(cc_smem));
+		cc_cg<T>(cc.abd + (size_t)blockIdx.x * cc.bstep * nab, Cg, xs);
 		__syncthreads();
 	}
 	for (int l = nl - 2; l >= 0; --l) {
-		const CoarseLevel<T> G = cc_level(cc, l), C = cc_level(cc, l + 1);
-		const CoarseLevel<T> F = cc_view(G, cc.relax, lvl);
-		cc_stage(G, F, cc.relax, true);
+		const CoarseLevel<T> F = cc_view(cc, l, base), C = cc_view(cc, l + 1, base);
 		cc_interp<T>(F, C);
 		__syncthreads();
 		if (F.ns == 5) cc_smooth<T, 5>(cc, F, CDR_UP, sm);
 		else cc_smooth<T, 3>(cc, F, CDR_UP, sm);
 		__syncthreads();
-		cc_copy<T>(F.x, F.pitch, (size_t)F.pitch * (F.ny + 2), G.x, G.pitch, (size_t)G.pitch * (G.ny + 2), G.nx + 2,
-		           G.ny + 2, 1);
-		__syncthreads();
+	}
+	{
+		const CoarseLevel<T> G = cc_global(cc, 0), S = cc_view(cc, 0, base);
+		cc_copy<T>(S.x, S.pitch, 0, G.x, G.pitch, 0, G.nx + 2, G.ny + 2, 1);
 	}
 }
 
-// Elements of the shared copy of one level (cc_view's layout)
 template <typename T>
-size_t cc_level_elems(const CoarseLevel<T> &L, int relax)
+size_t coarse_cycle_smem(const CoarseCycle<T> &cc)
 {
-	const size_t pl = (size_t)(L.nx + 2) * (L.ny + 2);
-	size_t planes = L.ns + 3;  // so, b, x, r
-	if (relax == CDR_RELAX_POINT) planes += 1;
-	else if (relax != CDR_RELAX_LINE_Y) planes += 2;
-	if (relax == CDR_RELAX_LINE_Y || relax == CDR_RELAX_LINE_XY) planes += 2;
-	return planes * pl;
-}
-
-template <typename T>
-size_t coarse_cycle_smem(const CoarseCycle<T> &cc, size_t *level_elems)
-{
-	size_t lvl = 0, lines = 0;
-	for (int l = 0; l + 1 < cc.nl; ++l) {
-		const CoarseLevel<T> &L = cc.lv[l];
-		lvl = std::max(lvl, cc_level_elems(L, cc.relax));
-		lines = std::max(lines, std::max((size_t)((L.ny + 1) / 2) * L.nx, (size_t)((L.nx + 1) / 2) * L.ny));
-	}
-	lvl = (lvl + 1) / 2 * 2;  // keep the line buffer 8-byte aligned
-	*level_elems = lvl;
-	const CoarseLevel<T> &Cg = cc.lv[cc.nl - 1];
-	const size_t n = (size_t)Cg.nx * Cg.ny;
-	return std::max((lvl + lines) * sizeof(T), (n + (size_t)(Cg.nx + 2) * n) * sizeof(double));
+	size_t nlv, nln, ndbl;
+	cc_layout(cc, &nlv, &nln, &ndbl);
+	return ((nlv + nln) * sizeof(T) + 7) / 8 * 8 + ndbl * sizeof(double);
 }
 
 // Shared memory a fused coarse cycle from level descriptor lv[0..nl) needs
 template <typename T>
 size_t coarse_cycle_bytes(const CoarseCycle<T> &cc)
 {
-	size_t e;
-	return coarse_cycle_smem(cc, &e);
+	return coarse_cycle_smem(cc);
 }
 template size_t coarse_cycle_bytes<double>(const CoarseCycle<double> &);
 template size_t coarse_cycle_bytes<float>(const CoarseCycle<float> &);
@@ -416,15 +457,12 @@ int coarse_cycle(const CoarseCycle<T> &cc, int nproblems, cudaStream_t st)
 		set_error(CDR_ERR_DIM, "fused coarse cycle over %d levels", cc.nl);
 		return CDR_ERR_DIM;
 	}
-	CoarseCycle<T> c2 = cc;
-	size_t lvl = 0;
-	const size_t smem = coarse_cycle_smem(c2, &lvl);
-	c2.level_elems = lvl;
+	const size_t smem = coarse_cycle_smem(cc);
 	if (smem > kCoarseSmemMax) {
 		set_error(CDR_ERR_DIM, "fused coarse cycle needs %zu bytes of shared memory", smem);
 		return CDR_ERR_DIM;
 	}
-	k_coarse_cycle<T><<<nproblems, CC_THREADS, smem, st>>>(c2);
+	k_coarse_cycle<T><<<nproblems, CC_THREADS, smem, st>>>(cc);
 	CDR_LAUNCH_CHECK();
 	return CDR_OK;
 }

@@ -10,8 +10,8 @@
 // The residual is formed anew from x every iteration (not updated as r -= alpha
 // q): on high-contrast operators the updated residual drifts from b - A x by
 // orders of magnitude before it converges, while the formed one stays at the
-// FP64 floor eps |A||x|.  Couplings into the ghost ring are taken as zero
-// (Dirichlet operators).  All of it is FP64.  Three kernels per iteration, each
+// FP64 floor eps |A||x|.  The products read the ghost ring as the residual
+// kernels do.  All of it is FP64.  Three kernels per iteration, each
 // ending in a deterministic grid reduction: every block writes its partial
 // sums, and the last block to finish (an atomic ticket) adds the partials in
 // block order and updates the device scalars, so the host only reads |r|.
@@ -23,9 +23,10 @@ namespace cdrgpu {
 
 namespace {
 
-constexpr int kFcgBlocks = 148 * 6;  // grid of every FCG kernel (partials: 2 slots of this)
+constexpr int FR = 4;  // rows per thread: each CTA covers 32 x 32 points, four independent rows in flight
 
-// Sum the NSUM per-thread values over the grid; the last block calls fin(totals).
+// Sum the NSUM per-thread values over the grid; the last block to finish adds
+// the blocks' partials in block order and calls fin(totals).
 template <int NSUM, typename F>
 __device__ __forceinline__ void grid_sums(const double (&acc)[NSUM], double *__restrict__ partial,
                                           unsigned *__restrict__ ticket, F fin)
@@ -33,24 +34,25 @@ __device__ __forceinline__ void grid_sums(const double (&acc)[NSUM], double *__r
 	__shared__ double sh[NSUM][TX * TY / 32];
 	__shared__ bool last;
 	const int tid = threadIdx.y * blockDim.x + threadIdx.x;
+	const int nb = gridDim.x * gridDim.y, bid = blockIdx.y * gridDim.x + blockIdx.x;
 	double tot[NSUM];
 #pragma unroll
 	for (int s = 0; s < NSUM; ++s) tot[s] = block_sum<TX * TY / 32>(acc[s], sh[s]);
 	if (tid == 0) {
 #pragma unroll
-		for (int s = 0; s < NSUM; ++s) partial[s * kFcgBlocks + blockIdx.x] = tot[s];
+		for (int s = 0; s < NSUM; ++s) partial[(size_t)s * nb + bid] = tot[s];
 		__threadfence();
-		last = atomicAdd(ticket, 1u) == gridDim.x - 1;
+		last = atomicAdd(ticket, 1u) == (unsigned)nb - 1u;
 	}
 	__syncthreads();
-	if (!last || tid >= 32) return;
+	if (!last) return;
 	__threadfence();
 	double v[NSUM];
 #pragma unroll
 	for (int s = 0; s < NSUM; ++s) {
-		v[s] = 0.0;
-		for (int b = tid; b < (int)gridDim.x; b += 32) v[s] += __ldcg(partial + s * kFcgBlocks + b);
-		for (int o = 16; o > 0; o >>= 1) v[s] += __shfl_down_sync(0xffffffffu, v[s], o);
+		double a = 0.0;
+		for (int b = tid; b < nb; b += TX * TY) a += __ldcg(partial + (size_t)s * nb + b);
+		v[s] = block_sum<TX * TY / 32>(a, sh[s]);
 	}
 	if (tid == 0) {
 		fin(v);
@@ -58,16 +60,13 @@ __device__ __forceinline__ void grid_sums(const double (&acc)[NSUM], double *__r
 	}
 }
 
-// Interior point t of the grid-stride loop -> (i, j); false when outside.
-__device__ __forceinline__ bool tile_point(const Dims2 &d, int t, int &i, int &j)
+// point (i, j) of row `row` of this thread; false outside the interior
+__device__ __forceinline__ bool fcg_point(const Dims2 &d, int row, int &i, int &j)
 {
-	const int tiles_x = (d.nx + TX - 1) / TX;
-	i = (t % tiles_x) * TX + threadIdx.x + 1;
-	j = (t / tiles_x) * TY + threadIdx.y + 1;
+	i = blockIdx.x * TX + threadIdx.x + 1;
+	j = blockIdx.y * (TY * FR) + threadIdx.y + 1 + row * TY;
 	return i <= d.nx && j <= d.ny;
 }
-
-__device__ __forceinline__ int tile_count(const Dims2 &d) { return ((d.nx + TX - 1) / TX) * ((d.ny + TY - 1) / TY); }
 
 // beta from z . q_prev
 template <typename TZ>
@@ -77,8 +76,9 @@ __global__ void __launch_bounds__(TX *TY) k_fcg_beta(const TZ *__restrict__ z, c
 	double acc[1] = {0.0};
 	if (!S->first) {
 		int i, j;
-		for (int t = blockIdx.x; t < tile_count(d); t += gridDim.x)
-			if (tile_point(d, t, i, j)) {
+#pragma unroll
+		for (int row = 0; row < FR; ++row)
+			if (fcg_point(d, row, i, j)) {
 				const size_t k = d.at(i, j);
 				acc[0] += (double)z[k] * q[k];
 			}
@@ -89,8 +89,9 @@ __global__ void __launch_bounds__(TX *TY) k_fcg_beta(const TZ *__restrict__ z, c
 	});
 }
 
-// p = z + beta p_prev (on the fly at the neighbours), q = A p on the interior
-// (couplings to the ghost ring dropped), p . q and p . r
+// p = z + beta p_prev (formed on the fly at the neighbours), q = A p, p . q and
+// p . r.  The products read the ghost ring as the residual kernels do (the
+// operator's couplings into it are zero); p is written on the interior only.
 template <typename TZ, int NS>
 __global__ void __launch_bounds__(TX *TY) k_fcg_dir(const double *__restrict__ so, const TZ *__restrict__ z,
                                                     double *__restrict__ p0, double *__restrict__ p1,
@@ -103,24 +104,19 @@ __global__ void __launch_bounds__(TX *TY) k_fcg_dir(const double *__restrict__ s
 	const double *__restrict__ pold = odd ? p1 : p0;
 	double *__restrict__ pnew = odd ? p0 : p1;
 	const double beta = S->beta;
-	const double *c = so, *w = so + ps, *s = so + 2 * ps;
+	const double *c = so, *w = so + ps, *s = so + 2 * ps, *sw = so + 3 * ps, *nw = so + 4 * ps;
+	auto P = [&](size_t k) -> double { return madd(beta, pold[k], (double)z[k]); };
 	double acc[2] = {0.0, 0.0};
-	auto P = [&](int ii, int jj) -> double {
-		if (ii < 1 || ii > d.nx || jj < 1 || jj > d.ny) return 0.0;
-		const size_t k = d.at(ii, jj);
-		return (double)z[k] + beta * pold[k];
-	};
 	int i, j;
-	for (int t = blockIdx.x; t < tile_count(d); t += gridDim.x)
-		if (tile_point(d, t, i, j)) {
-			const size_t k = d.at(i, j);
-			const double pc = P(i, j);
-			double nb = w[k] * P(i - 1, j) + w[k + 1] * P(i + 1, j) + s[k] * P(i, j - 1) + s[k + pitch] * P(i, j + 1);
-			if (NS == 5) {
-				const double *sw = so + 3 * ps, *nw = so + 4 * ps;
-				nb += sw[k] * P(i - 1, j - 1) + nw[k + 1] * P(i + 1, j - 1) + nw[k + pitch] * P(i - 1, j + 1)
-				      + sw[k + pitch + 1] * P(i + 1, j + 1);
-			}
+#pragma unroll
+	for (int row = 0; row < FR; ++row)
+		if (fcg_point(d, row, i, j)) {
+			const size_t k = (size_t)j * pitch + i;
+			const double pc = P(k);
+			double nb = w[k] * P(k - 1) + w[k + 1] * P(k + 1) + s[k] * P(k - pitch) + s[k + pitch] * P(k + pitch);
+			if (NS == 5)
+				nb += sw[k] * P(k - pitch - 1) + nw[k + 1] * P(k - pitch + 1) + nw[k + pitch] * P(k + pitch - 1)
+				      + sw[k + pitch + 1] * P(k + pitch + 1);
 			const double qk = c[k] * pc - nb;
 			pnew[k] = pc;
 			q[k] = qk;
@@ -152,24 +148,19 @@ __global__ void __launch_bounds__(TX *TY) k_fcg_update(const double *__restrict_
 	const double *__restrict__ xold = odd ? x1 : x0;
 	double *__restrict__ xnew = odd ? x0 : x1;
 	const double alpha = S->alpha;
-	const double *c = so, *w = so + ps, *s = so + 2 * ps;
-	auto X = [&](int ii, int jj) -> double {
-		if (ii < 1 || ii > d.nx || jj < 1 || jj > d.ny) return 0.0;
-		const size_t k = d.at(ii, jj);
-		return xold[k] + alpha * pnew[k];
-	};
+	const double *c = so, *w = so + ps, *s = so + 2 * ps, *sw = so + 3 * ps, *nw = so + 4 * ps;
+	auto X = [&](size_t k) -> double { return madd(alpha, pnew[k], xold[k]); };
 	double acc[1] = {0.0};
 	int i, j;
-	for (int t = blockIdx.x; t < tile_count(d); t += gridDim.x)
-		if (tile_point(d, t, i, j)) {
-			const size_t k = d.at(i, j);
-			const double xc = X(i, j);
-			double nb = w[k] * X(i - 1, j) + w[k + 1] * X(i + 1, j) + s[k] * X(i, j - 1) + s[k + pitch] * X(i, j + 1);
-			if (NS == 5) {
-				const double *sw = so + 3 * ps, *nw = so + 4 * ps;
-				nb += sw[k] * X(i - 1, j - 1) + nw[k + 1] * X(i + 1, j - 1) + nw[k + pitch] * X(i - 1, j + 1)
-				      + sw[k + pitch + 1] * X(i + 1, j + 1);
-			}
+#pragma unroll
+	for (int row = 0; row < FR; ++row)
+		if (fcg_point(d, row, i, j)) {
+			const size_t k = (size_t)j * pitch + i;
+			const double xc = X(k);
+			double nb = w[k] * X(k - 1) + w[k + 1] * X(k + 1) + s[k] * X(k - pitch) + s[k + pitch] * X(k + pitch);
+			if (NS == 5)
+				nb += sw[k] * X(k - pitch - 1) + nw[k + 1] * X(k - pitch + 1) + nw[k + pitch] * X(k + pitch - 1)
+				      + sw[k + pitch + 1] * X(k + pitch + 1);
 			const double rk = bb[k] + nb - c[k] * xc;
 			xnew[k] = xc;
 			r[k] = rk;
@@ -221,13 +212,13 @@ int fcg_load(const double *r, TZ *rin, TZ *z, Dims2 d, FcgScalars *S, cudaStream
 template int fcg_load<double>(const double *, double *, double *, Dims2, FcgScalars *, cudaStream_t);
 template int fcg_load<float>(const double *, float *, float *, Dims2, FcgScalars *, cudaStream_t);
 
+size_t fcg_scratch_doubles(Dims2 d) { return 2 * (size_t)ceil_div(d.nx, TX) * ceil_div(d.ny, TY * FR); }
+
 template <typename TZ>
 int fcg_step(const double *so, int ns, TZ *z, TZ *rin, double *x0, double *x1, const double *b, double *r,
              double *p0, double *p1, double *q, Dims2 d, double *partial, FcgScalars *S, cudaStream_t st)
 {
-	const int nt = ceil_div(d.nx, TX) * ceil_div(d.ny, TY);
-	const int nb = nt < kFcgBlocks ? nt : kFcgBlocks;
-	const dim3 blk(TX, TY);
+	const dim3 nb(ceil_div(d.nx, TX), ceil_div(d.ny, TY * FR)), blk(TX, TY);
 	k_fcg_beta<TZ><<<nb, blk, 0, st>>>(z, q, d, partial, S);
 	CDR_LAUNCH_CHECK();
 	if (ns == 5) k_fcg_dir<TZ, 5><<<nb, blk, 0, st>>>(so, z, p0, p1, q, r, d, partial, S);

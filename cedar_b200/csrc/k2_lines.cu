@@ -18,6 +18,9 @@
 // of the other colour.  With CDR_LINES_EXACT the substitutions instead run in
 // DPTTS2's sequential order (one thread per line): slower, bit-identical.
 #include <cstdint>
+#include <map>
+#include <mutex>
+#include <tuple>
 
 #include "k2_point.cuh"
 #include "kernels2d.cuh"
@@ -535,9 +538,75 @@ static int lines_per_cta(int n, int dir)
 	return G;
 }
 
+// ---------------------------------------------------------------- launch shapes
+// The register-chunk kernel's shape: K elements per thread and, for y-lines,
+// the CTA size cap (x-lines always run FAST_BLOCK_X threads).  The default is
+// K = 8 (16 for FP32 y-lines longer than 1024 points) and the largest CTA;
+// lines_autotune times the candidates on a level's own arrays at setup and
+// records the fastest per (direction, type, stencil, n, lines, single problem
+// or batch).  The
+// record lives for the process, so every solver of one shape in a process
+// runs the same launches (FP32 results depend on the chunking).
+namespace {
+struct LineKey {
+	int dir, tsize, ns, n, nl, nb;
+	bool operator<(const LineKey &o) const
+	{
+		return std::tie(dir, tsize, ns, n, nl, nb) < std::tie(o.dir, o.tsize, o.ns, o.n, o.nl, o.nb);
+	}
+};
+std::mutex g_shape_mu;
+std::map<LineKey, LineShape> &shape_table()
+{
+	static std::map<LineKey, LineShape> t;
+	return t;
+}
+}  // namespace
+
+template <typename T>
+static LineShape default_shape(int n, int dir)
+{
+	return LineShape{(dir == CDR_DIR_Y && sizeof(T) == 4 && n > 8 * 128) ? 16 : 8, FAST_BLOCK_Y};
+}
+
+template <typename T>
+static bool shape_ok(LineShape sh, int n, int dir)
+{
+	const bool kok = sizeof(T) == 4 ? (sh.K == 4 || sh.K == 8 || sh.K == 16) : (sh.K == 2 || sh.K == 4 || sh.K == 8);
+	if (!kok || n + 1 > 256 * sh.K) return false;
+	int tpl = 1;
+	while (tpl * sh.K < n + 1) tpl *= 2;
+	if (dir == CDR_DIR_X) return tpl <= FAST_BLOCK_X;
+	return sh.cap >= 32 && sh.cap <= FAST_BLOCK_Y && tpl <= sh.cap;
+}
+
+template <typename T>
+static LineShape shape_for(int n, int nl, int ns, int nb, int dir)
+{
+	std::lock_guard<std::mutex> lk(g_shape_mu);
+	auto it = shape_table().find(LineKey{dir, (int)sizeof(T), ns, n, nl, nb > 1 ? 2 : 1});
+	return it == shape_table().end() ? default_shape<T>(n, dir) : it->second;
+}
+
+template <typename T, int NS, int DIR, int K>
+static int launch_fast(const T *so, T *x, const T *b, const T *sor, Dims2 d, int tpitch, int first, int nlines,
+                       int cap, cudaStream_t st)
+{
+	const int n = DIR == CDR_DIR_X ? d.nx : d.ny;
+	int tpl_log2 = 0;
+	while ((1 << tpl_log2) * K < n + 1) ++tpl_log2;
+	const int TPL = 1 << tpl_log2;
+	const int block = DIR == CDR_DIR_X ? FAST_BLOCK_X : (TPL * 32 < cap ? TPL * 32 : cap);
+	const int G = block / TPL;
+	k_lines_fast<T, NS, DIR, K><<<dim3(ceil_div(nlines, G), 1, d.nb), block, 0, st>>>(so, x, b, sor, d, tpitch, first,
+	                                                                                  tpl_log2);
+	CDR_LAUNCH_CHECK();
+	return CDR_OK;
+}
+
 template <typename T, int NS, int DIR>
 static int launch_lines(const T *so, T *x, const T *b, const T *sor, Dims2 d, int tpitch, int first, bool exact,
-                        cudaStream_t st)
+                        cudaStream_t st, const LineShape *force = nullptr)
 {
 	const int n = DIR == CDR_DIR_X ? d.nx : d.ny;
 	const int nl = DIR == CDR_DIR_X ? d.ny : d.nx;
@@ -545,33 +614,20 @@ static int launch_lines(const T *so, T *x, const T *b, const T *sor, Dims2 d, in
 	if (nlines == 0) return CDR_OK;
 	// The register-chunk kernel reads whole 16-byte-aligned chunks of K elements:
 	// rows (x) or factor lines (y) must have a pitch that is a multiple of K and
-	// 16-byte aligned base pointers; lines up to 2048*8 - 1 points.
+	// 16-byte aligned base pointers; lines up to 256*K - 1 points.
 	const int fpitch = DIR == CDR_DIR_X ? d.pitch : tpitch;
 	const bool aligned = ((uintptr_t)so | (uintptr_t)x | (uintptr_t)b | (uintptr_t)sor) % 16 == 0;
-	// x: K = 8, 256 threads, 256/TPL lines per CTA.  y: K = 16 for lines longer
-	// than 1024 points so that a warp holds 8 lines side by side, at most 32 lines
-	// per CTA (lanes are line-fastest: every warp holds the same lines).  Fewer
-	// lines per CTA would fill more SMs on mid-size levels but halve the
-	// coalescing across lines, which costs more (measured).
-	const int K = (DIR == CDR_DIR_Y && sizeof(T) == 4 && n > 8 * 128) ? 16 : 8;
-	if (!exact && aligned && d.pitch % 16 == 0 && fpitch % 16 == 0 && n + 1 <= 256 * K) {
-		int tpl_log2 = 0;
-		while ((1 << tpl_log2) * K < n + 1) ++tpl_log2;
-		const int TPL = 1 << tpl_log2;
-		const int block = DIR == CDR_DIR_X ? FAST_BLOCK_X : (TPL * 32 < FAST_BLOCK_Y ? TPL * 32 : FAST_BLOCK_Y);
-		const int G = block / TPL;
-		if constexpr (DIR == CDR_DIR_Y && sizeof(T) == 4) {
-			if (K == 16) {
-				k_lines_fast<T, NS, DIR, 16>
-				    <<<dim3(ceil_div(nlines, G), 1, d.nb), block, 0, st>>>(so, x, b, sor, d, tpitch, first, tpl_log2);
-				CDR_LAUNCH_CHECK();
-				return CDR_OK;
-			}
+	LineShape sh = force ? *force : shape_for<T>(n, nl, NS, d.nb, DIR);
+	if (!shape_ok<T>(sh, n, DIR)) sh = default_shape<T>(n, DIR);
+	if (!exact && aligned && d.pitch % 16 == 0 && fpitch % 16 == 0 && shape_ok<T>(sh, n, DIR)) {
+		if constexpr (sizeof(T) == 4) {
+			if (sh.K == 4) return launch_fast<T, NS, DIR, 4>(so, x, b, sor, d, tpitch, first, nlines, sh.cap, st);
+			if (sh.K == 16) return launch_fast<T, NS, DIR, 16>(so, x, b, sor, d, tpitch, first, nlines, sh.cap, st);
+		} else {
+			if (sh.K == 2) return launch_fast<T, NS, DIR, 2>(so, x, b, sor, d, tpitch, first, nlines, sh.cap, st);
+			if (sh.K == 4) return launch_fast<T, NS, DIR, 4>(so, x, b, sor, d, tpitch, first, nlines, sh.cap, st);
 		}
-		k_lines_fast<T, NS, DIR, 8>
-		    <<<dim3(ceil_div(nlines, G), 1, d.nb), block, 0, st>>>(so, x, b, sor, d, tpitch, first, tpl_log2);
-		CDR_LAUNCH_CHECK();
-		return CDR_OK;
+		return launch_fast<T, NS, DIR, 8>(so, x, b, sor, d, tpitch, first, nlines, sh.cap, st);
 	}
 	const int G = lines_per_cta<T>(n, DIR);
 	size_t smem = sizeof(T) * (2 * LT + (size_t)G * n);
@@ -587,22 +643,97 @@ static int launch_lines(const T *so, T *x, const T *b, const T *sor, Dims2 d, in
 	return CDR_OK;
 }
 
+template <typename T, int NS, int DIR>
+static int tune_dir(const T *so, T *x, const T *b, const T *sor, Dims2 d, int tpitch, cudaStream_t st)
+{
+	const int n = DIR == CDR_DIR_X ? d.nx : d.ny;
+	const int nl = DIR == CDR_DIR_X ? d.ny : d.nx;
+	const LineKey key{DIR, (int)sizeof(T), NS, n, nl, d.nb > 1 ? 2 : 1};
+	{
+		std::lock_guard<std::mutex> lk(g_shape_mu);
+		if (shape_table().count(key)) return CDR_OK;
+	}
+	const int ks[3] = {sizeof(T) == 4 ? 4 : 2, sizeof(T) == 4 ? 8 : 4, sizeof(T) == 4 ? 16 : 8};
+	const int caps[3] = {256, 512, FAST_BLOCK_Y};
+	cudaEvent_t e0, e1;
+	CDR_CUDA_TRY(cudaEventCreate(&e0));
+	CDR_CUDA_TRY(cudaEventCreate(&e1));
+	LineShape best = default_shape<T>(n, DIR);
+	float best_ms = 1e30f;
+	int rc = CDR_OK;
+	for (int a = 0; a < 3 && rc == CDR_OK; ++a)
+		for (int c = 0; c < (DIR == CDR_DIR_X ? 1 : 3) && rc == CDR_OK; ++c) {
+			const LineShape sh{ks[a], DIR == CDR_DIR_X ? FAST_BLOCK_X : caps[c]};
+			if (!shape_ok<T>(sh, n, DIR)) continue;
+			float ms = 1e30f;
+			for (int rep = 0; rep < 3 && rc == CDR_OK; ++rep) {
+				rc = launch_lines<T, NS, DIR>(so, x, b, sor, d, tpitch, 1, false, st, &sh);
+				if (rc != CDR_OK) break;
+				if (cudaEventRecord(e0, st) != cudaSuccess) { rc = CDR_ERR_CUDA; break; }
+				for (int it = 0; it < 4 && rc == CDR_OK; ++it)
+					rc = launch_lines<T, NS, DIR>(so, x, b, sor, d, tpitch, 1 + (it & 1), false, st, &sh);
+				if (rc != CDR_OK) break;
+				float t = 0.f;
+				if (cudaEventRecord(e1, st) != cudaSuccess || cudaEventSynchronize(e1) != cudaSuccess ||
+				    cudaEventElapsedTime(&t, e0, e1) != cudaSuccess) {
+					rc = CDR_ERR_CUDA;
+					break;
+				}
+				ms = t < ms ? t : ms;
+			}
+			if (ms < best_ms) { best_ms = ms; best = sh; }
+		}
+	cudaEventDestroy(e0);
+	cudaEventDestroy(e1);
+	if (rc != CDR_OK) return rc;
+	std::lock_guard<std::mutex> lk(g_shape_mu);
+	shape_table()[key] = best;
+	return CDR_OK;
+}
+
+template <typename T>
+int lines_autotune(const T *so, int nstencil, T *x, const T *b, const T *sor, Dims2 d, int tpitch, int dir,
+                   cudaStream_t st)
+{
+	if (dir == CDR_DIR_X) {
+		if (nstencil == 5) return tune_dir<T, 5, CDR_DIR_X>(so, x, b, sor, d, tpitch, st);
+		return tune_dir<T, 3, CDR_DIR_X>(so, x, b, sor, d, tpitch, st);
+	}
+	if (nstencil == 5) return tune_dir<T, 5, CDR_DIR_Y>(so, x, b, sor, d, tpitch, st);
+	return tune_dir<T, 3, CDR_DIR_Y>(so, x, b, sor, d, tpitch, st);
+}
+template int lines_autotune<double>(const double *, int, double *, const double *, const double *, Dims2, int, int,
+                                    cudaStream_t);
+template int lines_autotune<float>(const float *, int, float *, const float *, const float *, Dims2, int, int,
+                                   cudaStream_t);
+
+bool lines_shape(int dir, int tsize, int ns, int n, int nl, int nb, LineShape *out)
+{
+	std::lock_guard<std::mutex> lk(g_shape_mu);
+	auto it = shape_table().find(LineKey{dir, tsize, ns, n, nl, nb > 1 ? 2 : 1});
+	if (it == shape_table().end()) return false;
+	*out = it->second;
+	return true;
+}
+
 template <typename T>
 int relax_lines_2d(const T *so, int nstencil, T *x, const T *b, const T *sor, Dims2 d, int tpitch, int dir,
                    int updown, int flags, cudaStream_t st)
 {
 	const bool exact = (flags & CDR_LINES_EXACT) != 0;
+	const LineShape dflt = default_shape<T>(dir == CDR_DIR_X ? d.nx : d.ny, dir);
+	const LineShape *force = (flags & CDR_LINES_NOTUNE) ? &dflt : nullptr;
 	// DOWN: lines with Fortran start index 3 (0-based even) first, then 2 (odd);
 	// UP: the opposite (relax_lines_x.f90:82-97).
 	const int firsts[2] = {updown == CDR_DOWN ? 2 : 1, updown == CDR_DOWN ? 1 : 2};
 	for (int c = 0; c < 2; ++c) {
 		int f = firsts[c];
 		if (dir == CDR_DIR_X) {
-			if (nstencil == 5) CDR_TRY((launch_lines<T, 5, CDR_DIR_X>(so, x, b, sor, d, tpitch, f, exact, st)));
-			else CDR_TRY((launch_lines<T, 3, CDR_DIR_X>(so, x, b, sor, d, tpitch, f, exact, st)));
+			if (nstencil == 5) CDR_TRY((launch_lines<T, 5, CDR_DIR_X>(so, x, b, sor, d, tpitch, f, exact, st, force)));
+			else CDR_TRY((launch_lines<T, 3, CDR_DIR_X>(so, x, b, sor, d, tpitch, f, exact, st, force)));
 		} else {
-			if (nstencil == 5) CDR_TRY((launch_lines<T, 5, CDR_DIR_Y>(so, x, b, sor, d, tpitch, f, exact, st)));
-			else CDR_TRY((launch_lines<T, 3, CDR_DIR_Y>(so, x, b, sor, d, tpitch, f, exact, st)));
+			if (nstencil == 5) CDR_TRY((launch_lines<T, 5, CDR_DIR_Y>(so, x, b, sor, d, tpitch, f, exact, st, force)));
+			else CDR_TRY((launch_lines<T, 3, CDR_DIR_Y>(so, x, b, sor, d, tpitch, f, exact, st, force)));
 		}
 	}
 	return CDR_OK;

@@ -94,6 +94,7 @@ int residual_2d(const T *so, int nstencil, const T *x, const T *b, T *r, Dims2 d
 }
 template int residual_2d<double>(const double *, int, const double *, const double *, double *, Dims2, double *,
                                  double *, cudaStream_t);
+
 template int residual_2d<float>(const float *, int, const float *, const float *, float *, Dims2, double *,
                                 double *, cudaStream_t);
 
@@ -479,50 +480,63 @@ int galerkin_2d(const double *so, int nstencil, const double *ci, double *soc, D
 // ABD fill of BMG2_SymStd_SETUP_cg_LU (src/2d/ftn/BMG2_SymStd_SETUP_cg_LU.f90:92-104,
 // 229-241) and LAPACK DPBTF2('U') (unblocked upper band Cholesky; DPBTRF takes it
 // for KD < 32).  The grid is at most a few dozen points: one thread.
-__global__ void k_cg_factor(const double *__restrict__ so, int ns, Dims2 d, double *__restrict__ ab, int *info)
+__global__ void __launch_bounds__(1024) k_cg_factor(const double *__restrict__ so, int ns, Dims2 d,
+                                                    double *__restrict__ ab, int *info)
 {
-	if (threadIdx.x != 0 || blockIdx.x != 0) return;
+	__shared__ double rcp_s;
+	__shared__ int stop_s;
+	const int tid = threadIdx.x, nt = blockDim.x;
 	const int ldab = d.nx + 2, kd = d.nx + 1, n = d.nx * d.ny;
 	const size_t ps = d.plane();
 	so += d.bofs(ns * ps);
 	ab += d.bofs((size_t)ldab * n);
-	for (size_t e = 0; e < (size_t)ldab * n; ++e) ab[e] = 0.0;
-	int kk = 0;
-	for (int j = 1; j <= d.ny; ++j)
-		for (int i = 1; i <= d.nx; ++i, ++kk) {
-			size_t k = d.at(i, j);
-			double *col = ab + (size_t)kk * ldab;  // column kk, rows 0..ldab-1
-			col[ldab - 1] = so[k];
-			col[ldab - 2] = -so[ps + k];
-			col[2] = ns == 5 ? -so[4 * ps + k + 1] : 0.0;
-			col[1] = -so[2 * ps + k];
-			col[0] = ns == 5 ? -so[3 * ps + k] : 0.0;
-		}
-	int kld = ldab - 1;
+	for (size_t e = tid; e < (size_t)ldab * n; e += nt) ab[e] = 0.0;
+	__syncthreads();
+	for (int kk = tid; kk < n; kk += nt) {
+		const size_t k = d.at(kk % d.nx + 1, kk / d.nx + 1);
+		double *col = ab + (size_t)kk * ldab;  // column kk, rows 0..ldab-1
+		col[ldab - 1] = so[k];
+		col[ldab - 2] = -so[ps + k];
+		col[2] = ns == 5 ? -so[4 * ps + k + 1] : 0.0;
+		col[1] = -so[2 * ps + k];
+		col[0] = ns == 5 ? -so[3 * ps + k] : 0.0;
+	}
+	// DPBTF2('U'): column jj's pivot by one thread, then its scaling and the
+	// rank-1 update of the trailing band triangle by all threads.  Every
+	// element receives the sequential routine's updates in the same order.
+	const int kld = ldab - 1;
 	int st = 0;
 	for (int jj = 0; jj < n; ++jj) {
-		double ajj = ab[(size_t)jj * ldab + kd];
-		if (ajj <= 0.0) { st = jj + 1; break; }
-		ajj = sqrt(ajj);
-		ab[(size_t)jj * ldab + kd] = ajj;
-		int kn = kd < n - jj - 1 ? kd : n - jj - 1;
-		if (kn > 0) {
-			double rcp = 1.0 / ajj;
-			double *x = ab + (size_t)(jj + 1) * ldab + (kd - 1);
-			for (int p = 0; p < kn; ++p) x[(size_t)p * kld] = rcp * x[(size_t)p * kld];
-			double *a = ab + (size_t)(jj + 1) * ldab + kd;
-			for (int q = 0; q < kn; ++q) {
-				double xq = x[(size_t)q * kld];
-				if (xq != 0.0) {
-					double temp = -1.0 * xq;
-					for (int p = 0; p <= q; ++p)
-						a[(size_t)p + (size_t)q * kld] = a[(size_t)p + (size_t)q * kld] + x[(size_t)p * kld] * temp;
-				}
+		__syncthreads();
+		if (tid == 0) {
+			double ajj = ab[(size_t)jj * ldab + kd];
+			stop_s = ajj <= 0.0;
+			if (!stop_s) {
+				ajj = sqrt(ajj);
+				ab[(size_t)jj * ldab + kd] = ajj;
+				rcp_s = 1.0 / ajj;
+			}
+		}
+		__syncthreads();
+		if (stop_s) { st = jj + 1; break; }
+		const int kn = kd < n - jj - 1 ? kd : n - jj - 1;
+		if (kn <= 0) continue;
+		double *x = ab + (size_t)(jj + 1) * ldab + (kd - 1);
+		for (int p = tid; p < kn; p += nt) x[(size_t)p * kld] = rcp_s * x[(size_t)p * kld];
+		__syncthreads();
+		double *a = ab + (size_t)(jj + 1) * ldab + kd;
+		for (int e = tid; e < kn * kn; e += nt) {
+			const int q = e / kn, p = e - q * kn;
+			if (p > q) continue;
+			const double xq = x[(size_t)q * kld];
+			if (xq != 0.0) {
+				const double temp = -1.0 * xq;
+				a[(size_t)p + (size_t)q * kld] = a[(size_t)p + (size_t)q * kld] + x[(size_t)p * kld] * temp;
 			}
 		}
 	}
 	// a batch records the first failure it meets (the caller zeroes info)
-	if (info) {
+	if (info && tid == 0) {
 		if (gridDim.z == 1) *info = st;
 		else if (st) atomicCAS(info, 0, st);
 	}
@@ -563,7 +577,7 @@ __global__ void k_cg_solve(const double *__restrict__ ab, T *__restrict__ q, con
 
 int setup_cg_2d(const double *so, int nstencil, Dims2 d, double *abd, int *info, cudaStream_t st)
 {
-	k_cg_factor<<<dim3(1, 1, d.nb), 32, 0, st>>>(so, nstencil, d, abd, info);
+	k_cg_factor<<<dim3(1, 1, d.nb), 1024, 0, st>>>(so, nstencil, d, abd, info);
 	CDR_LAUNCH_CHECK();
 	return CDR_OK;
 }

@@ -17,6 +17,16 @@ int lines_prepare();
 template <typename T>
 int relax_lines_2d(const T *so, int nstencil, T *x, const T *b, const T *sor, Dims2 d, int tpitch, int dir,
                    int updown, int flags, cudaStream_t st);
+// Launch shape of the line kernel (K elements per thread, y-line CTA cap) and
+// the setup-time autotuner that picks it per level (k2_lines.cu).  The tuner
+// runs line sweeps on the arrays it is given (x changes unless x = 0 and b = 0).
+struct LineShape {
+	int K = 8, cap = 1024;
+};
+template <typename T>
+int lines_autotune(const T *so, int nstencil, T *x, const T *b, const T *sor, Dims2 d, int tpitch, int dir,
+                   cudaStream_t st);
+bool lines_shape(int dir, int tsize, int ns, int n, int nl, int nb, LineShape *out);
 template <typename T>
 int restrict_2d(const T *ci, const T *rf, T *bc, Dims2 f, Dims2 c, cudaStream_t st);
 template <typename T>
@@ -27,6 +37,11 @@ int galerkin_2d(const double *so, int nstencil, const double *ci, double *soc, D
 int setup_cg_2d(const double *so, int nstencil, Dims2 d, double *abd, int *info, cudaStream_t st);
 template <typename T>
 int solve_cg_2d(const double *abd, T *x, const T *b, Dims2 d, cudaStream_t st);
+// Explicit inverse of the coarsest operator from its banded factor (n x n,
+// FP64, n = nx*ny) and its application (k2_cginv.cu)
+int cg_inverse_2d(const double *abd, Dims2 d, double *ainv, cudaStream_t st);
+template <typename T>
+int solve_cg_inv_2d(const T *ainv, T *x, const T *b, Dims2 d, cudaStream_t st);
 int convert_f64_f32(const double *in, float *out, size_t n, cudaStream_t st);
 int ir_residual_2d(const double *so, int nstencil, const double *x, const float *e, const double *b, double *xo,
                    float *r32, Dims2 d, Dims2 d32, double *norm_out, double *partial, int apply, cudaStream_t st,
@@ -34,14 +49,15 @@ int ir_residual_2d(const double *so, int nstencil, const double *x, const float 
 // partial-sum blocks per problem of a residual norm (partial holds nb times that)
 int norm_blocks(Dims2 d);
 
-// Device scalars of a flexible-CG solve (k2_krylov.cu); the partial-sum
-// scratch of its kernels is kNormScratchBytes.
+// Device scalars of a flexible-CG solve (k2_krylov.cu); its kernels' partial
+// sums need fcg_scratch_doubles(d) doubles of scratch.
 struct FcgScalars {
 	double zq, pq, beta, alpha, rr;
 	int first, iter;
 	unsigned ticket[3];
 };
 // r -> preconditioner input rin (zero ghost ring), z = 0, restart the recurrences
+size_t fcg_scratch_doubles(Dims2 d);
 template <typename TZ>
 int fcg_load(const double *r, TZ *rin, TZ *z, Dims2 d, FcgScalars *S, cudaStream_t st);
 // One FCG iteration after the preconditioner wrote z (3 launches); leaves the
@@ -70,7 +86,6 @@ struct CoarseCycle {
 	int nl = 0;
 	const double *abd = nullptr;
 	int relax = CDR_RELAX_POINT, npre = 2, npost = 1, bstep = 1;
-	size_t level_elems = 0;  // set by the launcher: shared elements of one level copy
 };
 // shared memory of the fused kernel (bytes) and its limit
 constexpr size_t kCoarseSmemMax = 220 * 1024;

@@ -55,6 +55,9 @@ struct cdr_gpu_solver {
 	// flexible CG: b, x, r, p (two buffers), q on the fine grid (FP64) and the scalars
 	double *kb = nullptr, *kx[2] = {nullptr, nullptr}, *kr = nullptr, *kp[2] = {nullptr, nullptr}, *kq = nullptr;
 	FcgScalars *ks = nullptr;
+	double *kpart = nullptr;  // partial sums of the FCG kernels
+	double *ainv = nullptr;   // CDR_COARSE_INVERSE: inverse of the coarsest operator
+	float *ainv32 = nullptr;
 	cudaGraphExec_t kexec[2] = {nullptr, nullptr};  // FCG iteration graphs: [0] FP64, [1] FP32 cycle
 	long long klaunches[2] = {0, 0};
 	double *h_norm = nullptr;   // pinned host copy of the norm
@@ -78,9 +81,10 @@ struct cdr_gpu_solver {
 	}
 
 	bool mixed() const { return s.precision == CDR_PREC_F32_IR; }
-	// the exact (sequential) line substitution applies to the FP64 cycle only
+	// the exact (sequential) line substitution applies to the FP64 cycle only;
+	// CDR_LINES_NOTUNE to both
 	template <typename T>
-	int lflags() const { return sizeof(T) == 8 ? s.line_flags : 0; }
+	int lflags() const { return sizeof(T) == 8 ? s.line_flags : (s.line_flags & CDR_LINES_NOTUNE); }
 	int L() const { return (int)lv.size(); }
 
 	// -------------------------------------------------------------- smoothing
@@ -92,10 +96,14 @@ struct cdr_gpu_solver {
 	int fused(int l0);
 	template <typename T>
 	int cycle(T *x, const T *b);
+	template <typename T>
+	int coarse_solve(T *x, const T *b);
 	int run_cycle(int prec);
 	template <typename T>
 	int fcg_iteration();
 	int run_fcg(int prec);
+	template <typename T>
+	int tune_lines();
 	int setup();
 };
 
@@ -161,7 +169,7 @@ int cdr_gpu_solver::ncycle(int l, T *x, const T *b)
 	CDR_TRY(residual_2d<T>(Arr<T>::so(F), F.ns, x, b, Arr<T>::r(F), F.d, nullptr, nullptr, st));
 	CDR_TRY(restrict_2d<T>(Arr<T>::ci(C), Arr<T>::r(F), Arr<T>::b(C), F.d, C.d, st));
 	CDR_CUDA_TRY(cudaMemsetAsync(Arr<T>::x(C), 0, sizeof(T) * C.d.plane(), st));
-	if (l + 1 == L() - 1) CDR_TRY(solve_cg_2d<T>(abd, Arr<T>::x(C), Arr<T>::b(C), C.d, st));
+	if (l + 1 == L() - 1) CDR_TRY(coarse_solve<T>(Arr<T>::x(C), Arr<T>::b(C)));
 	else if (l + 1 == lc[sizeof(T) == 4]) CDR_TRY(fused<T>(l + 1));
 	else CDR_TRY(ncycle<T>(l + 1, Arr<T>::x(C), Arr<T>::b(C)));
 	CDR_TRY(interp_add_2d<T>(Arr<T>::ci(C), Arr<T>::x(C), Arr<T>::r(F), Arr<T>::so(F), x, F.d, C.d, st));
@@ -226,9 +234,20 @@ int pick_fused_level(std::vector<Level> &lv, const cdr_gpu_settings &s)
 }
 
 template <typename T>
+int cdr_gpu_solver::coarse_solve(T *x, const T *b)
+{
+	const Dims2 d = lv.back().d;
+	if (s.coarse_solve == CDR_COARSE_INVERSE) {
+		if constexpr (sizeof(T) == 4) return solve_cg_inv_2d<float>(ainv32, x, b, d, st);
+		else return solve_cg_inv_2d<double>(ainv, x, b, d, st);
+	}
+	return solve_cg_2d<T>(abd, x, b, d, st);
+}
+
+template <typename T>
 int cdr_gpu_solver::cycle(T *x, const T *b)
 {
-	if (L() == 1) return solve_cg_2d<T>(abd, x, b, lv[0].d, st);
+	if (L() == 1) return coarse_solve<T>(x, b);
 	return ncycle<T>(0, x, b);
 }
 
@@ -272,7 +291,7 @@ int cdr_gpu_solver::fcg_iteration()
 	Level &F = lv[0];
 	T *z = Arr<T>::x(F), *rin = Arr<T>::b(F);
 	CDR_TRY(cycle<T>(z, rin));
-	return fcg_step<T>(F.so, F.ns, z, rin, kx[0], kx[1], kb, kr, kp[0], kp[1], kq, F.d, partial, ks, st);
+	return fcg_step<T>(F.so, F.ns, z, rin, kx[0], kx[1], kb, kr, kp[0], kp[1], kq, F.d, kpart, ks, st);
 }
 
 int cdr_gpu_solver::run_fcg(int prec)
@@ -303,6 +322,29 @@ int cdr_gpu_solver::run_fcg(int prec)
 	return CDR_OK;
 }
 
+// Launch shapes of the line kernels of every level the cycle sweeps with them
+// (all but the coarsest and the fused ones), timed on the levels' arrays.
+template <typename T>
+int cdr_gpu_solver::tune_lines()
+{
+	if (s.line_flags & CDR_LINES_NOTUNE) return CDR_OK;
+	if (sizeof(T) == 8 && (s.line_flags & CDR_LINES_EXACT)) return CDR_OK;
+	const bool lx = s.relaxation == CDR_RELAX_LINE_X || s.relaxation == CDR_RELAX_LINE_XY;
+	const bool ly = s.relaxation == CDR_RELAX_LINE_Y || s.relaxation == CDR_RELAX_LINE_XY;
+	const int f = lc[sizeof(T) == 4 ? 1 : 0];
+	const int stop = f >= 0 ? f : L() - 1;
+	for (int l = 0; l < stop; ++l) {
+		Level &F = lv[l];
+		if (lx)
+			CDR_TRY(lines_autotune<T>(Arr<T>::so(F), F.ns, Arr<T>::x(F), Arr<T>::b(F), Arr<T>::sor(F), F.d, F.tpitch,
+			                          CDR_DIR_X, st));
+		if (ly)
+			CDR_TRY(lines_autotune<T>(Arr<T>::so(F), F.ns, Arr<T>::x(F), Arr<T>::b(F), Arr<T>::sory(F), F.d, F.tpitch,
+			                          CDR_DIR_Y, st));
+	}
+	return CDR_OK;
+}
+
 // multilevel::setup (include/cedar/multilevel.h:243-265) on the device.
 int cdr_gpu_solver::setup()
 {
@@ -327,6 +369,10 @@ int cdr_gpu_solver::setup()
 	}
 	Level &Cg = lv[L() - 1];
 	CDR_TRY(setup_cg_2d(Cg.so, Cg.ns, Cg.d, abd, info + 1, st));
+	if (s.coarse_solve == CDR_COARSE_INVERSE) {
+		CDR_TRY(cg_inverse_2d(abd, Cg.d, ainv, st));
+		if (mixed()) CDR_TRY(convert_f64_f32(ainv, ainv32, (size_t)Cg.nx * Cg.ny * Cg.nx * Cg.ny, st));
+	}
 	if (mixed()) {
 		for (int l = 0; l < L(); ++l) {
 			Level &F = lv[l];
@@ -393,6 +439,7 @@ int cdr_gpu_settings_default(cdr_gpu_settings *s)
 	s->line_flags = 0;
 	s->fuse_coarse = 32;
 	s->krylov = CDR_KRYLOV_NONE;
+	s->coarse_solve = CDR_COARSE_BANDED;
 	return CDR_OK;
 }
 
@@ -423,7 +470,9 @@ static int load_and_setup(cdr_gpu_solver *h, const double *so, int src_pitch, cu
 	CDR_CUDA_TRY(cudaEventRecord(h->ev1, h->st));
 	CDR_CUDA_TRY(cudaEventSynchronize(h->ev1));
 	CDR_CUDA_TRY(cudaEventElapsedTime(&h->setup_ms, h->ev0, h->ev1));
-	return CDR_OK;
+	// launch shapes of the line kernels (once per shape and process; the sweeps
+	// run on the level arrays, which the solve reloads or overwrites)
+	return h->mixed() ? h->tune_lines<float>() : h->tune_lines<double>();
 }
 
 static int create_impl(cdr_gpu_solver *h, const double *so_src, int ns, int nx, int ny, int src_pitch,
@@ -483,6 +532,11 @@ static int create_impl(cdr_gpu_solver *h, const double *so_src, int ns, int nx, 
 		return CDR_ERR_DIM;
 	}
 	CDR_TRY(h->alloc(&h->abd, (size_t)(Cg.nx + 2) * Cg.nx * Cg.ny));
+	if (s.coarse_solve == CDR_COARSE_INVERSE) {
+		const size_t nn = (size_t)Cg.nx * Cg.ny * Cg.nx * Cg.ny;
+		CDR_TRY(h->alloc(&h->ainv, nn));
+		if (h->mixed()) CDR_TRY(h->alloc(&h->ainv32, nn));
+	}
 	CDR_TRY(h->alloc(&h->info, 2));
 	CDR_TRY(h->alloc(&h->norm, 4));
 	CDR_TRY(h->alloc(&h->partial, kNormScratchBytes / sizeof(double)));
@@ -494,6 +548,7 @@ static int create_impl(cdr_gpu_solver *h, const double *so_src, int ns, int nx, 
 		const size_t pl = h->lv[0].d.plane();
 		for (double **p : {&h->kb, &h->kx[0], &h->kx[1], &h->kr, &h->kp[0], &h->kp[1], &h->kq}) CDR_TRY(h->alloc(p, pl));
 		CDR_TRY(h->alloc(&h->ks, 1));
+		CDR_TRY(h->alloc(&h->kpart, fcg_scratch_doubles(h->lv[0].d)));
 	}
 	CDR_CUDA_TRY(cudaMallocHost(&h->h_norm, 4 * sizeof(double)));
 	// fine operator (source pitch) -> device pitch, then the device setup
@@ -516,6 +571,10 @@ static int create_any(const cdr_gpu_settings *s, const double *so_src, int ns, i
 	}
 	if (s->krylov != CDR_KRYLOV_NONE && s->krylov != CDR_KRYLOV_FCG) {
 		set_error(CDR_ERR_ARG, "invalid krylov %d", s->krylov);
+		return CDR_ERR_ARG;
+	}
+	if (s->coarse_solve != CDR_COARSE_BANDED && s->coarse_solve != CDR_COARSE_INVERSE) {
+		set_error(CDR_ERR_ARG, "invalid coarse_solve %d", s->coarse_solve);
 		return CDR_ERR_ARG;
 	}
 	*out = nullptr;

@@ -41,11 +41,14 @@ def _settings(ms: MLSettings, dim=2):
     s.min_coarse = ms.min_coarse
     s.precision = _lib.PREC[ms.precision]
     s.use_graph = 1 if ms.use_graph else 0
-    s.line_flags = _lib.LINES_EXACT if ms.line_solve == "sequential" else 0
+    s.line_flags = (_lib.LINES_EXACT if ms.line_solve == "sequential" else 0) | (0 if ms.autotune else _lib.LINES_NOTUNE)
     s.fuse_coarse = ms.fuse_coarse
     if ms.krylov != "none" and dim != 2:
         raise NotImplementedError("gpu.krylov = %r: the Krylov outer iteration is 2D only" % ms.krylov)
+    if ms.coarse_solve != "banded" and dim != 2:
+        raise NotImplementedError("gpu.coarse-solve = %r is a 2D-solver option" % ms.coarse_solve)
     s.krylov = _lib.KRYLOV[ms.krylov]
+    s.coarse_solve = _lib.COARSE[ms.coarse_solve]
     return s
 
 

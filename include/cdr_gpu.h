@@ -65,6 +65,15 @@ extern "C" {
 #define CDR_KRYLOV_NONE 0
 #define CDR_KRYLOV_FCG  1
 
+/* Coarsest-level solve of the 2D solver (settings.coarse_solve).
+ * CDR_COARSE_BANDED: DPBTRS with the banded Cholesky factor, as the reference
+ * (bit-identical).  CDR_COARSE_INVERSE (no counterpart in the reference): the
+ * setup forms the inverse from that factor and every cycle multiplies by it —
+ * equal to rounding, and fast when the coarsest level has thousands of
+ * unknowns (solver.num-levels set so that it stops at e.g. 63^2). */
+#define CDR_COARSE_BANDED  0
+#define CDR_COARSE_INVERSE 1
+
 /* Line direction */
 #define CDR_DIR_X 0
 #define CDR_DIR_Y 1
@@ -75,6 +84,12 @@ int cdr_gpu_version(void);
 /* Kernel launches issued by this library so far in this process (a replayed
  * cycle graph counts the launches it holds). */
 long long cdr_gpu_launch_count(void);
+/* Launch shape the line-kernel autotuner chose for lines of length n, nlines
+ * lines, direction dir (CDR_DIR_*), FP32 (fp32 = 1) or FP64 sweeps, nstencil 3
+ * or 5, a single problem (batch = 0) or a batch (batch = 1): elements per
+ * thread *K and the CTA size cap *cap.  Returns CDR_ERR_ARG when no solver of
+ * this process has tuned that shape.  No counterpart in the reference. */
+int cdr_gpu_lines_shape(int dir, int fp32, int nstencil, int n, int nlines, int batch, int *K, int *cap);
 
 /* ------------------------------------------------------------------------
  * 2D kernels.  T = double (_f64) or float (_f32).
@@ -141,8 +156,15 @@ int cdr_gpu_setup_lines_2d_f32(const double *so, int nstencil, float *sor, int n
  * BMG2_SymStd_relax_lines_y.f90:74-129).  flags = 0: the per-line DPTTRS
  * substitutions run as a parallel affine scan (fast; each element gets the
  * DPTTS2 update of its inputs, chunk-entry values may differ by rounding);
- * flags = CDR_LINES_EXACT: sequential substitutions, bit-identical to DPTTRS. */
+ * flags = CDR_LINES_EXACT: sequential substitutions, bit-identical to DPTTRS.
+ * The parallel kernel's launch shape is the one a solver of this process tuned
+ * for this line length and count (cdr_gpu_lines_shape), else the default;
+ * CDR_LINES_NOTUNE forces the default. */
 #define CDR_LINES_EXACT 1
+/* Solver settings.line_flags / kernel flags: keep the default launch shape of
+ * the line kernel instead of timing the candidates at setup (the autotuner,
+ * whose choice is kept for the process). */
+#define CDR_LINES_NOTUNE 2
 int cdr_gpu_relax_lines_2d_f64(const double *so, int nstencil, double *x, const double *b, const double *sor,
                                int nx, int ny, int pitch, int tpitch, int dir, int updown, int flags,
                                cudaStream_t stream);
@@ -233,9 +255,10 @@ typedef struct cdr_gpu_settings {
 	int min_coarse;   /* "solver.min_coarse"  (default 3)                              */
 	int precision;    /* CDR_PREC_F64 (default) or CDR_PREC_F32_IR                     */
 	int use_graph;    /* replay the cycle as a CUDA graph (default 1)                  */
-	int line_flags;   /* CDR_LINES_EXACT for sequential line substitutions (default 0) */
+	int line_flags;   /* CDR_LINES_EXACT: sequential line substitutions; CDR_LINES_NOTUNE (default 0) */
 	int fuse_coarse;  /* levels with both edges <= this run as one fused kernel (default 32, 0 = off) */
 	int krylov;       /* CDR_KRYLOV_NONE (default) or CDR_KRYLOV_FCG; 2D solver only    */
+	int coarse_solve; /* CDR_COARSE_BANDED (default) or CDR_COARSE_INVERSE; 2D solver only */
 } cdr_gpu_settings;
 
 typedef struct cdr_gpu_solver cdr_gpu_solver;

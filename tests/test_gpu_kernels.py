@@ -254,3 +254,36 @@ def test_coarse_cholesky_bitwise(lib, oracle, n):
     dx, db = dev(np.zeros_like(b)), dev(b)
     _lib.check(lib.cdr_gpu_solve_cg_2d_f64(ptr(dabd), ptr(dx), ptr(db), n, n, n + 2, stream()))
     np.testing.assert_array_equal(host(dx), x)
+
+
+def test_line_autotuner_records_shapes_and_keeps_results():
+    """The setup-time autotuner records a launch shape for every swept level; the
+    tuned FP32 solve converges like the default-shape one (same tolerance, at
+    most one cycle apart: the chunking changes FP32 rounding only)."""
+    import ctypes
+    from cedar_b200 import _lib
+    from cedar_b200 import problems as P
+    from cedar_b200.config import Config
+    from cedar_b200.solver import Solver2D
+    lib = _lib.load()
+    n = 255
+    so, b = P.hetero_diffusion(n, sigma=1.0, n_incl=4, contrast=100.0, aniso=0.5)
+    res = {}
+    for tune in (True, False):
+        s = Solver2D(so, Config({"solver": {"relaxation": "line-xy", "max-iter": 30, "tol": 1e-9},
+                                 "gpu": {"precision": "fp32-ir", "autotune": tune}}))
+        s.solve(b)
+        res[tune] = (s.iters, s.history[-1])
+        if tune:
+            for l in range(s.nlevels - 1):
+                _, nx, ny, *_ = s.level_info(l, "so")
+                if nx <= 32:
+                    break  # fused coarse levels do not use the line kernels
+                for d, (nn, nl) in ((0, (nx, ny)), (1, (ny, nx))):
+                    K, cap = ctypes.c_int(), ctypes.c_int()
+                    for first in (1,):
+                        rc = lib.cdr_gpu_lines_shape(d, 1, 5, nn, nl, 0, ctypes.byref(K), ctypes.byref(cap))
+                        assert rc == 0, (l, d)
+                        assert K.value in (4, 8, 16) and cap.value in (256, 512, 1024)
+    assert res[True][1] < 1e-9 and res[False][1] < 1e-9
+    assert abs(res[True][0] - res[False][0]) <= 1
