@@ -11,7 +11,8 @@ default; "sequential": DPTTRS order, bit-identical to the reference), ``autotune
 the line kernels' launch shapes per level at setup, once per shape and process), ``krylov`` ("none": the
 reference's outer loop, the default; "fcg": the cycle preconditions flexible conjugate gradients, 2D only) and
 ``coarse-solve`` ("banded": the reference's DPBTRS, the default; "inverse": the setup forms the coarsest
-operator's inverse and every cycle multiplies by it, 2D only — for a coarsest level of thousands of unknowns).
+operator's inverse and every cycle multiplies by it, 2D only — for a coarsest level of thousands of unknowns)
+and ``fp32-levels`` (the FP32 cycle keeps this many finest levels in FP32, the rest in FP64; 0 = all, 2D only).
 """
 import json
 import os
@@ -84,6 +85,9 @@ class MLSettings:
         self.krylov = conf.get("gpu.krylov", "none")
         if self.krylov not in ("none", "fcg"):
             raise ValueError("invalid gpu.krylov: %s" % self.krylov)
+        self.fp32_levels = int(conf.get("gpu.fp32-levels", 0))
+        if self.fp32_levels < 0:
+            raise ValueError("invalid gpu.fp32-levels: %d" % self.fp32_levels)
         self.coarse_solve = conf.get("gpu.coarse-solve", "banded")
         if self.coarse_solve not in ("banded", "inverse"):
             raise ValueError("invalid gpu.coarse-solve: %s" % self.coarse_solve)

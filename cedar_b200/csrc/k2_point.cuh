@@ -59,25 +59,28 @@ __device__ __forceinline__ void gs_at(const T *__restrict__ so, size_t ps, T *__
 }
 
 // Coarse point (ic, jc) of BMG2_SymStd_restrict (src/2d/ftn/BMG2_SymStd_restrict.f90:72-92);
-// it sits on fine (2ic-1, 2jc-1) (0-based, ghosts at 0).
-template <typename T>
-__device__ __forceinline__ void restrict_at(const T *__restrict__ ci, const T *__restrict__ q, T *__restrict__ qc,
+// it sits on fine (2ic-1, 2jc-1) (0-based, ghosts at 0).  TF/TC: fine and
+// coarse types (equal except where an FP32 level hands over to an FP64 one;
+// the sum is then formed in the coarse type).
+template <typename TF, typename TC = TF>
+__device__ __forceinline__ void restrict_at(const TC *__restrict__ ci, const TF *__restrict__ q, TC *__restrict__ qc,
                                             const Dims2 &f, const Dims2 &c, int ic, int jc)
 {
 	const size_t cps = c.plane();
 	const int cp = c.pitch, fp = f.pitch;
 	const size_t kc = c.at(ic, jc), kf = f.at(2 * ic - 1, 2 * jc - 1);
-	const T *cL = ci + IL * cps, *cR = ci + IR * cps, *cA = ci + IA * cps, *cB = ci + IB * cps;
-	const T *cSW = ci + ISW * cps, *cNW = ci + INW * cps, *cNE = ci + INE * cps, *cSE = ci + ISE * cps;
-	T a = cNE[kc] * q[kf - fp - 1];
-	a = madd(cA[kc], q[kf - fp], a);
-	a = madd(cNW[kc + 1], q[kf - fp + 1], a);
-	a = madd(cR[kc], q[kf - 1], a);
-	a = a + q[kf];
-	a = madd(cL[kc + 1], q[kf + 1], a);
-	a = madd(cSE[kc + cp], q[kf + fp - 1], a);
-	a = madd(cB[kc + cp], q[kf + fp], a);
-	qc[kc] = madd(cSW[kc + cp + 1], q[kf + fp + 1], a);
+	const TC *cL = ci + IL * cps, *cR = ci + IR * cps, *cA = ci + IA * cps, *cB = ci + IB * cps;
+	const TC *cSW = ci + ISW * cps, *cNW = ci + INW * cps, *cNE = ci + INE * cps, *cSE = ci + ISE * cps;
+	auto Q = [&](size_t k) -> TC { return (TC)q[k]; };
+	TC a = cNE[kc] * Q(kf - fp - 1);
+	a = madd(cA[kc], Q(kf - fp), a);
+	a = madd(cNW[kc + 1], Q(kf - fp + 1), a);
+	a = madd(cR[kc], Q(kf - 1), a);
+	a = a + Q(kf);
+	a = madd(cL[kc + 1], Q(kf + 1), a);
+	a = madd(cSE[kc + cp], Q(kf + fp - 1), a);
+	a = madd(cB[kc + cp], Q(kf + fp), a);
+	qc[kc] = madd(cSW[kc + cp + 1], Q(kf + fp + 1), a);
 }
 
 // Coarse cell (ic, jc) of BMG2_SymStd_interp_add (src/2d/ftn/BMG2_SymStd_interp_add.f90:101-137),
@@ -85,34 +88,39 @@ __device__ __forceinline__ void restrict_at(const T *__restrict__ ci, const T *_
 // r/c is formed on the fly; the reference divides r by c on interior points
 // only, and for even grid sizes its loop also reaches the ghost row/column,
 // where r is added undivided.
-template <typename T>
-__device__ __forceinline__ void interp_at(const T *__restrict__ ci, const T *__restrict__ qc,
-                                          const T *__restrict__ res, const T *__restrict__ soc, T *__restrict__ q,
+// TF/TC as in restrict_at: the correction is formed in the coarse type and
+// rounded to the fine one.
+template <typename TF, typename TC = TF>
+__device__ __forceinline__ void interp_at(const TC *__restrict__ ci, const TC *__restrict__ qc,
+                                          const TF *__restrict__ res, const TF *__restrict__ soc, TF *__restrict__ q,
                                           const Dims2 &f, const Dims2 &c, int ic, int jc)
 {
 	const size_t cps = c.plane();
 	const int cp = c.pitch, fp = f.pitch;
 	const int i = 2 * ic - 1, j = 2 * jc - 1;
 	const size_t kc = c.at(ic, jc), kf = f.at(i, j);
-	auto rc = [&](size_t k, int ii, int jj) -> T { return (ii <= f.nx && jj <= f.ny) ? res[k] / soc[k] : res[k]; };
-	const T qcc = qc[kc];
-	q[kf] = q[kf] + qcc;
+	auto rc = [&](size_t k, int ii, int jj) -> TC {
+		return (ii <= f.nx && jj <= f.ny) ? (TC)(res[k] / soc[k]) : (TC)res[k];
+	};
+	auto Q = [&](size_t k) -> TC { return (TC)q[k]; };
+	const TC qcc = qc[kc];
+	q[kf] = (TF)(Q(kf) + qcc);
 	if (ic >= 2) {
-		const T a = madd(ci[IL * cps + kc], qc[kc - 1], ci[IR * cps + kc] * qcc);
+		const TC a = madd(ci[IL * cps + kc], qc[kc - 1], ci[IR * cps + kc] * qcc);
 		const size_t k = kf - 1;
-		q[k] = q[k] + a + rc(k, i - 1, j);
+		q[k] = (TF)(Q(k) + a + rc(k, i - 1, j));
 	}
 	if (jc >= 2) {
-		const T aq = madd(ci[IB * cps + kc], qc[kc - cp], ci[IA * cps + kc] * qcc);
+		const TC aq = madd(ci[IB * cps + kc], qc[kc - cp], ci[IA * cps + kc] * qcc);
 		const size_t k = kf - fp;
-		q[k] = q[k] + aq + rc(k, i, j - 1);
+		q[k] = (TF)(Q(k) + aq + rc(k, i, j - 1));
 	}
 	if (ic >= 2 && jc >= 2) {
-		T a = madd(ci[INW * cps + kc], qc[kc - 1], ci[ISW * cps + kc] * qc[kc - cp - 1]);
+		TC a = madd(ci[INW * cps + kc], qc[kc - 1], ci[ISW * cps + kc] * qc[kc - cp - 1]);
 		a = madd(ci[INE * cps + kc], qcc, a);
 		a = madd(ci[ISE * cps + kc], qc[kc - cp], a);
 		const size_t k = kf - fp - 1;
-		q[k] = q[k] + a + rc(k, i - 1, j - 1);
+		q[k] = (TF)(Q(k) + a + rc(k, i - 1, j - 1));
 	}
 }
 

@@ -182,9 +182,9 @@ template int relax_point_2d<float>(const float *, int, float *, const float *, c
 // ---------------------------------------------------------------- restriction
 // BMG2_SymStd_restrict (src/2d/ftn/BMG2_SymStd_restrict.f90:72-92): coarse
 // (ic, jc) sits on fine (2ic-1, 2jc-1) (0-based, ghosts at 0).
-template <typename T>
-__global__ void __launch_bounds__(TX *TY) k_restrict(const T *__restrict__ ci, const T *__restrict__ q,
-                                                     T *__restrict__ qc, Dims2 f, Dims2 c)
+template <typename T, typename TC = T>
+__global__ void __launch_bounds__(TX *TY) k_restrict(const TC *__restrict__ ci, const T *__restrict__ q,
+                                                     TC *__restrict__ qc, Dims2 f, Dims2 c)
 {
 	int ic = blockIdx.x * TX + threadIdx.x + 1, jc = blockIdx.y * TY + threadIdx.y + 1;
 	if (ic > c.nx || jc > c.ny) return;
@@ -192,7 +192,7 @@ __global__ void __launch_bounds__(TX *TY) k_restrict(const T *__restrict__ ci, c
 	ci += c.bofs(8 * cps);
 	q += f.bofs(f.plane());
 	qc += c.bofs(cps);
-	restrict_at<T>(ci, q, qc, f, c, ic, jc);
+	restrict_at<T, TC>(ci, q, qc, f, c, ic, jc);
 }
 
 template <typename T>
@@ -205,13 +205,21 @@ int restrict_2d(const T *ci, const T *rf, T *bc, Dims2 f, Dims2 c, cudaStream_t 
 template int restrict_2d<double>(const double *, const double *, double *, Dims2, Dims2, cudaStream_t);
 template int restrict_2d<float>(const float *, const float *, float *, Dims2, Dims2, cudaStream_t);
 
+int restrict_2d_mixed(const double *ci, const float *rf, double *bc, Dims2 f, Dims2 c, cudaStream_t st)
+{
+	k_restrict<float, double><<<dim3(ceil_div(c.nx, TX), ceil_div(c.ny, TY), c.nb), dim3(TX, TY), 0, st>>>(ci, rf, bc,
+	                                                                                                     f, c);
+	CDR_LAUNCH_CHECK();
+	return CDR_OK;
+}
+
 // ------------------------------------------------------------ interpolate-add
 // BMG2_SymStd_interp_add (src/2d/ftn/BMG2_SymStd_interp_add.f90:101-137).  One
 // thread per coarse cell (IC, JC) of the reference loop (0-based ic in
 // [1, nxf/2+1]); it owns fine points (i, j), (i-1, j), (i, j-1), (i-1, j-1) with
 // i = 2ic-1.  r/c is formed on the fly instead of dividing r in place.
-template <typename T>
-__global__ void __launch_bounds__(TX *TY) k_interp_add(const T *__restrict__ ci, const T *__restrict__ qc,
+template <typename T, typename TC = T>
+__global__ void __launch_bounds__(TX *TY) k_interp_add(const TC *__restrict__ ci, const TC *__restrict__ qc,
                                                        const T *__restrict__ res, const T *__restrict__ soc,
                                                        T *__restrict__ q, Dims2 f, Dims2 c, int nsf)
 {
@@ -223,7 +231,7 @@ __global__ void __launch_bounds__(TX *TY) k_interp_add(const T *__restrict__ ci,
 	res += f.bofs(f.plane());
 	soc += f.bofs(nsf * f.plane());
 	q += f.bofs(f.plane());
-	interp_at<T>(ci, qc, res, soc, q, f, c, ic, jc);
+	interp_at<T, TC>(ci, qc, res, soc, q, f, c, ic, jc);
 }
 
 template <typename T>
@@ -239,6 +247,15 @@ template int interp_add_2d<double>(const double *, const double *, const double 
                                    Dims2, Dims2, cudaStream_t, int);
 template int interp_add_2d<float>(const float *, const float *, const float *, const float *, float *, Dims2,
                                   Dims2, cudaStream_t, int);
+
+int interp_add_2d_mixed(const double *ci, const double *xc, const float *rf, const float *sof, float *xf, Dims2 f,
+                        Dims2 c, cudaStream_t st, int nsf)
+{
+	k_interp_add<float, double><<<dim3(ceil_div(f.nx / 2 + 1, TX), ceil_div(f.ny / 2 + 1, TY), f.nb), dim3(TX, TY), 0,
+	                              st>>>(ci, xc, rf, sof, xf, f, c, nsf);
+	CDR_LAUNCH_CHECK();
+	return CDR_OK;
+}
 
 // ------------------------------------------------ operator-induced interpolation
 // BMG2_SymStd_SETUP_interp_OI (src/2d/ftn/BMG2_SymStd_SETUP_interp_OI.f90:109-253).

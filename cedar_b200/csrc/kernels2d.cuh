@@ -32,6 +32,10 @@ int restrict_2d(const T *ci, const T *rf, T *bc, Dims2 f, Dims2 c, cudaStream_t 
 template <typename T>
 int interp_add_2d(const T *ci, const T *xc, const T *rf, const T *sof, T *xf, Dims2 f, Dims2 c, cudaStream_t st,
                   int nstencil_fine = 5);
+// Hand-over from an FP32 fine level to an FP64 coarse one (mixed cycles)
+int restrict_2d_mixed(const double *ci, const float *rf, double *bc, Dims2 f, Dims2 c, cudaStream_t st);
+int interp_add_2d_mixed(const double *ci, const double *xc, const float *rf, const float *sof, float *xf, Dims2 f,
+                        Dims2 c, cudaStream_t st, int nsf_fine = 5);
 int setup_interp_2d(const double *so, int nstencil, double *ci, Dims2 f, Dims2 c, cudaStream_t st);
 int galerkin_2d(const double *so, int nstencil, const double *ci, double *soc, Dims2 f, Dims2 c, cudaStream_t st);
 int setup_cg_2d(const double *so, int nstencil, Dims2 d, double *abd, int *info, cudaStream_t st);

@@ -18,6 +18,7 @@
 // With settings.krylov = CDR_KRYLOV_FCG either cycle instead preconditions
 // flexible CG (k2_krylov.cu); the iteration (cycle + three FCG kernels) is one
 // CUDA graph.
+#include <algorithm>
 #include <vector>
 #include <cstring>
 #include <cmath>
@@ -167,6 +168,17 @@ int cdr_gpu_solver::ncycle(int l, T *x, const T *b)
 	Level &F = lv[l], &C = lv[l + 1];
 	CDR_TRY(smooth<T>(l, x, b, CDR_DOWN));
 	CDR_TRY(residual_2d<T>(Arr<T>::so(F), F.ns, x, b, Arr<T>::r(F), F.d, nullptr, nullptr, st));
+	if constexpr (sizeof(T) == 4) {
+		if (l + 1 == s.fp32_levels) {  // FP32 -> FP64 hand-over: the coarse sub-cycle in FP64
+			CDR_TRY(restrict_2d_mixed(C.ci, F.r32, C.b, F.d, C.d, st));
+			CDR_CUDA_TRY(cudaMemsetAsync(C.x, 0, sizeof(double) * C.d.plane(), st));
+			if (l + 1 == L() - 1) CDR_TRY(coarse_solve<double>(C.x, C.b));
+			else if (l + 1 == lc[0]) CDR_TRY(fused<double>(l + 1));
+			else CDR_TRY(ncycle<double>(l + 1, C.x, C.b));
+			CDR_TRY(interp_add_2d_mixed(C.ci, C.x, F.r32, F.so32, x, F.d, C.d, st, F.ns));
+			return smooth<T>(l, x, b, CDR_UP);
+		}
+	}
 	CDR_TRY(restrict_2d<T>(Arr<T>::ci(C), Arr<T>::r(F), Arr<T>::b(C), F.d, C.d, st));
 	CDR_CUDA_TRY(cudaMemsetAsync(Arr<T>::x(C), 0, sizeof(T) * C.d.plane(), st));
 	if (l + 1 == L() - 1) CDR_TRY(coarse_solve<T>(Arr<T>::x(C), Arr<T>::b(C)));
@@ -332,8 +344,12 @@ int cdr_gpu_solver::tune_lines()
 	const bool lx = s.relaxation == CDR_RELAX_LINE_X || s.relaxation == CDR_RELAX_LINE_XY;
 	const bool ly = s.relaxation == CDR_RELAX_LINE_Y || s.relaxation == CDR_RELAX_LINE_XY;
 	const int f = lc[sizeof(T) == 4 ? 1 : 0];
-	const int stop = f >= 0 ? f : L() - 1;
-	for (int l = 0; l < stop; ++l) {
+	int lo = 0, stop = f >= 0 ? f : L() - 1;
+	if (mixed() && s.fp32_levels > 0) {  // FP32 on the finest fp32_levels levels, FP64 below
+		if (sizeof(T) == 4) stop = std::min(stop, s.fp32_levels);
+		else lo = s.fp32_levels;
+	}
+	for (int l = lo; l < stop; ++l) {
 		Level &F = lv[l];
 		if (lx)
 			CDR_TRY(lines_autotune<T>(Arr<T>::so(F), F.ns, Arr<T>::x(F), Arr<T>::b(F), Arr<T>::sor(F), F.d, F.tpitch,
@@ -440,6 +456,7 @@ int cdr_gpu_settings_default(cdr_gpu_settings *s)
 	s->fuse_coarse = 32;
 	s->krylov = CDR_KRYLOV_NONE;
 	s->coarse_solve = CDR_COARSE_BANDED;
+	s->fp32_levels = 0;
 	return CDR_OK;
 }
 
@@ -472,7 +489,9 @@ static int load_and_setup(cdr_gpu_solver *h, const double *so, int src_pitch, cu
 	CDR_CUDA_TRY(cudaEventElapsedTime(&h->setup_ms, h->ev0, h->ev1));
 	// launch shapes of the line kernels (once per shape and process; the sweeps
 	// run on the level arrays, which the solve reloads or overwrites)
-	return h->mixed() ? h->tune_lines<float>() : h->tune_lines<double>();
+	if (!h->mixed()) return h->tune_lines<double>();
+	CDR_TRY(h->tune_lines<float>());
+	return h->s.fp32_levels > 0 ? h->tune_lines<double>() : CDR_OK;
 }
 
 static int create_impl(cdr_gpu_solver *h, const double *so_src, int ns, int nx, int ny, int src_pitch,
@@ -575,6 +594,10 @@ static int create_any(const cdr_gpu_settings *s, const double *so_src, int ns, i
 	}
 	if (s->coarse_solve != CDR_COARSE_BANDED && s->coarse_solve != CDR_COARSE_INVERSE) {
 		set_error(CDR_ERR_ARG, "invalid coarse_solve %d", s->coarse_solve);
+		return CDR_ERR_ARG;
+	}
+	if (s->fp32_levels < 0) {
+		set_error(CDR_ERR_ARG, "invalid fp32_levels %d", s->fp32_levels);
 		return CDR_ERR_ARG;
 	}
 	*out = nullptr;

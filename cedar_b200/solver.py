@@ -49,6 +49,9 @@ def _settings(ms: MLSettings, dim=2):
         raise NotImplementedError("gpu.coarse-solve = %r is a 2D-solver option" % ms.coarse_solve)
     s.krylov = _lib.KRYLOV[ms.krylov]
     s.coarse_solve = _lib.COARSE[ms.coarse_solve]
+    if ms.fp32_levels and dim != 2:
+        raise NotImplementedError("gpu.fp32-levels is a 2D-solver option")
+    s.fp32_levels = ms.fp32_levels
     return s
 
 

@@ -259,6 +259,8 @@ typedef struct cdr_gpu_settings {
 	int fuse_coarse;  /* levels with both edges <= this run as one fused kernel (default 32, 0 = off) */
 	int krylov;       /* CDR_KRYLOV_NONE (default) or CDR_KRYLOV_FCG; 2D solver only    */
 	int coarse_solve; /* CDR_COARSE_BANDED (default) or CDR_COARSE_INVERSE; 2D solver only */
+	int fp32_levels;  /* CDR_PREC_F32_IR, 2D solver: the FP32 cycle runs this many finest levels in FP32 and
+	                     the coarser ones in FP64 (latency-bound there, so FP64 costs little); 0 = all (default) */
 } cdr_gpu_settings;
 
 typedef struct cdr_gpu_solver cdr_gpu_solver;

@@ -136,3 +136,23 @@ def test_exact_coarse_solve_speeds_up_fcg(oracle):
         assert s.history[-1] < 1e-3
         its[nl] = s.iters
     assert its[3] < its[-1]
+
+
+def test_fp32_levels_hybrid_cycle_converges(oracle):
+    """gpu.fp32-levels: the FP32 cycle keeps the finest levels in FP32 and runs
+    the coarser ones in FP64 (restriction into and interpolation from an FP64
+    level); fp32-levels at least the level count is the all-FP32 cycle."""
+    from cedar_b200.solver import Solver2D
+    n = 255
+    so, b = P.hetero_diffusion(n, sigma=1.0, n_incl=4, contrast=100.0, aniso=0.5)
+    hist = {}
+    for f32l in (0, 1, 2, 99):
+        s = Solver2D(so, Config({"solver": {"relaxation": "line-xy", "max-iter": 30, "tol": 1e-9},
+                                 "gpu": {"precision": "fp32-ir", "fp32-levels": f32l, "autotune": False}}))
+        x = s.solve(b)
+        assert s.history[-1] < 1e-9, f32l
+        r = oracle.residual(np.ascontiguousarray(so), x, b)
+        assert np.linalg.norm(r) / np.linalg.norm(b[1:-1, 1:-1]) < 1e-9
+        hist[f32l] = s.history.copy()
+    assert np.array_equal(hist[0], hist[99])
+    assert abs(len(hist[1]) - len(hist[0])) <= 2
