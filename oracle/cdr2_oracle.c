@@ -23,9 +23,11 @@
  *   DTBSV   upper band triangular solves used by DPBTRS.
  */
 #include <math.h>
+#include <pthread.h>
 #include <stdlib.h>
 #include <string.h>
 #include <stdio.h>
+#include <unistd.h>
 
 #include "cdr2_oracle.h"
 
@@ -40,6 +42,66 @@ static inline size_t ix2(long i, long j, long ii) { return (size_t)(j - 1) * ii 
 static inline size_t ix3(long i, long j, long k, long ii, long jj)
 {
 	return ((size_t)(k - 1) * jj + (j - 1)) * ii + (i - 1);
+}
+
+/* ------------------------------------------------------------------ */
+/* Host threads                                                        */
+/* ------------------------------------------------------------------ */
+/* The cycle kernels split independent rows, or lines of one colour, over the
+ * host's cores.  Every element receives the same operations whatever the
+ * split, so no result depends on the thread count.  ORACLE_THREADS (else
+ * OMP_NUM_THREADS, else the online CPUs) sets the count; grids under 2^18
+ * points stay on the calling thread. */
+typedef void (*o_task_fn)(void *ctx, int t);
+struct o_chunk {
+	o_task_fn fn;
+	void *ctx;
+	int t0, t1;
+};
+
+static void *o_chunk_run(void *p)
+{
+	struct o_chunk *c = (struct o_chunk *)p;
+	for (int t = c->t0; t < c->t1; ++t) c->fn(c->ctx, t);
+	return NULL;
+}
+
+int o_num_threads(void)
+{
+	static int n = 0;
+	if (!n) {
+		const char *e = getenv("ORACLE_THREADS");
+		if (!e) e = getenv("OMP_NUM_THREADS");
+		long v = e ? atol(e) : sysconf(_SC_NPROCESSORS_ONLN);
+		n = v < 1 ? 1 : v > 64 ? 64 : (int)v;
+	}
+	return n;
+}
+
+/* tasks 0..ntasks-1 of fn, over the threads when the grid has `points` points */
+static void o_parallel(int ntasks, long points, o_task_fn fn, void *ctx)
+{
+	int T = o_num_threads();
+	if (T > ntasks) T = ntasks;
+	if (T <= 1 || points < (1L << 18)) {
+		for (int t = 0; t < ntasks; ++t) fn(ctx, t);
+		return;
+	}
+	pthread_t th[64];
+	int ok[64];
+	struct o_chunk ch[64];
+	for (int k = 0; k < T; ++k) {
+		ch[k].fn = fn;
+		ch[k].ctx = ctx;
+		ch[k].t0 = (int)((long)ntasks * k / T);
+		ch[k].t1 = (int)((long)ntasks * (k + 1) / T);
+	}
+	for (int k = 1; k < T; ++k) ok[k] = pthread_create(&th[k], NULL, o_chunk_run, &ch[k]) == 0;
+	o_chunk_run(&ch[0]);
+	for (int k = 1; k < T; ++k) {
+		if (ok[k]) pthread_join(th[k], NULL);
+		else o_chunk_run(&ch[k]);
+	}
 }
 
 /* ------------------------------------------------------------------ */
@@ -139,42 +201,55 @@ void o_dpbtrs_u(int n, int kd, const double *ab, int ldab, double *x)
 /* 2D kernels (non-periodic boundary branch)                           */
 /* ------------------------------------------------------------------ */
 
-/* BMG2_SymStd_residual, src/2d/ftn/BMG2_SymStd_residual.f90:85-119 */
-void o2_residual(const double *so, const double *qf, const double *q, double *res,
-                 int II, int JJ, int ifd)
+struct o2_resid_ctx {
+	const double *so, *qf, *q;
+	double *res;
+	int II, JJ, ifd;
+};
+
+static void o2_residual_row(void *vc, int t)
 {
+	const struct o2_resid_ctx *c = (const struct o2_resid_ctx *)vc;
+	const double *so = c->so, *qf = c->qf, *q = c->q;
+	double *res = c->res;
+	const int II = c->II, JJ = c->JJ, I1 = II - 1, J = t + 2;
 #define SO(i, j, k) so[ix3(i, j, k, II, JJ)]
 #define Q(i, j) q[ix2(i, j, II)]
 #define QF(i, j) qf[ix2(i, j, II)]
 #define RES(i, j) res[ix2(i, j, II)]
-	int J1 = JJ - 1, I1 = II - 1;
-	if (ifd != 1) {
-		for (int J = 2; J <= J1; ++J)
-			for (int I = 2; I <= I1; ++I)
-				RES(I, J) = QF(I, J)
-				          + SO(I, J, KW) * Q(I - 1, J)
-				          + SO(I + 1, J, KW) * Q(I + 1, J)
-				          + SO(I, J, KS) * Q(I, J - 1)
-				          + SO(I, J + 1, KS) * Q(I, J + 1)
-				          + SO(I, J, KSW) * Q(I - 1, J - 1)
-				          + SO(I + 1, J, KNW) * Q(I + 1, J - 1)
-				          + SO(I, J + 1, KNW) * Q(I - 1, J + 1)
-				          + SO(I + 1, J + 1, KSW) * Q(I + 1, J + 1)
-				          - SO(I, J, KO) * Q(I, J);
+	if (c->ifd != 1) {
+		for (int I = 2; I <= I1; ++I)
+			RES(I, J) = QF(I, J)
+			          + SO(I, J, KW) * Q(I - 1, J)
+			          + SO(I + 1, J, KW) * Q(I + 1, J)
+			          + SO(I, J, KS) * Q(I, J - 1)
+			          + SO(I, J + 1, KS) * Q(I, J + 1)
+			          + SO(I, J, KSW) * Q(I - 1, J - 1)
+			          + SO(I + 1, J, KNW) * Q(I + 1, J - 1)
+			          + SO(I, J + 1, KNW) * Q(I - 1, J + 1)
+			          + SO(I + 1, J + 1, KSW) * Q(I + 1, J + 1)
+			          - SO(I, J, KO) * Q(I, J);
 	} else {
-		for (int J = 2; J <= J1; ++J)
-			for (int I = 2; I <= I1; ++I)
-				RES(I, J) = QF(I, J)
-				          + SO(I, J, KW) * Q(I - 1, J)
-				          + SO(I + 1, J, KW) * Q(I + 1, J)
-				          + SO(I, J, KS) * Q(I, J - 1)
-				          + SO(I, J + 1, KS) * Q(I, J + 1)
-				          - SO(I, J, KO) * Q(I, J);
+		for (int I = 2; I <= I1; ++I)
+			RES(I, J) = QF(I, J)
+			          + SO(I, J, KW) * Q(I - 1, J)
+			          + SO(I + 1, J, KW) * Q(I + 1, J)
+			          + SO(I, J, KS) * Q(I, J - 1)
+			          + SO(I, J + 1, KS) * Q(I, J + 1)
+			          - SO(I, J, KO) * Q(I, J);
 	}
 #undef SO
 #undef Q
 #undef QF
 #undef RES
+}
+
+/* BMG2_SymStd_residual, src/2d/ftn/BMG2_SymStd_residual.f90:85-119 (rows in any order) */
+void o2_residual(const double *so, const double *qf, const double *q, double *res,
+                 int II, int JJ, int ifd)
+{
+	struct o2_resid_ctx c = {so, qf, q, res, II, JJ, ifd};
+	o_parallel(JJ - 2, (long)II * JJ, o2_residual_row, &c);
 }
 
 /* BMG2_SymStd_SETUP_recip, src/2d/ftn/BMG2_SymStd_SETUP_recip.f90:63-67 (MSOR = 2) */
@@ -185,53 +260,81 @@ void o2_setup_recip(const double *so, double *sor, int II, int JJ)
 			sor[ix3(i, j, 2, II, JJ)] = 1.0 / so[ix3(i, j, KO, II, JJ)];
 }
 
-/* BMG2_SymStd_relax_GS, src/2d/ftn/BMG2_SymStd_relax_GS.f90:68-137 */
-void o2_relax_gs(const double *so, const double *qf, double *q, const double *sor,
-                 int II, int JJ, int ifd, int updown)
+struct o2_gs_ctx {
+	const double *so, *qf, *sor;
+	double *q;
+	int II, JJ, lstart, lend, lstride, beg;
+};
+
+/* 9-point: row J = beg + 2t of the row colour, both point colours in order */
+static void o2_gs9_row(void *vc, int t)
 {
+	const struct o2_gs_ctx *c = (const struct o2_gs_ctx *)vc;
+	const double *so = c->so, *qf = c->qf, *sor = c->sor;
+	double *q = c->q;
+	const int II = c->II, JJ = c->JJ, I1 = II - 1, J = c->beg + 2 * t;
 #define SO(i, j, k) so[ix3(i, j, k, II, JJ)]
 #define Q(i, j) q[ix2(i, j, II)]
 #define QF(i, j) qf[ix2(i, j, II)]
 #define SOR(i, j) sor[ix3(i, j, 2, II, JJ)]
-	int J1 = JJ - 1, I1 = II - 1;
-	int lstart, lend, lstride;
-	if (updown == BMG_DOWN) { lstart = 2; lend = 3; lstride = 1; }
-	else { lstart = 3; lend = 2; lstride = -1; }
-	if (ifd != 1) {
-		for (int JBEG = lstart; lstride > 0 ? JBEG <= lend : JBEG >= lend; JBEG += lstride) {
-			int JEND = 2 * ((J1 - JBEG) / 2) + JBEG;
-			for (int J = JBEG; J <= JEND; J += 2)
-				for (int IBEG = lstart; lstride > 0 ? IBEG <= lend : IBEG >= lend; IBEG += lstride) {
-					int IEND = 2 * ((I1 - IBEG) / 2) + IBEG;
-					for (int I = IBEG; I <= IEND; I += 2)
-						Q(I, J) = (QF(I, J)
-						           + SO(I, J, KW) * Q(I - 1, J)
-						           + SO(I + 1, J, KW) * Q(I + 1, J)
-						           + SO(I, J, KS) * Q(I, J - 1)
-						           + SO(I, J + 1, KS) * Q(I, J + 1)
-						           + SO(I, J, KSW) * Q(I - 1, J - 1)
-						           + SO(I + 1, J, KNW) * Q(I + 1, J - 1)
-						           + SO(I, J + 1, KNW) * Q(I - 1, J + 1)
-						           + SO(I + 1, J + 1, KSW) * Q(I + 1, J + 1)) * SOR(I, J);
-				}
-		}
-	} else {
-		for (int JO = lstart; lstride > 0 ? JO <= lend : JO >= lend; JO += lstride)
-			for (int J = 2; J <= J1; ++J) {
-				int IBEG = (J + JO) % 2 + 2;
-				int IEND = 2 * ((I1 - IBEG) / 2) + IBEG;
-				for (int I = IBEG; I <= IEND; I += 2)
-					Q(I, J) = (QF(I, J)
-					           + SO(I, J, KW) * Q(I - 1, J)
-					           + SO(I + 1, J, KW) * Q(I + 1, J)
-					           + SO(I, J, KS) * Q(I, J - 1)
-					           + SO(I, J + 1, KS) * Q(I, J + 1)) * SOR(I, J);
-			}
+	for (int IBEG = c->lstart; c->lstride > 0 ? IBEG <= c->lend : IBEG >= c->lend; IBEG += c->lstride) {
+		int IEND = 2 * ((I1 - IBEG) / 2) + IBEG;
+		for (int I = IBEG; I <= IEND; I += 2)
+			Q(I, J) = (QF(I, J)
+			           + SO(I, J, KW) * Q(I - 1, J)
+			           + SO(I + 1, J, KW) * Q(I + 1, J)
+			           + SO(I, J, KS) * Q(I, J - 1)
+			           + SO(I, J + 1, KS) * Q(I, J + 1)
+			           + SO(I, J, KSW) * Q(I - 1, J - 1)
+			           + SO(I + 1, J, KNW) * Q(I + 1, J - 1)
+			           + SO(I, J + 1, KNW) * Q(I - 1, J + 1)
+			           + SO(I + 1, J + 1, KSW) * Q(I + 1, J + 1)) * SOR(I, J);
 	}
+}
+
+/* 5-point: the colour-JO points of row J = t + 2 */
+static void o2_gs5_row(void *vc, int t)
+{
+	const struct o2_gs_ctx *c = (const struct o2_gs_ctx *)vc;
+	const double *so = c->so, *qf = c->qf, *sor = c->sor;
+	double *q = c->q;
+	const int II = c->II, JJ = c->JJ, I1 = II - 1, J = t + 2;
+	int IBEG = (J + c->beg) % 2 + 2;
+	int IEND = 2 * ((I1 - IBEG) / 2) + IBEG;
+	for (int I = IBEG; I <= IEND; I += 2)
+		Q(I, J) = (QF(I, J)
+		           + SO(I, J, KW) * Q(I - 1, J)
+		           + SO(I + 1, J, KW) * Q(I + 1, J)
+		           + SO(I, J, KS) * Q(I, J - 1)
+		           + SO(I, J + 1, KS) * Q(I, J + 1)) * SOR(I, J);
 #undef SO
 #undef Q
 #undef QF
 #undef SOR
+}
+
+/* BMG2_SymStd_relax_GS, src/2d/ftn/BMG2_SymStd_relax_GS.f90:68-137.  Rows of
+ * one row colour (9-point) or the points of one colour (5-point) read only
+ * the other colour: any order of them gives the same values. */
+void o2_relax_gs(const double *so, const double *qf, double *q, const double *sor,
+                 int II, int JJ, int ifd, int updown)
+{
+	int J1 = JJ - 1;
+	struct o2_gs_ctx c = {so, qf, sor, q, II, JJ, 0, 0, 0, 0};
+	if (updown == BMG_DOWN) { c.lstart = 2; c.lend = 3; c.lstride = 1; }
+	else { c.lstart = 3; c.lend = 2; c.lstride = -1; }
+	if (ifd != 1) {
+		for (int JBEG = c.lstart; c.lstride > 0 ? JBEG <= c.lend : JBEG >= c.lend; JBEG += c.lstride) {
+			int JEND = 2 * ((J1 - JBEG) / 2) + JBEG;
+			c.beg = JBEG;
+			o_parallel((JEND - JBEG) / 2 + 1, (long)II * JJ, o2_gs9_row, &c);
+		}
+	} else {
+		for (int JO = c.lstart; c.lstride > 0 ? JO <= c.lend : JO >= c.lend; JO += c.lstride) {
+			c.beg = JO;
+			o_parallel(JJ - 2, (long)II * JJ, o2_gs5_row, &c);
+		}
+	}
 }
 
 /* BMG2_SymStd_SETUP_lines_x, src/2d/ftn/BMG2_SymStd_SETUP_lines_x.f90:68-87.
@@ -268,33 +371,77 @@ int o2_setup_lines_y(const double *so, double *sor, int Nx, int Ny)
 	return info;
 }
 
-/* BMG2_SymStd_relax_lines_x, src/2d/ftn/BMG2_SymStd_relax_lines_x.f90:74-131 */
-void o2_relax_lines_x(const double *so, const double *qf, double *q, const double *sor,
-                      int II, int JJ, int ifd, int updown)
+struct o2_lines_ctx {
+	const double *so, *qf, *sor;
+	double *q;
+	int II, JJ, ifd, beg;
+};
+
+/* x-line J = beg + 2t: right-hand side into Q(., J), then DPTTRS */
+static void o2_xline(void *vc, int t)
 {
+	const struct o2_lines_ctx *c = (const struct o2_lines_ctx *)vc;
+	const double *so = c->so, *qf = c->qf, *sor = c->sor;
+	double *q = c->q;
+	const int II = c->II, JJ = c->JJ, I1 = II - 1, J = c->beg + 2 * t;
 #define SO(i, j, k) so[ix3(i, j, k, II, JJ)]
 #define Q(i, j) q[ix2(i, j, II)]
 #define QF(i, j) qf[ix2(i, j, II)]
-	int J1 = JJ - 1, I1 = II - 1;
+	if (c->ifd != 1) {
+		for (int I = 2; I <= I1; ++I)
+			Q(I, J) = QF(I, J) + SO(I, J, KS) * Q(I, J - 1) + SO(I, J + 1, KS) * Q(I, J + 1)
+			        + SO(I, J, KSW) * Q(I - 1, J - 1) + SO(I + 1, J, KNW) * Q(I + 1, J - 1)
+			        + SO(I, J + 1, KNW) * Q(I - 1, J + 1) + SO(I + 1, J + 1, KSW) * Q(I + 1, J + 1);
+	} else {
+		for (int I = 2; I <= I1; ++I)
+			Q(I, J) = QF(I, J) + SO(I, J, KS) * Q(I, J - 1) + SO(I, J + 1, KS) * Q(I, J + 1);
+	}
+	o_dpttrs(I1 - 1, &sor[ix3(2, J, 1, II, JJ)], &sor[ix3(3, J, 2, II, JJ)], &Q(2, J));
+#undef SO
+#undef Q
+#undef QF
+}
+
+/* BMG2_SymStd_relax_lines_x, src/2d/ftn/BMG2_SymStd_relax_lines_x.f90:74-131.
+ * The reference forms all right-hand sides of a colour, then solves; lines of
+ * one colour read only the other colour, so line by line gives the same. */
+void o2_relax_lines_x(const double *so, const double *qf, double *q, const double *sor,
+                      int II, int JJ, int ifd, int updown)
+{
+	int J1 = JJ - 1;
 	int jstart, jend, jstride;
 	if (updown == BMG_DOWN) { jstart = 3; jend = 2; jstride = -1; }
 	else { jstart = 2; jend = 3; jstride = 1; }
+	struct o2_lines_ctx c = {so, qf, sor, q, II, JJ, ifd, 0};
 	for (int JBEG = jstart; jstride > 0 ? JBEG <= jend : JBEG >= jend; JBEG += jstride) {
 		int JEND = 2 * ((J1 - JBEG) / 2) + JBEG;
-		for (int J = JBEG; J <= JEND; J += 2) {
-			if (ifd != 1) {
-				for (int I = 2; I <= I1; ++I)
-					Q(I, J) = QF(I, J) + SO(I, J, KS) * Q(I, J - 1) + SO(I, J + 1, KS) * Q(I, J + 1)
-					        + SO(I, J, KSW) * Q(I - 1, J - 1) + SO(I + 1, J, KNW) * Q(I + 1, J - 1)
-					        + SO(I, J + 1, KNW) * Q(I - 1, J + 1) + SO(I + 1, J + 1, KSW) * Q(I + 1, J + 1);
-			} else {
-				for (int I = 2; I <= I1; ++I)
-					Q(I, J) = QF(I, J) + SO(I, J, KS) * Q(I, J - 1) + SO(I, J + 1, KS) * Q(I, J + 1);
-			}
-		}
-		for (int J = JBEG; J <= JEND; J += 2)
-			o_dpttrs(I1 - 1, &sor[ix3(2, J, 1, II, JJ)], &sor[ix3(3, J, 2, II, JJ)], &Q(2, J));
+		c.beg = JBEG;
+		o_parallel((JEND - JBEG) / 2 + 1, (long)II * JJ, o2_xline, &c);
 	}
+}
+
+/* y-line I = beg + 2t: right-hand side into a line buffer, DPTTRS, copy back */
+static void o2_yline(void *vc, int t)
+{
+	const struct o2_lines_ctx *c = (const struct o2_lines_ctx *)vc;
+	const double *so = c->so, *qf = c->qf, *sor = c->sor;
+	double *q = c->q;
+	const int II = c->II, JJ = c->JJ, J1 = JJ - 1, I = c->beg + 2 * t;
+	double *B = (double *)malloc(sizeof(double) * (size_t)JJ);
+#define SO(i, j, k) so[ix3(i, j, k, II, JJ)]
+#define Q(i, j) q[ix2(i, j, II)]
+#define QF(i, j) qf[ix2(i, j, II)]
+	for (int J = 2; J <= J1; ++J) {
+		if (c->ifd != 1)
+			B[J - 1] = QF(I, J) + SO(I, J, KW) * Q(I - 1, J) + SO(I + 1, J, KW) * Q(I + 1, J)
+			         + SO(I, J, KSW) * Q(I - 1, J - 1) + SO(I + 1, J, KNW) * Q(I + 1, J - 1)
+			         + SO(I, J + 1, KNW) * Q(I - 1, J + 1) + SO(I + 1, J + 1, KSW) * Q(I + 1, J + 1);
+		else
+			B[J - 1] = QF(I, J) + SO(I, J, KW) * Q(I - 1, J) + SO(I + 1, J, KW) * Q(I + 1, J);
+	}
+	o_dpttrs(J1 - 1, &sor[ix3(2, I, 1, JJ, II)], &sor[ix3(3, I, 2, JJ, II)], &B[1]);
+	for (int J = 2; J <= J1; ++J) Q(I, J) = B[J - 1];
+	free(B);
 #undef SO
 #undef Q
 #undef QF
@@ -306,81 +453,117 @@ void o2_relax_lines_x(const double *so, const double *qf, double *q, const doubl
 void o2_relax_lines_y(const double *so, const double *qf, double *q, const double *sor,
                       int II, int JJ, int ifd, int updown)
 {
-#define SO(i, j, k) so[ix3(i, j, k, II, JJ)]
-#define Q(i, j) q[ix2(i, j, II)]
-#define QF(i, j) qf[ix2(i, j, II)]
-	int J1 = JJ - 1, I1 = II - 1;
-	double *B = (double *)calloc((size_t)2 * JJ, sizeof(double));
+	int I1 = II - 1;
 	int istart, iend, istride;
 	if (updown == BMG_DOWN) { istart = 3; iend = 2; istride = -1; }
 	else { istart = 2; iend = 3; istride = 1; }
+	struct o2_lines_ctx c = {so, qf, sor, q, II, JJ, ifd, 0};
 	for (int IBEG = istart; istride > 0 ? IBEG <= iend : IBEG >= iend; IBEG += istride) {
 		int IEND = 2 * ((I1 - IBEG) / 2) + IBEG;
-		for (int I = IBEG; I <= IEND; I += 2) {
-			for (int J = 2; J <= J1; ++J) {
-				if (ifd != 1)
-					B[J - 1] = QF(I, J) + SO(I, J, KW) * Q(I - 1, J) + SO(I + 1, J, KW) * Q(I + 1, J)
-					         + SO(I, J, KSW) * Q(I - 1, J - 1) + SO(I + 1, J, KNW) * Q(I + 1, J - 1)
-					         + SO(I, J + 1, KNW) * Q(I - 1, J + 1) + SO(I + 1, J + 1, KSW) * Q(I + 1, J + 1);
-				else
-					B[J - 1] = QF(I, J) + SO(I, J, KW) * Q(I - 1, J) + SO(I + 1, J, KW) * Q(I + 1, J);
-			}
-			o_dpttrs(J1 - 1, &sor[ix3(2, I, 1, JJ, II)], &sor[ix3(3, I, 2, JJ, II)], &B[1]);
-			for (int J = 2; J <= J1; ++J) Q(I, J) = B[J - 1];
-		}
+		c.beg = IBEG;
+		o_parallel((IEND - IBEG) / 2 + 1, (long)II * JJ, o2_yline, &c);
 	}
-	free(B);
-#undef SO
+}
+
+struct o2_restrict_ctx {
+	const double *ci, *q;
+	double *qc;
+	int Nx, Nxc, Nyc;
+};
+
+static void o2_restrict_row(void *vc, int t)
+{
+	const struct o2_restrict_ctx *c = (const struct o2_restrict_ctx *)vc;
+	const double *ci = c->ci, *q = c->q;
+	double *qc = c->qc;
+	const int Nx = c->Nx, Nxc = c->Nxc, Nyc = c->Nyc, jc = t + 2, j = 2 * jc - 2;
+#define CI(i, j, k) ci[ix3(i, j, k, Nxc, Nyc)]
+#define Q(i, j) q[ix2(i, j, Nx)]
+#define QC(i, j) qc[ix2(i, j, Nxc)]
+	for (int ic = 2; ic <= Nxc - 1; ++ic) {
+		const int i = 2 * ic - 2;
+		QC(ic, jc) = CI(ic, jc, LNE) * Q(i - 1, j - 1)
+		           + CI(ic, jc, LA) * Q(i, j - 1)
+		           + CI(ic + 1, jc, LNW) * Q(i + 1, j - 1)
+		           + CI(ic, jc, LR) * Q(i - 1, j)
+		           + Q(i, j)
+		           + CI(ic + 1, jc, LL) * Q(i + 1, j)
+		           + CI(ic, jc + 1, LSE) * Q(i - 1, j + 1)
+		           + CI(ic, jc + 1, LB) * Q(i, j + 1)
+		           + CI(ic + 1, jc + 1, LSW) * Q(i + 1, j + 1);
+	}
+#undef CI
 #undef Q
-#undef QF
+#undef QC
 }
 
 /* BMG2_SymStd_restrict, src/2d/ftn/BMG2_SymStd_restrict.f90:72-92 */
 void o2_restrict(const double *ci, const double *q, double *qc,
                  int Nx, int Ny, int Nxc, int Nyc)
 {
-#define CI(i, j, k) ci[ix3(i, j, k, Nxc, Nyc)]
-#define Q(i, j) q[ix2(i, j, Nx)]
-#define QC(i, j) qc[ix2(i, j, Nxc)]
-	int j = 0;
-	for (int jc = 2; jc <= Nyc - 1; ++jc) {
-		j += 2;
-		int i = 0;
-		for (int ic = 2; ic <= Nxc - 1; ++ic) {
-			i += 2;
-			QC(ic, jc) = CI(ic, jc, LNE) * Q(i - 1, j - 1)
-			           + CI(ic, jc, LA) * Q(i, j - 1)
-			           + CI(ic + 1, jc, LNW) * Q(i + 1, j - 1)
-			           + CI(ic, jc, LR) * Q(i - 1, j)
-			           + Q(i, j)
-			           + CI(ic + 1, jc, LL) * Q(i + 1, j)
-			           + CI(ic, jc + 1, LSE) * Q(i - 1, j + 1)
-			           + CI(ic, jc + 1, LB) * Q(i, j + 1)
-			           + CI(ic + 1, jc + 1, LSW) * Q(i + 1, j + 1);
-		}
-	}
-	(void)Ny;
-#undef CI
-#undef Q
-#undef QC
+	struct o2_restrict_ctx c = {ci, q, qc, Nx, Nxc, Nyc};
+	o_parallel(Nyc - 2, (long)Nx * Ny, o2_restrict_row, &c);
 }
 
-/* BMG2_SymStd_interp_add, src/2d/ftn/BMG2_SymStd_interp_add.f90:89-137.
- * so_ko points at the fine operator's KO plane; res is divided in place. */
-void o2_interp_add(double *q, const double *qc, double *res, const double *so_ko,
-                   const double *ci, int IIC, int JJC, int IIF, int JJF)
-{
+struct o2_interp_ctx {
+	double *q, *res;
+	const double *qc, *so_ko, *ci;
+	int IIC, JJC, IIF, JJF;
+};
+
 #define CI(i, j, k) ci[ix3(i, j, k, IIC, JJC)]
 #define Q(i, j) q[ix2(i, j, IIF)]
 #define QC(i, j) qc[ix2(i, j, IIC)]
 #define RES(i, j) res[ix2(i, j, IIF)]
 #define SOKO(i, j) so_ko[ix2(i, j, IIF)]
-	int JJF1 = JJF - 1, IIF1 = IIF - 1;
+#define O2_INTERP_UNPACK                                                      \
+	const struct o2_interp_ctx *c = (const struct o2_interp_ctx *)vc;        \
+	double *q = c->q, *res = c->res;                                          \
+	const double *qc = c->qc, *so_ko = c->so_ko, *ci = c->ci;                 \
+	const int IIC = c->IIC, JJC = c->JJC, IIF = c->IIF;                       \
+	(void)so_ko; (void)ci; (void)qc; (void)JJC
+
+/* RES <- RES/c on fine row J = t + 2 */
+static void o2_interp_div_row(void *vc, int t)
+{
+	O2_INTERP_UNPACK;
+	const int J = t + 2;
+	for (int I = 2; I <= IIF - 1; ++I) RES(I, J) = RES(I, J) / SOKO(I, J);
+}
+
+/* coarse row JC = t + 3: fine rows 2JC-2 and 2JC-3 */
+static void o2_interp_row(void *vc, int t)
+{
+	O2_INTERP_UNPACK;
+	const int IICF1 = (IIF - 2) / 2 + 2, JC = t + 3, J = 2 * JC - 2;
+	int I = 2;
+	Q(2, J) = Q(2, J) + QC(2, JC);
+	double AQ = CI(2, JC, LA) * QC(2, JC) + CI(2, JC, LB) * QC(2, JC - 1);
+	Q(2, J - 1) = Q(2, J - 1) + AQ + RES(2, J - 1);
+	for (int IC = 3; IC <= IICF1; ++IC) {
+		I += 2;
+		Q(I, J) = Q(I, J) + QC(IC, JC);
+		double A = CI(IC, JC, LR) * QC(IC, JC) + CI(IC, JC, LL) * QC(IC - 1, JC);
+		Q(I - 1, J) = Q(I - 1, J) + A + RES(I - 1, J);
+		AQ = CI(IC, JC, LA) * QC(IC, JC) + CI(IC, JC, LB) * QC(IC, JC - 1);
+		Q(I, J - 1) = Q(I, J - 1) + AQ + RES(I, J - 1);
+		A = CI(IC, JC, LSW) * QC(IC - 1, JC - 1) + CI(IC, JC, LNW) * QC(IC - 1, JC)
+		  + CI(IC, JC, LNE) * QC(IC, JC) + CI(IC, JC, LSE) * QC(IC, JC - 1);
+		Q(I - 1, J - 1) = Q(I - 1, J - 1) + A + RES(I - 1, J - 1);
+	}
+}
+
+/* BMG2_SymStd_interp_add, src/2d/ftn/BMG2_SymStd_interp_add.f90:89-137.
+ * so_ko points at the fine operator's KO plane; res is divided in place.
+ * Coarse row JC writes only fine rows 2JC-2 and 2JC-3, so rows may run in
+ * any order. */
+void o2_interp_add(double *q, const double *qc, double *res, const double *so_ko,
+                   const double *ci, int IIC, int JJC, int IIF, int JJF)
+{
+	struct o2_interp_ctx c = {q, res, qc, so_ko, ci, IIC, JJC, IIF, JJF};
+	o_parallel(JJF - 2, (long)IIF * JJF, o2_interp_div_row, &c);
 	int IICF = (IIF - 2) / 2 + 3, JJCF = (JJF - 2) / 2 + 3;
 	int IICF1 = IICF - 1, JJCF1 = JJCF - 1;
-	for (int J = 2; J <= JJF1; ++J)
-		for (int I = 2; I <= IIF1; ++I)
-			RES(I, J) = RES(I, J) / SOKO(I, J);
 	int J = 2, I = 2;
 	Q(2, J) = Q(2, J) + QC(2, 2);
 	for (int IC = 3; IC <= IICF1; ++IC) {
@@ -389,30 +572,14 @@ void o2_interp_add(double *q, const double *qc, double *res, const double *so_ko
 		double A = CI(IC, 2, LR) * QC(IC, 2) + CI(IC, 2, LL) * QC(IC - 1, 2);
 		Q(I - 1, J) = Q(I - 1, J) + A + RES(I - 1, J);
 	}
-	for (int JC = 3; JC <= JJCF1; ++JC) {
-		J += 2;
-		I = 2;
-		Q(2, J) = Q(2, J) + QC(2, JC);
-		double AQ = CI(2, JC, LA) * QC(2, JC) + CI(2, JC, LB) * QC(2, JC - 1);
-		Q(2, J - 1) = Q(2, J - 1) + AQ + RES(2, J - 1);
-		for (int IC = 3; IC <= IICF1; ++IC) {
-			I += 2;
-			Q(I, J) = Q(I, J) + QC(IC, JC);
-			double A = CI(IC, JC, LR) * QC(IC, JC) + CI(IC, JC, LL) * QC(IC - 1, JC);
-			Q(I - 1, J) = Q(I - 1, J) + A + RES(I - 1, J);
-			AQ = CI(IC, JC, LA) * QC(IC, JC) + CI(IC, JC, LB) * QC(IC, JC - 1);
-			Q(I, J - 1) = Q(I, J - 1) + AQ + RES(I, J - 1);
-			A = CI(IC, JC, LSW) * QC(IC - 1, JC - 1) + CI(IC, JC, LNW) * QC(IC - 1, JC)
-			  + CI(IC, JC, LNE) * QC(IC, JC) + CI(IC, JC, LSE) * QC(IC, JC - 1);
-			Q(I - 1, J - 1) = Q(I - 1, J - 1) + A + RES(I - 1, J - 1);
-		}
-	}
+	if (JJCF1 >= 3) o_parallel(JJCF1 - 2, (long)IIF * JJF, o2_interp_row, &c);
+}
 #undef CI
 #undef Q
 #undef QC
 #undef RES
 #undef SOKO
-}
+#undef O2_INTERP_UNPACK
 
 /* BMG2_SymStd_SETUP_interp_OI, src/2d/ftn/BMG2_SymStd_SETUP_interp_OI.f90:85-257
  * (non-periodic).  emach = D1MACH(3) = 2^-53 (src/2d/ftn/util.f90:58-66). */

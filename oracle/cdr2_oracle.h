@@ -52,6 +52,7 @@ o2_solver *o2_create(const o2_settings *s, const double *so_fine, int nstncl, in
 void o2_destroy(o2_solver *h);
 void o2_vcycle(o2_solver *h, double *x, const double *b);
 int o2_solve(o2_solver *h, const double *b, double *x, double *hist, int maxhist);
+int o_num_threads(void);
 int o2_nlevels(const o2_solver *h);
 int o2_info(const o2_solver *h, int which);
 void o2_level_dims(const o2_solver *h, int l, int *dims);

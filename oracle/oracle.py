@@ -70,6 +70,7 @@ def lib(variant=""):
             "o2_vcycle": (None, [P, P, P]),
             "o2_solve": (I, [P, P, P, P, I]),
             "o2_nlevels": (I, [P]),
+            "o_num_threads": (I, []),
             "o2_info": (I, [P, I]),
             "o2_level_dims": (None, [P, P]),
             "o2_level_array": (ctypes.POINTER(ctypes.c_double), [P, I, I]),
@@ -232,6 +233,11 @@ def num_levels(nx, ny, min_coarse=3):
 
 
 # ------------------------------------------------------------------ solver
+def num_threads():
+    """Host threads the oracle's cycle kernels use (ORACLE_THREADS / OMP_NUM_THREADS / online CPUs)."""
+    return lib().o_num_threads()
+
+
 class Solver:
     """Serial BoxMG solver: setup in the constructor, as ``cdr2::solver``."""
 

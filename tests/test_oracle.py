@@ -421,3 +421,34 @@ def test_3d_seven_point_boxmg_converges_both_smoothers(oracle):
     _, h0 = oracle.Solver3(so, maxiter=20, tol=1e-10).solve(b)
     _, hp = oracle.Solver3(so, maxiter=20, tol=1e-10, relax="plane-xyz").solve(b)
     assert h0[-1] < 1e-10 and hp[-1] < 1e-10 and len(hp) <= len(h0)
+
+
+_THREAD_PROBE = r"""
+import hashlib, sys
+sys.path.insert(0, sys.argv[1])
+from oracle import oracle
+from cedar_b200 import problems as P
+so, b = P.hetero_diffusion(767, sigma=1.0, n_incl=4, contrast=100.0, aniso=0.5)
+out = [str(oracle.num_threads())]
+for relax in ("line-xy", "point"):
+    x, h = oracle.Solver(so, relax=relax, maxiter=2, tol=0).solve(b)
+    out.append(hashlib.sha256(x.tobytes()).hexdigest())
+print(" ".join(out))
+"""
+
+
+def test_oracle_threads_do_not_change_results(oracle):
+    """The 2D cycle kernels split rows / lines of one colour over host threads
+    (ORACLE_THREADS); every element gets the same operations, so one thread
+    and four give the same bits (767^2 is above the threading threshold)."""
+    import os
+    import subprocess
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    res = {}
+    for t in ("1", "4"):
+        p = subprocess.run([sys.executable, "-c", _THREAD_PROBE, root], env=dict(os.environ, ORACLE_THREADS=t),
+                           capture_output=True, text=True, check=True, timeout=300)
+        res[t] = p.stdout.split()
+    assert res["1"][0] == "1" and res["4"][0] == "4"
+    assert res["1"][1:] == res["4"][1:]
