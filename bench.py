@@ -367,6 +367,10 @@ def main():
         out["batch512"] = batch_leg()
         out["cpu_baseline"] = cpu_arm(args, so, b, it64, "config above", nlev)
         del out["cpu_baseline"]["setup_ms"], out["cpu_baseline"]["ms_per_cycle"]
+    elif world > 1 and not args.no_extras:
+        bl = batch_leg(dist=dist)  # every rank: its share of the work list
+        if rank == 0:
+            out["batch512"] = bl
     if rank == 0:
         print(json.dumps(out), flush=True)
     for v in plain.values():
@@ -510,15 +514,6 @@ def hetero3_leg(stream, n=255):
     return res
 
 
-def batch_sizes(count=512, seed=7):
-    """Edge sizes of the batched workload: drawn from {63,127,255,511,1023} with weights 8:4:2:1:1."""
-    import numpy as np
-    rng = np.random.default_rng(seed)
-    sizes = np.array([63, 127, 255, 511, 1023])
-    w = np.array([8, 4, 2, 1, 1], dtype=float)
-    return rng.choice(sizes, size=count, p=w / w.sum())
-
-
 def batch_class_problems(n, ids, pitch, ell=1.0 / 32, sigma=1.0):
     """Device operators and right-hand sides of the problems ``ids`` (edge n):
     lognormal cell coefficient (Gaussian field by FFT synthesis on the doubled
@@ -548,26 +543,34 @@ def batch_class_problems(n, ids, pitch, ell=1.0 / 32, sigma=1.0):
     return so, b
 
 
-def batch_leg(count=512):
+def batch_leg(count=512, dist=None):
     """512 independent 9-point problems, sizes 63..1023, FP32 V(1,1) line-xy cycles
-    inside FP64 refinement to 1e-8 per problem; one batch per size, the five
-    batches solved concurrently (one stream and host thread each)."""
+    inside FP64 refinement to 1e-8 per problem; one batch per size, the batches
+    of a rank solved concurrently (one stream and host thread each).  With a
+    process group the work list is split over the ranks by estimated cost
+    (cedar_b200.shard; no collective on the data path), and the per-problem
+    statistics are gathered at the end."""
     import threading
     import numpy as np
     import torch
+    from cedar_b200 import problems as P, shard
     from cedar_b200.config import Config
     from cedar_b200.solver import BatchSolver2D
-    sizes = batch_sizes(count)
+    world = dist.get_world_size() if dist else 1
+    rank = dist.get_rank() if dist else 0
+    sizes = P.batch_sizes(count)
+    parts = shard.partition(sizes, world)
+    mine = np.array(parts[rank], dtype=np.int64)
     conf = Config({"solver": {"relaxation": "line-xy", "cycle": {"nrelax-pre": 1, "nrelax-post": 1},
                               "max-iter": 60, "tol": 1e-8}, "gpu": {"precision": "fp32-ir"}})
     classes = []
-    for n in sorted(set(int(v) for v in sizes)):
-        ids = np.nonzero(sizes == n)[0]
+    for n in sorted(set(int(v) for v in sizes[mine])):
+        ids = mine[sizes[mine] == n]
         pitch = ((n + 2 + 15) // 16) * 16
         so, b = batch_class_problems(n, ids, pitch)
         st = torch.cuda.Stream()
         s = BatchSolver2D(so.data_ptr(), 5, n, n, pitch, len(ids), conf, stream=st.cuda_stream)
-        classes.append({"n": n, "count": len(ids), "so": so, "b": b, "x": torch.zeros_like(b), "s": s,
+        classes.append({"n": n, "ids": ids, "count": len(ids), "so": so, "b": b, "x": torch.zeros_like(b), "s": s,
                         "stream": st, "pitch": pitch})
 
     def run(c):
@@ -581,6 +584,8 @@ def batch_leg(count=512):
     for c in classes:
         c["x"].zero_()
     torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
     t0 = time.perf_counter()
     threads = [threading.Thread(target=lambda c=c: c["s"].solve_device(c["b"].data_ptr(), c["x"].data_ptr(),
                                                                        c["pitch"])) for c in classes]
@@ -590,21 +595,33 @@ def batch_leg(count=512):
         t.join()
     torch.cuda.synchronize()
     wall_ms = (time.perf_counter() - t0) * 1e3
-    done = np.concatenate([c["s"].done_ms.copy() for c in classes])
-    rel = np.concatenate([c["s"].rel.copy() for c in classes])
-    its = np.concatenate([c["s"].iters.copy() for c in classes])
+    if dist:
+        w = torch.tensor([wall_ms], device="cuda")
+        dist.all_reduce(w, op=dist.ReduceOp.MAX)
+        wall_ms = float(w.item())
+    ids = np.concatenate([c["ids"] for c in classes]) if classes else np.zeros(0, np.int64)
+    stats = np.stack([np.concatenate([c["s"].done_ms.copy() for c in classes]),
+                      np.concatenate([c["s"].rel.copy() for c in classes]),
+                      np.concatenate([c["s"].iters.copy() for c in classes]).astype(float)], axis=1) \
+        if classes else np.zeros((0, 3))
+    table = shard.gather_stats(ids, stats, dist)
+    done, rel, its = table[:, 0], table[:, 1], table[:, 2]
     per_class = {str(c["n"]): {"problems": c["count"], "solve_ms": c["s"].timings()[1],
                                "setup_ms": c["s"].timings()[0], "max_cycles": int(c["s"].iters.max())}
                  for c in classes}
     for c in classes:
         c["s"].close()
-    return {"workload": "%d independent 9-point FE problems, edges {63,127,255,511,1023} weights 8:4:2:1:1 "
-                        "(seed 7), lognormal k sigma=1 ell=1/32 (CUDA generator 1000+id), b=U[0,1]h^2; FP32 V(1,1) "
-                        "line-xy + FP64 IR to 1e-8 per problem; one batch per size, 5 concurrent streams" % count,
-            "problems_per_s": count / (wall_ms * 1e-3), "batch_ms": wall_ms, "timing": "host wall clock around "
-            "the concurrent solves (device-synchronised both sides); per-problem times from CUDA events",
-            "p50_ms": float(np.percentile(done, 50)), "p99_ms": float(np.percentile(done, 99)),
-            "all_converged": bool(np.all(rel < 1e-8)), "max_cycles": int(its.max()), "per_size": per_class}
+    out = {"workload": "%d independent 9-point FE problems, edges {63,127,255,511,1023} weights 8:4:2:1:1 "
+                       "(seed 7), lognormal k sigma=1 ell=1/32 (CUDA generator 1000+id), b=U[0,1]h^2; FP32 V(1,1) "
+                       "line-xy + FP64 IR to 1e-8 per problem; one batch per size, concurrent streams" % count,
+           "problems_per_s": count / (wall_ms * 1e-3), "batch_ms": wall_ms, "timing": "host wall clock around "
+           "the concurrent solves (device-synchronised both sides, max over ranks); per-problem times from CUDA "
+           "events", "p50_ms": float(np.percentile(done, 50)), "p99_ms": float(np.percentile(done, 99)),
+           "all_converged": bool(np.all(rel < 1e-8)), "max_cycles": int(its.max()), "ranks": world,
+           "rank_cost_share": [round(v / max(1, sum(shard.loads(sizes, parts))), 4) for v in shard.loads(sizes, parts)]}
+    if world == 1:
+        out["per_size"] = per_class
+    return out
 
 
 def to_1e10(args, stream):

@@ -173,3 +173,11 @@ def hetero3_rhs(n, seed=6):
     b = np.zeros((n + 2, n + 2, n + 2))
     b[1:-1, 1:-1, 1:-1] = rng.uniform(-1.0, 1.0, size=(n, n, n)) * h ** 3
     return b
+
+
+def batch_sizes(count=512, seed=7):
+    """Edge sizes of the batched workload: drawn from {63,127,255,511,1023} with weights 8:4:2:1:1."""
+    rng = np.random.default_rng(seed)
+    sizes = np.array([63, 127, 255, 511, 1023])
+    w = np.array([8, 4, 2, 1, 1], dtype=float)
+    return rng.choice(sizes, size=count, p=w / w.sum())
