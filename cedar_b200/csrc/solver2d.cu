@@ -99,6 +99,8 @@ struct cdr_gpu_solver {
 	int cycle(T *x, const T *b);
 	template <typename T>
 	int coarse_solve(T *x, const T *b);
+	template <typename T>
+	int fcycle(int l, T *x, const T *b);
 	int run_cycle(int prec);
 	template <typename T>
 	int fcg_iteration();
@@ -256,10 +258,25 @@ int cdr_gpu_solver::coarse_solve(T *x, const T *b)
 	return solve_cg_2d<T>(abd, x, b, d, st);
 }
 
+// cycle::fcycle::fmg_cycle / fmg_cycle_helper (include/cedar/cycle/fcycle.h:49-83)
+template <typename T>
+int cdr_gpu_solver::fcycle(int l, T *x, const T *b)
+{
+	if (l == L() - 1) return coarse_solve<T>(x, b);
+	Level &F = lv[l], &C = lv[l + 1];
+	CDR_TRY(restrict_2d<T>(Arr<T>::ci(C), b, Arr<T>::b(C), F.d, C.d, st));
+	CDR_TRY(fcycle<T>(l + 1, Arr<T>::x(C), Arr<T>::b(C)));
+	CDR_CUDA_TRY(cudaMemsetAsync(x, 0, sizeof(T) * F.d.plane(), st));
+	CDR_CUDA_TRY(cudaMemsetAsync(Arr<T>::r(F), 0, sizeof(T) * F.d.plane(), st));
+	CDR_TRY(interp_add_2d<T>(Arr<T>::ci(C), Arr<T>::x(C), Arr<T>::r(F), Arr<T>::so(F), x, F.d, C.d, st, F.ns));
+	return ncycle<T>(l, x, b);
+}
+
 template <typename T>
 int cdr_gpu_solver::cycle(T *x, const T *b)
 {
 	if (L() == 1) return coarse_solve<T>(x, b);
+	if (s.cycle == CDR_CYCLE_F) return fcycle<T>(0, x, b);
 	return ncycle<T>(0, x, b);
 }
 
@@ -457,6 +474,7 @@ int cdr_gpu_settings_default(cdr_gpu_settings *s)
 	s->krylov = CDR_KRYLOV_NONE;
 	s->coarse_solve = CDR_COARSE_BANDED;
 	s->fp32_levels = 0;
+	s->cycle = CDR_CYCLE_V;
 	return CDR_OK;
 }
 
@@ -598,6 +616,10 @@ static int create_any(const cdr_gpu_settings *s, const double *so_src, int ns, i
 	}
 	if (s->fp32_levels < 0) {
 		set_error(CDR_ERR_ARG, "invalid fp32_levels %d", s->fp32_levels);
+		return CDR_ERR_ARG;
+	}
+	if (s->cycle != CDR_CYCLE_V && s->cycle != CDR_CYCLE_F) {
+		set_error(CDR_ERR_ARG, "invalid cycle type %d", s->cycle);
 		return CDR_ERR_ARG;
 	}
 	*out = nullptr;

@@ -426,7 +426,8 @@ static int create3_any(const cdr_gpu_settings *s, const double *so_src, int src_
 		set_error(CDR_ERR_ARG, "invalid precision %d", s->precision);
 		return CDR_ERR_ARG;
 	}
-	if (s->krylov != CDR_KRYLOV_NONE || s->coarse_solve != CDR_COARSE_BANDED || s->fp32_levels != 0) {
+	if (s->krylov != CDR_KRYLOV_NONE || s->coarse_solve != CDR_COARSE_BANDED || s->fp32_levels != 0 ||
+	    s->cycle != CDR_CYCLE_V) {
 		set_error(CDR_ERR_UNSUPPORTED, "3D solver: the Krylov outer iteration is implemented for the 2D solver only");
 		return CDR_ERR_UNSUPPORTED;
 	}

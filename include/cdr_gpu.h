@@ -74,6 +74,14 @@ extern "C" {
 #define CDR_COARSE_BANDED  0
 #define CDR_COARSE_INVERSE 1
 
+/* Cycle type (ml_settings::cycle_type, include/cedar/multilevel_settings.h:32):
+ * CDR_CYCLE_F runs cycle::fcycle (include/cedar/cycle/fcycle.h:49-83): the
+ * right-hand side restricted level by level, the coarsest solved, and on the
+ * way up x = P x_coarse followed by a V-cycle at each level.  As in the
+ * reference, the F-cycle starts from zero whatever x the solve loop holds. */
+#define CDR_CYCLE_V 0
+#define CDR_CYCLE_F 1
+
 /* Line direction */
 #define CDR_DIR_X 0
 #define CDR_DIR_Y 1
@@ -261,6 +269,7 @@ typedef struct cdr_gpu_settings {
 	int coarse_solve; /* CDR_COARSE_BANDED (default) or CDR_COARSE_INVERSE; 2D solver only */
 	int fp32_levels;  /* CDR_PREC_F32_IR, 2D solver: the FP32 cycle runs this many finest levels in FP32 and
 	                     the coarser ones in FP64 (latency-bound there, so FP64 costs little); 0 = all (default) */
+	int cycle;        /* "solver.cycle.type": CDR_CYCLE_V (default) or CDR_CYCLE_F; 2D solver only */
 } cdr_gpu_settings;
 
 typedef struct cdr_gpu_solver cdr_gpu_solver;

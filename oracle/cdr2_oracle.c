@@ -1092,6 +1092,33 @@ void o2_vcycle(o2_solver *h, double *x, const double *b)
 	}
 }
 
+/* cycle::fcycle::fmg_cycle / fmg_cycle_helper, include/cedar/cycle/fcycle.h:49-83:
+ * b restricted to the next level, the F-cycle there, then x = P x_c (x and the
+ * level's residual zeroed first, so interp_add adds no residual term) and a
+ * V-cycle from that x.  The incoming x is not used. */
+static void fcycle(o2_solver *h, int l, double *x, const double *b)
+{
+	struct o2_level *L = &h->lv[l];
+	if (l == h->nlev - 1) {
+		o2_solve_cg(x, b, L->ii, L->jj, h->abd, h->bbd, h->nabd1);
+		return;
+	}
+	struct o2_level *C = &h->lv[l + 1];
+	o2_restrict(C->ci, b, C->b, L->ii, L->jj, C->ii, C->jj);
+	fcycle(h, l + 1, C->x, C->b);
+	memset(x, 0, sizeof(double) * (size_t)L->ii * L->jj);
+	memset(L->res, 0, sizeof(double) * (size_t)L->ii * L->jj);
+	o2_interp_add(x, C->x, L->res, L->so, C->ci, C->ii, C->jj, L->ii, L->jj);
+	ncycle(h, l, x, b);
+}
+
+/* cycle->run of multilevel::solve: the V- or the F-cycle (multilevel.h:68-78) */
+void o2_cycle(o2_solver *h, double *x, const double *b)
+{
+	if (h->s.cycle == 1 && h->nlev > 1) fcycle(h, 0, x, b);
+	else o2_vcycle(h, x, b);
+}
+
 /* multilevel::solve, include/cedar/multilevel.h:278-298.  Returns the number of
  * cycles run; hist[i] = relative l2 residual after cycle i. */
 int o2_solve(o2_solver *h, const double *b, double *x, double *hist, int maxhist)
@@ -1102,7 +1129,7 @@ int o2_solve(o2_solver *h, const double *b, double *x, double *hist, int maxhist
 	double res0 = o2_l2norm(L->res, L->ii, L->jj);
 	int it;
 	for (it = 0; it < h->s.maxiter; ++it) {
-		o2_vcycle(h, x, b);
+		o2_cycle(h, x, b);
 		o2_residual(L->so, b, x, L->res, L->ii, L->jj, ifd);
 		double rel = o2_l2norm(L->res, L->ii, L->jj) / res0;
 		if (hist && it < maxhist) hist[it] = rel;

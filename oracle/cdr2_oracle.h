@@ -21,6 +21,7 @@ typedef struct {
 	int maxiter;
 	double tol;
 	int min_coarse;
+	int cycle; /* 0: V-cycle, 1: F-cycle (ml_settings::cycle_type) */
 } o2_settings;
 
 typedef struct o2_solver o2_solver;
@@ -51,6 +52,8 @@ int o2_num_levels(int nx, int ny, int min_coarse);
 o2_solver *o2_create(const o2_settings *s, const double *so_fine, int nstncl, int nx, int ny);
 void o2_destroy(o2_solver *h);
 void o2_vcycle(o2_solver *h, double *x, const double *b);
+void o2_cycle(o2_solver *h, double *x, const double *b);
+void o2_cycle(o2_solver *h, double *x, const double *b);
 int o2_solve(o2_solver *h, const double *b, double *x, double *hist, int maxhist);
 int o_num_threads(void);
 int o2_nlevels(const o2_solver *h);

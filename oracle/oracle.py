@@ -26,7 +26,7 @@ class Settings(ctypes.Structure):
     _fields_ = [("relax", ctypes.c_int), ("nrelax_pre", ctypes.c_int),
                 ("nrelax_post", ctypes.c_int), ("num_levels", ctypes.c_int),
                 ("maxiter", ctypes.c_int), ("tol", ctypes.c_double),
-                ("min_coarse", ctypes.c_int)]
+                ("min_coarse", ctypes.c_int), ("cycle", ctypes.c_int)]
 
 
 def build():
@@ -68,6 +68,7 @@ def lib(variant=""):
             "o2_create": (P, [ctypes.POINTER(Settings), P, I, I, I]),
             "o2_destroy": (None, [P]),
             "o2_vcycle": (None, [P, P, P]),
+            "o2_cycle": (None, [P, P, P]),
             "o2_solve": (I, [P, P, P, P, I]),
             "o2_nlevels": (I, [P]),
             "o_num_threads": (I, []),
@@ -242,12 +243,13 @@ class Solver:
     """Serial BoxMG solver: setup in the constructor, as ``cdr2::solver``."""
 
     def __init__(self, so, relax="point", nrelax_pre=2, nrelax_post=1, num_levels=-1,
-                 maxiter=10, tol=1e-8, min_coarse=3, variant=""):
+                 maxiter=10, tol=1e-8, min_coarse=3, variant="", cycle="v"):
         self.L = lib(variant)
         so = np.ascontiguousarray(so, dtype=np.float64)
         self.nstncl = so.shape[0]
         self.ny, self.nx = so.shape[1] - 2, so.shape[2] - 2
-        self.settings = Settings(RELAX[relax], nrelax_pre, nrelax_post, num_levels, maxiter, tol, min_coarse)
+        self.settings = Settings(RELAX[relax], nrelax_pre, nrelax_post, num_levels, maxiter, tol, min_coarse,
+                                 {"v": 0, "f": 1}[cycle])
         self._so = so
         self.h = self.L.o2_create(ctypes.byref(self.settings), _p(so), self.nstncl, self.nx, self.ny)
 

@@ -452,3 +452,35 @@ def test_oracle_threads_do_not_change_results(oracle):
         res[t] = p.stdout.split()
     assert res["1"][0] == "1" and res["4"][0] == "4"
     assert res["1"][1:] == res["4"][1:]
+
+
+# ----------------------------------------------------------------- F-cycle
+def test_fcycle_two_levels_is_vcycle_from_interpolated_coarse_solve(oracle):
+    """cycle::fcycle (include/cedar/cycle/fcycle.h:49-83) on two levels: restrict
+    b, solve the coarse system exactly, x = P x_c (zero residual term), then one
+    V-cycle from that x.  Restated here with the oracle's own kernels and
+    compared bit for bit; the incoming x does not matter."""
+    n = 31
+    so, b = P.hetero_diffusion(n, sigma=1.0, n_incl=4, contrast=100.0, aniso=0.5)
+    so = np.ascontiguousarray(so)
+    sf = oracle.Solver(so, relax="line-xy", num_levels=2, maxiter=1, tol=0, cycle="f")
+    x_f, h_f = sf.solve(b, x=np.random.default_rng(0).random(b.shape))
+    ci = sf.level_array(1, "ci")
+    soc = sf.level_array(1, "so")
+    bc = oracle.restrict(ci, b)
+    abd, info = oracle.setup_cg(soc)
+    assert info == 0
+    xc = oracle.solve_cg(abd, bc)
+    x0 = oracle.interp_add(ci, xc, np.zeros_like(b), so, np.zeros_like(b))
+    sv = oracle.Solver(so, relax="line-xy", num_levels=2, maxiter=1, tol=0)
+    x_v = sv.vcycle(x0.copy(), b)
+    np.testing.assert_array_equal(x_f, x_v)
+
+
+def test_fcycle_solve_repeats_the_same_iterate(oracle):
+    """The reference's solve loop hands the F-cycle the current x, which
+    fmg_cycle discards: every iteration gives the same x and residual."""
+    n = 63
+    so, b = P.hetero_diffusion(n, sigma=1.0, n_incl=4, contrast=100.0, aniso=0.5)
+    x, h = oracle.Solver(so, relax="line-xy", maxiter=4, tol=0, cycle="f").solve(b)
+    assert len(h) == 4 and np.all(h == h[0]) and h[0] < 0.5
