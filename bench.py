@@ -40,7 +40,10 @@ sys.path.insert(0, ROOT)
 PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
 WORKLOAD = ("2D heterogeneous diffusion, 9-pt bilinear FE, 2047x2047 nodes (2048^2 cells), lognormal k "
             "(GRF ell=1/32 sigma=2, seed 1), 64 inclusions x1e4 (seed 2), ky=1e-3 k on y>0.5, rhs U[0,1] h^2 "
-            "(seed 3); line-xy relaxation, Galerkin coarsening to 4x4, banded-Cholesky coarsest")
+            "(seed 3); line-xy relaxation, Galerkin coarsening (levels and coarsest solve: config.solver)")
+# DRAM bytes (read + write) of one fine-level x-line colour launch of the 2047^2 FP32 level,
+# from one ncu capture (--set full, caches flushed): 84.2 MB read + 3.0 MB written
+LINE_X_TRAFFIC = 87.3e6
 
 
 def parse():
@@ -54,7 +57,33 @@ def parse():
     ap.add_argument("--tol", type=float, default=1e-3, help="relative residual of the headline solves")
     ap.add_argument("--maxiter", type=int, default=300, help="iteration cap of the headline solves")
     ap.add_argument("--no-extras", action="store_true", help="skip the to_1e-10 and cpu_baseline legs")
+    ap.add_argument("--profile", choices=["fcg", "vcycle"], default=None,
+                    help="profiling driver (for ncu): set up the headline FP32 solver (fcg: six-level FCG; vcycle: "
+                         "the reference loop's 10-level V(2,1)) with graphs off and default line shapes, run "
+                         "--steps iterations, print the launch counts, no timing")
     return ap.parse_args()
+
+
+def profile_main(args):
+    """Launch-list driver: every kernel of the headline solve launched directly (no graph)."""
+    from cedar_b200 import _lib, problems as P
+    from cedar_b200.config import Config
+    from cedar_b200.solver import Solver2D
+    so, b = P.hetero_diffusion(args.n)
+    if args.profile == "fcg":
+        conf = {"solver": {"relaxation": "line-xy", "max-iter": args.steps, "tol": 1e-30, "num-levels": 6,
+                           "cycle": {"nrelax-pre": 1, "nrelax-post": 1}},
+                "gpu": {"precision": "fp32-ir", "krylov": "fcg", "coarse-solve": "inverse"}}
+    else:
+        conf = {"solver": {"relaxation": "line-xy", "max-iter": args.steps, "tol": 1e-30},
+                "gpu": {"precision": "fp32-ir"}}
+    conf["gpu"].update({"graph": False, "autotune": False})
+    lib = _lib.load()
+    s = Solver2D(so, Config(conf))
+    l0 = lib.cdr_gpu_launch_count()
+    s.solve(b)
+    print(json.dumps({"profile": args.profile, "levels": s.nlevels, "setup_launches": int(l0),
+                      "solve_launches": int(lib.cdr_gpu_launch_count() - l0), "iterations": int(s.iters)}))
 
 
 def peaks():
@@ -182,6 +211,8 @@ def main():
     args = parse()
     if args.impl == "reference":
         return reference_main(args)
+    if args.profile:
+        return profile_main(args)
     import numpy as np
     import torch
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -354,7 +385,8 @@ def main():
                       "fp64_hbm_gbs": vcycle_bytes(vc64["solver"], word=8) / (vc64["ms_per_cycle"] * 1e-3) / 1e9},
            "roofline": {"kernel": "k_lines_fast<float,5,x> (fine-level x-line sweep, 2 launches)",
                         "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                        "frac": achieved / peak, "peak_kind": peak_kind, "traffic": None,
+                        "frac": achieved / peak, "peak_kind": peak_kind,
+                        "traffic": LINE_X_TRAFFIC if n == 2047 else None,
                         "algorithmic_bytes_per_launch": bytes_per_sweep / 2, "launch_ms": launch_ms},
            "e2e": {"value": e2e, "unit": "ms", "h2d_bytes_per_step": 2 * 8 * (n + 2) ** 2,
                    "d2h_bytes_per_step": 8 * (n + 2) ** 2 + 8 * it32},
