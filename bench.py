@@ -345,6 +345,15 @@ def main():
     torch.cuda.synchronize()
     sweep_ms = ev[0].elapsed_time(ev[1]) / reps
     launch_ms = sweep_ms / 2.0
+    # launch shapes the setup-time autotuner chose for the fine level (cap 0: streamed x-line kernel)
+    shapes = {}
+    for dname, dirn, nn, nl in (("x", 0, nx, ny), ("y", 1, ny, nx)):
+        K, cap = ctypes.c_int(), ctypes.c_int()
+        if lib.cdr_gpu_lines_shape(dirn, 1, ns, nn, nl, 0, ctypes.byref(K), ctypes.byref(cap)) == 0:
+            shapes[dname] = {"K": K.value, "cap": cap.value}
+    xkern = ("k_lines_xstream<float,%d,8> (fine-level x-line sweep, rows streamed into shared memory, 2 launches)"
+             % ns if shapes.get("x", {}).get("cap") == 0 else
+             "k_lines_fast<float,%d,x> (fine-level x-line sweep, 2 launches)" % ns)
     # algorithmic bytes of one x-line sweep (both colours), FP32, 9-point:
     # off-line couplings s, sw, nw (3 planes) + factors d, e (2) + b + x read + x write = 8 words per point
     bytes_per_sweep = 8 * 4 * nx * ny
@@ -383,7 +392,7 @@ def main():
                       "hbm_gbs": vcyc_bytes / (vc32["ms_per_cycle"] * 1e-3) / 1e9,
                       "fp64_ms": vc64["ms_per_cycle"],
                       "fp64_hbm_gbs": vcycle_bytes(vc64["solver"], word=8) / (vc64["ms_per_cycle"] * 1e-3) / 1e9},
-           "roofline": {"kernel": "k_lines_fast<float,5,x> (fine-level x-line sweep, 2 launches)",
+           "roofline": {"kernel": xkern, "line_shapes": shapes,
                         "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                         "frac": achieved / peak, "peak_kind": peak_kind,
                         "traffic": LINE_X_TRAFFIC if n == 2047 else None,

@@ -21,6 +21,7 @@ COARSE = {"banded": 0, "inverse": 1}
 DIR_X, DIR_Y = 0, 1
 LINES_EXACT = 1
 LINES_NOTUNE = 2
+LINES_STREAM = 4
 
 _lib = None
 

@@ -8,7 +8,9 @@ GPU options live under the ``"gpu"`` object: ``precision`` ("fp64" | "fp32-ir"),
 ``graph`` (bool), ``fuse-coarse`` (levels with both edges at most this many
 points run as one fused kernel; 0 = off; default 32), ``line-solve`` ("scan": parallel line substitutions, the
 default; "sequential": DPTTRS order, bit-identical to the reference), ``autotune`` (bool, default true: time
-the line kernels' launch shapes per level at setup, once per shape and process), ``krylov`` ("none": the
+the line kernels' launch shapes per level at setup, once per shape and process), ``line-stream`` (bool,
+default false: x-line sweeps of 256-2048 points by the persistent kernel whose rows arrive in shared memory
+by bulk copies; the autotuner also considers it), ``krylov`` ("none": the
 reference's outer loop, the default; "fcg": the cycle preconditions flexible conjugate gradients, 2D only) and
 ``coarse-solve`` ("banded": the reference's DPBTRS, the default; "inverse": the setup forms the coarsest
 operator's inverse and every cycle multiplies by it, 2D only — for a coarsest level of thousands of unknowns)
@@ -82,6 +84,7 @@ class MLSettings:
         if self.fuse_coarse < 0:
             raise ValueError("invalid gpu.fuse-coarse: %d" % self.fuse_coarse)
         self.autotune = bool(conf.get("gpu.autotune", True))
+        self.line_stream = bool(conf.get("gpu.line-stream", False))
         self.krylov = conf.get("gpu.krylov", "none")
         if self.krylov not in ("none", "fcg"):
             raise ValueError("invalid gpu.krylov: %s" % self.krylov)

@@ -78,7 +78,7 @@ int cdr_gpu_lines_shape(int dir, int fp32, int nstencil, int n, int nlines, int 
 		return CDR_ERR_ARG;
 	}
 	if (K) *K = sh.K;
-	if (cap) *cap = sh.cap;
+	if (cap) *cap = sh.stream ? 0 : sh.cap;
 	return CDR_OK;
 }
 

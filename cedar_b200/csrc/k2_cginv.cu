@@ -9,6 +9,8 @@
 // A^{-1} from the same factor (one column per thread, both sweeps per column,
 // FP64) and each cycle applies it as a matrix-vector product (memory bound,
 // ~n^2 words per solve).  The result equals DPBTRS's to rounding, not bitwise.
+#include <type_traits>
+
 #include "k2_point.cuh"
 #include "kernels2d.cuh"
 
@@ -77,24 +79,55 @@ __global__ void __launch_bounds__(32) k_cg_inverse(const double *__restrict__ ab
 	}
 }
 
-// x(interior) = A^{-1} b(interior): b compacted into shared memory, one warp
-// per row, FP64 accumulation
+// x(interior) = A^{-1} b(interior): b compacted into shared memory in the
+// inverse's type, one warp per row, 16-byte row loads (four independent FP64
+// accumulators per lane, so that each lane keeps four loads in flight) where
+// the row length is a multiple of the vector width, FP64 accumulation.  A
+// product of two FP32 (or the FP64) values is summed in FP64.
 template <typename T>
 __global__ void __launch_bounds__(256) k_cg_inv_apply(const T *__restrict__ ainv, T *__restrict__ q,
                                                       const T *__restrict__ qf, Dims2 d)
 {
-	extern __shared__ double bs[];
+	extern __shared__ __align__(16) unsigned char cgi_raw[];
+	T *bs = reinterpret_cast<T *>(cgi_raw);
+	constexpr int V = 16 / sizeof(T);
+	using VT = typename std::conditional<sizeof(T) == 4, float4, double2>::type;
 	const int n = d.nx * d.ny;
-	for (int e = threadIdx.x; e < n; e += blockDim.x) bs[e] = (double)qf[d.at(e % d.nx + 1, e / d.nx + 1)];
+	for (int e = threadIdx.x; e < n; e += blockDim.x) bs[e] = qf[d.at(e % d.nx + 1, e / d.nx + 1)];
 	__syncthreads();
 	const int lane = threadIdx.x & 31;
 	const int warps = gridDim.x * (blockDim.x >> 5);
+	const bool vec = n % V == 0;
 	for (int r = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); r < n; r += warps) {
 		const T *row = ainv + (size_t)r * n;
-		double a = 0.0;
-		for (int j = lane; j < n; j += 32) a += (double)row[j] * bs[j];
-		for (int o = 16; o > 0; o >>= 1) a += __shfl_down_sync(0xffffffffu, a, o);
-		if (lane == 0) q[d.at(r % d.nx + 1, r / d.nx + 1)] = (T)a;
+		double a[4] = {0.0, 0.0, 0.0, 0.0};
+		if (vec) {
+			const VT *rv = reinterpret_cast<const VT *>(row);
+			const int nv = n / V;
+			int j = lane;
+			for (; j + 96 < nv; j += 128) {
+#pragma unroll
+				for (int u = 0; u < 4; ++u) {
+					const VT w = __ldcs(rv + j + 32 * u);
+					const VT bv = reinterpret_cast<const VT *>(bs)[j + 32 * u];
+					const T *wt = reinterpret_cast<const T *>(&w), *bb = reinterpret_cast<const T *>(&bv);
+#pragma unroll
+					for (int v = 0; v < V; ++v) a[u] += (double)wt[v] * (double)bb[v];
+				}
+			}
+			for (; j < nv; j += 32) {
+				const VT w = __ldcs(rv + j);
+				const VT bv = reinterpret_cast<const VT *>(bs)[j];
+				const T *wt = reinterpret_cast<const T *>(&w), *bb = reinterpret_cast<const T *>(&bv);
+#pragma unroll
+				for (int v = 0; v < V; ++v) a[0] += (double)wt[v] * (double)bb[v];
+			}
+		} else {
+			for (int j = lane; j < n; j += 32) a[0] += (double)row[j] * (double)bs[j];
+		}
+		double s = (a[0] + a[1]) + (a[2] + a[3]);
+		for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+		if (lane == 0) q[d.at(r % d.nx + 1, r / d.nx + 1)] = (T)s;
 	}
 }
 
@@ -116,7 +149,7 @@ template <typename T>
 int solve_cg_inv_2d(const T *ainv, T *x, const T *b, Dims2 d, cudaStream_t st)
 {
 	const int n = d.nx * d.ny;
-	const size_t sm = sizeof(double) * (size_t)n;
+	const size_t sm = sizeof(T) * (size_t)n;
 	if (sm > 48 * 1024) {
 		set_error(CDR_ERR_DIM, "coarsest grid %dx%d too large for the inverse product", d.nx, d.ny);
 		return CDR_ERR_DIM;

@@ -337,6 +337,12 @@ __global__ void __launch_bounds__(XL ? FAST_BLOCK_X : FAST_BLOCK_Y, XL ? 2 : 1)
 	const bool active = lc <= nl;
 	const int p0 = t * K;
 	const bool has = active && p0 <= n;
+	// Chunks cover positions 0 .. TPL*K - 1 (position 0 is the ghost).  Where
+	// TPL*K == n, position n is left over and the last chunk takes it as one more
+	// element (rx, its rhs and then its solution): a level of 2^k + 1 positions
+	// then runs on 2^k / K threads per line instead of twice that.
+	const bool xtra = has && t == TPL - 1 && p0 + K == n;
+	T rx = T(0);
 	const size_t ps = d.plane();
 	const int P = d.pitch;
 	so += d.bofs(NS * ps);
@@ -362,6 +368,8 @@ __global__ void __launch_bounds__(XL ? FAST_BLOCK_X : FAST_BLOCK_Y, XL ? 2 : 1)
 			vload<T, K>(s + k0 + P, s1);
 #pragma unroll
 			for (int m = 0; m < K; ++m) r[m] = madd(s1[m], qp[m], madd(s0[m], qm[m], b_[m]));
+			const size_t kx = k0 + K;  // position n when xtra
+			if (xtra) rx = madd(s[kx + P], q[kx + P], madd(s[kx], q[kx - P], qf[kx]));
 			if (NS == 5) {
 				T sw0[K], nw0[K], nw1[K], sw1[K];
 				vload<T, K>(sw + k0, sw0);
@@ -385,6 +393,14 @@ __global__ void __launch_bounds__(XL ? FAST_BLOCK_X : FAST_BLOCK_Y, XL ? 2 : 1)
 					a = madd(nw1[m], qpl, a);
 					r[m] = madd(swr, qpr, a);
 				}
+				if (xtra) {
+					T a = madd(s[kx], q[kx - P], qf[kx]);
+					a = madd(s[kx + P], q[kx + P], a);
+					a = madd(sw[kx], qm[K - 1], a);
+					a = madd(nw[kx + 1], q[kx - P + 1], a);
+					a = madd(nw[kx + P], qp[K - 1], a);
+					rx = madd(sw[kx + P + 1], q[kx + P + 1], a);
+				}
 			}
 		} else {
 			const int i = lc;
@@ -394,6 +410,7 @@ __global__ void __launch_bounds__(XL ? FAST_BLOCK_X : FAST_BLOCK_Y, XL ? 2 : 1)
 				if (jj < 1 || jj > n) continue;
 				r[m] = line_rhs<T, NS, CDR_DIR_Y>(so, ps, q, qf, d.at(i, jj), P);
 			}
+			if (xtra) rx = line_rhs<T, NS, CDR_DIR_Y>(so, ps, q, qf, d.at(i, n), P);
 		}
 	}
 
@@ -430,6 +447,11 @@ __global__ void __launch_bounds__(XL ? FAST_BLOCK_X : FAST_BLOCK_Y, XL ? 2 : 1)
 			B = madd(a, B, r[m]);
 			A = a * A;
 		}
+		if (xtra) {
+			const T a = -E[n];
+			B = madd(a, B, rx);
+			A = a * A;
+		}
 	}
 	T y = scan_incoming<T>(A, B, true, u, S, CW, NWG, kgrp, slot, sstride, sA, sB);
 	if (has) {
@@ -440,6 +462,7 @@ __global__ void __launch_bounds__(XL ? FAST_BLOCK_X : FAST_BLOCK_Y, XL ? 2 : 1)
 			y = (!full && pos == 1) ? r[m] : madd(-y, Ev[m], r[m]);
 			r[m] = y;
 		}
+		if (xtra) rx = pivot_div(madd(-y, E[n], rx), D[n]);
 		// y(p)/D(p), the first operation of the DPTTS2 back substitution, in place
 		constexpr int W = 16 / sizeof(T);
 #pragma unroll
@@ -458,6 +481,10 @@ __global__ void __launch_bounds__(XL ? FAST_BLOCK_X : FAST_BLOCK_Y, XL ? 2 : 1)
 	A = T(1);
 	B = T(0);
 	if (has) {
+		if (xtra) {
+			B = madd(T(0), B, rx);
+			A = T(0) * A;
+		}
 #pragma unroll
 		for (int m = K - 1; m >= 0; --m) {
 			const int pos = p0 + m;
@@ -471,6 +498,7 @@ __global__ void __launch_bounds__(XL ? FAST_BLOCK_X : FAST_BLOCK_Y, XL ? 2 : 1)
 	if (NWG > 1) __syncthreads();  // the forward carries are still being read
 	T x = scan_incoming<T>(A, B, false, u, S, CW, NWG, kgrp, slot, sstride, sA, sB);
 	if (has) {
+		if (xtra) x = rx;
 #pragma unroll
 		for (int m = K - 1; m >= 0; --m) {
 			const int pos = p0 + m;
@@ -485,6 +513,7 @@ __global__ void __launch_bounds__(XL ? FAST_BLOCK_X : FAST_BLOCK_Y, XL ? 2 : 1)
 	if (has) {
 		if (DIR == CDR_DIR_X) {
 			const size_t k0 = d.at(p0, lc);
+			if (xtra) q[k0 + K] = rx;
 			if (p0 >= 1 && p0 + K - 1 <= n) vstore<T, K>(q + k0, r);
 			else {
 #pragma unroll
@@ -499,7 +528,302 @@ __global__ void __launch_bounds__(XL ? FAST_BLOCK_X : FAST_BLOCK_Y, XL ? 2 : 1)
 				const int pos = p0 + m;
 				if (pos >= 1 && pos <= n) q[d.at(lc, pos)] = r[m];
 			}
+			if (xtra) q[d.at(lc, n)] = rx;
 		}
+	}
+}
+
+// ---------------------------------------------------------- streamed x-lines
+// x-lines of one problem with 256 <= n: a persistent CTA walks the lines of a
+// colour (l = blockIdx.x, + gridDim.x, ...).  Each line's rows -- b, x of the
+// two neighbouring lines, the off-line couplings of rows j and j+1 and the
+// line's factors, 7 or 11 rows -- arrive in shared memory by bulk asynchronous
+// copies (cp.async.bulk, one mbarrier per stage) issued two lines ahead, so
+// that DRAM keeps streaming while the CTA runs the scans of the current line.
+// The arithmetic is k_lines_fast's x-line path with the same K on the staged
+// rows: results are bit-identical to it.  Every wait on a stage is bounded;
+// one that gives up is counted in g_xstream_timeouts and the CTA returns.
+namespace {
+__device__ unsigned g_xstream_timeouts;
+
+__device__ __forceinline__ unsigned smem_u32(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar, unsigned count)
+{
+	asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, unsigned bytes)
+{
+	asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+	             : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, unsigned parity)
+{
+	unsigned ok;
+	asm volatile(
+	    "{\n\t.reg .pred p;\n\t"
+	    "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+	    "selp.u32 %0, 1, 0, p;\n\t}"
+	    : "=r"(ok)
+	    : "r"(smem_u32(bar)), "r"(parity)
+	    : "memory");
+	return ok != 0;
+}
+
+// at most 2^18 polls (each try_wait may suspend the thread for a while)
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, unsigned parity)
+{
+	for (int it = 0; it < (1 << 18); ++it)
+		if (mbar_try_wait(bar, parity)) return true;
+	return false;
+}
+
+// global -> shared bulk copy completing on *bar (no multicast); 16-byte aligned
+// addresses, size a multiple of 16
+__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, unsigned bytes, uint64_t *bar)
+{
+	asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+	                 smem_u32(dst)),
+	             "l"(src), "r"(bytes), "r"(smem_u32(bar))
+	             : "memory");
+}
+}  // namespace
+
+unsigned lines_stream_timeouts(cudaStream_t st)
+{
+	unsigned v = 0;
+	if (cudaMemcpyFromSymbolAsync(&v, g_xstream_timeouts, sizeof v, 0, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+	    cudaStreamSynchronize(st) != cudaSuccess)
+		return 0;
+	if (v) {
+		const unsigned z = 0;
+		cudaMemcpyToSymbolAsync(g_xstream_timeouts, &z, sizeof z, 0, cudaMemcpyHostToDevice, st);
+		cudaStreamSynchronize(st);
+	}
+	return v;
+}
+
+constexpr int XS_BLOCK = 256;
+constexpr int XS_SMEM_MAX = 226 * 1024;  // dynamic part; the kernel's static carries take the rest
+template <int NS>
+__host__ __device__ constexpr int xs_rows()
+{
+	return NS == 5 ? 11 : 7;
+}
+// dynamic shared memory of the streamed kernel: two barriers (padded to 128
+// bytes), then two stages of R rows with the level's pitch
+template <typename T, int NS>
+static size_t xs_smem(int pitch)
+{
+	return 128 + 2 * (size_t)xs_rows<NS>() * pitch * sizeof(T);
+}
+
+template <typename T, int NS, int K>
+__global__ void __launch_bounds__(XS_BLOCK) k_lines_xstream(const T *__restrict__ so, T *__restrict__ q,
+                                                            const T *__restrict__ qf, const T *__restrict__ sor,
+                                                            Dims2 d, int first, int nlines)
+{
+	extern __shared__ __align__(128) unsigned char xs_raw[];
+	__shared__ T sA[XS_BLOCK / 32], sB[XS_BLOCK / 32];
+	constexpr int R = xs_rows<NS>();
+	uint64_t *bar = reinterpret_cast<uint64_t *>(xs_raw);
+	T *stage0 = reinterpret_cast<T *>(xs_raw + 128);
+	const int P = d.pitch, n = d.nx;
+	const size_t ps = d.plane(), stage_elems = (size_t)R * P;
+	const unsigned row_bytes = ((unsigned)(n + 2) * sizeof(T) + 15u) & ~15u;
+	const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+	const int TPL = blockDim.x;  // threads of the line: chunks of K positions
+	const T *s = so + 2 * ps, *sw = so + (NS == 5 ? 3 : 0) * ps, *nw = so + (NS == 5 ? 4 : 0) * ps;
+	const T *Dp = sor, *Ep = sor + ps;
+
+	// rows of line index li into stage st: b, x(j-1), x(j+1), s(j), s(j+1), d, e
+	// [, sw(j), sw(j+1), nw(j), nw(j+1)]
+	auto issue = [&](int li, int st) {
+		const size_t j = (size_t)(first + 2 * li) * P;
+		T *dst = stage0 + st * stage_elems;
+		const T *src[11] = {qf + j, q + j - P, q + j + P, s + j, s + j + P, Dp + j, Ep + j,
+		                    sw + j, sw + j + P, nw + j, nw + j + P};
+		asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+		mbar_expect_tx(&bar[st], R * row_bytes);
+#pragma unroll
+		for (int r = 0; r < R; ++r) bulk_g2s(dst + (size_t)r * P, src[r], row_bytes, &bar[st]);
+	};
+
+	if (tid == 0) {
+		mbar_init(&bar[0], 1);
+		mbar_init(&bar[1], 1);
+		asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+	}
+	__syncthreads();
+	const int G = gridDim.x;
+	if (tid == 0) {
+		if ((int)blockIdx.x < nlines) issue(blockIdx.x, 0);
+		if ((int)blockIdx.x + G < nlines) issue(blockIdx.x + G, 1);
+	}
+
+	// scan geometry of one line per CTA (k_lines_fast's x-line case with G = 1)
+	const int CW = TPL < 32 ? TPL : 32, NWG = TPL > 32 ? TPL / 32 : 1, kgrp = TPL > 32 ? warp : 0;
+	const int u = lane & (CW - 1);
+	const int p0 = tid * K;
+	const bool has = p0 <= n;
+	const bool xtra = has && tid == TPL - 1 && p0 + K == n;
+	const bool full = p0 >= 1 && p0 + K - 1 <= n;
+
+	int k = 0;
+	for (int li = blockIdx.x; li < nlines; li += G, ++k) {
+		const int st = k & 1;
+		const bool ok = mbar_wait_bounded(&bar[st], (k >> 1) & 1);
+		if (!__syncthreads_and(ok)) {
+			// give up: wait (bounded) for the other stage's copies, if any, then leave
+			if (tid == 0) {
+				atomicAdd(&g_xstream_timeouts, 1u);
+				if (li + G < nlines) mbar_wait_bounded(&bar[st ^ 1], ((k + 1) >> 1) & 1);
+			}
+			return;
+		}
+		const T *rows = stage0 + st * stage_elems;
+		const T *rb = rows, *rqm = rows + P, *rqp = rows + 2 * P, *rs0 = rows + 3 * P, *rs1 = rows + 4 * P;
+		const T *rD = rows + 5 * P, *rE = rows + 6 * P;
+		const int lc = first + 2 * li;
+
+		// 1. right-hand sides of the chunk
+		T r[K];
+		T rx = T(0);
+#pragma unroll
+		for (int m = 0; m < K; ++m) r[m] = T(0);
+		if (has) {
+			T b_[K], qm[K], qp[K], s0[K], s1[K];
+			vload<T, K>(rb + p0, b_);
+			vload<T, K>(rqm + p0, qm);
+			vload<T, K>(rqp + p0, qp);
+			vload<T, K>(rs0 + p0, s0);
+			vload<T, K>(rs1 + p0, s1);
+#pragma unroll
+			for (int m = 0; m < K; ++m) r[m] = madd(s1[m], qp[m], madd(s0[m], qm[m], b_[m]));
+			if (xtra) rx = madd(rs1[n], rqp[n], madd(rs0[n], rqm[n], rb[n]));
+			if (NS == 5) {
+				const T *rsw0 = rows + 7 * P, *rsw1 = rows + 8 * P, *rnw0 = rows + 9 * P, *rnw1 = rows + 10 * P;
+				T sw0[K], nw0[K], nw1[K], sw1[K];
+				vload<T, K>(rsw0 + p0, sw0);
+				vload<T, K>(rnw0 + p0, nw0);
+				vload<T, K>(rnw1 + p0, nw1);
+				vload<T, K>(rsw1 + p0, sw1);
+				const T qm_l = p0 >= 1 ? rqm[p0 - 1] : T(0), qp_l = p0 >= 1 ? rqp[p0 - 1] : T(0);
+				const bool rin = p0 + K <= n + 1;
+				const T qm_r = rin ? rqm[p0 + K] : T(0), qp_r = rin ? rqp[p0 + K] : T(0);
+				const T nw0_r = rin ? rnw0[p0 + K] : T(0), sw1_r = rin ? rsw1[p0 + K] : T(0);
+#pragma unroll
+				for (int m = 0; m < K; ++m) {
+					const T qml = m > 0 ? qm[m - 1] : qm_l, qmr = m < K - 1 ? qm[m + 1] : qm_r;
+					const T qpl = m > 0 ? qp[m - 1] : qp_l, qpr = m < K - 1 ? qp[m + 1] : qp_r;
+					const T nwr = m < K - 1 ? nw0[m + 1] : nw0_r, swr = m < K - 1 ? sw1[m + 1] : sw1_r;
+					// operand order of relax_lines_x.f90:106-110
+					T a = madd(s0[m], qm[m], b_[m]);
+					a = madd(s1[m], qp[m], a);
+					a = madd(sw0[m], qml, a);
+					a = madd(nwr, qmr, a);
+					a = madd(nw1[m], qpl, a);
+					r[m] = madd(swr, qpr, a);
+				}
+				if (xtra) {
+					T a = madd(rs0[n], rqm[n], rb[n]);
+					a = madd(rs1[n], rqp[n], a);
+					a = madd(rsw0[n], qm[K - 1], a);
+					a = madd(rnw0[n + 1], rqm[n + 1], a);
+					a = madd(rnw1[n], qp[K - 1], a);
+					rx = madd(rsw1[n + 1], rqp[n + 1], a);
+				}
+			}
+		}
+
+		// 2a. forward substitution y(p) = r(p) - y(p-1) E(p)
+		T Ev[K];
+		if (has) vload<T, K>(rE + p0, Ev);
+		T A = T(1), B = T(0);
+		if (has) {
+#pragma unroll
+			for (int m = 0; m < K; ++m) {
+				const int pos = p0 + m;
+				if (!full && (pos < 1 || pos > n)) continue;
+				const T a = (!full && pos == 1) ? T(0) : -Ev[m];
+				B = madd(a, B, r[m]);
+				A = a * A;
+			}
+			if (xtra) {
+				const T a = -rE[n];
+				B = madd(a, B, rx);
+				A = a * A;
+			}
+		}
+		T y = scan_incoming<T>(A, B, true, u, 1, CW, NWG, kgrp, warp, 1, sA, sB);
+		if (has) {
+#pragma unroll
+			for (int m = 0; m < K; ++m) {
+				const int pos = p0 + m;
+				if (!full && (pos < 1 || pos > n)) continue;
+				y = (!full && pos == 1) ? r[m] : madd(-y, Ev[m], r[m]);
+				r[m] = y;
+			}
+			if (xtra) rx = pivot_div(madd(-y, rE[n], rx), rD[n]);
+			constexpr int W = 16 / sizeof(T);
+#pragma unroll
+			for (int c = 0; c < K / W; ++c) {
+				T dv[W];
+				vload<T, W>(rD + p0 + c * W, dv);
+#pragma unroll
+				for (int w = 0; w < W; ++w) {
+					const int m = c * W + w, pos = p0 + m;
+					if (full || (pos >= 1 && pos <= n)) r[m] = pivot_div(r[m], dv[w]);
+				}
+			}
+		}
+		// 2b. backward substitution x(p) = y(p)/D(p) - x(p+1) E(p+1)
+		const T Enext = has && p0 + K <= n ? rE[p0 + K] : T(0);
+		A = T(1);
+		B = T(0);
+		if (has) {
+			if (xtra) {
+				B = madd(T(0), B, rx);
+				A = T(0) * A;
+			}
+#pragma unroll
+			for (int m = K - 1; m >= 0; --m) {
+				const int pos = p0 + m;
+				if (!full && (pos < 1 || pos > n)) continue;
+				const T e1 = m < K - 1 ? Ev[m + 1] : Enext;
+				const T a = pos == n ? T(0) : -e1;
+				B = madd(a, B, r[m]);
+				A = a * A;
+			}
+		}
+		if (NWG > 1) __syncthreads();  // the forward carries are still being read
+		T x = scan_incoming<T>(A, B, false, u, 1, CW, NWG, kgrp, warp, 1, sA, sB);
+		if (has) {
+			if (xtra) x = rx;
+#pragma unroll
+			for (int m = K - 1; m >= 0; --m) {
+				const int pos = p0 + m;
+				if (!full && (pos < 1 || pos > n)) continue;
+				const T e1 = m < K - 1 ? Ev[m + 1] : Enext;
+				x = pos == n ? r[m] : madd(-x, e1, r[m]);
+				r[m] = x;
+			}
+			// 3. write the line back
+			T *qo = q + (size_t)lc * P;
+			if (xtra) qo[n] = rx;
+			if (full) vstore<T, K>(qo + p0, r);
+			else {
+#pragma unroll
+				for (int m = 0; m < K; ++m) {
+					const int pos = p0 + m;
+					if (pos >= 1 && pos <= n) qo[pos] = r[m];
+				}
+			}
+		}
+		__syncthreads();  // the stage and the carries are free again
+		if (tid == 0 && li + 2 * G < nlines) issue(li + 2 * G, st);
 	}
 }
 
@@ -521,6 +845,10 @@ int lines_prepare()
 	CDR_LINES_ATTR(float, 5, CDR_DIR_X, true); CDR_LINES_ATTR(float, 5, CDR_DIR_Y, true);
 	CDR_LINES_ATTR(float, 3, CDR_DIR_X, true); CDR_LINES_ATTR(float, 3, CDR_DIR_Y, true);
 #undef CDR_LINES_ATTR
+#define CDR_XS_ATTR(T, NS, K) \
+	CDR_CUDA_TRY(cudaFuncSetAttribute(k_lines_xstream<T, NS, K>, cudaFuncAttributeMaxDynamicSharedMemorySize, XS_SMEM_MAX))
+	CDR_XS_ATTR(float, 5, 8); CDR_XS_ATTR(float, 3, 8); CDR_XS_ATTR(double, 5, 4); CDR_XS_ATTR(double, 3, 4);
+#undef CDR_XS_ATTR
 	CDR_TRY(coarse_prepare());
 	done = true;
 	return CDR_OK;
@@ -573,9 +901,9 @@ template <typename T>
 static bool shape_ok(LineShape sh, int n, int dir)
 {
 	const bool kok = sizeof(T) == 4 ? (sh.K == 4 || sh.K == 8 || sh.K == 16) : (sh.K == 2 || sh.K == 4 || sh.K == 8);
-	if (!kok || n + 1 > 256 * sh.K) return false;
+	if (!kok || n > 256 * sh.K) return false;
 	int tpl = 1;
-	while (tpl * sh.K < n + 1) tpl *= 2;
+	while (tpl * sh.K < n) tpl *= 2;
 	if (dir == CDR_DIR_X) return tpl <= FAST_BLOCK_X;
 	return sh.cap >= 32 && sh.cap <= FAST_BLOCK_Y && tpl <= sh.cap;
 }
@@ -594,12 +922,66 @@ static int launch_fast(const T *so, T *x, const T *b, const T *sor, Dims2 d, int
 {
 	const int n = DIR == CDR_DIR_X ? d.nx : d.ny;
 	int tpl_log2 = 0;
-	while ((1 << tpl_log2) * K < n + 1) ++tpl_log2;
+	while ((1 << tpl_log2) * K < n) ++tpl_log2;  // chunks cover 0 .. n - 1, the last one also n
 	const int TPL = 1 << tpl_log2;
 	const int block = DIR == CDR_DIR_X ? FAST_BLOCK_X : (TPL * 32 < cap ? TPL * 32 : cap);
 	const int G = block / TPL;
 	k_lines_fast<T, NS, DIR, K><<<dim3(ceil_div(nlines, G), 1, d.nb), block, 0, st>>>(so, x, b, sor, d, tpitch, first,
 	                                                                                  tpl_log2);
+	CDR_LAUNCH_CHECK();
+	return CDR_OK;
+}
+
+// The streamed x-line kernel: K = 8 (FP32) or 4 (FP64) elements per thread, one
+// line per CTA step (TPL = 32 .. 256 threads), a single problem, both stages
+// within the shared-memory budget.
+template <typename T>
+__host__ __device__ constexpr int xs_K()
+{
+	return sizeof(T) == 4 ? 8 : 4;
+}
+
+template <typename T, int NS>
+static bool xs_ok(Dims2 d)
+{
+	const int K = xs_K<T>(), n = d.nx;
+	return d.nb == 1 && n >= 32 * K && n <= XS_BLOCK * K && xs_smem<T, NS>(d.pitch) <= XS_SMEM_MAX;
+}
+
+// CTAs per SM of the streamed kernel for a (block, shared memory) pair, and the
+// SM count: looked up once per pair
+template <typename T, int NS>
+static int xs_grid_cap(int block, size_t smem)
+{
+	static std::mutex mu;
+	static std::map<std::pair<int, size_t>, int> cache;
+	std::lock_guard<std::mutex> lk(mu);
+	auto it = cache.find({block, smem});
+	if (it != cache.end()) return it->second;
+	int dev = 0, sms = 0, per_sm = 0;
+	if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+	    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_lines_xstream<T, NS, xs_K<T>()>, block, smem) != cudaSuccess)
+		return 0;
+	const int cap = sms * (per_sm > 0 ? per_sm : 1);
+	cache[{block, smem}] = cap;
+	return cap;
+}
+
+template <typename T, int NS>
+static int launch_xstream(const T *so, T *x, const T *b, const T *sor, Dims2 d, int first, int nlines, cudaStream_t st)
+{
+	constexpr int K = xs_K<T>();
+	int tpl = 1;
+	while (tpl * K < d.nx) tpl *= 2;
+	const size_t smem = xs_smem<T, NS>(d.pitch);
+	CDR_TRY(lines_prepare());
+	const int cap = xs_grid_cap<T, NS>(tpl, smem);
+	if (cap <= 0) {
+		set_error(CDR_ERR_CUDA, "occupancy query for the streamed line kernel failed");
+		return CDR_ERR_CUDA;
+	}
+	const int grid = nlines < cap ? nlines : cap;
+	k_lines_xstream<T, NS, K><<<grid, tpl, smem, st>>>(so, x, b, sor, d, first, nlines);
 	CDR_LAUNCH_CHECK();
 	return CDR_OK;
 }
@@ -620,6 +1002,9 @@ static int launch_lines(const T *so, T *x, const T *b, const T *sor, Dims2 d, in
 	LineShape sh = force ? *force : shape_for<T>(n, nl, NS, d.nb, DIR);
 	if (!shape_ok<T>(sh, n, DIR)) sh = default_shape<T>(n, DIR);
 	if (!exact && aligned && d.pitch % 16 == 0 && fpitch % 16 == 0 && shape_ok<T>(sh, n, DIR)) {
+		if constexpr (DIR == CDR_DIR_X)
+			if (sh.stream && sh.K == xs_K<T>() && xs_ok<T, NS>(d))
+				return launch_xstream<T, NS>(so, x, b, sor, d, first, nlines, st);
 		if constexpr (sizeof(T) == 4) {
 			if (sh.K == 4) return launch_fast<T, NS, DIR, 4>(so, x, b, sor, d, tpitch, first, nlines, sh.cap, st);
 			if (sh.K == 16) return launch_fast<T, NS, DIR, 16>(so, x, b, sor, d, tpitch, first, nlines, sh.cap, st);
@@ -683,6 +1068,26 @@ static int tune_dir(const T *so, T *x, const T *b, const T *sor, Dims2 d, int tp
 			}
 			if (ms < best_ms) { best_ms = ms; best = sh; }
 		}
+	if (DIR == CDR_DIR_X && rc == CDR_OK && xs_ok<T, NS>(d)) {
+		const LineShape sh{xs_K<T>(), FAST_BLOCK_X, 1};
+		float ms = 1e30f;
+		for (int rep = 0; rep < 3 && rc == CDR_OK; ++rep) {
+			rc = launch_lines<T, NS, DIR>(so, x, b, sor, d, tpitch, 1, false, st, &sh);
+			if (rc != CDR_OK) break;
+			if (cudaEventRecord(e0, st) != cudaSuccess) { rc = CDR_ERR_CUDA; break; }
+			for (int it = 0; it < 4 && rc == CDR_OK; ++it)
+				rc = launch_lines<T, NS, DIR>(so, x, b, sor, d, tpitch, 1 + (it & 1), false, st, &sh);
+			if (rc != CDR_OK) break;
+			float t = 0.f;
+			if (cudaEventRecord(e1, st) != cudaSuccess || cudaEventSynchronize(e1) != cudaSuccess ||
+			    cudaEventElapsedTime(&t, e0, e1) != cudaSuccess) {
+				rc = CDR_ERR_CUDA;
+				break;
+			}
+			ms = t < ms ? t : ms;
+		}
+		if (ms < best_ms) { best_ms = ms; best = sh; }
+	}
 	cudaEventDestroy(e0);
 	cudaEventDestroy(e1);
 	if (rc != CDR_OK) return rc;
@@ -722,7 +1127,9 @@ int relax_lines_2d(const T *so, int nstencil, T *x, const T *b, const T *sor, Di
 {
 	const bool exact = (flags & CDR_LINES_EXACT) != 0;
 	const LineShape dflt = default_shape<T>(dir == CDR_DIR_X ? d.nx : d.ny, dir);
+	const LineShape streamed{xs_K<T>(), FAST_BLOCK_X, 1};
 	const LineShape *force = (flags & CDR_LINES_NOTUNE) ? &dflt : nullptr;
+	if ((flags & CDR_LINES_STREAM) && dir == CDR_DIR_X) force = &streamed;
 	// DOWN: lines with Fortran start index 3 (0-based even) first, then 2 (odd);
 	// UP: the opposite (relax_lines_x.f90:82-97).
 	const int firsts[2] = {updown == CDR_DOWN ? 2 : 1, updown == CDR_DOWN ? 1 : 2};

@@ -22,7 +22,11 @@ int relax_lines_2d(const T *so, int nstencil, T *x, const T *b, const T *sor, Di
 // runs line sweeps on the arrays it is given (x changes unless x = 0 and b = 0).
 struct LineShape {
 	int K = 8, cap = 1024;
+	int stream = 0;  // x-lines: rows streamed into shared memory (k_lines_xstream)
 };
+// bounded waits of the streamed x-line kernel that gave up since the last call
+// (read and reset; 0 in a healthy run)
+unsigned lines_stream_timeouts(cudaStream_t st);
 template <typename T>
 int lines_autotune(const T *so, int nstencil, T *x, const T *b, const T *sor, Dims2 d, int tpitch, int dir,
                    cudaStream_t st);

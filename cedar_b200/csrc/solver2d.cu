@@ -85,7 +85,10 @@ struct cdr_gpu_solver {
 	// the exact (sequential) line substitution applies to the FP64 cycle only;
 	// CDR_LINES_NOTUNE to both
 	template <typename T>
-	int lflags() const { return sizeof(T) == 8 ? s.line_flags : (s.line_flags & CDR_LINES_NOTUNE); }
+	int lflags() const
+	{
+		return sizeof(T) == 8 ? s.line_flags : (s.line_flags & (CDR_LINES_NOTUNE | CDR_LINES_STREAM));
+	}
 	int L() const { return (int)lv.size(); }
 
 	// -------------------------------------------------------------- smoothing
@@ -767,6 +770,10 @@ static int solve_loaded(cdr_gpu_solver *h, int *iters, double *hist, int maxhist
 	CDR_CUDA_TRY(cudaEventSynchronize(h->ev1));
 	CDR_CUDA_TRY(cudaEventElapsedTime(&h->solve_ms, h->ev0, h->ev1));
 	if (iters) *iters = it;
+	if (const unsigned to = lines_stream_timeouts(st)) {
+		set_error(CDR_ERR_NUMERIC, "%u streamed line-sweep CTAs gave up waiting for their rows", to);
+		return CDR_ERR_NUMERIC;
+	}
 	return CDR_OK;
 }
 

@@ -41,7 +41,8 @@ def _settings(ms: MLSettings, dim=2):
     s.min_coarse = ms.min_coarse
     s.precision = _lib.PREC[ms.precision]
     s.use_graph = 1 if ms.use_graph else 0
-    s.line_flags = (_lib.LINES_EXACT if ms.line_solve == "sequential" else 0) | (0 if ms.autotune else _lib.LINES_NOTUNE)
+    s.line_flags = ((_lib.LINES_EXACT if ms.line_solve == "sequential" else 0) |
+                    (0 if ms.autotune else _lib.LINES_NOTUNE) | (_lib.LINES_STREAM if ms.line_stream else 0))
     s.fuse_coarse = ms.fuse_coarse
     if ms.krylov != "none" and dim != 2:
         raise NotImplementedError("gpu.krylov = %r: the Krylov outer iteration is 2D only" % ms.krylov)

@@ -95,7 +95,8 @@ long long cdr_gpu_launch_count(void);
 /* Launch shape the line-kernel autotuner chose for lines of length n, nlines
  * lines, direction dir (CDR_DIR_*), FP32 (fp32 = 1) or FP64 sweeps, nstencil 3
  * or 5, a single problem (batch = 0) or a batch (batch = 1): elements per
- * thread *K and the CTA size cap *cap.  Returns CDR_ERR_ARG when no solver of
+ * thread *K and the CTA size cap *cap (0: x-lines streamed through shared
+ * memory, CDR_LINES_STREAM).  Returns CDR_ERR_ARG when no solver of
  * this process has tuned that shape.  No counterpart in the reference. */
 int cdr_gpu_lines_shape(int dir, int fp32, int nstencil, int n, int nlines, int batch, int *K, int *cap);
 
@@ -173,6 +174,12 @@ int cdr_gpu_setup_lines_2d_f32(const double *so, int nstencil, float *sor, int n
  * the line kernel instead of timing the candidates at setup (the autotuner,
  * whose choice is kept for the process). */
 #define CDR_LINES_NOTUNE 2
+/* Kernel flags: x-lines of a single problem (32K <= nx <= 256K, K = 8 FP32 / 4
+ * FP64) by the streamed kernel: a persistent CTA per SM slot whose line rows
+ * arrive in shared memory by bulk asynchronous copies two lines ahead.  Same
+ * arithmetic as the default kernel with the same K (bit-identical results);
+ * the autotuner also times it as a candidate. */
+#define CDR_LINES_STREAM 4
 int cdr_gpu_relax_lines_2d_f64(const double *so, int nstencil, double *x, const double *b, const double *sor,
                                int nx, int ny, int pitch, int tpitch, int dir, int updown, int flags,
                                cudaStream_t stream);
