@@ -57,10 +57,13 @@ def parse():
     ap.add_argument("--tol", type=float, default=1e-3, help="relative residual of the headline solves")
     ap.add_argument("--maxiter", type=int, default=300, help="iteration cap of the headline solves")
     ap.add_argument("--no-extras", action="store_true", help="skip the to_1e-10 and cpu_baseline legs")
+    ap.add_argument("--no-autotune", action="store_true",
+                    help="default line-kernel launch shapes instead of the setup-time autotuner's")
     ap.add_argument("--profile", choices=["fcg", "vcycle"], default=None,
                     help="profiling driver (for ncu): set up the headline FP32 solver (fcg: six-level FCG; vcycle: "
-                         "the reference loop's 10-level V(2,1)) with graphs off and default line shapes, run "
-                         "--steps iterations, print the launch counts, no timing")
+                         "the reference loop's 10-level V(2,1)) with graphs off (line shapes autotuned as in the "
+                         "bench), run --steps iterations, print the launch counts (setup_launches: skip that many "
+                         "with ncu -s to reach the solve), no timing")
     return ap.parse_args()
 
 
@@ -77,7 +80,7 @@ def profile_main(args):
     else:
         conf = {"solver": {"relaxation": "line-xy", "max-iter": args.steps, "tol": 1e-30},
                 "gpu": {"precision": "fp32-ir"}}
-    conf["gpu"].update({"graph": False, "autotune": False})
+    conf["gpu"].update({"graph": False, "autotune": not args.no_autotune})
     lib = _lib.load()
     s = Solver2D(so, Config(conf))
     l0 = lib.cdr_gpu_launch_count()
@@ -242,7 +245,8 @@ def main():
     def mk(prec, krylov, npre, npost, tol, maxiter, levels=-1, coarse="banded"):
         conf = Config({"solver": {"relaxation": "line-xy", "max-iter": maxiter, "tol": tol, "num-levels": levels,
                                   "cycle": {"nrelax-pre": npre, "nrelax-post": npost}},
-                       "gpu": {"precision": prec, "graph": True, "krylov": krylov, "coarse-solve": coarse}})
+                       "gpu": {"precision": prec, "graph": True, "krylov": krylov, "coarse-solve": coarse,
+                               "autotune": not args.no_autotune}})
         return Solver2D(so, conf, stream=sh)
 
     # headline: flexible CG preconditioned by one line-xy V(1,1) cycle whose coarsest level is ~64^2,
@@ -367,7 +371,7 @@ def main():
            "value": ms32, "unit": "ms", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
            "ms_per_step": ms32, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
            "dtype": "f32 cycle + f64 outer iteration", "data": "synthetic",
-           "config": {"workload": WORKLOAD, "n": n, "levels": s32.nlevels,
+           "config": {"workload": WORKLOAD, "n": n, "levels": s32.nlevels, "line_autotune": not args.no_autotune,
                       "solver": "flexible CG (FP64 recurrences, true residual every iteration) preconditioned by "
                                 "one line-xy V(1,1) cycle over %d levels (coarsest %d^2, solved with its explicit "
                                 "inverse); FP32 cycle (value) vs FP64 cycle (fp64_ms)" % (nlev, m),

@@ -17,6 +17,7 @@
 // Both colours of a sweep are two launches: lines of one colour read only lines
 // of the other colour.  With CDR_LINES_EXACT the substitutions instead run in
 // DPTTS2's sequential order (one thread per line): slower, bit-identical.
+#include <algorithm>
 #include <cstdint>
 #include <map>
 #include <mutex>
@@ -904,7 +905,7 @@ static bool shape_ok(LineShape sh, int n, int dir)
 	if (!kok || n > 256 * sh.K) return false;
 	int tpl = 1;
 	while (tpl * sh.K < n) tpl *= 2;
-	if (dir == CDR_DIR_X) return tpl <= FAST_BLOCK_X;
+	if (dir == CDR_DIR_X) return tpl <= FAST_BLOCK_X && sh.cap >= 32;
 	return sh.cap >= 32 && sh.cap <= FAST_BLOCK_Y && tpl <= sh.cap;
 }
 
@@ -924,7 +925,9 @@ static int launch_fast(const T *so, T *x, const T *b, const T *sor, Dims2 d, int
 	int tpl_log2 = 0;
 	while ((1 << tpl_log2) * K < n) ++tpl_log2;  // chunks cover 0 .. n - 1, the last one also n
 	const int TPL = 1 << tpl_log2;
-	const int block = DIR == CDR_DIR_X ? FAST_BLOCK_X : (TPL * 32 < cap ? TPL * 32 : cap);
+	// x: cap CTA threads (at least one line, at most FAST_BLOCK_X); y: up to 32
+	// lines, at most cap threads
+	const int block = DIR == CDR_DIR_X ? std::min(FAST_BLOCK_X, std::max(TPL, cap)) : (TPL * 32 < cap ? TPL * 32 : cap);
 	const int G = block / TPL;
 	k_lines_fast<T, NS, DIR, K><<<dim3(ceil_div(nlines, G), 1, d.nb), block, 0, st>>>(so, x, b, sor, d, tpitch, first,
 	                                                                                  tpl_log2);
@@ -1039,44 +1042,34 @@ static int tune_dir(const T *so, T *x, const T *b, const T *sor, Dims2 d, int tp
 		if (shape_table().count(key)) return CDR_OK;
 	}
 	const int ks[3] = {sizeof(T) == 4 ? 4 : 2, sizeof(T) == 4 ? 8 : 4, sizeof(T) == 4 ? 16 : 8};
-	const int caps[3] = {256, 512, FAST_BLOCK_Y};
+	// small CTAs spread the few lines of a coarse level over more SMs
+	const int caps[6] = {32, 64, 128, 256, 512, FAST_BLOCK_Y};
+	// Each candidate is timed on one sweep (both colours) after L2 has been
+	// overwritten, best of three: the sweep of a level inside a cycle finds its
+	// arrays in DRAM, and a level that fits in L2 would otherwise favour shapes
+	// that only win on L2-resident data.
+	int dev = 0, l2 = 0;
+	CDR_CUDA_TRY(cudaGetDevice(&dev));
+	CDR_CUDA_TRY(cudaDeviceGetAttribute(&l2, cudaDevAttrL2CacheSize, dev));
+	const size_t flush_bytes = 2 * (size_t)(l2 > 0 ? l2 : 128 << 20);
+	void *flush = nullptr;
+	if (cudaMalloc(&flush, flush_bytes) != cudaSuccess) {  // no room: time without the flush
+		cudaGetLastError();
+		flush = nullptr;
+	}
 	cudaEvent_t e0, e1;
 	CDR_CUDA_TRY(cudaEventCreate(&e0));
 	CDR_CUDA_TRY(cudaEventCreate(&e1));
-	LineShape best = default_shape<T>(n, DIR);
-	float best_ms = 1e30f;
 	int rc = CDR_OK;
-	for (int a = 0; a < 3 && rc == CDR_OK; ++a)
-		for (int c = 0; c < (DIR == CDR_DIR_X ? 1 : 3) && rc == CDR_OK; ++c) {
-			const LineShape sh{ks[a], DIR == CDR_DIR_X ? FAST_BLOCK_X : caps[c]};
-			if (!shape_ok<T>(sh, n, DIR)) continue;
-			float ms = 1e30f;
-			for (int rep = 0; rep < 3 && rc == CDR_OK; ++rep) {
-				rc = launch_lines<T, NS, DIR>(so, x, b, sor, d, tpitch, 1, false, st, &sh);
-				if (rc != CDR_OK) break;
-				if (cudaEventRecord(e0, st) != cudaSuccess) { rc = CDR_ERR_CUDA; break; }
-				for (int it = 0; it < 4 && rc == CDR_OK; ++it)
-					rc = launch_lines<T, NS, DIR>(so, x, b, sor, d, tpitch, 1 + (it & 1), false, st, &sh);
-				if (rc != CDR_OK) break;
-				float t = 0.f;
-				if (cudaEventRecord(e1, st) != cudaSuccess || cudaEventSynchronize(e1) != cudaSuccess ||
-				    cudaEventElapsedTime(&t, e0, e1) != cudaSuccess) {
-					rc = CDR_ERR_CUDA;
-					break;
-				}
-				ms = t < ms ? t : ms;
-			}
-			if (ms < best_ms) { best_ms = ms; best = sh; }
-		}
-	if (DIR == CDR_DIR_X && rc == CDR_OK && xs_ok<T, NS>(d)) {
-		const LineShape sh{xs_K<T>(), FAST_BLOCK_X, 1};
+	auto time_shape = [&](const LineShape &sh) -> float {
 		float ms = 1e30f;
 		for (int rep = 0; rep < 3 && rc == CDR_OK; ++rep) {
-			rc = launch_lines<T, NS, DIR>(so, x, b, sor, d, tpitch, 1, false, st, &sh);
-			if (rc != CDR_OK) break;
-			if (cudaEventRecord(e0, st) != cudaSuccess) { rc = CDR_ERR_CUDA; break; }
-			for (int it = 0; it < 4 && rc == CDR_OK; ++it)
-				rc = launch_lines<T, NS, DIR>(so, x, b, sor, d, tpitch, 1 + (it & 1), false, st, &sh);
+			if ((flush && cudaMemsetAsync(flush, rep, flush_bytes, st) != cudaSuccess) ||
+			    cudaEventRecord(e0, st) != cudaSuccess) {
+				rc = CDR_ERR_CUDA;
+				break;
+			}
+			for (int f = 1; f <= 2 && rc == CDR_OK; ++f) rc = launch_lines<T, NS, DIR>(so, x, b, sor, d, tpitch, f, false, st, &sh);
 			if (rc != CDR_OK) break;
 			float t = 0.f;
 			if (cudaEventRecord(e1, st) != cudaSuccess || cudaEventSynchronize(e1) != cudaSuccess ||
@@ -1086,8 +1079,25 @@ static int tune_dir(const T *so, T *x, const T *b, const T *sor, Dims2 d, int tp
 			}
 			ms = t < ms ? t : ms;
 		}
-		if (ms < best_ms) { best_ms = ms; best = sh; }
+		return ms;
+	};
+	// the default shape stands unless a candidate is at least 5 % faster
+	LineShape best = default_shape<T>(n, DIR);
+	float best_ms = time_shape(best);
+	for (int a = 0; a < 3 && rc == CDR_OK; ++a)
+		for (int c = 0; c < (DIR == CDR_DIR_X ? 4 : 6) && rc == CDR_OK; ++c) {
+			const LineShape sh{ks[a], caps[c]};
+			if (!shape_ok<T>(sh, n, DIR)) continue;
+			const float ms = time_shape(sh);
+			if (ms < 0.95f * best_ms) { best_ms = ms; best = sh; }
+		}
+	if (DIR == CDR_DIR_X && rc == CDR_OK && xs_ok<T, NS>(d)) {
+		const LineShape sh{xs_K<T>(), FAST_BLOCK_X, 1};
+		const float ms = time_shape(sh);
+		if (ms < 0.95f * best_ms) { best_ms = ms; best = sh; }
 	}
+	cudaStreamSynchronize(st);
+	if (flush) cudaFree(flush);
 	cudaEventDestroy(e0);
 	cudaEventDestroy(e1);
 	if (rc != CDR_OK) return rc;

@@ -95,8 +95,8 @@ long long cdr_gpu_launch_count(void);
 /* Launch shape the line-kernel autotuner chose for lines of length n, nlines
  * lines, direction dir (CDR_DIR_*), FP32 (fp32 = 1) or FP64 sweeps, nstencil 3
  * or 5, a single problem (batch = 0) or a batch (batch = 1): elements per
- * thread *K and the CTA size cap *cap (0: x-lines streamed through shared
- * memory, CDR_LINES_STREAM).  Returns CDR_ERR_ARG when no solver of
+ * thread *K and the CTA size cap *cap (x-lines: the CTA size, at most 256;
+ * 0: x-lines streamed through shared memory, CDR_LINES_STREAM).  Returns CDR_ERR_ARG when no solver of
  * this process has tuned that shape.  No counterpart in the reference. */
 int cdr_gpu_lines_shape(int dir, int fp32, int nstencil, int n, int nlines, int batch, int *K, int *cap);
 

@@ -334,6 +334,6 @@ def test_line_autotuner_records_shapes_and_keeps_results():
                     for first in (1,):
                         rc = lib.cdr_gpu_lines_shape(d, 1, 5, nn, nl, 0, ctypes.byref(K), ctypes.byref(cap))
                         assert rc == 0, (l, d)
-                        assert K.value in (4, 8, 16) and cap.value in (0, 256, 512, 1024)
+                        assert K.value in (4, 8, 16) and cap.value in (0, 32, 64, 128, 256, 512, 1024)
     assert res[True][1] < 1e-9 and res[False][1] < 1e-9
     assert abs(res[True][0] - res[False][0]) <= 1

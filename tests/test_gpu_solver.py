@@ -206,18 +206,18 @@ def test_fcycle_fp64_matches_oracle(oracle, relax, ns):
     assert np.abs(s.history - h_ref).max() <= 1e-12 * h_ref.max()
 
 
-def test_fcycle_preconditions_fcg():
-    """The F-cycle as the FCG preconditioner (FP32 cycle) converges; it is not
-    symmetric, so flexible CG needs more iterations with it than with the
-    symmetric V(1,1) (about three times as many here: 133 against 44)."""
+def test_fcycle_fp32_ir_converges_in_fewer_cycles():
+    """The F-cycle (FP32 cycle, FP64 refinement) on a heterogeneous problem:
+    converges, in no more cycles than the V-cycle (each F-cycle also visits
+    the coarse levels first).  Default launch shapes, so the run is fixed."""
     from cedar_b200.solver import Solver2D
-    so, b = P.hetero_diffusion(255)
+    so, b = P.hetero_diffusion(255, sigma=1.0, n_incl=4, contrast=100.0, aniso=0.5)
     its = {}
     for cyc in ("v", "f"):
-        s = Solver2D(so, Config({"solver": {"relaxation": "line-xy", "max-iter": 200, "tol": 1e-3,
-                                            "cycle": {"type": cyc, "nrelax-pre": 1, "nrelax-post": 1}},
-                                 "gpu": {"precision": "fp32-ir", "krylov": "fcg"}}))
+        s = Solver2D(so, Config({"solver": {"relaxation": "line-xy", "max-iter": 60, "tol": 1e-8,
+                                            "cycle": {"type": cyc}},
+                                 "gpu": {"precision": "fp32-ir", "autotune": False}}))
         s.solve(b)
-        assert s.history[-1] < 1e-3
+        assert s.history[-1] < 1e-8, cyc
         its[cyc] = s.iters
-    assert its["f"] <= 4 * its["v"]
+    assert its["f"] <= its["v"]
