@@ -44,6 +44,9 @@ WORKLOAD = ("2D heterogeneous diffusion, 9-pt bilinear FE, 2047x2047 nodes (2048
 # DRAM bytes (read + write) of one fine-level x-line colour launch of the 2047^2 FP32 level,
 # from one ncu capture (--set full, caches flushed): 84.2 MB read + 3.0 MB written
 LINE_X_TRAFFIC = 87.3e6
+# headline FCG: the residual is formed (b - A x) every FCG_REPLACE-th iteration and to confirm convergence,
+# updated as r - alpha A p in between
+FCG_REPLACE = 10
 
 
 def parse():
@@ -76,7 +79,7 @@ def profile_main(args):
     if args.profile == "fcg":
         conf = {"solver": {"relaxation": "line-xy", "max-iter": args.steps, "tol": 1e-30, "num-levels": 6,
                            "cycle": {"nrelax-pre": 1, "nrelax-post": 1}},
-                "gpu": {"precision": "fp32-ir", "krylov": "fcg", "coarse-solve": "inverse"}}
+                "gpu": {"precision": "fp32-ir", "krylov": "fcg", "coarse-solve": "inverse", "fcg-replace": FCG_REPLACE}}
     else:
         conf = {"solver": {"relaxation": "line-xy", "max-iter": args.steps, "tol": 1e-30},
                 "gpu": {"precision": "fp32-ir"}}
@@ -242,11 +245,11 @@ def main():
     n = args.n
     pitch = ((n + 2 + 31) // 32) * 32
 
-    def mk(prec, krylov, npre, npost, tol, maxiter, levels=-1, coarse="banded"):
+    def mk(prec, krylov, npre, npost, tol, maxiter, levels=-1, coarse="banded", replace=1):
         conf = Config({"solver": {"relaxation": "line-xy", "max-iter": maxiter, "tol": tol, "num-levels": levels,
                                   "cycle": {"nrelax-pre": npre, "nrelax-post": npost}},
                        "gpu": {"precision": prec, "graph": True, "krylov": krylov, "coarse-solve": coarse,
-                               "autotune": not args.no_autotune}})
+                               "autotune": not args.no_autotune, "fcg-replace": replace}})
         return Solver2D(so, conf, stream=sh)
 
     # headline: flexible CG preconditioned by one line-xy V(1,1) cycle whose coarsest level is ~64^2,
@@ -255,8 +258,8 @@ def main():
     while m > 64:  # cdr2::solver's coarsening: (n - 1) / 2 + 1 per level
         m = (m - 1) // 2 + 1
         nlev += 1
-    s32 = mk("fp32-ir", "fcg", 1, 1, args.tol, args.maxiter, nlev, "inverse")
-    s64 = mk("fp64", "fcg", 1, 1, args.tol, args.maxiter, nlev, "inverse")
+    s32 = mk("fp32-ir", "fcg", 1, 1, args.tol, args.maxiter, nlev, "inverse", FCG_REPLACE)
+    s64 = mk("fp64", "fcg", 1, 1, args.tol, args.maxiter, nlev, "inverse", FCG_REPLACE)
     setup32, _ = s32.timings()
     setup64, _ = s64.timings()
     with torch.cuda.stream(stream):
@@ -372,9 +375,10 @@ def main():
            "ms_per_step": ms32, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
            "dtype": "f32 cycle + f64 outer iteration", "data": "synthetic",
            "config": {"workload": WORKLOAD, "n": n, "levels": s32.nlevels, "line_autotune": not args.no_autotune,
-                      "solver": "flexible CG (FP64 recurrences, true residual every iteration) preconditioned by "
-                                "one line-xy V(1,1) cycle over %d levels (coarsest %d^2, solved with its explicit "
-                                "inverse); FP32 cycle (value) vs FP64 cycle (fp64_ms)" % (nlev, m),
+                      "solver": "flexible CG (FP64 recurrences; residual formed as b - A x every %d iterations "
+                                "and to confirm convergence, updated in between) preconditioned by one line-xy "
+                                "V(1,1) cycle over %d levels (coarsest %d^2, solved with its explicit inverse); FP32 "
+                                "cycle (value) vs FP64 cycle (fp64_ms)" % (FCG_REPLACE, nlev, m),
                       "tol": args.tol,
                       "tol_note": "1e-10 is below this problem's FP64 rounding floor: eps*|A||x|/|b| = %.1e at "
                                   "the FP64 solution, and no solver's relative residual goes below ~5e-5 here "

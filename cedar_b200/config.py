@@ -11,7 +11,9 @@ default; "sequential": DPTTRS order, bit-identical to the reference), ``autotune
 the line kernels' launch shapes per level at setup, once per shape and process), ``line-stream`` (bool,
 default false: x-line sweeps of 256-2048 points by the persistent kernel whose rows arrive in shared memory
 by bulk copies; the autotuner also considers it), ``krylov`` ("none": the
-reference's outer loop, the default; "fcg": the cycle preconditions flexible conjugate gradients, 2D only) and
+reference's outer loop, the default; "fcg": the cycle preconditions flexible conjugate gradients, 2D only),
+``fcg-replace`` (FCG forms the residual b - A x every this many iterations and updates it as r - alpha A p in
+between; 1, the default: every iteration),
 ``coarse-solve`` ("banded": the reference's DPBTRS, the default; "inverse": the setup forms the coarsest
 operator's inverse and every cycle multiplies by it, 2D only — for a coarsest level of thousands of unknowns)
 and ``fp32-levels`` (the FP32 cycle keeps this many finest levels in FP32, the rest in FP64; 0 = all, 2D only).
@@ -91,6 +93,9 @@ class MLSettings:
         self.fp32_levels = int(conf.get("gpu.fp32-levels", 0))
         if self.fp32_levels < 0:
             raise ValueError("invalid gpu.fp32-levels: %d" % self.fp32_levels)
+        self.fcg_replace = int(conf.get("gpu.fcg-replace", 1))
+        if self.fcg_replace < 0:
+            raise ValueError("invalid gpu.fcg-replace: %d" % self.fcg_replace)
         self.coarse_solve = conf.get("gpu.coarse-solve", "banded")
         if self.coarse_solve not in ("banded", "inverse"):
             raise ValueError("invalid gpu.coarse-solve: %s" % self.coarse_solve)

@@ -6,11 +6,13 @@
 // z = M r of Notay's flexible CG:
 //   beta = -(z . q_prev) / (p_prev . q_prev)      (0 on the first iteration)
 //   p = z + beta p_prev,  q = A p,  alpha = (p . r) / (p . q)
-//   x += alpha p,  r = b - A x
-// The residual is formed anew from x every iteration (not updated as r -= alpha
-// q): on high-contrast operators the updated residual drifts from b - A x by
-// orders of magnitude before it converges, while the formed one stays at the
-// FP64 floor eps |A||x|.  The products read the ghost ring as the residual
+//   x += alpha p,  r = b - A x  (or r -= alpha q)
+// By default the residual is formed anew from x every iteration: on
+// high-contrast operators the updated residual r -= alpha q drifts from b - A x
+// by orders of magnitude before it converges, while the formed one stays at
+// the FP64 floor eps |A||x|.  With a replacement period m > 1 the solver forms
+// it every m-th iteration and updates it in between (k_fcg_update_rec, one
+// pass over the operator fewer).  The products read the ghost ring as the residual
 // kernels do.  All of it is FP64.  Three kernels per iteration, each
 // ending in a deterministic grid reduction: every block writes its partial
 // sums, and the last block to finish (an atomic ticket) adds the partials in
@@ -66,6 +68,22 @@ __device__ __forceinline__ bool fcg_point(const Dims2 &d, int row, int &i, int &
 	i = blockIdx.x * TX + threadIdx.x + 1;
 	j = blockIdx.y * (TY * FR) + threadIdx.y + 1 + row * TY;
 	return i <= d.nx && j <= d.ny;
+}
+
+// z = 0 at interior point (i, j) and, on the edges, at its ghost neighbours
+template <typename TZ>
+__device__ __forceinline__ void zero_z(TZ *__restrict__ z, size_t k, int i, int j, const Dims2 &d)
+{
+	const int pitch = d.pitch;
+	z[k] = TZ(0);
+	if (i == 1) z[k - 1] = TZ(0);
+	if (i == d.nx) z[k + 1] = TZ(0);
+	if (j == 1) z[k - pitch] = TZ(0);
+	if (j == d.ny) z[k + pitch] = TZ(0);
+	if (i == 1 && j == 1) z[k - pitch - 1] = TZ(0);
+	if (i == d.nx && j == 1) z[k - pitch + 1] = TZ(0);
+	if (i == 1 && j == d.ny) z[k + pitch - 1] = TZ(0);
+	if (i == d.nx && j == d.ny) z[k + pitch + 1] = TZ(0);
 }
 
 // beta from z . q_prev
@@ -166,15 +184,7 @@ __global__ void __launch_bounds__(TX *TY) k_fcg_update(const double *__restrict_
 			r[k] = rk;
 			acc[0] += rk * rk;
 			rin[k] = (TZ)rk;
-			z[k] = TZ(0);
-			if (i == 1) z[k - 1] = TZ(0);
-			if (i == d.nx) z[k + 1] = TZ(0);
-			if (j == 1) z[k - pitch] = TZ(0);
-			if (j == d.ny) z[k + pitch] = TZ(0);
-			if (i == 1 && j == 1) z[k - pitch - 1] = TZ(0);
-			if (i == d.nx && j == 1) z[k - pitch + 1] = TZ(0);
-			if (i == 1 && j == d.ny) z[k + pitch - 1] = TZ(0);
-			if (i == d.nx && j == d.ny) z[k + pitch + 1] = TZ(0);
+			zero_z(z, k, i, j, d);
 		}
 	grid_sums<1>(acc, partial, &S->ticket[2], [&](const double *v) {
 		S->rr = v[0];
@@ -183,10 +193,48 @@ __global__ void __launch_bounds__(TX *TY) k_fcg_update(const double *__restrict_
 	});
 }
 
-// Start (or restart) from r: the preconditioner input, a zero z and first = 1.
+// The same step with the residual updated instead of formed: x_new = x + alpha
+// p, r -= alpha q (q = A p of this iteration; no pass over the operator),
+// |r|^2, the preconditioner input and z = 0.
+template <typename TZ>
+__global__ void __launch_bounds__(TX *TY) k_fcg_update_rec(double *__restrict__ x0, double *__restrict__ x1,
+                                                           double *__restrict__ r, const double *__restrict__ p0,
+                                                           const double *__restrict__ p1,
+                                                           const double *__restrict__ q, TZ *__restrict__ rin,
+                                                           TZ *__restrict__ z, Dims2 d, double *__restrict__ partial,
+                                                           FcgScalars *S)
+{
+	const int pitch = d.pitch;
+	const bool odd = S->iter & 1;
+	const double *__restrict__ pnew = odd ? p0 : p1;
+	const double *__restrict__ xold = odd ? x1 : x0;
+	double *__restrict__ xnew = odd ? x0 : x1;
+	const double alpha = S->alpha;
+	double acc[1] = {0.0};
+	int i, j;
+#pragma unroll
+	for (int row = 0; row < FR; ++row)
+		if (fcg_point(d, row, i, j)) {
+			const size_t k = (size_t)j * pitch + i;
+			xnew[k] = madd(alpha, pnew[k], xold[k]);
+			const double rk = madd(-alpha, q[k], r[k]);
+			r[k] = rk;
+			acc[0] += rk * rk;
+			rin[k] = (TZ)rk;
+			zero_z(z, k, i, j, d);
+		}
+	grid_sums<1>(acc, partial, &S->ticket[2], [&](const double *v) {
+		S->rr = v[0];
+		S->iter += 1;
+		S->first = 0;
+	});
+}
+
+// Start from r: the preconditioner input, a zero z and (restart) first = 1,
+// iter = 0; without restart the recurrences go on from the new r.
 template <typename TZ>
 __global__ void __launch_bounds__(TX *TY) k_fcg_load(const double *__restrict__ r, TZ *__restrict__ rin,
-                                                     TZ *__restrict__ z, Dims2 d, FcgScalars *S)
+                                                     TZ *__restrict__ z, Dims2 d, FcgScalars *S, int restart)
 {
 	const int i = blockIdx.x * TX + threadIdx.x, j = blockIdx.y * TY + threadIdx.y;
 	if (i > d.nx + 1 || j > d.ny + 1) return;
@@ -194,7 +242,7 @@ __global__ void __launch_bounds__(TX *TY) k_fcg_load(const double *__restrict__ 
 	const bool in = i >= 1 && i <= d.nx && j >= 1 && j <= d.ny;
 	rin[k] = in ? (TZ)r[k] : TZ(0);
 	z[k] = TZ(0);
-	if (i == 0 && j == 0) {
+	if (restart && i == 0 && j == 0) {
 		S->first = 1;
 		S->iter = 0;
 	}
@@ -203,20 +251,21 @@ __global__ void __launch_bounds__(TX *TY) k_fcg_load(const double *__restrict__ 
 }  // namespace
 
 template <typename TZ>
-int fcg_load(const double *r, TZ *rin, TZ *z, Dims2 d, FcgScalars *S, cudaStream_t st)
+int fcg_load(const double *r, TZ *rin, TZ *z, Dims2 d, FcgScalars *S, cudaStream_t st, bool restart)
 {
-	k_fcg_load<TZ><<<dim3(ceil_div(d.nx + 2, TX), ceil_div(d.ny + 2, TY)), dim3(TX, TY), 0, st>>>(r, rin, z, d, S);
+	k_fcg_load<TZ><<<dim3(ceil_div(d.nx + 2, TX), ceil_div(d.ny + 2, TY)), dim3(TX, TY), 0, st>>>(r, rin, z, d, S,
+	                                                                                         restart ? 1 : 0);
 	CDR_LAUNCH_CHECK();
 	return CDR_OK;
 }
-template int fcg_load<double>(const double *, double *, double *, Dims2, FcgScalars *, cudaStream_t);
-template int fcg_load<float>(const double *, float *, float *, Dims2, FcgScalars *, cudaStream_t);
+template int fcg_load<double>(const double *, double *, double *, Dims2, FcgScalars *, cudaStream_t, bool);
+template int fcg_load<float>(const double *, float *, float *, Dims2, FcgScalars *, cudaStream_t, bool);
 
 size_t fcg_scratch_doubles(Dims2 d) { return 2 * (size_t)ceil_div(d.nx, TX) * ceil_div(d.ny, TY * FR); }
 
 template <typename TZ>
 int fcg_step(const double *so, int ns, TZ *z, TZ *rin, double *x0, double *x1, const double *b, double *r,
-             double *p0, double *p1, double *q, Dims2 d, double *partial, FcgScalars *S, cudaStream_t st)
+             double *p0, double *p1, double *q, Dims2 d, double *partial, FcgScalars *S, cudaStream_t st, bool formed)
 {
 	const dim3 nb(ceil_div(d.nx, TX), ceil_div(d.ny, TY * FR)), blk(TX, TY);
 	k_fcg_beta<TZ><<<nb, blk, 0, st>>>(z, q, d, partial, S);
@@ -224,14 +273,15 @@ int fcg_step(const double *so, int ns, TZ *z, TZ *rin, double *x0, double *x1, c
 	if (ns == 5) k_fcg_dir<TZ, 5><<<nb, blk, 0, st>>>(so, z, p0, p1, q, r, d, partial, S);
 	else k_fcg_dir<TZ, 3><<<nb, blk, 0, st>>>(so, z, p0, p1, q, r, d, partial, S);
 	CDR_LAUNCH_CHECK();
-	if (ns == 5) k_fcg_update<TZ, 5><<<nb, blk, 0, st>>>(so, x0, x1, b, r, p0, p1, rin, z, d, partial, S);
+	if (!formed) k_fcg_update_rec<TZ><<<nb, blk, 0, st>>>(x0, x1, r, p0, p1, q, rin, z, d, partial, S);
+	else if (ns == 5) k_fcg_update<TZ, 5><<<nb, blk, 0, st>>>(so, x0, x1, b, r, p0, p1, rin, z, d, partial, S);
 	else k_fcg_update<TZ, 3><<<nb, blk, 0, st>>>(so, x0, x1, b, r, p0, p1, rin, z, d, partial, S);
 	CDR_LAUNCH_CHECK();
 	return CDR_OK;
 }
 template int fcg_step<double>(const double *, int, double *, double *, double *, double *, const double *, double *,
-                              double *, double *, double *, Dims2, double *, FcgScalars *, cudaStream_t);
+                              double *, double *, double *, Dims2, double *, FcgScalars *, cudaStream_t, bool);
 template int fcg_step<float>(const double *, int, float *, float *, double *, double *, const double *, double *,
-                             double *, double *, double *, Dims2, double *, FcgScalars *, cudaStream_t);
+                             double *, double *, double *, Dims2, double *, FcgScalars *, cudaStream_t, bool);
 
 }  // namespace cdrgpu

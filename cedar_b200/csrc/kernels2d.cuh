@@ -67,13 +67,14 @@ struct FcgScalars {
 // r -> preconditioner input rin (zero ghost ring), z = 0, restart the recurrences
 size_t fcg_scratch_doubles(Dims2 d);
 template <typename TZ>
-int fcg_load(const double *r, TZ *rin, TZ *z, Dims2 d, FcgScalars *S, cudaStream_t st);
+int fcg_load(const double *r, TZ *rin, TZ *z, Dims2 d, FcgScalars *S, cudaStream_t st, bool restart = true);
 // One FCG iteration after the preconditioner wrote z (3 launches); leaves the
 // next preconditioner input in rin, z = 0 and |r|^2 in S->rr.  x alternates
 // between x0 and x1: after the step the iterate is in x[S->iter & 1].
 template <typename TZ>
 int fcg_step(const double *so, int ns, TZ *z, TZ *rin, double *x0, double *x1, const double *b, double *r,
-             double *p0, double *p1, double *q, Dims2 d, double *partial, FcgScalars *S, cudaStream_t st);
+             double *p0, double *p1, double *q, Dims2 d, double *partial, FcgScalars *S, cudaStream_t st,
+             bool formed = true);
 
 constexpr size_t kNormScratchBytes = 2048 * sizeof(double);
 

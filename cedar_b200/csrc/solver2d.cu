@@ -59,8 +59,9 @@ struct cdr_gpu_solver {
 	double *kpart = nullptr;  // partial sums of the FCG kernels
 	double *ainv = nullptr;   // CDR_COARSE_INVERSE: inverse of the coarsest operator
 	float *ainv32 = nullptr;
-	cudaGraphExec_t kexec[2] = {nullptr, nullptr};  // FCG iteration graphs: [0] FP64, [1] FP32 cycle
-	long long klaunches[2] = {0, 0};
+	// FCG iteration graphs: [0] FP64, [1] FP32 cycle; [.][0] residual updated, [.][1] formed
+	cudaGraphExec_t kexec[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
+	long long klaunches[2][2] = {{0, 0}, {0, 0}};
 	double *h_norm = nullptr;   // pinned host copy of the norm
 	cudaStream_t st = nullptr;
 	bool own_stream = false;
@@ -106,8 +107,8 @@ struct cdr_gpu_solver {
 	int fcycle(int l, T *x, const T *b);
 	int run_cycle(int prec);
 	template <typename T>
-	int fcg_iteration();
-	int run_fcg(int prec);
+	int fcg_iteration(bool formed);
+	int run_fcg(int prec, bool formed);
 	template <typename T>
 	int tune_lines();
 	int setup();
@@ -318,25 +319,27 @@ int cdr_gpu_solver::run_cycle(int prec)
 // One FCG iteration: the cycle on the preconditioner input (zero initial
 // guess) and the three FCG kernels.
 template <typename T>
-int cdr_gpu_solver::fcg_iteration()
+int cdr_gpu_solver::fcg_iteration(bool formed)
 {
 	Level &F = lv[0];
 	T *z = Arr<T>::x(F), *rin = Arr<T>::b(F);
 	CDR_TRY(cycle<T>(z, rin));
-	return fcg_step<T>(F.so, F.ns, z, rin, kx[0], kx[1], kb, kr, kp[0], kp[1], kq, F.d, kpart, ks, st);
+	return fcg_step<T>(F.so, F.ns, z, rin, kx[0], kx[1], kb, kr, kp[0], kp[1], kq, F.d, kpart, ks, st, formed);
 }
 
-int cdr_gpu_solver::run_fcg(int prec)
+int cdr_gpu_solver::run_fcg(int prec, bool formed)
 {
-	auto body = [&]() -> int { return prec == 0 ? fcg_iteration<double>() : fcg_iteration<float>(); };
+	auto body = [&]() -> int { return prec == 0 ? fcg_iteration<double>(formed) : fcg_iteration<float>(formed); };
 	if (!s.use_graph) return body();
-	if (!kexec[prec]) {
+	cudaGraphExec_t &exec = kexec[prec][formed ? 1 : 0];
+	long long &launches = klaunches[prec][formed ? 1 : 0];
+	if (!exec) {
 		cudaGraph_t g = nullptr;
 		CDR_CUDA_TRY(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
 		const long long before = cdr_gpu_launch_count();
 		int rc = body();
-		klaunches[prec] = cdr_gpu_launch_count() - before;
-		count_launches(-klaunches[prec]);  // captured, not launched
+		launches = cdr_gpu_launch_count() - before;
+		count_launches(-launches);  // captured, not launched
 		cudaError_t e = cudaStreamEndCapture(st, &g);
 		if (rc != CDR_OK) {
 			if (g) cudaGraphDestroy(g);
@@ -346,11 +349,11 @@ int cdr_gpu_solver::run_fcg(int prec)
 			set_error(CDR_ERR_CUDA, "graph capture: %s", cudaGetErrorString(e));
 			return CDR_ERR_CUDA;
 		}
-		CDR_CUDA_TRY(cudaGraphInstantiate(&kexec[prec], g, 0));
+		CDR_CUDA_TRY(cudaGraphInstantiate(&exec, g, 0));
 		cudaGraphDestroy(g);
 	}
-	CDR_CUDA_TRY(cudaGraphLaunch(kexec[prec], st));
-	count_launches(klaunches[prec]);
+	CDR_CUDA_TRY(cudaGraphLaunch(exec, st));
+	count_launches(launches);
 	return CDR_OK;
 }
 
@@ -478,6 +481,7 @@ int cdr_gpu_settings_default(cdr_gpu_settings *s)
 	s->coarse_solve = CDR_COARSE_BANDED;
 	s->fp32_levels = 0;
 	s->cycle = CDR_CYCLE_V;
+	s->krylov_replace = 1;
 	return CDR_OK;
 }
 
@@ -487,8 +491,9 @@ int cdr_gpu_solver_destroy(cdr_gpu_solver *h)
 	if (h->st) cudaStreamSynchronize(h->st);
 	for (auto &g : h->gexec)
 		if (g) cudaGraphExecDestroy(g);
-	for (auto &g : h->kexec)
-		if (g) cudaGraphExecDestroy(g);
+	for (auto &gp : h->kexec)
+		for (auto &g : gp)
+			if (g) cudaGraphExecDestroy(g);
 	for (void *p : h->allocs) cudaFree(p);
 	if (h->h_norm) cudaFreeHost(h->h_norm);
 	if (h->ev0) cudaEventDestroy(h->ev0);
@@ -625,6 +630,10 @@ static int create_any(const cdr_gpu_settings *s, const double *so_src, int ns, i
 		set_error(CDR_ERR_ARG, "invalid cycle type %d", s->cycle);
 		return CDR_ERR_ARG;
 	}
+	if (s->krylov_replace < 0) {
+		set_error(CDR_ERR_ARG, "invalid krylov_replace %d", s->krylov_replace);
+		return CDR_ERR_ARG;
+	}
 	*out = nullptr;
 	cdr_gpu_solver *h = new cdr_gpu_solver();
 	h->s = *s;
@@ -689,13 +698,28 @@ static int solve_fcg(cdr_gpu_solver *h, int *iters, double *hist, int maxhist)
 	if (res0 > 0) {
 		if (prec) CDR_TRY(fcg_load<float>(h->kr, F.b32, F.x32, F.d, h->ks, st));
 		else CDR_TRY(fcg_load<double>(h->kr, F.b, F.x, F.d, h->ks, st));
+		// the residual is formed (b - A x) every m-th iteration, updated in between
+		const int m = h->s.krylov_replace > 1 ? h->s.krylov_replace : 1;
 		while (it < h->s.maxiter) {
-			CDR_TRY(h->run_fcg(prec));
+			const bool formed = (it + 1) % m == 0;
+			CDR_TRY(h->run_fcg(prec, formed));
 			CDR_CUDA_TRY(cudaMemcpyAsync(h->h_norm, &h->ks->rr, sizeof(double), cudaMemcpyDeviceToHost, st));
 			CDR_CUDA_TRY(cudaStreamSynchronize(st));
-			const double rel = std::sqrt(h->h_norm[0]) / res0;
-			if (hist && it < maxhist) hist[it] = rel;
+			double rel = std::sqrt(h->h_norm[0]) / res0;
 			++it;
+			if (std::isfinite(rel) && rel < h->s.tol && !formed) {
+				// an updated residual met the tolerance: form b - A x of the iterate
+				// (in kx[it & 1]); stop only if that meets it too, else go on from it
+				CDR_TRY(residual_2d<double>(F.so, F.ns, h->kx[it & 1], h->kb, h->kr, F.d, h->norm, h->partial, st));
+				CDR_CUDA_TRY(cudaMemcpyAsync(h->h_norm, h->norm, sizeof(double), cudaMemcpyDeviceToHost, st));
+				CDR_CUDA_TRY(cudaStreamSynchronize(st));
+				rel = h->h_norm[0] / res0;
+				if (rel >= h->s.tol && std::isfinite(rel)) {
+					if (prec) CDR_TRY(fcg_load<float>(h->kr, F.b32, F.x32, F.d, h->ks, st, false));
+					else CDR_TRY(fcg_load<double>(h->kr, F.b, F.x, F.d, h->ks, st, false));
+				}
+			}
+			if (hist && it - 1 < maxhist) hist[it - 1] = rel;
 			if (!std::isfinite(rel)) {
 				set_error(CDR_ERR_NUMERIC, "non-finite residual norm at iteration %d", it - 1);
 				return CDR_ERR_NUMERIC;

@@ -54,6 +54,7 @@ def _settings(ms: MLSettings, dim=2):
         raise NotImplementedError("gpu.fp32-levels is a 2D-solver option")
     s.fp32_levels = ms.fp32_levels
     s.cycle = 1 if ms.cycle == "f" else 0
+    s.krylov_replace = ms.fcg_replace
     return s
 
 

@@ -60,8 +60,12 @@ extern "C" {
  * solve loop does.  CDR_KRYLOV_FCG (no counterpart in the reference) uses the
  * cycle, in the solve's precision, as the preconditioner of flexible conjugate
  * gradients (Notay's FCG(1)) with FP64 recurrences; for a symmetric
- * preconditioner choose nrelax_pre == nrelax_post.  The history holds the
- * recurrence residual; the final entry is the true residual b - A x. */
+ * preconditioner choose nrelax_pre == nrelax_post.  The residual is formed
+ * as b - A x every settings.krylov_replace iterations (default: every one)
+ * and updated as r - alpha A p in between; when an updated residual meets the
+ * tolerance the solve forms b - A x and stops only if that meets it too
+ * (otherwise it continues from the formed residual).  The history's final
+ * entry is always a formed residual b - A x. */
 #define CDR_KRYLOV_NONE 0
 #define CDR_KRYLOV_FCG  1
 
@@ -277,6 +281,9 @@ typedef struct cdr_gpu_settings {
 	int fp32_levels;  /* CDR_PREC_F32_IR, 2D solver: the FP32 cycle runs this many finest levels in FP32 and
 	                     the coarser ones in FP64 (latency-bound there, so FP64 costs little); 0 = all (default) */
 	int cycle;        /* "solver.cycle.type": CDR_CYCLE_V (default) or CDR_CYCLE_F; 2D solver only */
+	int krylov_replace; /* CDR_KRYLOV_FCG: form the residual as b - A x every this many iterations and to
+	                       confirm convergence, the iterations between update it as r - alpha A p (one pass
+	                       over the operator fewer); 0 or 1 (default): every iteration */
 } cdr_gpu_settings;
 
 typedef struct cdr_gpu_solver cdr_gpu_solver;
