@@ -70,6 +70,19 @@ int cdr_gpu_version(void) { return 100; }
 long long cdr_gpu_launch_count(void) { return g_launches.load(); }
 size_t cdr_gpu_norm_scratch_bytes(void) { return kNormScratchBytes; }
 
+int cdr_gpu_lines_set_shape(int dir, int fp32, int nstencil, int n, int nlines, int batch, int K, int cap)
+{
+	LineShape sh;
+	sh.K = K;
+	sh.cap = cap == 0 ? 256 : cap;
+	sh.stream = cap == 0 ? 1 : 0;
+	if (!lines_set_shape(dir, fp32 ? 4 : 8, nstencil, n, nlines, batch ? 2 : 1, sh)) {
+		set_error(CDR_ERR_ARG, "line shape K=%d cap=%d cannot run lines of %d points", K, cap, n);
+		return CDR_ERR_ARG;
+	}
+	return CDR_OK;
+}
+
 int cdr_gpu_lines_shape(int dir, int fp32, int nstencil, int n, int nlines, int batch, int *K, int *cap)
 {
 	LineShape sh;

@@ -5,6 +5,9 @@
 // reference's operand order and the library is compiled without FMA
 // contraction, so residual, point Gauss-Seidel, restriction, interpolation and
 // the interpolation setup give the same bits as Cedar's serial kernels.
+#include <cstdint>
+#include <type_traits>
+
 #include "k2_point.cuh"
 
 namespace cdrgpu {
@@ -55,6 +58,108 @@ __global__ void __launch_bounds__(TX *TY) k_residual(const T *__restrict__ so, c
 	}
 }
 
+// The same residual with V = 16 / sizeof(T) consecutive points of a row per
+// thread (16-byte loads; rows 16-byte aligned): a tile is 32 V x 8 points.
+// The left and right neighbours of the vector are separate loads (L1 hits).
+// Per point the operand order of resid_at, so the bits are the same.
+template <typename T, int NS, bool NORM>
+__global__ void __launch_bounds__(TX *TY) k_residual_v(const T *__restrict__ so, const T *__restrict__ q,
+                                                       const T *__restrict__ qf, T *__restrict__ res, Dims2 d,
+                                                       double *__restrict__ partial)
+{
+	constexpr int V = 16 / sizeof(T);
+	using VT = typename std::conditional<sizeof(T) == 4, float4, double2>::type;
+	__shared__ double sh[TX * TY / 32];
+	const int tiles_x = (d.nx + TX * V) / (TX * V);  // columns 0 .. nx
+	const int ntiles = tiles_x * ((d.ny + TY - 1) / TY);
+	const size_t ps = d.plane();
+	const int P = d.pitch;
+	so += d.bofs(NS * ps);
+	q += d.bofs(ps);
+	qf += d.bofs(ps);
+	res += d.bofs(ps);
+	const T *c = so, *w = so + ps, *s = so + 2 * ps, *sw = so + (NS == 5 ? 3 : 0) * ps,
+	        *nw = so + (NS == 5 ? 4 : 0) * ps;
+	auto vld = [](const T *p, T *out) {
+		const VT t = *reinterpret_cast<const VT *>(p);
+		const T *e = reinterpret_cast<const T *>(&t);
+#pragma unroll
+		for (int m = 0; m < V; ++m) out[m] = e[m];
+	};
+	double acc = 0.0;
+	for (int t = NORM ? blockIdx.x : 0; t < (NORM ? ntiles : 1); t += NORM ? gridDim.x : 1) {
+		const int tx = NORM ? t % tiles_x : blockIdx.x, ty = NORM ? t / tiles_x : blockIdx.y;
+		const int i0 = (tx * TX + threadIdx.x) * V;
+		const int j = ty * TY + threadIdx.y + 1;
+		if (i0 > d.nx || j > d.ny) continue;
+		const size_t k = (size_t)j * P + i0;
+		const bool lft = i0 >= 1, rgt = i0 + V <= d.nx + 1;
+		// rows j - 1 (m), j (c), j + 1 (p) of q with the left and right neighbours
+		T qm[V + 2], qc[V + 2], qp[V + 2];
+		vld(q + k - P, qm + 1);
+		vld(q + k, qc + 1);
+		vld(q + k + P, qp + 1);
+		qm[0] = lft ? q[k - P - 1] : T(0);
+		qc[0] = lft ? q[k - 1] : T(0);
+		qp[0] = lft ? q[k + P - 1] : T(0);
+		qm[V + 1] = rgt ? q[k - P + V] : T(0);
+		qc[V + 1] = rgt ? q[k + V] : T(0);
+		qp[V + 1] = rgt ? q[k + P + V] : T(0);
+		T cc[V], ww[V + 1], s0[V], s1[V], bb[V];
+		vld(c + k, cc);
+		vld(w + k, ww);
+		ww[V] = rgt ? w[k + V] : T(0);
+		vld(s + k, s0);
+		vld(s + k + P, s1);
+		vld(qf + k, bb);
+		T sw0[V], sw1[V + 1], nw0[V + 1], nw1[V];
+		if (NS == 5) {
+			vld(sw + k, sw0);
+			vld(sw + k + P, sw1);
+			sw1[V] = rgt ? sw[k + P + V] : T(0);
+			vld(nw + k, nw0);
+			nw0[V] = rgt ? nw[k + V] : T(0);
+			vld(nw + k + P, nw1);
+		}
+		T r[V];
+#pragma unroll
+		for (int m = 0; m < V; ++m) {
+			// column i0 + m: index m + 1 of the q rows
+			T a = madd(ww[m], qc[m], bb[m]);
+			a = madd(ww[m + 1], qc[m + 2], a);
+			a = madd(s0[m], qm[m + 1], a);
+			a = madd(s1[m], qp[m + 1], a);
+			if (NS == 5) {
+				a = madd(sw0[m], qm[m], a);
+				a = madd(nw0[m + 1], qm[m + 2], a);
+				a = madd(nw1[m], qp[m], a);
+				a = madd(sw1[m + 1], qp[m + 2], a);
+			}
+			r[m] = madd(-cc[m], qc[m + 1], a);
+		}
+		if (lft && i0 + V - 1 <= d.nx) {
+			VT o;
+			T *e = reinterpret_cast<T *>(&o);
+#pragma unroll
+			for (int m = 0; m < V; ++m) e[m] = r[m];
+			*reinterpret_cast<VT *>(res + k) = o;
+		} else {
+#pragma unroll
+			for (int m = 0; m < V; ++m)
+				if (i0 + m >= 1 && i0 + m <= d.nx) res[k + m] = r[m];
+		}
+		if (NORM) {
+#pragma unroll
+			for (int m = 0; m < V; ++m)
+				if (i0 + m >= 1 && i0 + m <= d.nx) acc += (double)r[m] * (double)r[m];
+		}
+	}
+	if (NORM) {
+		double sum = block_sum<TX * TY / 32>(acc, sh);
+		if (threadIdx.x == 0 && threadIdx.y == 0) partial[(size_t)blockIdx.z * gridDim.x + blockIdx.x] = sum;
+	}
+}
+
 // one block per problem: out[b] = sqrt(sum of partial[b*n .. b*n+n))
 __global__ void __launch_bounds__(1024) k_norm_finish(const double *__restrict__ partial, int n, double *out)
 {
@@ -79,6 +184,24 @@ int residual_2d(const T *so, int nstencil, const T *x, const T *b, T *r, Dims2 d
 {
 	const int ntiles = ceil_div(d.nx, TX) * ceil_div(d.ny, TY);
 	dim3 blk(TX, TY);
+	// 16-byte rows: the vector kernel (its tiles are V times wider, so fewer partials)
+	constexpr int V = 16 / sizeof(T);
+	if (((uintptr_t)so | (uintptr_t)x | (uintptr_t)b | (uintptr_t)r) % 16 == 0 && d.pitch % V == 0) {
+		const int tx = ceil_div(d.nx + 1, TX * V), ty = ceil_div(d.ny, TY);
+		if (norm_out) {
+			int nb = norm_blocks(d);
+			nb = nb < tx * ty ? nb : tx * ty;
+			if (nstencil == 5) k_residual_v<T, 5, true><<<dim3(nb, 1, d.nb), blk, 0, st>>>(so, x, b, r, d, partial);
+			else k_residual_v<T, 3, true><<<dim3(nb, 1, d.nb), blk, 0, st>>>(so, x, b, r, d, partial);
+			CDR_LAUNCH_CHECK();
+			k_norm_finish<<<d.nb, 1024, 0, st>>>(partial, nb, norm_out);
+		} else {
+			if (nstencil == 5) k_residual_v<T, 5, false><<<dim3(tx, ty, d.nb), blk, 0, st>>>(so, x, b, r, d, nullptr);
+			else k_residual_v<T, 3, false><<<dim3(tx, ty, d.nb), blk, 0, st>>>(so, x, b, r, d, nullptr);
+		}
+		CDR_LAUNCH_CHECK();
+		return CDR_OK;
+	}
 	if (norm_out) {
 		int nb = norm_blocks(d);
 		if (nstencil == 5) k_residual<T, 5, true><<<dim3(nb, 1, d.nb), blk, 0, st>>>(so, x, b, r, d, partial);

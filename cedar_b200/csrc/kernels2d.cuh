@@ -31,6 +31,9 @@ template <typename T>
 int lines_autotune(const T *so, int nstencil, T *x, const T *b, const T *sor, Dims2 d, int tpitch, int dir,
                    cudaStream_t st);
 bool lines_shape(int dir, int tsize, int ns, int n, int nl, int nb, LineShape *out);
+// pin a shape for a line geometry (the autotuner then leaves it); false if the
+// shape cannot run lines of length n
+bool lines_set_shape(int dir, int tsize, int ns, int n, int nl, int nb, LineShape sh);
 template <typename T>
 int restrict_2d(const T *ci, const T *rf, T *bc, Dims2 f, Dims2 c, cudaStream_t st);
 template <typename T>

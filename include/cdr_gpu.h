@@ -103,6 +103,12 @@ long long cdr_gpu_launch_count(void);
  * 0: x-lines streamed through shared memory, CDR_LINES_STREAM).  Returns CDR_ERR_ARG when no solver of
  * this process has tuned that shape.  No counterpart in the reference. */
 int cdr_gpu_lines_shape(int dir, int fp32, int nstencil, int n, int nlines, int batch, int *K, int *cap);
+/* Pin the launch shape (K elements per thread: 4/8/16 FP32, 2/4/8 FP64; CTA
+ * size cap 32..1024, x-lines at most 256; cap 0: streamed x-lines with K = 8
+ * FP32 / 4 FP64) for that geometry in this process; solvers created afterwards
+ * use it and the autotuner leaves it.  CDR_ERR_ARG if the shape cannot run
+ * lines of length n.  No counterpart in the reference. */
+int cdr_gpu_lines_set_shape(int dir, int fp32, int nstencil, int n, int nlines, int batch, int K, int cap);
 
 /* ------------------------------------------------------------------------
  * 2D kernels.  T = double (_f64) or float (_f32).

@@ -337,3 +337,25 @@ def test_line_autotuner_records_shapes_and_keeps_results():
                         assert K.value in (4, 8, 16) and cap.value in (0, 32, 64, 128, 256, 512, 1024)
     assert res[True][1] < 1e-9 and res[False][1] < 1e-9
     assert abs(res[True][0] - res[False][0]) <= 1
+
+
+def test_pinned_line_shape_is_used(lib):
+    """cdr_gpu_lines_set_shape pins a launch shape for a geometry: a solver
+    created afterwards (autotuner on) keeps it, and the solve converges; a shape
+    that cannot run the lines is refused."""
+    import ctypes
+    from cedar_b200.solver import Solver2D
+    from cedar_b200.config import Config
+    n = 383
+    so, b = P.hetero_diffusion(n, sigma=1.0, n_incl=4, contrast=100.0, aniso=0.5)
+    _lib.check(lib.cdr_gpu_lines_set_shape(_lib.DIR_Y, 1, 5, n, n, 0, 8, 64))
+    _lib.check(lib.cdr_gpu_lines_set_shape(_lib.DIR_X, 1, 5, n, n, 0, 8, 0))
+    assert lib.cdr_gpu_lines_set_shape(_lib.DIR_Y, 1, 5, 5000, 5000, 0, 4, 64) != 0
+    s = Solver2D(so, Config({"solver": {"relaxation": "line-xy", "max-iter": 30, "tol": 1e-9},
+                             "gpu": {"precision": "fp32-ir", "autotune": True}}))
+    s.solve(b)
+    assert s.history[-1] < 1e-9
+    for d, want in ((_lib.DIR_Y, (8, 64)), (_lib.DIR_X, (8, 0))):
+        K, cap = ctypes.c_int(), ctypes.c_int()
+        _lib.check(lib.cdr_gpu_lines_shape(d, 1, 5, n, n, 0, ctypes.byref(K), ctypes.byref(cap)))
+        assert (K.value, cap.value) == want
