@@ -86,6 +86,23 @@ __device__ __forceinline__ void zero_z(TZ *__restrict__ z, size_t k, int i, int 
 	if (i == d.nx && j == d.ny) z[k + pitch + 1] = TZ(0);
 }
 
+// The CTA's 32 x 32 points plus a one-point halo of u(k) = f(k), formed once
+// per point into shared memory (0 beyond the ghost ring); the stencil products
+// read their neighbours from there.
+constexpr int HT = TX + 2;  // halo tile edge (TY * FR == TX)
+static_assert(TY * FR == TX, "square tiles");
+
+template <typename F>
+__device__ __forceinline__ void fill_halo(double (&u)[HT][HT], const Dims2 &d, F f)
+{
+	const int i0 = blockIdx.x * TX, j0 = blockIdx.y * (TY * FR);  // halo origin (column i0, row j0)
+	for (int e = threadIdx.y * TX + threadIdx.x; e < HT * HT; e += TX * TY) {
+		const int li = e % HT, lj = e / HT, gi = i0 + li, gj = j0 + lj;
+		u[lj][li] = gi <= d.nx + 1 && gj <= d.ny + 1 ? f((size_t)gj * d.pitch + gi) : 0.0;
+	}
+	__syncthreads();
+}
+
 // beta from z . q_prev
 template <typename TZ>
 __global__ void __launch_bounds__(TX *TY) k_fcg_beta(const TZ *__restrict__ z, const double *__restrict__ q, Dims2 d,
@@ -123,18 +140,20 @@ __global__ void __launch_bounds__(TX *TY) k_fcg_dir(const double *__restrict__ s
 	double *__restrict__ pnew = odd ? p0 : p1;
 	const double beta = S->beta;
 	const double *c = so, *w = so + ps, *s = so + 2 * ps, *sw = so + 3 * ps, *nw = so + 4 * ps;
-	auto P = [&](size_t k) -> double { return madd(beta, pold[k], (double)z[k]); };
+	__shared__ double pt[HT][HT];
+	fill_halo(pt, d, [&](size_t k) -> double { return madd(beta, pold[k], (double)z[k]); });
 	double acc[2] = {0.0, 0.0};
 	int i, j;
 #pragma unroll
 	for (int row = 0; row < FR; ++row)
 		if (fcg_point(d, row, i, j)) {
 			const size_t k = (size_t)j * pitch + i;
-			const double pc = P(k);
-			double nb = w[k] * P(k - 1) + w[k + 1] * P(k + 1) + s[k] * P(k - pitch) + s[k + pitch] * P(k + pitch);
+			const int li = threadIdx.x + 1, lj = threadIdx.y + 1 + row * TY;
+			auto P = [&](int di, int dj) -> double { return pt[lj + dj][li + di]; };
+			const double pc = P(0, 0);
+			double nb = w[k] * P(-1, 0) + w[k + 1] * P(1, 0) + s[k] * P(0, -1) + s[k + pitch] * P(0, 1);
 			if (NS == 5)
-				nb += sw[k] * P(k - pitch - 1) + nw[k + 1] * P(k - pitch + 1) + nw[k + pitch] * P(k + pitch - 1)
-				      + sw[k + pitch + 1] * P(k + pitch + 1);
+				nb += sw[k] * P(-1, -1) + nw[k + 1] * P(1, -1) + nw[k + pitch] * P(-1, 1) + sw[k + pitch + 1] * P(1, 1);
 			const double qk = c[k] * pc - nb;
 			pnew[k] = pc;
 			q[k] = qk;
@@ -167,18 +186,20 @@ __global__ void __launch_bounds__(TX *TY) k_fcg_update(const double *__restrict_
 	double *__restrict__ xnew = odd ? x0 : x1;
 	const double alpha = S->alpha;
 	const double *c = so, *w = so + ps, *s = so + 2 * ps, *sw = so + 3 * ps, *nw = so + 4 * ps;
-	auto X = [&](size_t k) -> double { return madd(alpha, pnew[k], xold[k]); };
+	__shared__ double xt[HT][HT];
+	fill_halo(xt, d, [&](size_t k) -> double { return madd(alpha, pnew[k], xold[k]); });
 	double acc[1] = {0.0};
 	int i, j;
 #pragma unroll
 	for (int row = 0; row < FR; ++row)
 		if (fcg_point(d, row, i, j)) {
 			const size_t k = (size_t)j * pitch + i;
-			const double xc = X(k);
-			double nb = w[k] * X(k - 1) + w[k + 1] * X(k + 1) + s[k] * X(k - pitch) + s[k + pitch] * X(k + pitch);
+			const int li = threadIdx.x + 1, lj = threadIdx.y + 1 + row * TY;
+			auto X = [&](int di, int dj) -> double { return xt[lj + dj][li + di]; };
+			const double xc = X(0, 0);
+			double nb = w[k] * X(-1, 0) + w[k + 1] * X(1, 0) + s[k] * X(0, -1) + s[k + pitch] * X(0, 1);
 			if (NS == 5)
-				nb += sw[k] * X(k - pitch - 1) + nw[k + 1] * X(k - pitch + 1) + nw[k + pitch] * X(k + pitch - 1)
-				      + sw[k + pitch + 1] * X(k + pitch + 1);
+				nb += sw[k] * X(-1, -1) + nw[k + 1] * X(1, -1) + nw[k + pitch] * X(-1, 1) + sw[k + pitch + 1] * X(1, 1);
 			const double rk = bb[k] + nb - c[k] * xc;
 			xnew[k] = xc;
 			r[k] = rk;
