@@ -159,10 +159,27 @@ struct cdr_gpu_solver3 {
 		return CDR_OK;
 	}
 
+	// cycle::fcycle::fmg_cycle / fmg_cycle_helper (include/cedar/cycle/fcycle.h:49-83):
+	// restrict b, recurse (the coarsest level solved directly), then x = P x_c with
+	// a zero residual term and one V-cycle on this level
+	template <typename T>
+	int fcycle(int l, T *x, const T *b)
+	{
+		if (l == L() - 1) return solve_cg_3d<T>(abd, x, b, lv[l].d, st);
+		Level3 &F = lv[l], &C = lv[l + 1];
+		CDR_TRY(restrict_3d<T>(Arr3<T>::ci(C), b, Arr3<T>::b(C), F.d, C.d, st));
+		CDR_TRY(fcycle<T>(l + 1, Arr3<T>::x(C), Arr3<T>::b(C)));
+		CDR_CUDA_TRY(cudaMemsetAsync(x, 0, sizeof(T) * F.d.plane(), st));
+		CDR_CUDA_TRY(cudaMemsetAsync(Arr3<T>::r(F), 0, sizeof(T) * F.d.plane(), st));
+		CDR_TRY(interp_add_3d<T>(Arr3<T>::ci(C), Arr3<T>::x(C), Arr3<T>::r(F), Arr3<T>::so(F), x, F.d, C.d, st));
+		return ncycle<T>(l, x, b);
+	}
+
 	template <typename T>
 	int cycle(T *x, const T *b)
 	{
 		if (L() == 1) return solve_cg_3d<T>(abd, x, b, lv[0].d, st);
+		if (s.cycle == CDR_CYCLE_F) return fcycle<T>(0, x, b);
 		return ncycle<T>(0, x, b);
 	}
 
@@ -426,8 +443,11 @@ static int create3_any(const cdr_gpu_settings *s, const double *so_src, int src_
 		set_error(CDR_ERR_ARG, "invalid precision %d", s->precision);
 		return CDR_ERR_ARG;
 	}
-	if (s->krylov != CDR_KRYLOV_NONE || s->coarse_solve != CDR_COARSE_BANDED || s->fp32_levels != 0 ||
-	    s->cycle != CDR_CYCLE_V) {
+	if (s->cycle != CDR_CYCLE_V && s->cycle != CDR_CYCLE_F) {
+		set_error(CDR_ERR_ARG, "invalid cycle type %d", s->cycle);
+		return CDR_ERR_ARG;
+	}
+	if (s->krylov != CDR_KRYLOV_NONE || s->coarse_solve != CDR_COARSE_BANDED || s->fp32_levels != 0) {
 		set_error(CDR_ERR_UNSUPPORTED, "3D solver: the Krylov outer iteration is implemented for the 2D solver only");
 		return CDR_ERR_UNSUPPORTED;
 	}

@@ -26,8 +26,6 @@ def _settings(ms: MLSettings, dim=2):
         raise NotImplementedError("relaxation %r is a 3D smoother" % ms.relaxation)
     if dim == 3 and ms.relaxation.startswith("line"):
         raise NotImplementedError("relaxation %r is a 2D smoother (3D: point or plane-*)" % ms.relaxation)
-    if ms.cycle != "v" and dim != 2:
-        raise NotImplementedError("the F-cycle is implemented for the 2D solver")
     if ms.coarse_solver != "LU":
         raise NotImplementedError("only the LU (banded Cholesky) coarse solver is implemented")
     s = _lib.Settings()

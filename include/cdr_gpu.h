@@ -286,7 +286,7 @@ typedef struct cdr_gpu_settings {
 	int coarse_solve; /* CDR_COARSE_BANDED (default) or CDR_COARSE_INVERSE; 2D solver only */
 	int fp32_levels;  /* CDR_PREC_F32_IR, 2D solver: the FP32 cycle runs this many finest levels in FP32 and
 	                     the coarser ones in FP64 (latency-bound there, so FP64 costs little); 0 = all (default) */
-	int cycle;        /* "solver.cycle.type": CDR_CYCLE_V (default) or CDR_CYCLE_F; 2D solver only */
+	int cycle;        /* "solver.cycle.type": CDR_CYCLE_V (default) or CDR_CYCLE_F; 2D and 3D solvers (not batched) */
 	int krylov_replace; /* CDR_KRYLOV_FCG: form the residual as b - A x every this many iterations and to
 	                       confirm convergence, the iterations between update it as r - alpha A p (one pass
 	                       over the operator fewer); 0 or 1 (default): every iteration */

@@ -1261,6 +1261,32 @@ void o3_vcycle(o3_solver *h, double *x, const double *b)
 	}
 }
 
+/* cycle::fcycle::fmg_cycle / fmg_cycle_helper (include/cedar/cycle/fcycle.h:49-83):
+ * restrict b, recurse (the coarsest level solved directly), then x = P x_c with a
+ * zero residual term and one V-cycle on this level */
+static void fcycle3(o3_solver *h, int l, double *x, const double *b)
+{
+	struct o3_level *L = &h->lv[l];
+	if (l == h->nlev - 1) {
+		o3_solve_cg(x, b, L->ii, L->jj, L->kk, h->abd, h->bbd, h->nabd1);
+		return;
+	}
+	struct o3_level *C = &h->lv[l + 1];
+	const size_t n = (size_t)L->ii * L->jj * L->kk;
+	o3_restrict(C->ci, b, C->b, L->ii, L->jj, L->kk, C->ii, C->jj, C->kk);
+	fcycle3(h, l + 1, C->x, C->b);
+	memset(x, 0, sizeof(double) * n);
+	memset(L->res, 0, sizeof(double) * n);
+	o3_interp_add(x, C->x, L->res, L->so, C->ci, C->ii, C->jj, C->kk, L->ii, L->jj, L->kk);
+	ncycle3(h, l, x, b);
+}
+
+void o3_cycle(o3_solver *h, double *x, const double *b)
+{
+	if (h->s.cycle == 1 && h->nlev > 1) fcycle3(h, 0, x, b);
+	else o3_vcycle(h, x, b);
+}
+
 int o3_solve(o3_solver *h, const double *b, double *x, double *hist, int maxhist)
 {
 	struct o3_level *L = &h->lv[0];
@@ -1268,7 +1294,7 @@ int o3_solve(o3_solver *h, const double *b, double *x, double *hist, int maxhist
 	double res0 = o3_l2norm(L->res, L->ii, L->jj, L->kk);
 	int it;
 	for (it = 0; it < h->s.maxiter; ++it) {
-		o3_vcycle(h, x, b);
+		o3_cycle(h, x, b);
 		resid3(L, b, x);
 		double rel = o3_l2norm(L->res, L->ii, L->jj, L->kk) / res0;
 		if (hist && it < maxhist) hist[it] = rel;

@@ -14,6 +14,7 @@ typedef struct {
 	double tol;
 	int min_coarse;
 	int relax;
+	int cycle; /* 0: V-cycle, 1: F-cycle (cycle::fcycle) */
 } o3_settings;
 typedef struct o3_solver o3_solver;
 void o3_residual(const double *so, const double *qf, const double *q, double *res, int II, int JJ, int KK);
@@ -34,6 +35,8 @@ void o3_relax_gs7(const double *so, const double *qf, double *q, const double *s
 void o3_setup_interp7(const double *so, double *ci, int iif, int jjf, int kkf, int iic, int jjc, int kkc);
 void o3_destroy(o3_solver *h);
 void o3_vcycle(o3_solver *h, double *x, const double *b);
+/* the cycle of the settings (V or F) */
+void o3_cycle(o3_solver *h, double *x, const double *b);
 int o3_solve(o3_solver *h, const double *b, double *x, double *hist, int maxhist);
 int o3_nlevels(const o3_solver *h);
 int o3_cg_info(const o3_solver *h);

@@ -306,7 +306,7 @@ class Solver:
 class Settings3(ctypes.Structure):
     _fields_ = [("nrelax_pre", ctypes.c_int), ("nrelax_post", ctypes.c_int), ("num_levels", ctypes.c_int),
                 ("maxiter", ctypes.c_int), ("tol", ctypes.c_double), ("min_coarse", ctypes.c_int),
-                ("relax", ctypes.c_int)]
+                ("relax", ctypes.c_int), ("cycle", ctypes.c_int)]
 
 
 RELAX3 = {"point": 0, "plane-xy": 4, "plane-xz": 5, "plane-yz": 6, "plane-xyz": 7}
@@ -339,6 +339,7 @@ def lib3(variant=""):
             "o3_setup_interp7": (None, [P, P, I, I, I, I, I, I]),
             "o3_destroy": (None, [P]),
             "o3_vcycle": (None, [P, P, P]),
+            "o3_cycle": (None, [P, P, P]),
             "o3_solve": (I, [P, P, P, P, I]),
             "o3_nlevels": (I, [P]),
             "o3_cg_info": (I, [P]),
@@ -452,12 +453,13 @@ class Solver3:
     """Serial 3D BoxMG (27-point or seven-point fine operator; point or plane relaxation)."""
 
     def __init__(self, so, nrelax_pre=2, nrelax_post=1, num_levels=-1, maxiter=10, tol=1e-8, min_coarse=3,
-                 relax="point"):
+                 relax="point", cycle="v"):
         self.L = lib3()
         so = np.ascontiguousarray(so, dtype=np.float64)
         assert so.shape[0] in (4, 14)
         self.nz, self.ny, self.nx = so.shape[1] - 2, so.shape[2] - 2, so.shape[3] - 2
-        self.s = Settings3(nrelax_pre, nrelax_post, num_levels, maxiter, tol, min_coarse, RELAX3[relax])
+        self.s = Settings3(nrelax_pre, nrelax_post, num_levels, maxiter, tol, min_coarse, RELAX3[relax],
+                           1 if cycle == "f" else 0)
         self._so = so
         self.h = self.L.o3_create(ctypes.byref(self.s), _p(so), so.shape[0], self.nx, self.ny, self.nz)
 
@@ -489,6 +491,12 @@ class Solver3:
         hist = np.zeros(max(self.s.maxiter, 1))
         n = self.L.o3_solve(self.h, _p(b), _p(x), _p(hist), len(hist))
         return x, hist[:n].copy()
+
+    def vcycle(self, x, b):
+        """One V-cycle from x (in place)."""
+        b = np.ascontiguousarray(b, dtype=np.float64)
+        self.L.o3_vcycle(self.h, _p(x), _p(b))
+        return x
 
     def relax_planes(self, level, direction, x, b, updown):
         """One red-black plane sweep (direction 'xy', 'xz' or 'yz') on level arrays x, b (in place)."""

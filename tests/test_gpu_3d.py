@@ -190,6 +190,25 @@ def test_solver3_fp32_ir_reaches_tol(lib, oracle, nx, ny, nz):
     assert len(s.history) <= len(h_ref) + 2
 
 
+@pytest.mark.parametrize("nx,ny,nz,relax", [(15, 15, 15, "point"), (31, 33, 30, "point"), (15, 13, 16, "plane-xyz")])
+def test_solver3_fcycle_matches_oracle(lib, oracle, nx, ny, nz, relax):
+    """solver.cycle.type = f on the 3D solver (cycle::fcycle): every cycle
+    restarts from the restricted right-hand sides, as in the reference; FP64
+    iterate and history bit-identical to the oracle's F-cycle (sequential line
+    substitutions inside the plane solves)."""
+    from cedar_b200.solver import Solver3D
+    so = make_op3(nx, ny, nz, seed=17, sigma=1.5)
+    b = _rhs3(nx, ny, nz, seed=18)
+    gpu = {"line-solve": "sequential"} if relax != "point" else {}
+    s = Solver3D(so, Config({"solver": {"relaxation": relax, "max-iter": 3, "tol": 1e-30, "cycle": {"type": "f"}},
+                             "gpu": gpu}))
+    x = s.solve(b)
+    x_ref, h_ref = oracle.Solver3(so, maxiter=3, tol=1e-30, relax=relax, cycle="f").solve(b)
+    assert np.array_equal(x, x_ref)
+    assert np.abs(s.history - h_ref).max() <= 1e-12 * max(1.0, h_ref.max())
+    assert h_ref[0] < 0.5 and np.all(h_ref == h_ref[0])  # the F-cycle ignores the incoming x
+
+
 def test_solver3_rejects_unsupported(lib):
     from cedar_b200.solver import Solver3D
     so = make_op3(7, 7, 7)

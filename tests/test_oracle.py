@@ -484,3 +484,26 @@ def test_fcycle_solve_repeats_the_same_iterate(oracle):
     so, b = P.hetero_diffusion(n, sigma=1.0, n_incl=4, contrast=100.0, aniso=0.5)
     x, h = oracle.Solver(so, relax="line-xy", maxiter=4, tol=0, cycle="f").solve(b)
     assert len(h) == 4 and np.all(h == h[0]) and h[0] < 0.5
+
+
+def test_fcycle3_two_levels_is_vcycle_from_interpolated_coarse_solve(oracle):
+    """The 3D F-cycle (the same cycle::fcycle template, include/cedar/cycle/fcycle.h:49-83)
+    on two levels: restrict b, solve the coarse system exactly, x = P x_c with a
+    zero residual term, then one V-cycle from that x; the oracle's 3D kernels
+    composed here give the same bits, whatever the incoming x."""
+    from cedar_b200 import gallery as G
+    from cedar_b200 import problems as P3
+    n = 7
+    k = P3.hetero3_coefficients(n, sigma=1.0, n_incl=2, contrast=10.0)
+    so = np.ascontiguousarray(G.fe3_hetero(k))
+    b = P3.hetero3_rhs(n)
+    sf = oracle.Solver3(so, num_levels=2, maxiter=1, tol=0, cycle="f")
+    x_f, _ = sf.solve(b, x=np.random.default_rng(0).random(b.shape))
+    ci = sf.level_array(1, "ci")
+    soc = sf.level_array(1, "so")
+    abd, info = oracle.setup_cg3(soc)
+    assert info == 0
+    xc = oracle.solve_cg3(abd, oracle.restrict3(ci, b))
+    x0 = oracle.interp_add3(ci, xc, np.zeros_like(b), so, np.zeros_like(b))
+    x_v = oracle.Solver3(so, num_levels=2, maxiter=1, tol=0).vcycle(x0.copy(), b)
+    np.testing.assert_array_equal(x_f, x_v)
