@@ -4,6 +4,8 @@
 Keys and defaults are those of ``ml_settings::init`` (src/multilevel_settings.cc:15-61);
 note that the reference reads ``solver.min_coarse`` (underscore), so the
 ``"min-coarse"`` key found in its example configs has no effect there or here.
+``solver.cg-solver`` is validated as there but, as in the reference's serial
+solvers, does not change the coarsest-level solve (only its MPI solvers read it).
 GPU options live under the ``"gpu"`` object: ``precision`` ("fp64" | "fp32-ir"),
 ``graph`` (bool), ``fuse-coarse`` (levels with both edges at most this many
 points run as one fused kernel; 0 = off; default 32), ``line-solve`` ("scan": parallel line substitutions, the

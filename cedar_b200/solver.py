@@ -26,8 +26,9 @@ def _settings(ms: MLSettings, dim=2):
         raise NotImplementedError("relaxation %r is a 3D smoother" % ms.relaxation)
     if dim == 3 and ms.relaxation.startswith("line"):
         raise NotImplementedError("relaxation %r is a 2D smoother (3D: point or plane-*)" % ms.relaxation)
-    if ms.coarse_solver != "LU":
-        raise NotImplementedError("only the LU (banded Cholesky) coarse solver is implemented")
+    # solver.cg-solver ("LU", "cedar", "redist") is read by the reference's MPI solvers only
+    # (src/2d/mpi/solver.cc:68, include/cedar/3d/mpi/solver.h:212); its serial solvers, which
+    # these mirror, always factor the coarsest level (banded Cholesky)
     s = _lib.Settings()
     _lib.check(_lib.load().cdr_gpu_settings_default(ctypes.byref(s)))
     s.relaxation = _lib.RELAX[ms.relaxation]

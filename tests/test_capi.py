@@ -66,3 +66,25 @@ def test_config_keys():
     assert ms.tol == 1e-10 and ms.maxiter == 10
     with pytest.raises(ValueError):
         MLSettings(Config({"solver": {"relaxation": "jacobi"}}))
+
+
+def test_config_gpu_keys_map_to_settings():
+    """The GPU options of the "gpu" object and solver.cycle.type land in
+    cdr_gpu_settings; solver.cg-solver is validated but, as in the reference's
+    serial solvers, leaves the coarsest-level solve alone."""
+    from cedar_b200.config import Config, MLSettings
+    from cedar_b200.solver import _settings
+    ms = MLSettings(Config({"solver": {"relaxation": "line-xy", "cycle": {"type": "f"}, "cg-solver": "cedar"},
+                            "gpu": {"precision": "fp32-ir", "krylov": "fcg", "coarse-solve": "inverse",
+                                    "fp32-levels": 2, "fcg-replace": 10, "autotune": False, "line-stream": True,
+                                    "line-solve": "sequential"}}))
+    s = _settings(ms)
+    assert (s.cycle, s.krylov, s.coarse_solve, s.fp32_levels, s.krylov_replace) == (1, 1, 1, 2, 10)
+    assert s.precision == _lib.PREC["fp32-ir"]
+    assert s.line_flags == _lib.LINES_EXACT | _lib.LINES_NOTUNE | _lib.LINES_STREAM
+    s3 = _settings(MLSettings(Config({"solver": {"relaxation": "plane-xyz", "cycle": {"type": "f"}}})), dim=3)
+    assert s3.cycle == 1
+    with pytest.raises(ValueError):
+        MLSettings(Config({"solver": {"cg-solver": "dense"}}))
+    with pytest.raises(ValueError):
+        MLSettings(Config({"gpu": {"fcg-replace": -1}}))
