@@ -70,6 +70,15 @@ int cdr_gpu_version(void) { return 100; }
 long long cdr_gpu_launch_count(void) { return g_launches.load(); }
 size_t cdr_gpu_norm_scratch_bytes(void) { return kNormScratchBytes; }
 
+int cdr_gpu_lines_stream_status(cudaStream_t s)
+{
+	if (const unsigned to = lines_stream_timeouts(s)) {
+		set_error(CDR_ERR_NUMERIC, "%u streamed line-sweep CTAs gave up waiting for their rows", to);
+		return CDR_ERR_NUMERIC;
+	}
+	return CDR_OK;
+}
+
 int cdr_gpu_lines_set_shape(int dir, int fp32, int nstencil, int n, int nlines, int batch, int K, int cap)
 {
 	LineShape sh;

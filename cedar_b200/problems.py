@@ -134,7 +134,7 @@ def gaussian_field3(nc, ell, sigma, seed):
     K2 = kx[:, None, None] ** 2 + kx[None, :, None] ** 2 + kz[None, None, :] ** 2
     spec = np.sqrt(np.exp(-0.5 * ell * ell * K2))
     noise = rng.standard_normal((nc, nc, nc))
-    fld = np.fft.irfftn(np.fft.rfftn(noise) * spec, s=(nc, nc, nc))
+    fld = np.fft.irfftn(np.fft.rfftn(noise) * spec, s=(nc, nc, nc), axes=(0, 1, 2))
     fld -= fld.mean()
     std = fld.std()
     if std > 0:

@@ -190,6 +190,12 @@ int cdr_gpu_setup_lines_2d_f32(const double *so, int nstencil, float *sor, int n
  * arithmetic as the default kernel with the same K (bit-identical results);
  * the autotuner also times it as a candidate. */
 #define CDR_LINES_STREAM 4
+/* Status of the streamed x-line kernel since the last call, read on stream s
+ * (synchronises it): CDR_ERR_NUMERIC if a CTA gave up waiting for its staged
+ * rows (a bounded wait; the sweep's result is then incomplete), else CDR_OK.
+ * The 2D solver checks it after every solve; kernel-level callers that use
+ * CDR_LINES_STREAM or a streamed pinned shape call it themselves. */
+int cdr_gpu_lines_stream_status(cudaStream_t s);
 int cdr_gpu_relax_lines_2d_f64(const double *so, int nstencil, double *x, const double *b, const double *sor,
                                int nx, int ny, int pitch, int tpitch, int dir, int updown, int flags,
                                cudaStream_t stream);

@@ -274,6 +274,7 @@ def test_streamed_x_lines(lib, oracle, precision, nx, ny, ns):
         np.testing.assert_array_equal(g[-1], 0.0)
         np.testing.assert_array_equal(g[:, 0], 0.0)
         np.testing.assert_array_equal(g[:, nx + 1], 0.0)
+    assert lib.cdr_gpu_lines_stream_status(stream()) == 0  # no CTA gave up waiting
 
 
 def test_line_setup_reports_nonpositive_pivot(lib):
