@@ -9,8 +9,10 @@
 // A^{-1} from the same factor (one column per thread, both sweeps per column,
 // FP64) and each cycle applies it as a matrix-vector product (memory bound,
 // ~n^2 words per solve).  The result equals DPBTRS's to rounding, not bitwise.
+#include <cstdint>
 #include <type_traits>
 
+#include "k2_bulk.cuh"
 #include "k2_point.cuh"
 #include "kernels2d.cuh"
 
@@ -131,7 +133,105 @@ __global__ void __launch_bounds__(256) k_cg_inv_apply(const T *__restrict__ ainv
 	}
 }
 
+// The same product with the inverse's rows streamed into shared memory by bulk
+// asynchronous copies, IA_STAGES rows ahead per CTA (one mbarrier per stage;
+// two stages leave room for four CTAs per SM, whose rows overlap),
+// so that DRAM keeps streaming while the CTA sums the current row: one row per
+// CTA step, 256 threads, 16-byte row loads from shared memory, FP64 partial
+// sums reduced in a fixed order.  Rows must be 16-byte multiples.  Every wait
+// is bounded; a CTA that gives up is counted in g_inv_timeouts and returns.
+constexpr int IA_STAGES = 2, IA_BLOCK = 256;
+__device__ unsigned g_inv_timeouts;
+
+template <typename T>
+__global__ void __launch_bounds__(IA_BLOCK) k_cg_inv_apply_bulk(const T *__restrict__ ainv, T *__restrict__ q,
+                                                                const T *__restrict__ qf, Dims2 d)
+{
+	extern __shared__ __align__(128) unsigned char ia_raw[];
+	__shared__ double red[IA_BLOCK / 32];
+	constexpr int V = 16 / sizeof(T);
+	using VT = typename std::conditional<sizeof(T) == 4, float4, double2>::type;
+	const int n = d.nx * d.ny;
+	uint64_t *bar = reinterpret_cast<uint64_t *>(ia_raw);
+	T *bs = reinterpret_cast<T *>(ia_raw + 128);
+	T *rows = bs + ((n + 31) & ~31);
+	const unsigned row_bytes = (unsigned)n * sizeof(T);
+	const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, G = gridDim.x;
+	auto issue = [&](int r, int st) {
+		asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+		mbar_expect_tx(&bar[st], row_bytes);
+		bulk_g2s(rows + (size_t)st * n, ainv + (size_t)r * n, row_bytes, &bar[st]);
+	};
+	if (tid == 0) {
+		for (int st = 0; st < IA_STAGES; ++st) mbar_init(&bar[st], 1);
+		asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+	}
+	__syncthreads();
+	if (tid == 0)
+		for (int st = 0; st < IA_STAGES; ++st)
+			if ((int)blockIdx.x + st * G < n) issue(blockIdx.x + st * G, st);
+	for (int e = tid; e < n; e += IA_BLOCK) {  // b compacted while the first rows arrive
+		const int jj = e / d.nx;
+		bs[e] = qf[d.at(e - jj * d.nx + 1, jj + 1)];
+	}
+	__syncthreads();
+	int k = 0;
+	for (int r = blockIdx.x; r < n; r += G, ++k) {
+		const int st = k % IA_STAGES;
+		const bool ok = mbar_wait_bounded(&bar[st], (unsigned)(k / IA_STAGES) & 1u);
+		if (!__syncthreads_and(ok)) {
+			// give up: wait (bounded) for the other stages' copies in flight, then leave
+			if (tid == 0) {
+				atomicAdd(&g_inv_timeouts, 1u);
+				for (int s2 = 1; s2 < IA_STAGES; ++s2)
+					if (r + s2 * G < n) mbar_wait_bounded(&bar[(k + s2) % IA_STAGES], (unsigned)((k + s2) / IA_STAGES) & 1u);
+			}
+			return;
+		}
+		const VT *row = reinterpret_cast<const VT *>(rows + (size_t)st * n);
+		const VT *bv = reinterpret_cast<const VT *>(bs);
+		double a = 0.0;
+		for (int j = tid; j < n / V; j += IA_BLOCK) {
+			const VT w = row[j], x = bv[j];
+			const T *wt = reinterpret_cast<const T *>(&w), *xt = reinterpret_cast<const T *>(&x);
+#pragma unroll
+			for (int v = 0; v < V; ++v) a += (double)wt[v] * (double)xt[v];
+		}
+		for (int o = 16; o > 0; o >>= 1) a += __shfl_down_sync(0xffffffffu, a, o);
+		if (lane == 0) red[warp] = a;
+		__syncthreads();  // the stage is read, the warp sums are in
+		if (tid == 0) {
+			double sum = 0.0;
+#pragma unroll
+			for (int w = 0; w < IA_BLOCK / 32; ++w) sum += red[w];
+			q[d.at(r % d.nx + 1, r / d.nx + 1)] = (T)sum;
+			if (r + IA_STAGES * G < n) issue(r + IA_STAGES * G, st);
+		}
+		__syncthreads();  // red[] is free again
+	}
+}
+
+template <typename T>
+size_t inv_bulk_smem(int n)
+{
+	return 128 + sizeof(T) * ((size_t)((n + 31) & ~31) + (size_t)IA_STAGES * n);
+}
+
 }  // namespace
+
+unsigned cg_inv_timeouts(cudaStream_t st)
+{
+	unsigned v = 0;
+	if (cudaMemcpyFromSymbolAsync(&v, g_inv_timeouts, sizeof v, 0, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+	    cudaStreamSynchronize(st) != cudaSuccess)
+		return 0;
+	if (v) {
+		const unsigned z = 0;
+		cudaMemcpyToSymbolAsync(g_inv_timeouts, &z, sizeof z, 0, cudaMemcpyHostToDevice, st);
+		cudaStreamSynchronize(st);
+	}
+	return v;
+}
 
 int cg_inverse_2d(const double *abd, Dims2 d, double *ainv, cudaStream_t st)
 {
@@ -142,6 +242,10 @@ int cg_inverse_2d(const double *abd, Dims2 d, double *ainv, cudaStream_t st)
 	}
 	k_cg_inverse<<<ceil_div(n, 32), 32, 0, st>>>(abd, n, kd, ldab, ainv);
 	CDR_LAUNCH_CHECK();
+	// the streamed product's shared-memory opt-in (setup time, before any capture)
+	const size_t big = 226 * 1024;
+	CDR_CUDA_TRY(cudaFuncSetAttribute(k_cg_inv_apply_bulk<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)big));
+	CDR_CUDA_TRY(cudaFuncSetAttribute(k_cg_inv_apply_bulk<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)big));
 	return CDR_OK;
 }
 
@@ -153,6 +257,20 @@ int solve_cg_inv_2d(const T *ainv, T *x, const T *b, Dims2 d, cudaStream_t st)
 	if (sm > 48 * 1024) {
 		set_error(CDR_ERR_DIM, "coarsest grid %dx%d too large for the inverse product", d.nx, d.ny);
 		return CDR_ERR_DIM;
+	}
+	const size_t smb = inv_bulk_smem<T>(n);
+	if ((n * sizeof(T)) % 16 == 0 && (uintptr_t)ainv % 16 == 0 && smb <= 226 * 1024) {
+		static const int slots = [] {
+			int dev = 0, sms = 0;
+			if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+				return 148;
+			return sms;
+		}();
+		const int per_sm = (int)((228 * 1024) / (smb + 1024));
+		const int g = slots * (per_sm > 0 ? per_sm : 1);
+		k_cg_inv_apply_bulk<T><<<n < g ? n : g, IA_BLOCK, smb, st>>>(ainv, x, b, d);
+		CDR_LAUNCH_CHECK();
+		return CDR_OK;
 	}
 	const int rows_per_cta = 256 / 32, grid = ceil_div(n, rows_per_cta) < 148 * 4 ? ceil_div(n, rows_per_cta) : 148 * 4;
 	k_cg_inv_apply<T><<<grid, 256, sm, st>>>(ainv, x, b, d);

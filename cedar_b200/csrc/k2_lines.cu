@@ -23,6 +23,7 @@
 #include <mutex>
 #include <tuple>
 
+#include "k2_bulk.cuh"
 #include "k2_point.cuh"
 #include "kernels2d.cuh"
 
@@ -546,50 +547,6 @@ __global__ void __launch_bounds__(XL ? FAST_BLOCK_X : FAST_BLOCK_Y, XL ? 2 : 1)
 // one that gives up is counted in g_xstream_timeouts and the CTA returns.
 namespace {
 __device__ unsigned g_xstream_timeouts;
-
-__device__ __forceinline__ unsigned smem_u32(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
-
-__device__ __forceinline__ void mbar_init(uint64_t *bar, unsigned count)
-{
-	asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
-}
-
-__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, unsigned bytes)
-{
-	asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
-	             : "memory");
-}
-
-__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, unsigned parity)
-{
-	unsigned ok;
-	asm volatile(
-	    "{\n\t.reg .pred p;\n\t"
-	    "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-	    "selp.u32 %0, 1, 0, p;\n\t}"
-	    : "=r"(ok)
-	    : "r"(smem_u32(bar)), "r"(parity)
-	    : "memory");
-	return ok != 0;
-}
-
-// at most 2^18 polls (each try_wait may suspend the thread for a while)
-__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, unsigned parity)
-{
-	for (int it = 0; it < (1 << 18); ++it)
-		if (mbar_try_wait(bar, parity)) return true;
-	return false;
-}
-
-// global -> shared bulk copy completing on *bar (no multicast); 16-byte aligned
-// addresses, size a multiple of 16
-__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, unsigned bytes, uint64_t *bar)
-{
-	asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-	                 smem_u32(dst)),
-	             "l"(src), "r"(bytes), "r"(smem_u32(bar))
-	             : "memory");
-}
 }  // namespace
 
 unsigned lines_stream_timeouts(cudaStream_t st)

@@ -27,6 +27,8 @@ struct LineShape {
 // bounded waits of the streamed x-line kernel that gave up since the last call
 // (read and reset; 0 in a healthy run)
 unsigned lines_stream_timeouts(cudaStream_t st);
+// the same for the streamed explicit-inverse product (k2_cginv.cu)
+unsigned cg_inv_timeouts(cudaStream_t st);
 template <typename T>
 int lines_autotune(const T *so, int nstencil, T *x, const T *b, const T *sor, Dims2 d, int tpitch, int dir,
                    cudaStream_t st);

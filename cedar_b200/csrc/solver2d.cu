@@ -798,6 +798,11 @@ static int solve_loaded(cdr_gpu_solver *h, int *iters, double *hist, int maxhist
 		set_error(CDR_ERR_NUMERIC, "%u streamed line-sweep CTAs gave up waiting for their rows", to);
 		return CDR_ERR_NUMERIC;
 	}
+	if (h->s.coarse_solve == CDR_COARSE_INVERSE)
+		if (const unsigned to = cg_inv_timeouts(st)) {
+			set_error(CDR_ERR_NUMERIC, "%u inverse-product CTAs gave up waiting for their rows", to);
+			return CDR_ERR_NUMERIC;
+		}
 	return CDR_OK;
 }
 
