@@ -41,9 +41,10 @@ PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
 WORKLOAD = ("2D heterogeneous diffusion, 9-pt bilinear FE, 2047x2047 nodes (2048^2 cells), lognormal k "
             "(GRF ell=1/32 sigma=2, seed 1), 64 inclusions x1e4 (seed 2), ky=1e-3 k on y>0.5, rhs U[0,1] h^2 "
             "(seed 3); line-xy relaxation, Galerkin coarsening (levels and coarsest solve: config.solver)")
-# DRAM bytes (read + write) of one fine-level x-line colour launch of the 2047^2 FP32 level,
-# from one ncu capture (--set full, caches flushed): 84.2 MB read + 3.0 MB written
-LINE_X_TRAFFIC = 87.3e6
+# DRAM bytes (read + write) of one fine-level x-line colour launch of the 2047^2 FP32 level
+# (the streamed kernel, k_lines_xstream), from one ncu capture (--set full, caches flushed):
+# 85.1 MB read + 2.9 MB written
+LINE_X_TRAFFIC = 88.1e6
 # headline FCG: the residual is formed (b - A x) every FCG_REPLACE-th iteration and to confirm convergence,
 # updated as r - alpha A p in between
 FCG_REPLACE = 10

@@ -536,15 +536,18 @@ __global__ void __launch_bounds__(XL ? FAST_BLOCK_X : FAST_BLOCK_Y, XL ? 2 : 1)
 }
 
 // ---------------------------------------------------------- streamed x-lines
-// x-lines of one problem with 256 <= n: a persistent CTA walks the lines of a
-// colour (l = blockIdx.x, + gridDim.x, ...).  Each line's rows -- b, x of the
-// two neighbouring lines, the off-line couplings of rows j and j+1 and the
-// line's factors, 7 or 11 rows -- arrive in shared memory by bulk asynchronous
-// copies (cp.async.bulk, one mbarrier per stage) issued two lines ahead, so
-// that DRAM keeps streaming while the CTA runs the scans of the current line.
-// The arithmetic is k_lines_fast's x-line path with the same K on the staged
-// rows: results are bit-identical to it.  Every wait on a stage is bounded;
-// one that gives up is counted in g_xstream_timeouts and the CTA returns.
+// x-lines of one problem with 32K <= n <= 256K: a persistent CTA walks the
+// lines of a colour (l = blockIdx.x, + gridDim.x, ...).  Each line's rows --
+// b, x of the two neighbouring lines, the off-line couplings of rows j and j+1
+// and the line's factors, 7 or 11 rows -- arrive in shared memory by bulk
+// asynchronous copies (cp.async.bulk) completing on one mbarrier.  Every
+// thread takes its chunk of the rows into registers, the stage is released at
+// once and the next line's rows are requested, and the scans of the current
+// line then run while DRAM streams the next one (one stage per CTA, so two
+// CTAs share an SM).  The arithmetic is k_lines_fast's x-line path with the
+// same K: results are bit-identical to it.  Every wait on the stage is
+// bounded; one that gives up is counted in g_xstream_timeouts and the CTA
+// returns.
 namespace {
 __device__ unsigned g_xstream_timeouts;
 }  // namespace
@@ -570,56 +573,50 @@ __host__ __device__ constexpr int xs_rows()
 {
 	return NS == 5 ? 11 : 7;
 }
-// dynamic shared memory of the streamed kernel: two barriers (padded to 128
-// bytes), then two stages of R rows with the level's pitch
+// dynamic shared memory of the streamed kernel: the barrier (padded to 128
+// bytes), then one stage of R rows with the level's pitch
 template <typename T, int NS>
 static size_t xs_smem(int pitch)
 {
-	return 128 + 2 * (size_t)xs_rows<NS>() * pitch * sizeof(T);
+	return 128 + (size_t)xs_rows<NS>() * pitch * sizeof(T);
 }
 
 template <typename T, int NS, int K>
-__global__ void __launch_bounds__(XS_BLOCK) k_lines_xstream(const T *__restrict__ so, T *__restrict__ q,
-                                                            const T *__restrict__ qf, const T *__restrict__ sor,
-                                                            Dims2 d, int first, int nlines)
+__global__ void __launch_bounds__(XS_BLOCK, 2) k_lines_xstream(const T *__restrict__ so, T *__restrict__ q,
+                                                               const T *__restrict__ qf, const T *__restrict__ sor,
+                                                               Dims2 d, int first, int nlines)
 {
 	extern __shared__ __align__(128) unsigned char xs_raw[];
 	__shared__ T sA[XS_BLOCK / 32], sB[XS_BLOCK / 32];
 	constexpr int R = xs_rows<NS>();
 	uint64_t *bar = reinterpret_cast<uint64_t *>(xs_raw);
-	T *stage0 = reinterpret_cast<T *>(xs_raw + 128);
+	T *rows = reinterpret_cast<T *>(xs_raw + 128);
 	const int P = d.pitch, n = d.nx;
-	const size_t ps = d.plane(), stage_elems = (size_t)R * P;
+	const size_t ps = d.plane();
 	const unsigned row_bytes = ((unsigned)(n + 2) * sizeof(T) + 15u) & ~15u;
 	const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
 	const int TPL = blockDim.x;  // threads of the line: chunks of K positions
 	const T *s = so + 2 * ps, *sw = so + (NS == 5 ? 3 : 0) * ps, *nw = so + (NS == 5 ? 4 : 0) * ps;
 	const T *Dp = sor, *Ep = sor + ps;
 
-	// rows of line index li into stage st: b, x(j-1), x(j+1), s(j), s(j+1), d, e
-	// [, sw(j), sw(j+1), nw(j), nw(j+1)]
-	auto issue = [&](int li, int st) {
+	// rows of line index li: b, x(j-1), x(j+1), s(j), s(j+1), d, e [, sw(j), sw(j+1), nw(j), nw(j+1)]
+	auto issue = [&](int li) {
 		const size_t j = (size_t)(first + 2 * li) * P;
-		T *dst = stage0 + st * stage_elems;
 		const T *src[11] = {qf + j, q + j - P, q + j + P, s + j, s + j + P, Dp + j, Ep + j,
 		                    sw + j, sw + j + P, nw + j, nw + j + P};
 		asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-		mbar_expect_tx(&bar[st], R * row_bytes);
+		mbar_expect_tx(bar, R * row_bytes);
 #pragma unroll
-		for (int r = 0; r < R; ++r) bulk_g2s(dst + (size_t)r * P, src[r], row_bytes, &bar[st]);
+		for (int r = 0; r < R; ++r) bulk_g2s(rows + (size_t)r * P, src[r], row_bytes, bar);
 	};
 
 	if (tid == 0) {
-		mbar_init(&bar[0], 1);
-		mbar_init(&bar[1], 1);
+		mbar_init(bar, 1);
 		asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
 	}
 	__syncthreads();
 	const int G = gridDim.x;
-	if (tid == 0) {
-		if ((int)blockIdx.x < nlines) issue(blockIdx.x, 0);
-		if ((int)blockIdx.x + G < nlines) issue(blockIdx.x + G, 1);
-	}
+	if (tid == 0 && (int)blockIdx.x < nlines) issue(blockIdx.x);
 
 	// scan geometry of one line per CTA (k_lines_fast's x-line case with G = 1)
 	const int CW = TPL < 32 ? TPL : 32, NWG = TPL > 32 ? TPL / 32 : 1, kgrp = TPL > 32 ? warp : 0;
@@ -628,27 +625,22 @@ __global__ void __launch_bounds__(XS_BLOCK) k_lines_xstream(const T *__restrict_
 	const bool has = p0 <= n;
 	const bool xtra = has && tid == TPL - 1 && p0 + K == n;
 	const bool full = p0 >= 1 && p0 + K - 1 <= n;
+	const T *rb = rows, *rqm = rows + P, *rqp = rows + 2 * P, *rs0 = rows + 3 * P, *rs1 = rows + 4 * P;
+	const T *rD = rows + 5 * P, *rE = rows + 6 * P;
 
 	int k = 0;
 	for (int li = blockIdx.x; li < nlines; li += G, ++k) {
-		const int st = k & 1;
-		const bool ok = mbar_wait_bounded(&bar[st], (k >> 1) & 1);
+		const bool ok = mbar_wait_bounded(bar, (unsigned)k & 1u);
 		if (!__syncthreads_and(ok)) {
-			// give up: wait (bounded) for the other stage's copies, if any, then leave
-			if (tid == 0) {
-				atomicAdd(&g_xstream_timeouts, 1u);
-				if (li + G < nlines) mbar_wait_bounded(&bar[st ^ 1], ((k + 1) >> 1) & 1);
-			}
+			if (tid == 0) atomicAdd(&g_xstream_timeouts, 1u);
 			return;
 		}
-		const T *rows = stage0 + st * stage_elems;
-		const T *rb = rows, *rqm = rows + P, *rqp = rows + 2 * P, *rs0 = rows + 3 * P, *rs1 = rows + 4 * P;
-		const T *rD = rows + 5 * P, *rE = rows + 6 * P;
 		const int lc = first + 2 * li;
 
-		// 1. right-hand sides of the chunk
-		T r[K];
-		T rx = T(0);
+		// 1. everything this thread needs from the stage into registers, and the
+		// right-hand sides of the chunk
+		T r[K], Ev[K], dv[K];
+		T rx = T(0), Ex = T(0), Dx = T(0), Enext = T(0);
 #pragma unroll
 		for (int m = 0; m < K; ++m) r[m] = T(0);
 		if (has) {
@@ -658,6 +650,13 @@ __global__ void __launch_bounds__(XS_BLOCK) k_lines_xstream(const T *__restrict_
 			vload<T, K>(rqp + p0, qp);
 			vload<T, K>(rs0 + p0, s0);
 			vload<T, K>(rs1 + p0, s1);
+			vload<T, K>(rE + p0, Ev);
+			vload<T, K>(rD + p0, dv);
+			Enext = p0 + K <= n ? rE[p0 + K] : T(0);
+			if (xtra) {
+				Ex = rE[n];
+				Dx = rD[n];
+			}
 #pragma unroll
 			for (int m = 0; m < K; ++m) r[m] = madd(s1[m], qp[m], madd(s0[m], qm[m], b_[m]));
 			if (xtra) rx = madd(rs1[n], rqp[n], madd(rs0[n], rqm[n], rb[n]));
@@ -695,10 +694,10 @@ __global__ void __launch_bounds__(XS_BLOCK) k_lines_xstream(const T *__restrict_
 				}
 			}
 		}
+		__syncthreads();  // the stage is read: the next line's rows may come in
+		if (tid == 0 && li + G < nlines) issue(li + G);
 
 		// 2a. forward substitution y(p) = r(p) - y(p-1) E(p)
-		T Ev[K];
-		if (has) vload<T, K>(rE + p0, Ev);
 		T A = T(1), B = T(0);
 		if (has) {
 #pragma unroll
@@ -710,7 +709,7 @@ __global__ void __launch_bounds__(XS_BLOCK) k_lines_xstream(const T *__restrict_
 				A = a * A;
 			}
 			if (xtra) {
-				const T a = -rE[n];
+				const T a = -Ex;
 				B = madd(a, B, rx);
 				A = a * A;
 			}
@@ -724,21 +723,14 @@ __global__ void __launch_bounds__(XS_BLOCK) k_lines_xstream(const T *__restrict_
 				y = (!full && pos == 1) ? r[m] : madd(-y, Ev[m], r[m]);
 				r[m] = y;
 			}
-			if (xtra) rx = pivot_div(madd(-y, rE[n], rx), rD[n]);
-			constexpr int W = 16 / sizeof(T);
+			if (xtra) rx = pivot_div(madd(-y, Ex, rx), Dx);
 #pragma unroll
-			for (int c = 0; c < K / W; ++c) {
-				T dv[W];
-				vload<T, W>(rD + p0 + c * W, dv);
-#pragma unroll
-				for (int w = 0; w < W; ++w) {
-					const int m = c * W + w, pos = p0 + m;
-					if (full || (pos >= 1 && pos <= n)) r[m] = pivot_div(r[m], dv[w]);
-				}
+			for (int m = 0; m < K; ++m) {
+				const int pos = p0 + m;
+				if (full || (pos >= 1 && pos <= n)) r[m] = pivot_div(r[m], dv[m]);
 			}
 		}
 		// 2b. backward substitution x(p) = y(p)/D(p) - x(p+1) E(p+1)
-		const T Enext = has && p0 + K <= n ? rE[p0 + K] : T(0);
 		A = T(1);
 		B = T(0);
 		if (has) {
@@ -780,10 +772,9 @@ __global__ void __launch_bounds__(XS_BLOCK) k_lines_xstream(const T *__restrict_
 				}
 			}
 		}
-		__syncthreads();  // the stage and the carries are free again
-		if (tid == 0 && li + 2 * G < nlines) issue(li + 2 * G, st);
 	}
 }
+
 
 // Opt every line kernel into the large dynamic shared-memory carve-out once per
 // process (before any graph capture: the solver calls this at creation).
@@ -852,7 +843,11 @@ std::map<LineKey, LineShape> &shape_table()
 template <typename T>
 static LineShape default_shape(int n, int dir)
 {
-	return LineShape{(dir == CDR_DIR_Y && sizeof(T) == 4 && n > 8 * 128) ? 16 : 8, FAST_BLOCK_Y};
+	// FP32 x-lines longer than 1024 points: the streamed kernel (K = 8, the same
+	// results as the register-chunk kernel; a batch or a misaligned level falls
+	// back to that kernel with the same K)
+	const int stream = dir == CDR_DIR_X && sizeof(T) == 4 && n > 1024 ? 1 : 0;
+	return LineShape{(dir == CDR_DIR_Y && sizeof(T) == 4 && n > 8 * 128) ? 16 : 8, FAST_BLOCK_Y, stream};
 }
 
 template <typename T>
