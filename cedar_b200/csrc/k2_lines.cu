@@ -628,6 +628,24 @@ __global__ void __launch_bounds__(XS_BLOCK, 2) k_lines_xstream(const T *__restri
 	const T *rb = rows, *rqm = rows + P, *rqp = rows + 2 * P, *rs0 = rows + 3 * P, *rs1 = rows + 4 * P;
 	const T *rD = rows + 5 * P, *rE = rows + 6 * P;
 
+	// K-element chunk (two 16-byte pieces) from a staged row, the two pieces read
+	// in an order swapped for every other group of four lanes, so that a warp's
+	// 16-byte loads hit all 32 banks (lanes 32 bytes apart would otherwise meet
+	// in pairs)
+	constexpr int W = 16 / sizeof(T);
+	static_assert(K == 2 * W, "two 16-byte pieces per chunk");
+	const int rot = (lane >> 2) & 1;
+	auto sload = [&](const T *p, T(&v)[K]) {
+		using VT = typename Vec16<T>::type;
+		const VT *pv = reinterpret_cast<const VT *>(p);
+		const VT ta = pv[rot], tb = pv[rot ^ 1];
+		const T *ea = reinterpret_cast<const T *>(&ta), *eb = reinterpret_cast<const T *>(&tb);
+#pragma unroll
+		for (int w = 0; w < W; ++w) {
+			v[w] = rot ? eb[w] : ea[w];
+			v[W + w] = rot ? ea[w] : eb[w];
+		}
+	};
 	int k = 0;
 	for (int li = blockIdx.x; li < nlines; li += G, ++k) {
 		const bool ok = mbar_wait_bounded(bar, (unsigned)k & 1u);
@@ -645,13 +663,13 @@ __global__ void __launch_bounds__(XS_BLOCK, 2) k_lines_xstream(const T *__restri
 		for (int m = 0; m < K; ++m) r[m] = T(0);
 		if (has) {
 			T b_[K], qm[K], qp[K], s0[K], s1[K];
-			vload<T, K>(rb + p0, b_);
-			vload<T, K>(rqm + p0, qm);
-			vload<T, K>(rqp + p0, qp);
-			vload<T, K>(rs0 + p0, s0);
-			vload<T, K>(rs1 + p0, s1);
-			vload<T, K>(rE + p0, Ev);
-			vload<T, K>(rD + p0, dv);
+			sload(rb + p0, b_);
+			sload(rqm + p0, qm);
+			sload(rqp + p0, qp);
+			sload(rs0 + p0, s0);
+			sload(rs1 + p0, s1);
+			sload(rE + p0, Ev);
+			sload(rD + p0, dv);
 			Enext = p0 + K <= n ? rE[p0 + K] : T(0);
 			if (xtra) {
 				Ex = rE[n];
@@ -663,10 +681,10 @@ __global__ void __launch_bounds__(XS_BLOCK, 2) k_lines_xstream(const T *__restri
 			if (NS == 5) {
 				const T *rsw0 = rows + 7 * P, *rsw1 = rows + 8 * P, *rnw0 = rows + 9 * P, *rnw1 = rows + 10 * P;
 				T sw0[K], nw0[K], nw1[K], sw1[K];
-				vload<T, K>(rsw0 + p0, sw0);
-				vload<T, K>(rnw0 + p0, nw0);
-				vload<T, K>(rnw1 + p0, nw1);
-				vload<T, K>(rsw1 + p0, sw1);
+				sload(rsw0 + p0, sw0);
+				sload(rnw0 + p0, nw0);
+				sload(rnw1 + p0, nw1);
+				sload(rsw1 + p0, sw1);
 				const T qm_l = p0 >= 1 ? rqm[p0 - 1] : T(0), qp_l = p0 >= 1 ? rqp[p0 - 1] : T(0);
 				const bool rin = p0 + K <= n + 1;
 				const T qm_r = rin ? rqm[p0 + K] : T(0), qp_r = rin ? rqp[p0 + K] : T(0);
