@@ -41,10 +41,11 @@ PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
 WORKLOAD = ("2D heterogeneous diffusion, 9-pt bilinear FE, 2047x2047 nodes (2048^2 cells), lognormal k "
             "(GRF ell=1/32 sigma=2, seed 1), 64 inclusions x1e4 (seed 2), ky=1e-3 k on y>0.5, rhs U[0,1] h^2 "
             "(seed 3); line-xy relaxation, Galerkin coarsening (levels and coarsest solve: config.solver)")
-# DRAM bytes (read + write) of one fine-level x-line colour launch of the 2047^2 FP32 level
-# (the streamed kernel, k_lines_xstream), from one ncu capture (--set full, caches flushed):
-# 85.1 MB read + 2.9 MB written
+# DRAM bytes (read + write) of one fine-level colour launch of the 2047^2 FP32 level, from one ncu
+# capture each (--set full, caches flushed): x-lines (the streamed kernel, k_lines_xstream) 85.1 MB
+# read + 2.9 MB written; y-lines (k_lines_fast, K = 16, 1024 threads) 101.7 MB + 5.3 MB
 LINE_X_TRAFFIC = 88.1e6
+LINE_Y_TRAFFIC = 107.0e6
 # headline FCG: the residual is formed (b - A x) every FCG_REPLACE-th iteration and to confirm convergence,
 # updated as r - alpha A p in between
 FCG_REPLACE = 10
@@ -334,25 +335,33 @@ def main():
         e2e_ms.append((time.perf_counter() - t0) * 1e3)
     e2e = statistics.median(e2e_ms)
 
-    # roofline of the dominant kernel: FP32 x-line sweep of the fine level (2 launches, one per colour)
+    # roofline of the dominant kernel: the FP32 fine-level line sweeps (2 launches each, one per
+    # colour); the y-line sweep has the largest share of an FCG iteration, the x-line sweep is
+    # reported beside it
     p_so, nx, ny, pp, tp, ns = s32.level_info(0, "so", fp32=True)
     p_x, *_ = s32.level_info(0, "x", fp32=True)
     p_b, *_ = s32.level_info(0, "b", fp32=True)
     p_sx, *_ = s32.level_info(0, "sor", fp32=True)
-    reps = 20
-    with torch.cuda.stream(stream):
-        ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
-        for _ in range(3):
-            lib.cdr_gpu_relax_lines_2d_f32(ctypes.c_void_p(p_so), ns, ctypes.c_void_p(p_x), ctypes.c_void_p(p_b),
-                                           ctypes.c_void_p(p_sx), nx, ny, pp, tp, 0, 0, 0, ctypes.c_void_p(sh))
-        ev[0].record(stream)
-        for _ in range(reps):
-            lib.cdr_gpu_relax_lines_2d_f32(ctypes.c_void_p(p_so), ns, ctypes.c_void_p(p_x), ctypes.c_void_p(p_b),
-                                           ctypes.c_void_p(p_sx), nx, ny, pp, tp, 0, 0, 0, ctypes.c_void_p(sh))
-        ev[1].record(stream)
-    torch.cuda.synchronize()
-    sweep_ms = ev[0].elapsed_time(ev[1]) / reps
+    p_sy, *_ = s32.level_info(0, "sory", fp32=True)
+
+    def sweep_time(dirn, p_f):
+        reps = 20
+        with torch.cuda.stream(stream):
+            ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+            for _ in range(3):
+                lib.cdr_gpu_relax_lines_2d_f32(ctypes.c_void_p(p_so), ns, ctypes.c_void_p(p_x), ctypes.c_void_p(p_b),
+                                               ctypes.c_void_p(p_f), nx, ny, pp, tp, dirn, 0, 0, ctypes.c_void_p(sh))
+            ev[0].record(stream)
+            for _ in range(reps):
+                lib.cdr_gpu_relax_lines_2d_f32(ctypes.c_void_p(p_so), ns, ctypes.c_void_p(p_x), ctypes.c_void_p(p_b),
+                                               ctypes.c_void_p(p_f), nx, ny, pp, tp, dirn, 0, 0, ctypes.c_void_p(sh))
+            ev[1].record(stream)
+        torch.cuda.synchronize()
+        return ev[0].elapsed_time(ev[1]) / reps
+
+    sweep_ms = sweep_time(0, p_sx)
     launch_ms = sweep_ms / 2.0
+    ysweep_ms = sweep_time(1, p_sy)
     # launch shapes the setup-time autotuner chose for the fine level (cap 0: streamed x-line kernel)
     shapes = {}
     for dname, dirn, nn, nl in (("x", 0, nx, ny), ("y", 1, ny, nx)):
@@ -367,6 +376,7 @@ def main():
     bytes_per_sweep = 8 * 4 * nx * ny
     peak, peak_kind = peaks()
     achieved = bytes_per_sweep / (sweep_ms * 1e-3) / 1e9
+    y_achieved = bytes_per_sweep / (ysweep_ms * 1e-3) / 1e9
 
     # V-cycle HBM GB/s: algorithmic bytes of one FP32 V(2,1) cycle / measured cycle time
     vcyc_bytes = vcycle_bytes(vc32["solver"], word=4)
@@ -401,11 +411,14 @@ def main():
                       "hbm_gbs": vcyc_bytes / (vc32["ms_per_cycle"] * 1e-3) / 1e9,
                       "fp64_ms": vc64["ms_per_cycle"],
                       "fp64_hbm_gbs": vcycle_bytes(vc64["solver"], word=8) / (vc64["ms_per_cycle"] * 1e-3) / 1e9},
-           "roofline": {"kernel": xkern, "line_shapes": shapes,
-                        "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                        "frac": achieved / peak, "peak_kind": peak_kind,
-                        "traffic": LINE_X_TRAFFIC if n == 2047 else None,
-                        "algorithmic_bytes_per_launch": bytes_per_sweep / 2, "launch_ms": launch_ms},
+           "roofline": {"kernel": "k_lines_fast<float,%d,y,K=%d> (fine-level y-line sweep, 2 launches)"
+                                  % (ns, shapes.get("y", {}).get("K", 0)), "line_shapes": shapes,
+                        "bound": "hbm", "achieved": y_achieved, "peak": peak, "unit": "GB/s",
+                        "frac": y_achieved / peak, "peak_kind": peak_kind,
+                        "traffic": LINE_Y_TRAFFIC if n == 2047 else None,
+                        "algorithmic_bytes_per_launch": bytes_per_sweep / 2, "launch_ms": ysweep_ms / 2.0,
+                        "x_sweep": {"kernel": xkern, "achieved": achieved, "frac": achieved / peak,
+                                    "traffic": LINE_X_TRAFFIC if n == 2047 else None, "launch_ms": launch_ms}},
            "e2e": {"value": e2e, "unit": "ms", "h2d_bytes_per_step": 2 * 8 * (n + 2) ** 2,
                    "d2h_bytes_per_step": 8 * (n + 2) ** 2 + 8 * it32},
            "gpu_launches": int(launches), "clocks": clocks}
