@@ -859,17 +859,18 @@ std::map<LineKey, LineShape> &shape_table()
 }  // namespace
 
 template <typename T>
-static LineShape default_shape(int n, int dir)
+static LineShape default_shape(int n, int dir, int nb = 1)
 {
 	// FP32 x-lines longer than 1024 points: the streamed kernel (K = 8, the same
 	// results as the register-chunk kernel; a batch or a misaligned level falls
 	// back to that kernel with the same K)
 	const int stream = dir == CDR_DIR_X && sizeof(T) == 4 && n > 1024 ? 1 : 0;
 	if (dir == CDR_DIR_Y && sizeof(T) == 4) {
-		// FP32 y-lines: K = 4 in small CTAs for short lines (the shapes the timing
-		// picks there inside a cycle), K = 16 for lines longer than 1024 points
-		if (n <= 160) return LineShape{4, 256, 0};
-		if (n <= 320) return LineShape{4, 128, 0};
+		// FP32 y-lines: for a single problem, K = 4 in small CTAs for short lines
+		// (the shapes the timing picks there inside a cycle); K = 16 for lines
+		// longer than 1024 points
+		if (nb == 1 && n <= 160) return LineShape{4, 256, 0};
+		if (nb == 1 && n <= 320) return LineShape{4, 128, 0};
 		return LineShape{n > 8 * 128 ? 16 : 8, FAST_BLOCK_Y, 0};
 	}
 	return LineShape{8, FAST_BLOCK_Y, stream};
@@ -891,7 +892,7 @@ static LineShape shape_for(int n, int nl, int ns, int nb, int dir)
 {
 	std::lock_guard<std::mutex> lk(g_shape_mu);
 	auto it = shape_table().find(LineKey{dir, (int)sizeof(T), ns, n, nl, nb > 1 ? 2 : 1});
-	return it == shape_table().end() ? default_shape<T>(n, dir) : it->second;
+	return it == shape_table().end() ? default_shape<T>(n, dir, nb) : it->second;
 }
 
 template <typename T, int NS, int DIR, int K>
@@ -980,7 +981,7 @@ static int launch_lines(const T *so, T *x, const T *b, const T *sor, Dims2 d, in
 	const int fpitch = DIR == CDR_DIR_X ? d.pitch : tpitch;
 	const bool aligned = ((uintptr_t)so | (uintptr_t)x | (uintptr_t)b | (uintptr_t)sor) % 16 == 0;
 	LineShape sh = force ? *force : shape_for<T>(n, nl, NS, d.nb, DIR);
-	if (!shape_ok<T>(sh, n, DIR)) sh = default_shape<T>(n, DIR);
+	if (!shape_ok<T>(sh, n, DIR)) sh = default_shape<T>(n, DIR, d.nb);
 	if (!exact && aligned && d.pitch % 16 == 0 && fpitch % 16 == 0 && shape_ok<T>(sh, n, DIR)) {
 		if constexpr (DIR == CDR_DIR_X)
 			if (sh.stream && sh.K == xs_K<T>() && xs_ok<T, NS>(d))
@@ -1020,14 +1021,16 @@ static int tune_dir(const T *so, T *x, const T *b, const T *sor, Dims2 d, int tp
 	}
 	// FP32 results depend on K (and, for y-lines, on the lines per CTA) through
 	// the order in which the scans compose their maps, and the FP32 cycle's
-	// outer iteration count moves with that rounding: FP32 x-lines try only
-	// shapes with the default K (bit-identical among themselves), FP32 y-lines
-	// keep the default, so that every run of an FP32 solve gives the same bits
-	const int kdef = default_shape<T>(n, DIR).K;
-	const bool fixed_bits = sizeof(T) == 4;
+	// outer iteration count moves with that rounding: for a single problem,
+	// FP32 x-lines try only shapes with the default K (bit-identical among
+	// themselves) and FP32 y-lines keep the default, so that every run of an FP32
+	// solve gives the same bits.  Batches (many small problems, or the planes of
+	// a 3D plane smoother) time every candidate.
+	const int kdef = default_shape<T>(n, DIR, d.nb).K;
+	const bool fixed_bits = sizeof(T) == 4 && d.nb == 1;
 	if (fixed_bits && DIR == CDR_DIR_Y) {
 		std::lock_guard<std::mutex> lk(g_shape_mu);
-		shape_table()[key] = default_shape<T>(n, DIR);
+		shape_table()[key] = default_shape<T>(n, DIR, d.nb);
 		return CDR_OK;
 	}
 	const int ks[3] = {sizeof(T) == 4 ? 4 : 2, sizeof(T) == 4 ? 8 : 4, sizeof(T) == 4 ? 16 : 8};
@@ -1075,7 +1078,7 @@ static int tune_dir(const T *so, T *x, const T *b, const T *sor, Dims2 d, int tp
 	// by a few per cent from run to run)
 	const size_t level_bytes = 12 * d.plane() * sizeof(T) * (size_t)d.nb;
 	const float margin = 4 * level_bytes > flush_bytes / 2 ? 0.90f : 0.95f;
-	LineShape best = default_shape<T>(n, DIR);
+	LineShape best = default_shape<T>(n, DIR, d.nb);
 	float best_ms = time_shape(best);
 	for (int a = 0; a < 3 && rc == CDR_OK; ++a)
 		for (int c = 0; c < (DIR == CDR_DIR_X ? 4 : 6) && rc == CDR_OK; ++c) {
@@ -1141,7 +1144,7 @@ int relax_lines_2d(const T *so, int nstencil, T *x, const T *b, const T *sor, Di
                    int updown, int flags, cudaStream_t st)
 {
 	const bool exact = (flags & CDR_LINES_EXACT) != 0;
-	const LineShape dflt = default_shape<T>(dir == CDR_DIR_X ? d.nx : d.ny, dir);
+	const LineShape dflt = default_shape<T>(dir == CDR_DIR_X ? d.nx : d.ny, dir, d.nb);
 	const LineShape streamed{xs_K<T>(), FAST_BLOCK_X, 1};
 	const LineShape *force = (flags & CDR_LINES_NOTUNE) ? &dflt : nullptr;
 	if ((flags & CDR_LINES_STREAM) && dir == CDR_DIR_X) force = &streamed;

@@ -69,22 +69,23 @@ def test_batch_fp64_matches_oracle_per_problem(oracle, relax, ns):
 
 
 def test_batch_fp32_ir_matches_single_solves():
+    """Each problem of an FP32-refined batch converges like a single-problem
+    FP32-refined solve: same tolerance, cycle counts within one, iterates equal
+    to 1e-7 relative (the FP64 refinement pins them; the FP32 cycles differ in
+    rounding, since single problems and batches have different default line
+    shapes on short lines)."""
     from cedar_b200.solver import Solver2D
     nx, ny, nb = 63, 63, 4
     ops, rhs = _batch(nx, ny, nb, 5, seed=40)
-    # one launch shape for both (the autotuner tunes batches and single problems separately,
-    # and FP32 iterates depend on the line kernel's chunking)
     conf = Config({"solver": {"relaxation": "line-xy", "cycle": {"nrelax-pre": 1, "nrelax-post": 1},
                               "max-iter": 40, "tol": 1e-8}, "gpu": {"precision": "fp32-ir", "autotune": False}})
     x, s = _solve_batch(ops, rhs, conf)
     for p in range(nb):
         single = Solver2D(ops[p], conf)
         xs = single.solve(rhs[p])
-        assert s.rel[p] < 1e-8
-        if single.iters == s.iters[p]:
-            assert np.array_equal(x[p], xs)
-        else:  # the batch sums each norm in a different order: a stop may shift by one cycle
-            assert abs(single.iters - s.iters[p]) <= 1
+        assert s.rel[p] < 1e-8 and single.history[-1] < 1e-8
+        assert abs(single.iters - s.iters[p]) <= 1
+        assert np.abs(x[p] - xs).max() <= 1e-7 * np.abs(xs).max()
 
 
 def test_batch_rejects_bad_arguments():
