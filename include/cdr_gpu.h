@@ -185,10 +185,12 @@ int cdr_gpu_setup_lines_2d_f32(const double *so, int nstencil, float *sor, int n
  * whose choice is kept for the process). */
 #define CDR_LINES_NOTUNE 2
 /* Kernel flags: x-lines of a single problem (32K <= nx <= 256K, K = 8 FP32 / 4
- * FP64) by the streamed kernel: a persistent CTA per SM slot whose line rows
- * arrive in shared memory by bulk asynchronous copies two lines ahead.  Same
- * arithmetic as the default kernel with the same K (bit-identical results);
- * the autotuner also times it as a candidate. */
+ * FP64) by the streamed kernel: persistent CTAs (two per SM) whose line rows
+ * arrive in shared memory by bulk asynchronous copies; each CTA takes its
+ * chunks into registers and requests the next line before running the scans.
+ * Same arithmetic as the register-chunk kernel with the same K (bit-identical
+ * results); the default for FP32 x-lines longer than 1024 points, an
+ * autotuner candidate elsewhere. */
 #define CDR_LINES_STREAM 4
 /* Status of the streamed x-line kernel since the last call, read on stream s
  * (synchronises it): CDR_ERR_NUMERIC if a CTA gave up waiting for its staged
