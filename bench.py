@@ -11,12 +11,20 @@ rounding error of b - A x itself, eps*|A||x|/|b|, is ~1e-4 at 2047^2 (the
 coefficients span ~12 orders of magnitude), and the reference's own outer loop
 (repeated V(2,1) cycles; the oracle reproduces it bit for bit) stalls near
 residual 1 besides, contracting the error by ~0.97 per cycle.  The headline
-therefore times flexible CG (FP64 recurrences, true residual every iteration)
+therefore times flexible CG (FP64 recurrences; the residual formed as b - A x
+every FCG_REPLACE-th iteration and to confirm convergence, updated in between)
 preconditioned by one line-xy V(1,1) cycle (six levels, the 64^2 coarsest solved
 with its explicit inverse), FP32 cycle (value) against FP64 cycle (fp64_ms), to
---tol (default 1e-3, the tightest round tolerance both reach); `plain_vcycle` records the reference loop on the same problem and
-`to_1e-10` the 1e-10 solve on the same grid with a constant coefficient, where
-1e-10 is attainable and the reference loop converges.
+--tol (default 1e-3, the tightest round tolerance both reach); `plain_vcycle`
+records the reference loop on the same problem, `to_1e-10` the 1e-10 solve on
+the same grid with a constant coefficient, where 1e-10 is attainable and the
+reference loop converges, and `poisson511` the reference's own CPU case (511^2
+five-point Poisson, V(2,1) point relaxation) to 1e-10.
+
+The CPU figures are measured, not modelled: the oracle (the C restatement of
+the reference's kernels, oracle/cdr2_oracle.c) runs the same flexible-CG solve
+over its own FP64 cycle to the same tolerance on all host threads, and a
+single-thread sample of its iterations gives the serial figure.
 
 One process per GPU; N > 1 runs independent replicas (a single problem does
 not shard).  Timing: CUDA events on the solver's stream, max over ranks.
@@ -49,6 +57,18 @@ LINE_Y_TRAFFIC = 107.0e6
 # headline FCG: the residual is formed (b - A x) every FCG_REPLACE-th iteration and to confirm convergence,
 # updated as r - alpha A p in between
 FCG_REPLACE = 10
+METRIC = "ms to 1e-10 rel resid: FP32-MG+FP64-IR vs FP64 plain, 1 B200; V-cycle HBM GB/s"
+
+
+def workload_config(args):
+    """The workload both arms time (the same dict in both JSON lines)."""
+    return {"workload": WORKLOAD, "n": args.n, "tol": args.tol, "levels": 6,
+            "solver": "flexible CG (FP64 recurrences; residual formed as b - A x every %d iterations and to confirm "
+                      "convergence, updated in between) preconditioned by one line-xy V(1,1) cycle over 6 levels "
+                      "(coarsest 64^2); GPU: FP32 cycle (value) and FP64 cycle (fp64_ms), coarsest solved with its "
+                      "explicit inverse; CPU oracle: FP64 cycle, coarsest by banded Cholesky" % FCG_REPLACE,
+            "parallelism": "replicas" if int(os.environ.get("WORLD_SIZE", "1")) > 1 else "single",
+            "l2": "inputs larger than L2 (fine level ~1.5 GB/cycle vs 126 MB L2)"}
 
 
 def parse():
@@ -159,57 +179,84 @@ class ClockSampler:
 
 
 # ----------------------------------------------------------------------------- CPU arm
-def cpu_arm(args, so, b, n_cycles_equiv, label, levels=-1):
-    """Time the CPU oracle (C restatement of the reference, 1 thread) on a bounded
-    sample: setup + 2 FP64 line-xy V(1,1) cycles (the preconditioner of the
-    headline solve); extrapolate to n_cycles_equiv iterations.  The FCG vector
-    updates (a few percent of an iteration) are not included."""
-    from oracle import oracle as O
-    O.build()
-    t0 = time.perf_counter()
-    s = O.Solver(so, relax="line-xy", nrelax_pre=1, nrelax_post=1, maxiter=2, tol=0.0, num_levels=levels)
-    t1 = time.perf_counter()
-    x, h = s.solve(b)
-    t2 = time.perf_counter()
-    per_cycle_ms = (t2 - t1) * 1e3 / 2.0
-    setup_ms = (t1 - t0) * 1e3
-    cores = O.num_threads()
-    return {"value": setup_ms + per_cycle_ms * n_cycles_equiv, "unit": "ms", "cores": cores, "kind": "port",
-            "sample": "%s: setup %.0f ms + 2 FP64 line-xy V(1,1) cycles (%.0f ms/cycle incl. outer residual), "
-                      "extrapolated to setup + %d iterations; oracle/cdr2_oracle.c -O2, cycle kernels on %d host "
-                      "threads (rows / lines of a colour split; setup sequential)" % (
-                          label, setup_ms, per_cycle_ms, n_cycles_equiv, cores),
-            "setup_ms": setup_ms, "ms_per_cycle": per_cycle_ms}
-
-
-# iterations of the FP64-cycle FCG solve of the default workload to 1e-3 (GPU: six
-# levels, the coarsest inverted; the FP64 cycle matches the oracle's to rounding):
-# the reference arm's extrapolation
-FCG_ITERS_FP64 = 74
 FCG_LEVELS = 6
 
 
+def oracle_fcg_solver(so, tol, maxiter, levels=FCG_LEVELS):
+    """The oracle set up for the headline solve: FP64 line-xy V(1,1) cycle over
+    `levels` levels (the coarsest by its banded Cholesky factor)."""
+    from oracle import oracle as O
+    O.build()
+    t0 = time.perf_counter()
+    s = O.Solver(so, relax="line-xy", nrelax_pre=1, nrelax_post=1, maxiter=maxiter, tol=tol, num_levels=levels)
+    return s, (time.perf_counter() - t0) * 1e3
+
+
+def oracle_fcg_solve(s, b):
+    """One full flexible-CG solve by the oracle (timed): (ms, iterations, final relative residual)."""
+    t0 = time.perf_counter()
+    x, h = s.solve_fcg(b, replace=FCG_REPLACE)
+    return (time.perf_counter() - t0) * 1e3, len(h), float(h[-1]) if len(h) else None
+
+
+def cpu_arm(args, so, b, label):
+    """The CPU oracle on the headline workload, measured: one full flexible-CG
+    solve over its FP64 line-xy V(1,1) cycle to --tol on all host threads (the
+    stand-in for the reference's parallel build), and the serial stand-in: one
+    host thread running the first SERIAL_ITERS iterations of the same solve,
+    scaled to the full solve's iteration count (a bounded sample: the serial
+    solve takes about a minute)."""
+    from oracle import oracle as O
+    s, setup_ms = oracle_fcg_solver(so, args.tol, args.maxiter)
+    ms, its, final = oracle_fcg_solve(s, b)
+    cores = O.num_threads()
+    SERIAL_ITERS = 3
+    O.set_threads(1)
+    try:
+        s1, setup1_ms = oracle_fcg_solver(so, 0.0, SERIAL_ITERS)
+        ms1, its1, _ = oracle_fcg_solve(s1, b)
+    finally:
+        O.set_threads(0)
+    serial = ms1 / its1 * its
+    return {"value": ms, "unit": "ms", "cores": cores, "kind": "port",
+            "sample": "%s: full solve, %d iterations (flexible CG over the oracle's FP64 line-xy V(1,1) cycle, %d "
+                      "levels, residual formed every %d iterations, final relative residual %.3g), "
+                      "oracle/cdr2_oracle.c -O2 with its cycle and vector kernels on %d host threads; setup %.0f ms "
+                      "(sequential) not included" % (label, its, FCG_LEVELS, FCG_REPLACE, final if final else 0.0,
+                                                      cores, setup_ms),
+            "iterations": its, "setup_ms": setup_ms, "nproc": os.cpu_count(),
+            "serial": {"value": serial, "unit": "ms", "cores": 1,
+                       "sample": "one host thread: %d iterations measured (%.0f ms each), scaled to the %d of the "
+                                 "full solve" % (its1, ms1 / its1, its)}}
+
+
 def reference_main(args):
+    """The reference arm: the oracle's full flexible-CG solve of the headline
+    workload on all host threads, each step one solve (setup once, outside)."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
+    from oracle import oracle as O
     from cedar_b200 import problems as P
     so, b = P.hetero_diffusion(args.n)
-    vals = []
-    cb = None
+    s, setup_ms = oracle_fcg_solver(so, args.tol, args.maxiter)
+    for _ in range(args.warmup):
+        oracle_fcg_solve(s, b)
+    vals, its, final = [], 0, None
     for _ in range(max(args.steps, 1)):
-        cb = cpu_arm(args, so, b, FCG_ITERS_FP64, "reference-arm", FCG_LEVELS)
-        vals.append(cb["value"])
+        ms, its, final = oracle_fcg_solve(s, b)
+        vals.append(ms)
     v = statistics.median(vals)
-    out = {"metric": "ms to 1e-10 rel resid: FP32-MG+FP64-IR vs FP64 plain, 1 B200; V-cycle HBM GB/s",
-           "value": v, "unit": "ms", "impl": "reference", "n_gpus": args.gpus, "steps": args.steps,
-           "warmup": args.warmup, "higher_is_better": False, "dtype": "f64", "data": "synthetic",
-           "config": {"workload": WORKLOAD, "n": args.n, "tol": args.tol,
-                      "solver": "flexible CG preconditioned by one FP64 line-xy V(1,1) cycle over %d levels "
-                                "(oracle), %d iterations" % (FCG_LEVELS, FCG_ITERS_FP64)},
-           "cpu_baseline": {"value": v, "unit": "ms", "cores": cb["cores"], "kind": cb["kind"],
-                            "sample": cb["sample"]},
-           "e2e": {"value": v, "unit": "ms", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    cores = O.num_threads()
+    sample = ("full solve, %d iterations per step (flexible CG over the oracle's FP64 line-xy V(1,1) cycle, %d "
+              "levels, residual formed every %d iterations, final relative residual %.3g), oracle/cdr2_oracle.c -O2 "
+              "on %d host threads; setup %.0f ms once, outside the steps" % (its, FCG_LEVELS, FCG_REPLACE,
+                                                                             final or 0.0, cores, setup_ms))
+    out = {"metric": METRIC, "value": v, "unit": "ms", "impl": "reference", "n_gpus": args.gpus,
+           "steps": args.steps, "warmup": args.warmup, "ms_per_step": v, "higher_is_better": False, "scaling": "weak",
+           "dtype": "f64", "data": "synthetic", "config": workload_config(args),
+           "cpu_baseline": {"value": v, "unit": "ms", "cores": cores, "kind": "port", "sample": sample},
+           "iterations": its, "e2e": {"value": v, "unit": "ms", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
            "vs_baseline": None}
     print(json.dumps(out), flush=True)
 
@@ -306,7 +353,13 @@ def main():
     hist64 = s64.history.copy()
     it32, it64 = len(hist32), len(hist64)
     # FP64 rounding floor of the relative residual at the FP64 solution: eps |A||x| / |b|
-    floor = rounding_floor(so, host_x(xd, n), b)
+    x64h = host_x(xd, n)
+    floor = rounding_floor(so, x64h, b)
+    # the FP32-cycle solution against the FP64-cycle one (both FP64 flexible-CG iterates to --tol)
+    with torch.cuda.stream(stream):
+        solve(s32)
+    x32h = host_x(xd, n)
+    fp32_err = float(np.linalg.norm(x32h - x64h) / np.linalg.norm(x64h))
 
     # the reference's outer loop (repeated V(2,1) cycles) on the same problem, both precisions:
     # its residual after --cycles cycles, and the cycle time behind the V-cycle GB/s figure
@@ -381,28 +434,20 @@ def main():
     # V-cycle HBM GB/s: algorithmic bytes of one FP32 V(2,1) cycle / measured cycle time
     vcyc_bytes = vcycle_bytes(vc32["solver"], word=4)
     conv = bool(it32 and hist32[-1] < args.tol and it64 and hist64[-1] < args.tol)
-    out = {"metric": "ms to 1e-10 rel resid: FP32-MG+FP64-IR vs FP64 plain, 1 B200; V-cycle HBM GB/s",
-           "value": ms32, "unit": "ms", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+    out = {"metric": METRIC, "value": ms32, "unit": "ms", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
            "ms_per_step": ms32, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
-           "dtype": "f32 cycle + f64 outer iteration", "data": "synthetic",
-           "config": {"workload": WORKLOAD, "n": n, "levels": s32.nlevels, "line_autotune": not args.no_autotune,
-                      "solver": "flexible CG (FP64 recurrences; residual formed as b - A x every %d iterations "
-                                "and to confirm convergence, updated in between) preconditioned by one line-xy "
-                                "V(1,1) cycle over %d levels (coarsest %d^2, solved with its explicit inverse); FP32 "
-                                "cycle (value) vs FP64 cycle (fp64_ms)" % (FCG_REPLACE, nlev, m),
-                      "tol": args.tol,
-                      "tol_note": "1e-10 is below this problem's FP64 rounding floor: eps*|A||x|/|b| = %.1e at "
-                                  "the FP64 solution, and no solver's relative residual goes below ~5e-5 here "
-                                  "(a sparse direct solve stops at 3e-8 already at 255^2); %.0e is the tightest "
-                                  "round tolerance both precisions reach. The reference's own loop (repeated "
-                                  "V(2,1) cycles) stalls: see plain_vcycle; 1e-10 where it is attainable: "
-                                  "to_1e-10" % (floor, args.tol),
-                      "parallelism": "replicas" if world > 1 else "single",
-                      "l2": "inputs larger than L2 (fine level ~1.5 GB/cycle vs 126 MB L2)"},
+           "dtype": "f32 cycle + f64 outer iteration", "data": "synthetic", "config": workload_config(args),
+           "tol_note": "1e-10 is below this problem's FP64 rounding floor: eps*|A||x|/|b| = %.1e at the FP64 "
+                       "solution, and no solver's relative residual goes below ~5e-5 here (a sparse direct solve "
+                       "stops at 3e-8 already at 255^2); %.0e is the tightest round tolerance both precisions reach. "
+                       "The reference's own loop (repeated V(2,1) cycles) stalls: see plain_vcycle; 1e-10 where it "
+                       "is attainable: to_1e-10 and poisson511" % (floor, args.tol),
+           "line_autotune": not args.no_autotune,
            "converged": conv, "fp64_ms": ms64, "fp32_speedup_vs_fp64": ms64 / ms32,
            "iterations": {"fp32": it32, "fp64": it64},
            "final_rel_resid": {"fp32": float(hist32[-1]) if it32 else None,
                                "fp64": float(hist64[-1]) if it64 else None},
+           "fp32_rel_error_vs_fp64": fp32_err,
            "fp64_rounding_floor": floor,
            "setup_ms": {"fp32": setup32, "fp64": setup64},
            "plain_vcycle": {k: {kk: vv for kk, vv in v.items() if kk != "solver"} for k, v in plain.items()},
@@ -428,8 +473,8 @@ def main():
         out["inverse_diffusion"] = inverse_batch()
         out["hetero3d"] = hetero3_leg(stream)
         out["batch512"] = batch_leg()
-        out["cpu_baseline"] = cpu_arm(args, so, b, it64, "config above", nlev)
-        del out["cpu_baseline"]["setup_ms"], out["cpu_baseline"]["ms_per_cycle"]
+        out["poisson511"] = poisson511(stream)
+        out["cpu_baseline"] = cpu_arm(args, so, b, "config above")
     elif world > 1 and not args.no_extras:
         bl = batch_leg(dist=dist)  # every rank: its share of the work list
         if rank == 0:
@@ -685,6 +730,45 @@ def batch_leg(count=512, dist=None):
     if world == 1:
         out["per_size"] = per_class
     return out
+
+
+def poisson511(stream, n=511):
+    """The reference's own CPU case: 511^2 five-point Poisson (unit square,
+    Dirichlet zero), b = (sin(pi x) sin(pi y) + U[-1e-3, 1e-3], seed 0) h^2,
+    V(2,1) red-black point relaxation over the reference's 8 levels, to 1e-10:
+    plain FP64 cycles (the drop-in) and FP32 cycles in FP64 refinement."""
+    import torch
+    from cedar_b200 import problems as P
+    from cedar_b200.config import Config
+    from cedar_b200.solver import Solver2D
+    so, b = P.poisson_noise(n)
+    pitch = ((n + 2 + 31) // 32) * 32
+    bd = torch.zeros((n + 2, pitch), dtype=torch.float64, device="cuda")
+    bd[:, :n + 2] = torch.from_numpy(b).cuda()
+    xd = torch.zeros_like(bd)
+    res = {"workload": "511^2 five-point Poisson, rhs (sin(pi x) sin(pi y) + U[-1e-3,1e-3] seed 0) h^2, V(2,1) "
+                       "point relaxation, 1e-10"}
+    for prec in ("fp64", "fp32-ir"):
+        s = Solver2D(so, Config({"solver": {"relaxation": "point", "max-iter": 40, "tol": 1e-10},
+                                 "gpu": {"precision": prec}}), stream=stream.cuda_stream)
+        for _ in range(3):
+            xd.zero_()
+            s.solve_device(bd.data_ptr(), xd.data_ptr(), pitch)
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+        reps = 5
+        torch.cuda.synchronize()
+        with torch.cuda.stream(stream):
+            ev[0].record(stream)
+            for _ in range(reps):
+                xd.zero_()
+                s.solve_device(bd.data_ptr(), xd.data_ptr(), pitch)
+            ev[1].record(stream)
+        torch.cuda.synchronize()
+        res[prec] = {"ms": ev[0].elapsed_time(ev[1]) / reps, "iterations": int(s.iters),
+                     "final_rel_resid": float(s.history[-1]), "levels": s.nlevels}
+        s.close()
+    res["speedup"] = res["fp64"]["ms"] / res["fp32-ir"]["ms"]
+    return res
 
 
 def to_1e10(args, stream):

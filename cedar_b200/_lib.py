@@ -68,6 +68,8 @@ def load(path=LIB_PATH):
         "cdr_gpu_lines_shape": (I, [I, I, I, I, I, I, ctypes.POINTER(I), ctypes.POINTER(I)]),
         "cdr_gpu_lines_set_shape": (I, [I, I, I, I, I, I, I, I]),
         "cdr_gpu_lines_stream_status": (I, [S]),
+        "cdr_gpu_set_wait_limit_ns": (I, [ctypes.c_longlong]),
+        "cdr_gpu_inject_timeouts": (I, [ctypes.c_uint, ctypes.c_uint]),
         "cdr_gpu_norm_scratch_bytes": (Z, []),
         "cdr_gpu_settings_default": (I, [ctypes.POINTER(Settings)]),
         "cdr_gpu_solver_create_2d": (I, [ctypes.POINTER(Settings), P, I, I, I, S, ctypes.POINTER(P)]),

@@ -72,11 +72,26 @@ size_t cdr_gpu_norm_scratch_bytes(void) { return kNormScratchBytes; }
 
 int cdr_gpu_lines_stream_status(cudaStream_t s)
 {
-	if (const unsigned to = lines_stream_timeouts(s)) {
+	unsigned to = 0;
+	CDR_TRY(lines_stream_timeouts(s, &to));
+	if (to) {
 		set_error(CDR_ERR_NUMERIC, "%u streamed line-sweep CTAs gave up waiting for their rows", to);
 		return CDR_ERR_NUMERIC;
 	}
 	return CDR_OK;
+}
+
+int cdr_gpu_set_wait_limit_ns(long long ns)
+{
+	const unsigned long long v = ns < 0 ? kStreamWaitDefaultNs : (unsigned long long)ns;
+	CDR_TRY(lines_stream_set_wait(v));
+	return cg_inv_set_wait(v);
+}
+
+int cdr_gpu_inject_timeouts(unsigned lines, unsigned inverse)
+{
+	CDR_TRY(lines_stream_add_timeouts(lines));
+	return cg_inv_add_timeouts(inverse);
 }
 
 int cdr_gpu_lines_set_shape(int dir, int fp32, int nstencil, int n, int nlines, int batch, int K, int cap)

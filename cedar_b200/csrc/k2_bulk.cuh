@@ -1,5 +1,5 @@
 // k2_bulk.cuh -- bulk asynchronous global->shared copies completed on an
-// mbarrier (cp.async.bulk, no multicast), with waits bounded by a poll count.
+// mbarrier (cp.async.bulk, no multicast), with waits bounded in time.
 #pragma once
 #include <cstdint>
 
@@ -31,11 +31,30 @@ static __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, unsigned par
 	return ok != 0;
 }
 
-// at most 2^18 polls (each try_wait may suspend the thread for a while)
-static __device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, unsigned parity)
+static __device__ __forceinline__ unsigned long long globaltimer_ns()
 {
-	for (int it = 0; it < (1 << 18); ++it)
+	unsigned long long t;
+	asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+	return t;
+}
+
+// Default limits of the bounded waits: the first wait of a streamed kernel on
+// a stage, and the drain of a CTA that gave up (its copies still in flight).
+constexpr unsigned long long kWaitLimitNs = 200000000ull;   // 0.2 s
+constexpr unsigned long long kDrainLimitNs = 1000000000ull; // 1 s
+
+// Wait for the phase of `parity` to complete, for at most limit_ns
+// nanoseconds of the global timer (and at most 2^20 polls); limit_ns = 0 gives
+// up at once (the test setting of the give-up path).  Returns false if it gave up.
+static __device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, unsigned parity,
+                                                         unsigned long long limit_ns = kWaitLimitNs)
+{
+	if (limit_ns == 0) return false;
+	const unsigned long long t0 = globaltimer_ns();
+	for (int it = 0; it < (1 << 20); ++it) {
 		if (mbar_try_wait(bar, parity)) return true;
+		if (globaltimer_ns() - t0 > limit_ns) return false;
+	}
 	return false;
 }
 

@@ -139,9 +139,12 @@ __global__ void __launch_bounds__(256) k_cg_inv_apply(const T *__restrict__ ainv
 // so that DRAM keeps streaming while the CTA sums the current row: one row per
 // CTA step, 256 threads, 16-byte row loads from shared memory, FP64 partial
 // sums reduced in a fixed order.  Rows must be 16-byte multiples.  Every wait
-// is bounded; a CTA that gives up is counted in g_inv_timeouts and returns.
+// is bounded (g_inv_wait_ns of the global timer); a CTA that gives up is
+// counted in g_inv_timeouts, waits (bounded) for every copy it has in flight
+// (the stage it gave up on and the ones issued after it) and returns.
 constexpr int IA_STAGES = 2, IA_BLOCK = 256;
 __device__ unsigned g_inv_timeouts;
+__device__ unsigned long long g_inv_wait_ns = kWaitLimitNs;
 
 template <typename T>
 __global__ void __launch_bounds__(IA_BLOCK) k_cg_inv_apply_bulk(const T *__restrict__ ainv, T *__restrict__ q,
@@ -175,16 +178,20 @@ __global__ void __launch_bounds__(IA_BLOCK) k_cg_inv_apply_bulk(const T *__restr
 		bs[e] = qf[d.at(e - jj * d.nx + 1, jj + 1)];
 	}
 	__syncthreads();
+	const unsigned long long wait_ns = g_inv_wait_ns;
 	int k = 0;
 	for (int r = blockIdx.x; r < n; r += G, ++k) {
 		const int st = k % IA_STAGES;
-		const bool ok = mbar_wait_bounded(&bar[st], (unsigned)(k / IA_STAGES) & 1u);
+		const bool ok = mbar_wait_bounded(&bar[st], (unsigned)(k / IA_STAGES) & 1u, wait_ns);
 		if (!__syncthreads_and(ok)) {
-			// give up: wait (bounded) for the other stages' copies in flight, then leave
+			// give up: wait (bounded) for the copies in flight -- this stage's and
+			// those of the rows issued after it -- then leave
 			if (tid == 0) {
 				atomicAdd(&g_inv_timeouts, 1u);
-				for (int s2 = 1; s2 < IA_STAGES; ++s2)
-					if (r + s2 * G < n) mbar_wait_bounded(&bar[(k + s2) % IA_STAGES], (unsigned)((k + s2) / IA_STAGES) & 1u);
+				for (int s2 = 0; s2 < IA_STAGES; ++s2)
+					if (r + s2 * G < n)
+						mbar_wait_bounded(&bar[(k + s2) % IA_STAGES], (unsigned)((k + s2) / IA_STAGES) & 1u,
+						                  kDrainLimitNs);
 			}
 			return;
 		}
@@ -219,18 +226,34 @@ size_t inv_bulk_smem(int n)
 
 }  // namespace
 
-unsigned cg_inv_timeouts(cudaStream_t st)
+int cg_inv_timeouts(cudaStream_t st, unsigned *count)
 {
 	unsigned v = 0;
-	if (cudaMemcpyFromSymbolAsync(&v, g_inv_timeouts, sizeof v, 0, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
-	    cudaStreamSynchronize(st) != cudaSuccess)
-		return 0;
+	*count = 0;
+	CDR_CUDA_TRY(cudaMemcpyFromSymbolAsync(&v, g_inv_timeouts, sizeof v, 0, cudaMemcpyDeviceToHost, st));
+	CDR_CUDA_TRY(cudaStreamSynchronize(st));
 	if (v) {
 		const unsigned z = 0;
-		cudaMemcpyToSymbolAsync(g_inv_timeouts, &z, sizeof z, 0, cudaMemcpyHostToDevice, st);
-		cudaStreamSynchronize(st);
+		CDR_CUDA_TRY(cudaMemcpyToSymbolAsync(g_inv_timeouts, &z, sizeof z, 0, cudaMemcpyHostToDevice, st));
+		CDR_CUDA_TRY(cudaStreamSynchronize(st));
 	}
-	return v;
+	*count = v;
+	return CDR_OK;
+}
+
+int cg_inv_add_timeouts(unsigned n)
+{
+	unsigned v = 0;
+	CDR_CUDA_TRY(cudaMemcpyFromSymbol(&v, g_inv_timeouts, sizeof v));
+	v += n;
+	CDR_CUDA_TRY(cudaMemcpyToSymbol(g_inv_timeouts, &v, sizeof v));
+	return CDR_OK;
+}
+
+int cg_inv_set_wait(unsigned long long ns)
+{
+	CDR_CUDA_TRY(cudaMemcpyToSymbol(g_inv_wait_ns, &ns, sizeof ns));
+	return CDR_OK;
 }
 
 int cg_inverse_2d(const double *abd, Dims2 d, double *ainv, cudaStream_t st)

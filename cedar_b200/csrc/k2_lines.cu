@@ -546,24 +546,43 @@ __global__ void __launch_bounds__(XL ? FAST_BLOCK_X : FAST_BLOCK_Y, XL ? 2 : 1)
 // line then run while DRAM streams the next one (one stage per CTA, so two
 // CTAs share an SM).  The arithmetic is k_lines_fast's x-line path with the
 // same K: results are bit-identical to it.  Every wait on the stage is
-// bounded; one that gives up is counted in g_xstream_timeouts and the CTA
-// returns.
+// bounded (g_xstream_wait_ns of the global timer); a CTA that gives up counts
+// itself in g_xstream_timeouts, waits (bounded) for the copy it has in flight,
+// so that nothing lands in shared memory after it has left, and returns.
 namespace {
 __device__ unsigned g_xstream_timeouts;
+__device__ unsigned long long g_xstream_wait_ns = kWaitLimitNs;
 }  // namespace
+static_assert(kStreamWaitDefaultNs == kWaitLimitNs, "one default wait limit");
 
-unsigned lines_stream_timeouts(cudaStream_t st)
+int lines_stream_timeouts(cudaStream_t st, unsigned *count)
 {
 	unsigned v = 0;
-	if (cudaMemcpyFromSymbolAsync(&v, g_xstream_timeouts, sizeof v, 0, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
-	    cudaStreamSynchronize(st) != cudaSuccess)
-		return 0;
+	*count = 0;
+	CDR_CUDA_TRY(cudaMemcpyFromSymbolAsync(&v, g_xstream_timeouts, sizeof v, 0, cudaMemcpyDeviceToHost, st));
+	CDR_CUDA_TRY(cudaStreamSynchronize(st));
 	if (v) {
 		const unsigned z = 0;
-		cudaMemcpyToSymbolAsync(g_xstream_timeouts, &z, sizeof z, 0, cudaMemcpyHostToDevice, st);
-		cudaStreamSynchronize(st);
+		CDR_CUDA_TRY(cudaMemcpyToSymbolAsync(g_xstream_timeouts, &z, sizeof z, 0, cudaMemcpyHostToDevice, st));
+		CDR_CUDA_TRY(cudaStreamSynchronize(st));
 	}
-	return v;
+	*count = v;
+	return CDR_OK;
+}
+
+int lines_stream_add_timeouts(unsigned n)
+{
+	unsigned v = 0;
+	CDR_CUDA_TRY(cudaMemcpyFromSymbol(&v, g_xstream_timeouts, sizeof v));
+	v += n;
+	CDR_CUDA_TRY(cudaMemcpyToSymbol(g_xstream_timeouts, &v, sizeof v));
+	return CDR_OK;
+}
+
+int lines_stream_set_wait(unsigned long long ns)
+{
+	CDR_CUDA_TRY(cudaMemcpyToSymbol(g_xstream_wait_ns, &ns, sizeof ns));
+	return CDR_OK;
 }
 
 constexpr int XS_BLOCK = 256;
@@ -646,11 +665,16 @@ __global__ void __launch_bounds__(XS_BLOCK, 2) k_lines_xstream(const T *__restri
 			v[W + w] = rot ? ea[w] : eb[w];
 		}
 	};
+	const unsigned long long wait_ns = g_xstream_wait_ns;
 	int k = 0;
 	for (int li = blockIdx.x; li < nlines; li += G, ++k) {
-		const bool ok = mbar_wait_bounded(bar, (unsigned)k & 1u);
+		const bool ok = mbar_wait_bounded(bar, (unsigned)k & 1u, wait_ns);
 		if (!__syncthreads_and(ok)) {
-			if (tid == 0) atomicAdd(&g_xstream_timeouts, 1u);
+			// give up: count, then wait (bounded) for this line's copy, the one in flight
+			if (tid == 0) {
+				atomicAdd(&g_xstream_timeouts, 1u);
+				mbar_wait_bounded(bar, (unsigned)k & 1u, kDrainLimitNs);
+			}
 			return;
 		}
 		const int lc = first + 2 * li;

@@ -25,10 +25,19 @@ struct LineShape {
 	int stream = 0;  // x-lines: rows streamed into shared memory (k_lines_xstream)
 };
 // bounded waits of the streamed x-line kernel that gave up since the last call
-// (read and reset; 0 in a healthy run)
-unsigned lines_stream_timeouts(cudaStream_t st);
+// (read and reset into *count; 0 in a healthy run); CDR_ERR_CUDA if they
+// cannot be read
+int lines_stream_timeouts(cudaStream_t st, unsigned *count);
 // the same for the streamed explicit-inverse product (k2_cginv.cu)
-unsigned cg_inv_timeouts(cudaStream_t st);
+int cg_inv_timeouts(cudaStream_t st, unsigned *count);
+// Test hooks (current device): add to a give-up count from the host, and set
+// the limit of the streamed kernels' first wait on a stage (ns; 0: one
+// non-blocking test)
+int lines_stream_add_timeouts(unsigned n);
+int cg_inv_add_timeouts(unsigned n);
+int lines_stream_set_wait(unsigned long long ns);
+constexpr unsigned long long kStreamWaitDefaultNs = 200000000ull;  // kWaitLimitNs of k2_bulk.cuh
+int cg_inv_set_wait(unsigned long long ns);
 template <typename T>
 int lines_autotune(const T *so, int nstencil, T *x, const T *b, const T *sor, Dims2 d, int tpitch, int dir,
                    cudaStream_t st);

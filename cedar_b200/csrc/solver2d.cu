@@ -794,15 +794,15 @@ static int solve_loaded(cdr_gpu_solver *h, int *iters, double *hist, int maxhist
 	CDR_CUDA_TRY(cudaEventSynchronize(h->ev1));
 	CDR_CUDA_TRY(cudaEventElapsedTime(&h->solve_ms, h->ev0, h->ev1));
 	if (iters) *iters = it;
-	if (const unsigned to = lines_stream_timeouts(st)) {
-		set_error(CDR_ERR_NUMERIC, "%u streamed line-sweep CTAs gave up waiting for their rows", to);
+	// both give-up counts are read (and reset) before either is reported
+	unsigned to_lines = 0, to_inv = 0;
+	CDR_TRY(lines_stream_timeouts(st, &to_lines));
+	if (h->s.coarse_solve == CDR_COARSE_INVERSE) CDR_TRY(cg_inv_timeouts(st, &to_inv));
+	if (to_lines || to_inv) {
+		set_error(CDR_ERR_NUMERIC, "%u streamed line-sweep CTAs and %u inverse-product CTAs gave up waiting for their rows",
+		          to_lines, to_inv);
 		return CDR_ERR_NUMERIC;
 	}
-	if (h->s.coarse_solve == CDR_COARSE_INVERSE)
-		if (const unsigned to = cg_inv_timeouts(st)) {
-			set_error(CDR_ERR_NUMERIC, "%u inverse-product CTAs gave up waiting for their rows", to);
-			return CDR_ERR_NUMERIC;
-		}
 	return CDR_OK;
 }
 

@@ -198,6 +198,18 @@ int cdr_gpu_setup_lines_2d_f32(const double *so, int nstencil, float *sor, int n
  * The 2D solver checks it after every solve; kernel-level callers that use
  * CDR_LINES_STREAM or a streamed pinned shape call it themselves. */
 int cdr_gpu_lines_stream_status(cudaStream_t s);
+/* Test hooks for the bounded waits of the two streamed kernels (the x-line
+ * sweep above and the 2D solver's explicit-inverse coarsest product); no
+ * counterpart in the reference.  cdr_gpu_set_wait_limit_ns sets, for the
+ * current device, how long a CTA waits for its staged rows before it gives up
+ * (ns of the global timer; 0: give up at once, without waiting; negative: the
+ * default, 0.2 s).  A CTA that gives up counts itself, waits (at most 1 s) for
+ * the copies it still has in flight and leaves its rows unsolved; the status
+ * calls and the solver's solve then return CDR_ERR_NUMERIC.
+ * cdr_gpu_inject_timeouts adds to the two give-up counts from the host (the
+ * host side of that reporting path, without any device wait). */
+int cdr_gpu_set_wait_limit_ns(long long ns);
+int cdr_gpu_inject_timeouts(unsigned lines, unsigned inverse);
 int cdr_gpu_relax_lines_2d_f64(const double *so, int nstencil, double *x, const double *b, const double *sor,
                                int nx, int ny, int pitch, int tpitch, int dir, int updown, int flags,
                                cudaStream_t stream);

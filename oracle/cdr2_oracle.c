@@ -66,9 +66,15 @@ static void *o_chunk_run(void *p)
 	return NULL;
 }
 
+static int o_threads_set = 0;
+
+/* Thread count for the following calls (0: back to the environment's). */
+void o_set_threads(int n) { o_threads_set = n < 0 ? 0 : n > 64 ? 64 : n; }
+
 int o_num_threads(void)
 {
 	static int n = 0;
+	if (o_threads_set) return o_threads_set;
 	if (!n) {
 		const char *e = getenv("ORACLE_THREADS");
 		if (!e) e = getenv("OMP_NUM_THREADS");
@@ -1135,6 +1141,98 @@ int o2_solve(o2_solver *h, const double *b, double *x, double *hist, int maxhist
 		if (hist && it < maxhist) hist[it] = rel;
 		if (rel < h->s.tol) { ++it; break; }
 	}
+	return it;
+}
+
+/* ------------------------------------------------------------------ */
+/* Flexible CG around the cycle                                        */
+/* ------------------------------------------------------------------ */
+/* Notay's FCG(1) preconditioned by one cycle of the solver: the CPU
+ * counterpart of the GPU solver's flexible-CG outer iteration (the reference
+ * has none; its solve repeats the cycle).  Recurrences, as on the GPU:
+ *   beta = -(z . q_prev) / (p_prev . q_prev) (0 first), p = z + beta p_prev,
+ *   q = A p, alpha = (p . r) / (p . q), x += alpha p,
+ *   r = b - A x every `replace`-th iteration and to confirm convergence,
+ *   r -= alpha q in between.
+ * Vector work is split by rows over the host threads; each dot product sums
+ * per-row partials in row order (no result depends on the thread count). */
+struct o2_vec_ctx {
+	int op, II;
+	double a;
+	double *x, *y;
+	const double *u, *v;
+	double *part; /* per-row partial sums (dot products) */
+};
+
+static void o2_vec_row(void *vc, int t)
+{
+	const struct o2_vec_ctx *c = (const struct o2_vec_ctx *)vc;
+	const size_t k0 = (size_t)(t + 1) * c->II + 1, k1 = k0 + c->II - 2;
+	double s = 0.0;
+	switch (c->op) {
+	case 0: /* part = sum u*v */
+		for (size_t k = k0; k < k1; ++k) s += c->u[k] * c->v[k];
+		c->part[t] = s;
+		break;
+	case 1: /* x = u + a*x */
+		for (size_t k = k0; k < k1; ++k) c->x[k] = c->u[k] + c->a * c->x[k];
+		break;
+	case 2: /* x += a*u */
+		for (size_t k = k0; k < k1; ++k) c->x[k] += c->a * c->u[k];
+		break;
+	case 3: /* x = -u */
+		for (size_t k = k0; k < k1; ++k) c->x[k] = -c->u[k];
+		break;
+	}
+}
+
+static double o2_vec(int op, int II, int JJ, double a, double *x, const double *u, const double *v, double *part)
+{
+	struct o2_vec_ctx c = {op, II, a, x, NULL, u, v, part};
+	o_parallel(JJ - 2, (long)II * JJ, o2_vec_row, &c);
+	double s = 0.0;
+	if (op == 0)
+		for (int t = 0; t < JJ - 2; ++t) s += part[t];
+	return s;
+}
+
+int o2_solve_fcg(o2_solver *h, const double *b, double *x, int replace, double *hist, int maxhist)
+{
+	struct o2_level *L = &h->lv[0];
+	const int II = L->ii, JJ = L->jj, ifd = L->nstncl == 3 ? 1 : 0;
+	const size_t n = (size_t)II * JJ;
+	double *r = zalloc(n), *z = zalloc(n), *p = zalloc(n), *q = zalloc(n), *t = zalloc(n), *zero = zalloc(n);
+	double *part = zalloc((size_t)JJ);
+	const int m = replace > 1 ? replace : 1;
+	o2_residual(L->so, b, x, r, II, JJ, ifd);
+	const double res0 = sqrt(o2_vec(0, II, JJ, 0.0, NULL, r, r, part));
+	double pq = 1.0;
+	int it = 0, first = 1;
+	while (res0 > 0 && it < h->s.maxiter) {
+		memset(z, 0, sizeof(double) * n);
+		o2_cycle(h, z, r);
+		const double beta = first ? 0.0 : -o2_vec(0, II, JJ, 0.0, NULL, z, q, part) / pq;
+		o2_vec(1, II, JJ, beta, p, z, NULL, part);           /* p = z + beta p */
+		o2_residual(L->so, zero, p, t, II, JJ, ifd);         /* t = -A p */
+		o2_vec(3, II, JJ, 0.0, q, t, NULL, part);            /* q = A p */
+		pq = o2_vec(0, II, JJ, 0.0, NULL, p, q, part);
+		const double alpha = o2_vec(0, II, JJ, 0.0, NULL, p, r, part) / pq;
+		o2_vec(2, II, JJ, alpha, x, p, NULL, part);          /* x += alpha p */
+		const int formed = (it + 1) % m == 0;
+		if (formed) o2_residual(L->so, b, x, r, II, JJ, ifd);
+		else o2_vec(2, II, JJ, -alpha, r, q, NULL, part);    /* r -= alpha q */
+		first = 0;
+		double rel = sqrt(o2_vec(0, II, JJ, 0.0, NULL, r, r, part)) / res0;
+		++it;
+		if (rel < h->s.tol && !formed) {
+			/* an updated residual met the tolerance: form b - A x and go on from it */
+			o2_residual(L->so, b, x, r, II, JJ, ifd);
+			rel = sqrt(o2_vec(0, II, JJ, 0.0, NULL, r, r, part)) / res0;
+		}
+		if (hist && it - 1 < maxhist) hist[it - 1] = rel;
+		if (!(rel == rel) || rel < h->s.tol) break;
+	}
+	free(r); free(z); free(p); free(q); free(t); free(zero); free(part);
 	return it;
 }
 

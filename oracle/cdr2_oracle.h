@@ -55,7 +55,11 @@ void o2_vcycle(o2_solver *h, double *x, const double *b);
 void o2_cycle(o2_solver *h, double *x, const double *b);
 void o2_cycle(o2_solver *h, double *x, const double *b);
 int o2_solve(o2_solver *h, const double *b, double *x, double *hist, int maxhist);
+/* Flexible CG preconditioned by one cycle (residual formed every `replace`
+ * iterations and to confirm convergence); returns the iterations run. */
+int o2_solve_fcg(o2_solver *h, const double *b, double *x, int replace, double *hist, int maxhist);
 int o_num_threads(void);
+void o_set_threads(int n);
 int o2_nlevels(const o2_solver *h);
 int o2_info(const o2_solver *h, int which);
 void o2_level_dims(const o2_solver *h, int l, int *dims);

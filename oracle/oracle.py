@@ -70,6 +70,8 @@ def lib(variant=""):
             "o2_vcycle": (None, [P, P, P]),
             "o2_cycle": (None, [P, P, P]),
             "o2_solve": (I, [P, P, P, P, I]),
+            "o2_solve_fcg": (I, [P, P, P, I, P, I]),
+            "o_set_threads": (None, [I]),
             "o2_nlevels": (I, [P]),
             "o_num_threads": (I, []),
             "o2_info": (I, [P, I]),
@@ -234,6 +236,11 @@ def num_levels(nx, ny, min_coarse=3):
 
 
 # ------------------------------------------------------------------ solver
+def set_threads(n):
+    """Host threads of the following oracle calls (0: the environment's count)."""
+    lib().o_set_threads(int(n))
+
+
 def num_threads():
     """Host threads the oracle's cycle kernels use (ORACLE_THREADS / OMP_NUM_THREADS / online CPUs)."""
     return lib().o_num_threads()
@@ -296,6 +303,17 @@ class Solver:
             x = np.zeros_like(b)
         hist = np.zeros(max(self.settings.maxiter, 1))
         n = self.L.o2_solve(self.h, _p(b), _p(x), _p(hist), len(hist))
+        return x, hist[:n].copy()
+
+    def solve_fcg(self, b, x=None, replace=1):
+        """Flexible CG preconditioned by one cycle, to the settings' tol and
+        maxiter; the residual is formed every `replace` iterations and to
+        confirm convergence.  Returns (x, history)."""
+        b = np.ascontiguousarray(b, dtype=np.float64)
+        if x is None:
+            x = np.zeros_like(b)
+        hist = np.zeros(max(self.settings.maxiter, 1))
+        n = self.L.o2_solve_fcg(self.h, _p(b), _p(x), int(replace), _p(hist), len(hist))
         return x, hist[:n].copy()
 
 

@@ -7,12 +7,14 @@ import numpy as np
 from cedar_b200 import gallery as G
 
 
-def fcg(oracle, so, b, relax="line-xy", npre=1, npost=1, tol=1e-10, maxiter=200):
+def fcg(oracle, so, b, relax="line-xy", npre=1, npost=1, tol=1e-10, maxiter=200, num_levels=-1):
     """Returns (x, history of |b - A x_k| / |b - A x_0|, final relative residual).
-    The residual is formed from x every iteration, as the GPU solve does."""
+    The residual is formed from x every iteration, as the GPU solve does.
+    num_levels: levels of the oracle's cycle (-1: the reference's rule)."""
     ny, nx = b.shape[0] - 2, b.shape[1] - 2
     A = G.stencil_to_csr(so)
-    pre = oracle.Solver(so, relax=relax, maxiter=1, tol=1e-300, nrelax_pre=npre, nrelax_post=npost)
+    pre = oracle.Solver(so, relax=relax, maxiter=1, tol=1e-300, nrelax_pre=npre, nrelax_post=npost,
+                        num_levels=num_levels)
 
     def M(r):
         rr = np.zeros_like(b)

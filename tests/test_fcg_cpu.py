@@ -54,3 +54,40 @@ def test_symmetric_cycle_is_a_symmetric_preconditioner(oracle):
     assert abs(u @ M(v) - v @ M(u)) <= 1e-10 * abs(u @ M(v))
     A = G.stencil_to_csr(so)
     assert u @ M(A @ u) > 0
+
+
+def test_oracle_fcg_matches_python_restatement(oracle):
+    """The oracle's C flexible CG (the CPU baseline's solver) follows the numpy
+    restatement over the same cycle: same iteration count, histories equal to
+    rounding (the two sum their dot products in different orders), and with
+    residual replacement (formed every 4th iteration) the same tolerance."""
+    n = 63
+    so, b = P.hetero_diffusion(n)
+    x_ref, h_ref, _ = fcg(oracle, so, b, tol=1e-6, num_levels=3)
+    s = oracle.Solver(so, relax="line-xy", nrelax_pre=1, nrelax_post=1, num_levels=3, maxiter=200, tol=1e-6)
+    x, h = s.solve_fcg(b)
+    assert len(h) == len(h_ref)
+    np.testing.assert_allclose(h[:10], h_ref[:10], rtol=1e-7)
+    assert np.abs(x - x_ref).max() <= 1e-6 * np.abs(x_ref).max()
+    x4, h4 = oracle.Solver(so, relax="line-xy", nrelax_pre=1, nrelax_post=1, num_levels=3, maxiter=200,
+                           tol=1e-6).solve_fcg(b, replace=4)
+    r = oracle.residual(np.ascontiguousarray(so), x4, b)
+    r0 = oracle.residual(np.ascontiguousarray(so), np.zeros_like(b), b)
+    assert h4[-1] < 1e-6 and np.linalg.norm(r) / np.linalg.norm(r0) < 1e-6
+    assert abs(len(h4) - len(h)) <= 3
+    np.testing.assert_allclose(h4[:3], h[:3], rtol=1e-7)
+
+
+def test_oracle_fcg_thread_count_independent(oracle):
+    """Row partials summed in row order: one host thread and four give the same bits."""
+    n = 767
+    so, b = P.hetero_diffusion(n, sigma=1.0, n_incl=4, contrast=100.0, aniso=0.5)
+    out = []
+    for t in (1, 4):
+        oracle.set_threads(t)
+        try:
+            s = oracle.Solver(so, relax="line-xy", nrelax_pre=1, nrelax_post=1, num_levels=4, maxiter=3, tol=0.0)
+            out.append(s.solve_fcg(b))
+        finally:
+            oracle.set_threads(0)
+    assert np.array_equal(out[0][0], out[1][0]) and np.array_equal(out[0][1], out[1][1])
