@@ -49,11 +49,11 @@ PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
 WORKLOAD = ("2D heterogeneous diffusion, 9-pt bilinear FE, 2047x2047 nodes (2048^2 cells), lognormal k "
             "(GRF ell=1/32 sigma=2, seed 1), 64 inclusions x1e4 (seed 2), ky=1e-3 k on y>0.5, rhs U[0,1] h^2 "
             "(seed 3); line-xy relaxation, Galerkin coarsening (levels and coarsest solve: config.solver)")
-# DRAM bytes (read + write) of one fine-level colour launch of the 2047^2 FP32 level, from one ncu
-# capture each (--set full, caches flushed): x-lines (the streamed kernel, k_lines_xstream) 85.1 MB
-# read + 2.9 MB written; y-lines (k_lines_fast, K = 16, 1024 threads) 101.7 MB + 5.3 MB
+# DRAM bytes (read + write) per launch on the 2047^2 FP32 level, from one ncu capture each (caches
+# flushed): x-lines, one colour (the streamed kernel, k_lines_xstream) 85.1 MB read + 2.9 MB written;
+# y-lines, both colours in one launch (k_ylines_pair): None until captured
 LINE_X_TRAFFIC = 88.1e6
-LINE_Y_TRAFFIC = 107.0e6
+LINE_Y_TRAFFIC = None
 # headline FCG: the residual is formed (b - A x) every FCG_REPLACE-th iteration and to confirm convergence,
 # updated as r - alpha A p in between
 FCG_REPLACE = 10
@@ -397,19 +397,26 @@ def main():
     p_sx, *_ = s32.level_info(0, "sor", fp32=True)
     p_sy, *_ = s32.level_info(0, "sory", fp32=True)
 
+    # the solver's own sweeps: x-lines two launches (one per colour), y-lines both colours in one launch
+    ysync = torch.zeros(int(lib.cdr_gpu_lines_sync_words(nx)), dtype=torch.int32, device="cuda")
+
     def sweep_time(dirn, p_f):
         reps = 20
+
+        def one():
+            _lib.check(lib.cdr_gpu_relax_lines_2d_sync_f32(
+                ctypes.c_void_p(p_so), ns, ctypes.c_void_p(p_x), ctypes.c_void_p(p_b), ctypes.c_void_p(p_f), nx, ny,
+                pp, tp, dirn, 0, 0, ctypes.c_void_p(ysync.data_ptr()), ctypes.c_void_p(sh)))
         with torch.cuda.stream(stream):
             ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
             for _ in range(3):
-                lib.cdr_gpu_relax_lines_2d_f32(ctypes.c_void_p(p_so), ns, ctypes.c_void_p(p_x), ctypes.c_void_p(p_b),
-                                               ctypes.c_void_p(p_f), nx, ny, pp, tp, dirn, 0, 0, ctypes.c_void_p(sh))
+                one()
             ev[0].record(stream)
             for _ in range(reps):
-                lib.cdr_gpu_relax_lines_2d_f32(ctypes.c_void_p(p_so), ns, ctypes.c_void_p(p_x), ctypes.c_void_p(p_b),
-                                               ctypes.c_void_p(p_f), nx, ny, pp, tp, dirn, 0, 0, ctypes.c_void_p(sh))
+                one()
             ev[1].record(stream)
         torch.cuda.synchronize()
+        _lib.check(lib.cdr_gpu_lines_stream_status(ctypes.c_void_p(sh)))
         return ev[0].elapsed_time(ev[1]) / reps
 
     sweep_ms = sweep_time(0, p_sx)
@@ -456,12 +463,12 @@ def main():
                       "hbm_gbs": vcyc_bytes / (vc32["ms_per_cycle"] * 1e-3) / 1e9,
                       "fp64_ms": vc64["ms_per_cycle"],
                       "fp64_hbm_gbs": vcycle_bytes(vc64["solver"], word=8) / (vc64["ms_per_cycle"] * 1e-3) / 1e9},
-           "roofline": {"kernel": "k_lines_fast<float,%d,y,K=%d> (fine-level y-line sweep, 2 launches)"
-                                  % (ns, shapes.get("y", {}).get("K", 0)), "line_shapes": shapes,
+           "roofline": {"kernel": "k_ylines_pair<float,%d,K=%d> (fine-level y-line sweep, both colours in one "
+                                  "launch)" % (ns, shapes.get("y", {}).get("K", 0)), "line_shapes": shapes,
                         "bound": "hbm", "achieved": y_achieved, "peak": peak, "unit": "GB/s",
                         "frac": y_achieved / peak, "peak_kind": peak_kind,
                         "traffic": LINE_Y_TRAFFIC if n == 2047 else None,
-                        "algorithmic_bytes_per_launch": bytes_per_sweep / 2, "launch_ms": ysweep_ms / 2.0,
+                        "algorithmic_bytes_per_launch": bytes_per_sweep, "launch_ms": ysweep_ms,
                         "x_sweep": {"kernel": xkern, "achieved": achieved, "frac": achieved / peak,
                                     "traffic": LINE_X_TRAFFIC if n == 2047 else None, "launch_ms": launch_ms}},
            "e2e": {"value": e2e, "unit": "ms", "h2d_bytes_per_step": 2 * 8 * (n + 2) ** 2,

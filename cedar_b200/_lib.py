@@ -71,6 +71,7 @@ def load(path=LIB_PATH):
         "cdr_gpu_set_wait_limit_ns": (I, [ctypes.c_longlong]),
         "cdr_gpu_inject_timeouts": (I, [ctypes.c_uint, ctypes.c_uint]),
         "cdr_gpu_norm_scratch_bytes": (Z, []),
+        "cdr_gpu_lines_sync_words": (Z, [I]),
         "cdr_gpu_settings_default": (I, [ctypes.POINTER(Settings)]),
         "cdr_gpu_solver_create_2d": (I, [ctypes.POINTER(Settings), P, I, I, I, S, ctypes.POINTER(P)]),
         "cdr_gpu_solver_destroy": (I, [P]),
@@ -94,6 +95,7 @@ def load(path=LIB_PATH):
             "cdr_gpu_relax_point_2d_" + suf: (I, [P, I, P, P, P, I, I, I, I, S]),
             "cdr_gpu_setup_lines_2d_" + suf: (I, [P, I, P, I, I, I, I, I, P, S]),
             "cdr_gpu_relax_lines_2d_" + suf: (I, [P, I, P, P, P, I, I, I, I, I, I, I, S]),
+            "cdr_gpu_relax_lines_2d_sync_" + suf: (I, [P, I, P, P, P, I, I, I, I, I, I, I, P, S]),
             "cdr_gpu_restrict_2d_" + suf: (I, [P, P, P, I, I, I, I, I, I, S]),
             "cdr_gpu_interp_add_2d_" + suf: (I, [P, P, P, P, P, I, I, I, I, I, I, S]),
             "cdr_gpu_solve_cg_2d_" + suf: (I, [P, P, P, I, I, I, S]),

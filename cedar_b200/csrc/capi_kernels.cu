@@ -181,6 +181,23 @@ LSETUP_IMPL(float, f32)
 LRELAX_IMPL(double, f64)
 LRELAX_IMPL(float, f32)
 
+size_t cdr_gpu_lines_sync_words(int nx) { return lines_sync_words(Dims2{nx > 0 ? nx : 0, 1, nx + 2}); }
+
+#define LRELAX_SYNC_IMPL(T, SUF)                                                                                 \
+	int cdr_gpu_relax_lines_2d_sync_##SUF(const T *so, int ns, T *x, const T *b, const T *sor, int nx, int ny,    \
+	                                      int pitch, int tpitch, int dir, int updown, int flags, unsigned *sync,  \
+	                                      cudaStream_t s)                                                         \
+	{                                                                                                            \
+		CDR_TRY(check_grid(nx, ny, pitch));                                                                      \
+		CDR_TRY(check_ns(ns));                                                                                   \
+		CDR_NONNULL(so); CDR_NONNULL(x); CDR_NONNULL(b); CDR_NONNULL(sor); CDR_NONNULL(sync);                    \
+		if (dir != CDR_DIR_X && dir != CDR_DIR_Y) { set_error(CDR_ERR_ARG, "bad dir %d", dir); return CDR_ERR_ARG; } \
+		if (dir == CDR_DIR_Y && tpitch < ny + 2) { set_error(CDR_ERR_DIM, "tpitch %d < ny+2", tpitch); return CDR_ERR_DIM; } \
+		return relax_lines_2d<T>(so, ns, x, b, sor, Dims2{nx, ny, pitch}, tpitch, dir, updown, flags, s, sync);  \
+	}
+LRELAX_SYNC_IMPL(double, f64)
+LRELAX_SYNC_IMPL(float, f32)
+
 #define RESTRICT_IMPL(T, SUF)                                                                                   \
 	int cdr_gpu_restrict_2d_##SUF(const T *ci, const T *rf, T *bc, int nxf, int nyf, int pf, int nxc, int nyc,  \
 	                              int pc, cudaStream_t s)                                                       \

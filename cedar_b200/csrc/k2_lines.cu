@@ -271,74 +271,152 @@ __device__ __forceinline__ void after(T &A, T &B, T a2, T b2)
 	A = A * a2;
 }
 
-// Exclusive scan of the chunk maps of a line.  forward: element u composes the
-// maps of the chunks before it (lower t); backward: after it (higher t).  S is
-// the lane distance between consecutive chunks of a line in a warp, CW the
-// number of chunks of one line in a warp, NWG the number of warps a line spans;
-// slot(g, k) indexes the shared-memory carry of line g, warp group k.
-// Returns the map's value at 0 (the incoming value of the chunk).
+// Incoming value of a chunk (its exclusive prefix map applied to 0) by a tree
+// fixed over chunk indices, so that the bits do not depend on how the chunks
+// of a line are laid over lanes, warps and CTAs: positions s along the scan
+// direction (s = t forward, TPL - 1 - t backward) form groups of SG = 4; an
+// inclusive Kogge-Stone scan inside each group (warp shuffles, partner s - o
+// for o = 1, 2), then a scan of the ng <= 64 group totals by one warp per line
+// through shared memory (ng <= 32: Kogge-Stone over the groups, o = 1 .. 16;
+// else lane k pairs groups 2k and 2k + 1 and the Kogge-Stone runs over the
+// pairs), and the chunk's incoming map is its in-group exclusive prefix
+// composed after the prefix of the groups before it.  LS is the lane distance
+// between consecutive chunks of a line (groups must lie inside a warp:
+// SG * LS <= 32, or the whole line when TPL <= SG); `line` indexes the line
+// among the CTA's nlines; gA/gB hold nlines * ng entries.  Every thread of the
+// CTA calls it (threads of no chunk with identity maps): the __syncthreads
+// are uniform.
+constexpr int SG = 4;
+
 template <typename T>
-__device__ __forceinline__ T scan_incoming(T A, T B, bool forward, int u, int S, int CW, int NWG, int k, int slot_self,
-                                           int slot_stride, T *sA, T *sB)
+__device__ __forceinline__ T canon_incoming(T A, T B, bool forward, int t, int TPL, int LS, int line, int nlines,
+                                            T *gA, T *gB)
 {
 	const unsigned full = 0xffffffffu;
-	// inclusive within the warp segment
-	for (int off = 1; off < CW; off <<= 1) {
-		T a2 = forward ? __shfl_up_sync(full, A, off * S) : __shfl_down_sync(full, A, off * S);
-		T b2 = forward ? __shfl_up_sync(full, B, off * S) : __shfl_down_sync(full, B, off * S);
-		if (forward ? u >= off : u + off < CW) after(A, B, a2, b2);
+	const int s = forward ? t : TPL - 1 - t;
+	const int u = s & (SG - 1);
+#pragma unroll
+	for (int o = 1; o < SG; o <<= 1) {
+		const T a2 = forward ? __shfl_up_sync(full, A, o * LS) : __shfl_down_sync(full, A, o * LS);
+		const T b2 = forward ? __shfl_up_sync(full, B, o * LS) : __shfl_down_sync(full, B, o * LS);
+		if (u >= o && s < TPL) after(A, B, a2, b2);
 	}
-	// exclusive within the warp segment
-	T ae = forward ? __shfl_up_sync(full, A, S) : __shfl_down_sync(full, A, S);
-	T be = forward ? __shfl_up_sync(full, B, S) : __shfl_down_sync(full, B, S);
-	const bool first = forward ? u == 0 : u == CW - 1;
-	if (first) { ae = T(1); be = T(0); }
-	if (NWG == 1) return be;
-	// carry across warps: slot of group k holds the inclusive map of the whole group
-	const bool last = forward ? u == CW - 1 : u == 0;
+	T ae = forward ? __shfl_up_sync(full, A, LS) : __shfl_down_sync(full, A, LS);
+	T be = forward ? __shfl_up_sync(full, B, LS) : __shfl_down_sync(full, B, LS);
+	if (u == 0) {
+		ae = T(1);
+		be = T(0);
+	}
+	const int ng = (TPL + SG - 1) / SG;
+	if (ng == 1) return be;
+	const bool real = t < TPL && line < nlines;
+	__syncthreads();  // earlier readers of gA / gB are done
+	if (real && (u == SG - 1 || s == TPL - 1)) {
+		gA[line * ng + s / SG] = A;
+		gB[line * ng + s / SG] = B;
+	}
 	__syncthreads();
-	if (last) { sA[slot_self] = A; sB[slot_self] = B; }
-	__syncthreads();
-	T ca = T(1), cb = T(0);
-	if (forward) {
-		for (int kk = 0; kk < k; ++kk) {  // carry = M_{k-1} o ... o M_0
-			int sl = slot_self + (kk - k) * slot_stride;
-			T a2 = sA[sl], b2 = sB[sl];
-			T na = a2 * ca, nb = madd(a2, cb, b2);
-			ca = na; cb = nb;
-		}
-	} else {
-		for (int kk = NWG - 1; kk > k; --kk) {  // carry = M_{k+1} o ... o M_{NWG-1}
-			int sl = slot_self + (kk - k) * slot_stride;
-			T a2 = sA[sl], b2 = sB[sl];
-			T na = a2 * ca, nb = madd(a2, cb, b2);
-			ca = na; cb = nb;
+	const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+	for (int l = warp; l < nlines; l += nw) {
+		T *la = gA + l * ng, *lb = gB + l * ng;
+		if (ng <= 32) {
+			T ga = lane < ng ? la[lane] : T(1), gb = lane < ng ? lb[lane] : T(0);
+#pragma unroll
+			for (int o = 1; o < 32; o <<= 1) {
+				const T a2 = __shfl_up_sync(full, ga, o), b2 = __shfl_up_sync(full, gb, o);
+				if (lane >= o) after(ga, gb, a2, b2);
+			}
+			if (lane < ng) {
+				la[lane] = ga;
+				lb[lane] = gb;
+			}
+		} else {
+			const int k0 = 2 * lane, k1 = k0 + 1;
+			const T a0 = k0 < ng ? la[k0] : T(1), b0 = k0 < ng ? lb[k0] : T(0);
+			const T a1 = k1 < ng ? la[k1] : T(1), b1 = k1 < ng ? lb[k1] : T(0);
+			T pa = a1, pb = b1;  // the pair: group 2k+1 after group 2k
+			after(pa, pb, a0, b0);
+#pragma unroll
+			for (int o = 1; o < 32; o <<= 1) {
+				const T a2 = __shfl_up_sync(full, pa, o), b2 = __shfl_up_sync(full, pb, o);
+				if (lane >= o) after(pa, pb, a2, b2);
+			}
+			T ea = __shfl_up_sync(full, pa, 1), eb = __shfl_up_sync(full, pb, 1);
+			if (lane == 0) {
+				ea = T(1);
+				eb = T(0);
+			}
+			T qa = a0, qb = b0;  // group 2k after the pairs before it
+			after(qa, qb, ea, eb);
+			if (k0 < ng) {
+				la[k0] = qa;
+				lb[k0] = qb;
+			}
+			if (k1 < ng) {
+				la[k1] = pa;
+				lb[k1] = pb;
+			}
 		}
 	}
-	return madd(ae, cb, be);
+	__syncthreads();
+	const int k = s / SG;
+	if (k == 0 || !real) return be;
+	return madd(ae, gB[line * ng + k - 1], be);
 }
 
 constexpr int FAST_BLOCK_X = 256, FAST_BLOCK_Y = 1024;
 
-template <typename T, int NS, int DIR, int K, bool XL = DIR == CDR_DIR_X>
-__global__ void __launch_bounds__(XL ? FAST_BLOCK_X : FAST_BLOCK_Y, XL ? 2 : 1)
-    k_lines_fast(const T *__restrict__ so, T *__restrict__ q, const T *__restrict__ qf, const T *__restrict__ sor,
-                 Dims2 d, int tpitch, int first, int tpl_log2)
+// G lines of one colour per CTA.  x-lines: thread tid works on chunk
+// t = tid % TPL of line g = tid / TPL (blockDim = G * TPL); y-lines: chunk
+// t = tid / G of line g = tid % G (blockDim >= G * TPL, a multiple of 32; the
+// threads beyond G * TPL hold no chunk).  G * SG <= 32 for y-lines unless
+// TPL <= SG (the scan's groups lie inside a warp): a warp then reads 8 lines,
+// 16 columns of one row (two 32-byte sectors), per row of its chunks.
+// CTA thread bound of the y-line kernel: 1024 (FP32) or 512 (FP64) threads
+template <typename T>
+__host__ __device__ constexpr int yblock_max()
 {
-	// one carry slot per (warp, line of the warp): at most 32 warps x 32 lines
-	__shared__ T sA[FAST_BLOCK_Y], sB[FAST_BLOCK_Y];
-	const int TPL = 1 << tpl_log2;
-	const int G = blockDim.x >> tpl_log2;  // lines per CTA
-	const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-	int g, t;
-	if (XL) { g = tid >> tpl_log2; t = tid & (TPL - 1); }
-	else { g = tid % G; t = tid / G; }
+	return sizeof(T) == 4 ? FAST_BLOCK_Y : FAST_BLOCK_Y / 2;
+}
+
+// Right-hand side of a y-line at (i, j) (relax_lines_y.f90:102-106 operand
+// order, as line_rhs); CG reads x through L2 only (values other CTAs of the
+// same launch have written).
+template <typename T, int NS, bool CG>
+__device__ __forceinline__ T yline_rhs(const T *__restrict__ so, size_t ps, const T *__restrict__ q,
+                                       const T *__restrict__ qf, size_t k, int p)
+{
+	auto Q = [&](size_t i) -> T {
+		if constexpr (CG) return __ldcg(q + i);
+		else return q[i];
+	};
+	const T *w = so + ps;
+	T a = madd(w[k], Q(k - 1), qf[k]);
+	a = madd(w[k + 1], Q(k + 1), a);
+	if (NS == 5) {
+		const T *sw = so + 3 * ps, *nw = so + 4 * ps;
+		a = madd(sw[k], Q(k - p - 1), a);
+		a = madd(nw[k + 1], Q(k - p + 1), a);
+		a = madd(nw[k + p], Q(k + p - 1), a);
+		a = madd(sw[k + p + 1], Q(k + p + 1), a);
+	}
+	return a;
+}
+
+// One chunk (t of TPL) of line lc (0: none) of the CTA's G lines, the whole
+// sweep of a line: right-hand sides, both substitutions by the scans, write
+// back.  g is the line's slot among the CTA's lines; sA/sB hold G*TPL/SG
+// scan totals.  Every thread of the CTA calls it.
+template <typename T, int NS, int DIR, int K, bool CG = false, bool XL = DIR == CDR_DIR_X>
+__device__ __forceinline__ void line_chunk(const T *__restrict__ so, T *__restrict__ q, const T *__restrict__ qf,
+                                           const T *__restrict__ sor, const Dims2 &d, int tpitch, int lc, int g,
+                                           int t, int TPL, int G, T *sA, T *sB)
+{
 	const int n = DIR == CDR_DIR_X ? d.nx : d.ny;
 	const int nl = DIR == CDR_DIR_X ? d.ny : d.nx;
-	const int lc = first + 2 * (blockIdx.x * G + g);
-	const bool active = lc <= nl;
+	const bool active = lc >= 1 && lc <= nl;
 	const int p0 = t * K;
-	const bool has = active && p0 <= n;
+	const bool has = active && t < TPL && p0 <= n;
 	// Chunks cover positions 0 .. TPL*K - 1 (position 0 is the ghost).  Where
 	// TPL*K == n, position n is left over and the last chunk takes it as one more
 	// element (rx, its rhs and then its solution): a level of 2^k + 1 positions
@@ -360,41 +438,40 @@ __global__ void __launch_bounds__(XL ? FAST_BLOCK_X : FAST_BLOCK_Y, XL ? 2 : 1)
 	for (int m = 0; m < K; ++m) r[m] = T(0);
 	if (has) {
 		if (DIR == CDR_DIR_X) {
+			// operand order of relax_lines_x.f90:106-110, in stages so that only
+			// the two neighbour rows and one coupling row are live at a time
 			const size_t k0 = d.at(p0, lc);
 			const T *w = so + ps, *s = so + 2 * ps, *sw = so + 3 * ps, *nw = so + 4 * ps;
-			T b_[K], qm[K], qp[K], s0[K], s1[K];
-			vload<T, K>(qf + k0, b_);
+			T qm[K], qp[K], c[K];
+			vload<T, K>(qf + k0, r);
 			vload<T, K>(q + k0 - P, qm);
-			vload<T, K>(q + k0 + P, qp);
-			vload<T, K>(s + k0, s0);
-			vload<T, K>(s + k0 + P, s1);
+			vload<T, K>(s + k0, c);
 #pragma unroll
-			for (int m = 0; m < K; ++m) r[m] = madd(s1[m], qp[m], madd(s0[m], qm[m], b_[m]));
+			for (int m = 0; m < K; ++m) r[m] = madd(c[m], qm[m], r[m]);
+			vload<T, K>(q + k0 + P, qp);
+			vload<T, K>(s + k0 + P, c);
+#pragma unroll
+			for (int m = 0; m < K; ++m) r[m] = madd(c[m], qp[m], r[m]);
 			const size_t kx = k0 + K;  // position n when xtra
 			if (xtra) rx = madd(s[kx + P], q[kx + P], madd(s[kx], q[kx - P], qf[kx]));
 			if (NS == 5) {
-				T sw0[K], nw0[K], nw1[K], sw1[K];
-				vload<T, K>(sw + k0, sw0);
-				vload<T, K>(nw + k0, nw0);
-				vload<T, K>(nw + k0 + P, nw1);
-				vload<T, K>(sw + k0 + P, sw1);
 				const T qm_l = p0 >= 1 ? q[k0 - P - 1] : T(0), qp_l = p0 >= 1 ? q[k0 + P - 1] : T(0);
 				const bool rin = p0 + K <= n + 1;
 				const T qm_r = rin ? q[k0 - P + K] : T(0), qp_r = rin ? q[k0 + P + K] : T(0);
-				const T nw0_r = rin ? nw[k0 + K] : T(0), sw1_r = rin ? sw[k0 + P + K] : T(0);
+				vload<T, K>(sw + k0, c);
 #pragma unroll
-				for (int m = 0; m < K; ++m) {
-					const T qml = m > 0 ? qm[m - 1] : qm_l, qmr = m < K - 1 ? qm[m + 1] : qm_r;
-					const T qpl = m > 0 ? qp[m - 1] : qp_l, qpr = m < K - 1 ? qp[m + 1] : qp_r;
-					const T nwr = m < K - 1 ? nw0[m + 1] : nw0_r, swr = m < K - 1 ? sw1[m + 1] : sw1_r;
-					// operand order of relax_lines_x.f90:106-110
-					T a = madd(s0[m], qm[m], b_[m]);
-					a = madd(s1[m], qp[m], a);
-					a = madd(sw0[m], qml, a);
-					a = madd(nwr, qmr, a);
-					a = madd(nw1[m], qpl, a);
-					r[m] = madd(swr, qpr, a);
-				}
+				for (int m = 0; m < K; ++m) r[m] = madd(c[m], m > 0 ? qm[m - 1] : qm_l, r[m]);
+				vload<T, K>(nw + k0, c);
+				const T nw0_r = rin ? nw[k0 + K] : T(0);
+#pragma unroll
+				for (int m = 0; m < K; ++m) r[m] = madd(m < K - 1 ? c[m + 1] : nw0_r, m < K - 1 ? qm[m + 1] : qm_r, r[m]);
+				vload<T, K>(nw + k0 + P, c);
+#pragma unroll
+				for (int m = 0; m < K; ++m) r[m] = madd(c[m], m > 0 ? qp[m - 1] : qp_l, r[m]);
+				vload<T, K>(sw + k0 + P, c);
+				const T sw1_r = rin ? sw[k0 + P + K] : T(0);
+#pragma unroll
+				for (int m = 0; m < K; ++m) r[m] = madd(m < K - 1 ? c[m + 1] : sw1_r, m < K - 1 ? qp[m + 1] : qp_r, r[m]);
 				if (xtra) {
 					T a = madd(s[kx], q[kx - P], qf[kx]);
 					a = madd(s[kx + P], q[kx + P], a);
@@ -410,30 +487,13 @@ __global__ void __launch_bounds__(XL ? FAST_BLOCK_X : FAST_BLOCK_Y, XL ? 2 : 1)
 			for (int m = 0; m < K; ++m) {
 				const int jj = p0 + m;
 				if (jj < 1 || jj > n) continue;
-				r[m] = line_rhs<T, NS, CDR_DIR_Y>(so, ps, q, qf, d.at(i, jj), P);
+				r[m] = yline_rhs<T, NS, CG>(so, ps, q, qf, d.at(i, jj), P);
 			}
-			if (xtra) rx = line_rhs<T, NS, CDR_DIR_Y>(so, ps, q, qf, d.at(i, n), P);
+			if (xtra) rx = yline_rhs<T, NS, CG>(so, ps, q, qf, d.at(i, n), P);
 		}
 	}
 
-	// scan geometry
-	int S, CW, NWG, kgrp, slot, sstride;
-	if (XL) {
-		S = 1;
-		CW = TPL < 32 ? TPL : 32;
-		NWG = TPL > 32 ? TPL / 32 : 1;
-		kgrp = TPL > 32 ? (tid - (g << tpl_log2)) >> 5 : 0;
-		slot = warp;
-		sstride = 1;
-	} else {
-		S = G < 32 ? G : 32;
-		CW = 32 / S;
-		NWG = blockDim.x / 32;
-		kgrp = warp;
-		slot = warp * (32 / CW) + (lane % S);  // one slot per (warp, line of the warp)
-		sstride = 32 / CW;
-	}
-	const int u = XL ? (lane & (CW - 1)) : lane / S;
+	const int LS = XL ? 1 : G;  // lane distance of consecutive chunks of a line
 	const bool full = p0 >= 1 && p0 + K - 1 <= n;  // no ghost or beyond-end position in the chunk
 
 	// 2a. forward substitution y(p) = r(p) - y(p-1) E(p)
@@ -455,7 +515,7 @@ __global__ void __launch_bounds__(XL ? FAST_BLOCK_X : FAST_BLOCK_Y, XL ? 2 : 1)
 			A = a * A;
 		}
 	}
-	T y = scan_incoming<T>(A, B, true, u, S, CW, NWG, kgrp, slot, sstride, sA, sB);
+	T y = canon_incoming<T>(A, B, true, t, TPL, LS, g, G, sA, sB);
 	if (has) {
 #pragma unroll
 		for (int m = 0; m < K; ++m) {
@@ -497,8 +557,7 @@ __global__ void __launch_bounds__(XL ? FAST_BLOCK_X : FAST_BLOCK_Y, XL ? 2 : 1)
 			A = a * A;
 		}
 	}
-	if (NWG > 1) __syncthreads();  // the forward carries are still being read
-	T x = scan_incoming<T>(A, B, false, u, S, CW, NWG, kgrp, slot, sstride, sA, sB);
+	T x = canon_incoming<T>(A, B, false, t, TPL, LS, g, G, sA, sB);
 	if (has) {
 		if (xtra) x = rx;
 #pragma unroll
@@ -535,6 +594,115 @@ __global__ void __launch_bounds__(XL ? FAST_BLOCK_X : FAST_BLOCK_Y, XL ? 2 : 1)
 	}
 }
 
+
+// G lines of one colour per CTA.  x-lines: thread tid works on chunk
+// t = tid % TPL of line g = tid / TPL (blockDim = G * TPL); y-lines: chunk
+// t = tid / G of line g = tid % G (blockDim >= G * TPL, a multiple of 32; the
+// threads beyond G * TPL hold no chunk).  G * SG <= 32 for y-lines unless
+// TPL <= SG (the scan's groups lie inside a warp): a warp then reads 8 lines,
+// 16 columns of one row (two 32-byte sectors), per row of its chunks.
+template <typename T, int NS, int DIR, int K, bool XL = DIR == CDR_DIR_X>
+__global__ void __launch_bounds__(XL ? FAST_BLOCK_X : yblock_max<T>(), XL ? 2 : 1)
+    k_lines_fast(const T *__restrict__ so, T *__restrict__ q, const T *__restrict__ qf, const T *__restrict__ sor,
+                 Dims2 d, int tpitch, int first, int tpl_log2, int G)
+{
+	// group totals of the scans: lines * groups = blockDim / SG at most
+	__shared__ T sA[FAST_BLOCK_Y / SG], sB[FAST_BLOCK_Y / SG];
+	const int TPL = 1 << tpl_log2;
+	const int tid = threadIdx.x;
+	int g, t;
+	if (XL) { g = tid >> tpl_log2; t = tid & (TPL - 1); }
+	else { g = tid % G; t = tid / G; }
+	line_chunk<T, NS, DIR, K>(so, q, qf, sor, d, tpitch, first + 2 * (blockIdx.x * G + g), g, t, TPL, G, sA, sB);
+}
+
+// Give-ups of the bounded waits of the line kernels (streamed x-lines, the
+// fused y-line sweep) and the limit of those waits (device globals).
+namespace {
+__device__ unsigned g_xstream_timeouts;
+__device__ unsigned long long g_xstream_wait_ns = kWaitLimitNs;
+}  // namespace
+static_assert(kStreamWaitDefaultNs == kWaitLimitNs, "one default wait limit");
+
+// ------------------------------------------------- both colours in one launch
+// y-line sweep of a single problem, both colours in one launch.  Columns are
+// taken in pairs (p2, p1 = p2 + 1), p1 of the colour swept first; virtual
+// block vb (a ticket drawn at start, so that vb - 1 is already running) owns
+// pairs vb*G .. vb*G + G - 1.  Phase 1 solves its p1 lines, which read the
+// old x of the p2 columns beside them (its own and the next block's first);
+// phase 2 solves its p2 lines, which read the new x of the p1 columns (its
+// own and the previous block's last).  Between the phases the block raises
+// its flag and waits for block vb - 1's: that block has then written its last
+// p1 line and read the old x of our first p2 line, which phase 2 overwrites.
+// The waiting block resets the flag it consumed, and the last block raises
+// none, so all flags are 0 again when the launch ends.  Every coupling column
+// is read by phase 1 and again, moments later, by phase 2 of the same or the
+// next block: the second read comes from L2, so the sweep moves each array
+// through DRAM about once instead of once per colour.  Each line gets the
+// arithmetic of line_chunk: the result equals two k_lines_fast launches bit for
+// bit.  sync[0] is the ticket counter, sync[1 + vb] block vb's flag.  The wait
+// is bounded (g_xstream_wait_ns); a block that gives up counts itself in
+// g_xstream_timeouts and leaves its p2 lines unsolved.
+namespace {
+__device__ __forceinline__ unsigned ld_acquire(const unsigned *p)
+{
+	unsigned v;
+	asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+	return v;
+}
+}  // namespace
+
+template <typename T, int NS, int K>
+__global__ void __launch_bounds__(yblock_max<T>(), 1)
+    k_ylines_pair(const T *__restrict__ so, T *__restrict__ q, const T *__restrict__ qf, const T *__restrict__ sor,
+                  Dims2 d, int tpitch, int c2, int tpl_log2, int G, unsigned *__restrict__ sync, int nvb)
+{
+	__shared__ T sA[FAST_BLOCK_Y / SG], sB[FAST_BLOCK_Y / SG];
+	__shared__ int s_vb, s_ok;
+	const int TPL = 1 << tpl_log2;
+	const int tid = threadIdx.x, g = tid % G, t = tid / G;
+	if (tid == 0) {
+		const unsigned v = atomicAdd(&sync[0], 1u);
+		if (v == gridDim.x - 1) atomicExch(&sync[0], 0u);  // every block has its ticket
+		s_vb = (int)v;
+	}
+	__syncthreads();
+	const int vb = s_vb;
+	const int p2 = 2 * (vb * G + g) + c2, p1 = p2 + 1;
+	line_chunk<T, NS, CDR_DIR_Y, K>(so, q, qf, sor, d, tpitch, p1, g, t, TPL, G, sA, sB);
+	__threadfence();  // this thread's phase-1 lines reach L2 before phase 2 reads them there
+	__syncthreads();  // phase 1 read and written by every thread
+	if (tid == 0) {
+		int ok = 1;
+		if (vb + 1 < nvb) {
+			__threadfence();
+			atomicExch(&sync[1 + vb], 1u);
+		}
+		if (vb > 0) {
+			const unsigned long long limit = g_xstream_wait_ns;
+			ok = 0;
+			if (limit > 0) {
+				const unsigned long long t0 = globaltimer_ns();
+				for (int it = 0; it < (1 << 22); ++it) {
+					if (ld_acquire(&sync[vb])) { ok = 1; break; }
+					if (globaltimer_ns() - t0 > limit) break;
+					__nanosleep(64);
+				}
+			}
+			if (ok) {
+				atomicExch(&sync[vb], 0u);
+				__threadfence();
+			} else {
+				atomicAdd(&g_xstream_timeouts, 1u);
+			}
+		}
+		s_ok = ok;
+	}
+	__syncthreads();
+	if (!s_ok) return;
+	line_chunk<T, NS, CDR_DIR_Y, K, true>(so, q, qf, sor, d, tpitch, p2, g, t, TPL, G, sA, sB);
+}
+
 // ---------------------------------------------------------- streamed x-lines
 // x-lines of one problem with 32K <= n <= 256K: a persistent CTA walks the
 // lines of a colour (l = blockIdx.x, + gridDim.x, ...).  Each line's rows --
@@ -549,11 +717,7 @@ __global__ void __launch_bounds__(XL ? FAST_BLOCK_X : FAST_BLOCK_Y, XL ? 2 : 1)
 // bounded (g_xstream_wait_ns of the global timer); a CTA that gives up counts
 // itself in g_xstream_timeouts, waits (bounded) for the copy it has in flight,
 // so that nothing lands in shared memory after it has left, and returns.
-namespace {
-__device__ unsigned g_xstream_timeouts;
-__device__ unsigned long long g_xstream_wait_ns = kWaitLimitNs;
-}  // namespace
-static_assert(kStreamWaitDefaultNs == kWaitLimitNs, "one default wait limit");
+
 
 int lines_stream_timeouts(cudaStream_t st, unsigned *count)
 {
@@ -606,7 +770,7 @@ __global__ void __launch_bounds__(XS_BLOCK, 2) k_lines_xstream(const T *__restri
                                                                Dims2 d, int first, int nlines)
 {
 	extern __shared__ __align__(128) unsigned char xs_raw[];
-	__shared__ T sA[XS_BLOCK / 32], sB[XS_BLOCK / 32];
+	__shared__ T sA[XS_BLOCK / SG], sB[XS_BLOCK / SG];  // group totals of the scans
 	constexpr int R = xs_rows<NS>();
 	uint64_t *bar = reinterpret_cast<uint64_t *>(xs_raw);
 	T *rows = reinterpret_cast<T *>(xs_raw + 128);
@@ -637,9 +801,6 @@ __global__ void __launch_bounds__(XS_BLOCK, 2) k_lines_xstream(const T *__restri
 	const int G = gridDim.x;
 	if (tid == 0 && (int)blockIdx.x < nlines) issue(blockIdx.x);
 
-	// scan geometry of one line per CTA (k_lines_fast's x-line case with G = 1)
-	const int CW = TPL < 32 ? TPL : 32, NWG = TPL > 32 ? TPL / 32 : 1, kgrp = TPL > 32 ? warp : 0;
-	const int u = lane & (CW - 1);
 	const int p0 = tid * K;
 	const bool has = p0 <= n;
 	const bool xtra = has && tid == TPL - 1 && p0 + K == n;
@@ -756,7 +917,7 @@ __global__ void __launch_bounds__(XS_BLOCK, 2) k_lines_xstream(const T *__restri
 				A = a * A;
 			}
 		}
-		T y = scan_incoming<T>(A, B, true, u, 1, CW, NWG, kgrp, warp, 1, sA, sB);
+		T y = canon_incoming<T>(A, B, true, tid, TPL, 1, 0, 1, sA, sB);
 		if (has) {
 #pragma unroll
 			for (int m = 0; m < K; ++m) {
@@ -790,8 +951,7 @@ __global__ void __launch_bounds__(XS_BLOCK, 2) k_lines_xstream(const T *__restri
 				A = a * A;
 			}
 		}
-		if (NWG > 1) __syncthreads();  // the forward carries are still being read
-		T x = scan_incoming<T>(A, B, false, u, 1, CW, NWG, kgrp, warp, 1, sA, sB);
+		T x = canon_incoming<T>(A, B, false, tid, TPL, 1, 0, 1, sA, sB);
 		if (has) {
 			if (xtra) x = rx;
 #pragma unroll
@@ -838,7 +998,7 @@ int lines_prepare()
 #undef CDR_LINES_ATTR
 #define CDR_XS_ATTR(T, NS, K) \
 	CDR_CUDA_TRY(cudaFuncSetAttribute(k_lines_xstream<T, NS, K>, cudaFuncAttributeMaxDynamicSharedMemorySize, XS_SMEM_MAX))
-	CDR_XS_ATTR(float, 5, 8); CDR_XS_ATTR(float, 3, 8); CDR_XS_ATTR(double, 5, 4); CDR_XS_ATTR(double, 3, 4);
+	CDR_XS_ATTR(float, 5, 8); CDR_XS_ATTR(float, 3, 8);
 #undef CDR_XS_ATTR
 	CDR_TRY(coarse_prepare());
 	done = true;
@@ -858,14 +1018,14 @@ static int lines_per_cta(int n, int dir)
 }
 
 // ---------------------------------------------------------------- launch shapes
-// The register-chunk kernel's shape: K elements per thread and, for y-lines,
-// the CTA size cap (x-lines always run FAST_BLOCK_X threads).  The default is
-// K = 8 (16 for FP32 y-lines longer than 1024 points) and the largest CTA;
-// lines_autotune times the candidates on a level's own arrays at setup and
-// records the fastest per (direction, type, stencil, n, lines, single problem
-// or batch).  The
-// record lives for the process, so every solver of one shape in a process
-// runs the same launches (FP32 results depend on the chunking).
+// The register-chunk kernels run K elements per thread with K fixed by the
+// line length (8 up to 2048 points, 16 up to 4096 for FP32), so the chunks of
+// a line, and with them the scan's tree and every bit of the result, are the
+// same whatever the launch shape.  The shape is then free: the CTA size (x) or
+// the lines per CTA (y), and for x-lines the streamed kernel.  lines_autotune
+// times the candidates on a level's own arrays at setup and records the
+// fastest per (direction, type, stencil, n, lines, single problem or batch)
+// for the process.
 namespace {
 struct LineKey {
 	int dir, tsize, ns, n, nl, nb;
@@ -882,33 +1042,52 @@ std::map<LineKey, LineShape> &shape_table()
 }
 }  // namespace
 
+// Elements per thread of the register-chunk kernels for lines of n points in
+// direction dir (0: none): 8 up to 2048 points, with y-lines of more than 1024
+// points at 16 (a whole line within 128 threads, so that a CTA holds the 8
+// lines a warp's row reads need), and 16 up to 4096 (FP32 x-lines, y-lines).
+template <typename T>
+static int canon_K(int n, int dir)
+{
+	if (dir == CDR_DIR_Y && n > 1024 && n <= 16 * 256) return 16;
+	if (n <= 8 * 256) return 8;
+	if (sizeof(T) == 4 && n <= 16 * 256) return 16;
+	return 0;
+}
+
+static int tpl_log2_of(int n, int K)
+{
+	int l = 0;
+	while ((1 << l) * K < n) ++l;  // chunks cover 0 .. n - 1, the last one also n
+	return l;
+}
+
+// y-lines per CTA for a CTA thread cap: the scan's groups of SG chunks must lie
+// inside a warp (G * SG <= 32), or the whole line when TPL <= SG
+static int ylines_per_cta(int TPL, int cap)
+{
+	const int gmax = TPL > SG ? 32 / SG : 32 / TPL;  // at most 8 (TPL > 4) or 32 lines
+	int G = cap / TPL;
+	if (G < 1) G = 1;
+	if (G > gmax) G = gmax;
+	return G;
+}
+
 template <typename T>
 static LineShape default_shape(int n, int dir, int nb = 1)
 {
-	// FP32 x-lines longer than 1024 points: the streamed kernel (K = 8, the same
-	// results as the register-chunk kernel; a batch or a misaligned level falls
-	// back to that kernel with the same K)
-	const int stream = dir == CDR_DIR_X && sizeof(T) == 4 && n > 1024 ? 1 : 0;
-	if (dir == CDR_DIR_Y && sizeof(T) == 4) {
-		// FP32 y-lines: for a single problem, K = 4 in small CTAs for short lines
-		// (the shapes the timing picks there inside a cycle); K = 16 for lines
-		// longer than 1024 points
-		if (nb == 1 && n <= 160) return LineShape{4, 256, 0};
-		if (nb == 1 && n <= 320) return LineShape{4, 128, 0};
-		return LineShape{n > 8 * 128 ? 16 : 8, FAST_BLOCK_Y, 0};
-	}
-	return LineShape{8, FAST_BLOCK_Y, stream};
+	// FP32 x-lines longer than 1024 points of a single problem: the streamed
+	// kernel (a batch or a misaligned level falls back to the register-chunk one)
+	const int stream = dir == CDR_DIR_X && sizeof(T) == 4 && n > 1024 && nb == 1 ? 1 : 0;
+	return LineShape{canon_K<T>(n, dir), dir == CDR_DIR_X ? FAST_BLOCK_X : yblock_max<T>(), stream};
 }
 
 template <typename T>
 static bool shape_ok(LineShape sh, int n, int dir)
 {
-	const bool kok = sizeof(T) == 4 ? (sh.K == 4 || sh.K == 8 || sh.K == 16) : (sh.K == 2 || sh.K == 4 || sh.K == 8);
-	if (!kok || n > 256 * sh.K) return false;
-	int tpl = 1;
-	while (tpl * sh.K < n) tpl *= 2;
-	if (dir == CDR_DIR_X) return tpl <= FAST_BLOCK_X && sh.cap >= 32;
-	return sh.cap >= 32 && sh.cap <= FAST_BLOCK_Y && tpl <= sh.cap;
+	const int K = canon_K<T>(n, dir);
+	if (K == 0 || sh.K != K || sh.cap < 32) return false;
+	return dir == CDR_DIR_X ? sh.cap <= FAST_BLOCK_X || sh.stream : sh.cap <= yblock_max<T>();
 }
 
 template <typename T>
@@ -924,38 +1103,36 @@ static int launch_fast(const T *so, T *x, const T *b, const T *sor, Dims2 d, int
                        int cap, cudaStream_t st)
 {
 	const int n = DIR == CDR_DIR_X ? d.nx : d.ny;
-	int tpl_log2 = 0;
-	while ((1 << tpl_log2) * K < n) ++tpl_log2;  // chunks cover 0 .. n - 1, the last one also n
+	const int tpl_log2 = tpl_log2_of(n, K);
 	const int TPL = 1 << tpl_log2;
-	// x: cap CTA threads (at least one line, at most FAST_BLOCK_X); y: up to 32
-	// lines, at most cap threads
-	const int block = DIR == CDR_DIR_X ? std::min(FAST_BLOCK_X, std::max(TPL, cap)) : (TPL * 32 < cap ? TPL * 32 : cap);
-	const int G = block / TPL;
+	int G, block;
+	if (DIR == CDR_DIR_X) {  // cap CTA threads, at least one line, at most FAST_BLOCK_X
+		block = std::min(FAST_BLOCK_X, std::max(TPL, cap));
+		G = block / TPL;
+	} else {
+		G = ylines_per_cta(TPL, cap);
+		block = (G * TPL + 31) / 32 * 32;
+	}
 	k_lines_fast<T, NS, DIR, K><<<dim3(ceil_div(nlines, G), 1, d.nb), block, 0, st>>>(so, x, b, sor, d, tpitch, first,
-	                                                                                  tpl_log2);
+	                                                                                  tpl_log2, G);
 	CDR_LAUNCH_CHECK();
 	return CDR_OK;
 }
 
-// The streamed x-line kernel: K = 8 (FP32) or 4 (FP64) elements per thread, one
-// line per CTA step (TPL = 32 .. 256 threads), a single problem, both stages
-// within the shared-memory budget.
-template <typename T>
-__host__ __device__ constexpr int xs_K()
-{
-	return sizeof(T) == 4 ? 8 : 4;
-}
-
+// The streamed x-line kernel (FP32, K = 8, the register-chunk kernel's K for
+// these lengths): one line per CTA step (TPL = 32 .. 256 threads), a single
+// problem, the stage within the shared-memory budget.
 template <typename T, int NS>
 static bool xs_ok(Dims2 d)
 {
-	const int K = xs_K<T>(), n = d.nx;
-	return d.nb == 1 && n >= 32 * K && n <= XS_BLOCK * K && xs_smem<T, NS>(d.pitch) <= XS_SMEM_MAX;
+	const int n = d.nx;
+	return sizeof(T) == 4 && canon_K<T>(n, CDR_DIR_X) == 8 && d.nb == 1 && n >= 32 * 8 && n <= XS_BLOCK * 8 &&
+	       xs_smem<T, NS>(d.pitch) <= XS_SMEM_MAX;
 }
 
 // CTAs per SM of the streamed kernel for a (block, shared memory) pair, and the
 // SM count: looked up once per pair
-template <typename T, int NS>
+template <int NS>
 static int xs_grid_cap(int block, size_t smem)
 {
 	static std::mutex mu;
@@ -965,28 +1142,46 @@ static int xs_grid_cap(int block, size_t smem)
 	if (it != cache.end()) return it->second;
 	int dev = 0, sms = 0, per_sm = 0;
 	if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
-	    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_lines_xstream<T, NS, xs_K<T>()>, block, smem) != cudaSuccess)
+	    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_lines_xstream<float, NS, 8>, block, smem) != cudaSuccess)
 		return 0;
 	const int cap = sms * (per_sm > 0 ? per_sm : 1);
 	cache[{block, smem}] = cap;
 	return cap;
 }
 
-template <typename T, int NS>
-static int launch_xstream(const T *so, T *x, const T *b, const T *sor, Dims2 d, int first, int nlines, cudaStream_t st)
+template <int NS>
+static int launch_xstream(const float *so, float *x, const float *b, const float *sor, Dims2 d, int first, int nlines,
+                          cudaStream_t st)
 {
-	constexpr int K = xs_K<T>();
-	int tpl = 1;
-	while (tpl * K < d.nx) tpl *= 2;
-	const size_t smem = xs_smem<T, NS>(d.pitch);
+	const int tpl = 1 << tpl_log2_of(d.nx, 8);
+	const size_t smem = xs_smem<float, NS>(d.pitch);
 	CDR_TRY(lines_prepare());
-	const int cap = xs_grid_cap<T, NS>(tpl, smem);
+	const int cap = xs_grid_cap<NS>(tpl, smem);
 	if (cap <= 0) {
 		set_error(CDR_ERR_CUDA, "occupancy query for the streamed line kernel failed");
 		return CDR_ERR_CUDA;
 	}
 	const int grid = nlines < cap ? nlines : cap;
-	k_lines_xstream<T, NS, K><<<grid, tpl, smem, st>>>(so, x, b, sor, d, first, nlines);
+	k_lines_xstream<float, NS, 8><<<grid, tpl, smem, st>>>(so, x, b, sor, d, first, nlines);
+	CDR_LAUNCH_CHECK();
+	return CDR_OK;
+}
+
+// Words of the sync buffer of the fused y-line sweep of a level: a ticket
+// counter and one flag per virtual block (at most one block per column pair).
+size_t lines_sync_words(Dims2 d) { return 2 + (size_t)d.nx / 2 + 1; }
+
+template <typename T, int NS, int K>
+static int launch_ypair(const T *so, T *x, const T *b, const T *sor, Dims2 d, int tpitch, int updown, int cap,
+                        unsigned *sync, cudaStream_t st)
+{
+	const int tpl_log2 = tpl_log2_of(d.ny, K), TPL = 1 << tpl_log2;
+	const int G = ylines_per_cta(TPL, cap);
+	const int block = (G * TPL + 31) / 32 * 32;
+	// DOWN sweeps the even lines first (relax_lines_y.f90:82-97): pairs (odd, even)
+	const int c2 = updown == CDR_DOWN ? 1 : 0;
+	const int npairs = (d.nx - c2) / 2 + 1, nvb = ceil_div(npairs, G);
+	k_ylines_pair<T, NS, K><<<nvb, block, 0, st>>>(so, x, b, sor, d, tpitch, c2, tpl_log2, G, sync, nvb);
 	CDR_LAUNCH_CHECK();
 	return CDR_OK;
 }
@@ -1001,23 +1196,20 @@ static int launch_lines(const T *so, T *x, const T *b, const T *sor, Dims2 d, in
 	if (nlines == 0) return CDR_OK;
 	// The register-chunk kernel reads whole 16-byte-aligned chunks of K elements:
 	// rows (x) or factor lines (y) must have a pitch that is a multiple of K and
-	// 16-byte aligned base pointers; lines up to 256*K - 1 points.
+	// 16-byte aligned base pointers; lines up to 256*K points.
 	const int fpitch = DIR == CDR_DIR_X ? d.pitch : tpitch;
 	const bool aligned = ((uintptr_t)so | (uintptr_t)x | (uintptr_t)b | (uintptr_t)sor) % 16 == 0;
 	LineShape sh = force ? *force : shape_for<T>(n, nl, NS, d.nb, DIR);
 	if (!shape_ok<T>(sh, n, DIR)) sh = default_shape<T>(n, DIR, d.nb);
 	if (!exact && aligned && d.pitch % 16 == 0 && fpitch % 16 == 0 && shape_ok<T>(sh, n, DIR)) {
-		if constexpr (DIR == CDR_DIR_X)
-			if (sh.stream && sh.K == xs_K<T>() && xs_ok<T, NS>(d))
-				return launch_xstream<T, NS>(so, x, b, sor, d, first, nlines, st);
-		if constexpr (sizeof(T) == 4) {
-			if (sh.K == 4) return launch_fast<T, NS, DIR, 4>(so, x, b, sor, d, tpitch, first, nlines, sh.cap, st);
-			if (sh.K == 16) return launch_fast<T, NS, DIR, 16>(so, x, b, sor, d, tpitch, first, nlines, sh.cap, st);
+		if constexpr (DIR == CDR_DIR_X && sizeof(T) == 4)
+			if (sh.stream && xs_ok<T, NS>(d)) return launch_xstream<NS>(so, x, b, sor, d, first, nlines, st);
+		if (sh.K == 16) {
+			if constexpr (sizeof(T) == 4 || DIR == CDR_DIR_Y)
+				return launch_fast<T, NS, DIR, 16>(so, x, b, sor, d, tpitch, first, nlines, sh.cap, st);
 		} else {
-			if (sh.K == 2) return launch_fast<T, NS, DIR, 2>(so, x, b, sor, d, tpitch, first, nlines, sh.cap, st);
-			if (sh.K == 4) return launch_fast<T, NS, DIR, 4>(so, x, b, sor, d, tpitch, first, nlines, sh.cap, st);
+			return launch_fast<T, NS, DIR, 8>(so, x, b, sor, d, tpitch, first, nlines, sh.cap, st);
 		}
-		return launch_fast<T, NS, DIR, 8>(so, x, b, sor, d, tpitch, first, nlines, sh.cap, st);
 	}
 	const int G = lines_per_cta<T>(n, DIR);
 	size_t smem = sizeof(T) * (2 * LT + (size_t)G * n);
@@ -1034,7 +1226,8 @@ static int launch_lines(const T *so, T *x, const T *b, const T *sor, Dims2 d, in
 }
 
 template <typename T, int NS, int DIR>
-static int tune_dir(const T *so, T *x, const T *b, const T *sor, Dims2 d, int tpitch, cudaStream_t st)
+static int tune_dir(const T *so, T *x, const T *b, const T *sor, Dims2 d, int tpitch, cudaStream_t st,
+                    unsigned *ysync)
 {
 	const int n = DIR == CDR_DIR_X ? d.nx : d.ny;
 	const int nl = DIR == CDR_DIR_X ? d.ny : d.nx;
@@ -1043,23 +1236,17 @@ static int tune_dir(const T *so, T *x, const T *b, const T *sor, Dims2 d, int tp
 		std::lock_guard<std::mutex> lk(g_shape_mu);
 		if (shape_table().count(key)) return CDR_OK;
 	}
-	// FP32 results depend on K (and, for y-lines, on the lines per CTA) through
-	// the order in which the scans compose their maps, and the FP32 cycle's
-	// outer iteration count moves with that rounding: for a single problem,
-	// FP32 x-lines try only shapes with the default K (bit-identical among
-	// themselves) and FP32 y-lines keep the default, so that every run of an FP32
-	// solve gives the same bits.  Batches (many small problems, or the planes of
-	// a 3D plane smoother) time every candidate.
-	const int kdef = default_shape<T>(n, DIR, d.nb).K;
-	const bool fixed_bits = sizeof(T) == 4 && d.nb == 1;
-	if (fixed_bits && DIR == CDR_DIR_Y) {
+	// every candidate gives the same bits (the chunks are fixed by the line
+	// length); x: CTA sizes, y: lines per CTA
+	const int K = canon_K<T>(n, DIR);
+	if (K == 0) {
 		std::lock_guard<std::mutex> lk(g_shape_mu);
 		shape_table()[key] = default_shape<T>(n, DIR, d.nb);
 		return CDR_OK;
 	}
-	const int ks[3] = {sizeof(T) == 4 ? 4 : 2, sizeof(T) == 4 ? 8 : 4, sizeof(T) == 4 ? 16 : 8};
-	// small CTAs spread the few lines of a coarse level over more SMs
-	const int caps[6] = {32, 64, 128, 256, 512, FAST_BLOCK_Y};
+	const int TPL = 1 << tpl_log2_of(n, K);
+	const int caps_x[4] = {32, 64, 128, 256};
+	const int caps_y[4] = {TPL, 2 * TPL, 4 * TPL, 8 * TPL};
 	// Each candidate is timed on one sweep (both colours) after L2 has been
 	// overwritten, best of three: the sweep of a level inside a cycle finds its
 	// arrays in DRAM, and a level that fits in L2 would otherwise favour shapes
@@ -1085,7 +1272,13 @@ static int tune_dir(const T *so, T *x, const T *b, const T *sor, Dims2 d, int tp
 				rc = CDR_ERR_CUDA;
 				break;
 			}
-			for (int f = 1; f <= 2 && rc == CDR_OK; ++f) rc = launch_lines<T, NS, DIR>(so, x, b, sor, d, tpitch, f, false, st, &sh);
+			if (DIR == CDR_DIR_Y && ysync && d.nb == 1) {  // the one-launch sweep the solver runs
+				rc = sh.K == 16 ? launch_ypair<T, NS, 16>(so, x, b, sor, d, tpitch, CDR_DOWN, sh.cap, ysync, st)
+				                : launch_ypair<T, NS, 8>(so, x, b, sor, d, tpitch, CDR_DOWN, sh.cap, ysync, st);
+			} else {
+				for (int f = 1; f <= 2 && rc == CDR_OK; ++f)
+					rc = launch_lines<T, NS, DIR>(so, x, b, sor, d, tpitch, f, false, st, &sh);
+			}
 			if (rc != CDR_OK) break;
 			float t = 0.f;
 			if (cudaEventRecord(e1, st) != cudaSuccess || cudaEventSynchronize(e1) != cudaSuccess ||
@@ -1104,15 +1297,15 @@ static int tune_dir(const T *so, T *x, const T *b, const T *sor, Dims2 d, int tp
 	const float margin = 4 * level_bytes > flush_bytes / 2 ? 0.90f : 0.95f;
 	LineShape best = default_shape<T>(n, DIR, d.nb);
 	float best_ms = time_shape(best);
-	for (int a = 0; a < 3 && rc == CDR_OK; ++a)
-		for (int c = 0; c < (DIR == CDR_DIR_X ? 4 : 6) && rc == CDR_OK; ++c) {
-			const LineShape sh{ks[a], caps[c]};
-			if (!shape_ok<T>(sh, n, DIR) || (fixed_bits && sh.K != kdef)) continue;
-			const float ms = time_shape(sh);
-			if (ms < margin * best_ms) { best_ms = ms; best = sh; }
-		}
-	if (DIR == CDR_DIR_X && rc == CDR_OK && xs_ok<T, NS>(d) && (!fixed_bits || xs_K<T>() == kdef)) {
-		const LineShape sh{xs_K<T>(), FAST_BLOCK_X, 1};
+	for (int c = 0; c < 4 && rc == CDR_OK; ++c) {
+		const LineShape sh{K, DIR == CDR_DIR_X ? caps_x[c] : std::max(32, caps_y[c]), 0};
+		if (!shape_ok<T>(sh, n, DIR)) continue;
+		if (DIR == CDR_DIR_X && sh.cap < TPL && caps_x[c] != 32) continue;  // same CTA as a smaller cap
+		const float ms = time_shape(sh);
+		if (ms < margin * best_ms) { best_ms = ms; best = sh; }
+	}
+	if (DIR == CDR_DIR_X && rc == CDR_OK && xs_ok<T, NS>(d)) {
+		const LineShape sh{K, FAST_BLOCK_X, 1};
 		const float ms = time_shape(sh);
 		if (ms < margin * best_ms) { best_ms = ms; best = sh; }
 	}
@@ -1128,26 +1321,26 @@ static int tune_dir(const T *so, T *x, const T *b, const T *sor, Dims2 d, int tp
 
 template <typename T>
 int lines_autotune(const T *so, int nstencil, T *x, const T *b, const T *sor, Dims2 d, int tpitch, int dir,
-                   cudaStream_t st)
+                   cudaStream_t st, unsigned *ysync)
 {
 	if (dir == CDR_DIR_X) {
-		if (nstencil == 5) return tune_dir<T, 5, CDR_DIR_X>(so, x, b, sor, d, tpitch, st);
-		return tune_dir<T, 3, CDR_DIR_X>(so, x, b, sor, d, tpitch, st);
+		if (nstencil == 5) return tune_dir<T, 5, CDR_DIR_X>(so, x, b, sor, d, tpitch, st, ysync);
+		return tune_dir<T, 3, CDR_DIR_X>(so, x, b, sor, d, tpitch, st, ysync);
 	}
-	if (nstencil == 5) return tune_dir<T, 5, CDR_DIR_Y>(so, x, b, sor, d, tpitch, st);
-	return tune_dir<T, 3, CDR_DIR_Y>(so, x, b, sor, d, tpitch, st);
+	if (nstencil == 5) return tune_dir<T, 5, CDR_DIR_Y>(so, x, b, sor, d, tpitch, st, ysync);
+	return tune_dir<T, 3, CDR_DIR_Y>(so, x, b, sor, d, tpitch, st, ysync);
 }
 template int lines_autotune<double>(const double *, int, double *, const double *, const double *, Dims2, int, int,
-                                    cudaStream_t);
+                                    cudaStream_t, unsigned *);
 template int lines_autotune<float>(const float *, int, float *, const float *, const float *, Dims2, int, int,
-                                   cudaStream_t);
+                                   cudaStream_t, unsigned *);
 
 bool lines_set_shape(int dir, int tsize, int ns, int n, int nl, int nb, LineShape sh)
 {
 	bool ok;
 	if (tsize == 4) ok = shape_ok<float>(sh, n, dir);
 	else ok = shape_ok<double>(sh, n, dir);
-	if (sh.stream) ok = dir == CDR_DIR_X && nb == 1 && sh.K == (tsize == 4 ? 8 : 4);
+	if (sh.stream) ok = ok && dir == CDR_DIR_X && nb == 1 && tsize == 4 && sh.K == 8;
 	if (!ok) return false;
 	std::lock_guard<std::mutex> lk(g_shape_mu);
 	shape_table()[LineKey{dir, tsize, ns, n, nl, nb > 1 ? 2 : 1}] = sh;
@@ -1165,13 +1358,28 @@ bool lines_shape(int dir, int tsize, int ns, int n, int nl, int nb, LineShape *o
 
 template <typename T>
 int relax_lines_2d(const T *so, int nstencil, T *x, const T *b, const T *sor, Dims2 d, int tpitch, int dir,
-                   int updown, int flags, cudaStream_t st)
+                   int updown, int flags, cudaStream_t st, unsigned *ysync)
 {
 	const bool exact = (flags & CDR_LINES_EXACT) != 0;
 	const LineShape dflt = default_shape<T>(dir == CDR_DIR_X ? d.nx : d.ny, dir, d.nb);
-	const LineShape streamed{xs_K<T>(), FAST_BLOCK_X, 1};
+	const LineShape streamed{canon_K<T>(d.nx, CDR_DIR_X), FAST_BLOCK_X, 1};
 	const LineShape *force = (flags & CDR_LINES_NOTUNE) ? &dflt : nullptr;
 	if ((flags & CDR_LINES_STREAM) && dir == CDR_DIR_X) force = &streamed;
+	// y-lines of a single problem with a sync buffer: both colours in one launch
+	if (dir == CDR_DIR_Y && ysync && !exact && d.nb == 1 && d.nx >= 2 &&
+	    ((uintptr_t)so | (uintptr_t)x | (uintptr_t)b | (uintptr_t)sor) % 16 == 0 && d.pitch % 16 == 0 &&
+	    tpitch % 16 == 0) {
+		LineShape sh = force ? *force : shape_for<T>(d.ny, d.nx, nstencil, d.nb, dir);
+		if (!shape_ok<T>(sh, d.ny, dir)) sh = dflt;
+		if (shape_ok<T>(sh, d.ny, dir)) {
+			if (sh.K == 16) {
+				if (nstencil == 5) return launch_ypair<T, 5, 16>(so, x, b, sor, d, tpitch, updown, sh.cap, ysync, st);
+				return launch_ypair<T, 3, 16>(so, x, b, sor, d, tpitch, updown, sh.cap, ysync, st);
+			}
+			if (nstencil == 5) return launch_ypair<T, 5, 8>(so, x, b, sor, d, tpitch, updown, sh.cap, ysync, st);
+			return launch_ypair<T, 3, 8>(so, x, b, sor, d, tpitch, updown, sh.cap, ysync, st);
+		}
+	}
 	// DOWN: lines with Fortran start index 3 (0-based even) first, then 2 (odd);
 	// UP: the opposite (relax_lines_x.f90:82-97).
 	const int firsts[2] = {updown == CDR_DOWN ? 2 : 1, updown == CDR_DOWN ? 1 : 2};
@@ -1188,8 +1396,8 @@ int relax_lines_2d(const T *so, int nstencil, T *x, const T *b, const T *sor, Di
 	return CDR_OK;
 }
 template int relax_lines_2d<double>(const double *, int, double *, const double *, const double *, Dims2, int, int,
-                                    int, int, cudaStream_t);
+                                    int, int, cudaStream_t, unsigned *);
 template int relax_lines_2d<float>(const float *, int, float *, const float *, const float *, Dims2, int, int, int,
-                                   int, cudaStream_t);
+                                   int, cudaStream_t, unsigned *);
 
 }  // namespace cdrgpu

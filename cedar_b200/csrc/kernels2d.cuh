@@ -14,9 +14,14 @@ int relax_point_2d(const T *so, int nstencil, T *x, const T *b, const T *sor, Di
 template <typename TS>
 int setup_lines_2d(const double *so, int nstencil, TS *sor, Dims2 d, int tpitch, int dir, int *info, cudaStream_t st);
 int lines_prepare();
+// ysync (device, lines_sync_words(d) words, zero before the first use and
+// between uses): y-lines of a single problem sweep both colours in one launch
+// (k_ylines_pair, bit-identical to the two one-colour launches); one buffer
+// per stream, since concurrent sweeps on it would race.
 template <typename T>
 int relax_lines_2d(const T *so, int nstencil, T *x, const T *b, const T *sor, Dims2 d, int tpitch, int dir,
-                   int updown, int flags, cudaStream_t st);
+                   int updown, int flags, cudaStream_t st, unsigned *ysync = nullptr);
+size_t lines_sync_words(Dims2 d);
 // Launch shape of the line kernel (K elements per thread, y-line CTA cap) and
 // the setup-time autotuner that picks it per level (k2_lines.cu).  The tuner
 // runs line sweeps on the arrays it is given (x changes unless x = 0 and b = 0).
@@ -40,7 +45,7 @@ constexpr unsigned long long kStreamWaitDefaultNs = 200000000ull;  // kWaitLimit
 int cg_inv_set_wait(unsigned long long ns);
 template <typename T>
 int lines_autotune(const T *so, int nstencil, T *x, const T *b, const T *sor, Dims2 d, int tpitch, int dir,
-                   cudaStream_t st);
+                   cudaStream_t st, unsigned *ysync = nullptr);
 bool lines_shape(int dir, int tsize, int ns, int n, int nl, int nb, LineShape *out);
 // pin a shape for a line geometry (the autotuner then leaves it); false if the
 // shape cannot run lines of length n

@@ -57,6 +57,7 @@ struct cdr_gpu_solver {
 	double *kb = nullptr, *kx[2] = {nullptr, nullptr}, *kr = nullptr, *kp[2] = {nullptr, nullptr}, *kq = nullptr;
 	FcgScalars *ks = nullptr;
 	double *kpart = nullptr;  // partial sums of the FCG kernels
+	unsigned *ysync = nullptr;  // tickets and flags of the one-launch y-line sweeps (k2_lines.cu)
 	double *ainv = nullptr;   // CDR_COARSE_INVERSE: inverse of the coarsest operator
 	float *ainv32 = nullptr;
 	// FCG iteration graphs: [0] FP64, [1] FP32 cycle; [.][0] residual updated, [.][1] formed
@@ -150,14 +151,16 @@ int cdr_gpu_solver::smooth(int l, T *x, const T *b, int updown)
 			CDR_TRY(relax_lines_2d<T>(so, L.ns, x, b, sor, L.d, L.tpitch, CDR_DIR_X, updown, lflags<T>(), st));
 			break;
 		case CDR_RELAX_LINE_Y:
-			CDR_TRY(relax_lines_2d<T>(so, L.ns, x, b, sory, L.d, L.tpitch, CDR_DIR_Y, updown, lflags<T>(), st));
+			CDR_TRY(relax_lines_2d<T>(so, L.ns, x, b, sory, L.d, L.tpitch, CDR_DIR_Y, updown, lflags<T>(), st, ysync));
 			break;
 		case CDR_RELAX_LINE_XY:
 			if (updown == CDR_DOWN) {
 				CDR_TRY(relax_lines_2d<T>(so, L.ns, x, b, sor, L.d, L.tpitch, CDR_DIR_X, updown, lflags<T>(), st));
-				CDR_TRY(relax_lines_2d<T>(so, L.ns, x, b, sory, L.d, L.tpitch, CDR_DIR_Y, updown, lflags<T>(), st));
+				CDR_TRY(relax_lines_2d<T>(so, L.ns, x, b, sory, L.d, L.tpitch, CDR_DIR_Y, updown, lflags<T>(), st,
+				                          ysync));
 			} else {
-				CDR_TRY(relax_lines_2d<T>(so, L.ns, x, b, sory, L.d, L.tpitch, CDR_DIR_Y, updown, lflags<T>(), st));
+				CDR_TRY(relax_lines_2d<T>(so, L.ns, x, b, sory, L.d, L.tpitch, CDR_DIR_Y, updown, lflags<T>(), st,
+				                          ysync));
 				CDR_TRY(relax_lines_2d<T>(so, L.ns, x, b, sor, L.d, L.tpitch, CDR_DIR_X, updown, lflags<T>(), st));
 			}
 			break;
@@ -379,7 +382,7 @@ int cdr_gpu_solver::tune_lines()
 			                          CDR_DIR_X, st));
 		if (ly)
 			CDR_TRY(lines_autotune<T>(Arr<T>::so(F), F.ns, Arr<T>::x(F), Arr<T>::b(F), Arr<T>::sory(F), F.d, F.tpitch,
-			                          CDR_DIR_Y, st));
+			                          CDR_DIR_Y, st, ysync));
 	}
 	return CDR_OK;
 }
@@ -584,6 +587,7 @@ static int create_impl(cdr_gpu_solver *h, const double *so_src, int ns, int nx, 
 	}
 	CDR_TRY(h->alloc(&h->info, 2));
 	CDR_TRY(h->alloc(&h->norm, 4));
+	CDR_TRY(h->alloc(&h->ysync, lines_sync_words(h->lv[0].d)));
 	CDR_TRY(h->alloc(&h->partial, kNormScratchBytes / sizeof(double)));
 	if (h->mixed()) {
 		CDR_TRY(h->alloc(&h->x64[0], h->lv[0].d.plane()));
@@ -799,7 +803,10 @@ static int solve_loaded(cdr_gpu_solver *h, int *iters, double *hist, int maxhist
 	CDR_TRY(lines_stream_timeouts(st, &to_lines));
 	if (h->s.coarse_solve == CDR_COARSE_INVERSE) CDR_TRY(cg_inv_timeouts(st, &to_inv));
 	if (to_lines || to_inv) {
-		set_error(CDR_ERR_NUMERIC, "%u streamed line-sweep CTAs and %u inverse-product CTAs gave up waiting for their rows",
+		// a y-line block that gave up left its flags set: clear them for the next solve
+		CDR_CUDA_TRY(cudaMemsetAsync(h->ysync, 0, sizeof(unsigned) * lines_sync_words(F.d), st));
+		CDR_CUDA_TRY(cudaStreamSynchronize(st));
+		set_error(CDR_ERR_NUMERIC, "%u line-sweep CTAs and %u inverse-product CTAs gave up waiting for their rows",
 		          to_lines, to_inv);
 		return CDR_ERR_NUMERIC;
 	}

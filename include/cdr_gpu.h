@@ -99,15 +99,18 @@ long long cdr_gpu_launch_count(void);
 /* Launch shape the line-kernel autotuner chose for lines of length n, nlines
  * lines, direction dir (CDR_DIR_*), FP32 (fp32 = 1) or FP64 sweeps, nstencil 3
  * or 5, a single problem (batch = 0) or a batch (batch = 1): elements per
- * thread *K and the CTA size cap *cap (x-lines: the CTA size, at most 256;
- * 0: x-lines streamed through shared memory, CDR_LINES_STREAM).  Returns CDR_ERR_ARG when no solver of
- * this process has tuned that shape.  No counterpart in the reference. */
+ * thread *K and the CTA thread cap *cap (x-lines: the CTA size, at most 256,
+ * or 0: x-lines streamed through shared memory, CDR_LINES_STREAM; y-lines:
+ * lines per CTA = cap / threads per line, at most 4).  K is fixed by the line
+ * length (8 up to 2048 points, 16 up to 4096 for FP32), so every shape gives
+ * the same bits.  Returns CDR_ERR_ARG when no solver of this process has tuned
+ * that shape.  No counterpart in the reference. */
 int cdr_gpu_lines_shape(int dir, int fp32, int nstencil, int n, int nlines, int batch, int *K, int *cap);
-/* Pin the launch shape (K elements per thread: 4/8/16 FP32, 2/4/8 FP64; CTA
- * size cap 32..1024, x-lines at most 256; cap 0: streamed x-lines with K = 8
- * FP32 / 4 FP64) for that geometry in this process; solvers created afterwards
- * use it and the autotuner leaves it.  CDR_ERR_ARG if the shape cannot run
- * lines of length n.  No counterpart in the reference. */
+/* Pin the launch shape (K: the fixed one above; CTA thread cap 32..1024,
+ * x-lines at most 256; cap 0: streamed FP32 x-lines) for that geometry in this
+ * process; solvers created afterwards use it and the autotuner leaves it.
+ * CDR_ERR_ARG if the shape cannot run lines of length n.  No counterpart in
+ * the reference. */
 int cdr_gpu_lines_set_shape(int dir, int fp32, int nstencil, int n, int nlines, int batch, int K, int cap);
 
 /* ------------------------------------------------------------------------
@@ -184,13 +187,13 @@ int cdr_gpu_setup_lines_2d_f32(const double *so, int nstencil, float *sor, int n
  * the line kernel instead of timing the candidates at setup (the autotuner,
  * whose choice is kept for the process). */
 #define CDR_LINES_NOTUNE 2
-/* Kernel flags: x-lines of a single problem (32K <= nx <= 256K, K = 8 FP32 / 4
- * FP64) by the streamed kernel: persistent CTAs (two per SM) whose line rows
- * arrive in shared memory by bulk asynchronous copies; each CTA takes its
- * chunks into registers and requests the next line before running the scans.
- * Same arithmetic as the register-chunk kernel with the same K (bit-identical
- * results); the default for FP32 x-lines longer than 1024 points, an
- * autotuner candidate elsewhere. */
+/* Kernel flags: FP32 x-lines of a single problem (256 <= nx <= 2048) by the
+ * streamed kernel: persistent CTAs (two per SM) whose line rows arrive in
+ * shared memory by bulk asynchronous copies; each CTA takes its chunks into
+ * registers and requests the next line before running the scans.  Same
+ * arithmetic as the register-chunk kernel (bit-identical results); the default
+ * for FP32 x-lines longer than 1024 points, an autotuner candidate elsewhere
+ * (other lines take the register-chunk kernel). */
 #define CDR_LINES_STREAM 4
 /* Status of the streamed x-line kernel since the last call, read on stream s
  * (synchronises it): CDR_ERR_NUMERIC if a CTA gave up waiting for its staged
@@ -216,6 +219,24 @@ int cdr_gpu_relax_lines_2d_f64(const double *so, int nstencil, double *x, const 
 int cdr_gpu_relax_lines_2d_f32(const float *so, int nstencil, float *x, const float *b, const float *sor,
                                int nx, int ny, int pitch, int tpitch, int dir, int updown, int flags,
                                cudaStream_t stream);
+/* The same sweep with a caller-owned sync buffer (device, cdr_gpu_lines_sync_words(nx)
+ * unsigned words, zeroed before its first use; a sweep leaves it zeroed):
+ * y-lines (scan mode, 16-byte aligned rows and factor lines) then run both
+ * colours in one launch.  Blocks of column pairs draw their order from a
+ * ticket; each solves its first-colour lines, raises a flag, waits (bounded,
+ * as the streamed x-line kernel; a give-up is reported by
+ * cdr_gpu_lines_stream_status) for the flag of the block before it and solves
+ * its second-colour lines, so each coupling column is read from DRAM once per
+ * sweep.  The result is bit-identical to the two-launch sweep.  One buffer per
+ * stream: sweeps that run concurrently on one buffer race.  x-lines and the
+ * other cases run as cdr_gpu_relax_lines_2d_*.  No counterpart in the reference. */
+size_t cdr_gpu_lines_sync_words(int nx);
+int cdr_gpu_relax_lines_2d_sync_f64(const double *so, int nstencil, double *x, const double *b, const double *sor,
+                                    int nx, int ny, int pitch, int tpitch, int dir, int updown, int flags,
+                                    unsigned *sync, cudaStream_t stream);
+int cdr_gpu_relax_lines_2d_sync_f32(const float *so, int nstencil, float *x, const float *b, const float *sor,
+                                    int nx, int ny, int pitch, int tpitch, int dir, int updown, int flags,
+                                    unsigned *sync, cudaStream_t stream);
 
 /* b_coarse = P^T r_fine; replaces restriction::run (include/cedar/kernels/restrict.h:17-19)
  * -> BMG2_SymStd_restrict (src/2d/restrict.cc:14-29, src/2d/ftn/BMG2_SymStd_restrict.f90:72-92). */

@@ -308,9 +308,10 @@ def test_coarse_cholesky_bitwise(lib, oracle, n):
 
 
 def test_line_autotuner_records_shapes_and_keeps_results():
-    """The setup-time autotuner records a launch shape for every swept level; the
-    tuned FP32 solve converges like the default-shape one (same tolerance, at
-    most one cycle apart: the chunking changes FP32 rounding only)."""
+    """The setup-time autotuner records a launch shape for every swept level,
+    and the tuned FP32 solve is the default-shape one bit for bit: the chunks
+    of a line (K per thread) are fixed by its length and the scan's tree by the
+    chunk indices, so the shape changes only the timing."""
     import ctypes
     from cedar_b200 import _lib
     from cedar_b200 import problems as P
@@ -323,8 +324,8 @@ def test_line_autotuner_records_shapes_and_keeps_results():
     for tune in (True, False):
         s = Solver2D(so, Config({"solver": {"relaxation": "line-xy", "max-iter": 30, "tol": 1e-9},
                                  "gpu": {"precision": "fp32-ir", "autotune": tune}}))
-        s.solve(b)
-        res[tune] = (s.iters, s.history[-1])
+        x = s.solve(b)
+        res[tune] = (x, s.history.copy())
         if tune:
             for l in range(s.nlevels - 1):
                 _, nx, ny, *_ = s.level_info(l, "so")
@@ -332,12 +333,60 @@ def test_line_autotuner_records_shapes_and_keeps_results():
                     break  # fused coarse levels do not use the line kernels
                 for d, (nn, nl) in ((0, (nx, ny)), (1, (ny, nx))):
                     K, cap = ctypes.c_int(), ctypes.c_int()
-                    for first in (1,):
-                        rc = lib.cdr_gpu_lines_shape(d, 1, 5, nn, nl, 0, ctypes.byref(K), ctypes.byref(cap))
-                        assert rc == 0, (l, d)
-                        assert K.value in (4, 8, 16) and cap.value in (0, 32, 64, 128, 256, 512, 1024)
-    assert res[True][1] < 1e-9 and res[False][1] < 1e-9
-    assert abs(res[True][0] - res[False][0]) <= 1
+                    rc = lib.cdr_gpu_lines_shape(d, 1, 5, nn, nl, 0, ctypes.byref(K), ctypes.byref(cap))
+                    assert rc == 0, (l, d)
+                    assert K.value == 8 and cap.value in (0, 32, 64, 128, 256, 512, 1024)
+    assert res[True][1][-1] < 1e-9
+    np.testing.assert_array_equal(res[True][1], res[False][1])
+    np.testing.assert_array_equal(res[True][0], res[False][0])
+
+
+@pytest.mark.parametrize("precision", ["f32", "f64"])
+@pytest.mark.parametrize("n", [100, 383, 1024, 2047])
+def test_line_sweep_bits_independent_of_launch_shape(lib, oracle, precision, n):
+    """Every launch shape of the parallel line sweep gives the same bits: x-lines
+    in CTAs of 32 to 256 threads and (FP32, 256 to 2048 points) the streamed
+    kernel; y-lines with 1, 2, 4 or 8 lines per CTA."""
+    import torch
+    nl = 37
+    dt = torch.float64 if precision == "f64" else torch.float32
+    fn = lib.cdr_gpu_relax_lines_2d_f64 if precision == "f64" else lib.cdr_gpu_relax_lines_2d_f32
+    fp32 = 1 if precision == "f32" else 0
+    for direction, (nx, ny) in ((_lib.DIR_X, (n, nl)), (_lib.DIR_Y, (nl, n))):
+        # elements per thread: fixed by the line length (y-lines over 1024 points: 16)
+        K = 16 if direction == _lib.DIR_Y and n > 1024 else 8
+        tpl = 1
+        while tpl * K < n:
+            tpl *= 2
+        so, x, b = make_op(nx, ny, 5), grid(nx, ny, 8), grid(nx, ny, 9)
+        sor, _ = (oracle.setup_lines_x if direction == _lib.DIR_X else oracle.setup_lines_y)(so)
+        g = sor.copy()
+        if fp32:
+            g[0][1:-1, 1:-1] = 1.0 / sor[0][1:-1, 1:-1]
+        pitch = ((nx + 2 + 31) // 32) * 32
+        tpitch = ((ny + 2 + 31) // 32) * 32
+        dso, dbb = padded(so, pitch, dt), padded(b, pitch, dt)
+        dsor = padded(g, pitch if direction == _lib.DIR_X else tpitch, dt)
+        if direction == _lib.DIR_X:
+            caps = [32, 64, 128, 256] + ([0] if fp32 and 256 <= n <= 2048 else [])
+        else:
+            caps = sorted({max(32, tpl * gg) for gg in (1, 2, 4, 8) if tpl * gg <= (1024 if fp32 else 512)})
+        outs = []
+        for cap in caps:
+            _lib.check(lib.cdr_gpu_lines_set_shape(direction, fp32, 5, n, nl, 0, K, cap))
+            dx = padded(x, pitch, dt)
+            for updown in (0, 1):
+                _lib.check(fn(ptr(dso), 5, ptr(dx), ptr(dbb), ptr(dsor), nx, ny, pitch, tpitch, direction, updown, 0,
+                              stream()))
+            outs.append(host(dx))
+        assert lib.cdr_gpu_lines_stream_status(stream()) == 0
+        for cap, o in zip(caps[1:], outs[1:]):
+            np.testing.assert_array_equal(o, outs[0], err_msg="direction %d cap %d" % (direction, cap))
+        xr = x.copy()
+        ofn = oracle.relax_lines_x if direction == _lib.DIR_X else oracle.relax_lines_y
+        ofn(so, xr, b, sor, 0)
+        ofn(so, xr, b, sor, 1)
+        assert rel_err(outs[0][:, :nx + 2], xr) < (1e-12 if not fp32 else 2e-4)
 
 
 def test_pinned_line_shape_is_used(lib):
@@ -360,3 +409,46 @@ def test_pinned_line_shape_is_used(lib):
         K, cap = ctypes.c_int(), ctypes.c_int()
         _lib.check(lib.cdr_gpu_lines_shape(d, 1, 5, n, n, 0, ctypes.byref(K), ctypes.byref(cap)))
         assert (K.value, cap.value) == want
+
+
+@pytest.mark.parametrize("precision", ["f32", "f64"])
+@pytest.mark.parametrize("nx,ny,ns", [(37, 100, 5), (64, 383, 5), (255, 1024, 3), (96, 2047, 5), (2047, 2047, 5),
+                                      (9, 12, 5), (1, 40, 5)])
+def test_one_launch_y_sweep_equals_two_launches(lib, precision, nx, ny, ns):
+    """y-lines with a sync buffer sweep both colours in one launch (blocks of
+    column pairs, a flag between neighbouring blocks): bit-identical to the two
+    one-colour launches for every lines-per-CTA shape, both directions of
+    sweep; the buffer is left zeroed and no block gives up."""
+    import torch
+    dt = torch.float64 if precision == "f64" else torch.float32
+    fp32 = precision == "f32"
+    fn = lib.cdr_gpu_relax_lines_2d_f64 if not fp32 else lib.cdr_gpu_relax_lines_2d_f32
+    fns = lib.cdr_gpu_relax_lines_2d_sync_f64 if not fp32 else lib.cdr_gpu_relax_lines_2d_sync_f32
+    from oracle import oracle as O
+    so, x, b = make_op(nx, ny, ns), grid(nx, ny, 8), grid(nx, ny, 9)
+    sy, _ = O.setup_lines_y(so)
+    g = sy.copy()
+    if fp32:
+        g[0][1:-1, 1:-1] = 1.0 / sy[0][1:-1, 1:-1]
+    pitch = ((nx + 2 + 31) // 32) * 32
+    tpitch = ((ny + 2 + 31) // 32) * 32
+    dso, dbb, dsy = padded(so, pitch, dt), padded(b, pitch, dt), padded(g, tpitch, dt)
+    words = lib.cdr_gpu_lines_sync_words(nx)
+    sync = torch.zeros(words, dtype=torch.int32, device="cuda")
+    K = 16 if ny > 1024 else 8
+    tpl = 1
+    while tpl * K < ny:
+        tpl *= 2
+    caps = sorted({max(32, tpl * gg) for gg in (1, 2, 4, 8) if tpl * gg <= (1024 if fp32 else 512)})
+    for cap in caps:
+        _lib.check(lib.cdr_gpu_lines_set_shape(_lib.DIR_Y, 1 if fp32 else 0, ns, ny, nx, 0, K, cap))
+        for updown in (0, 1):
+            d1, d2 = padded(x, pitch, dt), padded(x, pitch, dt)
+            for _ in range(2):
+                _lib.check(fn(ptr(dso), ns, ptr(d1), ptr(dbb), ptr(dsy), nx, ny, pitch, tpitch, _lib.DIR_Y, updown, 0,
+                              stream()))
+                _lib.check(fns(ptr(dso), ns, ptr(d2), ptr(dbb), ptr(dsy), nx, ny, pitch, tpitch, _lib.DIR_Y, updown,
+                               0, ptr(sync), stream()))
+            np.testing.assert_array_equal(host(d2), host(d1), err_msg="cap %d updown %d" % (cap, updown))
+            assert int(sync.abs().sum().item()) == 0
+    assert lib.cdr_gpu_lines_stream_status(stream()) == 0
