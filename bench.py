@@ -84,9 +84,10 @@ def parse():
     ap.add_argument("--no-extras", action="store_true", help="skip the to_1e-10 and cpu_baseline legs")
     ap.add_argument("--no-autotune", action="store_true",
                     help="default line-kernel launch shapes instead of the setup-time autotuner's")
-    ap.add_argument("--profile", choices=["fcg", "vcycle"], default=None,
+    ap.add_argument("--profile", choices=["fcg", "vcycle", "3d"], default=None,
                     help="profiling driver (for ncu): set up the headline FP32 solver (fcg: six-level FCG; vcycle: "
-                         "the reference loop's 10-level V(2,1)) with graphs off (line shapes autotuned as in the "
+                         "the reference loop's 10-level V(2,1); 3d: the 3D FE problem at --n nodes per edge, "
+                         "FP64, point and plane-xyz relaxation) with graphs off (line shapes autotuned as in the "
                          "bench), run --steps iterations, print the launch counts (setup_launches: skip that many "
                          "with ncu -s to reach the solve), no timing")
     return ap.parse_args()
@@ -97,6 +98,8 @@ def profile_main(args):
     from cedar_b200 import _lib, problems as P
     from cedar_b200.config import Config
     from cedar_b200.solver import Solver2D
+    if args.profile == "3d":
+        return profile_3d(args)
     so, b = P.hetero_diffusion(args.n)
     if args.profile == "fcg":
         conf = {"solver": {"relaxation": "line-xy", "max-iter": args.steps, "tol": 1e-30, "num-levels": 6,
@@ -112,6 +115,30 @@ def profile_main(args):
     s.solve(b)
     print(json.dumps({"profile": args.profile, "levels": s.nlevels, "setup_launches": int(l0),
                       "solve_launches": int(lib.cdr_gpu_launch_count() - l0), "iterations": int(s.iters)}))
+
+
+def profile_3d(args):
+    """3D launch-list driver: the trilinear-FE problem of the 3D leg at --n nodes per
+    edge (host assembly), FP64 V(2,1), point relaxation then plane-xyz, --steps
+    cycles each, graphs off."""
+    from cedar_b200 import _lib, gallery as G, problems as P
+    from cedar_b200.config import Config
+    from cedar_b200.solver import Solver3D
+    lib = _lib.load()
+    n = args.n
+    so = G.fe3_hetero(P.hetero3_coefficients(n))
+    b = P.hetero3_rhs(n)
+    out = {"profile": "3d", "n": n}
+    for relax in ("point", "plane-xyz"):
+        l0 = lib.cdr_gpu_launch_count()
+        s = Solver3D(so, Config({"solver": {"relaxation": relax, "max-iter": args.steps, "tol": 1e-30},
+                                 "gpu": {"graph": False}}))
+        l1 = lib.cdr_gpu_launch_count()
+        s.solve(b)
+        out[relax] = {"levels": s.nlevels, "setup_launches": int(l1 - l0),
+                      "solve_launches": int(lib.cdr_gpu_launch_count() - l1)}
+        s.close()
+    print(json.dumps(out))
 
 
 def peaks():

@@ -360,3 +360,43 @@ def stencil3_to_csr(so):
         rows += [r1, r2]; cols += [r2, r1]; vals += [v, v]
     N = nx * ny * nz
     return sp.csr_matrix((np.concatenate(vals), (np.concatenate(rows), np.concatenate(cols))), shape=(N, N))
+
+
+def periodic_poisson(nx, ny, periodic=(True, False)):
+    """5-point Poisson on an nx x ny grid with periodic directions, as the
+    reference's periodic example builds it (examples/basic-2d-ser/periodic.cc:16-131):
+    a periodic direction has nx (ny) distinct points, h = 1/nx there, the
+    coupling to the ghost line enters the operator, and the ghost lines of the
+    operator and of b hold copies of the opposite interior lines.  Returns
+    (so, b, exact) with b = 8 pi^2 sin(2 pi x) sin(2 pi y) h^2 and
+    exact = sin(2 pi x) sin(2 pi y) at the interior points."""
+    px, py = bool(periodic[0]), bool(periodic[1])
+    l, m = nx, ny
+    so = np.zeros((3, ny + 2, nx + 2))
+    hx = 1.0 / ((nx - 1 if px else nx) + 1)
+    hy = 1.0 / ((ny - 1 if py else ny) + 1)
+    xh, yh = hy / hx, hx / hy
+    ibeg = 1 if px else 2
+    jbeg = 1 if py else 2
+    so[S, jbeg:m + 1, 1:l + 1] = 1.0 * yh
+    so[W, 1:m + 1, ibeg:l + 1] = 1.0 * xh
+    so[C, 1:m + 1, 1:l + 1] = 2 * xh + 2 * yh
+    if px:
+        so[:, 1:m + 1, 0] = so[:, 1:m + 1, l]
+        so[:, 1:m + 1, l + 1] = so[:, 1:m + 1, 1]
+    if py:
+        so[:, 0, 1:l + 1] = so[:, m, 1:l + 1]
+        so[:, m + 1, 1:l + 1] = so[:, 1, 1:l + 1]
+    x = np.arange(1, l + 1) * hx
+    y = np.arange(1, m + 1) * hy
+    b = np.zeros((ny + 2, nx + 2))
+    b[1:-1, 1:-1] = 8 * math.pi ** 2 * np.outer(np.sin(2 * math.pi * y), np.sin(2 * math.pi * x)) * (hx * hy)
+    if px:
+        b[:, 0] = b[:, l]
+        b[:, l + 1] = b[:, 1]
+    if py:
+        b[0, :] = b[m, :]
+        b[m + 1, :] = b[1, :]
+    exact = np.zeros_like(b)
+    exact[1:-1, 1:-1] = np.outer(np.sin(2 * math.pi * y), np.sin(2 * math.pi * x))
+    return so, b, exact

@@ -1008,7 +1008,10 @@ static void smooth(o2_solver *h, struct o2_level *L, int updown)
 	int n = updown == BMG_DOWN ? h->s.nrelax_pre : h->s.nrelax_post;
 	for (int it = 0; it < n; ++it) {
 		switch (h->s.relax) {
-		case O2_RELAX_POINT: o2_relax_gs(L->so, L->b, L->x, L->sor0, L->ii, L->jj, ifd, updown); break;
+		case O2_RELAX_POINT:
+			if (h->s.bc) o2_relax_gs_per(L->so, L->b, L->x, L->sor0, L->ii, L->jj, ifd, updown, h->s.bc);
+			else o2_relax_gs(L->so, L->b, L->x, L->sor0, L->ii, L->jj, ifd, updown);
+			break;
 		case O2_RELAX_LINE_X: o2_relax_lines_x(L->so, L->b, L->x, L->sor0, L->ii, L->jj, ifd, updown); break;
 		case O2_RELAX_LINE_Y: o2_relax_lines_y(L->so, L->b, L->x, L->sor0, L->ii, L->jj, ifd, updown); break;
 		case O2_RELAX_LINE_XY:
@@ -1044,17 +1047,25 @@ o2_solver *o2_create(const o2_settings *s, const double *so_fine, int nstncl, in
 	for (int l = 0; l < nl - 1; ++l) {
 		struct o2_level *F = &h->lv[l], *C = &h->lv[l + 1];
 		int ifd = F->nstncl == 3 ? 1 : 0;
-		o2_setup_interp(F->so, C->ci, F->ii, F->jj, C->ii, C->jj, ifd);
-		o2_setup_galerkin(F->so, C->so, C->ci, F->ii, F->jj, C->ii, C->jj, ifd);
+		if (h->s.bc) {
+			o2_setup_interp_per(F->so, C->ci, F->ii, F->jj, C->ii, C->jj, ifd, h->s.bc);
+			o2_setup_galerkin_per(F->so, C->so, C->ci, F->ii, F->jj, C->ii, C->jj, ifd, h->s.bc);
+		} else {
+			o2_setup_interp(F->so, C->ci, F->ii, F->jj, C->ii, C->jj, ifd);
+			o2_setup_galerkin(F->so, C->so, C->ci, F->ii, F->jj, C->ii, C->jj, ifd);
+		}
 		int r = setup_relax(h, F);
 		if (r && !h->setup_info) h->setup_info = r;
 	}
 	struct o2_level *Cg = &h->lv[nl - 1];
-	h->nabd1 = Cg->nx + 2;
+	/* periodic: a dense N x N factor (include/cedar/2d/solver.h:118-121) */
+	h->nabd1 = h->s.bc ? Cg->nx * Cg->ny : Cg->nx + 2;
 	h->nabd2 = Cg->nx * Cg->ny;
 	h->abd = zalloc((size_t)h->nabd1 * h->nabd2);
 	h->bbd = zalloc((size_t)h->nabd2);
-	h->cg_info = o2_setup_cg(Cg->so, Cg->ii, Cg->jj, Cg->nstncl, h->abd, h->nabd1);
+	if (h->s.bc) h->cg_info = o2_setup_cg_per(Cg->so, Cg->ii, Cg->jj, Cg->nstncl, h->abd, h->s.bc);
+	else h->cg_info = o2_setup_cg(Cg->so, Cg->ii, Cg->jj, Cg->nstncl, h->abd, h->nabd1);
+	if (h->s.bc && h->s.relax != O2_RELAX_POINT && !h->setup_info) h->setup_info = -1;
 	return h;
 }
 
@@ -1069,6 +1080,24 @@ void o2_destroy(o2_solver *h)
 	free(h->lv); free(h->abd); free(h->bbd); free(h);
 }
 
+static void coarse_solve(o2_solver *h, struct o2_level *C, double *x, const double *b)
+{
+	if (h->s.bc) o2_solve_cg_per(x, b, C->ii, C->jj, h->abd, h->bbd, h->s.bc);
+	else o2_solve_cg(x, b, C->ii, C->jj, h->abd, h->bbd, h->nabd1);
+}
+
+static void restrict_bc(o2_solver *h, struct o2_level *L, struct o2_level *C, const double *q)
+{
+	if (h->s.bc) o2_restrict_per(C->ci, (double *)q, C->b, L->ii, L->jj, C->ii, C->jj, h->s.bc);
+	else o2_restrict(C->ci, q, C->b, L->ii, L->jj, C->ii, C->jj);
+}
+
+static void interp_bc(o2_solver *h, struct o2_level *L, struct o2_level *C, double *x)
+{
+	if (h->s.bc) o2_interp_add_per(x, C->x, L->res, L->so, C->ci, C->ii, C->jj, L->ii, L->jj, h->s.bc);
+	else o2_interp_add(x, C->x, L->res, L->so, C->ci, C->ii, C->jj, L->ii, L->jj);
+}
+
 /* cycle::vcycle::ncycle_helper, include/cedar/cycle/vcycle.h:57-115 (n = 1) */
 static void ncycle(o2_solver *h, int l, double *x, const double *b)
 {
@@ -1077,13 +1106,13 @@ static void ncycle(o2_solver *h, int l, double *x, const double *b)
 	L->x = x; L->b = (double *)b;
 	smooth(h, L, BMG_DOWN);
 	o2_residual(L->so, L->b, L->x, L->res, L->ii, L->jj, L->nstncl == 3 ? 1 : 0);
-	o2_restrict(C->ci, L->res, C->b, L->ii, L->jj, C->ii, C->jj);
+	restrict_bc(h, L, C, L->res);
 	memset(C->x, 0, sizeof(double) * (size_t)C->ii * C->jj);
 	if (l + 1 == h->nlev - 1)
-		o2_solve_cg(C->x, C->b, C->ii, C->jj, h->abd, h->bbd, h->nabd1);
+		coarse_solve(h, C, C->x, C->b);
 	else
 		ncycle(h, l + 1, C->x, C->b);
-	o2_interp_add(L->x, C->x, L->res, L->so, C->ci, C->ii, C->jj, L->ii, L->jj);
+	interp_bc(h, L, C, L->x);
 	smooth(h, L, BMG_UP);
 	L->x = sx; L->b = sb;
 }
@@ -1091,8 +1120,7 @@ static void ncycle(o2_solver *h, int l, double *x, const double *b)
 void o2_vcycle(o2_solver *h, double *x, const double *b)
 {
 	if (h->nlev == 1) {
-		struct o2_level *L = &h->lv[0];
-		o2_solve_cg(x, b, L->ii, L->jj, h->abd, h->bbd, h->nabd1);
+		coarse_solve(h, &h->lv[0], x, b);
 	} else {
 		ncycle(h, 0, x, b);
 	}
@@ -1106,15 +1134,15 @@ static void fcycle(o2_solver *h, int l, double *x, const double *b)
 {
 	struct o2_level *L = &h->lv[l];
 	if (l == h->nlev - 1) {
-		o2_solve_cg(x, b, L->ii, L->jj, h->abd, h->bbd, h->nabd1);
+		coarse_solve(h, L, x, b);
 		return;
 	}
 	struct o2_level *C = &h->lv[l + 1];
-	o2_restrict(C->ci, b, C->b, L->ii, L->jj, C->ii, C->jj);
+	restrict_bc(h, L, C, b);
 	fcycle(h, l + 1, C->x, C->b);
 	memset(x, 0, sizeof(double) * (size_t)L->ii * L->jj);
 	memset(L->res, 0, sizeof(double) * (size_t)L->ii * L->jj);
-	o2_interp_add(x, C->x, L->res, L->so, C->ci, C->ii, C->jj, L->ii, L->jj);
+	interp_bc(h, L, C, x);
 	ncycle(h, l, x, b);
 }
 

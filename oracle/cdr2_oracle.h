@@ -22,6 +22,8 @@ typedef struct {
 	double tol;
 	int min_coarse;
 	int cycle; /* 0: V-cycle, 1: F-cycle (ml_settings::cycle_type) */
+	int bc;    /* boundary-condition code (BMG_get_bc of the periodic mask): 0 definite, 2 periodic x,
+	              1 periodic y, 3 both; periodic codes need point relaxation */
 } o2_settings;
 
 typedef struct o2_solver o2_solver;
@@ -59,6 +61,20 @@ int o2_solve(o2_solver *h, const double *b, double *x, double *hist, int maxhist
  * iterations and to confirm convergence); returns the iterations run. */
 int o2_solve_fcg(o2_solver *h, const double *b, double *x, int replace, double *hist, int maxhist);
 int o_num_threads(void);
+/* periodic branches (cdr2_periodic.c) */
+int o2_bc_code(int per_mask);
+void o2_relax_gs_per(const double *so, const double *qf, double *q, const double *sor, int II, int JJ, int ifd,
+                     int updown, int ipn);
+void o2_restrict_per(const double *ci, double *q, double *qc, int Nx, int Ny, int Nxc, int Nyc, int ipn);
+void o2_interp_add_per(double *q, const double *qc, double *res, const double *so_ko, const double *ci, int IIC,
+                       int JJC, int IIF, int JJF, int ipn);
+void o2_setup_galerkin_per(const double *so, double *soc, const double *ci, int IIF, int JJF, int IIC, int JJC,
+                           int ifd, int ipn);
+void o2_setup_interp_per(const double *so, double *ci, int IIF, int JJF, int IIC, int JJC, int ifd, int ipn);
+int o_dpotf2_u(int n, double *a, int lda);
+void o_dpotrs_u(int n, const double *a, int lda, double *b);
+int o2_setup_cg_per(const double *so, int II, int JJ, int nstncl, double *abd, int ipn);
+void o2_solve_cg_per(double *q, const double *qf, int II, int JJ, const double *abd, double *bbd, int ipn);
 void o_set_threads(int n);
 int o2_nlevels(const o2_solver *h);
 int o2_info(const o2_solver *h, int which);

@@ -1073,6 +1073,7 @@ static void plane_settings(o2_settings *s2)
 	s2->tol = 1e-8;
 	s2->min_coarse = 3;
 	s2->cycle = 0;
+	s2->bc = 0;
 }
 
 static void planes_setup(struct o3_level *L, int dir)

@@ -26,7 +26,7 @@ class Settings(ctypes.Structure):
     _fields_ = [("relax", ctypes.c_int), ("nrelax_pre", ctypes.c_int),
                 ("nrelax_post", ctypes.c_int), ("num_levels", ctypes.c_int),
                 ("maxiter", ctypes.c_int), ("tol", ctypes.c_double),
-                ("min_coarse", ctypes.c_int), ("cycle", ctypes.c_int)]
+                ("min_coarse", ctypes.c_int), ("cycle", ctypes.c_int), ("bc", ctypes.c_int)]
 
 
 def build():
@@ -71,6 +71,16 @@ def lib(variant=""):
             "o2_cycle": (None, [P, P, P]),
             "o2_solve": (I, [P, P, P, P, I]),
             "o2_solve_fcg": (I, [P, P, P, I, P, I]),
+            "o2_bc_code": (I, [I]),
+            "o2_relax_gs_per": (None, [P, P, P, P, I, I, I, I, I]),
+            "o2_restrict_per": (None, [P, P, P, I, I, I, I, I]),
+            "o2_interp_add_per": (None, [P, P, P, P, P, I, I, I, I, I]),
+            "o2_setup_interp_per": (None, [P, P, I, I, I, I, I, I]),
+            "o2_setup_galerkin_per": (None, [P, P, P, I, I, I, I, I, I]),
+            "o2_setup_cg_per": (I, [P, I, I, I, P, I]),
+            "o2_solve_cg_per": (None, [P, P, I, I, P, P, I]),
+            "o_dpotf2_u": (I, [I, P, I]),
+            "o_dpotrs_u": (None, [I, P, I, P]),
             "o_set_threads": (None, [I]),
             "o2_nlevels": (I, [P]),
             "o_num_threads": (I, []),
@@ -192,6 +202,68 @@ def solve_cg(abd, b):
     return x
 
 
+# ---- periodic branches (cdr2_periodic.c); ipn = o2_bc_code(mask): x -> 2, y -> 1, both -> 3
+def bc_code(periodic):
+    return lib().o2_bc_code((1 if periodic[0] else 0) | (2 if periodic[1] else 0))
+
+
+def relax_gs_per(so, x, b, sor, updown, ipn):
+    II, JJ = _dims(x)
+    lib().o2_relax_gs_per(_p(so), _p(b), _p(x), _p(sor), II, JJ, 1 if so.shape[0] == 3 else 0, updown, ipn)
+    return x
+
+
+def restrict_per(ci, r_fine, ipn):
+    """Restriction; the fine vector's ghosts are refreshed in place first (as the reference)."""
+    IIF, JJF = _dims(r_fine)
+    IIC, JJC = _dims(ci)
+    bc = np.zeros((JJC, IIC))
+    lib().o2_restrict_per(_p(ci), _p(r_fine), _p(bc), IIF, JJF, IIC, JJC, ipn)
+    return bc
+
+
+def interp_add_per(ci, xc, res, so_fine, x, ipn):
+    IIC, JJC = _dims(ci)
+    IIF, JJF = _dims(x)
+    ko = np.ascontiguousarray(so_fine[0])
+    lib().o2_interp_add_per(_p(x), _p(xc), _p(res), _p(ko), _p(ci), IIC, JJC, IIF, JJF, ipn)
+    return x
+
+
+def setup_interp_per(so_fine, nxc, nyc, ipn):
+    IIF, JJF = _dims(so_fine)
+    ci = np.zeros((8, nyc + 2, nxc + 2))
+    lib().o2_setup_interp_per(_p(so_fine), _p(ci), IIF, JJF, nxc + 2, nyc + 2, 1 if so_fine.shape[0] == 3 else 0,
+                              ipn)
+    return ci
+
+
+def galerkin_per(so_fine, ci, ipn):
+    IIF, JJF = _dims(so_fine)
+    IIC, JJC = _dims(ci)
+    soc = np.zeros((5, JJC, IIC))
+    lib().o2_setup_galerkin_per(_p(so_fine), _p(soc), _p(ci), IIF, JJF, IIC, JJC, 1 if so_fine.shape[0] == 3 else 0,
+                                ipn)
+    return soc
+
+
+def setup_cg_per(so, ipn):
+    """Dense upper Cholesky factor, column-major (N, N) with N = nx*ny (returned as its transpose in C order)."""
+    II, JJ = _dims(so)
+    n = (II - 2) * (JJ - 2)
+    abd = np.zeros((n, n))
+    info = lib().o2_setup_cg_per(_p(so), II, JJ, so.shape[0], _p(abd), ipn)
+    return abd, info
+
+
+def solve_cg_per(abd, b, ipn):
+    II, JJ = _dims(b)
+    x = np.zeros_like(b)
+    bbd = np.zeros((II - 2) * (JJ - 2))
+    lib().o2_solve_cg_per(_p(x), _p(b), II, JJ, _p(abd), _p(bbd), ipn)
+    return x
+
+
 def l2norm(r):
     II, JJ = _dims(r)
     return lib().o2_l2norm(_p(r), II, JJ)
@@ -250,13 +322,14 @@ class Solver:
     """Serial BoxMG solver: setup in the constructor, as ``cdr2::solver``."""
 
     def __init__(self, so, relax="point", nrelax_pre=2, nrelax_post=1, num_levels=-1,
-                 maxiter=10, tol=1e-8, min_coarse=3, variant="", cycle="v"):
+                 maxiter=10, tol=1e-8, min_coarse=3, variant="", cycle="v", periodic=(False, False)):
         self.L = lib(variant)
         so = np.ascontiguousarray(so, dtype=np.float64)
         self.nstncl = so.shape[0]
         self.ny, self.nx = so.shape[1] - 2, so.shape[2] - 2
+        mask = (1 if periodic[0] else 0) | (2 if periodic[1] else 0)
         self.settings = Settings(RELAX[relax], nrelax_pre, nrelax_post, num_levels, maxiter, tol, min_coarse,
-                                 {"v": 0, "f": 1}[cycle])
+                                 {"v": 0, "f": 1}[cycle], self.L.o2_bc_code(mask))
         self._so = so
         self.h = self.L.o2_create(ctypes.byref(self.settings), _p(so), self.nstncl, self.nx, self.ny)
 
