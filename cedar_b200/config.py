@@ -101,6 +101,14 @@ class MLSettings:
         self.coarse_solve = conf.get("gpu.coarse-solve", "banded")
         if self.coarse_solve not in ("banded", "inverse"):
             raise ValueError("invalid gpu.coarse-solve: %s" % self.coarse_solve)
+        # kernel_params::periodic from grid.periodic (src/kernel_params.cc:72-74)
+        pers = list(conf.get("grid.periodic", [False, False, False]))
+        self.periodic = tuple(bool(pers[i]) if i < len(pers) else False for i in range(3))
+
+    @property
+    def per_mask(self):
+        """kernel_params::per_mask: bit i set when direction i is periodic."""
+        return sum(1 << i for i, p in enumerate(self.periodic) if p)
 
     def __repr__(self):
         return ("MLSettings(relaxation=%r, cycle=%r, nrelax=(%d,%d), num_levels=%d, maxiter=%d, "

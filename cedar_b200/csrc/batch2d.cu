@@ -438,6 +438,10 @@ int cdr_gpu_batch2d_create(const cdr_gpu_settings *s, const double *so_dev, int 
 		set_error(CDR_ERR_ARG, "invalid precision %d", s->precision);
 		return CDR_ERR_ARG;
 	}
+	if (s->periodic) {
+		set_error(CDR_ERR_UNSUPPORTED, "batched solves: periodic boundaries are implemented for single problems");
+		return CDR_ERR_UNSUPPORTED;
+	}
 	if (s->krylov != CDR_KRYLOV_NONE || s->coarse_solve != CDR_COARSE_BANDED || s->fp32_levels != 0 ||
 	    s->cycle != CDR_CYCLE_V) {
 		set_error(CDR_ERR_UNSUPPORTED, "batched 2D solves: the Krylov outer iteration is implemented for the 2D solver only");

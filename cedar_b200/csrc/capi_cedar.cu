@@ -298,6 +298,13 @@ int settings_from(const Json &c, int nd, cdr_gpu_settings *s)
 	s->krylov_replace = (int)num("gpu.fcg-replace", 1);
 	if (nd == 3 && (s->krylov != CDR_KRYLOV_NONE || s->coarse_solve != CDR_COARSE_BANDED || s->fp32_levels))
 		return CEDAR_ERR_CONFIG;
+	// kernel_params::periodic from grid.periodic (src/kernel_params.cc:72-74)
+	if (const Json *pv = json_get(c, "grid.periodic")) {
+		if (pv->kind != Json::ARR) return CEDAR_ERR_CONFIG;
+		for (size_t i = 0; i < pv->arr.size() && i < 3; ++i)
+			if (pv->arr[i].kind == Json::BOOL && pv->arr[i].b) s->periodic |= 1 << i;
+		if (s->periodic >> nd) return CEDAR_ERR_CONFIG;
+	}
 	return CEDAR_SUCCESS;
 }
 

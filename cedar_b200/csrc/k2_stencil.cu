@@ -9,6 +9,7 @@
 #include <type_traits>
 
 #include "k2_point.cuh"
+#include "kernels2d.cuh"
 
 namespace cdrgpu {
 
@@ -270,11 +271,18 @@ __global__ void __launch_bounds__(TX *TY) k_gs_colour(const T *__restrict__ so, 
 	gs_at<T, NS>(so, ps, q, qf, sor, d.at(i, j), pitch);
 }
 
+// Periodic branch (BMG2_SymStd_relax_GS.f90:139-226): the reference copies a
+// row's x ghosts after the row's points of a colour and the y ghost rows after
+// the whole sweep.  Points of a colour never read another row's x ghosts that
+// the same colour changes (five-point: no diagonal couplings; nine-point: the
+// rows of one colour are two apart), so one copy launch after each colour
+// launch gives the same values.
 template <typename T>
 int relax_point_2d(const T *so, int nstencil, T *x, const T *b, const T *sor, Dims2 d, int updown,
-                   cudaStream_t st)
+                   cudaStream_t st, int per)
 {
 	dim3 blk(TX, TY);
+	const bool perx = per & 1, pery = (per >> 1) & 1;
 	if (nstencil == 5) {
 		// DOWN: (JBEG, IBEG) = (2,2),(2,3),(3,2),(3,3) with JBEG outer; UP reversed.
 		// Fortran index 2 is 0-based 1 (odd), 3 is 0-based 2 (even).
@@ -284,6 +292,7 @@ int relax_point_2d(const T *so, int nstencil, T *x, const T *b, const T *sor, Di
 			int o = updown == CDR_DOWN ? c : 3 - c;
 			k_gs_colour<T, 5><<<grd, blk, 0, st>>>(so, x, b, sor, d, order[o][1], order[o][0]);
 			CDR_LAUNCH_CHECK();
+			if (perx) CDR_TRY(ghost_copy_2d<T>(x, d, 1, 1, 0, order[o][0], st));
 		}
 	} else {
 		// DOWN: JO = 2 then 3; a point is swept in pass JO when (I + J + JO) is even,
@@ -293,14 +302,16 @@ int relax_point_2d(const T *so, int nstencil, T *x, const T *b, const T *sor, Di
 			int par = updown == CDR_DOWN ? c : 1 - c;
 			k_gs_colour<T, 3><<<grd, blk, 0, st>>>(so, x, b, sor, d, par, 0);
 			CDR_LAUNCH_CHECK();
+			if (perx) CDR_TRY(ghost_copy_2d<T>(x, d, 1, 1, 0, -1, st));
 		}
 	}
+	if (pery) CDR_TRY(ghost_copy_2d<T>(x, d, 1, 0, 1, -1, st));
 	return CDR_OK;
 }
 template int relax_point_2d<double>(const double *, int, double *, const double *, const double *, Dims2, int,
-                                    cudaStream_t);
+                                    cudaStream_t, int);
 template int relax_point_2d<float>(const float *, int, float *, const float *, const float *, Dims2, int,
-                                   cudaStream_t);
+                                   cudaStream_t, int);
 
 // ---------------------------------------------------------------- restriction
 // BMG2_SymStd_restrict (src/2d/ftn/BMG2_SymStd_restrict.f90:72-92): coarse

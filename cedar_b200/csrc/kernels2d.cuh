@@ -9,8 +9,10 @@ int residual_2d(const T *so, int nstencil, const T *x, const T *b, T *r, Dims2 d
                 double *partial, cudaStream_t st);
 template <typename T>
 int setup_recip_2d(const T *so, T *sor, Dims2 d, cudaStream_t st, int nstencil = 5);
+// per: periodic directions (bit 0 x, bit 1 y; single problems only)
 template <typename T>
-int relax_point_2d(const T *so, int nstencil, T *x, const T *b, const T *sor, Dims2 d, int updown, cudaStream_t st);
+int relax_point_2d(const T *so, int nstencil, T *x, const T *b, const T *sor, Dims2 d, int updown, cudaStream_t st,
+                   int per = 0);
 template <typename TS>
 int setup_lines_2d(const double *so, int nstencil, TS *sor, Dims2 d, int tpitch, int dir, int *info, cudaStream_t st);
 int lines_prepare();
@@ -60,6 +62,15 @@ int restrict_2d_mixed(const double *ci, const float *rf, double *bc, Dims2 f, Di
 int interp_add_2d_mixed(const double *ci, const double *xc, const float *rf, const float *sof, float *xf, Dims2 f,
                         Dims2 c, cudaStream_t st, int nsf_fine = 5);
 int setup_interp_2d(const double *so, int nstencil, double *ci, Dims2 f, Dims2 c, cudaStream_t st);
+// Periodic boundary conditions (k2_periodic.cu); per: bit 0 x, bit 1 y.
+// Ghost-line copies of `planes` planes: xmode 1 x ghosts of interior rows (of
+// parity jpar when jpar >= 0), 2 of all rows; ymode 1 the y ghost rows.
+template <typename T>
+int ghost_copy_2d(T *q, Dims2 d, int planes, int xmode, int ymode, int jpar, cudaStream_t st);
+int setup_interp_per_2d(const double *so, int nstencil, double *ci, Dims2 f, Dims2 c, int per, cudaStream_t st);
+// dense N x N factor (N = nx*ny) of the coarsest operator; info as setup_cg_2d
+int setup_cg_per_2d(const double *so, int nstencil, Dims2 d, double *abd, int *info, int per, cudaStream_t st);
+int solve_cg_per_2d(const double *abd, double *x, const double *b, Dims2 d, int per, cudaStream_t st);
 int galerkin_2d(const double *so, int nstencil, const double *ci, double *soc, Dims2 f, Dims2 c, cudaStream_t st);
 int setup_cg_2d(const double *so, int nstencil, Dims2 d, double *abd, int *info, cudaStream_t st);
 template <typename T>

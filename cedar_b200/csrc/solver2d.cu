@@ -67,6 +67,7 @@ struct cdr_gpu_solver {
 	cudaStream_t st = nullptr;
 	bool own_stream = false;
 	int lc[2] = {-1, -1};  // first level of the fused coarse cycle, [0] FP64, [1] FP32 (-1: none)
+	int per = 0;           // periodic directions (settings.periodic): bit 0 x, bit 1 y
 	cudaGraphExec_t gexec[2] = {nullptr, nullptr};  // cycle graphs: [0] FP64, [1] FP32
 	long long glaunches[2] = {0, 0};                 // kernel launches per replay
 	cudaEvent_t ev0 = nullptr, ev1 = nullptr;
@@ -106,6 +107,10 @@ struct cdr_gpu_solver {
 	int coarse_solve(T *x, const T *b);
 	template <typename T>
 	int fcycle(int l, T *x, const T *b);
+	template <typename T>
+	int restrict_to(int l, T *rf);
+	template <typename T>
+	int interp_from(int l, T *x);
 	int run_cycle(int prec);
 	template <typename T>
 	int fcg_iteration(bool formed);
@@ -146,7 +151,7 @@ int cdr_gpu_solver::smooth(int l, T *x, const T *b, int updown)
 	const T *so = Arr<T>::so(L), *sor = Arr<T>::sor(L), *sory = Arr<T>::sory(L);
 	for (int it = 0; it < n; ++it) {
 		switch (s.relaxation) {
-		case CDR_RELAX_POINT: CDR_TRY(relax_point_2d<T>(so, L.ns, x, b, sor, L.d, updown, st)); break;
+		case CDR_RELAX_POINT: CDR_TRY(relax_point_2d<T>(so, L.ns, x, b, sor, L.d, updown, st, per)); break;
 		case CDR_RELAX_LINE_X:
 			CDR_TRY(relax_lines_2d<T>(so, L.ns, x, b, sor, L.d, L.tpitch, CDR_DIR_X, updown, lflags<T>(), st));
 			break;
@@ -188,13 +193,39 @@ int cdr_gpu_solver::ncycle(int l, T *x, const T *b)
 			return smooth<T>(l, x, b, CDR_UP);
 		}
 	}
-	CDR_TRY(restrict_2d<T>(Arr<T>::ci(C), Arr<T>::r(F), Arr<T>::b(C), F.d, C.d, st));
+	CDR_TRY(restrict_to<T>(l, Arr<T>::r(F)));
 	CDR_CUDA_TRY(cudaMemsetAsync(Arr<T>::x(C), 0, sizeof(T) * C.d.plane(), st));
 	if (l + 1 == L() - 1) CDR_TRY(coarse_solve<T>(Arr<T>::x(C), Arr<T>::b(C)));
 	else if (l + 1 == lc[sizeof(T) == 4]) CDR_TRY(fused<T>(l + 1));
 	else CDR_TRY(ncycle<T>(l + 1, Arr<T>::x(C), Arr<T>::b(C)));
-	CDR_TRY(interp_add_2d<T>(Arr<T>::ci(C), Arr<T>::x(C), Arr<T>::r(F), Arr<T>::so(F), x, F.d, C.d, st));
+	CDR_TRY(interp_from<T>(l, x));
 	CDR_TRY(smooth<T>(l, x, b, CDR_UP));
+	return CDR_OK;
+}
+
+// Restriction of a level-l grid function to level l+1's right-hand side.  The
+// periodic branch (BMG2_SymStd_restrict.f90:94-130) first refreshes, in place,
+// the ghost lines of each periodic direction whose fine size is even (the
+// coarse grid then has Nf/2 + 1 points with its ghosts).
+template <typename T>
+int cdr_gpu_solver::restrict_to(int l, T *rf)
+{
+	Level &F = lv[l], &C = lv[l + 1];
+	if (per) {
+		const int xm = (per & 1) && F.nx % 2 == 0 ? 2 : 0, ym = (per & 2) && F.ny % 2 == 0 ? 1 : 0;
+		CDR_TRY(ghost_copy_2d<T>(rf, F.d, 1, xm, ym, -1, st));
+	}
+	return restrict_2d<T>(Arr<T>::ci(C), rf, Arr<T>::b(C), F.d, C.d, st);
+}
+
+// x(l) += P x(l+1), then (periodic, BMG2_SymStd_interp_add.f90:139-156) the
+// fine ghost lines.
+template <typename T>
+int cdr_gpu_solver::interp_from(int l, T *x)
+{
+	Level &F = lv[l], &C = lv[l + 1];
+	CDR_TRY(interp_add_2d<T>(Arr<T>::ci(C), Arr<T>::x(C), Arr<T>::r(F), Arr<T>::so(F), x, F.d, C.d, st, F.ns));
+	if (per) CDR_TRY(ghost_copy_2d<T>(x, F.d, 1, per & 1 ? 2 : 0, per & 2 ? 1 : 0, -1, st));
 	return CDR_OK;
 }
 
@@ -258,6 +289,11 @@ template <typename T>
 int cdr_gpu_solver::coarse_solve(T *x, const T *b)
 {
 	const Dims2 d = lv.back().d;
+	if (per) {
+		if constexpr (sizeof(T) == 8) return solve_cg_per_2d(abd, x, b, d, per, st);
+		set_error(CDR_ERR_UNSUPPORTED, "periodic coarse solve in FP32");
+		return CDR_ERR_UNSUPPORTED;
+	}
 	if (s.coarse_solve == CDR_COARSE_INVERSE) {
 		if constexpr (sizeof(T) == 4) return solve_cg_inv_2d<float>(ainv32, x, b, d, st);
 		else return solve_cg_inv_2d<double>(ainv, x, b, d, st);
@@ -271,11 +307,14 @@ int cdr_gpu_solver::fcycle(int l, T *x, const T *b)
 {
 	if (l == L() - 1) return coarse_solve<T>(x, b);
 	Level &F = lv[l], &C = lv[l + 1];
-	CDR_TRY(restrict_2d<T>(Arr<T>::ci(C), b, Arr<T>::b(C), F.d, C.d, st));
+	// b is a level array (the solver's copy of the caller's right-hand side on
+	// level 0): the periodic restriction refreshes its ghosts in place, as the
+	// reference does
+	CDR_TRY(restrict_to<T>(l, const_cast<T *>(b)));
 	CDR_TRY(fcycle<T>(l + 1, Arr<T>::x(C), Arr<T>::b(C)));
 	CDR_CUDA_TRY(cudaMemsetAsync(x, 0, sizeof(T) * F.d.plane(), st));
 	CDR_CUDA_TRY(cudaMemsetAsync(Arr<T>::r(F), 0, sizeof(T) * F.d.plane(), st));
-	CDR_TRY(interp_add_2d<T>(Arr<T>::ci(C), Arr<T>::x(C), Arr<T>::r(F), Arr<T>::so(F), x, F.d, C.d, st, F.ns));
+	CDR_TRY(interp_from<T>(l, x));
 	return ncycle<T>(l, x, b);
 }
 
@@ -392,8 +431,17 @@ int cdr_gpu_solver::setup()
 {
 	for (int l = 0; l + 1 < L(); ++l) {
 		Level &F = lv[l], &C = lv[l + 1];
-		CDR_TRY(setup_interp_2d(F.so, F.ns, C.ci, F.d, C.d, st));
-		CDR_TRY(galerkin_2d(F.so, F.ns, C.ci, C.so, F.d, C.d, st));
+		if (per) {
+			// periodic branches: the interpolation's own walk, then the definite
+			// product and the coarse operator's ghost lines
+			// (BMG2_SymStd_SETUP_ITLI_ex.f90:216-247, 333-363)
+			CDR_TRY(setup_interp_per_2d(F.so, F.ns, C.ci, F.d, C.d, per, st));
+			CDR_TRY(galerkin_2d(F.so, F.ns, C.ci, C.so, F.d, C.d, st));
+			CDR_TRY(ghost_copy_2d<double>(C.so, C.d, 5, per & 1 ? 2 : 0, per & 2 ? 1 : 0, -1, st));
+		} else {
+			CDR_TRY(setup_interp_2d(F.so, F.ns, C.ci, F.d, C.d, st));
+			CDR_TRY(galerkin_2d(F.so, F.ns, C.ci, C.so, F.d, C.d, st));
+		}
 		// smoother setup (multilevel::setup_relax_helper, multilevel.h:134-158)
 		switch (s.relaxation) {
 		case CDR_RELAX_POINT: CDR_TRY(setup_recip_2d<double>(F.so, F.sor, F.d, st)); break;
@@ -410,7 +458,8 @@ int cdr_gpu_solver::setup()
 		}
 	}
 	Level &Cg = lv[L() - 1];
-	CDR_TRY(setup_cg_2d(Cg.so, Cg.ns, Cg.d, abd, info + 1, st));
+	if (per) CDR_TRY(setup_cg_per_2d(Cg.so, Cg.ns, Cg.d, abd, info + 1, per, st));
+	else CDR_TRY(setup_cg_2d(Cg.so, Cg.ns, Cg.d, abd, info + 1, st));
 	if (s.coarse_solve == CDR_COARSE_INVERSE) {
 		CDR_TRY(cg_inverse_2d(abd, Cg.d, ainv, st));
 		if (mixed()) CDR_TRY(convert_f64_f32(ainv, ainv32, (size_t)Cg.nx * Cg.ny * Cg.nx * Cg.ny, st));
@@ -485,6 +534,7 @@ int cdr_gpu_settings_default(cdr_gpu_settings *s)
 	s->fp32_levels = 0;
 	s->cycle = CDR_CYCLE_V;
 	s->krylov_replace = 1;
+	s->periodic = 0;
 	return CDR_OK;
 }
 
@@ -572,14 +622,19 @@ static int create_impl(cdr_gpu_solver *h, const double *so_src, int ns, int nx, 
 	}
 	// the fused coarse cycle takes over from the first level that fits (not the
 	// fine level, whose arrays the caller may pass), when it spans two levels or more
-	h->lc[0] = pick_fused_level<double>(h->lv, s);
-	h->lc[1] = pick_fused_level<float>(h->lv, s);
+	h->per = s.periodic;
+	// the fused coarse cycle has no periodic branches
+	h->lc[0] = h->per ? -1 : pick_fused_level<double>(h->lv, s);
+	h->lc[1] = h->per ? -1 : pick_fused_level<float>(h->lv, s);
 	Level &Cg = h->lv[nl - 1];
 	if ((size_t)Cg.nx * Cg.ny > 4096) {
-		set_error(CDR_ERR_DIM, "coarsest grid %dx%d too large for the banded Cholesky", Cg.nx, Cg.ny);
+		set_error(CDR_ERR_DIM, "coarsest grid %dx%d too large for the %s Cholesky", Cg.nx, Cg.ny,
+		          h->per ? "dense" : "banded");
 		return CDR_ERR_DIM;
 	}
-	CDR_TRY(h->alloc(&h->abd, (size_t)(Cg.nx + 2) * Cg.nx * Cg.ny));
+	// periodic: a dense N x N factor (include/cedar/2d/solver.h:118-121)
+	const size_t ncg = (size_t)Cg.nx * Cg.ny;
+	CDR_TRY(h->alloc(&h->abd, h->per ? ncg * ncg : (size_t)(Cg.nx + 2) * ncg));
 	if (s.coarse_solve == CDR_COARSE_INVERSE) {
 		const size_t nn = (size_t)Cg.nx * Cg.ny * Cg.nx * Cg.ny;
 		CDR_TRY(h->alloc(&h->ainv, nn));
@@ -637,6 +692,15 @@ static int create_any(const cdr_gpu_settings *s, const double *so_src, int ns, i
 	if (s->krylov_replace < 0) {
 		set_error(CDR_ERR_ARG, "invalid krylov_replace %d", s->krylov_replace);
 		return CDR_ERR_ARG;
+	}
+	if (s->periodic & ~3) {
+		set_error(CDR_ERR_ARG, "invalid periodic mask %d (bit 0 x, bit 1 y)", s->periodic);
+		return CDR_ERR_ARG;
+	}
+	if (s->periodic && (s->relaxation != CDR_RELAX_POINT || s->precision != CDR_PREC_F64 ||
+	                    s->krylov != CDR_KRYLOV_NONE || s->coarse_solve != CDR_COARSE_BANDED)) {
+		set_error(CDR_ERR_UNSUPPORTED, "periodic boundaries: FP64 point relaxation and the direct coarse solve only");
+		return CDR_ERR_UNSUPPORTED;
 	}
 	*out = nullptr;
 	cdr_gpu_solver *h = new cdr_gpu_solver();

@@ -451,6 +451,10 @@ static int create3_any(const cdr_gpu_settings *s, const double *so_src, int src_
 		set_error(CDR_ERR_UNSUPPORTED, "3D solver: the Krylov outer iteration is implemented for the 2D solver only");
 		return CDR_ERR_UNSUPPORTED;
 	}
+	if (s->periodic) {
+		set_error(CDR_ERR_UNSUPPORTED, "3D solver: periodic boundaries are implemented for the 2D solver only");
+		return CDR_ERR_UNSUPPORTED;
+	}
 	cdr_gpu_solver3 *h = new cdr_gpu_solver3();
 	h->s = *s;
 	if (stream) h->st = stream;

@@ -54,6 +54,9 @@ def _settings(ms: MLSettings, dim=2):
     s.fp32_levels = ms.fp32_levels
     s.cycle = 1 if ms.cycle == "f" else 0
     s.krylov_replace = ms.fcg_replace
+    if dim == 2 and ms.periodic[2]:
+        raise ValueError("grid.periodic: a 2D grid has no z direction")
+    s.periodic = ms.per_mask
     return s
 
 

@@ -331,6 +331,10 @@ typedef struct cdr_gpu_settings {
 	int krylov_replace; /* CDR_KRYLOV_FCG: form the residual as b - A x every this many iterations and to
 	                       confirm convergence, the iterations between update it as r - alpha A p (one pass
 	                       over the operator fewer); 0 or 1 (default): every iteration */
+	int periodic;     /* "grid.periodic" as a mask: bit 0 x, bit 1 y (default 0).  2D solver with FP64
+	                     point relaxation (V or F cycle) and the direct coarse solve; the operator and b
+	                     hold the wrap-around couplings and copies of the opposite interior lines in
+	                     their ghost lines (examples/basic-2d-ser/periodic.cc) */
 } cdr_gpu_settings;
 
 typedef struct cdr_gpu_solver cdr_gpu_solver;

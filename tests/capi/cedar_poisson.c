@@ -2,8 +2,9 @@
  * libcdrgpu.so: 2D five- or nine-point Poisson entered vertex by vertex with
  * cedar_mat_set2d, a solve with cedar_solver_run and the residual by
  * cedar_matvec.  Usage: cedar_poisson config.json n stencil(5|9) out.bin
- * Writes the solution (ghost-inclusive, (n+2)^2 doubles) to out.bin and prints
- * the relative residual. */
+ * Writes the solution and then the right-hand side it solved with (each
+ * ghost-inclusive, (n+2)^2 doubles) to out.bin and prints the relative
+ * residual. */
 #include <math.h>
 #include <stdio.h>
 #include <stdlib.h>
@@ -82,6 +83,7 @@ int main(int argc, char **argv)
 	FILE *f = fopen(argv[4], "wb");
 	if (!f) return 4;
 	fwrite(xb, sizeof(double), (size_t)ilen * jlen, f);
+	fwrite(bb, sizeof(double), (size_t)ilen * jlen, f);
 	fclose(f);
 	CHECK(cedar_solver_destroy(&slv));
 	CHECK(cedar_vec_free(&x));

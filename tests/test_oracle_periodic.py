@@ -117,6 +117,36 @@ def test_periodic_galerkin_is_ptap_and_restriction_is_pt(oracle, per, n, ns):
 
 
 @pytest.mark.parametrize("per", PERS)
+@pytest.mark.parametrize("n,ns", [(19, 3), (21, 5), (37, 5)])
+def test_odd_periodic_galerkin_off_the_seam(oracle, per, n, ns):
+    """Odd periodic sizes: the last and first coarse points are fine
+    neighbours across the seam, yet the reference's product is the definite
+    loop plus ghost copies (src/2d/ftn/BMG2_SymStd_SETUP_ITLI_ex.f90:216-247),
+    which treats the fine ghost line (a copy of a coarse point) as a fine
+    point between them.  So the coarse operator equals P^T A P everywhere
+    except in the couplings of the two coarse lines at the seam, and differs
+    there -- the reference's own behaviour, restated."""
+    so = periodic_op(n, ns, per, seed=n)
+    ipn = oracle.bc_code(per)
+    nxc = (n - 1) // 2 + 1
+    ci = oracle.setup_interp_per(so, nxc, nxc, ipn)
+    soc = oracle.galerkin_per(so, ci, ipn)
+    Pm = prolongation(oracle, ci, so, n, nxc, per, ipn)
+    Ac = Pm.T @ assemble(so, per) @ Pm
+    G = assemble(soc, per)
+    ic, jc = np.meshgrid(np.arange(1, nxc + 1), np.arange(1, nxc + 1))
+    seam = np.zeros((nxc, nxc), bool)
+    if per[0]:
+        seam |= (ic == 1) | (ic == nxc)
+    if per[1]:
+        seam |= (jc == 1) | (jc == nxc)
+    off = ~seam.ravel()
+    blk = np.ix_(off, off)
+    assert np.abs(Ac[blk] - G[blk]).max() <= 1e-13 * np.abs(Ac).max()
+    assert np.abs(Ac - G).max() > 1e-2 * np.abs(Ac).max()
+
+
+@pytest.mark.parametrize("per", PERS)
 @pytest.mark.parametrize("ns", [3, 5])
 def test_periodic_gauss_seidel_sweep(oracle, per, ns):
     """One sweep of the periodic branch = the reference's sequential loops
