@@ -40,7 +40,8 @@ class Settings(ctypes.Structure):
                 ("min_coarse", ctypes.c_int), ("precision", ctypes.c_int),
                 ("use_graph", ctypes.c_int), ("line_flags", ctypes.c_int), ("fuse_coarse", ctypes.c_int),
                 ("krylov", ctypes.c_int), ("coarse_solve", ctypes.c_int), ("fp32_levels", ctypes.c_int),
-                ("cycle", ctypes.c_int), ("krylov_replace", ctypes.c_int), ("periodic", ctypes.c_int)]
+                ("cycle", ctypes.c_int), ("krylov_replace", ctypes.c_int), ("periodic", ctypes.c_int),
+                ("fp64_fine_iterate", ctypes.c_int)]
 
 
 def header_symbols():

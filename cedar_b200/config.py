@@ -18,7 +18,10 @@ reference's outer loop, the default; "fcg": the cycle preconditions flexible con
 between; 1, the default: every iteration),
 ``coarse-solve`` ("banded": the reference's DPBTRS, the default; "inverse": the setup forms the coarsest
 operator's inverse and every cycle multiplies by it, 2D only — for a coarsest level of thousands of unknowns)
-and ``fp32-levels`` (the FP32 cycle keeps this many finest levels in FP32, the rest in FP64; 0 = all, 2D only).
+``fp32-levels`` (the FP32 cycle keeps this many finest levels in FP32, the rest in FP64; 0 = all, 2D only)
+and ``fine-iterate`` ("fp64", the default: with "fcg" and line relaxation the FP32 cycle keeps the fine level's
+iterate in FP64 from the interpolate-add on, FP64 arithmetic over its FP32 operator data, so that the
+preconditioner's output carries no FP32 rounding of the iterate; "fp32": FP32 throughout).
 """
 import json
 import os
@@ -98,6 +101,9 @@ class MLSettings:
         self.fcg_replace = int(conf.get("gpu.fcg-replace", 1))
         if self.fcg_replace < 0:
             raise ValueError("invalid gpu.fcg-replace: %d" % self.fcg_replace)
+        self.fine_iterate = conf.get("gpu.fine-iterate", "fp64")
+        if self.fine_iterate not in ("fp64", "fp32"):
+            raise ValueError("invalid gpu.fine-iterate: %s" % self.fine_iterate)
         self.coarse_solve = conf.get("gpu.coarse-solve", "banded")
         if self.coarse_solve not in ("banded", "inverse"):
             raise ValueError("invalid gpu.coarse-solve: %s" % self.coarse_solve)

@@ -296,6 +296,9 @@ int settings_from(const Json &c, int nd, cdr_gpu_settings *s)
 	s->coarse_solve = cs == "inverse" ? CDR_COARSE_INVERSE : CDR_COARSE_BANDED;
 	s->fp32_levels = (int)num("gpu.fp32-levels", 0);
 	s->krylov_replace = (int)num("gpu.fcg-replace", 1);
+	const std::string fi = str("gpu.fine-iterate", "fp64");
+	if (fi != "fp64" && fi != "fp32") return CEDAR_ERR_CONFIG;
+	s->fp64_fine_iterate = fi == "fp64" ? 1 : 0;
 	if (nd == 3 && (s->krylov != CDR_KRYLOV_NONE || s->coarse_solve != CDR_COARSE_BANDED || s->fp32_levels))
 		return CEDAR_ERR_CONFIG;
 	// kernel_params::periodic from grid.periodic (src/kernel_params.cc:72-74)

@@ -220,6 +220,33 @@ RESTRICT_IMPL(float, f32)
 INTERP_IMPL(double, f64)
 INTERP_IMPL(float, f32)
 
+int cdr_gpu_rowsum_excess_2d(const double *so, int ns, float *dg, int nx, int ny, int pitch, cudaStream_t s)
+{
+	CDR_TRY(check_grid(nx, ny, pitch));
+	CDR_TRY(check_ns(ns));
+	CDR_NONNULL(so); CDR_NONNULL(dg);
+	return rowsum_excess_2d(so, ns, dg, Dims2{nx, ny, pitch}, s);
+}
+
+int cdr_gpu_residual_2d_wide(const float *so, const float *dg, int ns, const double *x, const float *b, float *r,
+                             float *zero, int nx, int ny, int pitch, cudaStream_t s)
+{
+	CDR_TRY(check_grid(nx, ny, pitch));
+	CDR_TRY(check_ns(ns));
+	CDR_NONNULL(so); CDR_NONNULL(dg); CDR_NONNULL(x); CDR_NONNULL(b); CDR_NONNULL(r); CDR_NONNULL(zero);
+	return residual_2d_wide(so, dg, ns, x, b, r, zero, Dims2{nx, ny, pitch}, s);
+}
+
+int cdr_gpu_interp_add_2d_wide(const float *ci, const float *xc, const float *rf, const float *sof, int nsf,
+                               const float *xin, double *xout, int nxf, int nyf, int pf, int nxc, int nyc, int pc,
+                               cudaStream_t s)
+{
+	CDR_TRY(check_pair(nxf, nyf, pf, nxc, nyc, pc));
+	CDR_TRY(check_ns(nsf));
+	CDR_NONNULL(ci); CDR_NONNULL(xc); CDR_NONNULL(rf); CDR_NONNULL(sof); CDR_NONNULL(xin); CDR_NONNULL(xout);
+	return interp_add_2d_wide(ci, xc, rf, sof, xin, xout, Dims2{nxf, nyf, pf}, Dims2{nxc, nyc, pc}, s, nsf);
+}
+
 int cdr_gpu_setup_interp_2d_f64(const double *so, int ns, double *ci, int nxf, int nyf, int pf, int nxc, int nyc,
                                 int pc, cudaStream_t s)
 {

@@ -103,9 +103,20 @@ __device__ __forceinline__ void fill_halo(double (&u)[HT][HT], const Dims2 &d, F
 	__syncthreads();
 }
 
+// The preconditioner's output at k: z, or (SPLIT) the sum of an FP64 part z
+// and an FP32 part zf (the FP32 cycle's fine level with a widened iterate:
+// the interpolated iterate and the post-smoothing correction)
+template <typename TZ, bool SPLIT>
+__device__ __forceinline__ double zval(const TZ *__restrict__ z, const float *__restrict__ zf, size_t k)
+{
+	if constexpr (SPLIT) return (double)z[k] + (double)zf[k];
+	else return (double)z[k];
+}
+
 // beta from z . q_prev
-template <typename TZ>
-__global__ void __launch_bounds__(TX *TY) k_fcg_beta(const TZ *__restrict__ z, const double *__restrict__ q, Dims2 d,
+template <typename TZ, bool SPLIT>
+__global__ void __launch_bounds__(TX *TY) k_fcg_beta(const TZ *__restrict__ z, const float *__restrict__ zf,
+                                                     const double *__restrict__ q, Dims2 d,
                                                      double *__restrict__ partial, FcgScalars *S)
 {
 	double acc[1] = {0.0};
@@ -115,7 +126,7 @@ __global__ void __launch_bounds__(TX *TY) k_fcg_beta(const TZ *__restrict__ z, c
 		for (int row = 0; row < FR; ++row)
 			if (fcg_point(d, row, i, j)) {
 				const size_t k = d.at(i, j);
-				acc[0] += (double)z[k] * q[k];
+				acc[0] += zval<TZ, SPLIT>(z, zf, k) * q[k];
 			}
 	}
 	grid_sums<1>(acc, partial, &S->ticket[0], [&](const double *v) {
@@ -127,8 +138,9 @@ __global__ void __launch_bounds__(TX *TY) k_fcg_beta(const TZ *__restrict__ z, c
 // p = z + beta p_prev (formed on the fly at the neighbours), q = A p, p . q and
 // p . r.  The products read the ghost ring as the residual kernels do (the
 // operator's couplings into it are zero); p is written on the interior only.
-template <typename TZ, int NS>
+template <typename TZ, int NS, bool SPLIT>
 __global__ void __launch_bounds__(TX *TY) k_fcg_dir(const double *__restrict__ so, const TZ *__restrict__ z,
+                                                    const float *__restrict__ zf,
                                                     double *__restrict__ p0, double *__restrict__ p1,
                                                     double *__restrict__ q, const double *__restrict__ r, Dims2 d,
                                                     double *__restrict__ partial, FcgScalars *S)
@@ -141,7 +153,7 @@ __global__ void __launch_bounds__(TX *TY) k_fcg_dir(const double *__restrict__ s
 	const double beta = S->beta;
 	const double *c = so, *w = so + ps, *s = so + 2 * ps, *sw = so + 3 * ps, *nw = so + 4 * ps;
 	__shared__ double pt[HT][HT];
-	fill_halo(pt, d, [&](size_t k) -> double { return madd(beta, pold[k], (double)z[k]); });
+	fill_halo(pt, d, [&](size_t k) -> double { return madd(beta, pold[k], zval<TZ, SPLIT>(z, zf, k)); });
 	double acc[2] = {0.0, 0.0};
 	int i, j;
 #pragma unroll
@@ -284,25 +296,38 @@ template int fcg_load<float>(const double *, float *, float *, Dims2, FcgScalars
 
 size_t fcg_scratch_doubles(Dims2 d) { return 2 * (size_t)ceil_div(d.nx, TX) * ceil_div(d.ny, TY * FR); }
 
-template <typename TZ>
-int fcg_step(const double *so, int ns, TZ *z, TZ *rin, double *x0, double *x1, const double *b, double *r,
-             double *p0, double *p1, double *q, Dims2 d, double *partial, FcgScalars *S, cudaStream_t st, bool formed)
+template <typename TZ, typename TR>
+int fcg_step(const double *so, int ns, const TZ *z, const float *zf, TR *rin, TR *zz, double *x0, double *x1,
+             const double *b, double *r, double *p0, double *p1, double *q, Dims2 d, double *partial, FcgScalars *S,
+             cudaStream_t st, bool formed)
 {
 	const dim3 nb(ceil_div(d.nx, TX), ceil_div(d.ny, TY * FR)), blk(TX, TY);
-	k_fcg_beta<TZ><<<nb, blk, 0, st>>>(z, q, d, partial, S);
+	if (zf) {
+		k_fcg_beta<TZ, true><<<nb, blk, 0, st>>>(z, zf, q, d, partial, S);
+		CDR_LAUNCH_CHECK();
+		if (ns == 5) k_fcg_dir<TZ, 5, true><<<nb, blk, 0, st>>>(so, z, zf, p0, p1, q, r, d, partial, S);
+		else k_fcg_dir<TZ, 3, true><<<nb, blk, 0, st>>>(so, z, zf, p0, p1, q, r, d, partial, S);
+	} else {
+		k_fcg_beta<TZ, false><<<nb, blk, 0, st>>>(z, nullptr, q, d, partial, S);
+		CDR_LAUNCH_CHECK();
+		if (ns == 5) k_fcg_dir<TZ, 5, false><<<nb, blk, 0, st>>>(so, z, nullptr, p0, p1, q, r, d, partial, S);
+		else k_fcg_dir<TZ, 3, false><<<nb, blk, 0, st>>>(so, z, nullptr, p0, p1, q, r, d, partial, S);
+	}
 	CDR_LAUNCH_CHECK();
-	if (ns == 5) k_fcg_dir<TZ, 5><<<nb, blk, 0, st>>>(so, z, p0, p1, q, r, d, partial, S);
-	else k_fcg_dir<TZ, 3><<<nb, blk, 0, st>>>(so, z, p0, p1, q, r, d, partial, S);
-	CDR_LAUNCH_CHECK();
-	if (!formed) k_fcg_update_rec<TZ><<<nb, blk, 0, st>>>(x0, x1, r, p0, p1, q, rin, z, d, partial, S);
-	else if (ns == 5) k_fcg_update<TZ, 5><<<nb, blk, 0, st>>>(so, x0, x1, b, r, p0, p1, rin, z, d, partial, S);
-	else k_fcg_update<TZ, 3><<<nb, blk, 0, st>>>(so, x0, x1, b, r, p0, p1, rin, z, d, partial, S);
+	if (!formed) k_fcg_update_rec<TR><<<nb, blk, 0, st>>>(x0, x1, r, p0, p1, q, rin, zz, d, partial, S);
+	else if (ns == 5) k_fcg_update<TR, 5><<<nb, blk, 0, st>>>(so, x0, x1, b, r, p0, p1, rin, zz, d, partial, S);
+	else k_fcg_update<TR, 3><<<nb, blk, 0, st>>>(so, x0, x1, b, r, p0, p1, rin, zz, d, partial, S);
 	CDR_LAUNCH_CHECK();
 	return CDR_OK;
 }
-template int fcg_step<double>(const double *, int, double *, double *, double *, double *, const double *, double *,
-                              double *, double *, double *, Dims2, double *, FcgScalars *, cudaStream_t, bool);
-template int fcg_step<float>(const double *, int, float *, float *, double *, double *, const double *, double *,
-                             double *, double *, double *, Dims2, double *, FcgScalars *, cudaStream_t, bool);
+template int fcg_step<double, double>(const double *, int, const double *, const float *, double *, double *,
+                                      double *, double *, const double *, double *, double *, double *, double *,
+                                      Dims2, double *, FcgScalars *, cudaStream_t, bool);
+template int fcg_step<float, float>(const double *, int, const float *, const float *, float *, float *, double *,
+                                    double *, const double *, double *, double *, double *, double *, Dims2, double *,
+                                    FcgScalars *, cudaStream_t, bool);
+template int fcg_step<double, float>(const double *, int, const double *, const float *, float *, float *, double *,
+                                     double *, const double *, double *, double *, double *, double *, Dims2,
+                                     double *, FcgScalars *, cudaStream_t, bool);
 
 }  // namespace cdrgpu

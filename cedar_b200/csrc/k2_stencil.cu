@@ -391,6 +391,187 @@ int interp_add_2d_mixed(const double *ci, const double *xc, const float *rf, con
 	return CDR_OK;
 }
 
+// The same interpolate-add on the FP32 cycle's fine level when its iterate is
+// widened: xout (FP64) = xin (FP32) + P xc + r/c, formed in FP64 from the FP32
+// weights, coarse iterate and residual (the points and ghost positions
+// interp_at writes).
+__global__ void __launch_bounds__(TX *TY) k_interp_add_wide(const float *__restrict__ ci, const float *__restrict__ qc,
+                                                            const float *__restrict__ res,
+                                                            const float *__restrict__ soc,
+                                                            const float *__restrict__ qin, double *__restrict__ qout,
+                                                            Dims2 f, Dims2 c, int nsf)
+{
+	const int ic = blockIdx.x * TX + threadIdx.x + 1, jc = blockIdx.y * TY + threadIdx.y + 1;
+	if (ic > f.nx / 2 + 1 || jc > f.ny / 2 + 1) return;
+	const size_t cps = c.plane();
+	ci += c.bofs(8 * cps);
+	qc += c.bofs(cps);
+	res += f.bofs(f.plane());
+	soc += f.bofs(nsf * f.plane());
+	qin += f.bofs(f.plane());
+	qout += f.bofs(f.plane());
+	const int cp = c.pitch, fp = f.pitch;
+	const int i = 2 * ic - 1, j = 2 * jc - 1;
+	const size_t kc = c.at(ic, jc), kf = f.at(i, j);
+	auto rc = [&](size_t k, int ii, int jj) -> double {
+		return (ii <= f.nx && jj <= f.ny) ? (double)res[k] / (double)soc[k] : (double)res[k];
+	};
+	auto W = [&](int plane, size_t k) -> double { return (double)ci[plane * cps + k]; };
+	auto QC = [&](size_t k) -> double { return (double)qc[k]; };
+	const double qcc = QC(kc);
+	qout[kf] = (double)qin[kf] + qcc;
+	if (ic >= 2) {
+		const double a = W(IL, kc) * QC(kc - 1) + W(IR, kc) * qcc;
+		const size_t k = kf - 1;
+		qout[k] = (double)qin[k] + a + rc(k, i - 1, j);
+	}
+	if (jc >= 2) {
+		const double a = W(IB, kc) * QC(kc - cp) + W(IA, kc) * qcc;
+		const size_t k = kf - fp;
+		qout[k] = (double)qin[k] + a + rc(k, i, j - 1);
+	}
+	if (ic >= 2 && jc >= 2) {
+		double a = W(INW, kc) * QC(kc - 1) + W(ISW, kc) * QC(kc - cp - 1);
+		a += W(INE, kc) * qcc;
+		a += W(ISE, kc) * QC(kc - cp);
+		const size_t k = kf - fp - 1;
+		qout[k] = (double)qin[k] + a + rc(k, i - 1, j - 1);
+	}
+}
+
+// Row-sum excess of a level's operator, dg = c - (w(i,j) + w(i+1,j) + s(i,j) +
+// s(i,j+1) [+ sw(i,j) + sw(i+1,j+1) + nw(i+1,j) + nw(i,j+1)]), in FP64 and
+// rounded once.
+__global__ void k_rowsum_excess(const double *__restrict__ so, int ns, float *__restrict__ dg, Dims2 d)
+{
+	const size_t ps = d.plane();
+	const int P = d.pitch;
+	const int i = blockIdx.x * TX + threadIdx.x + 1, j = blockIdx.y * TY + threadIdx.y + 1;
+	if (i > d.nx || j > d.ny) return;
+	const size_t k = d.at(i, j);
+	const double *w = so + ps, *s = so + 2 * ps;
+	double a = w[k] + w[k + 1] + s[k] + s[k + P];
+	if (ns == 5) {
+		const double *sw = so + 3 * ps, *nw = so + 4 * ps;
+		a = a + sw[k] + sw[k + P + 1] + nw[k + 1] + nw[k + P];
+	}
+	dg[k] = (float)(so[k] - a);
+}
+
+int rowsum_excess_2d(const double *so, int ns, float *dg, Dims2 d, cudaStream_t st)
+{
+	k_rowsum_excess<<<dim3(ceil_div(d.nx, TX), ceil_div(d.ny, TY)), dim3(TX, TY), 0, st>>>(so, ns, dg, d);
+	CDR_LAUNCH_CHECK();
+	return CDR_OK;
+}
+
+// Residual of the FP32 cycle's widened fine-level iterate (FP64 x) over the
+// FP32 operator in difference form, in FP64 arithmetic:
+//   r = b - dg x - sum over the couplings a of a (x - x_nb),
+// rounded to FP32, with dg the row-sum excess (k_rowsum_excess).  The sum is
+// the residual of the operator whose couplings and row-sum excess are the FP32
+// values: a zero row sum stays zero, and its rounding error scales with the
+// differences x - x_nb, not with x.  The post-smoothing that follows starts
+// from zero on r, so the kernel also zeroes that iterate (zero).  Four points
+// of a row per thread (rows 16-byte aligned, pitch a multiple of 4).
+template <int NS>
+__global__ void __launch_bounds__(TX *TY) k_residual_wide(const float *__restrict__ so, const float *__restrict__ dg,
+                                                          const double *__restrict__ q, const float *__restrict__ qf,
+                                                          float *__restrict__ res, float *__restrict__ zero, Dims2 d)
+{
+	constexpr int V = 4;
+	const size_t ps = d.plane();
+	const int P = d.pitch;
+	const int i0 = (blockIdx.x * TX + threadIdx.x) * V;
+	const int j = blockIdx.y * TY + threadIdx.y + 1;
+	if (i0 > d.nx || j > d.ny) return;
+	const size_t k = (size_t)j * P + i0;
+	const bool lft = i0 >= 1, rgt = i0 + V <= d.nx + 1;
+	auto ld4 = [](const float *p, float *o) {
+		const float4 t = *reinterpret_cast<const float4 *>(p);
+		o[0] = t.x; o[1] = t.y; o[2] = t.z; o[3] = t.w;
+	};
+	auto ldq = [&](size_t kk, double *o) {  // o[0] = q[kk-1], o[1..4] = q[kk..kk+3], o[5] = q[kk+4]
+		const double2 a = *reinterpret_cast<const double2 *>(q + kk), b = *reinterpret_cast<const double2 *>(q + kk + 2);
+		o[1] = a.x; o[2] = a.y; o[3] = b.x; o[4] = b.y;
+		o[0] = lft ? q[kk - 1] : 0.0;
+		o[V + 1] = rgt ? q[kk + V] : 0.0;
+	};
+	double qm[V + 2], qc[V + 2], qp[V + 2];
+	ldq(k - P, qm);
+	ldq(k, qc);
+	ldq(k + P, qp);
+	const float *w = so + ps, *s = so + 2 * ps, *sw = so + (NS == 5 ? 3 : 0) * ps, *nw = so + (NS == 5 ? 4 : 0) * ps;
+	float dd[V], bb[V], ww[V + 1], s0[V], s1[V];
+	ld4(dg + k, dd);
+	ld4(qf + k, bb);
+	ld4(w + k, ww);
+	ww[V] = rgt ? w[k + V] : 0.f;
+	ld4(s + k, s0);
+	ld4(s + k + P, s1);
+	float sw0[V], sw1[V + 1], nw0[V + 1], nw1[V];
+	if (NS == 5) {
+		ld4(sw + k, sw0);
+		ld4(sw + k + P, sw1);
+		sw1[V] = rgt ? sw[k + P + V] : 0.f;
+		ld4(nw + k, nw0);
+		nw0[V] = rgt ? nw[k + V] : 0.f;
+		ld4(nw + k + P, nw1);
+	}
+	float r[V];
+#pragma unroll
+	for (int m = 0; m < V; ++m) {
+		const double qk = qc[m + 1];
+		double a = (double)bb[m] - (double)dd[m] * qk;
+		a -= (double)ww[m] * (qk - qc[m]);
+		a -= (double)ww[m + 1] * (qk - qc[m + 2]);
+		a -= (double)s0[m] * (qk - qm[m + 1]);
+		a -= (double)s1[m] * (qk - qp[m + 1]);
+		if (NS == 5) {
+			a -= (double)sw0[m] * (qk - qm[m]);
+			a -= (double)nw0[m + 1] * (qk - qm[m + 2]);
+			a -= (double)nw1[m] * (qk - qp[m]);
+			a -= (double)sw1[m + 1] * (qk - qp[m + 2]);
+		}
+		r[m] = (float)a;
+	}
+	if (lft && i0 + V - 1 <= d.nx) {
+		*reinterpret_cast<float4 *>(res + k) = make_float4(r[0], r[1], r[2], r[3]);
+		*reinterpret_cast<float4 *>(zero + k) = make_float4(0.f, 0.f, 0.f, 0.f);
+	} else {
+#pragma unroll
+		for (int m = 0; m < V; ++m)
+			if (i0 + m >= 1 && i0 + m <= d.nx) {
+				res[k + m] = r[m];
+				zero[k + m] = 0.f;
+			}
+	}
+}
+
+int residual_2d_wide(const float *so, const float *dg, int ns, const double *x, const float *b, float *r, float *zero,
+                     Dims2 d, cudaStream_t st)
+{
+	if (((uintptr_t)so | (uintptr_t)dg | (uintptr_t)x | (uintptr_t)b | (uintptr_t)r | (uintptr_t)zero) % 16 != 0 ||
+	    d.pitch % 4 != 0 || d.nb != 1) {
+		set_error(CDR_ERR_ARG, "wide residual: rows must be 16-byte aligned with a pitch that is a multiple of 4");
+		return CDR_ERR_ARG;
+	}
+	const dim3 g(ceil_div(d.nx + 1, TX * 4), ceil_div(d.ny, TY)), blk(TX, TY);
+	if (ns == 5) k_residual_wide<5><<<g, blk, 0, st>>>(so, dg, x, b, r, zero, d);
+	else k_residual_wide<3><<<g, blk, 0, st>>>(so, dg, x, b, r, zero, d);
+	CDR_LAUNCH_CHECK();
+	return CDR_OK;
+}
+
+int interp_add_2d_wide(const float *ci, const float *xc, const float *rf, const float *sof, const float *xin,
+                       double *xout, Dims2 f, Dims2 c, cudaStream_t st, int nsf)
+{
+	k_interp_add_wide<<<dim3(ceil_div(f.nx / 2 + 1, TX), ceil_div(f.ny / 2 + 1, TY), f.nb), dim3(TX, TY), 0, st>>>(
+	    ci, xc, rf, sof, xin, xout, f, c, nsf);
+	CDR_LAUNCH_CHECK();
+	return CDR_OK;
+}
+
 // ------------------------------------------------ operator-induced interpolation
 // BMG2_SymStd_SETUP_interp_OI (src/2d/ftn/BMG2_SymStd_SETUP_interp_OI.f90:109-253).
 // Phase 1 computes the edge weights, phase 2 the corner weights that read

@@ -59,6 +59,16 @@ int interp_add_2d(const T *ci, const T *xc, const T *rf, const T *sof, T *xf, Di
                   int nstencil_fine = 5);
 // Hand-over from an FP32 fine level to an FP64 coarse one (mixed cycles)
 int restrict_2d_mixed(const double *ci, const float *rf, double *bc, Dims2 f, Dims2 c, cudaStream_t st);
+// The FP32 cycle's fine level with a widened (FP64) iterate: the row-sum
+// excess dg of the operator (FP64, rounded), the residual r = b - dg x -
+// sum a (x - x_nb) of the FP64 iterate in FP64 arithmetic over the FP32 data
+// (zeroing `zero`, the post-smoothing's initial guess), and the interpolate-add
+// xout (FP64) = xin + P xc + r/c in FP64
+int rowsum_excess_2d(const double *so, int ns, float *dg, Dims2 d, cudaStream_t st);
+int residual_2d_wide(const float *so, const float *dg, int ns, const double *x, const float *b, float *r, float *zero,
+                     Dims2 d, cudaStream_t st);
+int interp_add_2d_wide(const float *ci, const float *xc, const float *rf, const float *sof, const float *xin,
+                       double *xout, Dims2 f, Dims2 c, cudaStream_t st, int nsf);
 int interp_add_2d_mixed(const double *ci, const double *xc, const float *rf, const float *sof, float *xf, Dims2 f,
                         Dims2 c, cudaStream_t st, int nsf_fine = 5);
 int setup_interp_2d(const double *so, int nstencil, double *ci, Dims2 f, Dims2 c, cudaStream_t st);
@@ -98,13 +108,15 @@ struct FcgScalars {
 size_t fcg_scratch_doubles(Dims2 d);
 template <typename TZ>
 int fcg_load(const double *r, TZ *rin, TZ *z, Dims2 d, FcgScalars *S, cudaStream_t st, bool restart = true);
-// One FCG iteration after the preconditioner wrote z (3 launches); leaves the
-// next preconditioner input in rin, z = 0 and |r|^2 in S->rr.  x alternates
-// between x0 and x1: after the step the iterate is in x[S->iter & 1].
-template <typename TZ>
-int fcg_step(const double *so, int ns, TZ *z, TZ *rin, double *x0, double *x1, const double *b, double *r,
-             double *p0, double *p1, double *q, Dims2 d, double *partial, FcgScalars *S, cudaStream_t st,
-             bool formed = true);
+// One FCG iteration after the preconditioner wrote its output, z (+ zf when
+// zf is not null: an FP64 part and an FP32 part), 3 launches; leaves the next
+// preconditioner input in rin, zz = 0 (the cycle's initial guess) and |r|^2
+// in S->rr.  x alternates between x0 and x1: after the step the iterate is in
+// x[S->iter & 1].
+template <typename TZ, typename TR>
+int fcg_step(const double *so, int ns, const TZ *z, const float *zf, TR *rin, TR *zz, double *x0, double *x1,
+             const double *b, double *r, double *p0, double *p1, double *q, Dims2 d, double *partial, FcgScalars *S,
+             cudaStream_t st, bool formed = true);
 
 constexpr size_t kNormScratchBytes = 2048 * sizeof(double);
 

@@ -40,6 +40,11 @@ struct Level {
 	// FP32 preconditioner copies
 	float *so32 = nullptr, *x32 = nullptr, *b32 = nullptr, *r32 = nullptr, *sor32 = nullptr, *sory32 = nullptr,
 	      *ci32 = nullptr;
+	// fine level of the FP32 preconditioner (settings.fp64_fine_iterate): the
+	// iterate from the interpolate-add on, in FP64, and the row-sum excess of
+	// the operator (the difference form of its residual)
+	double *xw = nullptr;
+	float *dg32 = nullptr;
 };
 
 }  // namespace
@@ -72,6 +77,7 @@ struct cdr_gpu_solver {
 	long long glaunches[2] = {0, 0};                 // kernel launches per replay
 	cudaEvent_t ev0 = nullptr, ev1 = nullptr;
 	float setup_ms = 0.f, solve_ms = 0.f;
+	bool wide = false;  // inside an FCG iteration with a widened fine-level iterate (lv[0].xw)
 
 	template <typename T>
 	int alloc(T **p, size_t n)
@@ -198,6 +204,17 @@ int cdr_gpu_solver::ncycle(int l, T *x, const T *b)
 	if (l + 1 == L() - 1) CDR_TRY(coarse_solve<T>(Arr<T>::x(C), Arr<T>::b(C)));
 	else if (l + 1 == lc[sizeof(T) == 4]) CDR_TRY(fused<T>(l + 1));
 	else CDR_TRY(ncycle<T>(l + 1, Arr<T>::x(C), Arr<T>::b(C)));
+	if constexpr (sizeof(T) == 4) {
+		if (l == 0 && wide) {
+			// the fine level's iterate goes on in FP64, xw = x + P x_c + r/c; the
+			// post-smoothing runs in FP32 on the correction from zero, with the
+			// right-hand side b - A xw formed in FP64 over the difference form;
+			// the cycle's output is xw + x (read by the FCG step as two parts)
+			CDR_TRY(interp_add_2d_wide(C.ci32, C.x32, F.r32, F.so32, x, F.xw, F.d, C.d, st, F.ns));
+			CDR_TRY(residual_2d_wide(F.so32, F.dg32, F.ns, F.xw, b, F.r32, x, F.d, st));
+			return smooth<T>(l, x, F.r32, CDR_UP);
+		}
+	}
 	CDR_TRY(interp_from<T>(l, x));
 	CDR_TRY(smooth<T>(l, x, b, CDR_UP));
 	return CDR_OK;
@@ -365,8 +382,19 @@ int cdr_gpu_solver::fcg_iteration(bool formed)
 {
 	Level &F = lv[0];
 	T *z = Arr<T>::x(F), *rin = Arr<T>::b(F);
+	if constexpr (sizeof(T) == 4) {
+		if (F.xw) {  // the cycle's output is F.xw + z; the next cycle starts from z = 0
+			wide = true;
+			const int rc = cycle<T>(z, rin);
+			wide = false;
+			CDR_TRY(rc);
+			return fcg_step<double, float>(F.so, F.ns, F.xw, z, rin, z, kx[0], kx[1], kb, kr, kp[0], kp[1], kq, F.d,
+			                               kpart, ks, st, formed);
+		}
+	}
 	CDR_TRY(cycle<T>(z, rin));
-	return fcg_step<T>(F.so, F.ns, z, rin, kx[0], kx[1], kb, kr, kp[0], kp[1], kq, F.d, kpart, ks, st, formed);
+	return fcg_step<T, T>(F.so, F.ns, z, nullptr, rin, z, kx[0], kx[1], kb, kr, kp[0], kp[1], kq, F.d, kpart, ks, st,
+	                      formed);
 }
 
 int cdr_gpu_solver::run_fcg(int prec, bool formed)
@@ -468,6 +496,7 @@ int cdr_gpu_solver::setup()
 		for (int l = 0; l < L(); ++l) {
 			Level &F = lv[l];
 			CDR_TRY(convert_f64_f32(F.so, F.so32, F.d.plane() * F.ns, st));
+			if (F.dg32) CDR_TRY(rowsum_excess_2d(F.so, F.ns, F.dg32, F.d, st));
 			if (l > 0) CDR_TRY(convert_f64_f32(F.ci, F.ci32, F.d.plane() * 8, st));
 			if (l + 1 == L()) continue;
 			switch (s.relaxation) {
@@ -535,6 +564,7 @@ int cdr_gpu_settings_default(cdr_gpu_settings *s)
 	s->cycle = CDR_CYCLE_V;
 	s->krylov_replace = 1;
 	s->periodic = 0;
+	s->fp64_fine_iterate = 1;
 	return CDR_OK;
 }
 
@@ -626,6 +656,17 @@ static int create_impl(cdr_gpu_solver *h, const double *so_src, int ns, int nx, 
 	// the fused coarse cycle has no periodic branches
 	h->lc[0] = h->per ? -1 : pick_fused_level<double>(h->lv, s);
 	h->lc[1] = h->per ? -1 : pick_fused_level<float>(h->lv, s);
+	// FCG around the FP32 cycle: the fine level's iterate from the
+	// interpolate-add on in FP64 (the preconditioner's output), when level 1 is
+	// an FP32 level
+	{
+		Level &F0 = h->lv[0];
+		if (h->mixed() && s.krylov == CDR_KRYLOV_FCG && s.fp64_fine_iterate && !h->per && nl >= 2 &&
+		    s.fp32_levels != 1) {
+			CDR_TRY(h->alloc(&F0.xw, F0.d.plane()));
+			CDR_TRY(h->alloc(&F0.dg32, F0.d.plane()));
+		}
+	}
 	Level &Cg = h->lv[nl - 1];
 	if ((size_t)Cg.nx * Cg.ny > 4096) {
 		set_error(CDR_ERR_DIM, "coarsest grid %dx%d too large for the %s Cholesky", Cg.nx, Cg.ny,
@@ -691,6 +732,10 @@ static int create_any(const cdr_gpu_settings *s, const double *so_src, int ns, i
 	}
 	if (s->krylov_replace < 0) {
 		set_error(CDR_ERR_ARG, "invalid krylov_replace %d", s->krylov_replace);
+		return CDR_ERR_ARG;
+	}
+	if (s->fp64_fine_iterate != 0 && s->fp64_fine_iterate != 1) {
+		set_error(CDR_ERR_ARG, "invalid fp64_fine_iterate %d (0 or 1)", s->fp64_fine_iterate);
 		return CDR_ERR_ARG;
 	}
 	if (s->periodic & ~3) {

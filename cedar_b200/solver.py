@@ -57,6 +57,7 @@ def _settings(ms: MLSettings, dim=2):
     if dim == 2 and ms.periodic[2]:
         raise ValueError("grid.periodic: a 2D grid has no z direction")
     s.periodic = ms.per_mask
+    s.fp64_fine_iterate = 1 if ms.fine_iterate == "fp64" else 0
     return s
 
 

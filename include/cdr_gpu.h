@@ -238,6 +238,26 @@ int cdr_gpu_relax_lines_2d_sync_f32(const float *so, int nstencil, float *x, con
                                     int nx, int ny, int pitch, int tpitch, int dir, int updown, int flags,
                                     unsigned *sync, cudaStream_t stream);
 
+/* The FP32 preconditioner's fine level with its iterate kept in FP64
+ * (settings.fp64_fine_iterate); no counterpart in the reference (its cycle is
+ * FP64 throughout).  cdr_gpu_rowsum_excess_2d: dg = c - (sum of the point's
+ * 4 or 8 couplings) of an FP64 operator, formed in FP64 and rounded to FP32
+ * (interior points).  cdr_gpu_residual_2d_wide: r = b - dg x - sum a (x - x_nb)
+ * for an FP64 iterate x over the FP32 couplings a (so32, plane 0 unused) and dg,
+ * in FP64 arithmetic, r rounded to FP32; it also zeroes `zero` on the interior
+ * (the post-smoothing's initial guess).  Rows 16-byte aligned, pitch a multiple
+ * of 4.  cdr_gpu_interp_add_2d_wide: x_out (FP64) = x_in + P x_c + r/c over
+ * FP32 weights, coarse iterate, residual and operator diagonal, in FP64
+ * arithmetic (interp_add::run, BMG2_SymStd_interp_add.f90:101-137, with the
+ * fine iterate widened). */
+int cdr_gpu_rowsum_excess_2d(const double *so, int nstencil, float *dg, int nx, int ny, int pitch,
+                             cudaStream_t stream);
+int cdr_gpu_residual_2d_wide(const float *so, const float *dg, int nstencil, const double *x, const float *b,
+                             float *r, float *zero, int nx, int ny, int pitch, cudaStream_t stream);
+int cdr_gpu_interp_add_2d_wide(const float *ci, const float *x_coarse, const float *r_fine, const float *so_fine,
+                               int nstencil_fine, const float *x_in, double *x_out, int nxf, int nyf, int pf,
+                               int nxc, int nyc, int pc, cudaStream_t stream);
+
 /* b_coarse = P^T r_fine; replaces restriction::run (include/cedar/kernels/restrict.h:17-19)
  * -> BMG2_SymStd_restrict (src/2d/restrict.cc:14-29, src/2d/ftn/BMG2_SymStd_restrict.f90:72-92). */
 int cdr_gpu_restrict_2d_f64(const double *ci, const double *r_fine, double *b_coarse,
@@ -335,6 +355,14 @@ typedef struct cdr_gpu_settings {
 	                     point relaxation (V or F cycle) and the direct coarse solve; the operator and b
 	                     hold the wrap-around couplings and copies of the opposite interior lines in
 	                     their ghost lines (examples/basic-2d-ser/periodic.cc) */
+	int fp64_fine_iterate; /* CDR_PREC_F32_IR with CDR_KRYLOV_FCG, 2D solver: 1 (default) keeps the FP32
+	                          cycle's fine-level iterate in FP64 from the interpolate-add on: the post-smoothing
+	                          runs in FP32 on a correction from zero whose right-hand side is the residual of the
+	                          FP64 iterate, formed in FP64 arithmetic over the FP32 operator in difference form,
+	                          and the preconditioner's output is the FP64 iterate plus that correction.  The
+	                          output then carries no FP32 rounding of the iterate itself (of relative size
+	                          eps32 |A||x| in the residual, large on high-contrast operators); 0: FP32
+	                          throughout */
 } cdr_gpu_settings;
 
 typedef struct cdr_gpu_solver cdr_gpu_solver;

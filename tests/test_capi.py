@@ -88,3 +88,8 @@ def test_config_gpu_keys_map_to_settings():
         MLSettings(Config({"solver": {"cg-solver": "dense"}}))
     with pytest.raises(ValueError):
         MLSettings(Config({"gpu": {"fcg-replace": -1}}))
+    # the FP32 cycle's fine-level iterate: FP64 by default, "fp32" turns it off
+    assert s.fp64_fine_iterate == 1
+    assert _settings(MLSettings(Config({"gpu": {"fine-iterate": "fp32"}}))).fp64_fine_iterate == 0
+    with pytest.raises(ValueError):
+        MLSettings(Config({"gpu": {"fine-iterate": "fp16"}}))
