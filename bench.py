@@ -51,9 +51,9 @@ WORKLOAD = ("2D heterogeneous diffusion, 9-pt bilinear FE, 2047x2047 nodes (2048
             "(seed 3); line-xy relaxation, Galerkin coarsening (levels and coarsest solve: config.solver)")
 # DRAM bytes (read + write) per launch on the 2047^2 FP32 level, from one ncu capture each (caches
 # flushed): x-lines, one colour (the streamed kernel, k_lines_xstream) 85.1 MB read + 2.9 MB written;
-# y-lines, both colours in one launch (k_ylines_pair): None until captured
+# y-lines, both colours in one launch (k_ylines_pair) 179.6 MB read + 11.0 MB written
 LINE_X_TRAFFIC = 88.1e6
-LINE_Y_TRAFFIC = None
+LINE_Y_TRAFFIC = 190.6e6
 # headline FCG: the residual is formed (b - A x) every FCG_REPLACE-th iteration and to confirm convergence,
 # updated as r - alpha A p in between
 FCG_REPLACE = 10
@@ -65,8 +65,9 @@ def workload_config(args):
     return {"workload": WORKLOAD, "n": args.n, "tol": args.tol, "levels": 6,
             "solver": "flexible CG (FP64 recurrences; residual formed as b - A x every %d iterations and to confirm "
                       "convergence, updated in between) preconditioned by one line-xy V(1,1) cycle over 6 levels "
-                      "(coarsest 64^2); GPU: FP32 cycle (value) and FP64 cycle (fp64_ms), coarsest solved with its "
-                      "explicit inverse; CPU oracle: FP64 cycle, coarsest by banded Cholesky" % FCG_REPLACE,
+                      "(coarsest 64^2); GPU: FP32 cycle (value; its fine-level iterate kept in FP64 from the "
+                      "interpolate-add on) and FP64 cycle (fp64_ms), coarsest solved with its explicit inverse; CPU "
+                      "oracle: FP64 cycle, coarsest by banded Cholesky" % FCG_REPLACE,
             "parallelism": "replicas" if int(os.environ.get("WORLD_SIZE", "1")) > 1 else "single",
             "l2": "inputs larger than L2 (fine level ~1.5 GB/cycle vs 126 MB L2)"}
 
