@@ -508,6 +508,7 @@ def main():
         out["inverse_diffusion"] = inverse_batch()
         out["hetero3d"] = hetero3_leg(stream)
         out["batch512"] = batch_leg()
+        out["batch512_streams"] = batch_leg_streams()
         out["poisson511"] = poisson511(stream)
         out["cpu_baseline"] = cpu_arm(args, so, b, "config above")
     elif world > 1 and not args.no_extras:
@@ -688,8 +689,98 @@ def batch_class_problems(n, ids, pitch, ell=1.0 / 32, sigma=1.0):
 
 def batch_leg(count=512, dist=None):
     """512 independent 9-point problems, sizes 63..1023, FP32 V(1,1) line-xy cycles
-    inside FP64 refinement to 1e-8 per problem; one batch per size, the batches
-    of a rank solved concurrently (one stream and host thread each).  With a
+    inside FP64 refinement to 1e-8 per problem, all sizes in one mixed batch
+    (every level of every problem with the same grid size in one array, one
+    launch per cycle step over all of them, the cycle one CUDA graph on one
+    stream), timed with CUDA events on that stream.  With a process group the
+    work list is split over the ranks by estimated cost (cedar_b200.shard; no
+    collective on the data path), and the per-problem statistics are gathered
+    at the end."""
+    import numpy as np
+    import torch
+    from cedar_b200 import problems as P, shard
+    from cedar_b200.config import Config
+    from cedar_b200.solver import MixedBatchSolver2D
+    world = dist.get_world_size() if dist else 1
+    rank = dist.get_rank() if dist else 0
+    sizes = P.batch_sizes(count)
+    parts = shard.partition(sizes, world)
+    mine = np.array(parts[rank], dtype=np.int64)
+    conf = Config({"solver": {"relaxation": "line-xy", "cycle": {"nrelax-pre": 1, "nrelax-post": 1},
+                              "max-iter": 60, "tol": 1e-8}, "gpu": {"precision": "fp32-ir"}})
+    st = torch.cuda.Stream()
+    classes = []
+    for n in sorted(set(int(v) for v in sizes[mine]), reverse=True):
+        ids = mine[sizes[mine] == n]
+        pitch = ((n + 2 + 15) // 16) * 16
+        so, b = batch_class_problems(n, ids, pitch)
+        classes.append({"n": n, "ids": ids, "count": len(ids), "so": so, "b": b, "x": torch.zeros_like(b),
+                        "pitch": pitch})
+    torch.cuda.synchronize()
+    mb = MixedBatchSolver2D([(c["so"].data_ptr(), 5, c["n"], c["n"], c["pitch"], c["count"]) for c in classes],
+                            conf, stream=st.cuda_stream) if classes else None
+
+    def run():
+        for c in classes:
+            c["x"].zero_()
+        torch.cuda.synchronize()
+        mb.solve_device([c["b"].data_ptr() for c in classes], [c["x"].data_ptr() for c in classes])
+
+    ms = 0.0
+    if mb:
+        run()  # warm-up: captures the cycle graph
+        run()
+    if dist:
+        dist.barrier()
+    if mb:
+        for c in classes:
+            c["x"].zero_()
+        torch.cuda.synchronize()
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+        ev[0].record(st)
+        mb.solve_device([c["b"].data_ptr() for c in classes], [c["x"].data_ptr() for c in classes])
+        ev[1].record(st)
+        torch.cuda.synchronize()
+        ms = ev[0].elapsed_time(ev[1])
+    if dist:
+        w = torch.tensor([ms], device="cuda")
+        dist.all_reduce(w, op=dist.ReduceOp.MAX)
+        ms = float(w.item())
+    wall_ms = ms
+    ids = np.concatenate([c["ids"] for c in classes]) if classes else np.zeros(0, np.int64)
+    stats = np.stack([mb.done_ms.copy(), mb.rel.copy(), mb.iters.astype(float)], axis=1) if mb else np.zeros((0, 3))
+    table = shard.gather_stats(ids, stats, dist)
+    done, rel, its = table[:, 0], table[:, 1], table[:, 2]
+    per_class = {}
+    first = 0
+    for c in classes:
+        k = c["count"]
+        per_class[str(c["n"])] = {"problems": k, "max_cycles": int(mb.iters[first:first + k].max()),
+                                  "p99_done_ms": float(np.percentile(mb.done_ms[first:first + k], 99))}
+        first += k
+    setup_ms, _ = mb.timings() if mb else (0.0, 0.0)
+    launches = mb.cycle_launches if mb else 0
+    nsizes = mb.nsizes if mb else 0
+    if mb:
+        mb.close()
+    out = {"workload": "%d independent 9-point FE problems, edges {63,127,255,511,1023} weights 8:4:2:1:1 "
+                       "(seed 7), lognormal k sigma=1 ell=1/32 (CUDA generator 1000+id), b=U[0,1]h^2; FP32 V(1,1) "
+                       "line-xy + FP64 IR to 1e-8 per problem; all sizes in one mixed batch, one stream" % count,
+           "problems_per_s": count / (wall_ms * 1e-3), "batch_ms": wall_ms, "timing": "CUDA events on the batch's "
+           "stream around the whole solve (copies in and out included; max over ranks); per-problem times from "
+           "CUDA events", "p50_ms": float(np.percentile(done, 50)), "p99_ms": float(np.percentile(done, 99)),
+           "shared_sizes": nsizes, "cycle_launches": launches, "setup_ms": setup_ms,
+           "all_converged": bool(np.all(rel < 1e-8)), "max_cycles": int(its.max()), "ranks": world,
+           "rank_cost_share": [round(v / max(1, sum(shard.loads(sizes, parts))), 4) for v in shard.loads(sizes, parts)]}
+    if world == 1:
+        out["per_size"] = per_class
+    return out
+
+
+def batch_leg_streams(count=512, dist=None):
+    """The batch leg's workload as one batch per size, the batches of a rank
+    solved concurrently (one stream and host thread each; host wall clock): the
+    comparison for the mixed batch of batch_leg.  With a
     process group the work list is split over the ranks by estimated cost
     (cedar_b200.shard; no collective on the data path), and the per-problem
     statistics are gathered at the end."""

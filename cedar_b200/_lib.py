@@ -133,6 +133,13 @@ def load(path=LIB_PATH):
         "cdr_gpu_batch2d_solve_device": (I, [P, P, P, I, P, P, P]),
         "cdr_gpu_batch2d_nlevels": (I, [P]),
         "cdr_gpu_batch2d_timings": (I, [P, ctypes.POINTER(D), ctypes.POINTER(D)]),
+        # independent problems of several sizes
+        "cdr_gpu_batchmix_create": (I, [ctypes.POINTER(Settings), I, P, P, P, P, P, P, S, ctypes.POINTER(P)]),
+        "cdr_gpu_batchmix_destroy": (I, [P]),
+        "cdr_gpu_batchmix_solve_device": (I, [P, P, P, P, P, P, P]),
+        "cdr_gpu_batchmix_timings": (I, [P, ctypes.POINTER(D), ctypes.POINTER(D)]),
+        "cdr_gpu_batchmix_sizes": (I, [P]),
+        "cdr_gpu_batchmix_cycle_launches": (ctypes.c_longlong, [P]),
     })
     for name, (res, args) in sig.items():
         f = getattr(L, name)

@@ -61,7 +61,8 @@ int Batch2::alloc(T **p, size_t n)
 	return CDR_OK;
 }
 
-int Batch2::init(const cdr_gpu_settings &settings, int ns, int nx, int ny, int nbatch, cudaStream_t stream)
+int Batch2::init(const cdr_gpu_settings &settings, int ns, int nx, int ny, int nbatch, cudaStream_t stream,
+                 bool external32)
 {
 	s = settings;
 	nb = nbatch;
@@ -96,7 +97,7 @@ int Batch2::init(const cdr_gpu_settings &settings, int ns, int nx, int ny, int n
 			CDR_TRY(alloc(&L.sor, pl * 2));
 			if (lines) CDR_TRY(alloc(&L.sory, L.ysize() * nb));
 		}
-		if (mixed()) {
+		if (mixed() && !external32) {
 			CDR_TRY(alloc(&L.so32, pl * L.ns));
 			CDR_TRY(alloc(&L.x32, pl));
 			CDR_TRY(alloc(&L.b32, pl));
@@ -115,7 +116,7 @@ int Batch2::init(const cdr_gpu_settings &settings, int ns, int nx, int ny, int n
 		set_error(CDR_ERR_DIM, "coarsest grid %dx%d too large for the banded Cholesky", Cg.nx, Cg.ny);
 		return CDR_ERR_DIM;
 	}
-	CDR_TRY(alloc(&abd, abd_size() * nb));
+	if (!external32) CDR_TRY(alloc(&abd, abd_size() * nb));
 	CDR_TRY(alloc(&info, 2));
 	return CDR_OK;
 }

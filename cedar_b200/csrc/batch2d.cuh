@@ -50,8 +50,11 @@ public:
 	~Batch2();
 
 	// Allocate nb hierarchies for an nx x ny fine grid with ns-plane fine
-	// operators (the fine operators are then written into lv[0].so).
-	int init(const cdr_gpu_settings &settings, int ns, int nx, int ny, int nb, cudaStream_t stream);
+	// operators (the fine operators are then written into lv[0].so).  With
+	// external32 the FP32 level arrays and the coarsest factor (abd) are not
+	// allocated: the owner points them into its own storage before setup.
+	int init(const cdr_gpu_settings &settings, int ns, int nx, int ny, int nb, cudaStream_t stream,
+	         bool external32 = false);
 	// multilevel::setup (include/cedar/multilevel.h:243-265) for all problems;
 	// checks the factorizations (synchronises the stream) when check is set.
 	int setup(bool check);

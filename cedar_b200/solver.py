@@ -287,3 +287,68 @@ class BatchSolver2D:
         _lib.check(self.lib.cdr_gpu_batch2d_solve_device(
             self.h, ctypes.c_void_p(b_ptr), ctypes.c_void_p(x_ptr), pitch or self.pitch,
             self.iters.ctypes.data, self.rel.ctypes.data, self.done_ms.ctypes.data))
+
+
+class MixedBatchSolver2D:
+    """Independent 2D problems of several grid sizes solved together on the GPU
+    (each with its own hierarchy and stopping test, as ``cdr2::solver``): every
+    level of every problem with the same grid size shares one FP32 array, so
+    one launch of each V-cycle step covers that level of all problems.
+
+    ``classes``: a list of (so_ptr, nstencil, nx, ny, pitch, nb), so_ptr a
+    device pointer to nb fine operators back to back.  FP32 cycles with FP64
+    refinement (``gpu.precision = "fp32-ir"``)."""
+
+    def __init__(self, classes, conf=None, stream=0):
+        self.lib = _lib.load()
+        self.settings = conf if isinstance(conf, MLSettings) else MLSettings(conf)
+        self._s = _settings(self.settings)
+        k = len(classes)
+        P = ctypes.c_void_p * k
+        I = ctypes.c_int * k
+        self.classes = list(classes)
+        self._so = P(*[ctypes.c_void_p(c[0]) for c in classes])
+        self._ns, self._nx, self._ny = I(*[c[1] for c in classes]), I(*[c[2] for c in classes]), I(*[c[3] for c in classes])
+        self._pitch, self._nb = I(*[c[4] for c in classes]), I(*[c[5] for c in classes])
+        self.total = sum(c[5] for c in classes)
+        h = ctypes.c_void_p()
+        _lib.check(self.lib.cdr_gpu_batchmix_create(ctypes.byref(self._s), k, self._so, self._ns, self._nx, self._ny,
+                                                    self._pitch, self._nb, ctypes.c_void_p(stream), ctypes.byref(h)))
+        self.h = h
+        self.iters = np.zeros(self.total, dtype=np.int32)
+        self.rel = np.zeros(self.total)
+        self.done_ms = np.zeros(self.total, dtype=np.float32)
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.cdr_gpu_batchmix_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def nsizes(self):
+        return self.lib.cdr_gpu_batchmix_sizes(self.h)
+
+    @property
+    def cycle_launches(self):
+        return int(self.lib.cdr_gpu_batchmix_cycle_launches(self.h))
+
+    def timings(self):
+        a, b = ctypes.c_double(), ctypes.c_double()
+        _lib.check(self.lib.cdr_gpu_batchmix_timings(self.h, ctypes.byref(a), ctypes.byref(b)))
+        return a.value, b.value
+
+    def solve_device(self, b_ptrs, x_ptrs):
+        """Solve every problem: b_ptrs[c] / x_ptrs[c] (device) hold class c's right-hand sides and initial
+        guesses back to back at the class's pitch.  iters, rel, done_ms: per problem, classes in order."""
+        k = len(self.classes)
+        P = ctypes.c_void_p * k
+        bp = P(*[ctypes.c_void_p(p) for p in b_ptrs])
+        xp = P(*[ctypes.c_void_p(p) for p in x_ptrs])
+        _lib.check(self.lib.cdr_gpu_batchmix_solve_device(self.h, bp, xp, self._pitch, self.iters.ctypes.data,
+                                                          self.rel.ctypes.data, self.done_ms.ctypes.data))

@@ -513,6 +513,32 @@ int cdr_gpu_batch2d_solve_device(cdr_gpu_batch2d *h, const double *b_dev, double
 int cdr_gpu_batch2d_nlevels(const cdr_gpu_batch2d *h);
 int cdr_gpu_batch2d_timings(const cdr_gpu_batch2d *h, double *setup_ms, double *solve_ms);
 
+/* Independent 2D problems of several grid sizes solved together: nclass size
+ * classes, class c holding nb[c] problems of nx[c] x ny[c] points (fine
+ * operators so_dev[c], nstencil ns[c], back to back at pitch[c]).  No single
+ * reference call: each problem keeps the semantics of its own cdr2::solver
+ * (include/cedar/2d/solver.h:45-129), FP32 V-cycles refined in FP64 to its own
+ * relative tolerance (settings.precision CDR_PREC_F32_IR, V-cycles, banded
+ * coarsest solve).  Every hierarchy level of every problem with the same grid
+ * size shares one FP32 array (problems back to back), so one launch of each
+ * cycle step covers that level of all problems; the sizes at and below the
+ * classes' common fused coarse level run as one launch over all problems (when
+ * the classes fuse from different sizes, every level runs with its own
+ * launches); the cycle is one CUDA graph on one stream.  Solve: b_dev[c] / x_dev[c] per class
+ * at pitch[c] (x holds the initial guesses); iters, rel, done_ms per problem,
+ * classes in the caller's order (done_ms may be null). */
+typedef struct cdr_gpu_batchmix cdr_gpu_batchmix;
+int cdr_gpu_batchmix_create(const cdr_gpu_settings *s, int nclass, const double *const *so_dev, const int *ns,
+                            const int *nx, const int *ny, const int *pitch, const int *nb, cudaStream_t stream,
+                            cdr_gpu_batchmix **out);
+int cdr_gpu_batchmix_destroy(cdr_gpu_batchmix *h);
+int cdr_gpu_batchmix_solve_device(cdr_gpu_batchmix *h, const double *const *b_dev, double *const *x_dev,
+                                  const int *pitch, int *iters, double *rel, float *done_ms);
+int cdr_gpu_batchmix_timings(const cdr_gpu_batchmix *h, double *setup_ms, double *solve_ms);
+/* grid sizes shared by the classes' levels; kernel launches of one cycle (its graph) */
+int cdr_gpu_batchmix_sizes(const cdr_gpu_batchmix *h);
+long long cdr_gpu_batchmix_cycle_launches(const cdr_gpu_batchmix *h);
+
 #ifdef __cplusplus
 }
 #endif
