@@ -133,6 +133,7 @@ def load(path=LIB_PATH):
         "cdr_gpu_batch2d_solve_device": (I, [P, P, P, I, P, P, P]),
         "cdr_gpu_batch2d_nlevels": (I, [P]),
         "cdr_gpu_batch2d_timings": (I, [P, ctypes.POINTER(D), ctypes.POINTER(D)]),
+        "cdr_gpu_batch2d_resetup_device": (I, [P, P, I]),
         # independent problems of several sizes
         "cdr_gpu_batchmix_create": (I, [ctypes.POINTER(Settings), I, P, P, P, P, P, P, S, ctypes.POINTER(P)]),
         "cdr_gpu_batchmix_destroy": (I, [P]),

@@ -68,9 +68,16 @@ def _padded(t, pitch):
     return out
 
 
+def _ready():
+    """The library's solvers run on their own streams when handed torch's
+    default stream: torch's pending writes to the inputs finish first."""
+    torch.cuda.current_stream().synchronize()
+
+
 def _solve(h, b_pad, pitch, maxiter):
     lib = _lib.load()
     x = torch.zeros_like(b_pad)
+    _ready()
     it = ctypes.c_int()
     hist = (ctypes.c_double * max(maxiter, 1))()
     _lib.check(lib.cdr_gpu_solver_solve_device(h, ctypes.c_void_p(b_pad.data_ptr()), ctypes.c_void_p(x.data_ptr()),
@@ -95,6 +102,7 @@ class DiffusionSolve(torch.autograd.Function):
                                                   ncx, ctypes.c_void_p(so.data_ptr()), nx, ny, pitch,
                                                   ctypes.c_void_p(stream)))
         key = _conf_key(tol, maxiter, precision, relaxation)
+        _ready()
         h = _POOL.acquire(nx, ny, key, so.data_ptr(), pitch, stream)
         b = _padded(f.detach().to(torch.float64), pitch)
         u, iters, rel = _solve(h, b, pitch, maxiter)
@@ -143,3 +151,115 @@ def solve_log_diffusion(theta, f, **kw):
     """Isotropic k = exp(theta) per cell (theta may be an FP32 parameter)."""
     k = torch.exp(theta.to(torch.float64))
     return solve_diffusion(k, k, f, **kw)
+
+
+class _BatchPool:
+    """Reusable batch hierarchies (cdr_gpu_batch2d), keyed by batch size, grid
+    size and settings; a reused batch is set up again on the new operators."""
+
+    def __init__(self):
+        self.free = {}
+
+    def acquire(self, nb, nx, ny, key, so_ptr, pitch, stream):
+        lst = self.free.setdefault((nb, nx, ny, key), [])
+        lib = _lib.load()
+        if lst:
+            h = lst.pop()
+            _lib.check(lib.cdr_gpu_batch2d_resetup_device(h, ctypes.c_void_p(so_ptr), pitch))
+            return h
+        s = _settings(MLSettings(Config(_conf_dict(key))))
+        h = ctypes.c_void_p()
+        _lib.check(lib.cdr_gpu_batch2d_create(ctypes.byref(s), ctypes.c_void_p(so_ptr), 5, nx, ny, pitch, nb,
+                                              ctypes.c_void_p(stream), ctypes.byref(h)))
+        return h
+
+    def release(self, nb, nx, ny, key, h):
+        self.free.setdefault((nb, nx, ny, key), []).append(h)
+
+
+_BPOOL = _BatchPool()
+
+
+def _solve_batch(h, b_pad, pitch, nb):
+    """Every problem of the batch from a zero guess: (x, per-problem cycles, relative residuals)."""
+    import numpy as np
+    lib = _lib.load()
+    x = torch.zeros_like(b_pad)
+    iters = np.zeros(nb, dtype=np.int32)
+    _ready()
+    rel = np.zeros(nb)
+    _lib.check(lib.cdr_gpu_batch2d_solve_device(h, ctypes.c_void_p(b_pad.data_ptr()), ctypes.c_void_p(x.data_ptr()),
+                                                pitch, iters.ctypes.data, rel.ctypes.data, None))
+    return x, iters, rel
+
+
+class BatchDiffusionSolve(torch.autograd.Function):
+    """DiffusionSolve for B independent problems of one size at once: the B
+    operators are assembled, set up and solved as one batch (each problem with
+    its own stopping test), and backward runs the B adjoint solves as one batch
+    on the same hierarchies, then the gradient kernel per problem."""
+
+    @staticmethod
+    def forward(ctx, kx, ky, f, tol, maxiter, precision, relaxation):
+        lib = _lib.load()
+        nb, ncy, ncx = kx.shape
+        nx, ny = ncx - 1, ncy - 1
+        if f.shape != (nb, ny + 2, nx + 2):
+            raise ValueError("rhs must have shape (B, ny+2, nx+2) = %s" % ((nb, ny + 2, nx + 2),))
+        kx = kx.detach().to(torch.float64).contiguous()
+        ky = ky.detach().to(torch.float64).contiguous()
+        stream = torch.cuda.current_stream().cuda_stream
+        pitch = _pitch(nx)
+        so = torch.empty((nb, 5, ny + 2, pitch), dtype=torch.float64, device=kx.device)
+        for p in range(nb):
+            _lib.check(lib.cdr_gpu_fe_assemble_2d_f64(ctypes.c_void_p(kx[p].data_ptr()),
+                                                      ctypes.c_void_p(ky[p].data_ptr()), ncx,
+                                                      ctypes.c_void_p(so[p].data_ptr()), nx, ny, pitch,
+                                                      ctypes.c_void_p(stream)))
+        key = _conf_key(tol, maxiter, precision, relaxation)
+        _ready()
+        h = _BPOOL.acquire(nb, nx, ny, key, so.data_ptr(), pitch, stream)
+        b = torch.zeros((nb, ny + 2, pitch), dtype=torch.float64, device=kx.device)
+        b[:, :, :nx + 2] = f.detach().to(torch.float64)
+        u, iters, rel = _solve_batch(h, b, pitch, nb)
+        ctx.info = {"iterations": iters, "final_rel_resid": rel}
+        if any(ctx.needs_input_grad[:3]):
+            ctx.save_for_backward(u)
+            ctx.solver = h
+            ctx.geom = (nb, nx, ny, pitch, key)
+        else:
+            _BPOOL.release(nb, nx, ny, key, h)
+        return u[:, :, :nx + 2].contiguous()
+
+    @staticmethod
+    def backward(ctx, grad_u):
+        lib = _lib.load()
+        (u,) = ctx.saved_tensors
+        nb, nx, ny, pitch, key = ctx.geom
+        h = ctx.solver
+        g = torch.zeros((nb, ny + 2, pitch), dtype=torch.float64, device=u.device)
+        g[:, 1:ny + 1, 1:nx + 1] = grad_u.detach().to(torch.float64)[:, 1:ny + 1, 1:nx + 1]
+        lam, _, _ = _solve_batch(h, g, pitch, nb)  # A symmetric: adjoint = same hierarchies
+        gkx = torch.empty((nb, ny + 1, nx + 1), dtype=torch.float64, device=u.device)
+        gky = torch.empty_like(gkx)
+        stream = torch.cuda.current_stream().cuda_stream
+        for p in range(nb):
+            _lib.check(lib.cdr_gpu_fe_grad_2d_f64(ctypes.c_void_p(u[p].data_ptr()), ctypes.c_void_p(lam[p].data_ptr()),
+                                                  nx, ny, pitch, ctypes.c_void_p(gkx[p].data_ptr()),
+                                                  ctypes.c_void_p(gky[p].data_ptr()), nx + 1,
+                                                  ctypes.c_void_p(stream)))
+        _BPOOL.release(nb, nx, ny, key, h)
+        ctx.solver = None
+        return gkx, gky, lam[:, :, :nx + 2].contiguous(), None, None, None, None
+
+
+def solve_diffusion_batch(kx, ky, f, tol=1e-10, maxiter=60, precision="fp32-ir", relaxation="line-xy"):
+    """u[p] = A(kx[p], ky[p])^{-1} f[p] for a batch of B problems of one size
+    (kx, ky: (B, ny+1, nx+1) cells; f: (B, ny+2, nx+2)), differentiable in kx, ky and f."""
+    return BatchDiffusionSolve.apply(kx, ky, f, tol, maxiter, precision, relaxation)
+
+
+def solve_log_diffusion_batch(theta, f, **kw):
+    """Isotropic k = exp(theta) per cell for a batch (theta: (B, ny+1, nx+1), may be FP32)."""
+    k = torch.exp(theta.to(torch.float64))
+    return solve_diffusion_batch(k, k, f, **kw)

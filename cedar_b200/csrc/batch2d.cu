@@ -591,6 +591,27 @@ int cdr_gpu_batch2d_solve_device(cdr_gpu_batch2d *h, const double *b_dev, double
 	return CDR_OK;
 }
 
+// New fine operators for the same batch (same sizes and settings): copied in
+// and the whole hierarchy set up again (multilevel::setup,
+// include/cedar/multilevel.h:243-265, per problem); the cycle graph and the
+// line shapes stay.
+int cdr_gpu_batch2d_resetup_device(cdr_gpu_batch2d *h, const double *so_dev, int pitch)
+{
+	if (!h) { set_error(CDR_ERR_HANDLE, "null batch"); return CDR_ERR_HANDLE; }
+	if (!so_dev) { set_error(CDR_ERR_ARG, "null operator"); return CDR_ERR_ARG; }
+	B2Level &F = h->B.lv[0];
+	if (pitch < F.nx + 2) { set_error(CDR_ERR_DIM, "pitch %d < nx+2", pitch); return CDR_ERR_DIM; }
+	CDR_CUDA_TRY(cudaMemcpy2DAsync(F.so, F.pitch * sizeof(double), so_dev, pitch * sizeof(double),
+	                               (F.nx + 2) * sizeof(double), (size_t)(F.ny + 2) * F.ns * h->B.nb,
+	                               cudaMemcpyDeviceToDevice, h->st));
+	CDR_CUDA_TRY(cudaEventRecord(h->ev[0], h->st));
+	CDR_TRY(h->B.setup(true));
+	CDR_CUDA_TRY(cudaEventRecord(h->ev[1], h->st));
+	CDR_CUDA_TRY(cudaEventSynchronize(h->ev[1]));
+	CDR_CUDA_TRY(cudaEventElapsedTime(&h->setup_ms, h->ev[0], h->ev[1]));
+	return CDR_OK;
+}
+
 int cdr_gpu_batch2d_timings(const cdr_gpu_batch2d *h, double *setup_ms, double *solve_ms)
 {
 	if (!h) return CDR_ERR_HANDLE;

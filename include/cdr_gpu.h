@@ -512,6 +512,9 @@ int cdr_gpu_batch2d_solve_device(cdr_gpu_batch2d *h, const double *b_dev, double
                                  double *rel, float *done_ms);
 int cdr_gpu_batch2d_nlevels(const cdr_gpu_batch2d *h);
 int cdr_gpu_batch2d_timings(const cdr_gpu_batch2d *h, double *setup_ms, double *solve_ms);
+/* New fine operators (device, the create call's layout at pitch) for the same
+ * batch: the hierarchy is set up again (multilevel::setup per problem). */
+int cdr_gpu_batch2d_resetup_device(cdr_gpu_batch2d *h, const double *so_dev, int pitch);
 
 /* Independent 2D problems of several grid sizes solved together: nclass size
  * classes, class c holding nb[c] problems of nx[c] x ny[c] points (fine

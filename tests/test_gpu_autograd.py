@@ -117,3 +117,33 @@ def test_adjoint_gradient_matches_finite_differences_and_oracle(oracle, precisio
     gx, gy = _grad_formula(k, k, u, lam)
     g_or = (gx + gy) * k
     assert np.linalg.norm(g - g_or) <= 1e-6 * np.linalg.norm(g_or)
+
+
+@pytest.mark.parametrize("n,nb", [(63, 3), (127, 2)])
+def test_batched_forward_and_adjoint_match_single_problems(lib, n, nb):
+    """The batch form (one batched forward solve, one batched adjoint solve,
+    the gradient kernel per problem) gives every problem the loss and the
+    log-coefficient gradient of its own single-problem solve, to 1e-6
+    relative (both solves converge to 1e-10; the FP32 cycles of a batch and of
+    a single problem round differently)."""
+    import torch
+    from cedar_b200.autograd import solve_log_diffusion, solve_log_diffusion_batch
+    thetas, fs, uos = [], [], []
+    for p in range(nb):
+        theta, theta_obs, f = P.inverse_problem(n, seed_theta=8 + 100 * p, seed_src=9 + 100 * p,
+                                                seed_obs=10 + 100 * p)
+        thetas.append(torch.tensor(theta, dtype=torch.float32, device="cuda"))
+        fs.append(torch.from_numpy(f).cuda())
+        uos.append(solve_log_diffusion(torch.from_numpy(theta_obs).cuda(), fs[-1], tol=1e-10, maxiter=80).detach())
+    th_b = torch.stack(thetas).clone().requires_grad_(True)
+    u_b = solve_log_diffusion_batch(th_b, torch.stack(fs), tol=1e-10, maxiter=80)
+    loss_b = 0.5 * ((u_b - torch.stack(uos)) ** 2).sum(dim=(1, 2))
+    loss_b.sum().backward()
+    for p in range(nb):
+        th = thetas[p].clone().requires_grad_(True)
+        u = solve_log_diffusion(th, fs[p], tol=1e-10, maxiter=80)
+        loss = 0.5 * ((u - uos[p]) ** 2).sum()
+        loss.backward()
+        assert abs(float(loss_b[p].detach()) - float(loss.detach())) <= 1e-6 * abs(float(loss.detach()))
+        g, gb = th.grad.double().cpu().numpy(), th_b.grad[p].double().cpu().numpy()
+        assert np.abs(gb - g).max() <= 1e-6 * np.abs(g).max(), p
