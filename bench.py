@@ -449,7 +449,9 @@ def main():
 
     sweep_ms = sweep_time(0, p_sx)
     launch_ms = sweep_ms / 2.0
+    l0 = lib.cdr_gpu_launch_count()
     ysweep_ms = sweep_time(1, p_sy)
+    y_launches = (lib.cdr_gpu_launch_count() - l0) // 23  # 3 warm-up + 20 timed sweeps
     # launch shapes the setup-time autotuner chose for the fine level (cap 0: streamed x-line kernel)
     shapes = {}
     for dname, dirn, nn, nl in (("x", 0, nx, ny), ("y", 1, ny, nx)):
@@ -491,8 +493,10 @@ def main():
                       "hbm_gbs": vcyc_bytes / (vc32["ms_per_cycle"] * 1e-3) / 1e9,
                       "fp64_ms": vc64["ms_per_cycle"],
                       "fp64_hbm_gbs": vcycle_bytes(vc64["solver"], word=8) / (vc64["ms_per_cycle"] * 1e-3) / 1e9},
-           "roofline": {"kernel": "k_ylines_pair<float,%d,K=%d> (fine-level y-line sweep, both colours in one "
-                                  "launch)" % (ns, shapes.get("y", {}).get("K", 0)), "line_shapes": shapes,
+           "roofline": {"kernel": ("k_ylines_pair<float,%d,K=%d> (fine-level y-line sweep, both colours in one "
+                                   "launch)" if y_launches == 1 else
+                                   "k_lines_fast<float,%d,y,K=%d> (fine-level y-line sweep, one launch per colour)")
+                                  % (ns, shapes.get("y", {}).get("K", 0)), "line_shapes": shapes,
                         "bound": "hbm", "achieved": y_achieved, "peak": peak, "unit": "GB/s",
                         "frac": y_achieved / peak, "peak_kind": peak_kind,
                         "traffic": LINE_Y_TRAFFIC if n == 2047 else None,

@@ -866,7 +866,7 @@ static int tune_dir(const T *so, T *x, const T *b, const T *sor, Dims2 d, int tp
 				rc = CDR_ERR_CUDA;
 				break;
 			}
-			if (DIR == CDR_DIR_Y && ysync && d.nb == 1) {  // the one-launch sweep the solver runs
+			if (DIR == CDR_DIR_Y && ysync && d.nb == 1 && sh.pair) {  // both colours in one launch
 				rc = sh.K == 16 ? launch_ypair<T, NS, 16>(so, x, b, sor, d, tpitch, CDR_DOWN, sh.cap, ysync, st)
 				                : launch_ypair<T, NS, 8>(so, x, b, sor, d, tpitch, CDR_DOWN, sh.cap, ysync, st);
 			} else {
@@ -891,13 +891,19 @@ static int tune_dir(const T *so, T *x, const T *b, const T *sor, Dims2 d, int tp
 	const float margin = 4 * level_bytes > flush_bytes / 2 ? 0.90f : 0.95f;
 	LineShape best = default_shape<T>(n, DIR, d.nb);
 	float best_ms = time_shape(best);
-	for (int c = 0; c < 4 && rc == CDR_OK; ++c) {
-		const LineShape sh{K, DIR == CDR_DIR_X ? caps_x[c] : std::max(32, caps_y[c]), 0};
-		if (!shape_ok<T>(sh, n, DIR)) continue;
-		if (DIR == CDR_DIR_X && sh.cap < TPL && caps_x[c] != 32) continue;  // same CTA as a smaller cap
-		const float ms = time_shape(sh);
-		if (ms < margin * best_ms) { best_ms = ms; best = sh; }
-	}
+	// y-lines of a single problem: both colours in one launch or one launch per
+	// colour (the first re-reads the coupling columns from L2, the second has
+	// half the critical path per launch: it wins on small levels)
+	const int npair = DIR == CDR_DIR_Y && ysync && d.nb == 1 ? 2 : 1;
+	for (int pr = 0; pr < npair && rc == CDR_OK; ++pr)
+		for (int c = 0; c < 4 && rc == CDR_OK; ++c) {
+			LineShape sh{K, DIR == CDR_DIR_X ? caps_x[c] : std::max(32, caps_y[c]), 0};
+			sh.pair = pr == 0 ? 1 : 0;
+			if (!shape_ok<T>(sh, n, DIR)) continue;
+			if (DIR == CDR_DIR_X && sh.cap < TPL && caps_x[c] != 32) continue;  // same CTA as a smaller cap
+			const float ms = time_shape(sh);
+			if (ms < margin * best_ms) { best_ms = ms; best = sh; }
+		}
 	if (DIR == CDR_DIR_X && rc == CDR_OK && xs_ok<T, NS>(d)) {
 		const LineShape sh{K, FAST_BLOCK_X, 1};
 		const float ms = time_shape(sh);
@@ -965,7 +971,7 @@ int relax_lines_2d(const T *so, int nstencil, T *x, const T *b, const T *sor, Di
 	    tpitch % 16 == 0) {
 		LineShape sh = force ? *force : shape_for<T>(d.ny, d.nx, nstencil, d.nb, dir);
 		if (!shape_ok<T>(sh, d.ny, dir)) sh = dflt;
-		if (shape_ok<T>(sh, d.ny, dir)) {
+		if (shape_ok<T>(sh, d.ny, dir) && sh.pair) {
 			if (sh.K == 16) {
 				if (nstencil == 5) return launch_ypair<T, 5, 16>(so, x, b, sor, d, tpitch, updown, sh.cap, ysync, st);
 				return launch_ypair<T, 3, 16>(so, x, b, sor, d, tpitch, updown, sh.cap, ysync, st);

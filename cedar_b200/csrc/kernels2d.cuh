@@ -30,6 +30,8 @@ size_t lines_sync_words(Dims2 d);
 struct LineShape {
 	int K = 8, cap = 1024;
 	int stream = 0;  // x-lines: rows streamed into shared memory (k_lines_xstream)
+	int pair = 1;    // y-lines of a single problem with a sync buffer: both colours in one launch
+	                 // (k_ylines_pair), 0: one launch per colour (the same bits)
 };
 // bounded waits of the streamed x-line kernel that gave up since the last call
 // (read and reset into *count; 0 in a healthy run); CDR_ERR_CUDA if they

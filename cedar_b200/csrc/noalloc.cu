@@ -17,7 +17,8 @@
 //  * every GPU that loads the library holds the array until the process exits;
 //  * the first call on a device looks up the array's device address (once per
 //    device, with that device current); make that first call before any
-//    stream capture;
+//    stream capture.  The address is kept for the life of the process, so the
+//    entry point must not be called on a device after cudaDeviceReset of it;
 //  * every call uses the same array and overwrites the partial sums it reads,
 //    so calls whose kernels overlap on the GPU (different streams, or different
 //    host threads, without ordering between them) race and give wrong norms.

@@ -139,8 +139,10 @@ int cdr_gpu_residual_2d_f32(const float *so, int nstencil, const float *x, const
  * until the process exits; grids of more than 65536 tiles (e.g. beyond
  * 4096x4096 points) are rejected with CDR_ERR_DIM.  The first call on a device
  * looks the array up (once per device, device current): make it before any
- * stream capture.  All calls share the array: calls that overlap on the GPU
- * race.  norm_out (device, one double) is required. */
+ * stream capture.  The looked-up address is kept for the process: after a
+ * cudaDeviceReset of that device it is stale, so do not call this entry point
+ * on a device that has been reset.  All calls share the array: calls that
+ * overlap on the GPU race.  norm_out (device, one double) is required. */
 int cdr_gpu_residual_2d_f64_noalloc(const double *so, int nstencil, const double *x, const double *b, double *r,
                                    int nx, int ny, int pitch, double *norm_out, cudaStream_t stream);
 

@@ -7,7 +7,8 @@ r = b - A x and ||r||_2 with its partial sums in a fixed device array instead of
 caller scratch.  This file checks, through the C ABI, that two calls in a row
 give the same r (bit for bit) and the same norm (1e-13 relative; the partial
 sums are grouped per tile instead of per block) as the regular entry point, and
-that grids beyond the array's capacity are refused.  It is collected last.
+that grids beyond the array's capacity are refused, and that calls after
+the first leave the device's free memory unchanged.  It is collected last.
 """
 import ctypes
 
@@ -55,6 +56,29 @@ def test_noalloc_matches_allocating_residual_twice(lib, n, ns, pad):
         np.testing.assert_array_equal(host(r_new)[:, :n + 2], host(r_ref)[:, :n + 2])
         a, e = host(nrm_new)[0], host(nrm_ref)[0]
         assert np.isfinite(a) and abs(a - e) <= 1e-13 * e, (call, a, e)
+
+
+def test_noalloc_calls_allocate_no_device_memory(lib):
+    """After a first call (which looks up the array's address), further calls
+    leave the device's free memory unchanged: nothing is allocated."""
+    import torch
+    n = 1023
+    so, b = P.hetero_diffusion(n, sigma=1.0, n_incl=8, contrast=100.0, aniso=0.1)
+    pitch = ((n + 2 + 31) // 32) * 32
+    dso, db = padded(so, pitch), padded(b, pitch)
+    dx = padded(np.zeros_like(b), pitch)
+    dr = torch.zeros_like(dx)
+    nrm = torch.zeros(1, dtype=torch.float64, device="cuda")
+    _lib.check(lib.cdr_gpu_residual_2d_f64_noalloc(ptr(dso), 5, ptr(dx), ptr(db), ptr(dr), n, n, pitch, ptr(nrm),
+                                                   stream()))
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info()
+    for _ in range(5):
+        _lib.check(lib.cdr_gpu_residual_2d_f64_noalloc(ptr(dso), 5, ptr(dx), ptr(db), ptr(dr), n, n, pitch,
+                                                       ptr(nrm), stream()))
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info()
+    assert free1 == free0, (free0, free1)
 
 
 def test_noalloc_rejects_grids_beyond_its_scratch(lib):
