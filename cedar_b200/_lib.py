@@ -22,6 +22,8 @@ DIR_X, DIR_Y = 0, 1
 LINES_EXACT = 1
 LINES_NOTUNE = 2
 LINES_STREAM = 4
+LINES_ZERO_START = 8
+LINES_YPAIR = 16
 
 _lib = None
 

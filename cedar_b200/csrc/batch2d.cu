@@ -201,7 +201,7 @@ int Batch2::check_info()
 
 // multilevel::setup_relax_helper smoother closures (include/cedar/multilevel.h:160-222)
 template <typename T>
-int Batch2::smooth(int l, Sel sel, int updown)
+int Batch2::smooth(int l, Sel sel, int updown, bool zero)
 {
 	B2Level &F = lv[l];
 	const Dims2 d = F.dims(sel);
@@ -213,17 +213,22 @@ int Batch2::smooth(int l, Sel sel, int updown)
 	const T *sy = BA<T>::sory(F) ? BA<T>::sory(F) + f * F.ysize() : nullptr;
 	const int flags = sizeof(T) == 8 ? s.line_flags : (s.line_flags & CDR_LINES_NOTUNE);
 	const int n = updown == CDR_DOWN ? s.nrelax_pre : s.nrelax_post;
+	if (zero && (n == 0 || s.relaxation == CDR_RELAX_POINT)) {  // only the line sweeps skip reading it
+		CDR_CUDA_TRY(cudaMemset2DAsync(x, sel.step * pl * sizeof(T), 0, pl * sizeof(T), sel.count, st));
+		zero = false;
+	}
 	for (int it = 0; it < n; ++it) {
+		const int f = flags | (zero && it == 0 ? CDR_LINES_ZERO_START : 0);  // the first sweep of a zero iterate
 		switch (s.relaxation) {
 		case CDR_RELAX_POINT: CDR_TRY(relax_point_2d<T>(so, F.ns, x, b, sx, d, updown, st)); break;
-		case CDR_RELAX_LINE_X: CDR_TRY(relax_lines_2d<T>(so, F.ns, x, b, sx, d, F.tpitch, CDR_DIR_X, updown, flags, st)); break;
-		case CDR_RELAX_LINE_Y: CDR_TRY(relax_lines_2d<T>(so, F.ns, x, b, sy, d, F.tpitch, CDR_DIR_Y, updown, flags, st)); break;
+		case CDR_RELAX_LINE_X: CDR_TRY(relax_lines_2d<T>(so, F.ns, x, b, sx, d, F.tpitch, CDR_DIR_X, updown, f, st)); break;
+		case CDR_RELAX_LINE_Y: CDR_TRY(relax_lines_2d<T>(so, F.ns, x, b, sy, d, F.tpitch, CDR_DIR_Y, updown, f, st)); break;
 		default:
 			if (updown == CDR_DOWN) {
-				CDR_TRY(relax_lines_2d<T>(so, F.ns, x, b, sx, d, F.tpitch, CDR_DIR_X, updown, flags, st));
+				CDR_TRY(relax_lines_2d<T>(so, F.ns, x, b, sx, d, F.tpitch, CDR_DIR_X, updown, f, st));
 				CDR_TRY(relax_lines_2d<T>(so, F.ns, x, b, sy, d, F.tpitch, CDR_DIR_Y, updown, flags, st));
 			} else {
-				CDR_TRY(relax_lines_2d<T>(so, F.ns, x, b, sy, d, F.tpitch, CDR_DIR_Y, updown, flags, st));
+				CDR_TRY(relax_lines_2d<T>(so, F.ns, x, b, sy, d, F.tpitch, CDR_DIR_Y, updown, f, st));
 				CDR_TRY(relax_lines_2d<T>(so, F.ns, x, b, sx, d, F.tpitch, CDR_DIR_X, updown, flags, st));
 			}
 		}
@@ -232,7 +237,7 @@ int Batch2::smooth(int l, Sel sel, int updown)
 }
 
 template <typename T>
-int Batch2::ncycle(int l, Sel sel)
+int Batch2::ncycle(int l, Sel sel, bool zero)
 {
 	B2Level &F = lv[l], &C = lv[l + 1];
 	const Dims2 df = F.dims(sel), dc = C.dims(sel);
@@ -244,14 +249,17 @@ int Batch2::ncycle(int l, Sel sel)
 	const T *ci = BA<T>::ci(C) + f * 8 * cp;
 	T *xc = BA<T>::x(C) + f * cp;
 	T *bc = BA<T>::b(C) + f * cp;
-	CDR_TRY(smooth<T>(l, sel, CDR_DOWN));
+	CDR_TRY(smooth<T>(l, sel, CDR_DOWN, zero));
 	CDR_TRY(residual_2d<T>(so, F.ns, x, b, r, df, nullptr, nullptr, st));
 	CDR_TRY(restrict_2d<T>(ci, r, bc, df, dc, st));
-	// zero the selected coarse iterates: rows of cp elements, step*cp apart
-	CDR_CUDA_TRY(cudaMemset2DAsync(xc, sel.step * cp * sizeof(T), 0, cp * sizeof(T), sel.count, st));
+	// the selected coarse iterates are zero (include/cedar/cycle/vcycle.h:79):
+	// cleared here (rows of cp elements, step*cp apart) for the direct coarse
+	// solves, treated as zero without being read by a coarse cycle's first sweep
+	const bool direct = l + 1 == L() - 1 || l + 1 == lc[sizeof(T) == 4];
+	if (direct) CDR_CUDA_TRY(cudaMemset2DAsync(xc, sel.step * cp * sizeof(T), 0, cp * sizeof(T), sel.count, st));
 	if (l + 1 == L() - 1) CDR_TRY(solve_cg_2d<T>(abd + f * abd_size(), xc, bc, dc, st));
 	else if (l + 1 == lc[sizeof(T) == 4]) CDR_TRY(fused<T>(l + 1, sel));
-	else CDR_TRY(ncycle<T>(l + 1, sel));
+	else CDR_TRY(ncycle<T>(l + 1, sel, true));
 	CDR_TRY(interp_add_2d<T>(ci, xc, r, so, x, df, dc, st, F.ns));
 	CDR_TRY(smooth<T>(l, sel, CDR_UP));
 	return CDR_OK;
@@ -312,7 +320,7 @@ int Batch2::fused(int l0, Sel sel)
 }
 
 template <typename T>
-int Batch2::cycle(Sel sel)
+int Batch2::cycle(Sel sel, bool zero)
 {
 	if (sel.count < 1) return CDR_OK;
 	if (L() == 1) {
@@ -320,10 +328,10 @@ int Batch2::cycle(Sel sel)
 		const size_t f = sel.first, fp = F.plane();
 		return solve_cg_2d<T>(abd + f * abd_size(), BA<T>::x(F) + f * fp, BA<T>::b(F) + f * fp, F.dims(sel), st);
 	}
-	return ncycle<T>(0, sel);
+	return ncycle<T>(0, sel, zero);
 }
-template int Batch2::cycle<double>(Sel);
-template int Batch2::cycle<float>(Sel);
+template int Batch2::cycle<double>(Sel, bool);
+template int Batch2::cycle<float>(Sel, bool);
 
 }  // namespace cdrgpu
 
@@ -375,7 +383,8 @@ struct cdr_gpu_batch2d {
 	int run_cycle(int prec)
 	{
 		const Sel all{0, 1, B.nb};
-		auto body = [&]() -> int { return prec == 0 ? B.cycle<double>(all) : B.cycle<float>(all); };
+		// FP32: the refinement's correction, from zero
+		auto body = [&]() -> int { return prec == 0 ? B.cycle<double>(all) : B.cycle<float>(all, true); };
 		if (!B.s.use_graph) return body();
 		if (!gexec[prec]) {
 			cudaGraph_t g = nullptr;
@@ -545,8 +554,7 @@ int cdr_gpu_batch2d_solve_device(cdr_gpu_batch2d *h, const double *b_dev, double
 	const dim3 cgrid(ceil_div((long)pl, 256) < 256 ? ceil_div((long)pl, 256) : 256, 1, nb);
 	for (it = 0; it < B.s.maxiter && nactive > 0; ++it) {
 		if (mixed) {
-			CDR_CUDA_TRY(cudaMemsetAsync(F.x32, 0, sizeof(float) * pl * nb, st));
-			CDR_TRY(h->run_cycle(1));
+			CDR_TRY(h->run_cycle(1));  // the correction F.x32 from zero
 			CDR_TRY(ir_residual_2d(F.so, F.ns, h->x64[cur], F.x32, F.b, h->x64[1 - cur], F.b32, d, d, h->norm,
 			                       h->partial, 1, st, h->active));
 			cur = 1 - cur;

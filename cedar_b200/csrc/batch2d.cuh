@@ -65,7 +65,7 @@ public:
 	// One V-cycle of the selected problems on their level-0 x and b
 	// (cycle::vcycle::ncycle_helper, include/cedar/cycle/vcycle.h:57-115).
 	template <typename T>
-	int cycle(Sel sel);
+	int cycle(Sel sel, bool zero = false);  // zero: the level-0 iterate is zero on entry (not read)
 	bool mixed() const { return s.precision == CDR_PREC_F32_IR; }
 	int L() const { return (int)lv.size(); }
 	size_t ldab() const { return (size_t)lv.back().nx + 2; }
@@ -76,9 +76,9 @@ private:
 	template <typename T>
 	int alloc(T **p, size_t n);
 	template <typename T>
-	int smooth(int l, Sel sel, int updown);
+	int smooth(int l, Sel sel, int updown, bool zero = false);
 	template <typename T>
-	int ncycle(int l, Sel sel);
+	int ncycle(int l, Sel sel, bool zero = false);
 	template <typename T>
 	int fused(int l0, Sel sel);
 	template <typename T>

@@ -105,26 +105,32 @@ struct cdr_gpu_batchmix {
 		return CDR_OK;
 	}
 
-	int smooth(USize &U, int updown)
+	// zero: every entry's iterate is zero on entry (its interior is not read)
+	int smooth(USize &U, int updown, bool zero = false)
 	{
 		const Dims2 d = U.dims(U.entries);
 		const int flags = s.line_flags & CDR_LINES_NOTUNE;
 		const int n = updown == CDR_DOWN ? s.nrelax_pre : s.nrelax_post;
+		if (zero && (n == 0 || s.relaxation == CDR_RELAX_POINT)) {  // only the line sweeps skip reading it
+			CDR_CUDA_TRY(cudaMemsetAsync(U.x32, 0, sizeof(float) * U.plane() * U.entries, st));
+			zero = false;
+		}
 		for (int it = 0; it < n; ++it) {
+			const int f = flags | (zero && it == 0 ? CDR_LINES_ZERO_START : 0);
 			switch (s.relaxation) {
 			case CDR_RELAX_POINT: CDR_TRY(relax_point_2d<float>(U.so32, U.ns, U.x32, U.b32, U.sor32, d, updown, st)); break;
 			case CDR_RELAX_LINE_X:
-				CDR_TRY(relax_lines_2d<float>(U.so32, U.ns, U.x32, U.b32, U.sor32, d, U.tpitch, CDR_DIR_X, updown, flags, st));
+				CDR_TRY(relax_lines_2d<float>(U.so32, U.ns, U.x32, U.b32, U.sor32, d, U.tpitch, CDR_DIR_X, updown, f, st));
 				break;
 			case CDR_RELAX_LINE_Y:
-				CDR_TRY(relax_lines_2d<float>(U.so32, U.ns, U.x32, U.b32, U.sory32, d, U.tpitch, CDR_DIR_Y, updown, flags, st));
+				CDR_TRY(relax_lines_2d<float>(U.so32, U.ns, U.x32, U.b32, U.sory32, d, U.tpitch, CDR_DIR_Y, updown, f, st));
 				break;
 			default:
 				if (updown == CDR_DOWN) {
-					CDR_TRY(relax_lines_2d<float>(U.so32, U.ns, U.x32, U.b32, U.sor32, d, U.tpitch, CDR_DIR_X, updown, flags, st));
+					CDR_TRY(relax_lines_2d<float>(U.so32, U.ns, U.x32, U.b32, U.sor32, d, U.tpitch, CDR_DIR_X, updown, f, st));
 					CDR_TRY(relax_lines_2d<float>(U.so32, U.ns, U.x32, U.b32, U.sory32, d, U.tpitch, CDR_DIR_Y, updown, flags, st));
 				} else {
-					CDR_TRY(relax_lines_2d<float>(U.so32, U.ns, U.x32, U.b32, U.sory32, d, U.tpitch, CDR_DIR_Y, updown, flags, st));
+					CDR_TRY(relax_lines_2d<float>(U.so32, U.ns, U.x32, U.b32, U.sory32, d, U.tpitch, CDR_DIR_Y, updown, f, st));
 					CDR_TRY(relax_lines_2d<float>(U.so32, U.ns, U.x32, U.b32, U.sor32, d, U.tpitch, CDR_DIR_X, updown, flags, st));
 				}
 			}
@@ -132,21 +138,29 @@ struct cdr_gpu_batchmix {
 		return CDR_OK;
 	}
 
+	// sizes [0, smoothed_sizes()) are smoothed by the cycle's separate launches
+	int smoothed_sizes() const { return fused >= 0 ? fused : (int)sz.size() - 1; }
+
 	// One FP32 V-cycle of every problem on its fine-level x32 and b32
 	// (cycle::vcycle::ncycle_helper, include/cedar/cycle/vcycle.h:57-115, per
-	// problem): down the sizes, the coarse end, up the sizes.
+	// problem): down the sizes, the coarse end, up the sizes.  Every problem's
+	// iterate is zero when its first smoothing starts (the refinement's
+	// correction on its fine level, coarse_x.set(0.0) below it): the sizes the
+	// cycle smooths start with sweeps that treat it as zero without reading it,
+	// the coarse end's iterates are cleared.
 	int cycle()
 	{
 		const int ns = (int)sz.size();
-		const int stop = fused >= 0 ? fused : ns - 1;  // sizes [0, stop) are smoothed here
+		const int stop = smoothed_sizes();
 		for (int k = 0; k < stop; ++k) {
 			USize &F = sz[k], &C = sz[F.child];
 			const Dims2 df = F.dims(F.entries), dc = C.dims(F.entries);
-			CDR_TRY(smooth(F, CDR_DOWN));
+			CDR_TRY(smooth(F, CDR_DOWN, true));
 			CDR_TRY(residual_2d<float>(F.so32, F.ns, F.x32, F.b32, F.r32, df, nullptr, nullptr, st));
 			const size_t co = (size_t)F.child_off;
 			CDR_TRY(restrict_2d<float>(C.ci32 + co * 8 * C.plane(), F.r32, C.b32 + co * C.plane(), df, dc, st));
-			CDR_CUDA_TRY(cudaMemsetAsync(C.x32 + co * C.plane(), 0, sizeof(float) * C.plane() * F.entries, st));
+			if (F.child >= stop)
+				CDR_CUDA_TRY(cudaMemsetAsync(C.x32 + co * C.plane(), 0, sizeof(float) * C.plane() * F.entries, st));
 		}
 		if (fused >= 0) {
 			CoarseCycle<float> cc;
@@ -559,6 +573,7 @@ int cdr_gpu_batchmix_solve_device(cdr_gpu_batchmix *h, const double *const *b_de
 	int cur = 0, it = 0, bad = 0;
 	for (it = 0; it < h->s.maxiter && nactive > 0; ++it) {
 		for (Cls &C : h->cls) {
+			if (C.size[0] < h->smoothed_sizes()) continue;  // the cycle's first sweep treats it as zero
 			B2Level &F = C.B->lv[0];
 			const size_t n = F.plane() * C.nb;
 			k_zero_f32<<<(unsigned)std::min<size_t>((n + 255) / 256, 148 * 16), 256, 0, st>>>(F.x32, n);

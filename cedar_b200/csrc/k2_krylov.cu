@@ -71,6 +71,8 @@ __device__ __forceinline__ bool fcg_point(const Dims2 &d, int row, int &i, int &
 }
 
 // z = 0 at interior point (i, j) and, on the edges, at its ghost neighbours
+// (skipped when z is null: a cycle whose first sweep starts from zero without
+// reading its iterate)
 template <typename TZ>
 __device__ __forceinline__ void zero_z(TZ *__restrict__ z, size_t k, int i, int j, const Dims2 &d)
 {
@@ -217,7 +219,7 @@ __global__ void __launch_bounds__(TX *TY) k_fcg_update(const double *__restrict_
 			r[k] = rk;
 			acc[0] += rk * rk;
 			rin[k] = (TZ)rk;
-			zero_z(z, k, i, j, d);
+			if (z) zero_z(z, k, i, j, d);
 		}
 	grid_sums<1>(acc, partial, &S->ticket[2], [&](const double *v) {
 		S->rr = v[0];
@@ -254,7 +256,7 @@ __global__ void __launch_bounds__(TX *TY) k_fcg_update_rec(double *__restrict__ 
 			r[k] = rk;
 			acc[0] += rk * rk;
 			rin[k] = (TZ)rk;
-			zero_z(z, k, i, j, d);
+			if (z) zero_z(z, k, i, j, d);
 		}
 	grid_sums<1>(acc, partial, &S->ticket[2], [&](const double *v) {
 		S->rr = v[0];

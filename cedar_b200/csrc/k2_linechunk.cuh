@@ -197,7 +197,9 @@ __device__ __forceinline__ T yline_rhs(const T *__restrict__ so, size_t ps, cons
 // back.  g is the line's slot among the CTA's lines; sA/sB hold G*TPL/SG
 // scan totals.  Every thread of the CTA calls it.  CG (y-lines): the iterate is
 // read through L2 only (other CTAs of the launch have written it since).
-template <typename T, int NS, int DIR, int K, bool CG = false, bool XL = DIR == CDR_DIR_X>
+// ZERO: the iterate is zero on entry (its interior is not read), as at the
+// first sweep after a coarse-grid iterate is cleared.
+template <typename T, int NS, int DIR, int K, bool CG = false, bool ZERO = false, bool XL = DIR == CDR_DIR_X>
 __device__ __forceinline__ void line_chunk(const T *__restrict__ so, T *__restrict__ q, const T *__restrict__ qf,
                                            const T *__restrict__ sor, const Dims2 &d, int tpitch, int lc, int g,
                                            int t, int TPL, int G, T *sA, T *sB)
@@ -226,7 +228,23 @@ __device__ __forceinline__ void line_chunk(const T *__restrict__ so, T *__restri
 	T r[K];
 #pragma unroll
 	for (int m = 0; m < K; ++m) r[m] = T(0);
-	if (has) {
+	if (has && ZERO) {
+		// the iterate is zero: the right-hand side is b (b + a 0 for every
+		// coupling a, up to the sign of an exact zero); nothing else is read
+		if (DIR == CDR_DIR_X) {
+			const size_t k0 = d.at(p0, lc);
+			vload<T, K>(qf + k0, r);
+			if (xtra) rx = qf[k0 + K];
+		} else {
+#pragma unroll
+			for (int m = 0; m < K; ++m) {
+				const int jj = p0 + m;
+				if (jj < 1 || jj > n) continue;
+				r[m] = qf[d.at(lc, jj)];
+			}
+			if (xtra) rx = qf[d.at(lc, n)];
+		}
+	} else if (has) {
 		if (DIR == CDR_DIR_X) {
 			// operand order of relax_lines_x.f90:106-110, in stages so that only
 			// the two neighbour rows and one coupling row are live at a time
@@ -290,6 +308,11 @@ __device__ __forceinline__ void line_chunk(const T *__restrict__ so, T *__restri
 	// 2a. forward substitution y(p) = r(p) - y(p-1) E(p)
 	T Ev[K];
 	if (has) vload<T, K>(E + p0, Ev);
+	// short chunks: the pivots are loaded here too, before the scan's barriers
+	constexpr bool PRED = K <= 8;
+	T Dv[PRED ? K : 1];
+	if constexpr (PRED)
+		if (has) vload<T, K>(D + p0, Dv);
 	T A = T(1), B = T(0);
 	if (has) {
 #pragma unroll
@@ -321,7 +344,12 @@ __device__ __forceinline__ void line_chunk(const T *__restrict__ so, T *__restri
 #pragma unroll
 		for (int c = 0; c < K / W; ++c) {
 			T dv[W];
-			vload<T, W>(D + p0 + c * W, dv);
+			if constexpr (PRED) {
+#pragma unroll
+				for (int w = 0; w < W; ++w) dv[w] = Dv[c * W + w];
+			} else {
+				vload<T, W>(D + p0 + c * W, dv);
+			}
 #pragma unroll
 			for (int w = 0; w < W; ++w) {
 				const int m = c * W + w, pos = p0 + m;

@@ -31,6 +31,9 @@
 namespace cdrgpu {
 
 constexpr int LT = 256;  // threads per CTA
+// FP32 y-line CTAs of at most this many threads run a kernel instance built
+// for two such CTAs per SM (up to 128 registers per thread instead of 64)
+constexpr int YSMALL_BLOCK = 256;
 
 // ------------------------------------------------------------------ setup
 // BMG2_SymStd_SETUP_lines_{x,y} + DPTTRF: per line d = c, e = -w (x) or -s (y),
@@ -226,8 +229,8 @@ __global__ void __launch_bounds__(LT) k_lines(const T *__restrict__ so, T *__res
 // threads beyond G * TPL hold no chunk).  G * SG <= 32 for y-lines unless
 // TPL <= SG (the scan's groups lie inside a warp): a warp then reads 8 lines,
 // 16 columns of one row (two 32-byte sectors), per row of its chunks.
-template <typename T, int NS, int DIR, int K, bool XL = DIR == CDR_DIR_X>
-__global__ void __launch_bounds__(XL ? FAST_BLOCK_X : yblock_max<T>(), XL ? 2 : 1)
+template <typename T, int NS, int DIR, int K, int LB = 0, bool ZERO = false, bool XL = DIR == CDR_DIR_X>
+__global__ void __launch_bounds__(XL ? FAST_BLOCK_X : (LB ? LB : yblock_max<T>()), XL || LB ? 2 : 1)
     k_lines_fast(const T *__restrict__ so, T *__restrict__ q, const T *__restrict__ qf, const T *__restrict__ sor,
                  Dims2 d, int tpitch, int first, int tpl_log2, int G)
 {
@@ -238,7 +241,8 @@ __global__ void __launch_bounds__(XL ? FAST_BLOCK_X : yblock_max<T>(), XL ? 2 : 
 	int g, t;
 	if (XL) { g = tid >> tpl_log2; t = tid & (TPL - 1); }
 	else { g = tid % G; t = tid / G; }
-	line_chunk<T, NS, DIR, K>(so, q, qf, sor, d, tpitch, first + 2 * (blockIdx.x * G + g), g, t, TPL, G, sA, sB);
+	line_chunk<T, NS, DIR, K, false, ZERO>(so, q, qf, sor, d, tpitch, first + 2 * (blockIdx.x * G + g), g, t, TPL, G,
+	                                       sA, sB);
 }
 
 // Give-ups of the bounded waits of the line kernels (streamed x-lines, the
@@ -277,8 +281,8 @@ __device__ __forceinline__ unsigned ld_acquire(const unsigned *p)
 }
 }  // namespace
 
-template <typename T, int NS, int K>
-__global__ void __launch_bounds__(yblock_max<T>(), 1)
+template <typename T, int NS, int K, int LB = 0, bool Z1 = false>
+__global__ void __launch_bounds__(LB ? LB : yblock_max<T>(), LB ? 2 : 1)
     k_ylines_pair(const T *__restrict__ so, T *__restrict__ q, const T *__restrict__ qf, const T *__restrict__ sor,
                   Dims2 d, int tpitch, int c2, int tpl_log2, int G, unsigned *__restrict__ sync, int nvb)
 {
@@ -294,7 +298,7 @@ __global__ void __launch_bounds__(yblock_max<T>(), 1)
 	__syncthreads();
 	const int vb = s_vb;
 	const int p2 = 2 * (vb * G + g) + c2, p1 = p2 + 1;
-	line_chunk<T, NS, CDR_DIR_Y, K>(so, q, qf, sor, d, tpitch, p1, g, t, TPL, G, sA, sB);
+	line_chunk<T, NS, CDR_DIR_Y, K, false, Z1>(so, q, qf, sor, d, tpitch, p1, g, t, TPL, G, sA, sB);
 	__threadfence();  // this thread's phase-1 lines reach L2 before phase 2 reads them there
 	__syncthreads();  // phase 1 read and written by every thread
 	if (tid == 0) {
@@ -694,7 +698,7 @@ static LineShape shape_for(int n, int nl, int ns, int nb, int dir)
 
 template <typename T, int NS, int DIR, int K>
 static int launch_fast(const T *so, T *x, const T *b, const T *sor, Dims2 d, int tpitch, int first, int nlines,
-                       int cap, cudaStream_t st)
+                       int cap, cudaStream_t st, bool zero)
 {
 	const int n = DIR == CDR_DIR_X ? d.nx : d.ny;
 	const int tpl_log2 = tpl_log2_of(n, K);
@@ -707,8 +711,19 @@ static int launch_fast(const T *so, T *x, const T *b, const T *sor, Dims2 d, int
 		G = ylines_per_cta(TPL, cap);
 		block = (G * TPL + 31) / 32 * 32;
 	}
-	k_lines_fast<T, NS, DIR, K><<<dim3(ceil_div(nlines, G), 1, d.nb), block, 0, st>>>(so, x, b, sor, d, tpitch, first,
-	                                                                                  tpl_log2, G);
+	const dim3 grd(ceil_div(nlines, G), 1, d.nb);
+	constexpr bool ysmall = DIR == CDR_DIR_Y && sizeof(T) == 4;
+	if (ysmall && block <= YSMALL_BLOCK) {
+		constexpr int LB = ysmall ? YSMALL_BLOCK : 0;
+		if (zero)
+			k_lines_fast<T, NS, DIR, K, LB, true><<<grd, block, 0, st>>>(so, x, b, sor, d, tpitch, first, tpl_log2, G);
+		else
+			k_lines_fast<T, NS, DIR, K, LB><<<grd, block, 0, st>>>(so, x, b, sor, d, tpitch, first, tpl_log2, G);
+	} else if (zero) {
+		k_lines_fast<T, NS, DIR, K, 0, true><<<grd, block, 0, st>>>(so, x, b, sor, d, tpitch, first, tpl_log2, G);
+	} else {
+		k_lines_fast<T, NS, DIR, K><<<grd, block, 0, st>>>(so, x, b, sor, d, tpitch, first, tpl_log2, G);
+	}
 	CDR_LAUNCH_CHECK();
 	return CDR_OK;
 }
@@ -767,7 +782,7 @@ size_t lines_sync_words(Dims2 d) { return 2 + (size_t)d.nx / 2 + 1; }
 
 template <typename T, int NS, int K>
 static int launch_ypair(const T *so, T *x, const T *b, const T *sor, Dims2 d, int tpitch, int updown, int cap,
-                        unsigned *sync, cudaStream_t st)
+                        unsigned *sync, cudaStream_t st, bool zero = false)
 {
 	const int tpl_log2 = tpl_log2_of(d.ny, K), TPL = 1 << tpl_log2;
 	const int G = ylines_per_cta(TPL, cap);
@@ -775,35 +790,62 @@ static int launch_ypair(const T *so, T *x, const T *b, const T *sor, Dims2 d, in
 	// DOWN sweeps the even lines first (relax_lines_y.f90:82-97): pairs (odd, even)
 	const int c2 = updown == CDR_DOWN ? 1 : 0;
 	const int npairs = (d.nx - c2) / 2 + 1, nvb = ceil_div(npairs, G);
-	k_ylines_pair<T, NS, K><<<nvb, block, 0, st>>>(so, x, b, sor, d, tpitch, c2, tpl_log2, G, sync, nvb);
+	constexpr int LB = sizeof(T) == 4 ? YSMALL_BLOCK : 0;
+	const bool small = LB && block <= LB;
+	if (zero && small)
+		k_ylines_pair<T, NS, K, LB, true><<<nvb, block, 0, st>>>(so, x, b, sor, d, tpitch, c2, tpl_log2, G, sync, nvb);
+	else if (zero)
+		k_ylines_pair<T, NS, K, 0, true><<<nvb, block, 0, st>>>(so, x, b, sor, d, tpitch, c2, tpl_log2, G, sync, nvb);
+	else if (small)
+		k_ylines_pair<T, NS, K, LB><<<nvb, block, 0, st>>>(so, x, b, sor, d, tpitch, c2, tpl_log2, G, sync, nvb);
+	else
+		k_ylines_pair<T, NS, K><<<nvb, block, 0, st>>>(so, x, b, sor, d, tpitch, c2, tpl_log2, G, sync, nvb);
 	CDR_LAUNCH_CHECK();
 	return CDR_OK;
 }
 
+// The register-chunk kernels read whole 16-byte-aligned chunks of K elements:
+// rows (x) or factor lines (y) must have a pitch that is a multiple of K and
+// 16-byte aligned base pointers; lines up to 256*K points (16*256 FP32).
+template <typename T>
+static bool fast_lines_ok(const T *so, const T *x, const T *b, const T *sor, Dims2 d, int tpitch, int dir, bool exact)
+{
+	const int n = dir == CDR_DIR_X ? d.nx : d.ny;
+	const int fpitch = dir == CDR_DIR_X ? d.pitch : tpitch;
+	const bool aligned = ((uintptr_t)so | (uintptr_t)x | (uintptr_t)b | (uintptr_t)sor) % 16 == 0;
+	const int K = canon_K<T>(n, dir);
+	return !exact && aligned && d.pitch % 16 == 0 && fpitch % 16 == 0 && K != 0 &&
+	       (K == 8 || sizeof(T) == 4 || dir == CDR_DIR_Y);
+}
+
+// One colour of lines.  zero: x is zero on entry (the register-chunk kernels
+// only; the streamed x-line kernel's bits are the register-chunk kernel's).
 template <typename T, int NS, int DIR>
 static int launch_lines(const T *so, T *x, const T *b, const T *sor, Dims2 d, int tpitch, int first, bool exact,
-                        cudaStream_t st, const LineShape *force = nullptr)
+                        cudaStream_t st, const LineShape *force = nullptr, bool zero = false)
 {
 	const int n = DIR == CDR_DIR_X ? d.nx : d.ny;
 	const int nl = DIR == CDR_DIR_X ? d.ny : d.nx;
 	const int nlines = first > nl ? 0 : (nl - first) / 2 + 1;
 	if (nlines == 0) return CDR_OK;
-	// The register-chunk kernel reads whole 16-byte-aligned chunks of K elements:
-	// rows (x) or factor lines (y) must have a pitch that is a multiple of K and
-	// 16-byte aligned base pointers; lines up to 256*K points.
-	const int fpitch = DIR == CDR_DIR_X ? d.pitch : tpitch;
-	const bool aligned = ((uintptr_t)so | (uintptr_t)x | (uintptr_t)b | (uintptr_t)sor) % 16 == 0;
 	LineShape sh = force ? *force : shape_for<T>(n, nl, NS, d.nb, DIR);
 	if (!shape_ok<T>(sh, n, DIR)) sh = default_shape<T>(n, DIR, d.nb);
-	if (!exact && aligned && d.pitch % 16 == 0 && fpitch % 16 == 0 && shape_ok<T>(sh, n, DIR)) {
+	if (fast_lines_ok<T>(so, x, b, sor, d, tpitch, DIR, exact) && shape_ok<T>(sh, n, DIR)) {
 		if constexpr (DIR == CDR_DIR_X && sizeof(T) == 4)
-			if (sh.stream && xs_ok<T, NS>(d)) return launch_xstream<NS>(so, x, b, sor, d, first, nlines, st);
+			if (sh.stream && xs_ok<T, NS>(d)) {
+				if (!zero) return launch_xstream<NS>(so, x, b, sor, d, first, nlines, st);
+				sh.cap = FAST_BLOCK_X;
+			}
 		if (sh.K == 16) {
 			if constexpr (sizeof(T) == 4 || DIR == CDR_DIR_Y)
-				return launch_fast<T, NS, DIR, 16>(so, x, b, sor, d, tpitch, first, nlines, sh.cap, st);
+				return launch_fast<T, NS, DIR, 16>(so, x, b, sor, d, tpitch, first, nlines, sh.cap, st, zero);
 		} else {
-			return launch_fast<T, NS, DIR, 8>(so, x, b, sor, d, tpitch, first, nlines, sh.cap, st);
+			return launch_fast<T, NS, DIR, 8>(so, x, b, sor, d, tpitch, first, nlines, sh.cap, st, zero);
 		}
+	}
+	if (zero) {
+		set_error(CDR_ERR_ARG, "zero-start line sweep needs the register-chunk kernel");
+		return CDR_ERR_ARG;
 	}
 	const int G = lines_per_cta<T>(n, DIR);
 	size_t smem = sizeof(T) * (2 * LT + (size_t)G * n);
@@ -892,8 +934,8 @@ static int tune_dir(const T *so, T *x, const T *b, const T *sor, Dims2 d, int tp
 	LineShape best = default_shape<T>(n, DIR, d.nb);
 	float best_ms = time_shape(best);
 	// y-lines of a single problem: both colours in one launch or one launch per
-	// colour (the first re-reads the coupling columns from L2, the second has
-	// half the critical path per launch: it wins on small levels)
+	// colour (the default: the one-launch form's phase hand-over costs more than
+	// the second launch on a B200 at every size measured, 127^2 to 2047^2)
 	const int npair = DIR == CDR_DIR_Y && ysync && d.nb == 1 ? 2 : 1;
 	for (int pr = 0; pr < npair && rc == CDR_OK; ++pr)
 		for (int c = 0; c < 4 && rc == CDR_OK; ++c) {
@@ -961,36 +1003,46 @@ int relax_lines_2d(const T *so, int nstencil, T *x, const T *b, const T *sor, Di
                    int updown, int flags, cudaStream_t st, unsigned *ysync)
 {
 	const bool exact = (flags & CDR_LINES_EXACT) != 0;
+	bool zero = (flags & CDR_LINES_ZERO_START) != 0;
+	if (zero && !fast_lines_ok<T>(so, x, b, sor, d, tpitch, dir, exact)) {
+		// the sequential or shared-memory kernels read x: clear it (each of the
+		// batch's problems, bstep planes apart)
+		CDR_CUDA_TRY(cudaMemset2DAsync(x, sizeof(T) * (size_t)d.bstep * d.plane(), 0, sizeof(T) * d.plane(), d.nb, st));
+		zero = false;
+	}
 	const LineShape dflt = default_shape<T>(dir == CDR_DIR_X ? d.nx : d.ny, dir, d.nb);
 	const LineShape streamed{canon_K<T>(d.nx, CDR_DIR_X), FAST_BLOCK_X, 1};
 	const LineShape *force = (flags & CDR_LINES_NOTUNE) ? &dflt : nullptr;
 	if ((flags & CDR_LINES_STREAM) && dir == CDR_DIR_X) force = &streamed;
 	// y-lines of a single problem with a sync buffer: both colours in one launch
+	// where the tuned shape says so or the caller asks for it (CDR_LINES_YPAIR)
 	if (dir == CDR_DIR_Y && ysync && !exact && d.nb == 1 && d.nx >= 2 &&
 	    ((uintptr_t)so | (uintptr_t)x | (uintptr_t)b | (uintptr_t)sor) % 16 == 0 && d.pitch % 16 == 0 &&
 	    tpitch % 16 == 0) {
 		LineShape sh = force ? *force : shape_for<T>(d.ny, d.nx, nstencil, d.nb, dir);
 		if (!shape_ok<T>(sh, d.ny, dir)) sh = dflt;
-		if (shape_ok<T>(sh, d.ny, dir) && sh.pair) {
+		if (shape_ok<T>(sh, d.ny, dir) && (sh.pair || (flags & CDR_LINES_YPAIR))) {
 			if (sh.K == 16) {
-				if (nstencil == 5) return launch_ypair<T, 5, 16>(so, x, b, sor, d, tpitch, updown, sh.cap, ysync, st);
-				return launch_ypair<T, 3, 16>(so, x, b, sor, d, tpitch, updown, sh.cap, ysync, st);
+				if (nstencil == 5)
+					return launch_ypair<T, 5, 16>(so, x, b, sor, d, tpitch, updown, sh.cap, ysync, st, zero);
+				return launch_ypair<T, 3, 16>(so, x, b, sor, d, tpitch, updown, sh.cap, ysync, st, zero);
 			}
-			if (nstencil == 5) return launch_ypair<T, 5, 8>(so, x, b, sor, d, tpitch, updown, sh.cap, ysync, st);
-			return launch_ypair<T, 3, 8>(so, x, b, sor, d, tpitch, updown, sh.cap, ysync, st);
+			if (nstencil == 5) return launch_ypair<T, 5, 8>(so, x, b, sor, d, tpitch, updown, sh.cap, ysync, st, zero);
+			return launch_ypair<T, 3, 8>(so, x, b, sor, d, tpitch, updown, sh.cap, ysync, st, zero);
 		}
 	}
 	// DOWN: lines with Fortran start index 3 (0-based even) first, then 2 (odd);
 	// UP: the opposite (relax_lines_x.f90:82-97).
 	const int firsts[2] = {updown == CDR_DOWN ? 2 : 1, updown == CDR_DOWN ? 1 : 2};
 	for (int c = 0; c < 2; ++c) {
-		int f = firsts[c];
+		const int f = firsts[c];
+		const bool z = zero && c == 0;  // the second colour reads the first's new lines only
 		if (dir == CDR_DIR_X) {
-			if (nstencil == 5) CDR_TRY((launch_lines<T, 5, CDR_DIR_X>(so, x, b, sor, d, tpitch, f, exact, st, force)));
-			else CDR_TRY((launch_lines<T, 3, CDR_DIR_X>(so, x, b, sor, d, tpitch, f, exact, st, force)));
+			if (nstencil == 5) CDR_TRY((launch_lines<T, 5, CDR_DIR_X>(so, x, b, sor, d, tpitch, f, exact, st, force, z)));
+			else CDR_TRY((launch_lines<T, 3, CDR_DIR_X>(so, x, b, sor, d, tpitch, f, exact, st, force, z)));
 		} else {
-			if (nstencil == 5) CDR_TRY((launch_lines<T, 5, CDR_DIR_Y>(so, x, b, sor, d, tpitch, f, exact, st, force)));
-			else CDR_TRY((launch_lines<T, 3, CDR_DIR_Y>(so, x, b, sor, d, tpitch, f, exact, st, force)));
+			if (nstencil == 5) CDR_TRY((launch_lines<T, 5, CDR_DIR_Y>(so, x, b, sor, d, tpitch, f, exact, st, force, z)));
+			else CDR_TRY((launch_lines<T, 3, CDR_DIR_Y>(so, x, b, sor, d, tpitch, f, exact, st, force, z)));
 		}
 	}
 	return CDR_OK;

@@ -537,13 +537,13 @@ __global__ void __launch_bounds__(TX *TY) k_residual_wide(const float *__restric
 	}
 	if (lft && i0 + V - 1 <= d.nx) {
 		*reinterpret_cast<float4 *>(res + k) = make_float4(r[0], r[1], r[2], r[3]);
-		*reinterpret_cast<float4 *>(zero + k) = make_float4(0.f, 0.f, 0.f, 0.f);
+		if (zero) *reinterpret_cast<float4 *>(zero + k) = make_float4(0.f, 0.f, 0.f, 0.f);
 	} else {
 #pragma unroll
 		for (int m = 0; m < V; ++m)
 			if (i0 + m >= 1 && i0 + m <= d.nx) {
 				res[k + m] = r[m];
-				zero[k + m] = 0.f;
+				if (zero) zero[k + m] = 0.f;
 			}
 	}
 }

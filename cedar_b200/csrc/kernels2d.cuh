@@ -30,8 +30,8 @@ size_t lines_sync_words(Dims2 d);
 struct LineShape {
 	int K = 8, cap = 1024;
 	int stream = 0;  // x-lines: rows streamed into shared memory (k_lines_xstream)
-	int pair = 1;    // y-lines of a single problem with a sync buffer: both colours in one launch
-	                 // (k_ylines_pair), 0: one launch per colour (the same bits)
+	int pair = 0;    // y-lines of a single problem with a sync buffer: 1 both colours in one launch
+	                 // (k_ylines_pair), 0 one launch per colour (the same bits)
 };
 // bounded waits of the streamed x-line kernel that gave up since the last call
 // (read and reset into *count; 0 in a healthy run); CDR_ERR_CUDA if they
@@ -112,8 +112,9 @@ template <typename TZ>
 int fcg_load(const double *r, TZ *rin, TZ *z, Dims2 d, FcgScalars *S, cudaStream_t st, bool restart = true);
 // One FCG iteration after the preconditioner wrote its output, z (+ zf when
 // zf is not null: an FP64 part and an FP32 part), 3 launches; leaves the next
-// preconditioner input in rin, zz = 0 (the cycle's initial guess) and |r|^2
-// in S->rr.  x alternates between x0 and x1: after the step the iterate is in
+// preconditioner input in rin, zz = 0 (the cycle's initial guess; zz null:
+// left as it is, for a cycle that starts from zero without reading it) and
+// |r|^2 in S->rr.  x alternates between x0 and x1: after the step the iterate is in
 // x[S->iter & 1].
 template <typename TZ, typename TR>
 int fcg_step(const double *so, int ns, const TZ *z, const float *zf, TR *rin, TR *zz, double *x0, double *x1,

@@ -101,14 +101,16 @@ struct cdr_gpu_solver {
 	int L() const { return (int)lv.size(); }
 
 	// -------------------------------------------------------------- smoothing
+	// zero: x is zero on entry (its interior may hold anything; the ghost ring
+	// is zero): line sweeps start with CDR_LINES_ZERO_START, others clear x
 	template <typename T>
-	int smooth(int l, T *x, const T *b, int updown);
+	int smooth(int l, T *x, const T *b, int updown, bool zero = false);
 	template <typename T>
-	int ncycle(int l, T *x, const T *b);
+	int ncycle(int l, T *x, const T *b, bool zero = false);
 	template <typename T>
 	int fused(int l0);
 	template <typename T>
-	int cycle(T *x, const T *b);
+	int cycle(T *x, const T *b, bool zero = false);
 	template <typename T>
 	int coarse_solve(T *x, const T *b);
 	template <typename T>
@@ -150,28 +152,35 @@ template <> struct Arr<float> {
 
 // multilevel::setup_relax_helper smoother closures (include/cedar/multilevel.h:160-222)
 template <typename T>
-int cdr_gpu_solver::smooth(int l, T *x, const T *b, int updown)
+int cdr_gpu_solver::smooth(int l, T *x, const T *b, int updown, bool zero)
 {
 	Level &L = lv[l];
 	const int n = updown == CDR_DOWN ? s.nrelax_pre : s.nrelax_post;
 	const T *so = Arr<T>::so(L), *sor = Arr<T>::sor(L), *sory = Arr<T>::sory(L);
+	const bool lines = s.relaxation == CDR_RELAX_LINE_X || s.relaxation == CDR_RELAX_LINE_Y ||
+	                   s.relaxation == CDR_RELAX_LINE_XY;
+	if (zero && (n == 0 || !lines || per)) {  // only the line sweeps skip reading a zero iterate
+		CDR_CUDA_TRY(cudaMemsetAsync(x, 0, sizeof(T) * L.d.plane(), st));
+		zero = false;
+	}
 	for (int it = 0; it < n; ++it) {
+		// the first sweep of a zero iterate does not read it
+		const int f = lflags<T>() | (zero && it == 0 ? CDR_LINES_ZERO_START : 0);
 		switch (s.relaxation) {
 		case CDR_RELAX_POINT: CDR_TRY(relax_point_2d<T>(so, L.ns, x, b, sor, L.d, updown, st, per)); break;
 		case CDR_RELAX_LINE_X:
-			CDR_TRY(relax_lines_2d<T>(so, L.ns, x, b, sor, L.d, L.tpitch, CDR_DIR_X, updown, lflags<T>(), st));
+			CDR_TRY(relax_lines_2d<T>(so, L.ns, x, b, sor, L.d, L.tpitch, CDR_DIR_X, updown, f, st));
 			break;
 		case CDR_RELAX_LINE_Y:
-			CDR_TRY(relax_lines_2d<T>(so, L.ns, x, b, sory, L.d, L.tpitch, CDR_DIR_Y, updown, lflags<T>(), st, ysync));
+			CDR_TRY(relax_lines_2d<T>(so, L.ns, x, b, sory, L.d, L.tpitch, CDR_DIR_Y, updown, f, st, ysync));
 			break;
 		case CDR_RELAX_LINE_XY:
 			if (updown == CDR_DOWN) {
-				CDR_TRY(relax_lines_2d<T>(so, L.ns, x, b, sor, L.d, L.tpitch, CDR_DIR_X, updown, lflags<T>(), st));
+				CDR_TRY(relax_lines_2d<T>(so, L.ns, x, b, sor, L.d, L.tpitch, CDR_DIR_X, updown, f, st));
 				CDR_TRY(relax_lines_2d<T>(so, L.ns, x, b, sory, L.d, L.tpitch, CDR_DIR_Y, updown, lflags<T>(), st,
 				                          ysync));
 			} else {
-				CDR_TRY(relax_lines_2d<T>(so, L.ns, x, b, sory, L.d, L.tpitch, CDR_DIR_Y, updown, lflags<T>(), st,
-				                          ysync));
+				CDR_TRY(relax_lines_2d<T>(so, L.ns, x, b, sory, L.d, L.tpitch, CDR_DIR_Y, updown, f, st, ysync));
 				CDR_TRY(relax_lines_2d<T>(so, L.ns, x, b, sor, L.d, L.tpitch, CDR_DIR_X, updown, lflags<T>(), st));
 			}
 			break;
@@ -183,10 +192,10 @@ int cdr_gpu_solver::smooth(int l, T *x, const T *b, int updown)
 
 // cycle::vcycle::ncycle_helper (include/cedar/cycle/vcycle.h:57-115), n = 1
 template <typename T>
-int cdr_gpu_solver::ncycle(int l, T *x, const T *b)
+int cdr_gpu_solver::ncycle(int l, T *x, const T *b, bool zero)
 {
 	Level &F = lv[l], &C = lv[l + 1];
-	CDR_TRY(smooth<T>(l, x, b, CDR_DOWN));
+	CDR_TRY(smooth<T>(l, x, b, CDR_DOWN, zero));
 	CDR_TRY(residual_2d<T>(Arr<T>::so(F), F.ns, x, b, Arr<T>::r(F), F.d, nullptr, nullptr, st));
 	if constexpr (sizeof(T) == 4) {
 		if (l + 1 == s.fp32_levels) {  // FP32 -> FP64 hand-over: the coarse sub-cycle in FP64
@@ -200,10 +209,13 @@ int cdr_gpu_solver::ncycle(int l, T *x, const T *b)
 		}
 	}
 	CDR_TRY(restrict_to<T>(l, Arr<T>::r(F)));
-	CDR_CUDA_TRY(cudaMemsetAsync(Arr<T>::x(C), 0, sizeof(T) * C.d.plane(), st));
+	// coarse_x.set(0.0) (include/cedar/cycle/vcycle.h:79): the coarse cycle's
+	// first sweep treats its iterate as zero without reading it
+	const bool direct = l + 1 == L() - 1 || l + 1 == lc[sizeof(T) == 4];
+	if (direct) CDR_CUDA_TRY(cudaMemsetAsync(Arr<T>::x(C), 0, sizeof(T) * C.d.plane(), st));
 	if (l + 1 == L() - 1) CDR_TRY(coarse_solve<T>(Arr<T>::x(C), Arr<T>::b(C)));
 	else if (l + 1 == lc[sizeof(T) == 4]) CDR_TRY(fused<T>(l + 1));
-	else CDR_TRY(ncycle<T>(l + 1, Arr<T>::x(C), Arr<T>::b(C)));
+	else CDR_TRY(ncycle<T>(l + 1, Arr<T>::x(C), Arr<T>::b(C), true));
 	if constexpr (sizeof(T) == 4) {
 		if (l == 0 && wide) {
 			// the fine level's iterate goes on in FP64, xw = x + P x_c + r/c; the
@@ -211,8 +223,8 @@ int cdr_gpu_solver::ncycle(int l, T *x, const T *b)
 			// right-hand side b - A xw formed in FP64 over the difference form;
 			// the cycle's output is xw + x (read by the FCG step as two parts)
 			CDR_TRY(interp_add_2d_wide(C.ci32, C.x32, F.r32, F.so32, x, F.xw, F.d, C.d, st, F.ns));
-			CDR_TRY(residual_2d_wide(F.so32, F.dg32, F.ns, F.xw, b, F.r32, x, F.d, st));
-			return smooth<T>(l, x, F.r32, CDR_UP);
+			CDR_TRY(residual_2d_wide(F.so32, F.dg32, F.ns, F.xw, b, F.r32, nullptr, F.d, st));
+			return smooth<T>(l, x, F.r32, CDR_UP, true);
 		}
 	}
 	CDR_TRY(interp_from<T>(l, x));
@@ -336,11 +348,11 @@ int cdr_gpu_solver::fcycle(int l, T *x, const T *b)
 }
 
 template <typename T>
-int cdr_gpu_solver::cycle(T *x, const T *b)
+int cdr_gpu_solver::cycle(T *x, const T *b, bool zero)
 {
 	if (L() == 1) return coarse_solve<T>(x, b);
-	if (s.cycle == CDR_CYCLE_F) return fcycle<T>(0, x, b);
-	return ncycle<T>(0, x, b);
+	if (s.cycle == CDR_CYCLE_F) return fcycle<T>(0, x, b);  // discards x
+	return ncycle<T>(0, x, b, zero);
 }
 
 // One cycle on the level-0 work buffers, replayed from a CUDA graph when enabled.
@@ -348,7 +360,7 @@ int cdr_gpu_solver::run_cycle(int prec)
 {
 	auto body = [&]() -> int {
 		if (prec == 0) return cycle<double>(lv[0].x, lv[0].b);
-		return cycle<float>(lv[0].x32, lv[0].b32);
+		return cycle<float>(lv[0].x32, lv[0].b32, true);  // the refinement's correction starts at zero
 	};
 	if (!s.use_graph) return body();
 	if (!gexec[prec]) {
@@ -383,18 +395,20 @@ int cdr_gpu_solver::fcg_iteration(bool formed)
 	Level &F = lv[0];
 	T *z = Arr<T>::x(F), *rin = Arr<T>::b(F);
 	if constexpr (sizeof(T) == 4) {
-		if (F.xw) {  // the cycle's output is F.xw + z; the next cycle starts from z = 0
+		// every cycle starts from z = 0 without reading z (its first sweep treats
+		// the iterate as zero), so the step leaves z as it is
+		if (F.xw) {  // the cycle's output is F.xw + z
 			wide = true;
-			const int rc = cycle<T>(z, rin);
+			const int rc = cycle<T>(z, rin, true);
 			wide = false;
 			CDR_TRY(rc);
-			return fcg_step<double, float>(F.so, F.ns, F.xw, z, rin, z, kx[0], kx[1], kb, kr, kp[0], kp[1], kq, F.d,
-			                               kpart, ks, st, formed);
+			return fcg_step<double, float>(F.so, F.ns, F.xw, z, rin, (float *)nullptr, kx[0], kx[1], kb, kr, kp[0],
+			                               kp[1], kq, F.d, kpart, ks, st, formed);
 		}
 	}
-	CDR_TRY(cycle<T>(z, rin));
-	return fcg_step<T, T>(F.so, F.ns, z, nullptr, rin, z, kx[0], kx[1], kb, kr, kp[0], kp[1], kq, F.d, kpart, ks, st,
-	                      formed);
+	CDR_TRY(cycle<T>(z, rin, true));
+	return fcg_step<T, T>(F.so, F.ns, z, nullptr, rin, (T *)nullptr, kx[0], kx[1], kb, kr, kp[0], kp[1], kq, F.d, kpart,
+	                      ks, st, formed);
 }
 
 int cdr_gpu_solver::run_fcg(int prec, bool formed)
@@ -885,8 +899,7 @@ static int solve_loaded(cdr_gpu_solver *h, int *iters, double *hist, int maxhist
 		CDR_CUDA_TRY(cudaStreamSynchronize(st));
 		res0 = h->h_norm[0];
 		for (it = 0; it < h->s.maxiter;) {
-			CDR_CUDA_TRY(cudaMemsetAsync(F.x32, 0, sizeof(float) * F.d.plane(), st));
-			CDR_TRY(h->run_cycle(1));
+			CDR_TRY(h->run_cycle(1));  // the correction F.x32 from zero
 			CDR_TRY(ir_residual_2d(F.so, F.ns, h->x64[cur], F.x32, F.b, h->x64[1 - cur], F.b32, F.d, F.d, h->norm,
 			                       h->partial, 1, st));
 			cur = 1 - cur;

@@ -197,6 +197,17 @@ int cdr_gpu_setup_lines_2d_f32(const double *so, int nstencil, float *sor, int n
  * for FP32 x-lines longer than 1024 points, an autotuner candidate elsewhere
  * (other lines take the register-chunk kernel). */
 #define CDR_LINES_STREAM 4
+/* Kernel flags: x is zero on entry and its interior is not read (its ghost
+ * ring must be zero).  The first colour's right-hand sides are then b alone
+ * (b + a*0 for every coupling a, equal up to the sign of an exact zero), so the
+ * sweep neither clears x nor reads the couplings to the other colour for it:
+ * the first pre-smoothing sweep of a coarse level after restriction
+ * (coarse_x.set(0.0), include/cedar/cycle/vcycle.h:79). */
+#define CDR_LINES_ZERO_START 8
+/* Kernel flags, y-lines through cdr_gpu_relax_lines_2d_sync_*: both colours in
+ * one launch (blocks of column pairs, a bounded flag wait between neighbouring
+ * blocks) whatever shape the autotuner chose; the same bits as two launches. */
+#define CDR_LINES_YPAIR 16
 /* Status of the streamed x-line kernel since the last call, read on stream s
  * (synchronises it): CDR_ERR_NUMERIC if a CTA gave up waiting for its staged
  * rows (a bounded wait; the sweep's result is then incomplete), else CDR_OK.
@@ -223,15 +234,16 @@ int cdr_gpu_relax_lines_2d_f32(const float *so, int nstencil, float *x, const fl
                                cudaStream_t stream);
 /* The same sweep with a caller-owned sync buffer (device, cdr_gpu_lines_sync_words(nx)
  * unsigned words, zeroed before its first use; a sweep leaves it zeroed):
- * y-lines (scan mode, 16-byte aligned rows and factor lines) then run both
- * colours in one launch.  Blocks of column pairs draw their order from a
+ * y-lines (scan mode, 16-byte aligned rows and factor lines) may then run both
+ * colours in one launch, where the autotuner chose it for the level or flags
+ * hold CDR_LINES_YPAIR.  Blocks of column pairs draw their order from a
  * ticket; each solves its first-colour lines, raises a flag, waits (bounded,
  * as the streamed x-line kernel; a give-up is reported by
  * cdr_gpu_lines_stream_status) for the flag of the block before it and solves
- * its second-colour lines, so each coupling column is read from DRAM once per
- * sweep.  The result is bit-identical to the two-launch sweep.  One buffer per
- * stream: sweeps that run concurrently on one buffer race.  x-lines and the
- * other cases run as cdr_gpu_relax_lines_2d_*.  No counterpart in the reference. */
+ * its second-colour lines.  The result is bit-identical to the two-launch
+ * sweep.  One buffer per stream: sweeps that run concurrently on one buffer
+ * race.  x-lines and the other cases run as cdr_gpu_relax_lines_2d_*.  No
+ * counterpart in the reference. */
 size_t cdr_gpu_lines_sync_words(int nx);
 int cdr_gpu_relax_lines_2d_sync_f64(const double *so, int nstencil, double *x, const double *b, const double *sor,
                                     int nx, int ny, int pitch, int tpitch, int dir, int updown, int flags,

@@ -448,7 +448,55 @@ def test_one_launch_y_sweep_equals_two_launches(lib, precision, nx, ny, ns):
                 _lib.check(fn(ptr(dso), ns, ptr(d1), ptr(dbb), ptr(dsy), nx, ny, pitch, tpitch, _lib.DIR_Y, updown, 0,
                               stream()))
                 _lib.check(fns(ptr(dso), ns, ptr(d2), ptr(dbb), ptr(dsy), nx, ny, pitch, tpitch, _lib.DIR_Y, updown,
-                               0, ptr(sync), stream()))
+                               16, ptr(sync), stream()))  # CDR_LINES_YPAIR
             np.testing.assert_array_equal(host(d2), host(d1), err_msg="cap %d updown %d" % (cap, updown))
             assert int(sync.abs().sum().item()) == 0
+    assert lib.cdr_gpu_lines_stream_status(stream()) == 0
+
+
+@pytest.mark.parametrize("precision", ["f32", "f64"])
+@pytest.mark.parametrize("nx,ny,ns", [(37, 100, 5), (300, 41, 5), (64, 63, 3), (1023, 255, 5), (96, 2047, 5)])
+def test_zero_start_sweep_does_not_read_the_iterate(lib, precision, nx, ny, ns):
+    """CDR_LINES_ZERO_START (x zero on entry, its interior not read): a sweep of
+    an iterate whose interior holds garbage equals the sweep of a zero iterate,
+    x- and y-lines, both sweep directions, the one-launch y sweep, the streamed
+    x-line shape, and a pitch the register-chunk kernels cannot take (the sweep
+    then clears x itself)."""
+    import torch
+    dt = torch.float64 if precision == "f64" else torch.float32
+    fp32 = precision == "f32"
+    fn = lib.cdr_gpu_relax_lines_2d_f64 if not fp32 else lib.cdr_gpu_relax_lines_2d_f32
+    fns = lib.cdr_gpu_relax_lines_2d_sync_f64 if not fp32 else lib.cdr_gpu_relax_lines_2d_sync_f32
+    from oracle import oracle as O
+    so, junk, b = make_op(nx, ny, ns), grid(nx, ny, 8), grid(nx, ny, 9)
+    zero = np.zeros_like(junk)
+    sx, _ = O.setup_lines_x(so)
+    sy, _ = O.setup_lines_y(so)
+    gx, gy = sx.copy(), sy.copy()
+    if fp32:
+        gx[0][1:-1, 1:-1] = 1.0 / sx[0][1:-1, 1:-1]
+        gy[0][1:-1, 1:-1] = 1.0 / sy[0][1:-1, 1:-1]
+    sync = torch.zeros(lib.cdr_gpu_lines_sync_words(nx), dtype=torch.int32, device="cuda")
+    for pitch in (((nx + 2 + 31) // 32) * 32, nx + 3):
+        tpitch = ((ny + 2 + 31) // 32) * 32
+        dso, dbb = padded(so, pitch, dt), padded(b, pitch, dt)
+        dsx, dsy = padded(gx, pitch, dt), padded(gy, tpitch, dt)
+        for direction, fac in ((_lib.DIR_X, dsx), (_lib.DIR_Y, dsy)):
+            for updown in (0, 1):
+                for extra in ((0, 4) if direction == _lib.DIR_X and fp32 else (0,)):
+                    for use_sync in ((False, True) if direction == _lib.DIR_Y else (False,)):
+                        d1, d2 = padded(zero, pitch, dt), padded(junk, pitch, dt)
+                        if use_sync:  # both colours in one launch (CDR_LINES_YPAIR)
+                            _lib.check(fns(ptr(dso), ns, ptr(d1), ptr(dbb), ptr(fac), nx, ny, pitch, tpitch, direction,
+                                           updown, extra | 16, ptr(sync), stream()))
+                            _lib.check(fns(ptr(dso), ns, ptr(d2), ptr(dbb), ptr(fac), nx, ny, pitch, tpitch, direction,
+                                           updown, extra | 24, ptr(sync), stream()))
+                        else:
+                            _lib.check(fn(ptr(dso), ns, ptr(d1), ptr(dbb), ptr(fac), nx, ny, pitch, tpitch, direction,
+                                          updown, extra, stream()))
+                            _lib.check(fn(ptr(dso), ns, ptr(d2), ptr(dbb), ptr(fac), nx, ny, pitch, tpitch, direction,
+                                          updown, extra | 8, stream()))
+                        msg = "pitch %d dir %d updown %d flags %d sync %s" % (pitch, direction, updown, extra, use_sync)
+                        np.testing.assert_array_equal(host(d2), host(d1), err_msg=msg)
+    assert int(sync.abs().sum().item()) == 0
     assert lib.cdr_gpu_lines_stream_status(stream()) == 0
