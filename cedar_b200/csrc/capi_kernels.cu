@@ -198,6 +198,7 @@ size_t cdr_gpu_lines_sync_words(int nx) { return lines_sync_words(Dims2{nx > 0 ?
 LRELAX_SYNC_IMPL(double, f64)
 LRELAX_SYNC_IMPL(float, f32)
 
+
 #define RESTRICT_IMPL(T, SUF)                                                                                   \
 	int cdr_gpu_restrict_2d_##SUF(const T *ci, const T *rf, T *bc, int nxf, int nyf, int pf, int nxc, int nyc,  \
 	                              int pc, cudaStream_t s)                                                       \

@@ -52,6 +52,26 @@ __device__ __forceinline__ void vstore(T *__restrict__ p, const T (&v)[K])
 	}
 }
 
+// vload through L2 only (values other CTAs have written since the launch began)
+template <typename T, int K, bool CG>
+__device__ __forceinline__ void vload_q(const T *__restrict__ p, T (&v)[K])
+{
+	if constexpr (!CG) {
+		vload<T, K>(p, v);
+	} else {
+		using VT = typename Vec16<T>::type;
+		constexpr int W = 16 / sizeof(T);
+		const VT *pv = reinterpret_cast<const VT *>(p);
+#pragma unroll
+		for (int c = 0; c < K / W; ++c) {
+			VT t = __ldcg(pv + c);
+			const T *e = reinterpret_cast<const T *>(&t);
+#pragma unroll
+			for (int w = 0; w < W; ++w) v[c * W + w] = e[w];
+		}
+	}
+}
+
 // compose (A,B) <- (A,B) o (a2,b2): apply (a2,b2) first
 template <typename T>
 __device__ __forceinline__ void after(T &A, T &B, T a2, T b2)
@@ -195,15 +215,18 @@ __device__ __forceinline__ T yline_rhs(const T *__restrict__ so, size_t ps, cons
 // One chunk (t of TPL) of line lc (0: none) of the CTA's G lines, the whole
 // sweep of a line: right-hand sides, both substitutions by the scans, write
 // back.  g is the line's slot among the CTA's lines; sA/sB hold G*TPL/SG
-// scan totals.  Every thread of the CTA calls it.  CG (y-lines): the iterate is
+// scan totals.  Every thread of the CTA calls it.  CG: the iterate is
 // read through L2 only (other CTAs of the launch have written it since).
 // ZERO: the iterate is zero on entry (its interior is not read), as at the
-// first sweep after a coarse-grid iterate is cleared.
+// first sweep after a coarse-grid iterate is cleared.  nslots: line slots of
+// the CTA's scans when it holds several groups of G y-lines (g is then the
+// slot, G the lines of one group: the lane distance of a line's chunks).
 template <typename T, int NS, int DIR, int K, bool CG = false, bool ZERO = false, bool XL = DIR == CDR_DIR_X>
 __device__ __forceinline__ void line_chunk(const T *__restrict__ so, T *__restrict__ q, const T *__restrict__ qf,
                                            const T *__restrict__ sor, const Dims2 &d, int tpitch, int lc, int g,
-                                           int t, int TPL, int G, T *sA, T *sB)
+                                           int t, int TPL, int G, T *sA, T *sB, int nslots = 0)
 {
+	const int NL = nslots > 0 ? nslots : G;  // line slots of the CTA's scans (g < NL)
 	const int n = DIR == CDR_DIR_X ? d.nx : d.ny;
 	const int nl = DIR == CDR_DIR_X ? d.ny : d.nx;
 	const bool active = lc >= 1 && lc <= nl;
@@ -250,14 +273,17 @@ __device__ __forceinline__ void line_chunk(const T *__restrict__ so, T *__restri
 			// the two neighbour rows and one coupling row are live at a time
 			const size_t k0 = d.at(p0, lc);
 			const T *w = so + ps, *s = so + 2 * ps, *sw = so + 3 * ps, *nw = so + 4 * ps;
-			auto Q = [&](size_t i) -> T { return q[i]; };
+			auto Q = [&](size_t i) -> T {
+				if constexpr (CG) return __ldcg(q + i);
+				else return q[i];
+			};
 			T qm[K], qp[K], c[K];
 			vload<T, K>(qf + k0, r);
-			vload<T, K>(q + k0 - P, qm);
+			vload_q<T, K, CG>(q + k0 - P, qm);
 			vload<T, K>(s + k0, c);
 #pragma unroll
 			for (int m = 0; m < K; ++m) r[m] = madd(c[m], qm[m], r[m]);
-			vload<T, K>(q + k0 + P, qp);
+			vload_q<T, K, CG>(q + k0 + P, qp);
 			vload<T, K>(s + k0 + P, c);
 #pragma unroll
 			for (int m = 0; m < K; ++m) r[m] = madd(c[m], qp[m], r[m]);
@@ -329,7 +355,7 @@ __device__ __forceinline__ void line_chunk(const T *__restrict__ so, T *__restri
 			A = a * A;
 		}
 	}
-	T y = canon_incoming<T>(A, B, true, t, TPL, LS, g, G, sA, sB);
+	T y = canon_incoming<T>(A, B, true, t, TPL, LS, g, NL, sA, sB);
 	if (has) {
 #pragma unroll
 		for (int m = 0; m < K; ++m) {
@@ -376,7 +402,7 @@ __device__ __forceinline__ void line_chunk(const T *__restrict__ so, T *__restri
 			A = a * A;
 		}
 	}
-	T x = canon_incoming<T>(A, B, false, t, TPL, LS, g, G, sA, sB);
+	T x = canon_incoming<T>(A, B, false, t, TPL, LS, g, NL, sA, sB);
 	if (has) {
 		if (xtra) x = rx;
 #pragma unroll

@@ -439,6 +439,58 @@ __global__ void __launch_bounds__(TX *TY) k_interp_add_wide(const float *__restr
 	}
 }
 
+// The same interpolate-add by fine rows: thread (ic, jf) forms the fine points
+// (2ic - 2, jf) and (2ic - 1, jf) of row jf (a coarse row: the x-edge point and
+// the coarse point; otherwise the interior point and the y-edge point), with
+// k_interp_add_wide's arithmetic for each, so that a warp reads and writes 64
+// consecutive fine points of one row (8- and 16-byte accesses).  It covers the
+// points of k_interp_add_wide: ic = 1 .. nxf/2 + 1, jf = 1 .. 2 (nyf/2) + 1.
+__global__ void __launch_bounds__(256) k_interp_add_wide_rows(const float *__restrict__ ci,
+                                                             const float *__restrict__ qc,
+                                                             const float *__restrict__ res,
+                                                             const float *__restrict__ soc,
+                                                             const float *__restrict__ qin,
+                                                             double *__restrict__ qout, Dims2 f, Dims2 c)
+{
+	const int ic = blockIdx.x * blockDim.x + threadIdx.x + 1, jf = blockIdx.y + 1;
+	if (ic > f.nx / 2 + 1) return;
+	const size_t cps = c.plane();
+	const int cp = c.pitch;
+	const int i = 2 * ic - 1;
+	auto rc = [&](size_t k, int ii, int jj) -> double {
+		return (ii <= f.nx && jj <= f.ny) ? (double)res[k] / (double)soc[k] : (double)res[k];
+	};
+	auto W = [&](int plane, size_t k) -> double { return (double)ci[plane * cps + k]; };
+	auto QC = [&](size_t k) -> double { return (double)qc[k]; };
+	const size_t k = f.at(i, jf);  // i odd, rows 16-byte aligned: k - 1 is even
+	double v0 = 0.0, v1;           // points (i - 1, jf) and (i, jf)
+	float2 x01 = make_float2(0.f, 0.f);
+	if (ic >= 2) x01 = *reinterpret_cast<const float2 *>(qin + k - 1);
+	else x01.y = qin[k];
+	if (jf & 1) {  // coarse row jc: the x-edge point, then the coarse point
+		const size_t kc = c.at(ic, (jf + 1) / 2);
+		const double qcc = QC(kc);
+		v1 = (double)x01.y + qcc;
+		if (ic >= 2) {
+			const double a = W(IL, kc) * QC(kc - 1) + W(IR, kc) * qcc;
+			v0 = (double)x01.x + a + rc(k - 1, i - 1, jf);
+		}
+	} else {  // between coarse rows jc - 1 and jc: the interior point, then the y-edge point
+		const size_t kc = c.at(ic, jf / 2 + 1);
+		const double qcc = QC(kc);
+		const double a = W(IB, kc) * QC(kc - cp) + W(IA, kc) * qcc;
+		v1 = (double)x01.y + a + rc(k, i, jf);
+		if (ic >= 2) {
+			double b = W(INW, kc) * QC(kc - 1) + W(ISW, kc) * QC(kc - cp - 1);
+			b += W(INE, kc) * qcc;
+			b += W(ISE, kc) * QC(kc - cp);
+			v0 = (double)x01.x + b + rc(k - 1, i - 1, jf);
+		}
+	}
+	if (ic >= 2) *reinterpret_cast<double2 *>(qout + k - 1) = make_double2(v0, v1);
+	else qout[k] = v1;
+}
+
 // Row-sum excess of a level's operator, dg = c - (w(i,j) + w(i+1,j) + s(i,j) +
 // s(i,j+1) [+ sw(i,j) + sw(i+1,j+1) + nw(i+1,j) + nw(i,j+1)]), in FP64 and
 // rounded once.
@@ -566,8 +618,15 @@ int residual_2d_wide(const float *so, const float *dg, int ns, const double *x, 
 int interp_add_2d_wide(const float *ci, const float *xc, const float *rf, const float *sof, const float *xin,
                        double *xout, Dims2 f, Dims2 c, cudaStream_t st, int nsf)
 {
-	k_interp_add_wide<<<dim3(ceil_div(f.nx / 2 + 1, TX), ceil_div(f.ny / 2 + 1, TY), f.nb), dim3(TX, TY), 0, st>>>(
-	    ci, xc, rf, sof, xin, xout, f, c, nsf);
+	// rows of 16-byte alignment, a single problem: the row kernel; otherwise by
+	// 2 x 2 blocks of fine points
+	if (f.nb == 1 && f.pitch % 4 == 0 && ((uintptr_t)xin | (uintptr_t)xout) % 16 == 0) {
+		k_interp_add_wide_rows<<<dim3(ceil_div(f.nx / 2 + 1, 256), 2 * (f.ny / 2) + 1), 256, 0, st>>>(
+		    ci, xc, rf, sof, xin, xout, f, c);
+	} else {
+		k_interp_add_wide<<<dim3(ceil_div(f.nx / 2 + 1, TX), ceil_div(f.ny / 2 + 1, TY), f.nb), dim3(TX, TY), 0,
+		                    st>>>(ci, xc, rf, sof, xin, xout, f, c, nsf);
+	}
 	CDR_LAUNCH_CHECK();
 	return CDR_OK;
 }

@@ -117,12 +117,16 @@ def test_wide_interp_add_equals_fp64_interp_on_fp32_data(lib, nx, ny, ns):
     xc, r, x = f32(grid(nxc, nyc, 6)), f32(grid(nx, ny, 5)), f32(grid(nx, ny, 7))
     want = O.interp_add(ci, xc, r.copy(), so, x.copy())
     F = torch.float32
-    dout = torch.full((ny + 2, nx + 2), 3.0, dtype=torch.float64, device="cuda")
-    dci, dxc, dr, dso, dx = dev(ci, F), dev(xc, F), dev(r, F), dev(so, F), dev(x, F)
-    _lib.check(lib.cdr_gpu_interp_add_2d_wide(ptr(dci), ptr(dxc), ptr(dr), ptr(dso), ns, ptr(dx), ptr(dout), nx, ny,
-                                              nx + 2, nxc, nyc, nxc + 2, stream()))
-    got = host(dout)
-    np.testing.assert_array_equal(got[1:-1, 1:-1], want[1:-1, 1:-1])
+    dci, dxc = dev(ci, F), dev(xc, F)
+    # Cedar's pitch (2 x 2 blocks of fine points per thread) and a padded one
+    # (the row kernel: 16-byte rows)
+    for pitch in (nx + 2, ((nx + 2 + 31) // 32) * 32):
+        dout = torch.full((ny + 2, pitch), 3.0, dtype=torch.float64, device="cuda")
+        dr, dso, dx = padded(r, pitch, F), padded(so, pitch, F), padded(x, pitch, F)
+        _lib.check(lib.cdr_gpu_interp_add_2d_wide(ptr(dci), ptr(dxc), ptr(dr), ptr(dso), ns, ptr(dx), ptr(dout), nx,
+                                                  ny, pitch, nxc, nyc, nxc + 2, stream()))
+        got = host(dout)
+        np.testing.assert_array_equal(got[1:-1, 1:nx + 1], want[1:-1, 1:-1], err_msg="pitch %d" % pitch)
 
 
 def _fcg(so, b, prec, fine, tol=1e-4, levels=5):
