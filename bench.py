@@ -425,16 +425,20 @@ def main():
     p_sx, *_ = s32.level_info(0, "sor", fp32=True)
     p_sy, *_ = s32.level_info(0, "sory", fp32=True)
 
-    # the solver's own sweeps: x-lines two launches (one per colour), y-lines both colours in one launch
+    # the solver's own sweeps with its tuned launch shapes: x-lines two launches (one per colour),
+    # y-lines one or two launches, reading the packed couplings where the solver packed them (levels
+    # whose y-lines have at most 1024 points)
     ysync = torch.zeros(int(lib.cdr_gpu_lines_sync_words(nx)), dtype=torch.int32, device="cuda")
+    ypacked = ny <= 1024
 
     def sweep_time(dirn, p_f):
         reps = 20
+        flags = _lib.LINES_YPACKED if dirn == 1 and ypacked else 0
 
         def one():
             _lib.check(lib.cdr_gpu_relax_lines_2d_sync_f32(
                 ctypes.c_void_p(p_so), ns, ctypes.c_void_p(p_x), ctypes.c_void_p(p_b), ctypes.c_void_p(p_f), nx, ny,
-                pp, tp, dirn, 0, 0, ctypes.c_void_p(ysync.data_ptr()), ctypes.c_void_p(sh)))
+                pp, tp, dirn, 0, flags, ctypes.c_void_p(ysync.data_ptr()), ctypes.c_void_p(sh)))
         with torch.cuda.stream(stream):
             ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
             for _ in range(3):
@@ -493,10 +497,11 @@ def main():
                       "hbm_gbs": vcyc_bytes / (vc32["ms_per_cycle"] * 1e-3) / 1e9,
                       "fp64_ms": vc64["ms_per_cycle"],
                       "fp64_hbm_gbs": vcycle_bytes(vc64["solver"], word=8) / (vc64["ms_per_cycle"] * 1e-3) / 1e9},
-           "roofline": {"kernel": ("k_ylines_pair<float,%d,K=%d> (fine-level y-line sweep, both colours in one "
+           "roofline": {"kernel": ("k_ylines_pair<float,%d,K=%d> (fine-level y-line sweep%s, both colours in one "
                                    "launch)" if y_launches == 1 else
-                                   "k_lines_fast<float,%d,y,K=%d> (fine-level y-line sweep, one launch per colour)")
-                                  % (ns, shapes.get("y", {}).get("K", 0)), "line_shapes": shapes,
+                                   "k_lines_fast<float,%d,y,K=%d> (fine-level y-line sweep%s, one launch per colour)")
+                                  % (ns, shapes.get("y", {}).get("K", 0), ", packed couplings" if ypacked else ""),
+                        "line_shapes": shapes,
                         "bound": "hbm", "achieved": y_achieved, "peak": peak, "unit": "GB/s",
                         "frac": y_achieved / peak, "peak_kind": peak_kind,
                         "traffic": LINE_Y_TRAFFIC if n == 2047 else None,

@@ -24,6 +24,7 @@ LINES_NOTUNE = 2
 LINES_STREAM = 4
 LINES_ZERO_START = 8
 LINES_YPAIR = 16
+LINES_YPACKED = 32
 
 _lib = None
 
@@ -99,6 +100,7 @@ def load(path=LIB_PATH):
             "cdr_gpu_setup_lines_2d_" + suf: (I, [P, I, P, I, I, I, I, I, P, S]),
             "cdr_gpu_relax_lines_2d_" + suf: (I, [P, I, P, P, P, I, I, I, I, I, I, I, S]),
             "cdr_gpu_relax_lines_2d_sync_" + suf: (I, [P, I, P, P, P, I, I, I, I, I, I, I, P, S]),
+            "cdr_gpu_pack_ylines_2d_" + suf: (I, [P, I, P, I, I, I, I, S]),
             "cdr_gpu_restrict_2d_" + suf: (I, [P, P, P, I, I, I, I, I, I, S]),
             "cdr_gpu_interp_add_2d_" + suf: (I, [P, P, P, P, P, I, I, I, I, I, I, S]),
             "cdr_gpu_solve_cg_2d_" + suf: (I, [P, P, P, I, I, I, S]),

@@ -198,6 +198,18 @@ size_t cdr_gpu_lines_sync_words(int nx) { return lines_sync_words(Dims2{nx > 0 ?
 LRELAX_SYNC_IMPL(double, f64)
 LRELAX_SYNC_IMPL(float, f32)
 
+#define PACKY_IMPL(T, SUF)                                                                                       \
+	int cdr_gpu_pack_ylines_2d_##SUF(const T *so, int ns, T *sor, int nx, int ny, int pitch, int tpitch,         \
+	                                 cudaStream_t s)                                                            \
+	{                                                                                                           \
+		CDR_TRY(check_grid(nx, ny, pitch));                                                                     \
+		CDR_TRY(check_ns(ns));                                                                                  \
+		CDR_NONNULL(so); CDR_NONNULL(sor);                                                                      \
+		return pack_ylines_2d<T>(so, ns, sor, Dims2{nx, ny, pitch}, tpitch, s);                                 \
+	}
+PACKY_IMPL(double, f64)
+PACKY_IMPL(float, f32)
+
 
 #define RESTRICT_IMPL(T, SUF)                                                                                   \
 	int cdr_gpu_restrict_2d_##SUF(const T *ci, const T *rf, T *bc, int nxf, int nyf, int pf, int nxc, int nyc,  \

@@ -221,7 +221,10 @@ __device__ __forceinline__ T yline_rhs(const T *__restrict__ so, size_t ps, cons
 // first sweep after a coarse-grid iterate is cleared.  nslots: line slots of
 // the CTA's scans when it holds several groups of G y-lines (g is then the
 // slot, G the lines of one group: the lane distance of a line's chunks).
-template <typename T, int NS, int DIR, int K, bool CG = false, bool ZERO = false, bool XL = DIR == CDR_DIR_X>
+// PACK (y-lines): the factor array holds, after the two factor planes, the
+// line's couplings in line order (pack_ylines_2d), read as vectors.
+template <typename T, int NS, int DIR, int K, bool CG = false, bool ZERO = false, bool PACK = false,
+          bool XL = DIR == CDR_DIR_X>
 __device__ __forceinline__ void line_chunk(const T *__restrict__ so, T *__restrict__ q, const T *__restrict__ qf,
                                            const T *__restrict__ sor, const Dims2 &d, int tpitch, int lc, int g,
                                            int t, int TPL, int G, T *sA, T *sB, int nslots = 0)
@@ -316,6 +319,59 @@ __device__ __forceinline__ void line_chunk(const T *__restrict__ so, T *__restri
 					rx = madd(sw[kx + P + 1], Q(kx + P + 1), a);
 				}
 			}
+		} else if constexpr (PACK) {
+			// yline_rhs's operations in its order, the couplings from the line's
+			// packed planes (vector loads), the neighbour columns' rows loaded once
+			// per half-chunk of 8 positions
+			auto Q = [&](size_t e) -> T {
+				if constexpr (CG) return __ldcg(q + e);
+				else return q[e];
+			};
+			const size_t fps = (size_t)tpitch * (d.nx + 2);
+			const T *cpl = sor + 2 * fps + (size_t)lc * tpitch;  // plane m at cpl + m * fps
+			const size_t kq = d.at(lc, 0);
+			constexpr int H = 8;
+			static_assert(K % H == 0, "half-chunks of 8");
+#pragma unroll
+			for (int h = 0; h < K; h += H) {
+				T qL[H + 2], qR[H + 2];  // columns lc - 1 and lc + 1, rows p0 + h - 1 .. p0 + h + H
+#pragma unroll
+				for (int e = 0; e < H + 2; ++e) {
+					const int row = p0 + h - 1 + e;
+					const bool in = row >= 0 && row <= n + 1;
+					qL[e] = in ? Q(kq + (size_t)row * P - 1) : T(0);
+					qR[e] = in ? Q(kq + (size_t)row * P + 1) : T(0);
+				}
+				T a[H], c[H];
+#pragma unroll
+				for (int m = 0; m < H; ++m) {
+					const int pos = p0 + h + m;
+					a[m] = pos >= 1 && pos <= n ? qf[kq + (size_t)pos * P] : T(0);
+				}
+				vload<T, H>(cpl + p0 + h, c);  // w(i, j)
+#pragma unroll
+				for (int m = 0; m < H; ++m) a[m] = madd(c[m], qL[m + 1], a[m]);
+				vload<T, H>(cpl + fps + p0 + h, c);  // w(i+1, j)
+#pragma unroll
+				for (int m = 0; m < H; ++m) a[m] = madd(c[m], qR[m + 1], a[m]);
+				if (NS == 5) {
+					vload<T, H>(cpl + 2 * fps + p0 + h, c);  // sw(i, j)
+#pragma unroll
+					for (int m = 0; m < H; ++m) a[m] = madd(c[m], qL[m], a[m]);
+					vload<T, H>(cpl + 3 * fps + p0 + h, c);  // nw(i+1, j)
+#pragma unroll
+					for (int m = 0; m < H; ++m) a[m] = madd(c[m], qR[m], a[m]);
+					vload<T, H>(cpl + 4 * fps + p0 + h, c);  // nw(i, j+1)
+#pragma unroll
+					for (int m = 0; m < H; ++m) a[m] = madd(c[m], qL[m + 2], a[m]);
+					vload<T, H>(cpl + 5 * fps + p0 + h, c);  // sw(i+1, j+1)
+#pragma unroll
+					for (int m = 0; m < H; ++m) a[m] = madd(c[m], qR[m + 2], a[m]);
+				}
+#pragma unroll
+				for (int m = 0; m < H; ++m) r[h + m] = a[m];
+			}
+			if (xtra) rx = yline_rhs<T, NS, CG>(so, ps, q, qf, d.at(lc, n), P);
 		} else {
 			const int i = lc;
 #pragma unroll

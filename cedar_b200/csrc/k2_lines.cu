@@ -229,7 +229,8 @@ __global__ void __launch_bounds__(LT) k_lines(const T *__restrict__ so, T *__res
 // threads beyond G * TPL hold no chunk).  G * SG <= 32 for y-lines unless
 // TPL <= SG (the scan's groups lie inside a warp): a warp then reads 8 lines,
 // 16 columns of one row (two 32-byte sectors), per row of its chunks.
-template <typename T, int NS, int DIR, int K, int LB = 0, bool ZERO = false, bool XL = DIR == CDR_DIR_X>
+template <typename T, int NS, int DIR, int K, int LB = 0, bool ZERO = false, bool PACK = false,
+          bool XL = DIR == CDR_DIR_X>
 __global__ void __launch_bounds__(XL ? FAST_BLOCK_X : (LB ? LB : yblock_max<T>()), XL || LB ? 2 : 1)
     k_lines_fast(const T *__restrict__ so, T *__restrict__ q, const T *__restrict__ qf, const T *__restrict__ sor,
                  Dims2 d, int tpitch, int first, int tpl_log2, int G)
@@ -241,8 +242,8 @@ __global__ void __launch_bounds__(XL ? FAST_BLOCK_X : (LB ? LB : yblock_max<T>()
 	int g, t;
 	if (XL) { g = tid >> tpl_log2; t = tid & (TPL - 1); }
 	else { g = tid % G; t = tid / G; }
-	line_chunk<T, NS, DIR, K, false, ZERO>(so, q, qf, sor, d, tpitch, first + 2 * (blockIdx.x * G + g), g, t, TPL, G,
-	                                       sA, sB);
+	line_chunk<T, NS, DIR, K, false, ZERO, PACK>(so, q, qf, sor, d, tpitch, first + 2 * (blockIdx.x * G + g), g, t,
+	                                             TPL, G, sA, sB);
 }
 
 // Give-ups of the bounded waits of the line kernels (streamed x-lines, the
@@ -281,7 +282,7 @@ __device__ __forceinline__ unsigned ld_acquire(const unsigned *p)
 }
 }  // namespace
 
-template <typename T, int NS, int K, int LB = 0, bool Z1 = false>
+template <typename T, int NS, int K, int LB = 0, bool Z1 = false, bool PK = false>
 __global__ void __launch_bounds__(LB ? LB : yblock_max<T>(), LB ? 2 : 1)
     k_ylines_pair(const T *__restrict__ so, T *__restrict__ q, const T *__restrict__ qf, const T *__restrict__ sor,
                   Dims2 d, int tpitch, int c2, int tpl_log2, int G, unsigned *__restrict__ sync, int nvb)
@@ -298,7 +299,7 @@ __global__ void __launch_bounds__(LB ? LB : yblock_max<T>(), LB ? 2 : 1)
 	__syncthreads();
 	const int vb = s_vb;
 	const int p2 = 2 * (vb * G + g) + c2, p1 = p2 + 1;
-	line_chunk<T, NS, CDR_DIR_Y, K, false, Z1>(so, q, qf, sor, d, tpitch, p1, g, t, TPL, G, sA, sB);
+	line_chunk<T, NS, CDR_DIR_Y, K, false, Z1, PK && !Z1>(so, q, qf, sor, d, tpitch, p1, g, t, TPL, G, sA, sB);
 	__threadfence();  // this thread's phase-1 lines reach L2 before phase 2 reads them there
 	__syncthreads();  // phase 1 read and written by every thread
 	if (tid == 0) {
@@ -329,7 +330,7 @@ __global__ void __launch_bounds__(LB ? LB : yblock_max<T>(), LB ? 2 : 1)
 	}
 	__syncthreads();
 	if (!s_ok) return;
-	line_chunk<T, NS, CDR_DIR_Y, K, true>(so, q, qf, sor, d, tpitch, p2, g, t, TPL, G, sA, sB);
+	line_chunk<T, NS, CDR_DIR_Y, K, true, false, PK>(so, q, qf, sor, d, tpitch, p2, g, t, TPL, G, sA, sB);
 }
 
 // ---------------------------------------------------------- streamed x-lines
@@ -698,7 +699,7 @@ static LineShape shape_for(int n, int nl, int ns, int nb, int dir)
 
 template <typename T, int NS, int DIR, int K>
 static int launch_fast(const T *so, T *x, const T *b, const T *sor, Dims2 d, int tpitch, int first, int nlines,
-                       int cap, cudaStream_t st, bool zero)
+                       int cap, cudaStream_t st, bool zero, bool pack = false)
 {
 	const int n = DIR == CDR_DIR_X ? d.nx : d.ny;
 	const int tpl_log2 = tpl_log2_of(n, K);
@@ -713,6 +714,19 @@ static int launch_fast(const T *so, T *x, const T *b, const T *sor, Dims2 d, int
 	}
 	const dim3 grd(ceil_div(nlines, G), 1, d.nb);
 	constexpr bool ysmall = DIR == CDR_DIR_Y && sizeof(T) == 4;
+	if constexpr (DIR == CDR_DIR_Y) {
+		// packed couplings (zero-start sweeps read no couplings)
+		if (pack && !zero) {
+			if (ysmall && block <= YSMALL_BLOCK)
+				k_lines_fast<T, NS, DIR, K, ysmall ? YSMALL_BLOCK : 0, false, true><<<grd, block, 0, st>>>(
+				    so, x, b, sor, d, tpitch, first, tpl_log2, G);
+			else
+				k_lines_fast<T, NS, DIR, K, 0, false, true><<<grd, block, 0, st>>>(so, x, b, sor, d, tpitch, first,
+				                                                                    tpl_log2, G);
+			CDR_LAUNCH_CHECK();
+			return CDR_OK;
+		}
+	}
 	if (ysmall && block <= YSMALL_BLOCK) {
 		constexpr int LB = ysmall ? YSMALL_BLOCK : 0;
 		if (zero)
@@ -782,7 +796,7 @@ size_t lines_sync_words(Dims2 d) { return 2 + (size_t)d.nx / 2 + 1; }
 
 template <typename T, int NS, int K>
 static int launch_ypair(const T *so, T *x, const T *b, const T *sor, Dims2 d, int tpitch, int updown, int cap,
-                        unsigned *sync, cudaStream_t st, bool zero = false)
+                        unsigned *sync, cudaStream_t st, bool zero = false, bool pack = false)
 {
 	const int tpl_log2 = tpl_log2_of(d.ny, K), TPL = 1 << tpl_log2;
 	const int G = ylines_per_cta(TPL, cap);
@@ -792,14 +806,26 @@ static int launch_ypair(const T *so, T *x, const T *b, const T *sor, Dims2 d, in
 	const int npairs = (d.nx - c2) / 2 + 1, nvb = ceil_div(npairs, G);
 	constexpr int LB = sizeof(T) == 4 ? YSMALL_BLOCK : 0;
 	const bool small = LB && block <= LB;
-	if (zero && small)
-		k_ylines_pair<T, NS, K, LB, true><<<nvb, block, 0, st>>>(so, x, b, sor, d, tpitch, c2, tpl_log2, G, sync, nvb);
-	else if (zero)
-		k_ylines_pair<T, NS, K, 0, true><<<nvb, block, 0, st>>>(so, x, b, sor, d, tpitch, c2, tpl_log2, G, sync, nvb);
-	else if (small)
-		k_ylines_pair<T, NS, K, LB><<<nvb, block, 0, st>>>(so, x, b, sor, d, tpitch, c2, tpl_log2, G, sync, nvb);
-	else
-		k_ylines_pair<T, NS, K><<<nvb, block, 0, st>>>(so, x, b, sor, d, tpitch, c2, tpl_log2, G, sync, nvb);
+	// zero start and packed couplings: the first colour reads b only, the second the packed couplings
+	if (small) {
+		if (zero && pack)
+			k_ylines_pair<T, NS, K, LB, true, true><<<nvb, block, 0, st>>>(so, x, b, sor, d, tpitch, c2, tpl_log2, G, sync, nvb);
+		else if (zero)
+			k_ylines_pair<T, NS, K, LB, true><<<nvb, block, 0, st>>>(so, x, b, sor, d, tpitch, c2, tpl_log2, G, sync, nvb);
+		else if (pack)
+			k_ylines_pair<T, NS, K, LB, false, true><<<nvb, block, 0, st>>>(so, x, b, sor, d, tpitch, c2, tpl_log2, G, sync, nvb);
+		else
+			k_ylines_pair<T, NS, K, LB><<<nvb, block, 0, st>>>(so, x, b, sor, d, tpitch, c2, tpl_log2, G, sync, nvb);
+	} else {
+		if (zero && pack)
+			k_ylines_pair<T, NS, K, 0, true, true><<<nvb, block, 0, st>>>(so, x, b, sor, d, tpitch, c2, tpl_log2, G, sync, nvb);
+		else if (zero)
+			k_ylines_pair<T, NS, K, 0, true><<<nvb, block, 0, st>>>(so, x, b, sor, d, tpitch, c2, tpl_log2, G, sync, nvb);
+		else if (pack)
+			k_ylines_pair<T, NS, K, 0, false, true><<<nvb, block, 0, st>>>(so, x, b, sor, d, tpitch, c2, tpl_log2, G, sync, nvb);
+		else
+			k_ylines_pair<T, NS, K><<<nvb, block, 0, st>>>(so, x, b, sor, d, tpitch, c2, tpl_log2, G, sync, nvb);
+	}
 	CDR_LAUNCH_CHECK();
 	return CDR_OK;
 }
@@ -822,7 +848,7 @@ static bool fast_lines_ok(const T *so, const T *x, const T *b, const T *sor, Dim
 // only; the streamed x-line kernel's bits are the register-chunk kernel's).
 template <typename T, int NS, int DIR>
 static int launch_lines(const T *so, T *x, const T *b, const T *sor, Dims2 d, int tpitch, int first, bool exact,
-                        cudaStream_t st, const LineShape *force = nullptr, bool zero = false)
+                        cudaStream_t st, const LineShape *force = nullptr, bool zero = false, bool pack = false)
 {
 	const int n = DIR == CDR_DIR_X ? d.nx : d.ny;
 	const int nl = DIR == CDR_DIR_X ? d.ny : d.nx;
@@ -838,9 +864,9 @@ static int launch_lines(const T *so, T *x, const T *b, const T *sor, Dims2 d, in
 			}
 		if (sh.K == 16) {
 			if constexpr (sizeof(T) == 4 || DIR == CDR_DIR_Y)
-				return launch_fast<T, NS, DIR, 16>(so, x, b, sor, d, tpitch, first, nlines, sh.cap, st, zero);
+				return launch_fast<T, NS, DIR, 16>(so, x, b, sor, d, tpitch, first, nlines, sh.cap, st, zero, pack);
 		} else {
-			return launch_fast<T, NS, DIR, 8>(so, x, b, sor, d, tpitch, first, nlines, sh.cap, st, zero);
+			return launch_fast<T, NS, DIR, 8>(so, x, b, sor, d, tpitch, first, nlines, sh.cap, st, zero, pack);
 		}
 	}
 	if (zero) {
@@ -863,7 +889,7 @@ static int launch_lines(const T *so, T *x, const T *b, const T *sor, Dims2 d, in
 
 template <typename T, int NS, int DIR>
 static int tune_dir(const T *so, T *x, const T *b, const T *sor, Dims2 d, int tpitch, cudaStream_t st,
-                    unsigned *ysync)
+                    unsigned *ysync, bool pack)
 {
 	const int n = DIR == CDR_DIR_X ? d.nx : d.ny;
 	const int nl = DIR == CDR_DIR_X ? d.ny : d.nx;
@@ -909,11 +935,11 @@ static int tune_dir(const T *so, T *x, const T *b, const T *sor, Dims2 d, int tp
 				break;
 			}
 			if (DIR == CDR_DIR_Y && ysync && d.nb == 1 && sh.pair) {  // both colours in one launch
-				rc = sh.K == 16 ? launch_ypair<T, NS, 16>(so, x, b, sor, d, tpitch, CDR_DOWN, sh.cap, ysync, st)
-				                : launch_ypair<T, NS, 8>(so, x, b, sor, d, tpitch, CDR_DOWN, sh.cap, ysync, st);
+				rc = sh.K == 16 ? launch_ypair<T, NS, 16>(so, x, b, sor, d, tpitch, CDR_DOWN, sh.cap, ysync, st, false, pack)
+				                : launch_ypair<T, NS, 8>(so, x, b, sor, d, tpitch, CDR_DOWN, sh.cap, ysync, st, false, pack);
 			} else {
 				for (int f = 1; f <= 2 && rc == CDR_OK; ++f)
-					rc = launch_lines<T, NS, DIR>(so, x, b, sor, d, tpitch, f, false, st, &sh);
+					rc = launch_lines<T, NS, DIR>(so, x, b, sor, d, tpitch, f, false, st, &sh, false, pack);
 			}
 			if (rc != CDR_OK) break;
 			float t = 0.f;
@@ -963,19 +989,19 @@ static int tune_dir(const T *so, T *x, const T *b, const T *sor, Dims2 d, int tp
 
 template <typename T>
 int lines_autotune(const T *so, int nstencil, T *x, const T *b, const T *sor, Dims2 d, int tpitch, int dir,
-                   cudaStream_t st, unsigned *ysync)
+                   cudaStream_t st, unsigned *ysync, bool ypack)
 {
 	if (dir == CDR_DIR_X) {
-		if (nstencil == 5) return tune_dir<T, 5, CDR_DIR_X>(so, x, b, sor, d, tpitch, st, ysync);
-		return tune_dir<T, 3, CDR_DIR_X>(so, x, b, sor, d, tpitch, st, ysync);
+		if (nstencil == 5) return tune_dir<T, 5, CDR_DIR_X>(so, x, b, sor, d, tpitch, st, ysync, false);
+		return tune_dir<T, 3, CDR_DIR_X>(so, x, b, sor, d, tpitch, st, ysync, false);
 	}
-	if (nstencil == 5) return tune_dir<T, 5, CDR_DIR_Y>(so, x, b, sor, d, tpitch, st, ysync);
-	return tune_dir<T, 3, CDR_DIR_Y>(so, x, b, sor, d, tpitch, st, ysync);
+	if (nstencil == 5) return tune_dir<T, 5, CDR_DIR_Y>(so, x, b, sor, d, tpitch, st, ysync, ypack);
+	return tune_dir<T, 3, CDR_DIR_Y>(so, x, b, sor, d, tpitch, st, ysync, ypack);
 }
 template int lines_autotune<double>(const double *, int, double *, const double *, const double *, Dims2, int, int,
-                                    cudaStream_t, unsigned *);
+                                    cudaStream_t, unsigned *, bool);
 template int lines_autotune<float>(const float *, int, float *, const float *, const float *, Dims2, int, int,
-                                   cudaStream_t, unsigned *);
+                                   cudaStream_t, unsigned *, bool);
 
 bool lines_set_shape(int dir, int tsize, int ns, int n, int nl, int nb, LineShape sh)
 {
@@ -1022,18 +1048,22 @@ int relax_lines_2d(const T *so, int nstencil, T *x, const T *b, const T *sor, Di
 		LineShape sh = force ? *force : shape_for<T>(d.ny, d.nx, nstencil, d.nb, dir);
 		if (!shape_ok<T>(sh, d.ny, dir)) sh = dflt;
 		if (shape_ok<T>(sh, d.ny, dir) && (sh.pair || (flags & CDR_LINES_YPAIR))) {
+			const bool pk = (flags & CDR_LINES_YPACKED) != 0;
 			if (sh.K == 16) {
 				if (nstencil == 5)
-					return launch_ypair<T, 5, 16>(so, x, b, sor, d, tpitch, updown, sh.cap, ysync, st, zero);
-				return launch_ypair<T, 3, 16>(so, x, b, sor, d, tpitch, updown, sh.cap, ysync, st, zero);
+					return launch_ypair<T, 5, 16>(so, x, b, sor, d, tpitch, updown, sh.cap, ysync, st, zero, pk);
+				return launch_ypair<T, 3, 16>(so, x, b, sor, d, tpitch, updown, sh.cap, ysync, st, zero, pk);
 			}
-			if (nstencil == 5) return launch_ypair<T, 5, 8>(so, x, b, sor, d, tpitch, updown, sh.cap, ysync, st, zero);
-			return launch_ypair<T, 3, 8>(so, x, b, sor, d, tpitch, updown, sh.cap, ysync, st, zero);
+			if (nstencil == 5)
+				return launch_ypair<T, 5, 8>(so, x, b, sor, d, tpitch, updown, sh.cap, ysync, st, zero, pk);
+			return launch_ypair<T, 3, 8>(so, x, b, sor, d, tpitch, updown, sh.cap, ysync, st, zero, pk);
 		}
 	}
 	// DOWN: lines with Fortran start index 3 (0-based even) first, then 2 (odd);
 	// UP: the opposite (relax_lines_x.f90:82-97).
 	const int firsts[2] = {updown == CDR_DOWN ? 2 : 1, updown == CDR_DOWN ? 1 : 2};
+	// y-lines of a single problem whose factor array carries the packed couplings
+	const bool pack = (flags & CDR_LINES_YPACKED) && dir == CDR_DIR_Y && d.nb == 1;
 	for (int c = 0; c < 2; ++c) {
 		const int f = firsts[c];
 		const bool z = zero && c == 0;  // the second colour reads the first's new lines only
@@ -1041,8 +1071,9 @@ int relax_lines_2d(const T *so, int nstencil, T *x, const T *b, const T *sor, Di
 			if (nstencil == 5) CDR_TRY((launch_lines<T, 5, CDR_DIR_X>(so, x, b, sor, d, tpitch, f, exact, st, force, z)));
 			else CDR_TRY((launch_lines<T, 3, CDR_DIR_X>(so, x, b, sor, d, tpitch, f, exact, st, force, z)));
 		} else {
-			if (nstencil == 5) CDR_TRY((launch_lines<T, 5, CDR_DIR_Y>(so, x, b, sor, d, tpitch, f, exact, st, force, z)));
-			else CDR_TRY((launch_lines<T, 3, CDR_DIR_Y>(so, x, b, sor, d, tpitch, f, exact, st, force, z)));
+			if (nstencil == 5)
+				CDR_TRY((launch_lines<T, 5, CDR_DIR_Y>(so, x, b, sor, d, tpitch, f, exact, st, force, z, pack)));
+			else CDR_TRY((launch_lines<T, 3, CDR_DIR_Y>(so, x, b, sor, d, tpitch, f, exact, st, force, z, pack)));
 		}
 	}
 	return CDR_OK;
@@ -1051,5 +1082,50 @@ template int relax_lines_2d<double>(const double *, int, double *, const double 
                                     int, int, cudaStream_t, unsigned *);
 template int relax_lines_2d<float>(const float *, int, float *, const float *, const float *, Dims2, int, int, int,
                                    int, cudaStream_t, unsigned *);
+
+// ---------------------------------------------------- packed y-line couplings
+// For the y-line sweep of a single problem: after the two factor planes of a
+// level's y-line factor array (line-contiguous, tpitch), the couplings that
+// line i's right-hand side reads at position j, one plane each in line order:
+// w(i,j), w(i+1,j) [, sw(i,j), nw(i+1,j), nw(i,j+1), sw(i+1,j+1)] -- the
+// operands of relax_lines_y.f90:102-106 other than b and x.  The sweep then
+// reads them with vector loads of the line's own contiguous segments instead
+// of strided loads shared by the two colours.
+template <typename T, int NS>
+__global__ void k_pack_ylines(const T *__restrict__ so, T *__restrict__ sor, Dims2 d, int tpitch)
+{
+	const int j = blockIdx.x * blockDim.x + threadIdx.x + 1, i = blockIdx.y + 1;
+	if (j > d.ny || i > d.nx) return;
+	const size_t ps = d.plane(), fps = (size_t)tpitch * (d.nx + 2);
+	const int P = d.pitch;
+	const size_t k = d.at(i, j), o = (size_t)i * tpitch + j;
+	T *c = sor + 2 * fps;
+	const T *w = so + ps;
+	c[o] = w[k];
+	c[fps + o] = w[k + 1];
+	if (NS == 5) {
+		const T *sw = so + 3 * ps, *nw = so + 4 * ps;
+		c[2 * fps + o] = sw[k];
+		c[3 * fps + o] = nw[k + 1];
+		c[4 * fps + o] = nw[k + P];
+		c[5 * fps + o] = sw[k + P + 1];
+	}
+}
+
+template <typename T>
+int pack_ylines_2d(const T *so, int nstencil, T *sor, Dims2 d, int tpitch, cudaStream_t st)
+{
+	if (d.nb != 1 || tpitch < d.ny + 2) {
+		set_error(CDR_ERR_DIM, "packed y-line couplings: a single problem with tpitch >= ny+2");
+		return CDR_ERR_DIM;
+	}
+	const dim3 g(ceil_div(d.ny, 256), d.nx);
+	if (nstencil == 5) k_pack_ylines<T, 5><<<g, 256, 0, st>>>(so, sor, d, tpitch);
+	else k_pack_ylines<T, 3><<<g, 256, 0, st>>>(so, sor, d, tpitch);
+	CDR_LAUNCH_CHECK();
+	return CDR_OK;
+}
+template int pack_ylines_2d<double>(const double *, int, double *, Dims2, int, cudaStream_t);
+template int pack_ylines_2d<float>(const float *, int, float *, Dims2, int, cudaStream_t);
 
 }  // namespace cdrgpu

@@ -47,9 +47,15 @@ int cg_inv_add_timeouts(unsigned n);
 int lines_stream_set_wait(unsigned long long ns);
 constexpr unsigned long long kStreamWaitDefaultNs = 200000000ull;  // kWaitLimitNs of k2_bulk.cuh
 int cg_inv_set_wait(unsigned long long ns);
+// The packed y-line couplings after the two factor planes of a level's y-line
+// factor array (2 + 2 (5-point) or 2 + 6 (9-point) planes of tpitch * (nx+2));
+// y sweeps with CDR_LINES_YPACKED read them.  A single problem.
+template <typename T>
+int pack_ylines_2d(const T *so, int nstencil, T *sor, Dims2 d, int tpitch, cudaStream_t st);
+inline int ypack_planes(int nstencil) { return nstencil == 5 ? 6 : 2; }
 template <typename T>
 int lines_autotune(const T *so, int nstencil, T *x, const T *b, const T *sor, Dims2 d, int tpitch, int dir,
-                   cudaStream_t st, unsigned *ysync = nullptr);
+                   cudaStream_t st, unsigned *ysync = nullptr, bool ypack = false);
 bool lines_shape(int dir, int tsize, int ns, int n, int nl, int nb, LineShape *out);
 // pin a shape for a line geometry (the autotuner then leaves it); false if the
 // shape cannot run lines of length n

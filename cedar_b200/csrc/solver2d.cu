@@ -44,6 +44,7 @@ struct Level {
 	// iterate from the interpolate-add on, in FP64, and the row-sum excess of
 	// the operator (the difference form of its residual)
 	double *xw = nullptr;
+	bool ypk = false;  // the y-line factor arrays carry the packed couplings
 	float *dg32 = nullptr;
 };
 
@@ -78,6 +79,12 @@ struct cdr_gpu_solver {
 	cudaEvent_t ev0 = nullptr, ev1 = nullptr;
 	float setup_ms = 0.f, solve_ms = 0.f;
 	bool wide = false;  // inside an FCG iteration with a widened fine-level iterate (lv[0].xw)
+	// y-line factor arrays carry the packed couplings (pack_ylines_2d): y-line
+	// relaxation without periodic directions, on levels whose y-lines have at
+	// most 1024 points (K = 8 chunks; there the strided coupling loads, not
+	// DRAM, bound the sweep; the longer lines of a fine level stream from DRAM
+	// either way and run as fast unpacked)
+	bool ypack = false;
 
 	template <typename T>
 	int alloc(T **p, size_t n)
@@ -163,6 +170,7 @@ int cdr_gpu_solver::smooth(int l, T *x, const T *b, int updown, bool zero)
 		CDR_CUDA_TRY(cudaMemsetAsync(x, 0, sizeof(T) * L.d.plane(), st));
 		zero = false;
 	}
+	const int yf = L.ypk ? CDR_LINES_YPACKED : 0;
 	for (int it = 0; it < n; ++it) {
 		// the first sweep of a zero iterate does not read it
 		const int f = lflags<T>() | (zero && it == 0 ? CDR_LINES_ZERO_START : 0);
@@ -172,15 +180,15 @@ int cdr_gpu_solver::smooth(int l, T *x, const T *b, int updown, bool zero)
 			CDR_TRY(relax_lines_2d<T>(so, L.ns, x, b, sor, L.d, L.tpitch, CDR_DIR_X, updown, f, st));
 			break;
 		case CDR_RELAX_LINE_Y:
-			CDR_TRY(relax_lines_2d<T>(so, L.ns, x, b, sory, L.d, L.tpitch, CDR_DIR_Y, updown, f, st, ysync));
+			CDR_TRY(relax_lines_2d<T>(so, L.ns, x, b, sory, L.d, L.tpitch, CDR_DIR_Y, updown, f | yf, st, ysync));
 			break;
 		case CDR_RELAX_LINE_XY:
 			if (updown == CDR_DOWN) {
 				CDR_TRY(relax_lines_2d<T>(so, L.ns, x, b, sor, L.d, L.tpitch, CDR_DIR_X, updown, f, st));
-				CDR_TRY(relax_lines_2d<T>(so, L.ns, x, b, sory, L.d, L.tpitch, CDR_DIR_Y, updown, lflags<T>(), st,
+				CDR_TRY(relax_lines_2d<T>(so, L.ns, x, b, sory, L.d, L.tpitch, CDR_DIR_Y, updown, lflags<T>() | yf, st,
 				                          ysync));
 			} else {
-				CDR_TRY(relax_lines_2d<T>(so, L.ns, x, b, sory, L.d, L.tpitch, CDR_DIR_Y, updown, f, st, ysync));
+				CDR_TRY(relax_lines_2d<T>(so, L.ns, x, b, sory, L.d, L.tpitch, CDR_DIR_Y, updown, f | yf, st, ysync));
 				CDR_TRY(relax_lines_2d<T>(so, L.ns, x, b, sor, L.d, L.tpitch, CDR_DIR_X, updown, lflags<T>(), st));
 			}
 			break;
@@ -463,7 +471,7 @@ int cdr_gpu_solver::tune_lines()
 			                          CDR_DIR_X, st));
 		if (ly)
 			CDR_TRY(lines_autotune<T>(Arr<T>::so(F), F.ns, Arr<T>::x(F), Arr<T>::b(F), Arr<T>::sory(F), F.d, F.tpitch,
-			                          CDR_DIR_Y, st, ysync));
+			                          CDR_DIR_Y, st, ysync, F.ypk));
 	}
 	return CDR_OK;
 }
@@ -498,6 +506,7 @@ int cdr_gpu_solver::setup()
 			CDR_TRY(setup_lines_2d<double>(F.so, F.ns, F.sory, F.d, F.tpitch, CDR_DIR_Y, info, st));
 			break;
 		}
+		if (F.ypk) CDR_TRY(pack_ylines_2d<double>(F.so, F.ns, F.sory, F.d, F.tpitch, st));
 	}
 	Level &Cg = lv[L() - 1];
 	if (per) CDR_TRY(setup_cg_per_2d(Cg.so, Cg.ns, Cg.d, abd, info + 1, per, st));
@@ -526,6 +535,7 @@ int cdr_gpu_solver::setup()
 				CDR_TRY(setup_lines_2d<float>(F.so, F.ns, F.sory32, F.d, F.tpitch, CDR_DIR_Y, info, st));
 				break;
 			}
+			if (F.ypk) CDR_TRY(pack_ylines_2d<float>(F.so32, F.ns, F.sory32, F.d, F.tpitch, st));
 		}
 	}
 	int hinfo[2] = {0, 0};
@@ -630,6 +640,7 @@ static int create_impl(cdr_gpu_solver *h, const double *so_src, int ns, int nx, 
 		nl = s.num_levels;
 	}
 	h->lv.resize(nl);
+	h->ypack = (s.relaxation == CDR_RELAX_LINE_Y || s.relaxation == CDR_RELAX_LINE_XY) && s.periodic == 0;
 	for (int l = 0; l < nl; ++l) {
 		Level &L = h->lv[l];
 		if (l == 0) { L.nx = nx; L.ny = ny; L.ns = ns; }
@@ -648,9 +659,11 @@ static int create_impl(cdr_gpu_solver *h, const double *so_src, int ns, int nx, 
 		CDR_TRY(h->alloc(&L.b, pl));
 		CDR_TRY(h->alloc(&L.r, pl));
 		if (l > 0) CDR_TRY(h->alloc(&L.ci, pl * 8));
+		L.ypk = h->ypack && l + 1 < nl && L.ny <= 1024;
+		const int ypl = 2 + (L.ypk ? ypack_planes(L.ns) : 0);  // factors [+ packed couplings]
 		if (l + 1 < nl) {
 			CDR_TRY(h->alloc(&L.sor, pl * 2));
-			CDR_TRY(h->alloc(&L.sory, tpl * 2));
+			CDR_TRY(h->alloc(&L.sory, tpl * ypl));
 		}
 		if (h->mixed()) {
 			CDR_TRY(h->alloc(&L.so32, pl * L.ns));
@@ -660,7 +673,7 @@ static int create_impl(cdr_gpu_solver *h, const double *so_src, int ns, int nx, 
 			if (l > 0) CDR_TRY(h->alloc(&L.ci32, pl * 8));
 			if (l + 1 < nl) {
 				CDR_TRY(h->alloc(&L.sor32, pl * 2));
-				CDR_TRY(h->alloc(&L.sory32, tpl * 2));
+				CDR_TRY(h->alloc(&L.sory32, tpl * ypl));
 			}
 		}
 	}

@@ -208,6 +208,11 @@ int cdr_gpu_setup_lines_2d_f32(const double *so, int nstencil, float *sor, int n
  * one launch (blocks of column pairs, a bounded flag wait between neighbouring
  * blocks) whatever shape the autotuner chose; the same bits as two launches. */
 #define CDR_LINES_YPAIR 16
+/* Kernel flags, y-lines of a single problem: the factor array sor carries,
+ * after its two factor planes, the packed couplings that
+ * cdr_gpu_pack_ylines_2d_* wrote; the sweep reads those (the same values, the
+ * same bits) with vector loads of each line's own segment. */
+#define CDR_LINES_YPACKED 32
 /* Status of the streamed x-line kernel since the last call, read on stream s
  * (synchronises it): CDR_ERR_NUMERIC if a CTA gave up waiting for its staged
  * rows (a bounded wait; the sweep's result is then incomplete), else CDR_OK.
@@ -244,6 +249,17 @@ int cdr_gpu_relax_lines_2d_f32(const float *so, int nstencil, float *x, const fl
  * sweep.  One buffer per stream: sweeps that run concurrently on one buffer
  * race.  x-lines and the other cases run as cdr_gpu_relax_lines_2d_*.  No
  * counterpart in the reference. */
+/* Pack a level's y-line couplings after the two factor planes of its y-line
+ * factor array sor (transposed layout, tpitch): planes of tpitch*(nx+2)
+ * entries, line i's position j at i*tpitch + j, holding w(i,j), w(i+1,j) and
+ * for nine-point operators sw(i,j), nw(i+1,j), nw(i,j+1), sw(i+1,j+1) -- the
+ * couplings of relax_lines_y.f90:102-106.  sor must hold 2 + 2 (nstencil 3) or
+ * 2 + 6 (nstencil 5) planes.  A single problem.  No counterpart in the
+ * reference (its sweep reads the operator in place). */
+int cdr_gpu_pack_ylines_2d_f64(const double *so, int nstencil, double *sor, int nx, int ny, int pitch, int tpitch,
+                               cudaStream_t stream);
+int cdr_gpu_pack_ylines_2d_f32(const float *so, int nstencil, float *sor, int nx, int ny, int pitch, int tpitch,
+                               cudaStream_t stream);
 size_t cdr_gpu_lines_sync_words(int nx);
 int cdr_gpu_relax_lines_2d_sync_f64(const double *so, int nstencil, double *x, const double *b, const double *sor,
                                     int nx, int ny, int pitch, int tpitch, int dir, int updown, int flags,

@@ -500,3 +500,57 @@ def test_zero_start_sweep_does_not_read_the_iterate(lib, precision, nx, ny, ns):
                         np.testing.assert_array_equal(host(d2), host(d1), err_msg=msg)
     assert int(sync.abs().sum().item()) == 0
     assert lib.cdr_gpu_lines_stream_status(stream()) == 0
+
+
+@pytest.mark.parametrize("precision", ["f32", "f64"])
+@pytest.mark.parametrize("nx,ny,ns", [(37, 100, 5), (64, 63, 3), (255, 1024, 5), (96, 2047, 5), (9, 12, 5)])
+def test_packed_y_couplings_sweep_bitwise(lib, precision, nx, ny, ns):
+    """cdr_gpu_pack_ylines_2d_* writes line i's couplings after the y factors;
+    a y sweep with CDR_LINES_YPACKED reads them there: bit-identical to the
+    sweep that reads the operator, both directions of sweep, with and without
+    a zero start, over several launch shapes, one launch per colour and both
+    colours in one launch."""
+    import torch
+    dt = torch.float64 if precision == "f64" else torch.float32
+    fp32 = precision == "f32"
+    fn = lib.cdr_gpu_relax_lines_2d_f64 if not fp32 else lib.cdr_gpu_relax_lines_2d_f32
+    fns = lib.cdr_gpu_relax_lines_2d_sync_f64 if not fp32 else lib.cdr_gpu_relax_lines_2d_sync_f32
+    fp = lib.cdr_gpu_pack_ylines_2d_f64 if not fp32 else lib.cdr_gpu_pack_ylines_2d_f32
+    sync = torch.zeros(lib.cdr_gpu_lines_sync_words(nx), dtype=torch.int32, device="cuda")
+    from oracle import oracle as O
+    so, x, b = make_op(nx, ny, ns), grid(nx, ny, 8), grid(nx, ny, 9)
+    sy, _ = O.setup_lines_y(so)
+    g = sy.copy()
+    if fp32:
+        g[0][1:-1, 1:-1] = 1.0 / sy[0][1:-1, 1:-1]
+    pitch = ((nx + 2 + 31) // 32) * 32
+    tpitch = ((ny + 2 + 31) // 32) * 32
+    dso, dbb = padded(so, pitch, dt), padded(b, pitch, dt)
+    npk = 6 if ns == 5 else 2
+    big = np.zeros((2 + npk, nx + 2, ny + 2))
+    big[:2] = g
+    dsy = padded(big, tpitch, dt)
+    _lib.check(fp(ptr(dso), ns, ptr(dsy), nx, ny, pitch, tpitch, stream()))
+    K = 16 if ny > 1024 else 8
+    tpl = 1
+    while tpl * K < ny:
+        tpl *= 2
+    caps = sorted({max(32, tpl * gg) for gg in (1, 2, 4, 8) if tpl * gg <= (1024 if fp32 else 512)})
+    for cap in caps:
+        _lib.check(lib.cdr_gpu_lines_set_shape(_lib.DIR_Y, 1 if fp32 else 0, ns, ny, nx, 0, K, cap))
+        for updown in (0, 1):
+            for flags in (0, 8):
+                d1, d2, d3 = padded(x, pitch, dt), padded(x, pitch, dt), padded(x, pitch, dt)
+                for _ in range(2):
+                    _lib.check(fn(ptr(dso), ns, ptr(d1), ptr(dbb), ptr(dsy), nx, ny, pitch, tpitch, _lib.DIR_Y, updown,
+                                  flags, stream()))
+                    _lib.check(fn(ptr(dso), ns, ptr(d2), ptr(dbb), ptr(dsy), nx, ny, pitch, tpitch, _lib.DIR_Y, updown,
+                                  flags | 32, stream()))
+                    _lib.check(fns(ptr(dso), ns, ptr(d3), ptr(dbb), ptr(dsy), nx, ny, pitch, tpitch, _lib.DIR_Y,
+                                   updown, flags | 48, ptr(sync), stream()))  # CDR_LINES_YPAIR | CDR_LINES_YPACKED
+                np.testing.assert_array_equal(host(d2), host(d1),
+                                              err_msg="cap %d updown %d flags %d" % (cap, updown, flags))
+                np.testing.assert_array_equal(host(d3), host(d1),
+                                              err_msg="pair: cap %d updown %d flags %d" % (cap, updown, flags))
+    assert int(sync.abs().sum().item()) == 0
+    assert lib.cdr_gpu_lines_stream_status(stream()) == 0
