@@ -51,9 +51,9 @@ WORKLOAD = ("2D heterogeneous diffusion, 9-pt bilinear FE, 2047x2047 nodes (2048
             "(seed 3); line-xy relaxation, Galerkin coarsening (levels and coarsest solve: config.solver)")
 # DRAM bytes (read + write) per launch on the 2047^2 FP32 level, from one ncu capture each (caches
 # flushed): x-lines, one colour (the streamed kernel, k_lines_xstream) 85.1 MB read + 2.9 MB written;
-# y-lines, both colours in one launch (k_ylines_pair) 179.6 MB read + 11.0 MB written
+# y-lines, the sweep's two colour launches of k_lines_fast (each started cold) 106.0 + 107.2 MB
 LINE_X_TRAFFIC = 88.1e6
-LINE_Y_TRAFFIC = 190.6e6
+LINE_Y_TRAFFIC = 213.2e6
 # headline FCG: the residual is formed (b - A x) every FCG_REPLACE-th iteration and to confirm convergence,
 # updated as r - alpha A p in between
 FCG_REPLACE = 10
