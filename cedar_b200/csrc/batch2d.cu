@@ -15,6 +15,7 @@ template <> struct BA<double> {
 	static double *r(B2Level &L) { return L.r; }
 	static double *sor(B2Level &L) { return L.sor; }
 	static double *sory(B2Level &L) { return L.sory; }
+	static double *yc(B2Level &L) { return L.yc; }
 	static double *ci(B2Level &L) { return L.ci; }
 };
 template <> struct BA<float> {
@@ -24,6 +25,7 @@ template <> struct BA<float> {
 	static float *r(B2Level &L) { return L.r32; }
 	static float *sor(B2Level &L) { return L.sor32; }
 	static float *sory(B2Level &L) { return L.sory32; }
+	static float *yc(B2Level &L) { return L.yc32; }
 	static float *ci(B2Level &L) { return L.ci32; }
 };
 
@@ -93,9 +95,14 @@ int Batch2::init(const cdr_gpu_settings &settings, int ns, int nx, int ny, int n
 		CDR_TRY(alloc(&L.b, pl));
 		CDR_TRY(alloc(&L.r, pl));
 		if (l > 0) CDR_TRY(alloc(&L.ci, pl * 8));
+		// packed y couplings on levels with y-lines of at most 1024 points
+		const bool ypk = l + 1 < nl && L.ny <= 1024 &&
+		                 (s.relaxation == CDR_RELAX_LINE_Y || s.relaxation == CDR_RELAX_LINE_XY);
 		if (l + 1 < nl) {
 			CDR_TRY(alloc(&L.sor, pl * 2));
 			if (lines) CDR_TRY(alloc(&L.sory, L.ysize() * nb));
+			// FP64 sweeps only in FP64 batches (an FP32-refined batch cycles in FP32)
+			if (ypk && !mixed() && !(s.line_flags & CDR_LINES_EXACT)) CDR_TRY(alloc(&L.yc, L.ypsize() * nb));
 		}
 		if (mixed() && !external32) {
 			CDR_TRY(alloc(&L.so32, pl * L.ns));
@@ -106,6 +113,7 @@ int Batch2::init(const cdr_gpu_settings &settings, int ns, int nx, int ny, int n
 			if (l + 1 < nl) {
 				CDR_TRY(alloc(&L.sor32, pl * 2));
 				if (lines) CDR_TRY(alloc(&L.sory32, L.ysize() * nb));
+				if (ypk) CDR_TRY(alloc(&L.yc32, L.ypsize() * nb));
 			}
 		}
 	}
@@ -143,6 +151,7 @@ int Batch2::setup(bool check)
 		if (r == CDR_RELAX_LINE_Y || r == CDR_RELAX_LINE_XY) {
 			CDR_TRY(setup_lines_2d<double>(F.so, F.ns, F.sory, df, F.tpitch, CDR_DIR_Y, info, st));
 			if (mixed()) CDR_TRY(setup_lines_2d<float>(F.so, F.ns, F.sory32, df, F.tpitch, CDR_DIR_Y, info, st));
+			if (F.yc) CDR_TRY(pack_ylines_2d<double>(F.so, F.ns, F.yc, df, F.tpitch, st));
 		}
 	}
 	B2Level &Cg = lv.back();
@@ -152,6 +161,7 @@ int Batch2::setup(bool check)
 			B2Level &F = lv[l];
 			CDR_TRY(convert_f64_f32(F.so, F.so32, F.plane() * F.ns * nb, st));
 			if (l > 0) CDR_TRY(convert_f64_f32(F.ci, F.ci32, F.plane() * 8 * nb, st));
+			if (F.yc32) CDR_TRY(pack_ylines_2d<float>(F.so32, F.ns, F.yc32, F.dims(all), F.tpitch, st));
 		}
 	}
 	return check ? check_info() : CDR_OK;
@@ -178,7 +188,7 @@ int Batch2::tune_lines()
 			                          st));
 		if (ly)
 			CDR_TRY(lines_autotune<T>(BA<T>::so(F), F.ns, BA<T>::x(F), BA<T>::b(F), BA<T>::sory(F), d, F.tpitch,
-			                          CDR_DIR_Y, st));
+			                          CDR_DIR_Y, st, nullptr, BA<T>::yc(F)));
 	}
 	return CDR_OK;
 }
@@ -211,6 +221,7 @@ int Batch2::smooth(int l, Sel sel, int updown, bool zero)
 	const T *b = BA<T>::b(F) + f * pl;
 	const T *sx = BA<T>::sor(F) ? BA<T>::sor(F) + f * 2 * pl : nullptr;
 	const T *sy = BA<T>::sory(F) ? BA<T>::sory(F) + f * F.ysize() : nullptr;
+	const T *yc = BA<T>::yc(F) ? BA<T>::yc(F) + f * F.ypsize() : nullptr;  // packed y couplings
 	const int flags = sizeof(T) == 8 ? s.line_flags : (s.line_flags & CDR_LINES_NOTUNE);
 	const int n = updown == CDR_DOWN ? s.nrelax_pre : s.nrelax_post;
 	if (zero && (n == 0 || s.relaxation == CDR_RELAX_POINT)) {  // only the line sweeps skip reading it
@@ -222,13 +233,13 @@ int Batch2::smooth(int l, Sel sel, int updown, bool zero)
 		switch (s.relaxation) {
 		case CDR_RELAX_POINT: CDR_TRY(relax_point_2d<T>(so, F.ns, x, b, sx, d, updown, st)); break;
 		case CDR_RELAX_LINE_X: CDR_TRY(relax_lines_2d<T>(so, F.ns, x, b, sx, d, F.tpitch, CDR_DIR_X, updown, f, st)); break;
-		case CDR_RELAX_LINE_Y: CDR_TRY(relax_lines_2d<T>(so, F.ns, x, b, sy, d, F.tpitch, CDR_DIR_Y, updown, f, st)); break;
+		case CDR_RELAX_LINE_Y: CDR_TRY(relax_lines_2d<T>(so, F.ns, x, b, sy, d, F.tpitch, CDR_DIR_Y, updown, f, st, nullptr, yc)); break;
 		default:
 			if (updown == CDR_DOWN) {
 				CDR_TRY(relax_lines_2d<T>(so, F.ns, x, b, sx, d, F.tpitch, CDR_DIR_X, updown, f, st));
-				CDR_TRY(relax_lines_2d<T>(so, F.ns, x, b, sy, d, F.tpitch, CDR_DIR_Y, updown, flags, st));
+				CDR_TRY(relax_lines_2d<T>(so, F.ns, x, b, sy, d, F.tpitch, CDR_DIR_Y, updown, flags, st, nullptr, yc));
 			} else {
-				CDR_TRY(relax_lines_2d<T>(so, F.ns, x, b, sy, d, F.tpitch, CDR_DIR_Y, updown, f, st));
+				CDR_TRY(relax_lines_2d<T>(so, F.ns, x, b, sy, d, F.tpitch, CDR_DIR_Y, updown, f, st, nullptr, yc));
 				CDR_TRY(relax_lines_2d<T>(so, F.ns, x, b, sx, d, F.tpitch, CDR_DIR_X, updown, flags, st));
 			}
 		}

@@ -23,8 +23,13 @@ struct B2Level {
 	double *so = nullptr, *x = nullptr, *b = nullptr, *r = nullptr, *sor = nullptr, *sory = nullptr, *ci = nullptr;
 	float *so32 = nullptr, *x32 = nullptr, *b32 = nullptr, *r32 = nullptr, *sor32 = nullptr, *sory32 = nullptr,
 	      *ci32 = nullptr;
+	// packed y-line couplings (pack_ylines_2d) of levels whose y-lines have at
+	// most 1024 points, ypsize() per problem; null elsewhere
+	double *yc = nullptr;
+	float *yc32 = nullptr;
 	size_t plane() const { return (size_t)pitch * (ny + 2); }
 	size_t ysize() const { return 2 * (size_t)tpitch * (nx + 2); }  // y-line factors of one problem
+	size_t ypsize() const { return (size_t)ypack_planes(ns) * tpitch * (nx + 2); }
 	Dims2 dims(Sel s) const
 	{
 		Dims2 d{nx, ny, pitch};

@@ -40,11 +40,13 @@ struct USize {
 	bool smoothed = false;   // a smoothing level (not the coarsest) of its problems
 	float *so32 = nullptr, *x32 = nullptr, *b32 = nullptr, *r32 = nullptr, *ci32 = nullptr, *sor32 = nullptr,
 	      *sory32 = nullptr;
+	float *yc32 = nullptr;  // packed y-line couplings (y-lines of at most 1024 points)
 	double *abd = nullptr;
 	int child = -1;      // index of the next coarser size
 	int child_off = 0;   // entry of this size's first problem among the child's entries
 	size_t plane() const { return (size_t)pitch * (ny + 2); }
 	size_t ysize() const { return 2 * (size_t)tpitch * (nx + 2); }
+	size_t ypsize() const { return (size_t)ypack_planes(ns) * tpitch * (nx + 2); }
 	size_t abd_size() const { return (size_t)(nx + 2) * nx * ny; }
 	Dims2 dims(int count) const
 	{
@@ -123,14 +125,14 @@ struct cdr_gpu_batchmix {
 				CDR_TRY(relax_lines_2d<float>(U.so32, U.ns, U.x32, U.b32, U.sor32, d, U.tpitch, CDR_DIR_X, updown, f, st));
 				break;
 			case CDR_RELAX_LINE_Y:
-				CDR_TRY(relax_lines_2d<float>(U.so32, U.ns, U.x32, U.b32, U.sory32, d, U.tpitch, CDR_DIR_Y, updown, f, st));
+				CDR_TRY(relax_lines_2d<float>(U.so32, U.ns, U.x32, U.b32, U.sory32, d, U.tpitch, CDR_DIR_Y, updown, f, st, nullptr, U.yc32));
 				break;
 			default:
 				if (updown == CDR_DOWN) {
 					CDR_TRY(relax_lines_2d<float>(U.so32, U.ns, U.x32, U.b32, U.sor32, d, U.tpitch, CDR_DIR_X, updown, f, st));
-					CDR_TRY(relax_lines_2d<float>(U.so32, U.ns, U.x32, U.b32, U.sory32, d, U.tpitch, CDR_DIR_Y, updown, flags, st));
+					CDR_TRY(relax_lines_2d<float>(U.so32, U.ns, U.x32, U.b32, U.sory32, d, U.tpitch, CDR_DIR_Y, updown, flags, st, nullptr, U.yc32));
 				} else {
-					CDR_TRY(relax_lines_2d<float>(U.so32, U.ns, U.x32, U.b32, U.sory32, d, U.tpitch, CDR_DIR_Y, updown, f, st));
+					CDR_TRY(relax_lines_2d<float>(U.so32, U.ns, U.x32, U.b32, U.sory32, d, U.tpitch, CDR_DIR_Y, updown, f, st, nullptr, U.yc32));
 					CDR_TRY(relax_lines_2d<float>(U.so32, U.ns, U.x32, U.b32, U.sor32, d, U.tpitch, CDR_DIR_X, updown, flags, st));
 				}
 			}
@@ -411,6 +413,8 @@ int cdr_gpu_batchmix_create(const cdr_gpu_settings *s, int nclass, const double 
 		if (U.smoothed) {
 			if ((rc = h->alloc(&U.sor32, pl * 2))) return fail(rc);
 			if (lines && (rc = h->alloc(&U.sory32, U.ysize() * U.entries))) return fail(rc);
+			const bool ly = s->relaxation == CDR_RELAX_LINE_Y || s->relaxation == CDR_RELAX_LINE_XY;
+			if (ly && U.ny <= 1024 && (rc = h->alloc(&U.yc32, U.ypsize() * U.entries))) return fail(rc);
 		}
 		if (U.coarsest && (rc = h->alloc(&U.abd, U.abd_size() * U.entries))) return fail(rc);
 	}
@@ -428,6 +432,7 @@ int cdr_gpu_batchmix_create(const cdr_gpu_settings *s, int nclass, const double 
 			L.ci32 = l > 0 ? U.ci32 + o * 8 * pl : nullptr;
 			L.sor32 = U.sor32 ? U.sor32 + o * 2 * pl : nullptr;
 			L.sory32 = U.sory32 ? U.sory32 + o * U.ysize() : nullptr;
+			L.yc32 = U.yc32 ? U.yc32 + o * U.ypsize() : nullptr;
 			if (l + 1 == B.L()) B.abd = U.abd + o * U.abd_size();
 		}
 		const B2Level &F = B.lv[0];
@@ -511,7 +516,8 @@ int cdr_gpu_batchmix_create(const cdr_gpu_settings *s, int nclass, const double 
 			const Dims2 d = U.dims(U.entries);
 			if (lx && (rc = lines_autotune<float>(U.so32, U.ns, U.x32, U.b32, U.sor32, d, U.tpitch, CDR_DIR_X, h->st)))
 				return fail(rc);
-			if (ly && (rc = lines_autotune<float>(U.so32, U.ns, U.x32, U.b32, U.sory32, d, U.tpitch, CDR_DIR_Y, h->st)))
+			if (ly && (rc = lines_autotune<float>(U.so32, U.ns, U.x32, U.b32, U.sory32, d, U.tpitch, CDR_DIR_Y, h->st,
+			                                      nullptr, U.yc32)))
 				return fail(rc);
 		}
 	}

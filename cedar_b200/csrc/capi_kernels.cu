@@ -205,7 +205,7 @@ LRELAX_SYNC_IMPL(float, f32)
 		CDR_TRY(check_grid(nx, ny, pitch));                                                                     \
 		CDR_TRY(check_ns(ns));                                                                                  \
 		CDR_NONNULL(so); CDR_NONNULL(sor);                                                                      \
-		return pack_ylines_2d<T>(so, ns, sor, Dims2{nx, ny, pitch}, tpitch, s);                                 \
+		return pack_ylines_2d<T>(so, ns, sor + 2 * (size_t)tpitch * (nx + 2), Dims2{nx, ny, pitch}, tpitch, s);  \
 	}
 PACKY_IMPL(double, f64)
 PACKY_IMPL(float, f32)

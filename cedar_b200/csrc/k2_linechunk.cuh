@@ -221,13 +221,14 @@ __device__ __forceinline__ T yline_rhs(const T *__restrict__ so, size_t ps, cons
 // first sweep after a coarse-grid iterate is cleared.  nslots: line slots of
 // the CTA's scans when it holds several groups of G y-lines (g is then the
 // slot, G the lines of one group: the lane distance of a line's chunks).
-// PACK (y-lines): the factor array holds, after the two factor planes, the
-// line's couplings in line order (pack_ylines_2d), read as vectors.
+// PACK (y-lines): yc holds the lines' couplings in line order
+// (pack_ylines_2d), read as vectors.
 template <typename T, int NS, int DIR, int K, bool CG = false, bool ZERO = false, bool PACK = false,
           bool XL = DIR == CDR_DIR_X>
 __device__ __forceinline__ void line_chunk(const T *__restrict__ so, T *__restrict__ q, const T *__restrict__ qf,
                                            const T *__restrict__ sor, const Dims2 &d, int tpitch, int lc, int g,
-                                           int t, int TPL, int G, T *sA, T *sB, int nslots = 0)
+                                           int t, int TPL, int G, T *sA, T *sB, int nslots = 0,
+                                           const T *__restrict__ yc = nullptr)
 {
 	const int NL = nslots > 0 ? nslots : G;  // line slots of the CTA's scans (g < NL)
 	const int n = DIR == CDR_DIR_X ? d.nx : d.ny;
@@ -328,7 +329,8 @@ __device__ __forceinline__ void line_chunk(const T *__restrict__ so, T *__restri
 				else return q[e];
 			};
 			const size_t fps = (size_t)tpitch * (d.nx + 2);
-			const T *cpl = sor + 2 * fps + (size_t)lc * tpitch;  // plane m at cpl + m * fps
+			// the problem's planes of packed couplings, line lc: plane m at cpl + m * fps
+			const T *cpl = yc + d.bofs((size_t)(NS == 5 ? 6 : 2) * fps) + (size_t)lc * tpitch;
 			const size_t kq = d.at(lc, 0);
 			constexpr int H = 8;
 			static_assert(K % H == 0, "half-chunks of 8");

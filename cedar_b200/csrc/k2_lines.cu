@@ -233,7 +233,7 @@ template <typename T, int NS, int DIR, int K, int LB = 0, bool ZERO = false, boo
           bool XL = DIR == CDR_DIR_X>
 __global__ void __launch_bounds__(XL ? FAST_BLOCK_X : (LB ? LB : yblock_max<T>()), XL || LB ? 2 : 1)
     k_lines_fast(const T *__restrict__ so, T *__restrict__ q, const T *__restrict__ qf, const T *__restrict__ sor,
-                 Dims2 d, int tpitch, int first, int tpl_log2, int G)
+                 Dims2 d, int tpitch, int first, int tpl_log2, int G, const T *__restrict__ yc)
 {
 	// group totals of the scans: lines * groups = blockDim / SG at most
 	__shared__ T sA[FAST_BLOCK_Y / SG], sB[FAST_BLOCK_Y / SG];
@@ -243,7 +243,7 @@ __global__ void __launch_bounds__(XL ? FAST_BLOCK_X : (LB ? LB : yblock_max<T>()
 	if (XL) { g = tid >> tpl_log2; t = tid & (TPL - 1); }
 	else { g = tid % G; t = tid / G; }
 	line_chunk<T, NS, DIR, K, false, ZERO, PACK>(so, q, qf, sor, d, tpitch, first + 2 * (blockIdx.x * G + g), g, t,
-	                                             TPL, G, sA, sB);
+	                                             TPL, G, sA, sB, 0, yc);
 }
 
 // Give-ups of the bounded waits of the line kernels (streamed x-lines, the
@@ -285,7 +285,8 @@ __device__ __forceinline__ unsigned ld_acquire(const unsigned *p)
 template <typename T, int NS, int K, int LB = 0, bool Z1 = false, bool PK = false>
 __global__ void __launch_bounds__(LB ? LB : yblock_max<T>(), LB ? 2 : 1)
     k_ylines_pair(const T *__restrict__ so, T *__restrict__ q, const T *__restrict__ qf, const T *__restrict__ sor,
-                  Dims2 d, int tpitch, int c2, int tpl_log2, int G, unsigned *__restrict__ sync, int nvb)
+                  Dims2 d, int tpitch, int c2, int tpl_log2, int G, unsigned *__restrict__ sync, int nvb,
+                  const T *__restrict__ yc)
 {
 	__shared__ T sA[FAST_BLOCK_Y / SG], sB[FAST_BLOCK_Y / SG];
 	__shared__ int s_vb, s_ok;
@@ -299,7 +300,7 @@ __global__ void __launch_bounds__(LB ? LB : yblock_max<T>(), LB ? 2 : 1)
 	__syncthreads();
 	const int vb = s_vb;
 	const int p2 = 2 * (vb * G + g) + c2, p1 = p2 + 1;
-	line_chunk<T, NS, CDR_DIR_Y, K, false, Z1, PK && !Z1>(so, q, qf, sor, d, tpitch, p1, g, t, TPL, G, sA, sB);
+	line_chunk<T, NS, CDR_DIR_Y, K, false, Z1, PK && !Z1>(so, q, qf, sor, d, tpitch, p1, g, t, TPL, G, sA, sB, 0, yc);
 	__threadfence();  // this thread's phase-1 lines reach L2 before phase 2 reads them there
 	__syncthreads();  // phase 1 read and written by every thread
 	if (tid == 0) {
@@ -330,7 +331,7 @@ __global__ void __launch_bounds__(LB ? LB : yblock_max<T>(), LB ? 2 : 1)
 	}
 	__syncthreads();
 	if (!s_ok) return;
-	line_chunk<T, NS, CDR_DIR_Y, K, true, false, PK>(so, q, qf, sor, d, tpitch, p2, g, t, TPL, G, sA, sB);
+	line_chunk<T, NS, CDR_DIR_Y, K, true, false, PK>(so, q, qf, sor, d, tpitch, p2, g, t, TPL, G, sA, sB, 0, yc);
 }
 
 // ---------------------------------------------------------- streamed x-lines
@@ -699,8 +700,9 @@ static LineShape shape_for(int n, int nl, int ns, int nb, int dir)
 
 template <typename T, int NS, int DIR, int K>
 static int launch_fast(const T *so, T *x, const T *b, const T *sor, Dims2 d, int tpitch, int first, int nlines,
-                       int cap, cudaStream_t st, bool zero, bool pack = false)
+                       int cap, cudaStream_t st, bool zero, const T *yc = nullptr)
 {
+	const bool pack = yc != nullptr;
 	const int n = DIR == CDR_DIR_X ? d.nx : d.ny;
 	const int tpl_log2 = tpl_log2_of(n, K);
 	const int TPL = 1 << tpl_log2;
@@ -719,10 +721,10 @@ static int launch_fast(const T *so, T *x, const T *b, const T *sor, Dims2 d, int
 		if (pack && !zero) {
 			if (ysmall && block <= YSMALL_BLOCK)
 				k_lines_fast<T, NS, DIR, K, ysmall ? YSMALL_BLOCK : 0, false, true><<<grd, block, 0, st>>>(
-				    so, x, b, sor, d, tpitch, first, tpl_log2, G);
+				    so, x, b, sor, d, tpitch, first, tpl_log2, G, yc);
 			else
 				k_lines_fast<T, NS, DIR, K, 0, false, true><<<grd, block, 0, st>>>(so, x, b, sor, d, tpitch, first,
-				                                                                    tpl_log2, G);
+				                                                                    tpl_log2, G, yc);
 			CDR_LAUNCH_CHECK();
 			return CDR_OK;
 		}
@@ -730,13 +732,13 @@ static int launch_fast(const T *so, T *x, const T *b, const T *sor, Dims2 d, int
 	if (ysmall && block <= YSMALL_BLOCK) {
 		constexpr int LB = ysmall ? YSMALL_BLOCK : 0;
 		if (zero)
-			k_lines_fast<T, NS, DIR, K, LB, true><<<grd, block, 0, st>>>(so, x, b, sor, d, tpitch, first, tpl_log2, G);
+			k_lines_fast<T, NS, DIR, K, LB, true><<<grd, block, 0, st>>>(so, x, b, sor, d, tpitch, first, tpl_log2, G, yc);
 		else
-			k_lines_fast<T, NS, DIR, K, LB><<<grd, block, 0, st>>>(so, x, b, sor, d, tpitch, first, tpl_log2, G);
+			k_lines_fast<T, NS, DIR, K, LB><<<grd, block, 0, st>>>(so, x, b, sor, d, tpitch, first, tpl_log2, G, yc);
 	} else if (zero) {
-		k_lines_fast<T, NS, DIR, K, 0, true><<<grd, block, 0, st>>>(so, x, b, sor, d, tpitch, first, tpl_log2, G);
+		k_lines_fast<T, NS, DIR, K, 0, true><<<grd, block, 0, st>>>(so, x, b, sor, d, tpitch, first, tpl_log2, G, yc);
 	} else {
-		k_lines_fast<T, NS, DIR, K><<<grd, block, 0, st>>>(so, x, b, sor, d, tpitch, first, tpl_log2, G);
+		k_lines_fast<T, NS, DIR, K><<<grd, block, 0, st>>>(so, x, b, sor, d, tpitch, first, tpl_log2, G, yc);
 	}
 	CDR_LAUNCH_CHECK();
 	return CDR_OK;
@@ -796,8 +798,9 @@ size_t lines_sync_words(Dims2 d) { return 2 + (size_t)d.nx / 2 + 1; }
 
 template <typename T, int NS, int K>
 static int launch_ypair(const T *so, T *x, const T *b, const T *sor, Dims2 d, int tpitch, int updown, int cap,
-                        unsigned *sync, cudaStream_t st, bool zero = false, bool pack = false)
+                        unsigned *sync, cudaStream_t st, bool zero = false, const T *yc = nullptr)
 {
+	const bool pack = yc != nullptr;
 	const int tpl_log2 = tpl_log2_of(d.ny, K), TPL = 1 << tpl_log2;
 	const int G = ylines_per_cta(TPL, cap);
 	const int block = (G * TPL + 31) / 32 * 32;
@@ -809,22 +812,22 @@ static int launch_ypair(const T *so, T *x, const T *b, const T *sor, Dims2 d, in
 	// zero start and packed couplings: the first colour reads b only, the second the packed couplings
 	if (small) {
 		if (zero && pack)
-			k_ylines_pair<T, NS, K, LB, true, true><<<nvb, block, 0, st>>>(so, x, b, sor, d, tpitch, c2, tpl_log2, G, sync, nvb);
+			k_ylines_pair<T, NS, K, LB, true, true><<<nvb, block, 0, st>>>(so, x, b, sor, d, tpitch, c2, tpl_log2, G, sync, nvb, yc);
 		else if (zero)
-			k_ylines_pair<T, NS, K, LB, true><<<nvb, block, 0, st>>>(so, x, b, sor, d, tpitch, c2, tpl_log2, G, sync, nvb);
+			k_ylines_pair<T, NS, K, LB, true><<<nvb, block, 0, st>>>(so, x, b, sor, d, tpitch, c2, tpl_log2, G, sync, nvb, yc);
 		else if (pack)
-			k_ylines_pair<T, NS, K, LB, false, true><<<nvb, block, 0, st>>>(so, x, b, sor, d, tpitch, c2, tpl_log2, G, sync, nvb);
+			k_ylines_pair<T, NS, K, LB, false, true><<<nvb, block, 0, st>>>(so, x, b, sor, d, tpitch, c2, tpl_log2, G, sync, nvb, yc);
 		else
-			k_ylines_pair<T, NS, K, LB><<<nvb, block, 0, st>>>(so, x, b, sor, d, tpitch, c2, tpl_log2, G, sync, nvb);
+			k_ylines_pair<T, NS, K, LB><<<nvb, block, 0, st>>>(so, x, b, sor, d, tpitch, c2, tpl_log2, G, sync, nvb, yc);
 	} else {
 		if (zero && pack)
-			k_ylines_pair<T, NS, K, 0, true, true><<<nvb, block, 0, st>>>(so, x, b, sor, d, tpitch, c2, tpl_log2, G, sync, nvb);
+			k_ylines_pair<T, NS, K, 0, true, true><<<nvb, block, 0, st>>>(so, x, b, sor, d, tpitch, c2, tpl_log2, G, sync, nvb, yc);
 		else if (zero)
-			k_ylines_pair<T, NS, K, 0, true><<<nvb, block, 0, st>>>(so, x, b, sor, d, tpitch, c2, tpl_log2, G, sync, nvb);
+			k_ylines_pair<T, NS, K, 0, true><<<nvb, block, 0, st>>>(so, x, b, sor, d, tpitch, c2, tpl_log2, G, sync, nvb, yc);
 		else if (pack)
-			k_ylines_pair<T, NS, K, 0, false, true><<<nvb, block, 0, st>>>(so, x, b, sor, d, tpitch, c2, tpl_log2, G, sync, nvb);
+			k_ylines_pair<T, NS, K, 0, false, true><<<nvb, block, 0, st>>>(so, x, b, sor, d, tpitch, c2, tpl_log2, G, sync, nvb, yc);
 		else
-			k_ylines_pair<T, NS, K><<<nvb, block, 0, st>>>(so, x, b, sor, d, tpitch, c2, tpl_log2, G, sync, nvb);
+			k_ylines_pair<T, NS, K><<<nvb, block, 0, st>>>(so, x, b, sor, d, tpitch, c2, tpl_log2, G, sync, nvb, yc);
 	}
 	CDR_LAUNCH_CHECK();
 	return CDR_OK;
@@ -848,7 +851,7 @@ static bool fast_lines_ok(const T *so, const T *x, const T *b, const T *sor, Dim
 // only; the streamed x-line kernel's bits are the register-chunk kernel's).
 template <typename T, int NS, int DIR>
 static int launch_lines(const T *so, T *x, const T *b, const T *sor, Dims2 d, int tpitch, int first, bool exact,
-                        cudaStream_t st, const LineShape *force = nullptr, bool zero = false, bool pack = false)
+                        cudaStream_t st, const LineShape *force = nullptr, bool zero = false, const T *yc = nullptr)
 {
 	const int n = DIR == CDR_DIR_X ? d.nx : d.ny;
 	const int nl = DIR == CDR_DIR_X ? d.ny : d.nx;
@@ -864,9 +867,9 @@ static int launch_lines(const T *so, T *x, const T *b, const T *sor, Dims2 d, in
 			}
 		if (sh.K == 16) {
 			if constexpr (sizeof(T) == 4 || DIR == CDR_DIR_Y)
-				return launch_fast<T, NS, DIR, 16>(so, x, b, sor, d, tpitch, first, nlines, sh.cap, st, zero, pack);
+				return launch_fast<T, NS, DIR, 16>(so, x, b, sor, d, tpitch, first, nlines, sh.cap, st, zero, yc);
 		} else {
-			return launch_fast<T, NS, DIR, 8>(so, x, b, sor, d, tpitch, first, nlines, sh.cap, st, zero, pack);
+			return launch_fast<T, NS, DIR, 8>(so, x, b, sor, d, tpitch, first, nlines, sh.cap, st, zero, yc);
 		}
 	}
 	if (zero) {
@@ -889,7 +892,7 @@ static int launch_lines(const T *so, T *x, const T *b, const T *sor, Dims2 d, in
 
 template <typename T, int NS, int DIR>
 static int tune_dir(const T *so, T *x, const T *b, const T *sor, Dims2 d, int tpitch, cudaStream_t st,
-                    unsigned *ysync, bool pack)
+                    unsigned *ysync, const T *yc)
 {
 	const int n = DIR == CDR_DIR_X ? d.nx : d.ny;
 	const int nl = DIR == CDR_DIR_X ? d.ny : d.nx;
@@ -935,11 +938,11 @@ static int tune_dir(const T *so, T *x, const T *b, const T *sor, Dims2 d, int tp
 				break;
 			}
 			if (DIR == CDR_DIR_Y && ysync && d.nb == 1 && sh.pair) {  // both colours in one launch
-				rc = sh.K == 16 ? launch_ypair<T, NS, 16>(so, x, b, sor, d, tpitch, CDR_DOWN, sh.cap, ysync, st, false, pack)
-				                : launch_ypair<T, NS, 8>(so, x, b, sor, d, tpitch, CDR_DOWN, sh.cap, ysync, st, false, pack);
+				rc = sh.K == 16 ? launch_ypair<T, NS, 16>(so, x, b, sor, d, tpitch, CDR_DOWN, sh.cap, ysync, st, false, yc)
+				                : launch_ypair<T, NS, 8>(so, x, b, sor, d, tpitch, CDR_DOWN, sh.cap, ysync, st, false, yc);
 			} else {
 				for (int f = 1; f <= 2 && rc == CDR_OK; ++f)
-					rc = launch_lines<T, NS, DIR>(so, x, b, sor, d, tpitch, f, false, st, &sh, false, pack);
+					rc = launch_lines<T, NS, DIR>(so, x, b, sor, d, tpitch, f, false, st, &sh, false, yc);
 			}
 			if (rc != CDR_OK) break;
 			float t = 0.f;
@@ -989,19 +992,19 @@ static int tune_dir(const T *so, T *x, const T *b, const T *sor, Dims2 d, int tp
 
 template <typename T>
 int lines_autotune(const T *so, int nstencil, T *x, const T *b, const T *sor, Dims2 d, int tpitch, int dir,
-                   cudaStream_t st, unsigned *ysync, bool ypack)
+                   cudaStream_t st, unsigned *ysync, const T *ycpl)
 {
 	if (dir == CDR_DIR_X) {
-		if (nstencil == 5) return tune_dir<T, 5, CDR_DIR_X>(so, x, b, sor, d, tpitch, st, ysync, false);
-		return tune_dir<T, 3, CDR_DIR_X>(so, x, b, sor, d, tpitch, st, ysync, false);
+		if (nstencil == 5) return tune_dir<T, 5, CDR_DIR_X>(so, x, b, sor, d, tpitch, st, ysync, nullptr);
+		return tune_dir<T, 3, CDR_DIR_X>(so, x, b, sor, d, tpitch, st, ysync, nullptr);
 	}
-	if (nstencil == 5) return tune_dir<T, 5, CDR_DIR_Y>(so, x, b, sor, d, tpitch, st, ysync, ypack);
-	return tune_dir<T, 3, CDR_DIR_Y>(so, x, b, sor, d, tpitch, st, ysync, ypack);
+	if (nstencil == 5) return tune_dir<T, 5, CDR_DIR_Y>(so, x, b, sor, d, tpitch, st, ysync, ycpl);
+	return tune_dir<T, 3, CDR_DIR_Y>(so, x, b, sor, d, tpitch, st, ysync, ycpl);
 }
 template int lines_autotune<double>(const double *, int, double *, const double *, const double *, Dims2, int, int,
-                                    cudaStream_t, unsigned *, bool);
+                                    cudaStream_t, unsigned *, const double *);
 template int lines_autotune<float>(const float *, int, float *, const float *, const float *, Dims2, int, int,
-                                   cudaStream_t, unsigned *, bool);
+                                   cudaStream_t, unsigned *, const float *);
 
 bool lines_set_shape(int dir, int tsize, int ns, int n, int nl, int nb, LineShape sh)
 {
@@ -1026,7 +1029,7 @@ bool lines_shape(int dir, int tsize, int ns, int n, int nl, int nb, LineShape *o
 
 template <typename T>
 int relax_lines_2d(const T *so, int nstencil, T *x, const T *b, const T *sor, Dims2 d, int tpitch, int dir,
-                   int updown, int flags, cudaStream_t st, unsigned *ysync)
+                   int updown, int flags, cudaStream_t st, unsigned *ysync, const T *ycpl)
 {
 	const bool exact = (flags & CDR_LINES_EXACT) != 0;
 	bool zero = (flags & CDR_LINES_ZERO_START) != 0;
@@ -1035,6 +1038,13 @@ int relax_lines_2d(const T *so, int nstencil, T *x, const T *b, const T *sor, Di
 		// batch's problems, bstep planes apart)
 		CDR_CUDA_TRY(cudaMemset2DAsync(x, sizeof(T) * (size_t)d.bstep * d.plane(), 0, sizeof(T) * d.plane(), d.nb, st));
 		zero = false;
+	}
+	// packed y couplings: the caller's array, or (CDR_LINES_YPACKED, a single
+	// problem) the planes after the two factor planes of sor
+	const T *yc = nullptr;
+	if (dir == CDR_DIR_Y) {
+		if (ycpl) yc = ycpl;
+		else if ((flags & CDR_LINES_YPACKED) && d.nb == 1) yc = sor + 2 * (size_t)tpitch * (d.nx + 2);
 	}
 	const LineShape dflt = default_shape<T>(dir == CDR_DIR_X ? d.nx : d.ny, dir, d.nb);
 	const LineShape streamed{canon_K<T>(d.nx, CDR_DIR_X), FAST_BLOCK_X, 1};
@@ -1048,22 +1058,19 @@ int relax_lines_2d(const T *so, int nstencil, T *x, const T *b, const T *sor, Di
 		LineShape sh = force ? *force : shape_for<T>(d.ny, d.nx, nstencil, d.nb, dir);
 		if (!shape_ok<T>(sh, d.ny, dir)) sh = dflt;
 		if (shape_ok<T>(sh, d.ny, dir) && (sh.pair || (flags & CDR_LINES_YPAIR))) {
-			const bool pk = (flags & CDR_LINES_YPACKED) != 0;
 			if (sh.K == 16) {
 				if (nstencil == 5)
-					return launch_ypair<T, 5, 16>(so, x, b, sor, d, tpitch, updown, sh.cap, ysync, st, zero, pk);
-				return launch_ypair<T, 3, 16>(so, x, b, sor, d, tpitch, updown, sh.cap, ysync, st, zero, pk);
+					return launch_ypair<T, 5, 16>(so, x, b, sor, d, tpitch, updown, sh.cap, ysync, st, zero, yc);
+				return launch_ypair<T, 3, 16>(so, x, b, sor, d, tpitch, updown, sh.cap, ysync, st, zero, yc);
 			}
 			if (nstencil == 5)
-				return launch_ypair<T, 5, 8>(so, x, b, sor, d, tpitch, updown, sh.cap, ysync, st, zero, pk);
-			return launch_ypair<T, 3, 8>(so, x, b, sor, d, tpitch, updown, sh.cap, ysync, st, zero, pk);
+				return launch_ypair<T, 5, 8>(so, x, b, sor, d, tpitch, updown, sh.cap, ysync, st, zero, yc);
+			return launch_ypair<T, 3, 8>(so, x, b, sor, d, tpitch, updown, sh.cap, ysync, st, zero, yc);
 		}
 	}
 	// DOWN: lines with Fortran start index 3 (0-based even) first, then 2 (odd);
 	// UP: the opposite (relax_lines_x.f90:82-97).
 	const int firsts[2] = {updown == CDR_DOWN ? 2 : 1, updown == CDR_DOWN ? 1 : 2};
-	// y-lines of a single problem whose factor array carries the packed couplings
-	const bool pack = (flags & CDR_LINES_YPACKED) && dir == CDR_DIR_Y && d.nb == 1;
 	for (int c = 0; c < 2; ++c) {
 		const int f = firsts[c];
 		const bool z = zero && c == 0;  // the second colour reads the first's new lines only
@@ -1072,56 +1079,57 @@ int relax_lines_2d(const T *so, int nstencil, T *x, const T *b, const T *sor, Di
 			else CDR_TRY((launch_lines<T, 3, CDR_DIR_X>(so, x, b, sor, d, tpitch, f, exact, st, force, z)));
 		} else {
 			if (nstencil == 5)
-				CDR_TRY((launch_lines<T, 5, CDR_DIR_Y>(so, x, b, sor, d, tpitch, f, exact, st, force, z, pack)));
-			else CDR_TRY((launch_lines<T, 3, CDR_DIR_Y>(so, x, b, sor, d, tpitch, f, exact, st, force, z, pack)));
+				CDR_TRY((launch_lines<T, 5, CDR_DIR_Y>(so, x, b, sor, d, tpitch, f, exact, st, force, z, yc)));
+			else CDR_TRY((launch_lines<T, 3, CDR_DIR_Y>(so, x, b, sor, d, tpitch, f, exact, st, force, z, yc)));
 		}
 	}
 	return CDR_OK;
 }
 template int relax_lines_2d<double>(const double *, int, double *, const double *, const double *, Dims2, int, int,
-                                    int, int, cudaStream_t, unsigned *);
+                                    int, int, cudaStream_t, unsigned *, const double *);
 template int relax_lines_2d<float>(const float *, int, float *, const float *, const float *, Dims2, int, int, int,
-                                   int, cudaStream_t, unsigned *);
+                                   int, cudaStream_t, unsigned *, const float *);
 
 // ---------------------------------------------------- packed y-line couplings
-// For the y-line sweep of a single problem: after the two factor planes of a
-// level's y-line factor array (line-contiguous, tpitch), the couplings that
-// line i's right-hand side reads at position j, one plane each in line order:
-// w(i,j), w(i+1,j) [, sw(i,j), nw(i+1,j), nw(i,j+1), sw(i+1,j+1)] -- the
-// operands of relax_lines_y.f90:102-106 other than b and x.  The sweep then
-// reads them with vector loads of the line's own contiguous segments instead
-// of strided loads shared by the two colours.
+// For the y-line sweep: the couplings that line i's right-hand side reads at
+// position j, one plane each in line order (line-contiguous, tpitch, like the
+// transposed y factors): w(i,j), w(i+1,j) [, sw(i,j), nw(i+1,j), nw(i,j+1),
+// sw(i+1,j+1)] -- the operands of relax_lines_y.f90:102-106 other than b and
+// x.  The sweep then reads them with vector loads of the line's own
+// contiguous segments instead of strided loads shared by the two colours.
+// Problem z of a batch (bstep apart) at yc + z * bstep * planes * tpitch * (nx+2).
 template <typename T, int NS>
-__global__ void k_pack_ylines(const T *__restrict__ so, T *__restrict__ sor, Dims2 d, int tpitch)
+__global__ void k_pack_ylines(const T *__restrict__ so, T *__restrict__ yc, Dims2 d, int tpitch)
 {
 	const int j = blockIdx.x * blockDim.x + threadIdx.x + 1, i = blockIdx.y + 1;
 	if (j > d.ny || i > d.nx) return;
 	const size_t ps = d.plane(), fps = (size_t)tpitch * (d.nx + 2);
+	so += d.bofs(NS * ps);
+	yc += d.bofs((size_t)(NS == 5 ? 6 : 2) * fps);
 	const int P = d.pitch;
 	const size_t k = d.at(i, j), o = (size_t)i * tpitch + j;
-	T *c = sor + 2 * fps;
 	const T *w = so + ps;
-	c[o] = w[k];
-	c[fps + o] = w[k + 1];
+	yc[o] = w[k];
+	yc[fps + o] = w[k + 1];
 	if (NS == 5) {
 		const T *sw = so + 3 * ps, *nw = so + 4 * ps;
-		c[2 * fps + o] = sw[k];
-		c[3 * fps + o] = nw[k + 1];
-		c[4 * fps + o] = nw[k + P];
-		c[5 * fps + o] = sw[k + P + 1];
+		yc[2 * fps + o] = sw[k];
+		yc[3 * fps + o] = nw[k + 1];
+		yc[4 * fps + o] = nw[k + P];
+		yc[5 * fps + o] = sw[k + P + 1];
 	}
 }
 
 template <typename T>
-int pack_ylines_2d(const T *so, int nstencil, T *sor, Dims2 d, int tpitch, cudaStream_t st)
+int pack_ylines_2d(const T *so, int nstencil, T *yc, Dims2 d, int tpitch, cudaStream_t st)
 {
-	if (d.nb != 1 || tpitch < d.ny + 2) {
-		set_error(CDR_ERR_DIM, "packed y-line couplings: a single problem with tpitch >= ny+2");
+	if (tpitch < d.ny + 2) {
+		set_error(CDR_ERR_DIM, "packed y-line couplings: tpitch %d < ny+2", tpitch);
 		return CDR_ERR_DIM;
 	}
-	const dim3 g(ceil_div(d.ny, 256), d.nx);
-	if (nstencil == 5) k_pack_ylines<T, 5><<<g, 256, 0, st>>>(so, sor, d, tpitch);
-	else k_pack_ylines<T, 3><<<g, 256, 0, st>>>(so, sor, d, tpitch);
+	const dim3 g(ceil_div(d.ny, 256), d.nx, d.nb);
+	if (nstencil == 5) k_pack_ylines<T, 5><<<g, 256, 0, st>>>(so, yc, d, tpitch);
+	else k_pack_ylines<T, 3><<<g, 256, 0, st>>>(so, yc, d, tpitch);
 	CDR_LAUNCH_CHECK();
 	return CDR_OK;
 }

@@ -22,7 +22,7 @@ int lines_prepare();
 // per stream, since concurrent sweeps on it would race.
 template <typename T>
 int relax_lines_2d(const T *so, int nstencil, T *x, const T *b, const T *sor, Dims2 d, int tpitch, int dir,
-                   int updown, int flags, cudaStream_t st, unsigned *ysync = nullptr);
+                   int updown, int flags, cudaStream_t st, unsigned *ysync = nullptr, const T *ycpl = nullptr);
 size_t lines_sync_words(Dims2 d);
 // Launch shape of the line kernel (K elements per thread, y-line CTA cap) and
 // the setup-time autotuner that picks it per level (k2_lines.cu).  The tuner
@@ -47,15 +47,15 @@ int cg_inv_add_timeouts(unsigned n);
 int lines_stream_set_wait(unsigned long long ns);
 constexpr unsigned long long kStreamWaitDefaultNs = 200000000ull;  // kWaitLimitNs of k2_bulk.cuh
 int cg_inv_set_wait(unsigned long long ns);
-// The packed y-line couplings after the two factor planes of a level's y-line
-// factor array (2 + 2 (5-point) or 2 + 6 (9-point) planes of tpitch * (nx+2));
-// y sweeps with CDR_LINES_YPACKED read them.  A single problem.
+// The packed y-line couplings of a level: ypack_planes(nstencil) planes of
+// tpitch * (nx+2) per problem (d.nb problems, bstep apart), line-contiguous;
+// relax_lines_2d's y sweeps read them when given the array (ycpl).
 template <typename T>
-int pack_ylines_2d(const T *so, int nstencil, T *sor, Dims2 d, int tpitch, cudaStream_t st);
+int pack_ylines_2d(const T *so, int nstencil, T *yc, Dims2 d, int tpitch, cudaStream_t st);
 inline int ypack_planes(int nstencil) { return nstencil == 5 ? 6 : 2; }
 template <typename T>
 int lines_autotune(const T *so, int nstencil, T *x, const T *b, const T *sor, Dims2 d, int tpitch, int dir,
-                   cudaStream_t st, unsigned *ysync = nullptr, bool ypack = false);
+                   cudaStream_t st, unsigned *ysync = nullptr, const T *ycpl = nullptr);
 bool lines_shape(int dir, int tsize, int ns, int n, int nl, int nb, LineShape *out);
 // pin a shape for a line geometry (the autotuner then leaves it); false if the
 // shape cannot run lines of length n

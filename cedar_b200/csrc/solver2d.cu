@@ -45,6 +45,7 @@ struct Level {
 	// the operator (the difference form of its residual)
 	double *xw = nullptr;
 	bool ypk = false;  // the y-line factor arrays carry the packed couplings
+	size_t ysize() const { return 2 * (size_t)tpitch * (nx + 2); }  // the two y factor planes
 	float *dg32 = nullptr;
 };
 
@@ -170,7 +171,7 @@ int cdr_gpu_solver::smooth(int l, T *x, const T *b, int updown, bool zero)
 		CDR_CUDA_TRY(cudaMemsetAsync(x, 0, sizeof(T) * L.d.plane(), st));
 		zero = false;
 	}
-	const int yf = L.ypk ? CDR_LINES_YPACKED : 0;
+	const int yf = L.ypk ? CDR_LINES_YPACKED : 0;  // the packed couplings follow the y factors
 	for (int it = 0; it < n; ++it) {
 		// the first sweep of a zero iterate does not read it
 		const int f = lflags<T>() | (zero && it == 0 ? CDR_LINES_ZERO_START : 0);
@@ -471,7 +472,7 @@ int cdr_gpu_solver::tune_lines()
 			                          CDR_DIR_X, st));
 		if (ly)
 			CDR_TRY(lines_autotune<T>(Arr<T>::so(F), F.ns, Arr<T>::x(F), Arr<T>::b(F), Arr<T>::sory(F), F.d, F.tpitch,
-			                          CDR_DIR_Y, st, ysync, F.ypk));
+			                          CDR_DIR_Y, st, ysync, F.ypk ? Arr<T>::sory(F) + F.ysize() : nullptr));
 	}
 	return CDR_OK;
 }
@@ -506,7 +507,7 @@ int cdr_gpu_solver::setup()
 			CDR_TRY(setup_lines_2d<double>(F.so, F.ns, F.sory, F.d, F.tpitch, CDR_DIR_Y, info, st));
 			break;
 		}
-		if (F.ypk) CDR_TRY(pack_ylines_2d<double>(F.so, F.ns, F.sory, F.d, F.tpitch, st));
+		if (F.ypk) CDR_TRY(pack_ylines_2d<double>(F.so, F.ns, F.sory + F.ysize(), F.d, F.tpitch, st));
 	}
 	Level &Cg = lv[L() - 1];
 	if (per) CDR_TRY(setup_cg_per_2d(Cg.so, Cg.ns, Cg.d, abd, info + 1, per, st));
@@ -535,7 +536,7 @@ int cdr_gpu_solver::setup()
 				CDR_TRY(setup_lines_2d<float>(F.so, F.ns, F.sory32, F.d, F.tpitch, CDR_DIR_Y, info, st));
 				break;
 			}
-			if (F.ypk) CDR_TRY(pack_ylines_2d<float>(F.so32, F.ns, F.sory32, F.d, F.tpitch, st));
+			if (F.ypk) CDR_TRY(pack_ylines_2d<float>(F.so32, F.ns, F.sory32 + F.ysize(), F.d, F.tpitch, st));
 		}
 	}
 	int hinfo[2] = {0, 0};
