@@ -1066,13 +1066,106 @@ __global__ void __launch_bounds__(TX *TY) k_ir_residual(const double *__restrict
 	if (threadIdx.x == 0 && threadIdx.y == 0) partial[(size_t)blockIdx.z * gridDim.x + blockIdx.x] = s;
 }
 
+// The same step with two points per thread, i0 and i0 + 1 (i0 even, 16-byte
+// loads and stores along the rows; the neighbours beyond the pair as single
+// loads): k_ir_residual's operations on each point in its order, so xo and r32
+// are the same bits; the norm's partial sums run in another order.
+template <int NS>
+__global__ void __launch_bounds__(TX *TY) k_ir_residual_v(const double *__restrict__ so, const double *__restrict__ x,
+                                                          const float *__restrict__ e, const double *__restrict__ b,
+                                                          double *__restrict__ xo, float *__restrict__ r32, Dims2 d,
+                                                          Dims2 d32, double *__restrict__ partial, int apply,
+                                                          const int *__restrict__ active)
+{
+	__shared__ double sh[TX * TY / 32];
+	const int tiles_x = (d.nx + 2 * TX) / (2 * TX);  // pairs (0,1), (2,3), ... up to nx
+	const int ntiles = tiles_x * ((d.ny + TY - 1) / TY);
+	const size_t ps = d.plane();
+	const int p = d.pitch, p32 = d32.pitch;
+	so += d.bofs(NS * ps);
+	x += d.bofs(ps);
+	b += d.bofs(ps);
+	xo += d.bofs(ps);
+	e += d32.bofs(d32.plane());
+	r32 += d32.bofs(d32.plane());
+	if (active && !active[blockIdx.z * d.bstep]) apply = 0;
+	const double *c = so, *w = so + ps, *s = so + 2 * ps, *sw = so + (NS == 5 ? 3 : 0) * ps,
+	             *nw = so + (NS == 5 ? 4 : 0) * ps;
+	auto ld2 = [](const double *q) { return *reinterpret_cast<const double2 *>(q); };
+	double acc = 0.0;
+	for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+		const int i0 = (t % tiles_x) * 2 * TX + 2 * threadIdx.x;
+		const int j = (t / tiles_x) * TY + threadIdx.y + 1;
+		if (i0 > d.nx || j > d.ny) continue;
+		const bool v0 = i0 >= 1, v1 = i0 + 1 <= d.nx;  // the pair's points inside the grid
+		const size_t k = d.at(i0, j), k32 = d32.at(i0, j);
+		// x (+ e) at columns i0 - 1 .. i0 + 2 of rows j - 1, j, j + 1
+		double xn[3][4];
+#pragma unroll
+		for (int dj = -1; dj <= 1; ++dj) {
+			const size_t kr = k + (long)dj * p, kr32 = k32 + (long)dj * p32;
+			const double2 m = ld2(x + kr);
+			double v[4] = {v0 ? x[kr - 1] : 0.0, m.x, m.y, v1 ? x[kr + 2] : 0.0};
+			if (apply) {
+				const float2 em = *reinterpret_cast<const float2 *>(e + kr32);
+				v[0] = v0 ? v[0] + (double)e[kr32 - 1] : 0.0;
+				v[1] = v[1] + (double)em.x;
+				v[2] = v[2] + (double)em.y;
+				v[3] = v1 ? v[3] + (double)e[kr32 + 2] : 0.0;
+			}
+#pragma unroll
+			for (int q = 0; q < 4; ++q) xn[dj + 1][q] = v[q];
+		}
+		const double2 cc = ld2(c + k), bb = ld2(b + k), ww = ld2(w + k), s0 = ld2(s + k), s1 = ld2(s + k + p);
+		const double w2 = v1 ? w[k + 2] : 0.0;
+		double rr[2];
+		if (NS == 5) {
+			const double2 sw0 = ld2(sw + k), sw1 = ld2(sw + k + p), nw0 = ld2(nw + k), nw1 = ld2(nw + k + p);
+			const double sw12 = v1 ? sw[k + p + 2] : 0.0, nw02 = v1 ? nw[k + 2] : 0.0;
+			// point i0 (column index 1 of xn), then i0 + 1 (index 2)
+			rr[0] = bb.x + ww.x * xn[1][0] + ww.y * xn[1][2] + s0.x * xn[0][1] + s1.x * xn[2][1] + sw0.x * xn[0][0] +
+			        nw0.y * xn[0][2] + nw1.x * xn[2][0] + sw1.y * xn[2][2] - cc.x * xn[1][1];
+			rr[1] = bb.y + ww.y * xn[1][1] + w2 * xn[1][3] + s0.y * xn[0][2] + s1.y * xn[2][2] + sw0.y * xn[0][1] +
+			        nw02 * xn[0][3] + nw1.y * xn[2][1] + sw12 * xn[2][3] - cc.y * xn[1][2];
+		} else {
+			rr[0] = bb.x + ww.x * xn[1][0] + ww.y * xn[1][2] + s0.x * xn[0][1] + s1.x * xn[2][1] - cc.x * xn[1][1];
+			rr[1] = bb.y + ww.y * xn[1][1] + w2 * xn[1][3] + s0.y * xn[0][2] + s1.y * xn[2][2] - cc.y * xn[1][2];
+		}
+		if (v0 && v1) {
+			acc += rr[0] * rr[0];
+			acc += rr[1] * rr[1];
+			*reinterpret_cast<float2 *>(r32 + k32) = make_float2((float)rr[0], (float)rr[1]);
+			*reinterpret_cast<double2 *>(xo + k) = make_double2(xn[1][1], xn[1][2]);
+		} else if (v0) {
+			acc += rr[0] * rr[0];
+			r32[k32] = (float)rr[0];
+			xo[k] = xn[1][1];
+		} else if (v1) {
+			acc += rr[1] * rr[1];
+			r32[k32 + 1] = (float)rr[1];
+			xo[k + 1] = xn[1][2];
+		}
+	}
+	double sum = block_sum<TX * TY / 32>(acc, sh);
+	if (threadIdx.x == 0 && threadIdx.y == 0) partial[(size_t)blockIdx.z * gridDim.x + blockIdx.x] = sum;
+}
+
 int ir_residual_2d(const double *so, int nstencil, const double *x, const float *e, const double *b, double *xo,
                    float *r32, Dims2 d, Dims2 d32, double *norm_out, double *partial, int apply, cudaStream_t st,
                    const int *active)
 {
 	const int nb = norm_blocks(d);
 	const dim3 grd(nb, 1, d.nb);
-	if (nstencil == 5)
+	// pairs of points along 16-byte rows where the pitches allow it
+	const bool vec = d.pitch % 2 == 0 && d32.pitch % 2 == 0 && (d.bstep * d.plane()) % 2 == 0 &&
+	                 (d32.bstep * d32.plane()) % 2 == 0 &&
+	                 ((uintptr_t)so | (uintptr_t)x | (uintptr_t)b | (uintptr_t)xo) % 16 == 0 &&
+	                 ((uintptr_t)e | (uintptr_t)r32) % 8 == 0;
+	if (vec && nstencil == 5)
+		k_ir_residual_v<5><<<grd, dim3(TX, TY), 0, st>>>(so, x, e, b, xo, r32, d, d32, partial, apply, active);
+	else if (vec)
+		k_ir_residual_v<3><<<grd, dim3(TX, TY), 0, st>>>(so, x, e, b, xo, r32, d, d32, partial, apply, active);
+	else if (nstencil == 5)
 		k_ir_residual<5><<<grd, dim3(TX, TY), 0, st>>>(so, x, e, b, xo, r32, d, d32, partial, apply, active);
 	else
 		k_ir_residual<3><<<grd, dim3(TX, TY), 0, st>>>(so, x, e, b, xo, r32, d, d32, partial, apply, active);
