@@ -62,10 +62,21 @@ __global__ void k3_plane_copy(T *__restrict__ x3, Dims3 F, int dir, int first, i
 	else x3[k3] = x2[k2];
 }
 
+template <typename T, bool TO_PLANE>
+__global__ void __launch_bounds__(TX *TY) k3_plane_copy_yz(T *__restrict__ x3, Dims3 F, int first, int step,
+                                                           int count, T *__restrict__ x2, int n1, int n2, int pitch2);
+
 template <typename T>
 int plane_copy(T *x3, Dims3 F, int dir, int first, int step, int count, T *x2, int n1, int n2, int pitch2,
                bool to_plane, cudaStream_t st)
 {
+	if (dir == 2) {  // yz planes: through a shared-memory transpose
+		const dim3 grd(ceil_div(count, TX), ceil_div(n1 + 2, TX), n2 + 2);
+		if (to_plane) k3_plane_copy_yz<T, true><<<grd, dim3(TX, TY), 0, st>>>(x3, F, first, step, count, x2, n1, n2, pitch2);
+		else k3_plane_copy_yz<T, false><<<grd, dim3(TX, TY), 0, st>>>(x3, F, first, step, count, x2, n1, n2, pitch2);
+		CDR_LAUNCH_CHECK();
+		return CDR_OK;
+	}
 	const dim3 grd(ceil_div(n1 + 2, TX), ceil_div(n2 + 2, TY), count);
 	if (to_plane) k3_plane_copy<T, true><<<grd, dim3(TX, TY), 0, st>>>(x3, F, dir, first, step, x2, n1, n2, pitch2);
 	else k3_plane_copy<T, false><<<grd, dim3(TX, TY), 0, st>>>(x3, F, dir, first, step, x2, n1, n2, pitch2);
@@ -142,10 +153,97 @@ __global__ void __launch_bounds__(TX *TY) k3_plane_rhs(const T *__restrict__ so,
 	b2[(size_t)(ipl - 1) * pitch2 * (n2 + 2) + (size_t)q * pitch2 + p] = v;
 }
 
+// yz planes (fixed i): the 3D arrays run along i, across the planes, and the
+// planes' 2D arrays along j.  A CTA takes 32 planes of the colour x 32 j at one
+// k: it forms (rhs) or reads the values with consecutive threads on
+// consecutive planes, and writes them through a shared-memory transpose with
+// consecutive threads on consecutive j (and the reverse for the copy back).
+// The same values as the kernels above, moved in coalesced rows.
+template <typename T, int NS>
+__global__ void __launch_bounds__(TX *TY) k3_plane_rhs_yz(const T *__restrict__ so, const T *__restrict__ x,
+                                                          const T *__restrict__ bb, Dims3 F, int first, int step,
+                                                          int count, T *__restrict__ b2, int n1, int n2, int pitch2)
+{
+	__shared__ T tile[TX][TX + 1];
+	const int z0 = blockIdx.x * TX, a0 = blockIdx.y * TX + 1, q = blockIdx.z + 1;
+	const size_t P = F.plane();
+#define X3(a, i, j, k) a[o3(F, i, j, k)]
+#define S3(pl, i, j, k) so[(size_t)((pl)-1) * P + o3(F, i, j, k)]
+	for (int r = threadIdx.y; r < TX; r += TY) {
+		const int zi = z0 + threadIdx.x, p = a0 + r;
+		if (zi >= count || p > n1) continue;
+		const int j = p, k = q, i = first + 1 + zi * step;
+		T v;
+		if (NS == 4) {
+			v = X3(bb, i, j, k) + S3(KPW, i, j, k) * X3(x, i - 1, j, k) + S3(KPW, i + 1, j, k) * X3(x, i + 1, j, k);
+		} else {
+			v = X3(bb, i, j, k) + S3(KPNW, i, j + 1, k) * X3(x, i - 1, j + 1, k) + S3(KPW, i, j, k) * X3(x, i - 1, j, k)
+			    + S3(KPSW, i, j, k) * X3(x, i - 1, j - 1, k) + S3(KBNW, i, j + 1, k) * X3(x, i - 1, j + 1, k - 1)
+			    + S3(KBW, i, j, k) * X3(x, i - 1, j, k - 1) + S3(KBSW, i, j, k) * X3(x, i - 1, j - 1, k - 1)
+			    + S3(KBSE, i, j + 1, k + 1) * X3(x, i - 1, j + 1, k + 1) + S3(KBE, i, j, k + 1) * X3(x, i - 1, j, k + 1)
+			    + S3(KBNE, i, j, k + 1) * X3(x, i - 1, j - 1, k + 1) + S3(KPSW, i + 1, j + 1, k) * X3(x, i + 1, j + 1, k)
+			    + S3(KPW, i + 1, j, k) * X3(x, i + 1, j, k) + S3(KPNW, i + 1, j, k) * X3(x, i + 1, j - 1, k)
+			    + S3(KBNE, i + 1, j + 1, k) * X3(x, i + 1, j + 1, k - 1) + S3(KBE, i + 1, j, k) * X3(x, i + 1, j, k - 1)
+			    + S3(KBSE, i + 1, j, k) * X3(x, i + 1, j - 1, k - 1)
+			    + S3(KBSW, i + 1, j + 1, k + 1) * X3(x, i + 1, j + 1, k + 1)
+			    + S3(KBW, i + 1, j, k + 1) * X3(x, i + 1, j, k + 1) + S3(KBNW, i + 1, j, k + 1) * X3(x, i + 1, j - 1, k + 1);
+		}
+		tile[threadIdx.x][r] = v;
+	}
+#undef X3
+#undef S3
+	__syncthreads();
+	for (int r = threadIdx.y; r < TX; r += TY) {
+		const int zi = z0 + r, p = a0 + threadIdx.x;
+		if (zi >= count || p > n1) continue;
+		const int ipl = first + 1 + zi * step;
+		b2[(size_t)(ipl - 1) * pitch2 * (n2 + 2) + (size_t)q * pitch2 + p] = tile[r][threadIdx.x];
+	}
+}
+
+template <typename T, bool TO_PLANE>
+__global__ void __launch_bounds__(TX *TY) k3_plane_copy_yz(T *__restrict__ x3, Dims3 F, int first, int step,
+                                                           int count, T *__restrict__ x2, int n1, int n2, int pitch2)
+{
+	__shared__ T tile[TX][TX + 1];
+	const int z0 = blockIdx.x * TX, a0 = blockIdx.y * TX, b = blockIdx.z;
+	const size_t pl2 = (size_t)pitch2 * (n2 + 2);
+	// 3D side: consecutive threads on consecutive planes (i); plane side:
+	// consecutive threads on consecutive a (j)
+	if (TO_PLANE) {
+		for (int r = threadIdx.y; r < TX; r += TY) {
+			const int zi = z0 + threadIdx.x, a = a0 + r;
+			if (zi < count && a <= n1 + 1) tile[threadIdx.x][r] = x3[o3(F, first + 1 + zi * step, a, b)];
+		}
+		__syncthreads();
+		for (int r = threadIdx.y; r < TX; r += TY) {
+			const int zi = z0 + r, a = a0 + threadIdx.x;
+			if (zi < count && a <= n1 + 1) x2[(size_t)(first + zi * step) * pl2 + (size_t)b * pitch2 + a] = tile[r][threadIdx.x];
+		}
+	} else {
+		for (int r = threadIdx.y; r < TX; r += TY) {
+			const int zi = z0 + r, a = a0 + threadIdx.x;
+			if (zi < count && a <= n1 + 1) tile[r][threadIdx.x] = x2[(size_t)(first + zi * step) * pl2 + (size_t)b * pitch2 + a];
+		}
+		__syncthreads();
+		for (int r = threadIdx.y; r < TX; r += TY) {
+			const int zi = z0 + threadIdx.x, a = a0 + r;
+			if (zi < count && a <= n1 + 1) x3[o3(F, first + 1 + zi * step, a, b)] = tile[threadIdx.x][r];
+		}
+	}
+}
+
 template <typename T>
 int plane_rhs(const T *so, const T *x, const T *b, Dims3 F, int dir, int first, int step, int count, T *b2, int n1,
               int n2, int pitch2, cudaStream_t st, int ns)
 {
+	if (dir == 2) {
+		const dim3 grd(ceil_div(count, TX), ceil_div(n1, TX), n2);
+		if (ns == 4) k3_plane_rhs_yz<T, 4><<<grd, dim3(TX, TY), 0, st>>>(so, x, b, F, first, step, count, b2, n1, n2, pitch2);
+		else k3_plane_rhs_yz<T, 14><<<grd, dim3(TX, TY), 0, st>>>(so, x, b, F, first, step, count, b2, n1, n2, pitch2);
+		CDR_LAUNCH_CHECK();
+		return CDR_OK;
+	}
 	const dim3 grd(ceil_div(n1, TX), ceil_div(n2, TY), count);
 	if (ns == 4) k3_plane_rhs<T, 4><<<grd, dim3(TX, TY), 0, st>>>(so, x, b, F, dir, first, step, b2, n1, n2, pitch2);
 	else k3_plane_rhs<T, 14><<<grd, dim3(TX, TY), 0, st>>>(so, x, b, F, dir, first, step, b2, n1, n2, pitch2);
