@@ -311,6 +311,7 @@ static int create3(cdr_gpu_solver3 *h, const double *so_src, int src_pitch, cuda
 			s2.maxiter = 1;
 			s2.precision = s.precision;
 			s2.line_flags = s.line_flags;
+			s2.fuse_coarse = s.fuse_coarse;  // the planes' coarse levels fused as the caller asks
 			const int np = dir == 0 ? L.nz : dir == 1 ? L.ny : L.nx;
 			const int n1 = dir == 2 ? L.ny : L.nx, n2 = dir == 0 ? L.ny : L.nz;
 			L.pl[dir].reset(new Batch2());
