@@ -205,6 +205,9 @@ __device__ void cc_lines(const CoarseLevel<T> &L, int updown, T *sm)
 	const T *fac = DIR == CDR_DIR_X ? L.sor : L.sory;
 	const size_t eplane = DIR == CDR_DIR_X ? ps : (size_t)L.tpitch * (L.nx + 2);
 	const int firsts[2] = {updown == CDR_DOWN ? 2 : 1, updown == CDR_DOWN ? 1 : 2};
+	// x of position m (0-based) of line lc: the solves write their lines' x
+	// directly (lines of one colour read only lines of the other)
+	auto xat = [&](int lc, int m) -> size_t { return DIR == CDR_DIR_X ? d.at(m + 1, lc) : d.at(lc, m + 1); };
 	for (int c = 0; c < 2; ++c) {
 		const int first = firsts[c];
 		const int ml = first > nl ? 0 : (nl - first) / 2 + 1;  // lines of this colour
@@ -233,10 +236,10 @@ __device__ void cc_lines(const CoarseLevel<T> &L, int updown, T *sm)
 					r[m] = y;
 				}
 				T xv = pivot_div(y, dd[n]);
-				r[n - 1] = xv;
+				L.x[xat(lc, n - 1)] = xv;
 				for (int m = n - 2; m >= 0; --m) {
 					xv = pivot_div(r[m], dd[m + 1]) - xv * ee[m + 2];
-					r[m] = xv;
+					L.x[xat(lc, m)] = xv;
 				}
 			}
 		} else {
@@ -284,17 +287,12 @@ __device__ void cc_lines(const CoarseLevel<T> &L, int updown, T *sm)
 				if (lane == 31) xv = T(0);
 				for (int m = hi - 1; m >= lo; --m) {
 					xv = m == n - 1 ? r[m] : madd(-xv, ee[m + 2], r[m]);
-					r[m] = xv;
+					L.x[xat(lc, m)] = xv;
 				}
 				__syncwarp();
 			}
 		}
-		__syncthreads();
-		if (DIR == CDR_DIR_X)
-			cc_rows(0, n - 1, 0, ml - 1, [&](int m, int g) { L.x[d.at(m + 1, first + 2 * g)] = R[g * n + m]; });
-		else
-			cc_rows(0, ml - 1, 0, n - 1, [&](int g, int m) { L.x[d.at(first + 2 * g, m + 1)] = R[g * n + m]; });
-		__syncthreads();
+		__syncthreads();  // this colour's lines are written into x
 	}
 }
 
