@@ -212,17 +212,17 @@ __device__ void cc_lines(const CoarseLevel<T> &L, int updown, T *sm)
 		const int first = firsts[c];
 		const int ml = first > nl ? 0 : (nl - first) / 2 + 1;  // lines of this colour
 		T *R = sm;
-		// rows over warps, lanes along the rows of the level (lines for y, positions for x)
-		if (DIR == CDR_DIR_X)
-			cc_rows(0, n - 1, 0, ml - 1, [&](int m, int g) {
-				R[g * n + m] = line_rhs<T, NS, DIR>(L.so, ps, L.x, L.b, d.at(m + 1, first + 2 * g), L.pitch);
-			});
-		else
-			cc_rows(0, ml - 1, 0, n - 1, [&](int g, int m) {
-				R[g * n + m] = line_rhs<T, NS, DIR>(L.so, ps, L.x, L.b, d.at(first + 2 * g, m + 1), L.pitch);
-			});
-		__syncthreads();
 		if constexpr (sizeof(T) == 8) {
+			// rows over warps, lanes along the rows of the level (lines for y, positions for x)
+			if (DIR == CDR_DIR_X)
+				cc_rows(0, n - 1, 0, ml - 1, [&](int m, int g) {
+					R[g * n + m] = line_rhs<T, NS, DIR>(L.so, ps, L.x, L.b, d.at(m + 1, first + 2 * g), L.pitch);
+				});
+			else
+				cc_rows(0, ml - 1, 0, n - 1, [&](int g, int m) {
+					R[g * n + m] = line_rhs<T, NS, DIR>(L.so, ps, L.x, L.b, d.at(first + 2 * g, m + 1), L.pitch);
+				});
+			__syncthreads();
 			// FP64: DPTTS2's sequential substitutions, one thread per line
 			if (threadIdx.x < ml) {
 				const int lc = first + 2 * threadIdx.x;
@@ -252,6 +252,10 @@ __device__ void cc_lines(const CoarseLevel<T> &L, int updown, T *sm)
 				const T *dd = fac + (DIR == CDR_DIR_X ? (size_t)lc * L.pitch : (size_t)lc * L.tpitch);
 				const T *ee = dd + eplane;
 				T *r = R + g * n;
+				// the line's right-hand sides by its own warp (the other warps solve
+				// lines of the same colour, which this line does not read)
+				for (int m = lane; m < n; m += 32) r[m] = line_rhs<T, NS, DIR>(L.so, ps, L.x, L.b, xat(lc, m), L.pitch);
+				__syncwarp();
 				const int lo = lane * cs < n ? lane * cs : n, hi = lo + cs < n ? lo + cs : n;
 				// forward y(m) = r(m) - y(m-1) E(m+1), y(0) = r(0)
 				T A = T(1), B = T(0);
