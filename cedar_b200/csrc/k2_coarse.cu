@@ -190,9 +190,10 @@ __device__ void cc_gs(const CoarseLevel<T> &L, int updown)
 }
 
 // One zebra line sweep (both colours, relax_lines_2d's order).  Each colour:
-// the right-hand sides of its lines are formed by all threads into sm, then the
+// each line's warp forms its right-hand sides into sm (the other warps solve
+// lines of the same colour, which this line does not read), then the
 // substitutions run with the level's (shared-memory) pivots and multipliers:
-// DPTTS2's sequential order in FP64 (one thread per line), affine-map scans over
+// DPTTS2's sequential order in FP64 (one warp per line), affine-map scans over
 // the lanes of one warp per line in FP32 (the preconditioner has no bitwise
 // target; the separate FP32 kernels scan too).
 template <typename T, int NS, int DIR>
@@ -213,34 +214,65 @@ __device__ void cc_lines(const CoarseLevel<T> &L, int updown, T *sm)
 		const int ml = first > nl ? 0 : (nl - first) / 2 + 1;  // lines of this colour
 		T *R = sm;
 		if constexpr (sizeof(T) == 8) {
-			// rows over warps, lanes along the rows of the level (lines for y, positions for x)
-			if (DIR == CDR_DIR_X)
-				cc_rows(0, n - 1, 0, ml - 1, [&](int m, int g) {
-					R[g * n + m] = line_rhs<T, NS, DIR>(L.so, ps, L.x, L.b, d.at(m + 1, first + 2 * g), L.pitch);
-				});
-			else
-				cc_rows(0, ml - 1, 0, n - 1, [&](int g, int m) {
-					R[g * n + m] = line_rhs<T, NS, DIR>(L.so, ps, L.x, L.b, d.at(first + 2 * g, m + 1), L.pitch);
-				});
-			__syncthreads();
-			// FP64: DPTTS2's sequential substitutions, one thread per line
-			if (threadIdx.x < ml) {
-				const int lc = first + 2 * threadIdx.x;
+			// FP64: DPTTS2's sequential substitutions, one warp per line: the
+			// line's right-hand sides and the quotients of the backward
+			// substitution (which do not depend on its recurrence) by all lanes,
+			// the two recurrences by lane 0, four positions per step with their
+			// operands loaded ahead of the arithmetic
+			const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+			for (int g = warp; g < ml; g += CC_THREADS / 32) {
+				const int lc = first + 2 * g;
 				// factors of position p at dd[p], ee[p] (position 1 is r[0])
 				const T *dd = fac + (DIR == CDR_DIR_X ? (size_t)lc * L.pitch : (size_t)lc * L.tpitch);
 				const T *ee = dd + eplane;
-				T *r = R + threadIdx.x * n;
-				T y = r[0];
-				for (int m = 1; m < n; ++m) {
-					y = r[m] - y * ee[m + 1];
-					r[m] = y;
+				T *r = R + g * n;
+				for (int m = lane; m < n; m += 32) r[m] = line_rhs<T, NS, DIR>(L.so, ps, L.x, L.b, xat(lc, m), L.pitch);
+				__syncwarp();
+				if (lane == 0) {  // y(m) = r(m) - y(m-1) e(m+1), y(0) = r(0)
+					T y = r[0];
+					int m = 1;
+					for (; m + 3 < n; m += 4) {
+						const T e0 = ee[m + 1], e1 = ee[m + 2], e2 = ee[m + 3], e3 = ee[m + 4];
+						const T a0 = r[m], a1 = r[m + 1], a2 = r[m + 2], a3 = r[m + 3];
+						y = a0 - y * e0;
+						r[m] = y;
+						y = a1 - y * e1;
+						r[m + 1] = y;
+						y = a2 - y * e2;
+						r[m + 2] = y;
+						y = a3 - y * e3;
+						r[m + 3] = y;
+					}
+					for (; m < n; ++m) {
+						y = r[m] - y * ee[m + 1];
+						r[m] = y;
+					}
 				}
-				T xv = pivot_div(y, dd[n]);
-				L.x[xat(lc, n - 1)] = xv;
-				for (int m = n - 2; m >= 0; --m) {
-					xv = pivot_div(r[m], dd[m + 1]) - xv * ee[m + 2];
-					L.x[xat(lc, m)] = xv;
+				__syncwarp();
+				for (int m = lane; m < n; m += 32) r[m] = pivot_div(r[m], dd[m + 1]);
+				__syncwarp();
+				if (lane == 0) {  // x(m) = y(m)/d(m+1) - x(m+1) e(m+2), x(n-1) = y(n-1)/d(n)
+					T xv = r[n - 1];
+					L.x[xat(lc, n - 1)] = xv;
+					int m = n - 2;
+					for (; m >= 3; m -= 4) {
+						const T e0 = ee[m + 2], e1 = ee[m + 1], e2 = ee[m], e3 = ee[m - 1];
+						const T q0 = r[m], q1 = r[m - 1], q2 = r[m - 2], q3 = r[m - 3];
+						xv = q0 - xv * e0;
+						L.x[xat(lc, m)] = xv;
+						xv = q1 - xv * e1;
+						L.x[xat(lc, m - 1)] = xv;
+						xv = q2 - xv * e2;
+						L.x[xat(lc, m - 2)] = xv;
+						xv = q3 - xv * e3;
+						L.x[xat(lc, m - 3)] = xv;
+					}
+					for (; m >= 0; --m) {
+						xv = r[m] - xv * ee[m + 2];
+						L.x[xat(lc, m)] = xv;
+					}
 				}
+				__syncwarp();
 			}
 		} else {
 			// FP32: one warp per line, each lane a chunk of consecutive positions;
