@@ -128,6 +128,36 @@ __device__ void cc_copy(const T *__restrict__ src, int sp, size_t splane, T *__r
 	}
 }
 
+// The same copy from global into shared memory by asynchronous copies
+// (cp.async, one element each, consecutive threads on consecutive elements of
+// the flattened planes and rows): every load of the staging is in flight at
+// once instead of one row per warp at a time; cc_stage_wait completes them.
+template <typename T>
+__device__ __forceinline__ void cp_async_elem(T *dst_smem, const T *src)
+{
+	const unsigned d = (unsigned)__cvta_generic_to_shared(dst_smem);
+	if constexpr (sizeof(T) == 8)
+		asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(src) : "memory");
+	else
+		asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(d), "l"(src) : "memory");
+}
+
+template <typename T>
+__device__ void cc_stage(const T *__restrict__ src, int sp, size_t splane, T *__restrict__ dst, int dp,
+                         size_t dplane, int rowlen, int rows, int nplanes)
+{
+	const int per = rowlen * rows, total = per * nplanes;
+	for (int e = threadIdx.x; e < total; e += CC_THREADS) {
+		const int q = e / per, rem = e - q * per, j = rem / rowlen, i = rem - j * rowlen;
+		cp_async_elem(dst + (size_t)q * dplane + (size_t)j * dp + i, src + (size_t)q * splane + (size_t)j * sp + i);
+	}
+}
+
+__device__ __forceinline__ void cc_stage_wait()
+{
+	asm volatile("cp.async.wait_all;\n" ::: "memory");
+}
+
 template <typename T>
 __device__ void cc_fill(T *p, size_t n)
 {
@@ -423,18 +453,19 @@ __global__ void __launch_bounds__(CC_THREADS) k_coarse_cycle(CoarseCycle<T> cc)
 		const size_t gpl = (size_t)G.pitch * (G.ny + 2), spl = (size_t)S.pitch * (S.ny + 2);
 		const int ii = G.nx + 2, jj = G.ny + 2;
 		if (l < nl - 1) {
-			cc_copy<T>(G.so, G.pitch, gpl, const_cast<T *>(S.so), S.pitch, spl, ii, jj, G.ns);
-			if (S.sor) cc_copy<T>(G.sor, G.pitch, gpl, const_cast<T *>(S.sor), S.pitch, spl, ii, jj, cc_sor_planes(cc.relax));
+			cc_stage<T>(G.so, G.pitch, gpl, const_cast<T *>(S.so), S.pitch, spl, ii, jj, G.ns);
+			if (S.sor) cc_stage<T>(G.sor, G.pitch, gpl, const_cast<T *>(S.sor), S.pitch, spl, ii, jj, cc_sor_planes(cc.relax));
 			if (S.sory)  // transposed: nx+2 rows of ny+2 elements
-				cc_copy<T>(G.sory, G.tpitch, (size_t)G.tpitch * ii, const_cast<T *>(S.sory), S.tpitch,
-				           (size_t)S.tpitch * ii, jj, ii, 2);
+				cc_stage<T>(G.sory, G.tpitch, (size_t)G.tpitch * ii, const_cast<T *>(S.sory), S.tpitch,
+				            (size_t)S.tpitch * ii, jj, ii, 2);
 			cc_fill(S.r, spl);
 		}
-		if (l > 0) cc_copy<T>(G.ci, G.pitch, gpl, const_cast<T *>(S.ci), S.pitch, spl, ii, jj, 8);
-		if (l == 0) cc_copy<T>(G.b, G.pitch, gpl, S.b, S.pitch, spl, ii, jj, 1);
+		if (l > 0) cc_stage<T>(G.ci, G.pitch, gpl, const_cast<T *>(S.ci), S.pitch, spl, ii, jj, 8);
+		if (l == 0) cc_stage<T>(G.b, G.pitch, gpl, S.b, S.pitch, spl, ii, jj, 1);
 		else cc_fill(S.b, spl);
 		cc_fill(S.x, spl);
 	}
+	cc_stage_wait();
 	__syncthreads();
 	for (int l = 0; l + 1 < nl; ++l) {
 		const CoarseLevel<T> F = cc_view(cc, l, base), C = cc_view(cc, l + 1, base);
