@@ -383,15 +383,14 @@ __device__ void cc_smooth(const CoarseCycle<T> &cc, const CoarseLevel<T> &L, int
 	}
 }
 
-// BMG2_SymStd_SOLVE_cg with DPBTRS('U') on the coarsest level: the factor and
-// the right-hand side staged in shared memory (xs, then the factor), the
-// substitutions by one thread (k_cg_solve's operations)
+// BMG2_SymStd_SOLVE_cg with DPBTRS('U') on the coarsest level: the right-hand
+// side in shared memory (xs) and the factor after it (staged with the levels),
+// the substitutions by one thread (k_cg_solve's operations)
 template <typename T>
-__device__ void cc_cg(const double *__restrict__ ab, const CoarseLevel<T> &L, double *xs)
+__device__ void cc_cg(const CoarseLevel<T> &L, double *xs)
 {
 	const int ldab = L.nx + 2, kd = L.nx + 1, n = L.nx * L.ny;
-	double *abs = xs + n;
-	for (int e = threadIdx.x; e < ldab * n; e += CC_THREADS) abs[e] = ab[e];
+	const double *abs = xs + n;
 	cc_rows(1, L.nx, 1, L.ny, [&](int i, int j) { xs[(j - 1) * L.nx + i - 1] = (double)L.b[(size_t)j * L.pitch + i]; });
 	__syncthreads();
 	if (threadIdx.x == 0) {
@@ -465,6 +464,11 @@ __global__ void __launch_bounds__(CC_THREADS) k_coarse_cycle(CoarseCycle<T> cc)
 		else cc_fill(S.b, spl);
 		cc_fill(S.x, spl);
 	}
+	{  // the coarsest level's band factor, after its right-hand side xs
+		const CoarseLevel<T> &Cg = cc.lv[nl - 1];
+		const int n = Cg.nx * Cg.ny, nab = (Cg.nx + 2) * n;
+		cc_stage<double>(cc.abd + (size_t)blockIdx.x * cc.bstep * nab, 0, 0, xs + n, 0, 0, nab, 1, 1);
+	}
 	cc_stage_wait();
 	__syncthreads();
 	for (int l = 0; l + 1 < nl; ++l) {
@@ -480,8 +484,7 @@ __global__ void __launch_bounds__(CC_THREADS) k_coarse_cycle(CoarseCycle<T> cc)
 	}
 	{
 		const CoarseLevel<T> Cg = cc_view(cc, nl - 1, base);
-		const size_t nab = (size_t)(Cg.nx + 2) * Cg.nx * Cg.ny;
-		cc_cg<T>(cc.abd + (size_t)blockIdx.x * cc.bstep * nab, Cg, xs);
+		cc_cg<T>(Cg, xs);
 		__syncthreads();
 	}
 	for (int l = nl - 2; l >= 0; --l) {
