@@ -371,13 +371,10 @@ __device__ void cc_smooth(const CoarseCycle<T> &cc, const CoarseLevel<T> &L, int
 		case CDR_RELAX_POINT: cc_gs<T, NS>(L, updown); break;
 		case CDR_RELAX_LINE_X: cc_lines<T, NS, CDR_DIR_X>(L, updown, sm); break;
 		case CDR_RELAX_LINE_Y: cc_lines<T, NS, CDR_DIR_Y>(L, updown, sm); break;
-		default:
-			if (updown == CDR_DOWN) {
-				cc_lines<T, NS, CDR_DIR_X>(L, updown, sm);
-				cc_lines<T, NS, CDR_DIR_Y>(L, updown, sm);
-			} else {
-				cc_lines<T, NS, CDR_DIR_Y>(L, updown, sm);
-				cc_lines<T, NS, CDR_DIR_X>(L, updown, sm);
+		default:  // x then y down, y then x up: one copy of each direction's code
+			for (int h = 0; h < 2; ++h) {
+				if ((h == 0) == (updown == CDR_DOWN)) cc_lines<T, NS, CDR_DIR_X>(L, updown, sm);
+				else cc_lines<T, NS, CDR_DIR_Y>(L, updown, sm);
 			}
 		}
 	}
@@ -471,29 +468,40 @@ __global__ void __launch_bounds__(CC_THREADS) k_coarse_cycle(CoarseCycle<T> cc)
 	}
 	cc_stage_wait();
 	__syncthreads();
-	for (int l = 0; l + 1 < nl; ++l) {
-		const CoarseLevel<T> F = cc_view(cc, l, base), C = cc_view(cc, l + 1, base);
-		if (F.ns == 5) cc_smooth<T, 5>(cc, F, CDR_DOWN, sm);
-		else cc_smooth<T, 3>(cc, F, CDR_DOWN, sm);
-		if (F.ns == 5) cc_residual<T, 5>(F);
-		else cc_residual<T, 3>(F);
-		__syncthreads();
-		cc_restrict<T>(F, C);
-		cc_fill(C.x, (size_t)C.pitch * (C.ny + 2));
+	// The cycle as one sequence of steps (down: smooth, residual, restriction,
+	// and the coarsest solve after the last; up: interpolation, smooth), so that
+	// the code of each kind of step exists once: the first fetch of a code
+	// region from instruction memory costs several microseconds, and separate
+	// copies for the two legs paid it twice.
+	if (nl == 1) {
+		cc_cg<T>(cc_view(cc, 0, base), xs);
 		__syncthreads();
 	}
-	{
-		const CoarseLevel<T> Cg = cc_view(cc, nl - 1, base);
-		cc_cg<T>(Cg, xs);
-		__syncthreads();
-	}
-	for (int l = nl - 2; l >= 0; --l) {
+	for (int step = 0; step < 2 * (nl - 1); ++step) {
+		const bool down = step < nl - 1;
+		const int l = down ? step : 2 * (nl - 1) - 1 - step;
 		const CoarseLevel<T> F = cc_view(cc, l, base), C = cc_view(cc, l + 1, base);
-		cc_interp<T>(F, C);
-		__syncthreads();
-		if (F.ns == 5) cc_smooth<T, 5>(cc, F, CDR_UP, sm);
-		else cc_smooth<T, 3>(cc, F, CDR_UP, sm);
-		__syncthreads();
+		if (!down) {
+			cc_interp<T>(F, C);
+			__syncthreads();
+		}
+		const int updown = down ? CDR_DOWN : CDR_UP;
+		if (F.ns == 5) cc_smooth<T, 5>(cc, F, updown, sm);
+		else cc_smooth<T, 3>(cc, F, updown, sm);
+		if (down) {
+			if (F.ns == 5) cc_residual<T, 5>(F);
+			else cc_residual<T, 3>(F);
+			__syncthreads();
+			cc_restrict<T>(F, C);
+			cc_fill(C.x, (size_t)C.pitch * (C.ny + 2));
+			__syncthreads();
+			if (l == nl - 2) {
+				cc_cg<T>(cc_view(cc, nl - 1, base), xs);
+				__syncthreads();
+			}
+		} else {
+			__syncthreads();
+		}
 	}
 	{
 		const CoarseLevel<T> G = cc_global(cc, 0), S = cc_view(cc, 0, base);
