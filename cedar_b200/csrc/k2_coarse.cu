@@ -147,8 +147,11 @@ __device__ void cc_stage(const T *__restrict__ src, int sp, size_t splane, T *__
                          size_t dplane, int rowlen, int rows, int nplanes)
 {
 	const int per = rowlen * rows, total = per * nplanes;
+	// quotients by FP64 reciprocals: (e + 1/2) / d lies at least 1/(2d) from an
+	// integer, far beyond the product's rounding error, so the truncation is exact
+	const double ip = 1.0 / per, ir = 1.0 / rowlen;
 	for (int e = threadIdx.x; e < total; e += CC_THREADS) {
-		const int q = e / per, rem = e - q * per, j = rem / rowlen, i = rem - j * rowlen;
+		const int q = (int)((e + 0.5) * ip), rem = e - q * per, j = (int)((rem + 0.5) * ir), i = rem - j * rowlen;
 		cp_async_elem(dst + (size_t)q * dplane + (size_t)j * dp + i, src + (size_t)q * splane + (size_t)j * sp + i);
 	}
 }
@@ -391,18 +394,74 @@ __device__ void cc_cg(const CoarseLevel<T> &L, double *xs)
 	cc_rows(1, L.nx, 1, L.ny, [&](int i, int j) { xs[(j - 1) * L.nx + i - 1] = (double)L.b[(size_t)j * L.pitch + i]; });
 	__syncthreads();
 	if (threadIdx.x == 0) {
-		for (int j = 0; j < n; ++j) {
-			double temp = xs[j];
-			const int i0 = j - kd > 0 ? j - kd : 0;
-			for (int i = i0; i < j; ++i) temp = temp - abs[(size_t)j * ldab + kd + i - j] * xs[i];
-			xs[j] = temp / abs[(size_t)j * ldab + kd];
-		}
-		for (int j = n - 1; j >= 0; --j) {
-			if (xs[j] != 0.0) {
-				xs[j] = xs[j] / abs[(size_t)j * ldab + kd];
-				const double temp = xs[j];
-				const int i1 = j - kd > 0 ? j - kd : 0;
-				for (int i = j - 1; i >= i1; --i) xs[i] = xs[i] - temp * abs[(size_t)j * ldab + kd + i - j];
+		constexpr int KW = 6;
+		if (kd < KW) {
+			// the same operations in the same order, the band's last KW entries of
+			// xs in registers (w[t] = xs[j - KW + t]) and each row's multipliers
+			// loaded ahead of the recurrence
+			double w[KW];
+#pragma unroll
+			for (int t = 0; t < KW; ++t) w[t] = 0.0;
+			for (int j = 0; j < n; ++j) {
+				const double *arow = abs + (size_t)j * ldab + kd - j;  // arow[i]: row j, column i
+				double a[KW];
+#pragma unroll
+				for (int t = 0; t < KW; ++t) {
+					const int i = j - KW + t;
+					a[t] = i >= 0 && i >= j - kd ? arow[i] : 0.0;
+				}
+				double temp = xs[j];
+#pragma unroll
+				for (int t = 0; t < KW; ++t) {
+					const int i = j - KW + t;
+					if (i >= 0 && i >= j - kd) temp = temp - a[t] * w[t];
+				}
+				const double v = temp / abs[(size_t)j * ldab + kd];
+				xs[j] = v;
+#pragma unroll
+				for (int t = 0; t < KW - 1; ++t) w[t] = w[t + 1];
+				w[KW - 1] = v;
+			}
+			// backward: cur = xs[j] with the updates of the rows below applied,
+			// w[t] = xs[j - KW + t] pending
+#pragma unroll
+			for (int t = 0; t < KW; ++t) {
+				const int i = n - 1 - KW + t;
+				w[t] = i >= 0 ? xs[i] : 0.0;
+			}
+			double cur = xs[n - 1];
+			for (int j = n - 1; j >= 0; --j) {
+				if (cur != 0.0) {
+					cur = cur / abs[(size_t)j * ldab + kd];
+					const double temp = cur;
+					const double *arow = abs + (size_t)j * ldab + kd - j;
+#pragma unroll
+					for (int t = KW - 1; t >= 0; --t) {
+						const int i = j - KW + t;
+						if (i >= 0 && i >= j - kd) w[t] = w[t] - temp * arow[i];
+					}
+				}
+				xs[j] = cur;
+				cur = w[KW - 1];
+#pragma unroll
+				for (int t = KW - 1; t >= 1; --t) w[t] = w[t - 1];
+				const int i = j - 1 - KW;  // no row at or below j updates it
+				w[0] = i >= 0 ? xs[i] : 0.0;
+			}
+		} else {
+			for (int j = 0; j < n; ++j) {
+				double temp = xs[j];
+				const int i0 = j - kd > 0 ? j - kd : 0;
+				for (int i = i0; i < j; ++i) temp = temp - abs[(size_t)j * ldab + kd + i - j] * xs[i];
+				xs[j] = temp / abs[(size_t)j * ldab + kd];
+			}
+			for (int j = n - 1; j >= 0; --j) {
+				if (xs[j] != 0.0) {
+					xs[j] = xs[j] / abs[(size_t)j * ldab + kd];
+					const double temp = xs[j];
+					const int i1 = j - kd > 0 ? j - kd : 0;
+					for (int i = j - 1; i >= i1; --i) xs[i] = xs[i] - temp * abs[(size_t)j * ldab + kd + i - j];
+				}
 			}
 		}
 	}
